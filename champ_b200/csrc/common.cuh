@@ -1,0 +1,508 @@
+// common.cuh — device-side building blocks of the walker engine.
+//
+// System constants live in __constant__ memory (every lane of a warp reads
+// the same centre/type parameters in lock-step, so constant-cache broadcast
+// is the right home).  Large tables (radial splines, LCAO coefficients) live
+// in global memory and stay L2-resident.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define CW_MAX_CENT 512
+#define CW_MAX_TYPES 8
+#define CW_MAX_RWF 16
+#define CW_MAX_TERMS 64
+#define CW_MAX_NORD 7
+#define CW_MAX_QUAD 86
+#define CW_MAX_ELEC 1024
+
+// ---------------------------------------------------------------------------
+// Constant-memory system description
+// ---------------------------------------------------------------------------
+struct CSys {
+  int N, nup, ndn, M, nctype, K, Oa, nmax;
+  int norda, nordb, nordc, isc, nspin2b, nocuspb, nterms;
+  int nloc, nquad;
+  double scalek, asymp_r, asymp_jasb[2];
+  double deltar, deltat, fbias, pecent, cdet;
+  int mrwf, mpts, mbastyp;
+  // per centre
+  double cent[CW_MAX_CENT * 3];
+  int iwctype[CW_MAX_CENT];
+  int ao_first[CW_MAX_CENT + 1];
+  // per type
+  double znuc[CW_MAX_TYPES];
+  int nrbas[CW_MAX_TYPES], igrid[CW_MAX_TYPES], nr[CW_MAX_TYPES], nbastyp[CW_MAX_TYPES];
+  double arg[CW_MAX_TYPES], r0[CW_MAX_TYPES];
+  double rmaxwf[CW_MAX_TYPES * CW_MAX_RWF];
+  double ce[CW_MAX_TYPES * CW_MAX_RWF * 5];
+  double ae[CW_MAX_TYPES * CW_MAX_RWF * 2];
+  double a4[CW_MAX_TYPES * (CW_MAX_NORD + 1)];
+  double b[2 * (CW_MAX_NORD + 1)];
+  double c[CW_MAX_TYPES * CW_MAX_TERMS];
+  double asymp_jasa[CW_MAX_TYPES];
+  // ECP
+  int lpot[CW_MAX_TYPES];
+  int necp_term[CW_MAX_TYPES * 4];
+  int necp_power[CW_MAX_TYPES * 4 * 16];
+  double ecp_exponent[CW_MAX_TYPES * 4 * 16];
+  double ecp_coef[CW_MAX_TYPES * 4 * 16];
+  double xq0[CW_MAX_QUAD], yq0[CW_MAX_QUAD], zq0[CW_MAX_QUAD], wq[CW_MAX_QUAD];
+};
+
+// the one system block of the engine translation unit
+__constant__ CSys cs;
+
+// Global-memory tables of the system.
+struct GSys {
+  const double *rwf, *d2rwf;      // [nctype][mrwf][mpts]
+  const int *iwlbas, *iwrwf;      // [nctype][mbastyp]
+  const double *coefT;            // [K][Oa]  (active orbitals)
+  const int *slot_orb;            // [2][nmax] active-orbital index of Slater column j, spin s
+};
+
+// ---------------------------------------------------------------------------
+// Per-walker state (walker-major; component planes so lanes over electrons
+// coalesce).
+// ---------------------------------------------------------------------------
+struct WState {
+  int W;
+  double *x;          // [W][3][N]
+  uint64_t *rng;      // [W][4]
+  double *xq;         // [W][3][nquad] rotated quadrature
+  double *rmino;      // [W][N]
+  int *nearesto;      // [W][N]
+  double *rvmino;     // [W][3][N]
+  double *psido, *psijo, *psi2o, *eold, *ekino;   // [W]
+  double *slmi;       // [W][2][nmax*nmax]   slmi(j + nel*(i)) per spin
+  double *detiab;     // [W][2]
+  double *orbs;       // [W][N][nmax]   Slater-column orbital values of electron e
+  double *dorbs;      // [W][3][N][nmax]
+  double *fso;        // [W][N][N] symmetric pair values, diagonal = e-n term
+  double *fijo;       // [W][3][N][N] fijo(k,i,j) -> [k][i][j]
+  double *fjo;        // [W][3][N]
+  double *fsumo;      // [W]
+  // estimators [W][8]: wsum esum pesum tpbsum acc ecum1s ecm21s (spare)
+  double *sums;
+  int *status;        // [W] nonzero: singular matrix / NaN
+};
+
+// Scratch of one single-electron move.
+struct MoveScratch {
+  double xnew[3];
+  double rvminn[3];
+  double rminn, rminon, rminno, delttn, fxop, areao, rratio;
+  int nearestn, igeo;
+  double rvminon[3];
+  double pad;
+};
+
+struct MoveBuf {
+  MoveScratch *ms;    // [W]
+  double *fsn;        // [W][N]      new pair value of (iel,j); [iel] = e-n term
+  double *fijn_i;     // [W][3][N]   grad wrt iel of pair (iel,j)
+  double *fijn_j;     // [W][3][N]   grad wrt j of pair (iel,j)
+  double *fsumn;      // [W]
+  double *vjn;        // [W][3]
+  double *phi;        // [W][4][K]  basis at xnew (value, dx, dy, dz)
+  double *orbn;       // [W][4][Oa]
+};
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// xoshiro256** (CHAMP vmc/xoroshiro256starstar.c next / next_uniform_double)
+struct DRng {
+  uint64_t s0, s1, s2, s3;
+  __device__ __forceinline__ uint64_t next() {
+    const uint64_t r1 = s1 * 5;
+    const uint64_t result = ((r1 << 7) | (r1 >> 57)) * 9;
+    const uint64_t t = s1 << 17;
+    s2 ^= s0;
+    s3 ^= s1;
+    s1 ^= s2;
+    s0 ^= s3;
+    s2 ^= t;
+    s3 = (s3 << 45) | (s3 >> 19);
+    return result;
+  }
+  __device__ __forceinline__ double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }
+  __device__ void load(const uint64_t *p) { s0 = p[0]; s1 = p[1]; s2 = p[2]; s3 = p[3]; }
+  __device__ void store(uint64_t *p) const { p[0] = s0; p[1] = s1; p[2] = s2; p[3] = s3; }
+};
+
+// ---------------------------------------------------------------------------
+// scale_dist family (vmc/scale_dist.f90:57-353)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T scale0(T r) {
+  const T k = (T)cs.scalek;
+  if (cs.scalek == 0) return r;
+  if (cs.isc == 2) return (T(1) - exp(-k * r)) / k;
+  if (cs.isc == 3) {
+    T rsc = k * r, rsc2 = rsc * rsc, rsc3 = rsc * rsc2;
+    return (T(1) - exp(-rsc - T(0.5) * rsc2 - (T(1) / T(3)) * rsc3)) / k;
+  }
+  if (cs.isc == 4) return r * (T(1) / (T(1) + k * r));
+  return r * (T(1) / pow(T(1) + pow(k * r, T(3)), T(1) / T(3)));
+}
+template <typename T>
+__device__ __forceinline__ void scale2(T r, T &rr, T &dd1, T &dd2) {
+  const T k = (T)cs.scalek;
+  if (cs.scalek == 0) { rr = r; dd1 = 1; dd2 = 0; return; }
+  if (cs.isc == 2) {
+    rr = (T(1) - exp(-k * r)) / k;
+    dd1 = T(1) - k * rr;
+    dd2 = -k * dd1;
+  } else if (cs.isc == 3) {
+    T rsc = k * r, rsc2 = rsc * rsc, rsc3 = rsc * rsc2;
+    T e = exp(-rsc - T(0.5) * rsc2 - (T(1) / T(3)) * rsc3);
+    rr = (T(1) - e) / k;
+    dd1 = (T(1) + rsc + rsc2) * e;
+    dd2 = -k * rsc2 * (T(3) + T(2) * rsc + rsc2) * e;
+  } else if (cs.isc == 4) {
+    T deni = T(1) / (T(1) + k * r);
+    rr = r * deni;
+    dd1 = deni * deni;
+    dd2 = -T(2) * k * deni * dd1;
+  } else {
+    T deni = T(1) / pow(T(1) + pow(k * r, T(3)), T(1) / T(3));
+    rr = r * deni;
+    dd1 = deni * deni * deni * deni;
+    dd2 = -T(4) * (k * r) * (k * r) * k * dd1 * dd1 / deni;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// e-e-n polynomial of jastrow4 / jastrow4e / psinl: the (n,k,l,m) term table
+// unrolled at compile time for a given order.
+//   MODE 0: value only, 1: value + first derivs, 2: + second derivs
+// ---------------------------------------------------------------------------
+template <typename T>
+struct EenOut { T fc, fu, fuu, fi, fii, fj, fjj, fui, fuj; };
+
+template <int NORD, int MODE, typename T>
+__device__ __forceinline__ EenOut<T> een_poly(const T *__restrict__ cc, T u1, T ri1, T rj1) {
+  T uu[NORD + 1], rri[NORD + 1], rrj[NORD + 1], ss[NORD + 1], tt[NORD + 1];
+  uu[0] = 1; rri[0] = 1; rrj[0] = 1; ss[0] = 2; tt[0] = 1;
+#pragma unroll
+  for (int p = 1; p <= NORD; p++) {
+    uu[p] = (p == 1) ? u1 : uu[1] * uu[p - 1];
+    rri[p] = (p == 1) ? ri1 : rri[1] * rri[p - 1];
+    rrj[p] = (p == 1) ? rj1 : rrj[1] * rrj[p - 1];
+    ss[p] = rri[p] + rrj[p];
+    tt[p] = rri[p] * rrj[p];
+  }
+  EenOut<T> e{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int ll = 0;
+#pragma unroll
+  for (int n = 2; n <= NORD; n++) {
+#pragma unroll
+    for (int k = n - 1; k >= 0; k--) {
+      const int l_hi = (k == 0) ? n - k - 2 : n - k;
+#pragma unroll
+      for (int l = l_hi; l >= 0; l--) {
+        const int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) {
+          const T c = cc[ll];
+          ll++;
+          const T ukm = (k >= 1) ? uu[k - 1] : T(0);
+          const T st = ss[l] * tt[m];
+          e.fc += c * uu[k] * st;
+          if (MODE >= 1) {
+            e.fu += c * T(k) * ukm * st;
+            const T gi = T(l + m) * ((l + m >= 1) ? rri[l + m - 1] : T(0)) * rrj[m] +
+                         T(m) * ((m >= 1) ? rri[m - 1] : T(0)) * rrj[l + m];
+            const T gj = T(l + m) * ((l + m >= 1) ? rrj[l + m - 1] : T(0)) * rri[m] +
+                         T(m) * ((m >= 1) ? rrj[m - 1] : T(0)) * rri[l + m];
+            e.fi += c * uu[k] * gi;
+            e.fj += c * uu[k] * gj;
+            if (MODE >= 2) {
+              e.fuu += c * T(k * (k - 1)) * ((k >= 2) ? uu[k - 2] : T(0)) * st;
+              e.fii += c * uu[k] *
+                       (T((l + m) * (l + m - 1)) * ((l + m >= 2) ? rri[l + m - 2] : T(0)) * rrj[m] +
+                        T(m * (m - 1)) * ((m >= 2) ? rri[m - 2] : T(0)) * rrj[l + m]);
+              e.fjj += c * uu[k] *
+                       (T((l + m) * (l + m - 1)) * ((l + m >= 2) ? rrj[l + m - 2] : T(0)) * rri[m] +
+                        T(m * (m - 1)) * ((m >= 2) ? rrj[m - 2] : T(0)) * rri[l + m]);
+              e.fui += c * T(k) * ukm * gi;
+              e.fuj += c * T(k) * ukm * gj;
+            }
+          }
+        }
+      }
+    }
+  }
+  return e;
+}
+
+// Padé + polynomial e-e term (jastrow4.f90 ee part) at scaled u:
+// returns fee, d fee/du, d2 fee/du2 (MODE>=2)
+template <int MODE, typename T>
+__device__ __forceinline__ void ee_term(int isb, int ipar, T sspinn, T u, T &fee, T &feeu, T &feeuu) {
+  const int nb = cs.nordb + 1;
+  T b0 = (T)cs.b[isb * nb + 0], b1 = (T)cs.b[isb * nb + 1];
+  T top = sspinn * b0 * u, topu = sspinn * b0;
+  T bot = T(1) + b1 * u, botu = b1, bot2 = bot * bot;
+  fee = top / bot - (T)cs.asymp_jasb[ipar];
+  feeu = topu / bot - botu * top / bot2;
+  if (MODE >= 2) feeuu = (-(T(2) * botu * topu) / bot + T(2) * botu * botu * top / bot2) / bot;
+  T up = u;  // u^(iord-1)
+  T upm = 1; // u^(iord-2)
+  for (int iord = 2; iord <= cs.nordb; iord++) {
+    T bc = (T)cs.b[isb * nb + iord];
+    T uord = up * u;
+    fee += bc * uord;
+    feeu += bc * T(iord) * up;
+    if (MODE >= 2) feeuu += bc * T(iord * (iord - 1)) * upm;
+    upm = up;
+    up = uord;
+  }
+}
+
+// Padé + polynomial e-n term (jastrow4.f90 en part) at scaled r
+template <int MODE, typename T>
+__device__ __forceinline__ void en_term(int it, T r, T &fen, T &feni, T &fenii) {
+  const int na = cs.norda + 1;
+  T a0 = (T)cs.a4[it * na + 0], a1 = (T)cs.a4[it * na + 1];
+  T top = a0 * r, topi = a0;
+  T bot = T(1) + a1 * r, boti = a1, bot2 = bot * bot;
+  fen = top / bot - (T)cs.asymp_jasa[it];
+  feni = topi / bot - boti * top / bot2;
+  if (MODE >= 2) fenii = (-(T(2) * boti * topi) / bot + T(2) * boti * boti * top / bot2) / bot;
+  T rp = r, rpm = 1;
+  for (int iord = 2; iord <= cs.norda; iord++) {
+    T ac = (T)cs.a4[it * na + iord];
+    T rord = rp * r;
+    fen += ac * rord;
+    feni += ac * T(iord) * rp;
+    if (MODE >= 2) fenii += ac * T(iord * (iord - 1)) * rpm;
+    rpm = rp;
+    rp = rord;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// splfit (vmc/splfit.f90:3-94)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void splfit_d(const GSys &g, double r, int irb, int it, double *wfv, int ider) {
+  const int ig = cs.igrid[it];
+  const double arg = cs.arg[it], r0 = cs.r0[it];
+  double xr, ref0, ref1, delh;
+  int jx;
+  if (ig == 1) {
+    xr = (r - r0) / arg + 1;
+    jx = (int)xr;
+    ref0 = r0 + arg * (jx - 1);
+    ref1 = ref0 + arg;
+    delh = arg;
+  } else if (ig == 2) {
+    double dlrad0 = log(r0), dlogag = log(arg);
+    xr = (log(r) - dlrad0) / dlogag + 1;
+    jx = (int)xr;
+    ref0 = r0 * pow(arg, (double)(jx - 1));
+    ref1 = ref0 * arg;
+    delh = ref1 - ref0;
+  } else {
+    double dlogag = log(arg);
+    xr = (log((r + r0) / r0)) / dlogag + 1.0;
+    jx = (int)xr;
+    ref0 = r0 * pow(arg, (double)(jx - 1)) - r0;
+    ref1 = (ref0 + r0) * arg - r0;
+    delh = ref1 - ref0;
+  }
+  const int tb = irb + cs.mrwf * it;
+  if (jx < 1) {
+    const double *ce = &cs.ce[(it * CW_MAX_RWF + irb) * 5];
+    const double rpow[5] = {1.0, r, r * r, r * r * r, r * r * r * r};
+    double v = ce[0];
+    for (int ii = 2; ii <= 5; ii++) v += ce[ii - 1] * rpow[ii - 1];
+    wfv[0] = v;
+    if (ider >= 1) {
+      double p1 = 0, p2 = 0, p3 = 0;
+      for (int ii = 2; ii <= 5; ii++) {
+        const double c = ce[ii - 1];
+        p1 += (ii - 1) * c * rpow[ii - 2];
+        if (ii >= 3) p2 += (ii - 1) * (ii - 2) * c * rpow[ii - 3];
+        if (ii >= 4) p3 += (ii - 1) * (ii - 2) * (ii - 3) * c * rpow[ii - 4];
+      }
+      wfv[1] = p1; wfv[2] = p2; wfv[3] = p3;
+    }
+  } else if (jx >= cs.nr[it]) {
+    const double *ae = &cs.ae[(it * CW_MAX_RWF + irb) * 2];
+    wfv[0] = ae[0] * exp(-ae[1] * r);
+    if (ider >= 1) {
+      wfv[1] = -ae[1] * wfv[0];
+      wfv[2] = -ae[1] * wfv[1];
+      wfv[3] = -ae[1] * wfv[2];
+    }
+  } else {
+    const double *y = g.rwf + (size_t)tb * cs.mpts;
+    const double *y2 = g.d2rwf + (size_t)tb * cs.mpts;
+    const double y0 = __ldg(y + jx - 1), y1 = __ldg(y + jx);
+    const double d0 = __ldg(y2 + jx - 1), d1 = __ldg(y2 + jx);
+    const double sixth = 1.0 / 6.0;
+    const double delhi = 1.0 / delh;
+    const double bb = (r - ref0) * delhi;
+    const double aa = (ref1 - r) * delhi;
+    const double cc = aa * (aa * aa - 1.0) * delh * delh * sixth;
+    const double dd = bb * (bb * bb - 1.0) * delh * delh * sixth;
+    wfv[0] = aa * y0 + bb * y1 + cc * d0 + dd * d1;
+    if (ider >= 1) {
+      wfv[1] = (y1 - y0) * delhi + (-(3.0 * aa * aa - 1.0) * d0 + (3.0 * bb * bb - 1.0) * d1) * delh * sixth;
+      wfv[2] = aa * d0 + bb * d1;
+      wfv[3] = (-d0 + d1) * delhi;
+    }
+  }
+}
+
+// Slm (vmc/slm.f90): monomial exponents and constants of index l (1-based).
+__device__ __forceinline__ void slm_def(int l, int &a, int &b, int &c, double &k) {
+  const double CS_ = 0.28209479177387814, CP_ = 0.48860251190291992, CD1 = 0.630783130505040,
+               CD2 = 1.092548430592079, CF_ = 0.74635266518023078, CF2 = 1.66889529453113635,
+               CF3 = 2.89061144264055405, CG_ = 0.8462843753216345, CG2 = 2.2390579955406924,
+               CG3 = 2.890611442640554, CG4 = 5.006685883593409;
+  switch (l) {
+    case 1: a = 0; b = 0; c = 0; k = CS_; break;
+    case 2: a = 1; b = 0; c = 0; k = CP_; break;
+    case 3: a = 0; b = 1; c = 0; k = CP_; break;
+    case 4: a = 0; b = 0; c = 1; k = CP_; break;
+    case 5: a = 2; b = 0; c = 0; k = CD1; break;
+    case 6: a = 1; b = 1; c = 0; k = CD2; break;
+    case 7: a = 1; b = 0; c = 1; k = CD2; break;
+    case 8: a = 0; b = 2; c = 0; k = CD1; break;
+    case 9: a = 0; b = 1; c = 1; k = CD2; break;
+    case 10: a = 0; b = 0; c = 2; k = CD1; break;
+    case 11: a = 3; b = 0; c = 0; k = CF_; break;
+    case 12: a = 2; b = 1; c = 0; k = CF2; break;
+    case 13: a = 2; b = 0; c = 1; k = CF2; break;
+    case 14: a = 1; b = 2; c = 0; k = CF2; break;
+    case 15: a = 1; b = 1; c = 1; k = CF3; break;
+    case 16: a = 1; b = 0; c = 2; k = CF2; break;
+    case 17: a = 0; b = 3; c = 0; k = CF_; break;
+    case 18: a = 0; b = 2; c = 1; k = CF2; break;
+    case 19: a = 0; b = 1; c = 2; k = CF2; break;
+    case 20: a = 0; b = 0; c = 3; k = CF_; break;
+    case 21: a = 4; b = 0; c = 0; k = CG_; break;
+    case 22: a = 3; b = 1; c = 0; k = CG2; break;
+    case 23: a = 3; b = 0; c = 1; k = CG2; break;
+    case 24: a = 2; b = 2; c = 0; k = CG3; break;
+    case 25: a = 2; b = 1; c = 1; k = CG4; break;
+    case 26: a = 2; b = 0; c = 2; k = CG3; break;
+    case 27: a = 1; b = 3; c = 0; k = CG2; break;
+    case 28: a = 1; b = 2; c = 1; k = CG4; break;
+    case 29: a = 1; b = 1; c = 2; k = CG4; break;
+    case 30: a = 1; b = 0; c = 3; k = CG2; break;
+    case 31: a = 0; b = 4; c = 0; k = CG_; break;
+    case 32: a = 0; b = 3; c = 1; k = CG2; break;
+    case 33: a = 0; b = 2; c = 2; k = CG3; break;
+    case 34: a = 0; b = 1; c = 3; k = CG2; break;
+    default: a = 0; b = 0; c = 4; k = CG_; break;
+  }
+}
+__device__ __forceinline__ double ipw(double x, int n) {
+  double r = 1;
+  for (int i = 0; i < n; i++) r *= x;
+  return r;
+}
+__device__ __forceinline__ void slm_eval(int l, double x, double y, double z, double &v, double *dv, double &lap) {
+  int a, b, c;
+  double k;
+  slm_def(l, a, b, c, k);
+  double px = ipw(x, a), py = ipw(y, b), pz = ipw(z, c);
+  v = k * px * py * pz;
+  dv[0] = a ? k * a * ipw(x, a - 1) * py * pz : 0.0;
+  dv[1] = b ? k * b * px * ipw(y, b - 1) * pz : 0.0;
+  dv[2] = c ? k * c * px * py * ipw(z, c - 1) : 0.0;
+  lap = 0;
+  if (a >= 2) lap += k * a * (a - 1) * ipw(x, a - 2) * py * pz;
+  if (b >= 2) lap += k * b * (b - 1) * px * ipw(y, b - 2) * pz;
+  if (c >= 2) lap += k * c * (c - 1) * px * py * ipw(z, c - 2);
+}
+
+// basis_fns + phi_combine for one centre: writes the AOs of centre ic at
+// displacement xc (= x - cent).  out(m, d) receives value (d=0), gradient
+// (d=1..3, ider>=1) and Laplacian (d=4, ider>=2).
+template <typename Store>
+__device__ __forceinline__ void basis_centre(const GSys &g, int ic, const double *xc, int ider, Store out) {
+  const int it = cs.iwctype[ic];
+  const double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
+  const double ri = 1.0 / r;
+  double wfv[CW_MAX_RWF][4];
+  const int nrb = cs.nrbas[it];
+  for (int irb = 0; irb < nrb; irb++) {
+    if (r <= cs.rmaxwf[it * CW_MAX_RWF + irb]) {
+      splfit_d(g, r, irb, it, wfv[irb], ider);
+    } else {
+      wfv[irb][0] = wfv[irb][1] = wfv[irb][2] = wfv[irb][3] = 0.0;
+    }
+  }
+  const int nbt = cs.nbastyp[it];
+  const int m0 = cs.ao_first[ic];
+  const double xcri[3] = {xc[0] * ri, xc[1] * ri, xc[2] * ri};
+  for (int ib = 0; ib < nbt; ib++) {
+    const int l = __ldg(g.iwlbas + it * cs.mbastyp + ib);
+    const int irb = __ldg(g.iwrwf + it * cs.mbastyp + ib) - 1;
+    double y, dy[3], lap;
+    slm_eval(l, xc[0], xc[1], xc[2], y, dy, lap);
+    const double *w = wfv[irb];
+    out(m0 + ib, 0, y * w[0]);
+    if (ider >= 1) {
+      double dum = 0;
+      for (int jj = 0; jj < 3; jj++) {
+        out(m0 + ib, 1 + jj, y * xcri[jj] * w[1] + dy[jj] * w[0]);
+        dum += dy[jj] * xcri[jj];
+      }
+      if (ider >= 2) {
+        double d2 = y * w[2] + y * 2.0 * ri * w[1] + lap * w[0];
+        d2 += 2.0 * dum * w[1];
+        out(m0 + ib, 4, d2);
+      }
+    }
+  }
+}
+
+// gauss_pot (vmc/readps_gauss.f90:57): channel l is CHAMP's 1-based index
+__device__ __forceinline__ double gauss_pot_d(double r, int l, int ict) {
+  double v = 0, rsq = r * r;
+  const int base = (ict * 4 + (l - 1)) * 16;
+  const int nt = cs.necp_term[ict * 4 + (l - 1)];
+  for (int i = 0; i < nt; i++) {
+    int pw = cs.necp_power[base + i];
+    double p = (pw != 2) ? pow(r, (double)(pw - 2)) : 1.0;
+    double ex = cs.ecp_exponent[base + i];
+    double e = (ex * rsq > 7.0e2) ? 0.0 : cs.ecp_coef[base + i] * exp(-ex * rsq);
+    v += p * e;
+  }
+  return v;
+}
+
+__device__ __forceinline__ double yl0_d(int l, double costh) {
+  if (l == 1) return 1.0;
+  if (l == 2) return 3.0 * costh;
+  if (l == 3) return 2.5 * (3 * costh * costh - 1);
+  return 3.5 * (5 * costh * costh * costh - 3 * costh);
+}
+
+// pair spin classification of jastrow4 (isb, ipar, sspinn) for i > j
+__device__ __forceinline__ void pair_spin(int i, int j, int &isb, int &ipar, double &sspinn) {
+  sspinn = 1;
+  isb = 0;
+  ipar = 0;
+  if (i < cs.nup || j >= cs.nup) {
+    if (cs.nspin2b == 2) isb = 1;
+    else if (cs.nocuspb == 0) sspinn = 0.5;
+    ipar = 1;
+  }
+}

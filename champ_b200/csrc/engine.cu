@@ -1,0 +1,778 @@
+// engine.cu — the C ABI of include/champ_b200.h on top of the move and
+// local-energy kernels.  One translation unit so the __constant__ system
+// block is shared by every kernel without relocatable device code.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/champ_b200.h"
+#include "common.cuh"
+#include "gemm.cuh"
+#include "hpsi.cuh"
+#include "move.cuh"
+
+
+using namespace cw;
+
+struct cw_ctx {
+  int device = 0, precision = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  CSys h;                 // host copy of the constant block
+  GSys g{};               // device tables
+  std::vector<void *> sys_allocs;
+  // walkers
+  int W = 0;
+  WState st{};
+  MoveBuf mb{};
+  HBuf hb{};
+  std::vector<void *> w_allocs;
+  size_t smem_jmove = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0;
+  // rank-0 cumulative estimators (acuest_reduce)
+  double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
+  double ecum1s = 0, ecm21s = 0;
+  long iblk = 0, passes = 0;
+  double last_ms = 0;
+};
+
+namespace {
+
+int fail(cw_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(c, e_ == cudaErrorMemoryAllocation ? CW_ERR_OOM : CW_ERR_CUDA,        \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+int nterms4(int nord) {
+  int i = 0;
+  for (int n = 2; n <= nord; n++)
+    for (int k = n - 1; k >= 0; k--) {
+      int l_hi = (k == 0) ? n - k - 2 : n - k;
+      for (int l = l_hi; l >= 0; l--) {
+        int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) i++;
+      }
+    }
+  return i;
+}
+
+template <typename T>
+int dalloc(cw_ctx *c, std::vector<void *> &list, T **p, size_t n) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess)
+    return fail(c, CW_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+  list.push_back(q);
+  *p = (T *)q;
+  return CW_OK;
+}
+
+#define DALLOC(list, p, n)                         \
+  do {                                             \
+    int rc_ = dalloc(c, list, &(p), (size_t)(n));  \
+    if (rc_) return rc_;                           \
+  } while (0)
+
+void free_list(std::vector<void *> &l) {
+  for (void *p : l) cudaFree(p);
+  l.clear();
+}
+
+int launch_check(cw_ctx *c, const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  return CW_OK;
+}
+
+#define LCHK(name)                        \
+  do {                                    \
+    int rc_ = launch_check(c, name);      \
+    if (rc_) return rc_;                  \
+  } while (0)
+
+template <int NORD>
+void launch_jmove(cw_ctx *c, int iel) {
+  const int warps = 4;
+  dim3 grid((c->W + warps - 1) / warps);
+  k_jastrow_move<NORD><<<grid, 32 * warps, c->smem_jmove, c->stream>>>(c->st, c->mb, iel);
+}
+template <int NORD>
+void launch_jfull(cw_ctx *c) {
+  k_jastrow_full<NORD><<<c->W, 256, c->smem_jfull, c->stream>>>(c->st, c->hb);
+}
+template <int NORD>
+void launch_ecp(cw_ctx *c) {
+  k_ecp<NORD><<<c->W, 32 * c->h.nquad, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+}
+template <int NORD>
+int set_attrs(cw_ctx *c) {
+  CK(cudaFuncSetAttribute(k_jastrow_move<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_jmove));
+  CK(cudaFuncSetAttribute(k_jastrow_full<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_jfull));
+  if (c->h.nloc > 0)
+    CK(cudaFuncSetAttribute(k_ecp<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
+  return CW_OK;
+}
+
+#define NORD_DISPATCH(fn, ...)            \
+  switch (c->h.nordc <= 1 ? 1 : c->h.nordc) { \
+    case 1: fn<1>(__VA_ARGS__); break;    \
+    case 2: fn<2>(__VA_ARGS__); break;    \
+    case 3: fn<3>(__VA_ARGS__); break;    \
+    case 4: fn<4>(__VA_ARGS__); break;    \
+    case 5: fn<5>(__VA_ARGS__); break;    \
+    case 6: fn<6>(__VA_ARGS__); break;    \
+    default: fn<7>(__VA_ARGS__); break;   \
+  }
+
+int nord_attrs(cw_ctx *c) {
+  switch (c->h.nordc <= 1 ? 1 : c->h.nordc) {
+    case 1: return set_attrs<1>(c);
+    case 2: return set_attrs<2>(c);
+    case 3: return set_attrs<3>(c);
+    case 4: return set_attrs<4>(c);
+    case 5: return set_attrs<5>(c);
+    case 6: return set_attrs<6>(c);
+    default: return set_attrs<7>(c);
+  }
+}
+
+// Full local energy of every walker (hpsi).  mode 1 also adds metrop6's sums.
+int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullptr) {
+  const CSys &h = c->h;
+  const int W = c->W, N = h.N, M = h.M;
+  NORD_DISPATCH(launch_jfull, c);
+  LCHK("k_jastrow_full");
+  // orbitals in electron chunks
+  const int ec = c->hb.chunk;
+  for (int e0 = 0; e0 < N; e0 += ec) {
+    const int ne = std::min(ec, N - e0);
+    const long nt = (long)W * ne * M;
+    k_basis_all<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    LCHK("k_basis_all");
+    dgemm(c->stream, W * ne * 5, h.Oa, h.K, c->hb.phi, c->g.coefT, c->hb.orball);
+    LCHK("dgemm(all)");
+    const long ns = (long)W * ne * h.nmax;
+    k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    LCHK("k_scatter_orbs");
+  }
+  k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->st, c->hb);
+  LCHK("k_slater_inv");
+  if (h.nloc > 0) {
+    const int nchunk = (h.K + 63) / 64;
+    k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->st, c->hb, c->g);
+    LCHK("k_ctilde");
+    NORD_DISPATCH(launch_ecp, c);
+    LCHK("k_ecp");
+  }
+  k_energy<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->hb, mode, d_e, d_ekin);
+  LCHK("k_energy");
+  return CW_OK;
+}
+
+int check_status(cw_ctx *c) {
+  std::vector<int> s(c->W);
+  CK(cudaMemcpyAsync(s.data(), c->st.status, sizeof(int) * c->W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int w = 0; w < c->W; w++)
+    if (s[w] & 1) return fail(c, CW_ERR_SINGULAR, "walker %d: singular Slater matrix", w);
+  for (int w = 0; w < c->W; w++)
+    if (s[w]) return fail(c, CW_ERR_STATE, "walker %d: non-finite state (status %d)", w, s[w]);
+  return CW_OK;
+}
+
+int alloc_walkers(cw_ctx *c, int W) {
+  free_list(c->w_allocs);
+  const CSys &h = c->h;
+  const int N = h.N, M = h.M, K = h.K, Oa = h.Oa, nmax = h.nmax, NQ = std::max(h.nquad, 1);
+  auto &L = c->w_allocs;
+  WState &s = c->st;
+  s.W = W;
+  DALLOC(L, s.x, (size_t)W * 3 * N);
+  DALLOC(L, s.rng, (size_t)W * 4);
+  DALLOC(L, s.xq, (size_t)W * 3 * NQ);
+  DALLOC(L, s.rmino, (size_t)W * N);
+  DALLOC(L, s.nearesto, (size_t)W * N);
+  DALLOC(L, s.rvmino, (size_t)W * 3 * N);
+  DALLOC(L, s.psido, W);
+  DALLOC(L, s.psijo, W);
+  DALLOC(L, s.psi2o, W);
+  DALLOC(L, s.eold, W);
+  DALLOC(L, s.ekino, W);
+  DALLOC(L, s.slmi, (size_t)W * 2 * nmax * nmax);
+  DALLOC(L, s.detiab, (size_t)W * 2);
+  DALLOC(L, s.orbs, (size_t)W * N * nmax);
+  DALLOC(L, s.dorbs, (size_t)W * 3 * N * nmax);
+  DALLOC(L, s.fso, (size_t)W * N * N);
+  DALLOC(L, s.fijo, (size_t)W * 3 * N * N);
+  DALLOC(L, s.fjo, (size_t)W * 3 * N);
+  DALLOC(L, s.fsumo, W);
+  DALLOC(L, s.sums, (size_t)W * 8);
+  DALLOC(L, s.status, W);
+  MoveBuf &m = c->mb;
+  DALLOC(L, m.ms, W);
+  DALLOC(L, m.fsn, (size_t)W * N);
+  DALLOC(L, m.fijn_i, (size_t)W * 3 * N);
+  DALLOC(L, m.fijn_j, (size_t)W * 3 * N);
+  DALLOC(L, m.fsumn, W);
+  DALLOC(L, m.vjn, (size_t)W * 3);
+  DALLOC(L, m.phi, (size_t)W * 4 * K);
+  DALLOC(L, m.orbn, (size_t)W * 4 * Oa);
+  HBuf &b = c->hb;
+  DALLOC(L, b.d2o, W);
+  DALLOC(L, b.pe_ee, W);
+  DALLOC(L, b.pe_ecp, W);
+  DALLOC(L, b.vpsp, (size_t)W * 2);
+  DALLOC(L, b.ddx, (size_t)W * N * 4);
+  DALLOC(L, b.ddorbs, (size_t)W * N * nmax);
+  // electron chunk of the all-electron orbital stage, bounded by a byte budget
+  size_t budget = (size_t)1 << 30;
+  if (const char *e = getenv("CW_CHUNK_BYTES")) budget = (size_t)atoll(e);
+  const size_t per_e = (size_t)W * 5 * (K + Oa) * sizeof(double);
+  int chunk = (int)std::max<size_t>(1, budget / std::max<size_t>(per_e, 1));
+  chunk = std::min(chunk, N);
+  b.chunk = chunk;
+  DALLOC(L, b.phi, (size_t)W * chunk * 5 * K);
+  DALLOC(L, b.orball, (size_t)W * chunk * 5 * Oa);
+  if (h.nloc > 0) DALLOC(L, b.ctilde, (size_t)W * N * K);
+  CK(cudaMemsetAsync(s.status, 0, sizeof(int) * W, c->stream));
+  CK(cudaMemsetAsync(s.sums, 0, sizeof(double) * W * 8, c->stream));
+  c->W = W;
+  return CW_OK;
+}
+
+int zerest(cw_ctx *c) {
+  const CSys &h = c->h;
+  const int W = c->W, NQ = h.nquad;
+  if (NQ > 0) {
+    std::vector<double> xq((size_t)W * 3 * NQ);
+    for (int w = 0; w < W; w++)
+      for (int q = 0; q < NQ; q++) {
+        xq[(size_t)w * 3 * NQ + q] = h.xq0[q];
+        xq[(size_t)w * 3 * NQ + NQ + q] = h.yq0[q];
+        xq[(size_t)w * 3 * NQ + 2 * NQ + q] = h.zq0[q];
+      }
+    CK(cudaMemcpyAsync(c->st.xq, xq.data(), sizeof(double) * xq.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  int rc = run_hpsi(c, 0);
+  if (rc) return rc;
+  const long nt = (long)W * h.N;
+  k_nearest<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st);
+  LCHK("k_nearest");
+  CK(cudaMemsetAsync(c->st.sums, 0, sizeof(double) * W * 8, c->stream));
+  c->ecum = c->ecm2 = c->wcum = c->pecum = c->tpbcum = c->pecm2 = c->tpbcm2 = c->acc = 0;
+  c->ecum1s = c->ecm21s = 0;
+  c->iblk = 0;
+  c->passes = 0;
+  return check_status(c);
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) {
+  cw_ctx *c = nullptr;
+  if (!out || !d) return CW_ERR_ARG;
+  *out = nullptr;
+  c = new cw_ctx();
+  c->device = device;
+  c->precision = precision;
+  auto bad = [&](const char *msg) {
+    c->err = msg;
+    *out = c;
+    return CW_ERR_ARG;
+  };
+  if (d->ncent > CW_MAX_CENT) return bad("ncent exceeds CW_MAX_CENT");
+  if (d->nctype > CW_MAX_TYPES) return bad("nctype exceeds CW_MAX_TYPES");
+  if (d->mrwf > CW_MAX_RWF) return bad("mrwf exceeds CW_MAX_RWF");
+  if (d->nordc > CW_MAX_NORD || d->norda > CW_MAX_NORD || d->nordb > CW_MAX_NORD) return bad("Jastrow order > 7");
+  if (d->ndet != 1) return bad("this engine version evaluates single-determinant wave functions (ndet=1)");
+  if (d->nloc != 0 && d->nloc != 4) return bad("nloc must be 0 or 4");
+  if (d->nquad > 32) return bad("nquad > 32 not supported");
+  if (d->isc < 2 || d->isc > 5) return bad("isc must be 2..5");
+  const int ndn = d->nelec - d->nup;
+  const int nmax = std::max(d->nup, ndn);
+  if (nmax > 128) return bad("more than 128 electrons of one spin");
+  if (precision != CW_PREC_FP64 && precision != CW_PREC_MIXED) return bad("unknown precision");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    c->err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+    *out = c;
+    return CW_ERR_CUDA;
+  }
+  *out = c;
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&c->ev0));
+  CK(cudaEventCreate(&c->ev1));
+  CSys &h = c->h;
+  std::memset(&h, 0, sizeof h);
+  h.N = d->nelec; h.nup = d->nup; h.ndn = ndn; h.M = d->ncent; h.nctype = d->nctype;
+  h.K = d->nbasis; h.Oa = d->norb; h.nmax = nmax;
+  h.norda = d->norda; h.nordb = d->nordb; h.nordc = d->nordc; h.isc = d->isc;
+  h.nspin2b = d->nspin2b; h.nocuspb = d->nocuspb; h.nterms = nterms4(d->nordc);
+  if (h.nterms > CW_MAX_TERMS) return fail(c, CW_ERR_ARG, "too many e-e-n terms");
+  h.nloc = d->nloc; h.nquad = d->nloc ? d->nquad : 0;
+  h.scalek = d->scalek;
+  h.deltar = d->deltar; h.deltat = d->deltat; h.fbias = d->fbias; h.pecent = d->pecent;
+  h.cdet = d->cdet[0];
+  h.mrwf = d->mrwf; h.mpts = d->mrwf_pts; h.mbastyp = d->mbastyp;
+  int m = 0;
+  for (int ic = 0; ic < d->ncent; ic++) {
+    for (int k = 0; k < 3; k++) h.cent[3 * ic + k] = d->cent[3 * ic + k];
+    h.iwctype[ic] = d->iwctype[ic];
+    h.ao_first[ic] = m;
+    m += d->nbastyp[d->iwctype[ic]];
+  }
+  h.ao_first[d->ncent] = m;
+  if (m != d->nbasis) return fail(c, CW_ERR_ARG, "sum of nbastyp over centres (%d) != nbasis (%d)", m, d->nbasis);
+  for (int it = 0; it < d->nctype; it++) {
+    h.znuc[it] = d->znuc[it];
+    h.nrbas[it] = d->nrbas[it]; h.igrid[it] = d->igrid[it]; h.nr[it] = d->nr[it];
+    h.nbastyp[it] = d->nbastyp[it];
+    h.arg[it] = d->arg[it]; h.r0[it] = d->r0[it];
+    for (int irb = 0; irb < d->nrbas[it]; irb++) {
+      const int src = irb + d->mrwf * it;
+      h.rmaxwf[it * CW_MAX_RWF + irb] = d->rmaxwf[src];
+      for (int k = 0; k < 5; k++) h.ce[(it * CW_MAX_RWF + irb) * 5 + k] = d->ce[src * CW_NCOEF + k];
+      for (int k = 0; k < 2; k++) h.ae[(it * CW_MAX_RWF + irb) * 2 + k] = d->ae[src * 2 + k];
+    }
+    for (int k = 0; k <= d->norda; k++) h.a4[it * (d->norda + 1) + k] = d->a4[it * (d->norda + 1) + k];
+    for (int k = 0; k < h.nterms; k++) h.c[it * CW_MAX_TERMS + k] = d->c[it * h.nterms + k];
+    if (d->nloc) {
+      h.lpot[it] = d->lpot[it];
+      for (int l = 0; l < CW_MPS_L; l++) {
+        h.necp_term[it * 4 + l] = d->necp_term[it * CW_MPS_L + l];
+        for (int k = 0; k < CW_MGAUSS; k++) {
+          const int s = (it * CW_MPS_L + l) * CW_MGAUSS + k;
+          h.necp_power[(it * 4 + l) * 16 + k] = d->necp_power[s];
+          h.ecp_exponent[(it * 4 + l) * 16 + k] = d->ecp_exponent[s];
+          h.ecp_coef[(it * 4 + l) * 16 + k] = d->ecp_coef[s];
+        }
+      }
+    }
+  }
+  for (int isb = 0; isb < d->nspin2b; isb++)
+    for (int k = 0; k <= d->nordb; k++) h.b[isb * (d->nordb + 1) + k] = d->b[isb * (d->nordb + 1) + k];
+  for (int q = 0; q < h.nquad; q++) {
+    h.xq0[q] = d->xq0[q]; h.yq0[q] = d->yq0[q]; h.zq0[q] = d->zq0[q]; h.wq[q] = d->wq[q];
+  }
+  // set_scale_dist (vmc/scale_dist.f90:3-55)
+  h.asymp_r = 1.0 / h.scalek;
+  for (int it = 0; it < d->nctype; it++) {
+    const double *a = &h.a4[it * (d->norda + 1)];
+    double v = a[0] * h.asymp_r / (1 + a[1] * h.asymp_r);
+    for (int iord = 2; iord <= d->norda; iord++) v += a[iord] * std::pow(h.asymp_r, iord);
+    h.asymp_jasa[it] = v;
+  }
+  for (int i = 0; i < 2; i++) {
+    double sspinn;
+    int isp;
+    if (i == 0) { sspinn = 1; isp = 0; }
+    else { sspinn = (d->nspin2b == 1 && d->nocuspb == 0) ? 0.5 : 1.0; isp = d->nspin2b - 1; }
+    const double *bb = &h.b[isp * (d->nordb + 1)];
+    double v = sspinn * bb[0] * h.asymp_r / (1 + bb[1] * h.asymp_r);
+    for (int iord = 2; iord <= d->nordb; iord++) v += bb[iord] * std::pow(h.asymp_r, iord);
+    h.asymp_jasb[i] = v;
+  }
+  CK(cudaMemcpyToSymbol(cs, &h, sizeof(CSys)));
+  // global tables
+  auto &L = c->sys_allocs;
+  const size_t nt = (size_t)d->nctype * d->mrwf * d->mrwf_pts;
+  double *rwf, *d2rwf, *coefT;
+  int *iwl, *iwr, *slot;
+  DALLOC(L, rwf, nt);
+  DALLOC(L, d2rwf, nt);
+  CK(cudaMemcpy(rwf, d->rwf, nt * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d2rwf, d->d2rwf, nt * sizeof(double), cudaMemcpyHostToDevice));
+  const size_t nb = (size_t)d->nctype * d->mbastyp;
+  DALLOC(L, iwl, nb);
+  DALLOC(L, iwr, nb);
+  CK(cudaMemcpy(iwl, d->iwlbas, nb * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(iwr, d->iwrwf, nb * sizeof(int), cudaMemcpyHostToDevice));
+  // coefT[m][o] = coef(m,o)
+  std::vector<double> ct((size_t)d->nbasis * d->norb);
+  for (int o = 0; o < d->norb; o++)
+    for (int mm = 0; mm < d->nbasis; mm++) ct[(size_t)mm * d->norb + o] = d->coef[(size_t)o * d->nbasis + mm];
+  DALLOC(L, coefT, ct.size());
+  CK(cudaMemcpy(coefT, ct.data(), ct.size() * sizeof(double), cudaMemcpyHostToDevice));
+  std::vector<int> so(2 * nmax, 0);
+  for (int j = 0; j < d->nup; j++) so[j] = d->iworbd[j] - 1;
+  for (int j = 0; j < ndn; j++) so[nmax + j] = d->iworbd[d->nup + j] - 1;
+  for (int v : so)
+    if (v < 0 || v >= d->norb) return fail(c, CW_ERR_ARG, "iworbd entry out of range");
+  DALLOC(L, slot, so.size());
+  CK(cudaMemcpy(slot, so.data(), so.size() * sizeof(int), cudaMemcpyHostToDevice));
+  c->g.rwf = rwf; c->g.d2rwf = d2rwf; c->g.iwlbas = iwl; c->g.iwrwf = iwr; c->g.coefT = coefT; c->g.slot_orb = slot;
+  // dynamic shared memory sizes
+  c->smem_jmove = sizeof(double) * 4 * 6 * (size_t)h.M;
+  c->smem_jfull = sizeof(double) * 3 * (size_t)h.N;
+  c->smem_sinv = sizeof(double) * ((size_t)nmax * nmax + nmax);
+  c->smem_ctil = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64);
+  c->smem_ecp = sizeof(double) * ((size_t)h.N * h.M + 3 * h.N + 4 * h.M + (size_t)h.nquad * h.K + (size_t)h.nquad * h.M);
+  CK(cudaFuncSetAttribute(k_slater_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_sinv));
+  CK(cudaFuncSetAttribute(k_ctilde, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ctil));
+  int rc = nord_attrs(c);
+  if (rc) return rc;
+  if (c->smem_ecp > 227 * 1024 && h.nloc) return fail(c, CW_ERR_UNSUPPORTED, "ECP stage shared memory too large");
+  return CW_OK;
+}
+
+void cw_destroy(cw_ctx *c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_list(c->w_allocs);
+  free_list(c->sys_allocs);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char *cw_last_error(const cw_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int cw_sync(cw_ctx *c) {
+  if (!c) return CW_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  return CW_OK;
+}
+
+double cw_last_ms(const cw_ctx *c) { return c ? c->last_ms : 0.0; }
+
+int cw_set_walkers(cw_ctx *c, int nwalk, const double *x, const uint64_t *rng) {
+  if (!c || nwalk <= 0 || !x || !rng) return fail(c, CW_ERR_ARG, "cw_set_walkers: bad arguments");
+  CK(cudaSetDevice(c->device));
+  if (nwalk != c->W) {
+    int rc = alloc_walkers(c, nwalk);
+    if (rc) return rc;
+  }
+  const int N = c->h.N;
+  std::vector<double> xt((size_t)nwalk * 3 * N);
+  for (int w = 0; w < nwalk; w++)
+    for (int e = 0; e < N; e++)
+      for (int k = 0; k < 3; k++) xt[((size_t)w * 3 + k) * N + e] = x[((size_t)w * N + e) * 3 + k];
+  CK(cudaMemcpyAsync(c->st.x, xt.data(), sizeof(double) * xt.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->st.rng, rng, sizeof(uint64_t) * 4 * nwalk, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->st.status, 0, sizeof(int) * nwalk, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return zerest(c);
+}
+
+int cw_get_walkers(cw_ctx *c, double *x, uint64_t *rng) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  const int N = c->h.N, W = c->W;
+  if (x) {
+    std::vector<double> xt((size_t)W * 3 * N);
+    CK(cudaMemcpyAsync(xt.data(), c->st.x, sizeof(double) * xt.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int w = 0; w < W; w++)
+      for (int e = 0; e < N; e++)
+        for (int k = 0; k < 3; k++) x[((size_t)w * N + e) * 3 + k] = xt[((size_t)w * 3 + k) * N + e];
+  }
+  if (rng) {
+    CK(cudaMemcpyAsync(rng, c->st.rng, sizeof(uint64_t) * 4 * W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return CW_OK;
+}
+
+int cw_vmc_steps(cw_ctx *c, int nstep) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  CK(cudaSetDevice(c->device));
+  const CSys &h = c->h;
+  const int W = c->W;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int s = 0; s < nstep; s++) {
+    if (h.nloc > 0) {
+      k_rotqua<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st);
+      LCHK("k_rotqua");
+    }
+    for (int i = 0; i < h.N; i++) {
+      k_propose<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->mb, i);
+      LCHK("k_propose");
+      NORD_DISPATCH(launch_jmove, c, i);
+      LCHK("k_jastrow_move");
+      const long nt = (long)W * h.M;
+      k_basis_move<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->mb, c->g);
+      LCHK("k_basis_move");
+      dgemm(c->stream, W * 4, h.Oa, h.K, c->mb.phi, c->g.coefT, c->mb.orbn);
+      LCHK("dgemm(move)");
+      k_accept<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+      LCHK("k_accept");
+    }
+    int rc = run_hpsi(c, 1);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  c->passes += nstep;
+  return check_status(c);
+}
+
+int cw_end_block(cw_ctx *c, double *block_energy) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  const int W = c->W;
+  std::vector<double> s((size_t)W * 8);
+  CK(cudaMemcpyAsync(s.data(), c->st.sums, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemsetAsync(c->st.sums, 0, sizeof(double) * s.size(), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double es = 0, wsm = 0;
+  for (int w = 0; w < W; w++) {
+    const double *v = &s[(size_t)w * 8];
+    const double enow = v[1] / v[0];
+    c->wcum += v[0];
+    c->ecum += v[1];
+    c->ecm2 += v[1] * enow;
+    const double penow = v[2] / v[0], tpbnow = v[3] / v[0];
+    c->pecm2 += v[2] * penow;
+    c->tpbcm2 += v[3] * tpbnow;
+    c->pecum += v[2];
+    c->tpbcum += v[3];
+    c->acc += v[4];
+    c->ecum1s += v[5];
+    c->ecm21s += v[6];
+    es += v[1];
+    wsm += v[0];
+  }
+  c->iblk += W;
+  if (block_energy) *block_energy = es / wsm;
+  return CW_OK;
+}
+
+int cw_results(cw_ctx *c, double *out) {
+  if (!c || !out || c->iblk == 0) return fail(c, CW_ERR_STATE, "no completed blocks");
+  const double passes = (double)c->passes * c->W;
+  auto err = [&](double x, double x2) {
+    return std::sqrt(std::fabs(x2 / c->wcum - (x / c->wcum) * (x / c->wcum)) / (double)c->iblk);
+  };
+  const double eerr = err(c->ecum, c->ecm2);
+  const double eerr1s = std::sqrt(std::fabs(c->ecm21s / c->wcum - (c->ecum1s / c->wcum) * (c->ecum1s / c->wcum)) / passes);
+  const double tcsq = eerr1s == 0 ? 0 : eerr / eerr1s;
+  out[0] = c->ecum / c->wcum;
+  out[1] = eerr;
+  out[2] = eerr1s * std::sqrt(passes);
+  out[3] = tcsq * tcsq;
+  out[4] = c->acc / (passes * c->h.N);
+  out[5] = c->pecum / c->wcum;
+  out[6] = c->tpbcum / c->wcum;
+  out[7] = (double)c->iblk;
+  return CW_OK;
+}
+
+int cw_hpsi(cw_ctx *c, const double *xq, const double *yq, const double *zq, double *energy, double *psid,
+            double *psij, double *ekin) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  const CSys &h = c->h;
+  const int W = c->W, NQ = h.nquad;
+  if (NQ > 0) {
+    std::vector<double> t((size_t)W * 3 * NQ);
+    for (int w = 0; w < W; w++)
+      for (int q = 0; q < NQ; q++) {
+        t[(size_t)w * 3 * NQ + q] = xq ? xq[q] : h.xq0[q];
+        t[(size_t)w * 3 * NQ + NQ + q] = yq ? yq[q] : h.yq0[q];
+        t[(size_t)w * 3 * NQ + 2 * NQ + q] = zq ? zq[q] : h.zq0[q];
+      }
+    CK(cudaMemcpyAsync(c->st.xq, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, c->stream));
+  }
+  int rc = run_hpsi(c, 0);
+  if (rc) return rc;
+  rc = check_status(c);
+  if (rc) return rc;
+  return cw_get_state(c, energy, psid, psij) || (ekin && cudaMemcpy(ekin, c->st.ekino, sizeof(double) * W,
+                                                                    cudaMemcpyDeviceToHost) != cudaSuccess)
+             ? fail(c, CW_ERR_CUDA, "copy-out failed")
+             : CW_OK;
+}
+
+int cw_get_state(cw_ctx *c, double *eold, double *psido, double *psijo) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  CK(cudaStreamSynchronize(c->stream));
+  if (eold) CK(cudaMemcpy(eold, c->st.eold, sizeof(double) * c->W, cudaMemcpyDeviceToHost));
+  if (psido) CK(cudaMemcpy(psido, c->st.psido, sizeof(double) * c->W, cudaMemcpyDeviceToHost));
+  if (psijo) CK(cudaMemcpy(psijo, c->st.psijo, sizeof(double) * c->W, cudaMemcpyDeviceToHost));
+  return CW_OK;
+}
+
+int cw_get_sums(cw_ctx *c, double *out) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  std::vector<double> s((size_t)c->W * 8);
+  CK(cudaMemcpyAsync(s.data(), c->st.sums, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int w = 0; w < c->W; w++)
+    for (int k = 0; k < 5; k++) out[(size_t)w * 5 + k] = s[(size_t)w * 8 + k];
+  return CW_OK;
+}
+
+int cw_orbitals(cw_ctx *c, double *orb, double *dorb, double *ddorb) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  const CSys &h = c->h;
+  const int W = c->W, N = h.N, M = h.M, Oa = h.Oa, K = h.K;
+  const int ec = c->hb.chunk;
+  std::vector<double> buf;
+  for (int e0 = 0; e0 < N; e0 += ec) {
+    const int ne = std::min(ec, N - e0);
+    const long nt = (long)W * ne * M;
+    k_basis_all<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    LCHK("k_basis_all");
+    dgemm(c->stream, W * ne * 5, Oa, K, c->hb.phi, c->g.coefT, c->hb.orball);
+    LCHK("dgemm(all)");
+    buf.resize((size_t)W * ne * 5 * Oa);
+    CK(cudaMemcpyAsync(buf.data(), c->hb.orball, sizeof(double) * buf.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int w = 0; w < W; w++)
+      for (int el = 0; el < ne; el++) {
+        const int e = e0 + el;
+        const double *ob = &buf[((size_t)w * ne + el) * 5 * Oa];
+        for (int o = 0; o < Oa; o++) {
+          if (orb) orb[((size_t)w * Oa + o) * N + e] = ob[o];
+          if (dorb)
+            for (int k = 0; k < 3; k++) dorb[(((size_t)w * 3 + k) * N + e) * Oa + o] = ob[(1 + k) * Oa + o];
+          if (ddorb) ddorb[((size_t)w * N + e) * Oa + o] = ob[4 * Oa + o];
+        }
+      }
+  }
+  return CW_OK;
+}
+
+int cw_jastrow(cw_ctx *c, double *psij, double *v, double *d2j) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  NORD_DISPATCH(launch_jfull, c);
+  LCHK("k_jastrow_full");
+  const int W = c->W, N = c->h.N;
+  CK(cudaStreamSynchronize(c->stream));
+  if (psij) CK(cudaMemcpy(psij, c->st.fsumo, sizeof(double) * W, cudaMemcpyDeviceToHost));
+  if (d2j) CK(cudaMemcpy(d2j, c->hb.d2o, sizeof(double) * W, cudaMemcpyDeviceToHost));
+  if (v) {
+    std::vector<double> t((size_t)W * 3 * N);
+    CK(cudaMemcpy(t.data(), c->st.fjo, sizeof(double) * t.size(), cudaMemcpyDeviceToHost));
+    for (int w = 0; w < W; w++)
+      for (int e = 0; e < N; e++)
+        for (int k = 0; k < 3; k++) v[((size_t)w * N + e) * 3 + k] = t[((size_t)w * 3 + k) * N + e];
+  }
+  return CW_OK;
+}
+
+int cw_slater(cw_ctx *c, double *slmi, double *det) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  int rc = run_hpsi(c, 0);
+  if (rc) return rc;
+  rc = check_status(c);
+  if (rc) return rc;
+  const int W = c->W, nmax = c->h.nmax;
+  if (slmi) CK(cudaMemcpy(slmi, c->st.slmi, sizeof(double) * W * 2 * nmax * nmax, cudaMemcpyDeviceToHost));
+  if (det) CK(cudaMemcpy(det, c->st.detiab, sizeof(double) * W * 2, cudaMemcpyDeviceToHost));
+  return CW_OK;
+}
+
+// --------------------------------------------------------------------------
+// host-only helpers
+// --------------------------------------------------------------------------
+namespace {
+struct HRng {
+  uint64_t s[4];
+  static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+  uint64_t next() {
+    const uint64_t result = rotl(s[1] * 5, 7) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl(s[3], 45);
+    return result;
+  }
+  double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }
+  void jump() {
+    static const uint64_t J[] = {0x180ec6d33cfd0abaULL, 0xd5a61266f0c9392cULL, 0xa9582618e03fc9aaULL,
+                                 0x39abdc4529b1661cULL};
+    uint64_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    for (int i = 0; i < 4; i++)
+      for (int b = 0; b < 64; b++) {
+        if (J[i] & (1ULL << b)) {
+          t0 ^= s[0]; t1 ^= s[1]; t2 ^= s[2]; t3 ^= s[3];
+        }
+        next();
+      }
+    s[0] = t0; s[1] = t1; s[2] = t2; s[3] = t3;
+  }
+};
+}  // namespace
+
+int cw_rng_states(const int32_t *irn8, int nwalk, uint64_t *out) {
+  if (!irn8 || !out || nwalk < 0) return CW_ERR_ARG;
+  HRng r;
+  std::memcpy(r.s, irn8, 32);
+  for (int w = 0; w < nwalk; w++) {
+    std::memcpy(out + 4 * (size_t)w, r.s, 32);
+    r.jump();
+  }
+  return CW_OK;
+}
+
+int cw_sites(const cw_system_desc *d, int nwalk, uint64_t *rng, double *x) {
+  if (!d || !rng || !x || nwalk < 0) return CW_ERR_ARG;
+  const int M = d->ncent, N = d->nelec;
+  std::vector<int> nsite(M);
+  int l = 0;
+  for (int i = 0; i < M; i++) {
+    nsite[i] = (int)(d->znuc[d->iwctype[i]] + 0.5);
+    l += nsite[i];
+    if (l > N) {
+      nsite[i] -= (l - N);
+      l = N;
+    }
+  }
+  if (l < N) nsite[0] += (N - l);
+  for (int w = 0; w < nwalk; w++) {
+    HRng r;
+    std::memcpy(r.s, rng + 4 * (size_t)w, 32);
+    double *xw = x + (size_t)w * N * 3;
+    l = 0;
+    for (int ispin = 1; ispin <= 2; ispin++)
+      for (int i = 0; i < M && l < N; i++) {
+        const int ju = (nsite[i] + 2 - ispin) / 2;
+        for (int j = 1; j <= ju; j++) {
+          l++;
+          if (l > N) break;
+          const double z = d->znuc[d->iwctype[i]];
+          double sitsca;
+          if (j == 1) sitsca = 1 / z;
+          else if (j <= 5) sitsca = 2 / (z - 2);
+          else sitsca = 3 / (z - 10);
+          for (int ic = 0; ic < 3; ic++) {
+            double site = -std::log(r.uniform());
+            const double sg = r.uniform() - 0.5;
+            site = sg >= 0 ? std::fabs(site) : -std::fabs(site);
+            xw[(size_t)(l - 1) * 3 + ic] = sitsca * site + d->cent[3 * i + ic];
+          }
+        }
+      }
+    std::memcpy(rng + 4 * (size_t)w, r.s, 32);
+  }
+  return CW_OK;
+}
+
+}  // extern "C"

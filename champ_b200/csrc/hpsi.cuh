@@ -1,0 +1,695 @@
+// hpsi.cuh — full local energy of every walker, hpsi (vmc/hpsi.f90:3).
+//
+//   k_jastrow_full   jastrow_factor4 (vmc/jastrow4.f90:3) + e-e Coulomb sum
+//   k_basis_all      basis_fns ider=2 for a chunk of electrons
+//   gemm             LCAO (vmc/orbitals_no_qmckl.f90:19)
+//   k_scatter_orbs   Slater columns of each electron (determinant.f90:40-49)
+//   k_slater_inv     matinv + ddx/d2dx2 (vmc/determinant.f90:50-70, matinv.f90:22)
+//   k_ctilde         c~(i,m) = sum_j slmi(j,i) coef(m,occ_j): ratio vectors of
+//                    nonlocd_quad (vmc/nonloc.f90:462) contracted once per electron
+//   k_ecp            getvps_gauss + nonloc quadrature (vmc/nonloc_pot.f90:3,
+//                    vmc/nonloc.f90:5, nonlocj_quad4 :656)
+//   k_energy         E_L assembly (vmc/hpsi.f90:176-246) and metrop6 sums
+#pragma once
+#include "common.cuh"
+
+namespace cw {
+
+struct HBuf {
+  double *d2o;      // [W]
+  double *pe_ee;    // [W]   sum 1/r_ij
+  double *pe_ecp;   // [W]   local ECP part (or -Z/r for nloc=0)
+  double *vpsp;     // [W][2]
+  double *ddx;      // [W][N][4]  ddx(3), d2dx2
+  double *ddorbs;   // [W][N][nmax]
+  double *phi;      // [rows][K] chunk basis
+  double *orball;   // [rows][Oa] chunk orbitals
+  double *ctilde;   // [W][N][K]
+  int chunk;        // electrons per chunk
+};
+
+__device__ __forceinline__ void pair_of(long p, int &i, int &j) {
+  // p = i*(i-1)/2 + j, 0 <= j < i
+  int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+  while ((long)ii * (ii - 1) / 2 > p) ii--;
+  while ((long)(ii + 1) * ii / 2 <= p) ii++;
+  i = ii;
+  j = (int)(p - (long)ii * (ii - 1) / 2);
+}
+
+template <int BS>
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < BS / 32; k++) r += red[k];
+  return r;  // valid on thread 0
+}
+
+// ---------------------------------------------------------------------------
+// jastrow_factor4: CTA per walker, threads over pairs.
+// ---------------------------------------------------------------------------
+template <int NORD>
+__global__ void __launch_bounds__(256) k_jastrow_full(WState st, HBuf hb) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, M = cs.M;
+  extern __shared__ double smem[];
+  double *sx = smem;            // [3][N]
+  __shared__ double red[8];
+  for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
+  __syncthreads();
+  const double kap = cs.scalek;
+  double *fso = st.fso + (size_t)w * N * N;
+  double *fij0 = st.fijo + ((size_t)w * 3 + 0) * N * N;
+  double *fij1 = st.fijo + ((size_t)w * 3 + 1) * N * N;
+  double *fij2 = st.fijo + ((size_t)w * 3 + 2) * N * N;
+  double fsum = 0, d2sum = 0, pee = 0;
+  const long npair = (long)N * (N - 1) / 2;
+  for (long p = threadIdx.x; p < npair; p += blockDim.x) {
+    int i, j;
+    pair_of(p, i, j);
+    int isb, ipar;
+    double sspinn;
+    pair_spin(i, j, isb, ipar, sspinn);
+    const double rv[3] = {sx[i] - sx[j], sx[N + i] - sx[N + j], sx[2 * N + i] - sx[2 * N + j]};
+    const double rij = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+    pee += 1 / rij;
+    double u, dd1, dd2;
+    scale2<double>(rij, u, dd1, dd2);
+    double fs = 0, d2 = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
+    if (u != cs.asymp_r) {
+      double fee, feeu, feeuu;
+      ee_term<2, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+      feeuu = feeuu * dd1 * dd1 + feeu * dd2;
+      feeu = feeu * dd1 / rij;
+      fs += fee;
+      for (int k = 0; k < 3; k++) {
+        gi[k] += feeu * rv[k];
+        gj[k] -= feeu * rv[k];
+      }
+      d2 += 2 * (feeuu + 2 * feeu);
+    }
+    if (NORD > 1) {
+      const double u1 = 1 - kap * u, du1 = -kap * dd1, du2 = -kap * dd2;
+      for (int ic = 0; ic < M; ic++) {
+        const int it = cs.iwctype[ic];
+        const double *cc = &cs.cent[3 * ic];
+        const double ri_v[3] = {sx[i] - cc[0], sx[N + i] - cc[1], sx[2 * N + i] - cc[2]};
+        const double rj_v[3] = {sx[j] - cc[0], sx[N + j] - cc[1], sx[2 * N + j] - cc[2]};
+        const double ri = sqrt(ri_v[0] * ri_v[0] + ri_v[1] * ri_v[1] + ri_v[2] * ri_v[2]);
+        const double rj = sqrt(rj_v[0] * rj_v[0] + rj_v[1] * rj_v[1] + rj_v[2] * rj_v[2]);
+        double rri, dd7, dd9, rrj, dd8, dd10;
+        scale2<double>(ri, rri, dd7, dd9);
+        scale2<double>(rj, rrj, dd8, dd10);
+        if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
+        dd7 = -kap * dd7; dd9 = -kap * dd9; dd8 = -kap * dd8; dd10 = -kap * dd10;
+        const EenOut<double> e = een_poly<NORD, 2, double>(&cs.c[it * CW_MAX_TERMS], u1, 1 - kap * rri, 1 - kap * rrj);
+        const double sgs = ri + rj, tgs = ri - rj;
+        const double u2pst = rij * rij + sgs * tgs, u2mst = rij * rij - sgs * tgs;
+        const double fuu = e.fuu * du1 * du1 + e.fu * du2;
+        const double fu = e.fu * du1 / rij;
+        const double fui = e.fui * du1 * dd7, fuj = e.fuj * du1 * dd8;
+        const double fii = e.fii * dd7 * dd7 + e.fi * dd9, fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
+        const double fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
+        fs += e.fc;
+        for (int k = 0; k < 3; k++) {
+          gi[k] += fi * ri_v[k] + fu * rv[k];
+          gj[k] += fj * rj_v[k] - fu * rv[k];
+        }
+        d2 += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rij) + fuj * u2mst / (rj * rij) + fii + 2 * fi + fjj + 2 * fj;
+      }
+    }
+    fso[(size_t)i * N + j] = fs;
+    fso[(size_t)j * N + i] = fs;
+    fij0[(size_t)i * N + j] = gi[0]; fij0[(size_t)j * N + i] = gj[0];
+    fij1[(size_t)i * N + j] = gi[1]; fij1[(size_t)j * N + i] = gj[1];
+    fij2[(size_t)i * N + j] = gi[2]; fij2[(size_t)j * N + i] = gj[2];
+    fsum += fs;
+    d2sum += d2;
+  }
+  // e-n terms
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    double fs = 0, d2 = 0, g[3] = {0, 0, 0};
+    for (int ic = 0; ic < M; ic++) {
+      const int it = cs.iwctype[ic];
+      const double *cc = &cs.cent[3 * ic];
+      const double rvv[3] = {sx[i] - cc[0], sx[N + i] - cc[1], sx[2 * N + i] - cc[2]};
+      const double ri = sqrt(rvv[0] * rvv[0] + rvv[1] * rvv[1] + rvv[2] * rvv[2]);
+      double rri, dd7, dd9;
+      scale2<double>(ri, rri, dd7, dd9);
+      if (rri == cs.asymp_r) continue;
+      double fen, feni, fenii;
+      en_term<2, double>(it, rri, fen, feni, fenii);
+      fenii = fenii * dd7 * dd7 + feni * dd9;
+      feni = feni * dd7 / ri;
+      fs += fen;
+      for (int k = 0; k < 3; k++) g[k] += feni * rvv[k];
+      d2 += fenii + 2 * feni;
+    }
+    fso[(size_t)i * N + i] = fs;
+    fij0[(size_t)i * N + i] = g[0];
+    fij1[(size_t)i * N + i] = g[1];
+    fij2[(size_t)i * N + i] = g[2];
+    fsum += fs;
+    d2sum += d2;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int j = 0; j < N; j++) {
+      a0 += fij0[(size_t)i * N + j];
+      a1 += fij1[(size_t)i * N + j];
+      a2 += fij2[(size_t)i * N + j];
+    }
+    st.fjo[((size_t)w * 3 + 0) * N + i] = a0;
+    st.fjo[((size_t)w * 3 + 1) * N + i] = a1;
+    st.fjo[((size_t)w * 3 + 2) * N + i] = a2;
+  }
+  const double tf = block_sum<256>(fsum, red);
+  const double td = block_sum<256>(d2sum, red);
+  const double tp = block_sum<256>(pee, red);
+  if (threadIdx.x == 0) {
+    st.fsumo[w] = tf;
+    hb.d2o[w] = td;
+    hb.pe_ee[w] = tp;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// basis functions with Laplacian for electrons [e0, e0+ne): thread per
+// (walker, electron, centre); rows ((w*ne + e)*5 + d).
+// ---------------------------------------------------------------------------
+__global__ void k_basis_all(WState st, HBuf hb, GSys g, int e0, int ne) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int M = cs.M, K = cs.K, N = cs.N;
+  if (t >= (long)st.W * ne * M) return;
+  const int ic = (int)(t % M);
+  const long we = t / M;
+  const int el = (int)(we % ne);
+  const int w = (int)(we / ne);
+  const int e = e0 + el;
+  const double xc[3] = {st.x[((size_t)w * 3 + 0) * N + e] - cs.cent[3 * ic],
+                        st.x[((size_t)w * 3 + 1) * N + e] - cs.cent[3 * ic + 1],
+                        st.x[((size_t)w * 3 + 2) * N + e] - cs.cent[3 * ic + 2]};
+  double *phi = hb.phi + ((size_t)we * 5) * K;
+  basis_centre(g, ic, xc, 2, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
+}
+
+__global__ void k_scatter_orbs(WState st, HBuf hb, GSys g, int e0, int ne) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
+  if (t >= (long)st.W * ne * nmax) return;
+  const int j = (int)(t % nmax);
+  const long we = t / nmax;
+  const int el = (int)(we % ne), w = (int)(we / ne), e = e0 + el;
+  const int iab = e < cs.nup ? 0 : 1;
+  const int nel = iab == 0 ? cs.nup : cs.ndn;
+  if (j >= nel) return;
+  const int o = g.slot_orb[iab * nmax + j];
+  const double *ob = hb.orball + (size_t)we * 5 * Oa;
+  st.orbs[((size_t)w * N + e) * nmax + j] = ob[o];
+  for (int k = 0; k < 3; k++) st.dorbs[(((size_t)w * 3 + k) * N + e) * nmax + j] = ob[(1 + k) * Oa + o];
+  hb.ddorbs[((size_t)w * N + e) * nmax + j] = ob[4 * Oa + o];
+}
+
+// ---------------------------------------------------------------------------
+// matinv + ddx/d2dx2: CTA per (walker, spin); matrix in shared memory.
+// ---------------------------------------------------------------------------
+__global__ void k_slater_inv(WState st, HBuf hb) {
+  const int w = blockIdx.x >> 1, iab = blockIdx.x & 1;
+  if (w >= st.W) return;
+  const int N = cs.N, nmax = cs.nmax;
+  const int nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
+  const int n = nel;
+  extern __shared__ double smem[];
+  double *A = smem;              // n*n column-major: A(e,j) = orb of slot j at electron e
+  double *col = smem + n * n;    // n
+  __shared__ int ipvt[256];
+  __shared__ int s_p, s_sing;
+  double *slmi = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
+  if (n == 0) {
+    if (threadIdx.x == 0) st.detiab[2 * w + iab] = 1.0;
+    return;
+  }
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+    const int e = t % n, j = t / n;
+    A[t] = st.orbs[((size_t)w * N + ish + e) * nmax + j];
+  }
+  if (threadIdx.x == 0) s_sing = 0;
+  __syncthreads();
+  double det = 0;
+  if (n == 1) {
+    if (threadIdx.x == 0) {
+      det = A[0];
+      A[0] = 1.0 / A[0];
+      if (det == 0.0) s_sing = 1;
+    }
+  } else if (n == 2) {
+    if (threadIdx.x == 0) {
+      det = A[0] * A[3] - A[2] * A[1];
+      const double deti = 1.0 / det, aux = A[0];
+      A[0] = A[3] * deti;
+      A[3] = aux * deti;
+      A[1] = -A[1] * deti;
+      A[2] = -A[2] * deti;
+      if (det == 0.0) s_sing = 1;
+    }
+  } else {
+    // LU with partial pivoting (first entry of maximal |a|, as idamax)
+    for (int k = 0; k < n; k++) {
+      if (threadIdx.x < 32) {
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + threadIdx.x; i < n; i += 32) {
+          const double v = fabs(A[i + n * k]);
+          if (v > best) { best = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if (threadIdx.x == 0) {
+          s_p = bi;
+          ipvt[k] = bi;
+          if (A[bi + n * k] == 0.0) s_sing = 1;
+        }
+      }
+      __syncthreads();
+      if (s_sing) break;
+      const int p = s_p;
+      if (p != k)
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+          const double tmp = A[k + n * j];
+          A[k + n * j] = A[p + n * j];
+          A[p + n * j] = tmp;
+        }
+      __syncthreads();
+      const double piv = 1.0 / A[k + n * k];
+      for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) A[i + n * k] *= piv;
+      __syncthreads();
+      const int m = n - k - 1;
+      for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+        const int i = k + 1 + t % m, j = k + 1 + t / m;
+        A[i + n * j] -= A[i + n * k] * A[k + n * j];
+      }
+      __syncthreads();
+    }
+    if (!s_sing) {
+      if (threadIdx.x == 0) {
+        double det1 = 1.0, det2 = 0.0;
+        for (int i = 0; i < n; i++) {
+          if (ipvt[i] != i) det1 = -det1;
+          det1 = A[i + n * i] * det1;
+          if (det1 == 0.0) break;
+          while (fabs(det1) < 1.0) { det1 = 10.0 * det1; det2 = det2 - 1.0; }
+          while (fabs(det1) >= 10.0) { det1 = det1 / 10.0; det2 = det2 + 1.0; }
+        }
+        det = det1 * pow(10.0, det2);
+      }
+      // inv(U) in place, column by column
+      for (int j = 0; j < n; j++) {
+        if (threadIdx.x == 0) A[j + n * j] = 1.0 / A[j + n * j];
+        __syncthreads();
+        const double ajj = -A[j + n * j];
+        for (int i = threadIdx.x; i < j; i += blockDim.x) {
+          double s = 0;
+          for (int kk = i; kk < j; kk++) s += A[i + n * kk] * A[kk + n * j];
+          col[i] = s;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < j; i += blockDim.x) A[i + n * j] = col[i] * ajj;
+        __syncthreads();
+      }
+      // solve inv(A) * L = inv(U)
+      for (int j = n - 2; j >= 0; j--) {
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+          col[i] = A[i + n * j];
+          A[i + n * j] = 0.0;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          double s = 0;
+          for (int kk = j + 1; kk < n; kk++) s += A[i + n * kk] * col[kk];
+          A[i + n * j] -= s;
+        }
+        __syncthreads();
+      }
+      for (int j = n - 2; j >= 0; j--) {
+        const int jp = ipvt[j];
+        if (jp != j)
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double tmp = A[i + n * j];
+            A[i + n * j] = A[i + n * jp];
+            A[i + n * jp] = tmp;
+          }
+        __syncthreads();
+      }
+    }
+  }
+  __syncthreads();
+  if (s_sing) {
+    if (threadIdx.x == 0) st.status[w] = 1;
+    return;
+  }
+  if (threadIdx.x == 0) st.detiab[2 * w + iab] = det;
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) slmi[t] = A[t];
+  // ddx, d2dx2 (determinant.f90 ddot loops)
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    const int eg = ish + e;
+    for (int j = 0; j < n; j++) {
+      const double s = A[j + n * e];
+      a0 += s * st.dorbs[(((size_t)w * 3 + 0) * N + eg) * nmax + j];
+      a1 += s * st.dorbs[(((size_t)w * 3 + 1) * N + eg) * nmax + j];
+      a2 += s * st.dorbs[(((size_t)w * 3 + 2) * N + eg) * nmax + j];
+      a3 += s * hb.ddorbs[((size_t)w * N + eg) * nmax + j];
+    }
+    double *d = hb.ddx + ((size_t)w * N + eg) * 4;
+    d[0] = a0; d[1] = a1; d[2] = a2; d[3] = a3;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// c~ vectors: CTA per (walker, spin, 64-AO chunk).
+// ---------------------------------------------------------------------------
+__global__ void k_ctilde(WState st, HBuf hb, GSys g) {
+  const int nchunk = (cs.K + 63) / 64;
+  const int b = blockIdx.x;
+  const int chunk = b % nchunk, iab = (b / nchunk) & 1, w = b / (2 * nchunk);
+  if (w >= st.W) return;
+  const int nmax = cs.nmax, K = cs.K, Oa = cs.Oa, N = cs.N;
+  const int nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
+  if (nel == 0) return;
+  extern __shared__ double smem[];
+  double *S = smem;                 // nel*nel
+  double *Co = smem + nel * nel;    // [nel][64]
+  const double *slmi = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
+  for (int t = threadIdx.x; t < nel * nel; t += blockDim.x) S[t] = slmi[t];
+  const int m0 = chunk * 64;
+  for (int t = threadIdx.x; t < nel * 64; t += blockDim.x) {
+    const int j = t / 64, mm = t % 64;
+    Co[t] = (m0 + mm < K) ? g.coefT[(size_t)(m0 + mm) * Oa + g.slot_orb[iab * nmax + j]] : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nel * 64; t += blockDim.x) {
+    const int i = t / 64, mm = t % 64;
+    if (m0 + mm >= K) continue;
+    double s = 0;
+    for (int j = 0; j < nel; j++) s += S[j + nel * i] * Co[j * 64 + mm];
+    hb.ctilde[((size_t)w * N + ish + i) * K + m0 + mm] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pseudopotential: CTA per walker, one warp per quadrature point.
+// ---------------------------------------------------------------------------
+template <int NORD>
+__device__ __forceinline__ double psinl_d(double u, double rri, double rrj, int it) {
+  if (rri == cs.asymp_r && rrj == cs.asymp_r) return 0.0;
+  const double k = cs.scalek;
+  return een_poly<NORD, 0, double>(&cs.c[it * CW_MAX_TERMS], 1 - k * u, 1 - k * rri, 1 - k * rrj).fc;
+}
+__device__ __forceinline__ double psianl_d(double rri, int it) {
+  if (rri == cs.asymp_r) return 0.0;
+  const int na = cs.norda + 1;
+  double v = cs.a4[it * na] * rri / (1.0 + cs.a4[it * na + 1] * rri) - cs.asymp_jasa[it];
+  double rrip = rri;
+  for (int i = 2; i <= cs.norda; i++) {
+    rrip *= rri;
+    v += cs.a4[it * na + i] * rrip;
+  }
+  return v;
+}
+__device__ __forceinline__ double psibnl_d(double u, int isb, int ipar, double sspinn) {
+  if (u == cs.asymp_r) return 0.0;
+  const int nb = cs.nordb + 1;
+  double fee = cs.b[isb * nb] * u / (1 + cs.b[isb * nb + 1] * u);
+  double v = sspinn * fee - cs.asymp_jasb[ipar];
+  double uu = u;
+  for (int i = 2; i <= cs.nordb; i++) {
+    uu *= u;
+    v += cs.b[isb * nb + i] * uu;
+  }
+  return v;
+}
+
+template <int NORD>
+__global__ void k_ecp(WState st, HBuf hb, GSys g) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, M = cs.M, K = cs.K, NQ = cs.nquad;
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;  // warp q <-> quadrature point q
+  extern __shared__ double smem[];
+  double *rr_en = smem;                 // [N][M] scaled e-n distances
+  double *sx = rr_en + N * M;           // [3][N]
+  double *vps = sx + 3 * N;             // [M][4] channel potentials of the current electron
+  double *phiq = vps + 4 * M;           // [NQ][K]
+  double *rrq = phiq + (size_t)NQ * K;  // [NQ][M]
+  __shared__ int s_act[CW_MAX_CENT];
+  __shared__ int s_nact;
+  for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
+  __syncthreads();
+  for (int t = threadIdx.x; t < N * M; t += blockDim.x) {
+    const int jj = t / M, jc = t % M;
+    const double d0 = sx[jj] - cs.cent[3 * jc], d1 = sx[N + jj] - cs.cent[3 * jc + 1], d2 = sx[2 * N + jj] - cs.cent[3 * jc + 2];
+    rr_en[t] = scale0<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+  }
+  const double *xqw = st.xq + (size_t)w * 3 * NQ;
+  const double *fso = st.fso + (size_t)w * N * N;
+  double vp_acc[2] = {0, 0};
+  double vloc = 0;
+  for (int i = 0; i < N; i++) {
+    __syncthreads();
+    // vps of electron i for every centre (getvps_gauss)
+    for (int ic = threadIdx.x; ic < M; ic += blockDim.x) {
+      const int ict = cs.iwctype[ic];
+      const double d0 = sx[i] - cs.cent[3 * ic], d1 = sx[N + i] - cs.cent[3 * ic + 1], d2 = sx[2 * N + i] - cs.cent[3 * ic + 2];
+      const double r = fmax(1.0e-10, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+      const int lp = cs.lpot[ict];
+      vps[4 * ic + (lp - 1)] = gauss_pot_d(r, lp, ict) - cs.znuc[ict] * (1.0 / r);
+      for (int l = 1; l <= lp - 1; l++) vps[4 * ic + (l - 1)] = gauss_pot_d(r, l, ict);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int na = 0;
+      for (int ic = 0; ic < M; ic++) {
+        const int ict = cs.iwctype[ic];
+        vloc += vps[4 * ic + cs.lpot[ict] - 1];
+        int skip = 1;
+        for (int l = 1; l <= cs.lpot[ict] - 1; l++)
+          if (fabs(vps[4 * ic + l - 1]) > 1.0e-4) skip = 0;
+        if (!skip) s_act[na++] = ic;
+      }
+      s_nact = na;
+    }
+    __syncthreads();
+    const int na = s_nact;
+    if (q >= NQ) continue;
+    const int iab = i < cs.nup ? 0 : 1;
+    for (int a = 0; a < na; a++) {
+      const int ic = s_act[a];
+      const int ict = cs.iwctype[ic];
+      const double ri_v[3] = {sx[i] - cs.cent[3 * ic], sx[N + i] - cs.cent[3 * ic + 1], sx[2 * N + i] - cs.cent[3 * ic + 2]};
+      const double rin = sqrt(ri_v[0] * ri_v[0] + ri_v[1] * ri_v[1] + ri_v[2] * ri_v[2]);
+      const double xqq = xqw[q], yqq = xqw[NQ + q], zqq = xqw[2 * NQ + q];
+      const double costh = (ri_v[0] * xqq + ri_v[1] * yqq + ri_v[2] * zqq) * (1.0 / rin);
+      const double xp[3] = {rin * xqq + cs.cent[3 * ic], rin * yqq + cs.cent[3 * ic + 1], rin * zqq + cs.cent[3 * ic + 2]};
+      double *ph = phiq + (size_t)q * K;
+      double *rq = rrq + (size_t)q * M;
+      // distance_quad + basis values at the quadrature point (ider=0)
+      for (int jc = lane; jc < M; jc += 32) {
+        double xc[3] = {xp[0] - cs.cent[3 * jc], xp[1] - cs.cent[3 * jc + 1], xp[2] - cs.cent[3 * jc + 2]};
+        double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
+        if (jc == ic) r = rin;  // r_en_quad(iq,ic) = r_en(i,ic)
+        rq[jc] = scale0<double>(r);
+        basis_centre(g, jc, xc, 0, [&](int m, int d, double v) { if (d == 0) ph[m] = v; });
+      }
+      __syncwarp();
+      // determinant ratio (nonlocd_quad) via c~
+      const double *ct = hb.ctilde + ((size_t)w * N + i) * K;
+      double dr = 0;
+      for (int m = lane; m < K; m += 32) dr += ph[m] * ct[m];
+      dr = warp_sum(dr);
+      // Jastrow ratio (nonlocj_quad4)
+      double fsum = 0;
+      for (int jj = lane; jj < N; jj += 32) {
+        if (jj == i) continue;
+        const int pi = jj < i ? i : jj, pj = jj < i ? jj : i;
+        int isb, ipar;
+        double sspinn;
+        pair_spin(pi, pj, isb, ipar, sspinn);
+        const double dx0 = sx[jj] - xp[0], dx1 = sx[N + jj] - xp[1], dx2 = sx[2 * N + jj] - xp[2];
+        const double rij = sqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+        const double u = scale0<double>(rij);
+        double f = psibnl_d(u, isb, ipar, sspinn);
+        if (NORD > 1)
+          for (int jc = 0; jc < M; jc++) f += psinl_d<NORD>(u, rq[jc], rr_en[jj * M + jc], cs.iwctype[jc]);
+        fsum += f - fso[(size_t)i * N + jj];
+      }
+      double fen = 0;
+      for (int jc = lane; jc < M; jc += 32) fen += psianl_d(rq[jc], cs.iwctype[jc]);
+      fsum = warp_sum(fsum) + (warp_sum(fen) - fso[(size_t)i * N + i]);
+      double term = 0;
+      for (int l = 1; l <= cs.lpot[ict] - 1; l++) term += yl0_d(l, costh) * vps[4 * ic + (l - 1)];
+      vp_acc[iab] += term * cs.wq[q] * exp(fsum) * dr;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  __shared__ double s_vp[32][2];
+  if (lane == 0 && q < 32) {
+    s_vp[q][0] = vp_acc[0];
+    s_vp[q][1] = vp_acc[1];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int k = 0; k < NQ; k++) { a += s_vp[k][0]; b += s_vp[k][1]; }
+    hb.vpsp[2 * w] = a;
+    hb.vpsp[2 * w + 1] = b;
+    hb.pe_ecp[w] = vloc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// E_L assembly + metrop6's per-step sums (warp per walker).
+// mode: 0 = hpsi only (zerest, parity hook), 1 = end of a metrop6 sweep
+// ---------------------------------------------------------------------------
+__global__ void k_energy(WState st, HBuf hb, int mode, double *out_e, double *out_ekin) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= st.W) return;
+  const int N = cs.N;
+  const double hb_ = 0.5;
+  double ek[2] = {0, 0}, v2 = 0, pen = 0;
+  for (int e = lane; e < N; e += 32) {
+    const double *d = hb.ddx + ((size_t)w * N + e) * 4;
+    const double vx = st.fjo[((size_t)w * 3 + 0) * N + e], vy = st.fjo[((size_t)w * 3 + 1) * N + e],
+                 vz = st.fjo[((size_t)w * 3 + 2) * N + e];
+    const double tmp = -hb_ * (d[3] + 2.0 * (vx * d[0] + vy * d[1] + vz * d[2]));
+    ek[e < cs.nup ? 0 : 1] += tmp;
+    v2 += -hb_ * (vx * vx + vy * vy + vz * vz);
+    if (cs.nloc == 0) {
+      for (int ic = 0; ic < cs.M; ic++) {
+        const double d0 = st.x[((size_t)w * 3 + 0) * N + e] - cs.cent[3 * ic];
+        const double d1 = st.x[((size_t)w * 3 + 1) * N + e] - cs.cent[3 * ic + 1];
+        const double d2 = st.x[((size_t)w * 3 + 2) * N + e] - cs.cent[3 * ic + 2];
+        pen += -cs.znuc[cs.iwctype[ic]] / sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+      }
+    }
+  }
+  ek[0] = warp_sum(ek[0]);
+  ek[1] = warp_sum(ek[1]);
+  v2 = warp_sum(v2);
+  pen = warp_sum(pen);
+  if (lane != 0) return;
+  double pe = cs.pecent + hb.pe_ee[w];
+  if (cs.nloc == 0) pe += pen;
+  else pe += hb.pe_ecp[w];
+  const double vp0 = cs.nloc ? hb.vpsp[2 * w] : 0.0, vp1 = cs.nloc ? hb.vpsp[2 * w + 1] : 0.0;
+  const double ekin_other = -hb_ * hb.d2o[w] + v2;
+  const double e_other = ekin_other + pe;
+  const double energy = 0.0 + (ek[0] + vp0) + (ek[1] + vp1) + e_other;
+  const double ekin = 0.0 + ek[0] + ek[1] + ekin_other;
+  const double psid = st.detiab[2 * w] * st.detiab[2 * w + 1] * cs.cdet;
+  const double psij = st.fsumo[w];
+  st.eold[w] = energy;
+  st.ekino[w] = ekin;
+  st.psido[w] = psid;
+  st.psijo[w] = psij;
+  st.psi2o[w] = 2 * (log(fabs(psid)) + psij);
+  if (!isfinite(energy)) st.status[w] |= 2;
+  if (out_e) out_e[w] = energy;
+  if (out_ekin) out_ekin[w] = ekin;
+  if (mode == 1) {
+    const double wtg_sqrt = psid / psid * exp(psij - psij) / sqrt(1.0);
+    const double wtg = wtg_sqrt * wtg_sqrt;
+    double *s = st.sums + (size_t)w * 8;
+    s[0] += wtg;
+    s[1] += energy * wtg;
+    s[2] += (energy - ekin) * wtg;
+    s[3] += ekin * wtg;
+    s[5] += energy * wtg;
+    s[6] += energy * energy * wtg;
+  }
+}
+
+// rotqua (vmc/rotqua.f90:357): thread per walker
+__global__ void k_rotqua(WState st) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  DRng rng;
+  rng.load(st.rng + 4 * (size_t)w);
+  double x1, x2, x3, xsum;
+  int guard = 0;
+  do {
+    x1 = 1.0 - 2.0 * rng.uniform();
+    x2 = 1.0 - 2.0 * rng.uniform();
+    xsum = x1 * x1 + x2 * x2;
+  } while (xsum >= 1.0 && ++guard < 1000000);
+  double xsum2 = 2.0 * sqrt(fabs(1.0 - xsum));
+  x1 = x1 * xsum2;
+  x2 = x2 * xsum2;
+  x3 = 1.0 - 2.0 * xsum;
+  double theta = acos(x3), sthet = sin(theta), cfi, sfi;
+  if (sthet < 1.0e-05) {
+    cfi = 1; sfi = 0; x1 = 0; x2 = 0; x3 = 1; sthet = 0;
+  } else {
+    cfi = x1 / sthet;
+    sfi = x2 / sthet;
+  }
+  const double yy1 = x3 * cfi, yy2 = x3 * sfi, yy3 = -sthet;
+  const double zz1 = -sfi, zz2 = cfi, zz3 = 0.0;
+  double u1, u2, usum;
+  guard = 0;
+  do {
+    u1 = rng.uniform() * 2.0 - 1.0;
+    u2 = rng.uniform() * 2.0 - 1.0;
+    usum = u1 * u1 + u2 * u2;
+  } while (usum >= 1.0 && ++guard < 1000000);
+  const double uu = sqrt(usum);
+  u1 = u1 / uu;
+  u2 = u2 / uu;
+  const double y1 = yy1 * u1 + zz1 * u2, y2 = yy2 * u1 + zz2 * u2, y3 = yy3 * u1 + zz3 * u2;
+  const double z1 = yy1 * u2 - zz1 * u1, z2 = yy2 * u2 - zz2 * u1, z3 = yy3 * u2 - zz3 * u1;
+  const int NQ = cs.nquad;
+  double *xq = st.xq + (size_t)w * 3 * NQ;
+  for (int iq = 0; iq < NQ; iq++) {
+    xq[iq] = cs.xq0[iq] * x1 + cs.yq0[iq] * y1 + cs.zq0[iq] * z1;
+    xq[NQ + iq] = cs.xq0[iq] * x2 + cs.yq0[iq] * y2 + cs.zq0[iq] * z2;
+    xq[2 * NQ + iq] = cs.xq0[iq] * x3 + cs.yq0[iq] * y3 + cs.zq0[iq] * z3;
+  }
+  rng.store(st.rng + 4 * (size_t)w);
+}
+
+// zerest's nearest-nucleus tables: thread per (walker, electron)
+__global__ void k_nearest(WState st) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = cs.N;
+  if (t >= (long)st.W * N) return;
+  const int w = (int)(t / N), i = (int)(t % N);
+  double rmin = 99.0e9;
+  int near = 0;
+  double x[3];
+  for (int k = 0; k < 3; k++) x[k] = st.x[((size_t)w * 3 + k) * N + i];
+  for (int ic = 0; ic < cs.M; ic++) {
+    double r2 = 0;
+    for (int k = 0; k < 3; k++) {
+      const double d = x[k] - cs.cent[3 * ic + k];
+      r2 += d * d;
+    }
+    const double r = sqrt(r2);
+    if (r < rmin) { rmin = r; near = ic; }
+  }
+  st.rmino[(size_t)w * N + i] = rmin;
+  st.nearesto[(size_t)w * N + i] = near;
+  for (int k = 0; k < 3; k++) st.rvmino[((size_t)w * 3 + k) * N + i] = x[k] - cs.cent[3 * near + k];
+}
+
+}  // namespace cw

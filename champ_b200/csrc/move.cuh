@@ -1,0 +1,582 @@
+// move.cuh — single-electron accelerated-Metropolis move, batched over walkers.
+//
+// One move of electron `iel` for all walkers is five launches:
+//   k_propose       metrop6 proposal (vmc/metrop_mov1_slat.f90:131-361)
+//   k_jastrow_move  jastrow4e iflag=0 (vmc/jastrow4e.f90:3)
+//   k_basis_move    basis_fns for the moved electron (vmc/basis_fns.f90:8)
+//   gemm            LCAO contraction (vmc/orbitals_no_qmckl.f90:195)
+//   k_accept        ratio + drift at the new point, reverse transition
+//                   probability, accept/reject, and on accept the commit of
+//                   determinante/detsav (Sherman–Morrison) and jassav.
+#pragma once
+#include "common.cuh"
+
+namespace cw {
+
+__device__ __forceinline__ double thetamx_d(double r, double z) {
+  return cs.deltat + (2.0 - cs.deltat) / (1.0 + (z * r) * (z * r));
+}
+
+// gammai (vmc/gammai.f90:3)
+__device__ double gammai_d(double a, double x, double xae, int &iflag) {
+  if (x < a + 4) {
+    iflag = 1;
+    double ap = a, sum = 1 / a, del = sum;
+    int iter = (int)(21 + 3 * (x - a));
+    for (int n = 1; n <= iter; n++) {
+      ap = ap + 1;
+      del = del * x / ap;
+      sum = sum + del;
+    }
+    return sum * xae;
+  }
+  iflag = -1;
+  double a0 = 1, a1 = x, b0 = 0, b1 = 1, fac = 1, g = 0;
+  int iter = max(20 + (int)llround(a - x), 7);
+  for (int n = 1; n <= iter; n++) {
+    double an = (double)n, ana = an - a;
+    a0 = (a1 + a0 * ana) * fac;
+    b0 = (b1 + b0 * ana) * fac;
+    double anf = an * fac;
+    a1 = x * a0 + anf * a1;
+    b1 = x * b0 + anf * b1;
+    fac = 1 / a1;
+    g = b1 * fac;
+  }
+  return -(g * xae);
+}
+
+// Integral of the Slater-form radial transition density (metrop6 :246-280 / :480-512)
+__device__ double t_area_d(double zeta, double co, double rbot, double rtop, double bot) {
+  const double d5b2 = 2.5, d2b3 = .666666666666667, g5b2 = 1.329340388179137;
+  double rzero = -1.0 / co;
+  double zrbot = zeta * rbot, zrtop = zeta * rtop;
+  double zebot = sqrt(zrbot * zrbot * zrbot) * exp(-zrbot);
+  double zetop = sqrt(zrtop * zrtop * zrtop) * exp(-zrtop);
+  int iflagb, iflagt, iflagz;
+  double g52bot = gammai_d(d5b2, zrbot, zrbot * zebot, iflagb);
+  double g52top = gammai_d(d5b2, zrtop, zrtop * zetop, iflagt);
+  if (rzero < rbot || rzero > rtop) {
+    double g52dif = (iflagb * iflagt == 1) ? g52top - g52bot : g52top - g52bot + g5b2;
+    double g32dif = d2b3 * (g52dif + zetop - zebot);
+    return fabs(g32dif + co * g52dif / zeta) / (bot * sqrt(zeta * zeta * zeta));
+  }
+  double zrzer = zeta * rzero;
+  double zezer = sqrt(zrzer * zrzer * zrzer) * exp(-zrzer);
+  double g52zer = gammai_d(d5b2, zrzer, zrzer * zezer, iflagz);
+  double g52dif1 = (iflagb * iflagz == 1) ? g52zer - g52bot : g52zer - g52bot + g5b2;
+  double g32dif1 = d2b3 * (g52dif1 + zezer - zebot);
+  double g52dif2 = (iflagt * iflagz == 1) ? g52top - g52zer : g52top - g52zer + g5b2;
+  double g32dif2 = d2b3 * (g52dif2 + zetop - zezer);
+  return (fabs(g32dif1 + co * g52dif1 / zeta) + fabs(g32dif2 + co * g52dif2 / zeta)) /
+         (bot * sqrt(zeta * zeta * zeta));
+}
+
+__device__ __forceinline__ void spin_of(int iel, int &iab, int &nel, int &ish) {
+  if (iel < cs.nup) { iab = 0; nel = cs.nup; ish = 0; }
+  else { iab = 1; nel = cs.ndn; ish = cs.nup; }
+}
+
+// ---------------------------------------------------------------------------
+// Proposal: warp per walker.  Lanes form the drift at the old position
+// (compute_determinante_grad iflag_move=1: slmi column · dorb + vj), lane 0
+// then samples the move exactly as metrop6 does.
+// ---------------------------------------------------------------------------
+__global__ void k_propose(WState st, MoveBuf mb, int iel) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= st.W) return;
+  const int N = cs.N, nmax = cs.nmax;
+  int iab, nel, ish;
+  spin_of(iel, iab, nel, ish);
+  const int iloc = iel - ish;
+  const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * iloc;
+  double g0 = 0, g1 = 0, g2 = 0;
+  for (int j = lane; j < nel; j += 32) {
+    const double s = sl[j];
+    g0 += s * st.dorbs[(((size_t)w * 3 + 0) * N + iel) * nmax + j];
+    g1 += s * st.dorbs[(((size_t)w * 3 + 1) * N + iel) * nmax + j];
+    g2 += s * st.dorbs[(((size_t)w * 3 + 2) * N + iel) * nmax + j];
+  }
+  g0 = warp_sum(g0);
+  g1 = warp_sum(g1);
+  g2 = warp_sum(g2);
+  if (lane != 0) return;
+
+  const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, d3b2 = 1.5, eps = 1.0e-10;
+  const double deltar = cs.deltar, deltri = one / deltar, fbias = cs.fbias;
+  const double *fjo = st.fjo + (size_t)w * 3 * N;
+  double vo[3] = {0.0 + g0 + fjo[0 * N + iel], 0.0 + g1 + fjo[1 * N + iel], 0.0 + g2 + fjo[2 * N + iel]};
+  DRng rng;
+  rng.load(st.rng + 4 * (size_t)w);
+  MoveScratch m;
+  double fxop = one;
+  const int nearo = st.nearesto[(size_t)w * N + iel];
+  const double znear = cs.znuc[cs.iwctype[nearo]];
+  const double zcusp = (cs.nloc == 0) ? znear : zero;
+  double rv[3];
+  for (int k = 0; k < 3; k++) rv[k] = st.rvmino[((size_t)w * 3 + k) * N + iel];
+  const double rmin = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+  st.rmino[(size_t)w * N + iel] = rmin;
+  double rbot = rmin * deltri, rtop = rmin * deltar;
+  double voldr = zero;
+  for (int ic = 0; ic < 3; ic++) voldr += vo[ic] * rv[ic];
+  voldr = voldr / rmin;
+  double voldp = zero, xaxis[3], yaxis[3], zaxis[3];
+  for (int ic = 0; ic < 3; ic++) {
+    zaxis[ic] = rv[ic] / rmin;
+    xaxis[ic] = vo[ic] - voldr * zaxis[ic];
+    voldp += xaxis[ic] * xaxis[ic];
+  }
+  voldp = sqrt(voldp);
+  if (voldp < eps) {
+    xaxis[0] = eps * (one - zaxis[0] * zaxis[0]);
+    xaxis[1] = eps * (-zaxis[0] * zaxis[1]);
+    xaxis[2] = eps * (-zaxis[0] * zaxis[2]);
+    voldp = eps * sqrt(one - zaxis[0] * zaxis[0]);
+  }
+  for (int ic = 0; ic < 3; ic++) xaxis[ic] = xaxis[ic] / voldp;
+  voldr = fmax(voldr, -2 * znear);
+  yaxis[0] = zaxis[1] * xaxis[2] - zaxis[2] * xaxis[1];
+  yaxis[1] = zaxis[2] * xaxis[0] - zaxis[0] * xaxis[2];
+  yaxis[2] = zaxis[0] * xaxis[1] - zaxis[1] * xaxis[0];
+  voldp = voldp * fbias;
+  double root = (zcusp + voldr) * (zcusp + voldr - four / rmin), zeta;
+  if (root >= zero) {
+    root = sqrt(root);
+    zeta = half * (zcusp - voldr - root);
+    if (zeta <= zero) zeta = half * (zcusp - voldr + root);
+    if (zeta <= zero) zeta = eps;
+  } else {
+    zeta = (voldr < zero) ? -voldr - eps : one;
+  }
+  double co = (zeta + voldr) / (one - (zeta + voldr) * rmin);
+  root = sqrt((d3b2 * co - zeta) * (d3b2 * co - zeta) + two * zeta * co);
+  double rmax1 = (d3b2 * co - zeta + root) / (two * zeta * co);
+  if (rmax1 < rbot) rmax1 = rbot;
+  if (rmax1 > rtop) rmax1 = rtop;
+  double fmx = sqrt(rmax1) * fabs(one + co * rmax1) * exp(-zeta * rmax1);
+  if (co < zero) {
+    double rmax2 = (d3b2 * co - zeta - root) / (two * zeta * co);
+    if (rmax2 < rbot) rmax2 = rbot;
+    if (rmax2 > rtop) rmax2 = rtop;
+    double fmax2 = sqrt(rmax2) * fabs(one + co * rmax2) * exp(-zeta * rmax2);
+    fmx = fmx > fmax2 ? fmx : fmax2;
+  }
+  double bot = sqrt(rmin) * fabs(one + co * rmin) * exp(-zeta * rmin);
+  double rtry, top;
+  // rejection sampling of r; bounded so that a non-finite walker cannot spin
+  for (int guard = 0;; guard++) {
+    rtry = ((deltar - deltri) * rng.uniform() + deltri) * rmin;
+    top = sqrt(rtry) * fabs(one + co * rtry) * exp(-zeta * rtry);
+    double ratio = top / fmx;
+    if (ratio > rng.uniform()) break;
+    if (guard > 1000000) { st.status[w] |= 4; break; }
+  }
+  fxop = fxop * top / bot;
+  double areao = t_area_d(zeta, co, rbot, rtop, bot);
+  double raver = half * (rmin + rtry);
+  double deltt = thetamx_d(raver, znear);
+  double costht = one - deltt * rng.uniform();
+  double zprime = rtry * costht;
+  double sintht = sqrt(one - costht * costht);
+  areao = areao * deltt;
+  double term = fmin(voldp * raver * sintht, one);
+  fmx = one + term;
+  double phitry;
+  const double PI = 3.141592653589793115997963468544185161590576171875;
+  for (int guard = 0;; guard++) {
+    phitry = PI * rng.uniform();
+    double cosphi = cos(phitry);
+    top = one + term * cosphi;
+    if (top > rng.uniform() * fmx) break;
+    if (guard > 1000000) { st.status[w] |= 4; break; }
+  }
+  fxop = fxop * top;
+  double xprime = rtry * sintht * cos(phitry);
+  double yprime = sqrt(fmax(zero, rtry * rtry - xprime * xprime - zprime * zprime));
+  if (rng.uniform() < half) yprime = -yprime;
+  const double *cn = &cs.cent[3 * nearo];
+  double xn[3];
+  for (int ic = 0; ic < 3; ic++) {
+    const double d = xaxis[ic] * xprime + yaxis[ic] * yprime + zaxis[ic] * zprime;
+    xn[ic] = d + cn[ic];
+  }
+  m.rminno = rtry;
+  // geometrical rejection
+  double rminn = 99.0e9;
+  int nearn = 0;
+  for (int j = 0; j < cs.M; j++) {
+    double dist = zero;
+    for (int ic = 0; ic < 3; ic++) dist += (xn[ic] - cs.cent[3 * j + ic]) * (xn[ic] - cs.cent[3 * j + ic]);
+    if (dist < rminn) {
+      rminn = dist;
+      nearn = j;
+    }
+  }
+  rminn = sqrt(rminn);
+  double rminon = zero, dot = zero, rvminn[3], rvminon[3];
+  for (int ic = 0; ic < 3; ic++) {
+    rvminn[ic] = xn[ic] - cs.cent[3 * nearn + ic];
+    rvminon[ic] = st.x[((size_t)w * 3 + ic) * N + iel] - cs.cent[3 * nearn + ic];
+    rminon += rvminon[ic] * rvminon[ic];
+    dot += rvminn[ic] * rvminon[ic];
+  }
+  rminon = sqrt(rminon);
+  dot = dot / (rminn * rminon);
+  const double ravern = half * (rminn + rminon);
+  const double delttn = thetamx_d(ravern, cs.znuc[cs.iwctype[nearn]]);
+  m.igeo = (rminon > rminn * deltar || dot < one - delttn) ? 1 : 0;
+  for (int k = 0; k < 3; k++) {
+    m.xnew[k] = xn[k];
+    m.rvminn[k] = rvminn[k];
+    m.rvminon[k] = rvminon[k];
+  }
+  m.rminn = rminn;
+  m.rminon = rminon;
+  m.delttn = delttn;
+  m.fxop = fxop;
+  m.areao = areao;
+  m.rratio = m.rminno / rminon;
+  m.nearestn = nearn;
+  m.pad = 0;
+  mb.ms[w] = m;
+  rng.store(st.rng + 4 * (size_t)w);
+}
+
+// ---------------------------------------------------------------------------
+// jastrow4e, iflag=0: warp per walker, lanes over the partner electron.
+// Per-centre quantities of the moved electron are staged in shared memory.
+// ---------------------------------------------------------------------------
+template <int NORD>
+__global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
+  extern __shared__ double smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int M = cs.M, N = cs.N;
+  double *sh = smem + (size_t)wib * M * 6;  // per centre: rvec(3), r, scaled r, dd1
+  double *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M;
+  const bool active = (w < st.W);
+  int igeo = 1;
+  double xi[3] = {0, 0, 0};
+  if (active) {
+    const MoveScratch &m = mb.ms[w];
+    igeo = m.igeo;
+    xi[0] = m.xnew[0]; xi[1] = m.xnew[1]; xi[2] = m.xnew[2];
+  }
+  if (!active || igeo) return;  // whole warp leaves together (same walker)
+  for (int ic = lane; ic < M; ic += 32) {
+    double r2 = 0;
+    for (int k = 0; k < 3; k++) {
+      const double d = xi[k] - cs.cent[3 * ic + k];
+      sh_rv[k * M + ic] = d;
+      r2 += d * d;
+    }
+    const double r = sqrt(r2);
+    sh_r[ic] = r;
+    double rr, dd1, dd2;
+    scale2<double>(r, rr, dd1, dd2);
+    sh_s[ic] = rr;
+    sh_d[ic] = dd1;
+  }
+  __syncwarp();
+  const double kap = cs.scalek;
+  const double *xw = st.x + (size_t)w * 3 * N;
+  const double *fso_i = st.fso + ((size_t)w * N + iel) * N;
+  double dfs = 0, dv0 = 0, dv1 = 0, dv2 = 0;
+  for (int jj = lane; jj < N; jj += 32) {
+    if (jj == iel) continue;
+    const double xj[3] = {xw[jj], xw[N + jj], xw[2 * N + jj]};
+    const int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
+    int isb, ipar;
+    double sspinn;
+    pair_spin(i, j, isb, ipar, sspinn);
+    double rvee[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};  // x_iel - x_jj
+    const double rij = sqrt(rvee[0] * rvee[0] + rvee[1] * rvee[1] + rvee[2] * rvee[2]);
+    double u, dd1, dd2;
+    scale2<double>(rij, u, dd1, dd2);
+    double fs = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
+    if (u != cs.asymp_r) {
+      double fee, feeu, feeuu;
+      ee_term<1, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+      feeu = feeu * dd1 / rij;
+      fs += fee;
+      for (int k = 0; k < 3; k++) {
+        gi[k] += feeu * rvee[k];
+        gj[k] -= feeu * rvee[k];
+      }
+    }
+    if (NORD > 1) {
+      const double u1 = 1 - kap * u;
+      const double du = -kap * dd1;
+      for (int ic = 0; ic < M; ic++) {
+        const int it = cs.iwctype[ic];
+        const double rj_v[3] = {xj[0] - cs.cent[3 * ic], xj[1] - cs.cent[3 * ic + 1], xj[2] - cs.cent[3 * ic + 2]};
+        const double rj = sqrt(rj_v[0] * rj_v[0] + rj_v[1] * rj_v[1] + rj_v[2] * rj_v[2]);
+        double rrj, dd8, dd10;
+        scale2<double>(rj, rrj, dd8, dd10);
+        const double rri = sh_s[ic];
+        if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
+        const double ri = sh_r[ic];
+        const double dd7 = sh_d[ic];
+        const EenOut<double> e = een_poly<NORD, 1, double>(&cs.c[it * CW_MAX_TERMS], u1, 1 - kap * rri, 1 - kap * rrj);
+        const double fu = e.fu * du / rij;
+        const double fi = e.fi * (-kap * dd7) / ri;
+        const double fj = e.fj * (-kap * dd8) / rj;
+        fs += e.fc;
+        for (int k = 0; k < 3; k++) {
+          gi[k] += fi * sh_rv[k * M + ic] + fu * rvee[k];
+          gj[k] += fj * rj_v[k] - fu * rvee[k];
+        }
+      }
+    }
+    mb.fsn[(size_t)w * N + jj] = fs;
+    for (int k = 0; k < 3; k++) {
+      mb.fijn_i[((size_t)w * 3 + k) * N + jj] = gi[k];
+      mb.fijn_j[((size_t)w * 3 + k) * N + jj] = gj[k];
+    }
+    dfs += fs - fso_i[jj];
+    dv0 += gi[0] - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + jj];
+    dv1 += gi[1] - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + jj];
+    dv2 += gi[2] - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + jj];
+  }
+  // e-n part of the moved electron
+  double fen_s = 0, ge0 = 0, ge1 = 0, ge2 = 0;
+  for (int ic = lane; ic < M; ic += 32) {
+    const int it = cs.iwctype[ic];
+    const double rri = sh_s[ic];
+    if (rri == cs.asymp_r) continue;
+    const double ri = sh_r[ic];
+    const double dd7 = sh_d[ic];
+    double fen, feni, fenii;
+    en_term<1, double>(it, rri, fen, feni, fenii);
+    feni = feni * dd7 / ri;
+    fen_s += fen;
+    ge0 += feni * sh_rv[0 * M + ic];
+    ge1 += feni * sh_rv[1 * M + ic];
+    ge2 += feni * sh_rv[2 * M + ic];
+  }
+  fen_s = warp_sum(fen_s);
+  ge0 = warp_sum(ge0);
+  ge1 = warp_sum(ge1);
+  ge2 = warp_sum(ge2);
+  dfs = warp_sum(dfs);
+  dv0 = warp_sum(dv0);
+  dv1 = warp_sum(dv1);
+  dv2 = warp_sum(dv2);
+  if (lane == 0) {
+    mb.fsn[(size_t)w * N + iel] = fen_s;
+    mb.fijn_i[((size_t)w * 3 + 0) * N + iel] = ge0;
+    mb.fijn_i[((size_t)w * 3 + 1) * N + iel] = ge1;
+    mb.fijn_i[((size_t)w * 3 + 2) * N + iel] = ge2;
+    dfs += fen_s - fso_i[iel];
+    dv0 += ge0 - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + iel];
+    dv1 += ge1 - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + iel];
+    dv2 += ge2 - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + iel];
+    mb.fsumn[w] = st.fsumo[w] + dfs;
+    const double *fjo = st.fjo + (size_t)w * 3 * N;
+    mb.vjn[3 * w + 0] = fjo[0 * N + iel] + dv0;
+    mb.vjn[3 * w + 1] = fjo[1 * N + iel] + dv1;
+    mb.vjn[3 * w + 2] = fjo[2 * N + iel] + dv2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Basis functions of the moved electron: thread per (walker, centre).
+// ---------------------------------------------------------------------------
+__global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int M = cs.M, K = cs.K;
+  if (t >= (long)st.W * M) return;
+  const int w = (int)(t / M), ic = (int)(t % M);
+  const MoveScratch &m = mb.ms[w];
+  double *phi = mb.phi + (size_t)w * 4 * K;
+  if (m.igeo) {
+    // the GEMM still reads these rows: keep them finite
+    const int m0 = cs.ao_first[ic], m1 = cs.ao_first[ic + 1];
+    for (int a = m0; a < m1; a++)
+      for (int d = 0; d < 4; d++) phi[(size_t)d * K + a] = 0.0;
+    return;
+  }
+  const double xc[3] = {m.xnew[0] - cs.cent[3 * ic], m.xnew[1] - cs.cent[3 * ic + 1], m.xnew[2] - cs.cent[3 * ic + 2]};
+  basis_centre(g, ic, xc, 1, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
+}
+
+// ---------------------------------------------------------------------------
+// Accept / reject and commit: CTA per walker.
+// ---------------------------------------------------------------------------
+__global__ void k_accept(WState st, MoveBuf mb, GSys g, int iel) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+  const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
+  int iab, nel, ish;
+  spin_of(iel, iab, nel, ish);
+  const int iloc = iel - ish;
+  __shared__ double s_col[256];     // slmin column iel (= slmi column / ratio)
+  __shared__ double s_orb[256];     // new orbital values of the Slater columns
+  __shared__ int s_acc;
+  __shared__ double s_ratio;
+  const MoveScratch m = mb.ms[w];
+  double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
+  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const int *slot = g.slot_orb + iab * nmax;
+  if (wid == 0) {
+    double ratio = 0;
+    if (!m.igeo) {
+      for (int j = lane; j < nel; j += 32) {
+        const double o = orbn[slot[j]];
+        s_orb[j] = o;
+        ratio += sl[(size_t)nel * iloc + j] * o;
+      }
+      ratio = warp_sum(ratio);
+    }
+    double v0 = 0, v1 = 0, v2 = 0;
+    if (!m.igeo && ratio != 0.0) {
+      for (int j = lane; j < nel; j += 32) {
+        const double sc = sl[(size_t)nel * iloc + j] / ratio;
+        s_col[j] = sc;
+        v0 += sc * orbn[1 * Oa + slot[j]];
+        v1 += sc * orbn[2 * Oa + slot[j]];
+        v2 += sc * orbn[3 * Oa + slot[j]];
+      }
+      v0 = warp_sum(v0);
+      v1 = warp_sum(v1);
+      v2 = warp_sum(v2);
+    }
+    if (lane == 0) {
+      const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, eps = 1.0e-10;
+      DRng rng;
+      rng.load(st.rng + 4 * (size_t)w);
+      double p = zero, psidn = 0, psi2n = 0;
+      const double fsumn = mb.fsumn[w];
+      if (!m.igeo) {
+        const double detn = st.detiab[2 * w + iab] * ratio;
+        psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
+        if (detn != 0.0) {
+          const double vn[3] = {0.0 + v0 + mb.vjn[3 * w + 0], 0.0 + v1 + mb.vjn[3 * w + 1],
+                                0.0 + v2 + mb.vjn[3 * w + 2]};
+          psi2n = log(fabs(1.0)) + 2 * (log(fabs(psidn)) + fsumn);
+          const double deltar = cs.deltar, deltri = one / deltar;
+          const double rminn = m.rminn, rminon = m.rminon;
+          double rbot = rminn * deltri, rtop = rminn * deltar;
+          double vnewr = zero;
+          for (int ic = 0; ic < 3; ic++) vnewr += vn[ic] * m.rvminn[ic];
+          vnewr = vnewr / rminn;
+          double vnewp = zero, xaxis[3];
+          for (int ic = 0; ic < 3; ic++) {
+            xaxis[ic] = vn[ic] - vnewr * m.rvminn[ic] / rminn;
+            vnewp += xaxis[ic] * xaxis[ic];
+          }
+          vnewp = sqrt(vnewp);
+          if (vnewp < eps) {
+            xaxis[0] = eps * (one - m.rvminn[0] * m.rvminn[0]);
+            xaxis[1] = eps * (-m.rvminn[0] * m.rvminn[1]);
+            xaxis[2] = eps * (-m.rvminn[0] * m.rvminn[2]);
+            vnewp = eps * sqrt(one - m.rvminn[0] * m.rvminn[0] * (two - rminn * rminn));
+          }
+          for (int ic = 0; ic < 3; ic++) xaxis[ic] = xaxis[ic] / vnewp;
+          const double zn = cs.znuc[cs.iwctype[m.nearestn]];
+          const double zc = (cs.nloc == 0) ? zn : zero;
+          vnewr = fmax(vnewr, -2 * zn);
+          vnewp = vnewp * cs.fbias;
+          double root = (zc + vnewr) * (zc + vnewr - four / rminn), zeta;
+          if (root >= zero) {
+            root = sqrt(root);
+            zeta = half * (zc - vnewr - root);
+            if (zeta <= zero) zeta = half * (zc - vnewr + root);
+            if (zeta <= zero) zeta = eps;
+          } else {
+            zeta = (vnewr < zero) ? -vnewr - eps : one;
+          }
+          const double co = (zeta + vnewr) / (one - (zeta + vnewr) * rminn);
+          const double bot = sqrt(rminn) * fabs(one + co * rminn) * exp(-zeta * rminn);
+          const double top = sqrt(rminon) * fabs(one + co * rminon) * exp(-zeta * rminon);
+          double fxnp = one * top / bot;
+          double arean = t_area_d(zeta, co, rbot, rtop, bot);
+          arean = arean * m.delttn;
+          // costht/sintht of the reverse move (geometric block of metrop6)
+          double dot = 0;
+          for (int ic = 0; ic < 3; ic++) dot += m.rvminn[ic] * m.rvminon[ic];
+          dot = dot / (rminn * rminon);
+          const double costht = dot;
+          const double sintht = sqrt(one - costht * costht);
+          const double ravern = half * (rminn + rminon);
+          const double term = fmin(vnewp * ravern * sintht, one);
+          double cosphi = zero, rnorm = zero;
+          for (int ic = 0; ic < 3; ic++) {
+            const double term2 = m.rvminon[ic] / rminon - costht * m.rvminn[ic] / rminn;
+            rnorm += term2 * term2;
+            cosphi += term2 * xaxis[ic];
+          }
+          cosphi = cosphi / sqrt(rnorm);
+          fxnp = fxnp * (one + term * cosphi);
+          p = m.rratio * m.rratio * exp(psi2n - st.psi2o[w]) * fabs((fxnp * m.areao) / (m.fxop * arean));
+          p = fmin(one, p);
+        }
+      }
+      const int acc = (rng.uniform() < p) ? 1 : 0;
+      rng.store(st.rng + 4 * (size_t)w);
+      if (acc) {
+        st.psi2o[w] = psi2n;
+        st.psido[w] = psidn;
+        st.psijo[w] = fsumn;
+        st.fsumo[w] = fsumn;
+        st.detiab[2 * w + iab] = st.detiab[2 * w + iab] * ratio;
+        st.sums[(size_t)w * 8 + 4] += 1.0;
+        st.rmino[(size_t)w * N + iel] = m.rminn;
+        st.nearesto[(size_t)w * N + iel] = m.nearestn;
+        for (int k = 0; k < 3; k++) {
+          st.rvmino[((size_t)w * 3 + k) * N + iel] = m.rvminn[k];
+          st.x[((size_t)w * 3 + k) * N + iel] = m.xnew[k];
+        }
+      }
+      s_acc = acc;
+      s_ratio = ratio;
+    }
+  }
+  __syncthreads();
+  if (!s_acc) return;
+  const double ratio = s_ratio;
+  // --- detsav: Sherman–Morrison update of the spin block (determinante :47-62)
+  // rows k != iloc: slmi(:,k) -= slmi(:,iloc) * (slmi(:,k)·orb_new)/ratio
+  for (int k = wid; k < nel; k += nwarp) {
+    if (k == iloc) continue;
+    double s = 0;
+    for (int j = lane; j < nel; j += 32) s += sl[(size_t)nel * k + j] * s_orb[j];
+    s = warp_sum(s) / ratio;
+    for (int j = lane; j < nel; j += 32) sl[(size_t)nel * k + j] = sl[(size_t)nel * k + j] - sl[(size_t)nel * iloc + j] * s;
+  }
+  __syncthreads();
+  for (int j = tid; j < nel; j += blockDim.x) sl[(size_t)nel * iloc + j] = s_col[j];
+  // orbital rows of the moved electron
+  for (int j = tid; j < nel; j += blockDim.x) {
+    st.orbs[((size_t)w * N + iel) * nmax + j] = s_orb[j];
+    for (int k = 0; k < 3; k++)
+      st.dorbs[(((size_t)w * 3 + k) * N + iel) * nmax + j] = orbn[(1 + k) * Oa + slot[j]];
+  }
+  // --- jassav: pair tables and per-electron gradients
+  double *fso = st.fso + (size_t)w * N * N;
+  for (int jj = tid; jj < N; jj += blockDim.x) {
+    const double fsn = mb.fsn[(size_t)w * N + jj];
+    fso[(size_t)iel * N + jj] = fsn;
+    fso[(size_t)jj * N + iel] = fsn;
+    for (int k = 0; k < 3; k++) {
+      double *fij = st.fijo + ((size_t)w * 3 + k) * N * N;
+      const double gi = mb.fijn_i[((size_t)w * 3 + k) * N + jj];
+      if (jj == iel) {
+        fij[(size_t)iel * N + iel] = gi;
+        st.fjo[((size_t)w * 3 + k) * N + iel] = mb.vjn[3 * w + k];
+      } else {
+        const double gj = mb.fijn_j[((size_t)w * 3 + k) * N + jj];
+        const double old_ji = fij[(size_t)jj * N + iel];
+        st.fjo[((size_t)w * 3 + k) * N + jj] = st.fjo[((size_t)w * 3 + k) * N + jj] + gj - old_ji;
+        fij[(size_t)iel * N + jj] = gi;
+        fij[(size_t)jj * N + iel] = gj;
+      }
+    }
+  }
+}
+
+}  // namespace cw

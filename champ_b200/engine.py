@@ -1,0 +1,165 @@
+"""Host-side mirror of CHAMP's VMC driver over the CUDA walker engine.
+
+``Engine`` owns one ``cw_ctx`` (one molecule, one walker population) and
+exposes the batched drop-ins for CHAMP's per-walker routines with CHAMP's
+names and argument meaning:
+
+* ``set_walkers``  — mc_configs_start + zerest (vmc/mc_configs.f90:33,
+  vmc/acuest.f90:179)
+* ``vmc_steps``    — rotqua + metrop6 per step (vmc/vmc.f90:108-134)
+* ``end_block``    — acuest + acuest_reduce (vmc/acuest.f90:61)
+* ``results``      — finwrt (vmc/finwrt.f90:75)
+* ``hpsi``         — hpsi (vmc/hpsi.f90:3)
+* ``orbitals``, ``jastrow``, ``slater`` — orbitals / jastrow_factor /
+  determinant parity hooks.
+
+Every call goes through the C ABI of include/champ_b200.h; a nonzero status
+raises ``EngineError`` carrying cw_last_error, the way CHAMP's fatal_error
+aborts (module/m_error.f90:31).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .abi import CW_PREC_FP64, CW_PREC_MIXED, dptr, load_engine, u64ptr
+
+DEFAULT_SEED = "18123437465549275475255231234865"  # vmc/parser.f90:315
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+def seed_ints(cseed: str = DEFAULT_SEED) -> np.ndarray:
+    """read(cseed,'(8i4)') irn (vmc/parser.f90:651)."""
+    if len(cseed) < 32:
+        raise ValueError("Random number seed is shorter than 32 characters.")
+    return np.array([int(cseed[4 * i:4 * i + 4]) for i in range(8)], np.int32)
+
+
+def rng_states(nwalk: int, cseed: str = DEFAULT_SEED) -> np.ndarray:
+    """Stream of walker w = setrn(seed) + w jumps, as CHAMP's MPI rank w."""
+    lib = load_engine()
+    out = np.zeros((nwalk, 4), np.uint64)
+    irn = seed_ints(cseed)
+    rc = lib.cw_rng_states(irn.ctypes.data_as(C.POINTER(C.c_int32)), nwalk, u64ptr(out))
+    if rc:
+        raise EngineError("cw_rng_states failed")
+    return out
+
+
+def initial_configs(system, rng: np.ndarray):
+    """sites-based initial electrons of every walker; advances rng in place."""
+    lib = load_engine()
+    desc = system.desc()
+    W = rng.shape[0]
+    x = np.zeros((W, system.nelec, 3))
+    rc = lib.cw_sites(C.byref(desc), W, u64ptr(rng), dptr(x))
+    if rc:
+        raise EngineError("cw_sites failed")
+    return x
+
+
+class Engine:
+    def __init__(self, system, device: int = 0, precision: str = "fp64"):
+        self.lib = load_engine()
+        self.system = system
+        self._desc = system.desc()
+        self.h = C.c_void_p()
+        prec = {"fp64": CW_PREC_FP64, "mixed": CW_PREC_MIXED}[precision]
+        rc = self.lib.cw_create(C.byref(self.h), C.byref(self._desc), device, prec)
+        self._check(rc, "cw_create")
+        self.W = 0
+
+    def _check(self, rc, what):
+        if rc:
+            msg = self.lib.cw_last_error(self.h).decode() if self.h else ""
+            raise EngineError(f"{what} failed (status {rc}): {msg}")
+
+    def close(self):
+        if self.h:
+            self.lib.cw_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- walkers -----------------------------------------------------------
+    def set_walkers(self, x, rng):
+        x = np.ascontiguousarray(x, np.float64)
+        rng = np.ascontiguousarray(rng, np.uint64)
+        self.W = rng.shape[0]
+        self._check(self.lib.cw_set_walkers(self.h, self.W, dptr(x), u64ptr(rng)), "cw_set_walkers")
+
+    def walkers(self):
+        x = np.zeros((self.W, self.system.nelec, 3))
+        r = np.zeros((self.W, 4), np.uint64)
+        self._check(self.lib.cw_get_walkers(self.h, dptr(x), u64ptr(r)), "cw_get_walkers")
+        return x, r
+
+    # -- VMC driver --------------------------------------------------------
+    def vmc_steps(self, nstep: int):
+        self._check(self.lib.cw_vmc_steps(self.h, nstep), "cw_vmc_steps")
+
+    def last_ms(self) -> float:
+        return float(self.lib.cw_last_ms(self.h))
+
+    def end_block(self) -> float:
+        e = np.zeros(1)
+        self._check(self.lib.cw_end_block(self.h, dptr(e)), "cw_end_block")
+        return float(e[0])
+
+    def results(self) -> dict:
+        o = np.zeros(8)
+        self._check(self.lib.cw_results(self.h, dptr(o)), "cw_results")
+        return dict(energy=o[0], err=o[1], sigma=o[2], tcorr=o[3], accept=o[4], pe=o[5], ke=o[6],
+                    nblocks=o[7])
+
+    def sums(self):
+        out = np.zeros((self.W, 5))
+        self._check(self.lib.cw_get_sums(self.h, dptr(out)), "cw_get_sums")
+        return out
+
+    def state(self):
+        e, p, j = np.zeros(self.W), np.zeros(self.W), np.zeros(self.W)
+        self._check(self.lib.cw_get_state(self.h, dptr(e), dptr(p), dptr(j)), "cw_get_state")
+        return e, p, j
+
+    # -- per-walker routines ----------------------------------------------
+    def hpsi(self, quad=None) -> dict:
+        W = self.W
+        e, p, j, k = np.zeros(W), np.zeros(W), np.zeros(W), np.zeros(W)
+        if quad is None:
+            rc = self.lib.cw_hpsi(self.h, None, None, None, dptr(e), dptr(p), dptr(j), dptr(k))
+        else:
+            q = [np.ascontiguousarray(a, np.float64) for a in quad]
+            rc = self.lib.cw_hpsi(self.h, dptr(q[0]), dptr(q[1]), dptr(q[2]), dptr(e), dptr(p), dptr(j), dptr(k))
+        self._check(rc, "cw_hpsi")
+        return dict(energy=e, psid=p, psij=j, ekin=k)
+
+    def orbitals(self):
+        s = self.system
+        orb = np.zeros((self.W, s.norb, s.nelec))
+        dorb = np.zeros((self.W, 3, s.nelec, s.norb))
+        ddorb = np.zeros((self.W, s.nelec, s.norb))
+        self._check(self.lib.cw_orbitals(self.h, dptr(orb), dptr(dorb), dptr(ddorb)), "cw_orbitals")
+        return orb, dorb, ddorb
+
+    def jastrow(self):
+        psij = np.zeros(self.W)
+        v = np.zeros((self.W, self.system.nelec, 3))
+        d2 = np.zeros(self.W)
+        self._check(self.lib.cw_jastrow(self.h, dptr(psij), dptr(v), dptr(d2)), "cw_jastrow")
+        return psij, v, d2
+
+    def slater(self):
+        nmax = max(self.system.nup, self.system.ndn)
+        slmi = np.zeros((self.W, 2, nmax * nmax))
+        det = np.zeros((self.W, 2))
+        self._check(self.lib.cw_slater(self.h, dptr(slmi), dptr(det)), "cw_slater")
+        return slmi, det

@@ -1,0 +1,568 @@
+"""Molecular systems for the walker engine.
+
+``System`` holds the contents of CHAMP's modules after ``parser()`` for one
+molecule, laid out as in ``cw_system_desc`` (C order == Fortran order
+reversed).  The set-up steps CHAMP performs while reading its input are
+restated here because every engine input passes through them:
+
+* ``prepare_radial``  — read_bas_num (vmc/read_bas_num.f90:11-247): small-r
+  polynomial fit, cutoff radius, large-r exponential fit (fitting.f90
+  exp_fit), cubic-spline second derivatives (vmc/spline2.f90:3);
+* ``tabulate_gaussians`` — the numerical-grid tabulation of contracted
+  Gaussians of CHAMP's converter (tools/trex_tools/trex2champ.py:560-760:
+  grid type 3, 2000 points, arg 1.003, r0 20, gnorm normalisation);
+* ``cuspexact4`` — e-e-n cusp conditions (vmc/cuspinit4.f90:3,
+  vmc/cuspexact4.f90:3);
+* ``gesqua`` — the angular quadrature (vmc/rotqua.f90:3);
+* ``pot_nn`` — nuclear repulsion.
+
+``make_synthetic`` builds the seeded synthetic molecules the benchmarks run
+on (no public data set is involved).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .abi import CW_MGAUSS, CW_MPS_L, CW_NCOEF, CwSystemDesc, dptr, iptr
+
+# ---------------------------------------------------------------------------
+# CHAMP set-up restatements
+# ---------------------------------------------------------------------------
+
+
+def spline2(x, y, yp1, ypn):
+    """spline2 (vmc/spline2.f90:3): second derivatives of the cubic spline."""
+    n = len(x)
+    y2 = np.zeros(n)
+    work = np.zeros(n)
+    if yp1 > 1e30:
+        y2[0] = 0.0
+        work[0] = 0.0
+    else:
+        y2[0] = -0.5
+        work[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1)
+    for i in range(1, n - 1):
+        sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1])
+        p = sig * y2[i - 1] + 2.0
+        y2[i] = (sig - 1.0) / p
+        work[i] = (6.0 * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1])
+                          / (x[i] - x[i - 1])) / (x[i + 1] - x[i - 1]) - sig * work[i - 1]) / p
+    if ypn > 1e30:
+        qn = 0.0
+        workn = 0.0
+    else:
+        qn = 0.5
+        workn = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]))
+    y2[n - 1] = (workn - qn * work[n - 2]) / (qn * y2[n - 2] + 1.0)
+    for k in range(n - 2, -1, -1):
+        y2[k] = y2[k] * y2[k + 1] + work[k]
+    return y2
+
+
+def exp_fit(x, y):
+    """exp_fit (vmc/fitting.f90:11): least squares of log|y| = A - b x."""
+    n = len(x)
+    w = np.log(np.abs(y))
+    x_sum = float(np.sum(x))
+    w_sum = float(np.sum(w))
+    xw_sum = float(np.sum(x * w))
+    xx_sum = float(np.sum(x * x))
+    x_mean, w_mean = x_sum / n, w_sum / n
+    denom = xx_sum - n * x_mean * x_mean
+    b = (n * x_mean * w_mean - xw_sum) / denom
+    a = math.exp((w_mean * xx_sum - x_mean * xw_sum) / denom)
+    return a, b
+
+
+def prepare_radial(x, rwf_cols, igrid, arg, r0_in, znuc, nloc, lvals=None, icusp=0):
+    """read_bas_num (vmc/read_bas_num.f90:11-247) for one atom type.
+
+    x: grid as read from the basis file, rwf_cols: (nrbas, nr) values.
+    Returns dict(arg, r0, rwf, d2rwf, ce, ae, rmaxwf).
+    """
+    nr = len(x)
+    nrbas = rwf_cols.shape[0]
+    if igrid == 2 and arg <= 1.0:
+        arg = x[1] / x[0]
+    r0 = r0_in
+    if igrid == 3:
+        r0 = r0_in / (arg ** (nr - 1) - 1.0)
+    cutoff_rmax = 1.0e-12
+    ce = np.zeros((nrbas, CW_NCOEF))
+    ae = np.zeros((nrbas, 2))
+    rmaxwf = np.zeros(nrbas)
+    d2 = np.zeros((nrbas, nr))
+    for irb in range(nrbas):
+        y = rwf_cols[irb]
+        if nloc == 0 and lvals is not None and lvals[irb] == 0 and icusp == 1:
+            n1 = CW_NCOEF - 1
+            A = np.zeros((n1, n1))
+            A[:, 0] = 1.0 - znuc * x[:n1]
+            for jj in range(2, CW_NCOEF):
+                A[:, jj - 1] = x[:n1] ** jj
+            sol = np.linalg.solve(A, y[:n1].copy())
+            ce[irb, 0] = sol[0]
+            ce[irb, 1] = -znuc * sol[0]
+            ce[irb, 2:5] = sol[1:4]
+        else:
+            A = np.array([[x[ii] ** jj for jj in range(CW_NCOEF)] for ii in range(CW_NCOEF)])
+            ce[irb] = np.linalg.solve(A, y[:CW_NCOEF].copy())
+        dwf1 = 0.0
+        for icoef in range(2, CW_NCOEF + 1):
+            dwf1 += (icoef - 1) * ce[irb, icoef - 1] * (x[0] ** (icoef - 2))
+        rmax = x[nr - 1]
+        for ir in range(nr - 1, -1, -1):
+            if abs(y[ir]) > cutoff_rmax:
+                rmax = x[ir]
+                break
+        if abs(rmax - x[nr - 1]) < 1.0e-10:
+            a, b = exp_fit(x[nr - 10:], y[nr - 10:])
+            if b < 0:
+                raise ValueError("BASIS_READ_NUM: ak<0")
+            ae[irb] = (a, b)
+            rmax = -math.log(cutoff_rmax / abs(a)) / b
+            dwfn = -b * a * math.exp(-b * x[nr - 1])
+        else:
+            dwfn = 0.0
+        rmaxwf[irb] = rmax
+        d2[irb] = spline2(x, y, dwf1, dwfn)
+    return dict(arg=arg, r0=r0, rwf=rwf_cols.copy(), d2rwf=d2, ce=ce, ae=ae, rmaxwf=rmaxwf)
+
+
+def gnorm(alp, l):
+    """Normalisation of a primitive Gaussian (trex2champ.py write_champ_file_basis_grid)."""
+    if l == 0:
+        return (2.0 * alp) ** (3.0 / 4.0) * 2.0 * (1.0 / (np.pi ** (1.0 / 4.0)))
+    if l == 1:
+        return (2.0 * alp) ** (5.0 / 4.0) * np.sqrt(8.0 / 3.0) * (1.0 / (np.pi ** (1.0 / 4.0)))
+    if l == 2:
+        return (2.0 * alp) ** (7.0 / 4.0) * np.sqrt(16.0 / 15.0) * (1.0 / (np.pi ** (1.0 / 4.0)))
+    if l == 3:
+        return (2.0 * alp) ** (9.0 / 4.0) * np.sqrt(32.0 / 105.0) * (1.0 / (np.pi ** (1.0 / 4.0)))
+    if l == 4:
+        return (2.0 * alp) ** (11.0 / 4.0) * np.sqrt(64.0 / 945.0) * (1.0 / (np.pi ** (1.0 / 4.0)))
+    return 1.0
+
+
+GRID_TYPE, GRID_POINTS, GRID_ARG, GRID_R0 = 3, 2000, 1.003, 20.0
+
+
+def _round12(a):
+    # the converter writes ' %.12e'; CHAMP reads those rounded values back
+    return np.array([float(f"{v:.12e}") for v in np.ravel(a)]).reshape(np.shape(a))
+
+
+def tabulate_gaussians(shells):
+    """Radial grid file contents for one atom type.
+
+    shells: list of (l, exponents, coefficients).  Returns (x, rwf[nshell, nr])
+    rounded as the converter writes them.
+    """
+    r0 = GRID_R0 / (GRID_ARG ** (GRID_POINTS - 1) - 1)
+    i = np.arange(GRID_POINTS)
+    x = r0 * GRID_ARG ** i - r0
+    r2 = x * x
+    rwf = np.zeros((len(shells), GRID_POINTS))
+    for s, (l, ex, co) in enumerate(shells):
+        v = np.zeros(GRID_POINTS)
+        for e, c in zip(ex, co):
+            v += gnorm(e, l) * c * np.exp(-e * r2)
+        rwf[s] = v
+    return _round12(x), _round12(rwf)
+
+
+def nterms4(nord):
+    i = 0
+    for n in range(2, nord + 1):
+        for k in range(n - 1, -1, -1):
+            l_hi = n - k - 2 if k == 0 else n - k
+            for l in range(l_hi, -1, -1):
+                m = (n - k - l) // 2
+                if 2 * m == n - k - l:
+                    i += 1
+    return i
+
+
+def cuspinit4(nordc):
+    """cuspinit4 (vmc/cuspinit4.f90:3): constraint matrix d and fixed terms iwc4."""
+    nt = nterms4(nordc)
+    neq = 2 * (nordc - 1)
+    d = np.zeros((neq + 1, nt + 1))  # 1-based
+    iwc4 = [0] * (neq + 1)
+    i = 0
+    for n in range(2, nordc + 1):
+        for k in range(n - 1, -1, -1):
+            l_hi = n - k - 2 if k == 0 else n - k
+            for l in range(l_hi, -1, -1):
+                m = (n - k - l) // 2
+                if 2 * m == n - k - l:
+                    i += 1
+                    if k == 1 and iwc4[n - 1] == 0:
+                        iwc4[n - 1] = i
+                    if k == 0 and iwc4[n + nordc - 2] == 0:
+                        iwc4[n + nordc - 2] = i
+                    iord = l + 2 * m
+                    d[iord, i] -= 2 * k
+                    if l + m > 0:
+                        d[nordc - 1 + k + m, i] -= (l + m)
+                    if m > 0:
+                        d[nordc - 1 + k + l + m, i] -= m
+    return d, iwc4, nt
+
+
+def cuspexact4(c, nordc):
+    """cuspexact4 (vmc/cuspexact4.f90:3) applied to c[nctype, nterms] in place."""
+    if nordc <= 1:
+        return c
+    d, iwc4, nt = cuspinit4(nordc)
+    cc = np.zeros(nt + 1)
+    order = list(range(1, nordc)) + list(range(nordc + 1, 2 * (nordc - 1) + 1)) + [nordc]
+    for it in range(c.shape[0]):
+        cc[1:] = c[it]
+        for i in order:
+            s = 0.0
+            for j in range(1, nt + 1):
+                if j != iwc4[i]:
+                    s += d[i, j] * cc[j]
+            cc[iwc4[i]] = -s / d[i, iwc4[i]]
+        c[it] = cc[1:]
+    return c
+
+
+def gesqua(nq):
+    """gesqua (vmc/rotqua.f90:3) for the tetrahedron (4) and octahedron (6) rules."""
+    if nq == 4:
+        q = 1.0 / math.sqrt(3.0)
+        xq = np.array([q, q, -q, -q])
+        yq = np.array([q, -q, q, -q])
+        zq = np.array([q, -q, -q, q])
+        return xq, yq, zq, np.full(4, 0.25)
+    if nq != 6:
+        raise ValueError("only nquad 4 or 6 are generated here")
+    xq = np.array([1.0, -1.0, 0, 0, 0, 0])
+    yq = np.array([0, 0, 1.0, -1.0, 0, 0])
+    zq = np.array([0, 0, 0, 0, 1.0, -1.0])
+    return xq, yq, zq, np.full(6, 1.0 / 6.0)
+
+
+def pot_nn(cent, znuc, iwctype):
+    pe = 0.0
+    for i in range(1, len(cent)):
+        for j in range(i):
+            r = math.sqrt(sum((cent[i][k] - cent[j][k]) ** 2 for k in range(3)))
+            pe += znuc[iwctype[i]] * znuc[iwctype[j]] / r
+    return pe
+
+
+# ---------------------------------------------------------------------------
+# System container
+# ---------------------------------------------------------------------------
+
+# Slm index sets per shell type (vmc/slm.f90 table)
+SLM_OF_L = {0: [1], 1: [2, 3, 4], 2: [5, 6, 7, 8, 9, 10], 3: list(range(11, 21)), 4: list(range(21, 36))}
+
+
+@dataclass
+class System:
+    name: str
+    nelec: int
+    nup: int
+    iwctype: np.ndarray
+    cent: np.ndarray
+    znuc: np.ndarray
+    # numerical basis per type
+    nrbas: np.ndarray
+    igrid: np.ndarray
+    nr: np.ndarray
+    arg: np.ndarray
+    r0: np.ndarray
+    rwf: np.ndarray
+    d2rwf: np.ndarray
+    ce: np.ndarray
+    ae: np.ndarray
+    rmaxwf: np.ndarray
+    nbastyp: np.ndarray
+    iwlbas: np.ndarray
+    iwrwf: np.ndarray
+    coef: np.ndarray      # [norb, nbasis]
+    iworbd: np.ndarray    # [ndet, nelec]
+    cdet: np.ndarray
+    norda: int
+    nordb: int
+    nordc: int
+    scalek: float
+    a4: np.ndarray
+    b: np.ndarray
+    c: np.ndarray
+    isc: int = 2
+    nspin2b: int = 1
+    nocuspb: int = 0
+    nloc: int = 0
+    lpot: np.ndarray | None = None
+    necp_term: np.ndarray | None = None
+    necp_power: np.ndarray | None = None
+    ecp_exponent: np.ndarray | None = None
+    ecp_coef: np.ndarray | None = None
+    nquad: int = 0
+    xq0: np.ndarray | None = None
+    yq0: np.ndarray | None = None
+    zq0: np.ndarray | None = None
+    wq: np.ndarray | None = None
+    deltar: float = 5.0
+    deltat: float = 1.0
+    fbias: float = 1.0
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def ncent(self):
+        return len(self.iwctype)
+
+    @property
+    def nctype(self):
+        return len(self.znuc)
+
+    @property
+    def ndn(self):
+        return self.nelec - self.nup
+
+    @property
+    def nbasis(self):
+        return self.coef.shape[1]
+
+    @property
+    def norb(self):
+        return self.coef.shape[0]
+
+    @property
+    def pecent(self):
+        return pot_nn(self.cent, self.znuc, self.iwctype)
+
+    def desc(self) -> CwSystemDesc:
+        """ctypes cw_system_desc pointing at this object's arrays."""
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        keep = []
+
+        def D(a):
+            a = f64(a)
+            keep.append(a)
+            return dptr(a)
+
+        def I(a):
+            a = i32(a)
+            keep.append(a)
+            return iptr(a)
+
+        d = CwSystemDesc()
+        d.nelec, d.nup, d.ncent, d.nctype = self.nelec, self.nup, self.ncent, self.nctype
+        d.iwctype, d.cent, d.znuc = I(self.iwctype), D(self.cent), D(self.znuc)
+        d.pecent = self.pecent
+        d.mrwf, d.mrwf_pts = self.rwf.shape[1], self.rwf.shape[2]
+        d.nrbas, d.igrid, d.nr = I(self.nrbas), I(self.igrid), I(self.nr)
+        d.arg, d.r0 = D(self.arg), D(self.r0)
+        d.rwf, d.d2rwf, d.ce, d.ae, d.rmaxwf = (D(self.rwf), D(self.d2rwf), D(self.ce), D(self.ae),
+                                               D(self.rmaxwf))
+        d.mbastyp = self.iwlbas.shape[1]
+        d.nbastyp, d.iwlbas, d.iwrwf = I(self.nbastyp), I(self.iwlbas), I(self.iwrwf)
+        d.nbasis, d.norb = self.nbasis, self.norb
+        d.coef = D(self.coef)
+        d.ndet = len(self.cdet)
+        d.iworbd, d.cdet = I(self.iworbd), D(self.cdet)
+        d.norda, d.nordb, d.nordc = self.norda, self.nordb, self.nordc
+        d.isc, d.nspin2b, d.nocuspb = self.isc, self.nspin2b, self.nocuspb
+        d.scalek = self.scalek
+        d.a4, d.b = D(self.a4), D(self.b)
+        d.c = D(self.c if self.c.size else np.zeros(1))
+        d.nloc = self.nloc
+        if self.nloc > 0:
+            d.lpot, d.necp_term, d.necp_power = I(self.lpot), I(self.necp_term), I(self.necp_power)
+            d.ecp_exponent, d.ecp_coef = D(self.ecp_exponent), D(self.ecp_coef)
+            d.nquad = self.nquad
+            d.xq0, d.yq0, d.zq0, d.wq = D(self.xq0), D(self.yq0), D(self.zq0), D(self.wq)
+        else:
+            d.nquad = 0
+        d.deltar, d.deltat, d.fbias = self.deltar, self.deltat, self.fbias
+        self._keep = keep
+        return d
+
+
+def assemble_basis(types):
+    """Pack per-type radial tables into the padded arrays of cw_system_desc.
+
+    types: list of dicts with keys x, rwf (nrbas, nr), shells_l (per radial
+    function, its l), aos: list of (slm, irb) and prepared radial data.
+    """
+    nct = len(types)
+    mrwf = max(t["prep"]["rwf"].shape[0] for t in types)
+    mpts = max(t["prep"]["rwf"].shape[1] for t in types)
+    mbas = max(len(t["aos"]) for t in types)
+    rwf = np.zeros((nct, mrwf, mpts))
+    d2 = np.zeros((nct, mrwf, mpts))
+    ce = np.zeros((nct, mrwf, CW_NCOEF))
+    ae = np.zeros((nct, mrwf, 2))
+    rmax = np.zeros((nct, mrwf))
+    iwl = np.zeros((nct, mbas), np.int32)
+    iwr = np.zeros((nct, mbas), np.int32)
+    for it, t in enumerate(types):
+        p = t["prep"]
+        n, npt = p["rwf"].shape
+        rwf[it, :n, :npt] = p["rwf"]
+        d2[it, :n, :npt] = p["d2rwf"]
+        ce[it, :n] = p["ce"]
+        ae[it, :n] = p["ae"]
+        rmax[it, :n] = p["rmaxwf"]
+        for ib, (slm, irb) in enumerate(t["aos"]):
+            iwl[it, ib] = slm
+            iwr[it, ib] = irb
+    return dict(
+        nrbas=np.array([t["prep"]["rwf"].shape[0] for t in types], np.int32),
+        igrid=np.array([t["igrid"] for t in types], np.int32),
+        nr=np.array([t["prep"]["rwf"].shape[1] for t in types], np.int32),
+        arg=np.array([t["prep"]["arg"] for t in types]),
+        r0=np.array([t["prep"]["r0"] for t in types]),
+        rwf=rwf, d2rwf=d2, ce=ce, ae=ae, rmaxwf=rmax,
+        nbastyp=np.array([len(t["aos"]) for t in types], np.int32), iwlbas=iwl, iwrwf=iwr)
+
+
+# ---------------------------------------------------------------------------
+# Seeded synthetic systems
+# ---------------------------------------------------------------------------
+
+def _random_shells(rng, spec):
+    """spec: list of (l, count); 3 primitives per shell, exponents log-uniform in [0.1, 20]."""
+    shells = []
+    for l, cnt in spec:
+        for _ in range(cnt):
+            ex = np.exp(rng.uniform(np.log(0.1), np.log(20.0), size=3))
+            co = rng.uniform(0.2, 1.0, size=3)
+            shells.append((l, ex, co))
+    return shells
+
+
+def _type_from_shells(shells, znuc, nloc):
+    x, rwf = tabulate_gaussians(shells)
+    prep = prepare_radial(x, rwf, GRID_TYPE, GRID_ARG, GRID_R0, znuc, nloc)
+    aos = []
+    for irb, (l, _, _) in enumerate(shells):
+        for slm in SLM_OF_L[l]:
+            aos.append((slm, irb + 1))
+    return dict(prep=prep, aos=aos, igrid=GRID_TYPE)
+
+
+def _bfd_like_ecp(rng, zval, lpot):
+    """Seeded BFD-form semilocal ECP: local channel removes the -Z/r singularity."""
+    nterm = np.zeros(CW_MPS_L, np.int32)
+    power = np.zeros((CW_MPS_L, CW_MGAUSS), np.int32)
+    expo = np.zeros((CW_MPS_L, CW_MGAUSS))
+    coef = np.zeros((CW_MPS_L, CW_MGAUSS))
+    if lpot == 1:  # zero-coefficient local term (bare Coulomb atom)
+        nterm[0] = 1
+        power[0, 0] = 2
+        expo[0, 0] = 1.0
+        coef[0, 0] = 0.0
+        return nterm, power, expo, coef
+    f = lambda v: v * rng.uniform(0.8, 1.2)
+    # local channel stored at index lpot-1 (CHAMP idx=lpot)
+    a1 = f(8.36)
+    loc = lpot - 1
+    nterm[loc] = 3
+    power[loc, :3] = (1, 3, 2)
+    expo[loc, :3] = (a1, f(4.48), f(3.94))
+    coef[loc, :3] = (zval, zval * a1, -f(19.2))
+    # nonlocal channels l = 0 .. lpot-2 stored at index l
+    for l in range(lpot - 1):
+        nterm[l] = 1
+        power[l, 0] = 2
+        expo[l, 0] = f(5.03)
+        coef[l, 0] = f(22.6)
+    return nterm, power, expo, coef
+
+
+def _jastrow(rng, nctype, cusp_a1, nord=5):
+    a4 = rng.normal(0.0, 0.05, size=(nctype, nord + 1))
+    a4[:, 0] = cusp_a1
+    b = rng.normal(0.0, 0.05, size=(1, nord + 1))
+    b[0, 0] = 0.5
+    nt = nterms4(nord)
+    c = rng.normal(0.0, 0.05, size=(nctype, nt))
+    cuspexact4(c, nord)
+    return a4, b, c
+
+
+def _orthonormal(rng, k, o):
+    q, _ = np.linalg.qr(rng.normal(size=(k, o)))
+    return np.ascontiguousarray(q.T)  # [norb, nbasis]
+
+
+def _assemble(name, rng, cent, types_of_centre, type_defs, nelec, nup, norb, nocc_up, nocc_dn,
+              nloc=4, nquad=6):
+    nct = len(type_defs)
+    basis = assemble_basis([td["basis"] for td in type_defs])
+    nbasis = int(sum(len(type_defs[t]["basis"]["aos"]) for t in types_of_centre))
+    znuc = np.array([td["z"] for td in type_defs], float)
+    coef = _orthonormal(rng, nbasis, norb)
+    iworbd = np.array([list(range(1, nocc_up + 1)) + list(range(1, nocc_dn + 1))], np.int32)
+    a4, b, c = _jastrow(rng, nct, np.array([td["a1"] for td in type_defs]))
+    sysd = dict(name=name, nelec=nelec, nup=nup, iwctype=np.array(types_of_centre, np.int32),
+                cent=np.asarray(cent, float), znuc=znuc, coef=coef, iworbd=iworbd,
+                cdet=np.array([1.0]), norda=5, nordb=5, nordc=5, scalek=0.6, a4=a4, b=b, c=c,
+                **basis)
+    if nloc:
+        lpot = np.array([td["lpot"] for td in type_defs], np.int32)
+        nterm = np.zeros((nct, CW_MPS_L), np.int32)
+        power = np.zeros((nct, CW_MPS_L, CW_MGAUSS), np.int32)
+        expo = np.zeros((nct, CW_MPS_L, CW_MGAUSS))
+        ecoef = np.zeros((nct, CW_MPS_L, CW_MGAUSS))
+        for it, td in enumerate(type_defs):
+            nterm[it], power[it], expo[it], ecoef[it] = _bfd_like_ecp(rng, td["z"], td["lpot"])
+        xq, yq, zq, wq = gesqua(nquad)
+        sysd.update(nloc=nloc, lpot=lpot, necp_term=nterm, necp_power=power, ecp_exponent=expo,
+                    ecp_coef=ecoef, nquad=nquad, xq0=xq, yq0=yq, zq0=zq, wq=wq)
+    return System(**sysd)
+
+
+def make_synthetic(config: str, seed: int = 20261203) -> System:
+    """Seeded synthetic molecule of one benchmark configuration.
+
+    c0: 3 nuclei in a 4 bohr box (Z 6/1/1, ECP on the heavy atom, l_max=1,
+        6-point quadrature), 8 electrons (4/4), 60 Gaussians (s/p/d,
+        exponents log-uniform 0.1-20), 4 orbitals, order-5 Jastrow.
+    c1: 30 nuclei on a zig-zag chain alternating C-like (Z=4, ECP) and H-like
+        (Z=1) centres, 120 electrons (60/60), 540 Gaussians, 60 orbitals.
+    tiny: 2 nuclei, 6 electrons, small basis (fast parity cases).
+    """
+    rng = np.random.default_rng(seed)
+    if config == "c0":
+        while True:
+            cent = rng.uniform(-2.0, 2.0, size=(3, 3))
+            dmin = min(np.linalg.norm(cent[i] - cent[j]) for i in range(3) for j in range(i))
+            if dmin > 1.2:
+                break
+        heavy = dict(z=6.0, lpot=2, a1=0.0,
+                     basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 2)]), 6.0, 4))
+        hyd = dict(z=1.0, lpot=1, a1=-1.0,
+                   basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4)]), 1.0, 4))
+        return _assemble("c0", rng, cent, [0, 1, 1], [heavy, hyd], 8, 4, 4, 4, 4)
+    if config == "c1":
+        nat = 30
+        cent = np.zeros((nat, 3))
+        for i in range(nat):
+            cent[i] = (1.30 * i + rng.normal(0, 0.05), 0.75 * (i % 2) + rng.normal(0, 0.05),
+                       rng.normal(0, 0.05))
+        heavy = dict(z=4.0, lpot=2, a1=0.0,
+                     basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 1)]), 4.0, 4))
+        hyd = dict(z=1.0, lpot=1, a1=-1.0,
+                   basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 4)]), 1.0, 4))
+        types = [0 if i % 2 == 0 else 1 for i in range(nat)]
+        return _assemble("c1", rng, cent, types, [heavy, hyd], 120, 60, 60, 60, 60)
+    if config == "tiny":
+        cent = np.array([[0.0, 0.0, -0.7], [0.3, 0.2, 0.8]])
+        heavy = dict(z=4.0, lpot=2, a1=0.0,
+                     basis=_type_from_shells(_random_shells(rng, [(0, 3), (1, 2), (2, 1)]), 4.0, 4))
+        hyd = dict(z=1.0, lpot=1, a1=-1.0,
+                   basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 1)]), 1.0, 4))
+        return _assemble("tiny", rng, cent, [0, 1], [heavy, hyd], 5, 3, 4, 3, 2)
+    raise ValueError(f"unknown synthetic config {config!r}")

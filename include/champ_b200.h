@@ -1,0 +1,205 @@
+/*
+ * champ_b200.h — C ABI of the B200 walker engine for CHAMP's VMC/DMC inner loop.
+ *
+ * Plain C: pointers, sizes and status codes only.  Every array is laid out
+ * exactly like the corresponding CHAMP Fortran module array with the index
+ * order reversed (Fortran a(i,j,k) column-major == C a[k][j][i] row-major),
+ * so a Fortran caller passes its module arrays by reference through
+ * iso_c_binding without copying.  Electron, orbital, centre and type indices
+ * stored INSIDE arrays (iworbd, iwlbas, iwrwf) keep CHAMP's 1-based values;
+ * iwctype is 0-based.
+ *
+ * Each entry point names the CHAMP routine (file:line, paths relative to the
+ * CHAMP source tree) whose role it takes over.
+ */
+#ifndef CHAMP_B200_H
+#define CHAMP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Fixed dimensions of CHAMP's parameter modules. */
+#define CW_NCOEF    5    /* small-r polynomial, vmc_mod NCOEF (module/m_vmc.f90:96)      */
+#define CW_MPS_L    4    /* max pseudopotential channels + local (pseudo_mod MPS_L)       */
+#define CW_MGAUSS   16   /* max Gaussian terms per ECP channel                            */
+#define CW_MPS_QUAD 86   /* max angular quadrature points (gesqua, vmc/rotqua.f90:3)      */
+
+/* Status codes returned by every cw_* call. */
+enum {
+  CW_OK = 0,
+  CW_ERR_ARG = 1,         /* invalid argument / unsupported size                      */
+  CW_ERR_CUDA = 2,        /* CUDA runtime error (message in cw_last_error)            */
+  CW_ERR_OOM = 3,         /* device allocation failed                                 */
+  CW_ERR_SINGULAR = 4,    /* a Slater matrix was singular (matinv, vmc/matinv.f90:59) */
+  CW_ERR_UNSUPPORTED = 5, /* input outside what the engine implements                 */
+  CW_ERR_STATE = 6        /* call out of order (e.g. no walkers set)                  */
+};
+
+/* Arithmetic of the move/energy kernels. */
+enum {
+  CW_PREC_FP64 = 0,   /* plain FP64 everywhere (parity path)                           */
+  CW_PREC_MIXED = 1   /* FP32/3xBF16 LCAO + FP32 Jastrow sums, FP64 Slater algebra     */
+};
+
+/*
+ * Description of one molecular system, i.e. the contents of CHAMP's modules
+ * after parser() (vmc/parser.f90) has read the input: geometry (system),
+ * numerical basis (numbas, numbas1, numexp), LCAO (slater, dorb_m), Jastrow
+ * type 4 (jastrow, bparm), Gaussian ECP (pseudo, gauss_ecp, qua) and the
+ * Metropolis parameters (metropolis).  The engine copies everything it needs
+ * at cw_create; the caller's arrays are borrowed for that call only.
+ */
+typedef struct cw_system_desc {
+  /* --- system (module/m_system.f90) --- */
+  int32_t nelec, nup;          /* ndn = nelec - nup                                  */
+  int32_t ncent, nctype;
+  const int32_t *iwctype;      /* [ncent], 0-based atom type of each centre          */
+  const double *cent;          /* [ncent][3] bohr                                    */
+  const double *znuc;          /* [nctype] (valence) charges                         */
+  double pecent;               /* nuclear repulsion, pot_nn                          */
+
+  /* --- numerical radial basis (read_bas_num, vmc/read_bas_num.f90:11) --- */
+  int32_t mrwf;                /* leading dim: max radial functions per type         */
+  int32_t mrwf_pts;            /* leading dim: max grid points                       */
+  const int32_t *nrbas;        /* [nctype]                                           */
+  const int32_t *igrid;        /* [nctype] 1, 2 or 3                                 */
+  const int32_t *nr;           /* [nctype]                                           */
+  const double *arg;           /* [nctype]                                           */
+  const double *r0;            /* [nctype] after read_bas_num's igrid=3 rescaling    */
+  const double *rwf;           /* [nctype][mrwf][mrwf_pts]                           */
+  const double *d2rwf;         /* [nctype][mrwf][mrwf_pts] spline2 second derivs     */
+  const double *ce;            /* [nctype][mrwf][CW_NCOEF] small-r polynomial        */
+  const double *ae;            /* [nctype][mrwf][2] large-r exponential              */
+  const double *rmaxwf;        /* [nctype][mrwf] cutoff radius                       */
+  int32_t mbastyp;             /* leading dim of iwlbas/iwrwf                        */
+  const int32_t *nbastyp;      /* [nctype] AOs on a centre of this type              */
+  const int32_t *iwlbas;       /* [nctype][mbastyp] Slm index 1..35                  */
+  const int32_t *iwrwf;        /* [nctype][mbastyp] radial function 1..nrbas         */
+
+  /* --- orbitals and determinants (slater, dorb_m) --- */
+  int32_t nbasis, norb;
+  const double *coef;          /* [norb][nbasis] = Fortran coef(nbasis,norb)          */
+  int32_t ndet;                /* this engine version: ndet == 1                      */
+  const int32_t *iworbd;       /* [ndet][nelec] 1-based orbital of each electron slot */
+  const double *cdet;          /* [ndet]                                              */
+
+  /* --- Jastrow ijas=4 (jastrow, bparm; read_jastrow_file) --- */
+  int32_t norda, nordb, nordc;
+  int32_t isc;                 /* scaling type 2..5 (scale_dist.f90)                  */
+  int32_t nspin2b, nocuspb;
+  double scalek;
+  const double *a4;            /* [nctype][norda+1]                                   */
+  const double *b;             /* [nspin2b][nordb+1]                                  */
+  const double *c;             /* [nctype][nterms4(nordc)]                            */
+
+  /* --- Gaussian ECP (pseudo, gauss_ecp; readps_gauss) --- */
+  int32_t nloc;                /* 0 all-electron, 4 Gaussian ECP                      */
+  const int32_t *lpot;         /* [nctype] channels incl. local (local = index lpot)  */
+  const int32_t *necp_term;    /* [nctype][CW_MPS_L]   (l index 0..lpot-1 = CHAMP 1..lpot) */
+  const int32_t *necp_power;   /* [nctype][CW_MPS_L][CW_MGAUSS]                        */
+  const double *ecp_exponent;  /* [nctype][CW_MPS_L][CW_MGAUSS]                        */
+  const double *ecp_coef;      /* [nctype][CW_MPS_L][CW_MGAUSS]                        */
+  int32_t nquad;
+  const double *xq0, *yq0, *zq0, *wq;  /* [nquad] unrotated quadrature (gesqua)      */
+
+  /* --- metropolis (parser.f90:398-404) --- */
+  double deltar, deltat, fbias;
+} cw_system_desc;
+
+typedef struct cw_ctx cw_ctx;
+
+/* ------------------------------------------------------------------------ */
+/* Life cycle                                                               */
+/* ------------------------------------------------------------------------ */
+
+/* Upload one system and set up the engine on CUDA device `device`.
+ * Replaces the module set-up CHAMP does after parser() (vmc/parser.f90:~150-700,
+ * set_scale_dist vmc/scale_dist.f90:3). */
+int cw_create(cw_ctx **ctx, const cw_system_desc *desc, int device, int precision);
+void cw_destroy(cw_ctx *ctx);
+const char *cw_last_error(const cw_ctx *ctx);
+int cw_sync(cw_ctx *ctx);
+
+/* Set the walker population: x [nwalk][nelec][3] (= CHAMP xold(3,nelec) per
+ * walker) and xoshiro256** states rng [nwalk][4] (= the 8 int32 of setrn,
+ * vmc/random.f90:27, reinterpreted as 4 uint64).  Replaces mc_configs_start
+ * (vmc/mc_configs.f90:33) plus the per-rank jumprn (vmc/parser.f90:654-661).
+ * Also runs the initial hpsi of zerest (vmc/acuest.f90:179) on every walker
+ * with the unrotated quadrature, and zeroes the estimators. */
+int cw_set_walkers(cw_ctx *ctx, int nwalk, const double *x, const uint64_t *rng);
+int cw_get_walkers(cw_ctx *ctx, double *x, uint64_t *rng);
+
+/* ------------------------------------------------------------------------ */
+/* Batched drop-ins for CHAMP's per-walker routines                          */
+/* ------------------------------------------------------------------------ */
+
+/* `nstep` VMC steps for every walker: per step rotqua (vmc/rotqua.f90:357,
+ * only if nloc>0) then metrop6 (vmc/metrop_mov1_slat.f90:3: one accelerated
+ * Metropolis move per electron, hpsi at the end, weighted sums).  Same random
+ * number consumption as CHAMP rank w with the walker's own stream.
+ * Accumulates per-walker esum/wsum/pesum/tpbsum and acceptance. */
+int cw_vmc_steps(cw_ctx *ctx, int nstep);
+
+/* Close a block for every walker: acuest (vmc/acuest.f90:61) +
+ * acuest_reduce (vmc/acuest_reduce.f90:3) with walkers in the role of ranks.
+ * Writes, if non-NULL, block_energy = Σ esum / Σ wsum of the block. */
+int cw_end_block(cw_ctx *ctx, double *block_energy);
+
+/* Final estimates, finwrt (vmc/finwrt.f90:75-187): out[0]=E, out[1]=err,
+ * out[2]=sigma, out[3]=Tcor, out[4]=acceptance, out[5]=PE, out[6]=KE,
+ * out[7]=blocks so far (iblk). */
+int cw_results(cw_ctx *ctx, double *out);
+
+/* Local energy of every walker at its current configuration, hpsi
+ * (vmc/hpsi.f90:3) with the quadrature grid (xq,yq,zq)[nquad] given (NULL:
+ * the unrotated one).  Outputs per walker (any may be NULL): energy, psid,
+ * psij, ekin. */
+int cw_hpsi(cw_ctx *ctx, const double *xq, const double *yq, const double *zq,
+            double *energy, double *psid, double *psij, double *ekin);
+
+/* Orbitals of all electrons of every walker, orbitals (vmc/orbitals.f90:18):
+ * orb [nwalk][norb][nelec] (= orb(nelec,norb)), dorb [nwalk][3][nelec][norb]
+ * (= dorb(norb,nelec,3)), ddorb [nwalk][nelec][norb] (= ddorb(norb,nelec)). */
+int cw_orbitals(cw_ctx *ctx, double *orb, double *dorb, double *ddorb);
+
+/* Jastrow factor of every walker, jastrow_factor (vmc/jastrow.f90:3):
+ * psij [nwalk], v [nwalk][nelec][3], d2j [nwalk]. */
+int cw_jastrow(cw_ctx *ctx, double *psij, double *v, double *d2j);
+
+/* Slater inverses and determinants after the full recompute of determinant
+ * (vmc/determinant.f90:9): slmi [nwalk][2][nmax*nmax] with nmax=max(nup,ndn)
+ * (spin iab: slmi(j+nel*(i-1)) of CHAMP), det [nwalk][2]. */
+int cw_slater(cw_ctx *ctx, double *slmi, double *det);
+
+/* Per-walker sums since the last cw_end_block: out [nwalk][5] =
+ * (wsum, esum, pesum, tpbsum, accepted moves). */
+int cw_get_sums(cw_ctx *ctx, double *out);
+
+/* Per-walker current values: eold, psido, psijo [nwalk] (any may be NULL). */
+int cw_get_state(cw_ctx *ctx, double *eold, double *psido, double *psijo);
+
+/* Device milliseconds of the last cw_vmc_steps call (CUDA events on the
+ * engine stream). */
+double cw_last_ms(const cw_ctx *ctx);
+
+/* ------------------------------------------------------------------------ */
+/* Host-only helpers (no GPU needed)                                        */
+/* ------------------------------------------------------------------------ */
+
+/* Random streams of nwalk walkers: setrn(irn) (vmc/random.f90:27) followed
+ * by w calls of jump() (vmc/xoroshiro256starstar.c:51) for walker w, as
+ * CHAMP does for MPI rank w (vmc/parser.f90:651-661).  out [nwalk][4]. */
+int cw_rng_states(const int32_t *irn8, int nwalk, uint64_t *out);
+
+/* Initial electron positions of every walker: mc_configs_start's nsite rule
+ * (vmc/mc_configs.f90:75-96) + sites (vmc/sites.f90:3), drawing from each
+ * walker's stream (rng [nwalk][4] advanced in place).  x [nwalk][nelec][3]. */
+int cw_sites(const cw_system_desc *desc, int nwalk, uint64_t *rng, double *x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHAMP_B200_H */

@@ -1,0 +1,2067 @@
+// oracle.cpp — CPU FP64 restatement of CHAMP's VMC hot path.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle.h).  Arrays keep CHAMP's Fortran
+// column-major layout with 0-based indices; the index helpers below spell out
+// the Fortran subscript each one stands for.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using std::vector;
+
+// ---------------------------------------------------------------------------
+// xoshiro256** — restates vmc/xoroshiro256starstar.c:22-65 (next, jump) and
+// :125 (next_uniform_double).
+// ---------------------------------------------------------------------------
+struct Rng {
+  uint64_t s[4];
+  static inline uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+  uint64_t next() {
+    const uint64_t result = rotl(s[1] * 5, 7) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl(s[3], 45);
+    return result;
+  }
+  double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }
+  void jump() {
+    static const uint64_t J[] = {0x180ec6d33cfd0abaULL, 0xd5a61266f0c9392cULL,
+                                 0xa9582618e03fc9aaULL, 0x39abdc4529b1661cULL};
+    uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int i = 0; i < 4; i++)
+      for (int b = 0; b < 64; b++) {
+        if (J[i] & (1ULL << b)) {
+          s0 ^= s[0]; s1 ^= s[1]; s2 ^= s[2]; s3 ^= s[3];
+        }
+        next();
+      }
+    s[0] = s0; s[1] = s1; s[2] = s2; s[3] = s3;
+  }
+};
+
+const double PI = 4.0 * std::atan(1.0);  // module constants, m_constant.f90:52
+
+// ---------------------------------------------------------------------------
+// System: copies of the module arrays plus the derived Jastrow asymptotes.
+// ---------------------------------------------------------------------------
+struct Sys {
+  int N, nup, ndn, M, nctype;
+  vector<int> iwctype;
+  vector<double> cent, znuc;
+  double pecent;
+  int mrwf, mpts;
+  vector<int> nrbas, igrid, nr;
+  vector<double> arg, r0, rwf, d2rwf, ce, ae, rmaxwf;
+  int mbastyp;
+  vector<int> nbastyp, iwlbas, iwrwf;
+  int K, O, ndet;
+  vector<double> coef, cdet;
+  vector<int> iworbd;  // iworbd(j) for kref=1, 1-based orbital
+  int norda, nordb, nordc, isc, nspin2b, nocuspb, nterms;
+  double scalek;
+  vector<double> a4, b, c;
+  double asymp_r;
+  vector<double> asymp_jasa;  // [nctype]
+  double asymp_jasb[2];
+  int nloc;
+  vector<int> lpot, necp_term, necp_power;
+  vector<double> ecp_exponent, ecp_coef;
+  int nquad;
+  vector<double> xq0, yq0, zq0, wq;
+  double deltar, deltat, fbias;
+  // index helpers
+  double RWF(int ir, int irb, int it) const { return rwf[ir + mpts * (irb + mrwf * it)]; }
+  double D2RWF(int ir, int irb, int it) const { return d2rwf[ir + mpts * (irb + mrwf * it)]; }
+  double CE(int ii, int irb, int it) const { return ce[ii + CW_NCOEF * (irb + mrwf * it)]; }
+  double AE(int ii, int irb, int it) const { return ae[ii + 2 * (irb + mrwf * it)]; }
+  double COEF(int m, int iorb) const { return coef[m + K * iorb]; }
+  double A4(int ip, int it) const { return a4[ip + (norda + 1) * it]; }   // a4(ip+1,it)
+  double B(int ip, int isb) const { return b[ip + (nordb + 1) * isb]; }    // b(ip+1,isb)
+  double C(int ll, int it) const { return c[ll + nterms * it]; }           // c(ll+1,it)
+};
+
+int nterms4(int nord) {
+  // nterms4 (vmc/jastrow4.f90): same enumeration as the e-e-n loops.
+  int i = 0;
+  for (int n = 2; n <= nord; n++)
+    for (int k = n - 1; k >= 0; k--) {
+      int l_hi = (k == 0) ? n - k - 2 : n - k;
+      for (int l = l_hi; l >= 0; l--) {
+        int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) i++;
+      }
+    }
+  return i;
+}
+
+// set_scale_dist (vmc/scale_dist.f90:3-55)
+void set_scale_dist(Sys &s) {
+  s.asymp_r = 1.0 / s.scalek;
+  s.asymp_jasa.assign(s.nctype, 0.0);
+  for (int it = 0; it < s.nctype; it++) {
+    double v = s.A4(0, it) * s.asymp_r / (1 + s.A4(1, it) * s.asymp_r);
+    for (int iord = 2; iord <= s.norda; iord++) v += s.A4(iord, it) * std::pow(s.asymp_r, iord);
+    s.asymp_jasa[it] = v;
+  }
+  for (int i = 0; i < 2; i++) {
+    double sspinn;
+    int isp;
+    if (i == 0) {
+      sspinn = 1;
+      isp = 0;
+    } else {
+      sspinn = (s.nspin2b == 1 && s.nocuspb == 0) ? 0.5 : 1.0;
+      isp = s.nspin2b - 1;
+    }
+    double v = sspinn * s.B(0, isp) * s.asymp_r / (1 + s.B(1, isp) * s.asymp_r);
+    for (int iord = 2; iord <= s.nordb; iord++) v += s.B(iord, isp) * std::pow(s.asymp_r, iord);
+    s.asymp_jasb[i] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// scale_dist family (vmc/scale_dist.f90:57-353), isc = 2..5
+// ---------------------------------------------------------------------------
+inline void scale_dist0(const Sys &s, double r, double &rr) {
+  double k = s.scalek;
+  if (k == 0) { rr = r; return; }
+  if (s.isc == 2) rr = (1 - std::exp(-k * r)) / k;
+  else if (s.isc == 3) {
+    double rsc = k * r, rsc2 = rsc * rsc, rsc3 = rsc * rsc2;
+    rr = (1 - std::exp(-rsc - 0.5 * rsc2 - (1.0 / 3.0) * rsc3)) / k;
+  } else if (s.isc == 4) rr = r * (1 / (1 + k * r));
+  else rr = r * (1 / std::pow(1 + std::pow(k * r, 3), 1.0 / 3.0));
+}
+inline void scale_dist1(const Sys &s, double r, double &rr, double &dd1) {
+  double k = s.scalek;
+  if (k == 0) { rr = r; dd1 = 1; return; }
+  if (s.isc == 2) {
+    rr = (1 - std::exp(-k * r)) / k;
+    dd1 = 1 - k * rr;
+  } else if (s.isc == 3) {
+    double rsc = k * r, rsc2 = rsc * rsc, rsc3 = rsc * rsc2;
+    double e = std::exp(-rsc - 0.5 * rsc2 - (1.0 / 3.0) * rsc3);
+    rr = (1 - e) / k;
+    dd1 = (1 + rsc + rsc2) * e;
+  } else if (s.isc == 4) {
+    double deni = 1 / (1 + k * r);
+    rr = r * deni;
+    dd1 = deni * deni;
+  } else {
+    double deni = 1 / std::pow(1 + std::pow(k * r, 3), 1.0 / 3.0);
+    rr = r * deni;
+    dd1 = std::pow(deni, 4);
+  }
+}
+inline void scale_dist2(const Sys &s, double r, double &rr, double &dd1, double &dd2) {
+  double k = s.scalek;
+  if (k == 0) { rr = r; dd1 = 1; dd2 = 0; return; }
+  if (s.isc == 2) {
+    rr = (1 - std::exp(-k * r)) / k;
+    dd1 = 1 - k * rr;
+    dd2 = -k * dd1;
+  } else if (s.isc == 3) {
+    double rsc = k * r, rsc2 = rsc * rsc, rsc3 = rsc * rsc2;
+    double e = std::exp(-rsc - 0.5 * rsc2 - (1.0 / 3.0) * rsc3);
+    rr = (1 - e) / k;
+    dd1 = (1 + rsc + rsc2) * e;
+    dd2 = -k * rsc2 * (3 + 2 * rsc + rsc2) * e;
+  } else if (s.isc == 4) {
+    double deni = 1 / (1 + k * r);
+    rr = r * deni;
+    dd1 = deni * deni;
+    dd2 = -2 * k * deni * dd1;
+  } else {
+    double deni = 1 / std::pow(1 + std::pow(k * r, 3), 1.0 / 3.0);
+    rr = r * deni;
+    dd1 = std::pow(deni, 4);
+    dd2 = -4 * (k * r) * (k * r) * k * dd1 * dd1 / deni;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Slm (vmc/slm.f90:7): Cartesian monomials x^a y^b z^c times a constant.
+// ---------------------------------------------------------------------------
+const double CS = 0.28209479177387814, CP = 0.48860251190291992, CD1 = 0.630783130505040,
+             CD2 = 1.092548430592079, CF = 0.74635266518023078, CF2 = 1.66889529453113635,
+             CF3 = 2.89061144264055405, CG = 0.8462843753216345, CG2 = 2.2390579955406924,
+             CG3 = 2.890611442640554, CG4 = 5.006685883593409;
+struct SlmDef { int a, b, c; double k; };
+const SlmDef SLM[35] = {
+    {0, 0, 0, CS},  {1, 0, 0, CP},  {0, 1, 0, CP},  {0, 0, 1, CP},                     // 1-4
+    {2, 0, 0, CD1}, {1, 1, 0, CD2}, {1, 0, 1, CD2}, {0, 2, 0, CD1}, {0, 1, 1, CD2},
+    {0, 0, 2, CD1},                                                                    // 5-10
+    {3, 0, 0, CF},  {2, 1, 0, CF2}, {2, 0, 1, CF2}, {1, 2, 0, CF2}, {1, 1, 1, CF3},
+    {1, 0, 2, CF2}, {0, 3, 0, CF},  {0, 2, 1, CF2}, {0, 1, 2, CF2}, {0, 0, 3, CF},    // 11-20
+    {4, 0, 0, CG},  {3, 1, 0, CG2}, {3, 0, 1, CG2}, {2, 2, 0, CG3}, {2, 1, 1, CG4},
+    {2, 0, 2, CG3}, {1, 3, 0, CG2}, {1, 2, 1, CG4}, {1, 1, 2, CG4}, {1, 0, 3, CG2},
+    {0, 4, 0, CG},  {0, 3, 1, CG2}, {0, 2, 2, CG3}, {0, 1, 3, CG2}, {0, 0, 4, CG}};  // 21-35
+
+inline double ipow(double x, int n) {
+  double r = 1;
+  for (int i = 0; i < n; i++) r *= x;
+  return r;
+}
+// l is CHAMP's 1-based Slm index
+void slm(int l, const double *rv, double &y, double *dy, double &lap) {
+  const SlmDef &d = SLM[l - 1];
+  double x = rv[0], yy = rv[1], z = rv[2];
+  double px = ipow(x, d.a), py = ipow(yy, d.b), pz = ipow(z, d.c);
+  y = d.k * px * py * pz;
+  dy[0] = d.a ? d.k * d.a * ipow(x, d.a - 1) * py * pz : 0.0;
+  dy[1] = d.b ? d.k * d.b * px * ipow(yy, d.b - 1) * pz : 0.0;
+  dy[2] = d.c ? d.k * d.c * px * py * ipow(z, d.c - 1) : 0.0;
+  lap = 0;
+  if (d.a >= 2) lap += d.k * d.a * (d.a - 1) * ipow(x, d.a - 2) * py * pz;
+  if (d.b >= 2) lap += d.k * d.b * (d.b - 1) * px * ipow(yy, d.b - 2) * pz;
+  if (d.c >= 2) lap += d.k * d.c * (d.c - 1) * px * py * ipow(z, d.c - 2);
+}
+
+// ---------------------------------------------------------------------------
+// splfit (vmc/splfit.f90:3-94): radial function irb of type it at r.
+// ---------------------------------------------------------------------------
+void splfit(const Sys &s, double r, int irb, int it, double *wfv, int ider) {
+  int ig = s.igrid[it];
+  double arg = s.arg[it], r0 = s.r0[it];
+  double xr, ref0 = 0, ref1 = 0, delh = 0;
+  int jx;
+  if (ig == 1) {
+    xr = (r - r0) / arg + 1;
+    jx = (int)xr;
+    ref0 = r0 + arg * (jx - 1);
+    ref1 = ref0 + arg;
+    delh = arg;
+  } else if (ig == 2) {
+    double dlrad0 = std::log(r0), dlogag = std::log(arg);
+    xr = (std::log(r) - dlrad0) / dlogag + 1;
+    jx = (int)xr;
+    ref0 = r0 * std::pow(arg, jx - 1);
+    ref1 = ref0 * arg;
+    delh = ref1 - ref0;
+  } else {
+    double dlogag = std::log(arg);
+    xr = (std::log((r + r0) / r0)) / dlogag + 1.0;
+    jx = (int)xr;
+    ref0 = r0 * std::pow(arg, jx - 1) - r0;
+    ref1 = (ref0 + r0) * arg - r0;
+    delh = ref1 - ref0;
+  }
+  if (jx < 1) {
+    wfv[0] = s.CE(0, irb, it);
+    for (int ii = 2; ii <= CW_NCOEF; ii++) wfv[0] += s.CE(ii - 1, irb, it) * ipow(r, ii - 1);
+    if (ider >= 1) {
+      wfv[1] = wfv[2] = wfv[3] = 0;
+      for (int ii = 2; ii <= CW_NCOEF; ii++) {
+        double cc = s.CE(ii - 1, irb, it);
+        wfv[1] += (ii - 1) * cc * ipow(r, ii - 2);
+        if (ii >= 3) wfv[2] += (ii - 1) * (ii - 2) * cc * ipow(r, ii - 3);
+        if (ii >= 4) wfv[3] += (ii - 1) * (ii - 2) * (ii - 3) * cc * ipow(r, ii - 4);
+      }
+    }
+  } else if (jx >= s.nr[it]) {
+    wfv[0] = s.AE(0, irb, it) * std::exp(-s.AE(1, irb, it) * r);
+    if (ider >= 1) {
+      wfv[1] = -s.AE(1, irb, it) * wfv[0];
+      wfv[2] = -s.AE(1, irb, it) * wfv[1];
+      wfv[3] = -s.AE(1, irb, it) * wfv[2];
+    }
+  } else {
+    // Fortran jx is 1-based: rwf(jx) -> index jx-1
+    double y0 = s.RWF(jx - 1, irb, it), y1 = s.RWF(jx, irb, it);
+    double d0 = s.D2RWF(jx - 1, irb, it), d1 = s.D2RWF(jx, irb, it);
+    const double sixth = 1.0 / 6.0;
+    double delhi = 1.0 / delh;
+    double bb = (r - ref0) * delhi;
+    double aa = (ref1 - r) * delhi;
+    double cc = aa * (aa * aa - 1.0) * delh * delh * sixth;
+    double dd = bb * (bb * bb - 1.0) * delh * delh * sixth;
+    wfv[0] = aa * y0 + bb * y1 + cc * d0 + dd * d1;
+    if (ider >= 1) {
+      wfv[1] = (y1 - y0) * delhi + (-(3.0 * aa * aa - 1.0) * d0 + (3.0 * bb * bb - 1.0) * d1) * delh * sixth;
+      wfv[2] = aa * d0 + bb * d1;
+      wfv[3] = (-d0 + d1) * delhi;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// basis_fns (vmc/basis_fns.f90:8-214) + phi_combine (:217-296) for the
+// electrons/points k in [k1,k2): fills phin(m,k), dphin(m,k,3), d2phin(m,k)
+// with leading dimension ncoord.
+// ---------------------------------------------------------------------------
+void basis_fns(const Sys &s, int k1, int k2, int ncoord, const double *rvec_en, const double *r_en,
+               int ider, double *phin, double *dphin, double *d2phin) {
+  const int K = s.K;
+  int lilm = 0;
+  double wfv[64][4];
+  for (int ic = 0; ic < s.M; ic++) {
+    int it = s.iwctype[ic];
+    int nrb = s.nrbas[it], nbt = s.nbastyp[it];
+    int num_slms = 0;
+    for (int ib = 0; ib < nbt; ib++) num_slms = std::max(num_slms, s.iwlbas[ib + s.mbastyp * it]);
+    vector<double> yv(num_slms), dyv(3 * num_slms), lapv(num_slms);
+    for (int k = k1; k < k2; k++) {
+      double xc[3] = {rvec_en[0 + 3 * (k + ncoord * ic)], rvec_en[1 + 3 * (k + ncoord * ic)],
+                      rvec_en[2 + 3 * (k + ncoord * ic)]};
+      double r = r_en[k + ncoord * ic];
+      double r2 = r * r, ri = 1.0 / r, ri2 = ri * ri;
+      (void)ri2;
+      for (int irb = 0; irb < nrb; irb++) {
+        if (r <= s.rmaxwf[irb + s.mrwf * it])
+          splfit(s, r, irb, it, wfv[irb], ider);
+        else
+          wfv[irb][0] = wfv[irb][1] = wfv[irb][2] = wfv[irb][3] = 0.0;
+      }
+      (void)r2;
+      for (int i = 0; i < num_slms; i++) slm(i + 1, xc, yv[i], &dyv[3 * i], lapv[i]);
+      for (int ib = 0; ib < nbt; ib++) {
+        int l = s.iwlbas[ib + s.mbastyp * it];
+        int irb = s.iwrwf[ib + s.mbastyp * it] - 1;
+        const double *w = wfv[irb];
+        double y = yv[l - 1];
+        const double *dy = &dyv[3 * (l - 1)];
+        double ddy_lap = lapv[l - 1];
+        int m = lilm + ib;
+        phin[m + K * k] = y * w[0];
+        if (ider == 1) {
+          double xcri[3] = {xc[0] * ri, xc[1] * ri, xc[2] * ri};
+          for (int jj = 0; jj < 3; jj++) dphin[m + K * (k + ncoord * jj)] = y * xcri[jj] * w[1] + dy[jj] * w[0];
+        } else if (ider >= 2) {
+          double xcri[3] = {xc[0] * ri, xc[1] * ri, xc[2] * ri};
+          double d2phi = y * w[2] + y * 2.0 * ri * w[1] + ddy_lap * w[0];
+          double dum = 0;
+          for (int jj = 0; jj < 3; jj++) {
+            dphin[m + K * (k + ncoord * jj)] = y * xcri[jj] * w[1] + dy[jj] * w[0];
+            dum += dy[jj] * xcri[jj];
+          }
+          d2phi += 2.0 * dum * w[1];
+          d2phin[m + K * k] = d2phi;
+        }
+      }
+    }
+    lilm += nbt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Walker state: the CHAMP module variables one rank holds.
+// ---------------------------------------------------------------------------
+struct Walker {
+  const Sys *s;
+  int N, M, K, O;
+  // config (module config)
+  vector<double> xold, xnew, vold, vnew;
+  double psido, psijo, psi2o, eold, ekino;
+  vector<double> rmino, rminn, rminno, rminon, rvmino, rvminn, rvminno, rvminon, delttn;
+  vector<int> nearesto, nearestn;
+  // distances (distance_mod, distances_sav)
+  vector<double> r_en, rvec_en, r_ee, rvec_ee;
+  vector<double> r_en_sav, rvec_en_sav, r_ee_sav, rvec_ee_sav;
+  // jastrow_update
+  vector<double> fso, fijo, d2ijo, fjo, fsn, fijn, d2ijn, fjn;
+  double fsumo, d2o, fsumn, d2n;
+  vector<double> vj, vjn;  // velocity_jastrow (== fjo/fjn)
+  // phifun
+  vector<double> phin, dphin, d2phin;
+  // orbval / multislatern
+  vector<double> orb, dorb, ddorb, orbn, dorbn, ddorbn;
+  // slater
+  vector<double> slmi[2], slmin, fp[2], fpp[2], ddx, d2dx2, dorb_tmp;
+  double detiab[2], detn;
+  // quadrature (qua), rotated per step
+  vector<double> xq, yq, zq;
+  // ecp
+  vector<double> vps;  // vps(i,ic,l) [i + N*(ic + M*l)]
+  // estimators (estsum, forcewt, est*)
+  double esum, wsum, pesum, tpbsum, acc, esum1;
+  double ecum, ecm2, wcum, pecum, tpbcum, pecm2, tpbcm2, ecum1, ecm21, ecum1s, ecm21s;
+  Rng rng;
+  bool singular = false;
+
+  explicit Walker(const Sys *sys) : s(sys) {
+    N = s->N; M = s->M; K = s->K; O = s->O;
+    xold.assign(3 * N, 0); xnew = vold = vnew = xold;
+    rmino.assign(N, 0); rminn = rminno = rminon = delttn = rmino;
+    rvmino.assign(3 * N, 0); rvminn = rvminno = rvminon = rvmino;
+    nearesto.assign(N, 0); nearestn = nearesto;
+    r_en.assign(N * M, 0); rvec_en.assign(3 * N * M, 0);
+    int np = N * (N - 1) / 2;
+    r_ee.assign(std::max(np, 1), 0); rvec_ee.assign(3 * std::max(np, 1), 0);
+    r_en_sav.assign(M, 0); rvec_en_sav.assign(3 * M, 0); r_ee_sav.assign(N, 0); rvec_ee_sav.assign(3 * N, 0);
+    fso.assign(N * N, 0); fijo.assign(3 * N * N, 0); d2ijo.assign(N * N, 0); fjo.assign(3 * N, 0);
+    fsn = fso; fijn = fijo; d2ijn = d2ijo; fjn = fjo;
+    fsumo = d2o = fsumn = d2n = 0;
+    vj.assign(3 * N, 0); vjn = vj;
+    int ncoord = std::max(N, 2 * N * std::max(s->nquad, 1));
+    phin.assign((size_t)K * ncoord, 0); dphin.assign((size_t)K * ncoord * 3, 0); d2phin.assign((size_t)K * ncoord, 0);
+    orb.assign(N * O, 0); dorb.assign(O * N * 3, 0); ddorb.assign(O * N, 0);
+    orbn.assign(O, 0); dorbn.assign(O * 3, 0); ddorbn.assign(O, 0);
+    int n1 = s->nup, n2 = s->ndn;
+    slmi[0].assign(std::max(n1 * n1, 1), 0); slmi[1].assign(std::max(n2 * n2, 1), 0);
+    slmin.assign(std::max(std::max(n1 * n1, n2 * n2), 1), 0);
+    fp[0].assign(3 * std::max(n1 * n1, 1), 0); fp[1].assign(3 * std::max(n2 * n2, 1), 0);
+    fpp[0].assign(std::max(n1 * n1, 1), 0); fpp[1].assign(std::max(n2 * n2, 1), 0);
+    ddx.assign(3 * N, 0); d2dx2.assign(N, 0); dorb_tmp.assign(3 * O, 0);
+    detiab[0] = detiab[1] = detn = 0;
+    xq = s->xq0; yq = s->yq0; zq = s->zq0;
+    vps.assign((size_t)N * M * CW_MPS_L, 0);
+    zero_estimators();
+  }
+  void zero_estimators() {
+    esum = wsum = pesum = tpbsum = acc = esum1 = 0;
+    ecum = ecm2 = wcum = pecum = tpbcum = pecm2 = tpbcm2 = ecum1 = ecm21 = ecum1s = ecm21s = 0;
+  }
+
+  // ---- distances (vmc/distances.f90:3-109) ----
+  void distances(int iel, const double *x) {  // iel: -1 == all (CHAMP iel=0)
+    int i1, i2;
+    if (iel < 0) {
+      i1 = 0; i2 = N - 1;
+    } else {
+      i1 = i2 = iel;
+      for (int ic = 0; ic < M; ic++) {
+        r_en_sav[ic] = r_en[iel + N * ic];
+        for (int m = 0; m < 3; m++) rvec_en_sav[m + 3 * ic] = rvec_en[m + 3 * (iel + N * ic)];
+      }
+      for (int jj = 0; jj < iel; jj++) {
+        int ij = iel * (iel - 1) / 2 + jj;
+        r_ee_sav[jj] = r_ee[ij];
+        for (int m = 0; m < 3; m++) rvec_ee_sav[m + 3 * jj] = rvec_ee[m + 3 * ij];
+      }
+      for (int jj = iel + 1; jj < N; jj++) {
+        int ij = jj * (jj - 1) / 2 + iel;
+        r_ee_sav[jj] = r_ee[ij];
+        for (int m = 0; m < 3; m++) rvec_ee_sav[m + 3 * jj] = rvec_ee[m + 3 * ij];
+      }
+    }
+    for (int i = i1; i <= i2; i++)
+      for (int ic = 0; ic < M; ic++) {
+        double r = 0;
+        for (int m = 0; m < 3; m++) {
+          double d = x[m + 3 * i] - s->cent[m + 3 * ic];
+          rvec_en[m + 3 * (i + N * ic)] = d;
+        }
+        for (int m = 0; m < 3; m++) r += rvec_en[m + 3 * (i + N * ic)] * rvec_en[m + 3 * (i + N * ic)];
+        r_en[i + N * ic] = std::sqrt(r);
+      }
+    auto pair = [&](int i, int j, int ij) {  // rvec_ee(ij) = x(i) - x(j)
+      double r = 0;
+      for (int m = 0; m < 3; m++) rvec_ee[m + 3 * ij] = x[m + 3 * i] - x[m + 3 * j];
+      for (int m = 0; m < 3; m++) r += rvec_ee[m + 3 * ij] * rvec_ee[m + 3 * ij];
+      r_ee[ij] = std::sqrt(r);
+    };
+    if (iel < 0) {
+      for (int i = 1; i < N; i++)
+        for (int j = 0; j < i; j++) pair(i, j, i * (i - 1) / 2 + j);
+    } else {
+      for (int i = 0; i < iel; i++) pair(iel, i, iel * (iel - 1) / 2 + i);
+      for (int i = iel + 1; i < N; i++) pair(i, iel, i * (i - 1) / 2 + iel);
+    }
+  }
+  // distancese_restore (vmc/distances.f90:164)
+  void distancese_restore(int iel) {
+    for (int ic = 0; ic < M; ic++) {
+      r_en[iel + N * ic] = r_en_sav[ic];
+      for (int m = 0; m < 3; m++) rvec_en[m + 3 * (iel + N * ic)] = rvec_en_sav[m + 3 * ic];
+    }
+    for (int jj = 0; jj < N; jj++) {
+      if (jj == iel) continue;
+      int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
+      int ij = i * (i - 1) / 2 + j;
+      r_ee[ij] = r_ee_sav[jj];
+      for (int m = 0; m < 3; m++) rvec_ee[m + 3 * ij] = rvec_ee_sav[m + 3 * jj];
+    }
+  }
+
+  // ---- e-e-n polynomial shared by jastrow_factor4 / jastrow4e ----
+  // Accumulates fc, fu, fuu, fi, fii, fj, fjj, fui, fuj (vmc/jastrow4.f90 n/k/l loop).
+  struct Een { double fc, fu, fuu, fi, fii, fj, fjj, fui, fuj; };
+  Een een_terms(const double *uu, const double *ss, const double *tt, const double *rri,
+                const double *rrj, int it, bool second) const {
+    // arrays are offset so index -3 .. nordj is valid: pass pointers to index 0
+    Een e{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int ll = 0;
+    for (int n = 2; n <= s->nordc; n++)
+      for (int k = n - 1; k >= 0; k--) {
+        int l_hi = (k == 0) ? n - k - 2 : n - k;
+        for (int l = l_hi; l >= 0; l--) {
+          int m = (n - k - l) / 2;
+          if (2 * m == n - k - l) {
+            double cc = s->C(ll, it);
+            ll++;
+            e.fc += cc * uu[k] * ss[l] * tt[m];
+            e.fu += cc * k * uu[k - 1] * ss[l] * tt[m];
+            e.fi += cc * uu[k] * ((l + m) * rri[l + m - 1] * rrj[m] + m * rri[m - 1] * rrj[l + m]);
+            e.fj += cc * uu[k] * ((l + m) * rrj[l + m - 1] * rri[m] + m * rrj[m - 1] * rri[l + m]);
+            if (second) {
+              e.fuu += cc * k * (k - 1) * uu[k - 2] * ss[l] * tt[m];
+              e.fii += cc * uu[k] * ((l + m) * (l + m - 1) * rri[l + m - 2] * rrj[m] + m * (m - 1) * rri[m - 2] * rrj[l + m]);
+              e.fjj += cc * uu[k] * ((l + m) * (l + m - 1) * rrj[l + m - 2] * rri[m] + m * (m - 1) * rrj[m - 2] * rri[l + m]);
+              e.fui += cc * k * uu[k - 1] * ((l + m) * rri[l + m - 1] * rrj[m] + m * rri[m - 1] * rrj[l + m]);
+              e.fuj += cc * k * uu[k - 1] * ((l + m) * rrj[l + m - 1] * rri[m] + m * rrj[m - 1] * rri[l + m]);
+            }
+          }
+        }
+      }
+    return e;
+  }
+
+  static inline int FI(int i, int j, int N) { return i + N * j; }
+  static inline int FIJ(int k, int i, int j, int N) { return k + 3 * (i + N * j); }
+
+  // ---- jastrow_factor4 (vmc/jastrow4.f90:3): full J with Laplacian ----
+  void jastrow_factor4() {
+    const int nordj = std::max(std::max(s->norda, s->nordb), s->nordc);
+    vector<double> UU(nordj + 4, 0), SS(nordj + 4, 0), TT(nordj + 4, 0), RI(nordj + 4, 0), RJ(nordj + 4, 0);
+    double *uu = &UU[3], *ss = &SS[3], *tt = &TT[3], *rri = &RI[3], *rrj = &RJ[3];
+    fsumo = 0; d2o = 0;
+    std::fill(fjo.begin(), fjo.end(), 0.0);
+    uu[0] = 1; ss[0] = 2; tt[0] = 1; rri[0] = 1; rrj[0] = 1;
+    if (N >= 2) {
+      int ij = 0;
+      for (int i = 1; i < N; i++)
+        for (int j = 0; j < i; j++, ij++) {
+          fso[FI(i, j, N)] = 0;
+          d2ijo[FI(i, j, N)] = 0;
+          for (int k = 0; k < 3; k++) fijo[FIJ(k, i, j, N)] = fijo[FIJ(k, j, i, N)] = 0;
+          double sspinn = 1;
+          int isb = 0, ipar = 0;
+          if (i < s->nup || j >= s->nup) {
+            if (s->nspin2b == 2) isb = 1;
+            else if (s->nocuspb == 0) sspinn = 0.5;
+            ipar = 1;
+          }
+          double rij = r_ee[ij], dd1, dd2;
+          scale_dist2(*s, rij, uu[1], dd1, dd2);
+          if (uu[1] != s->asymp_r) {
+            double top = sspinn * s->B(0, isb) * uu[1], topu = sspinn * s->B(0, isb), topuu = 0;
+            double bot = 1 + s->B(1, isb) * uu[1], botu = s->B(1, isb), botuu = 0, bot2 = bot * bot;
+            double fee = top / bot - s->asymp_jasb[ipar];
+            double feeu = topu / bot - botu * top / bot2;
+            double feeuu = topuu - (botuu * top + 2 * botu * topu) / bot + 2 * botu * botu * top / bot2;
+            feeuu = feeuu / bot;
+            for (int iord = 2; iord <= s->nordb; iord++) {
+              uu[iord] = uu[1] * uu[iord - 1];
+              fee += s->B(iord, isb) * uu[iord];
+              feeu += s->B(iord, isb) * iord * uu[iord - 1];
+              feeuu += s->B(iord, isb) * iord * (iord - 1) * uu[iord - 2];
+            }
+            feeuu = feeuu * dd1 * dd1 + feeu * dd2;
+            feeu = feeu * dd1 / rij;
+            fso[FI(i, j, N)] += fee;
+            for (int k = 0; k < 3; k++) {
+              fijo[FIJ(k, i, j, N)] += feeu * rvec_ee[k + 3 * ij];
+              fijo[FIJ(k, j, i, N)] -= feeu * rvec_ee[k + 3 * ij];
+            }
+            d2ijo[FI(i, j, N)] += 2 * (feeuu + 2 * feeu);
+          }
+          if (s->nordc > 1) {
+            // switch_scale2 on uu(1)
+            uu[1] = 1 - s->scalek * uu[1];
+            dd1 = -s->scalek * dd1;
+            dd2 = -s->scalek * dd2;
+            for (int iord = 2; iord <= s->nordc; iord++) uu[iord] = uu[1] * uu[iord - 1];
+            for (int ic = 0; ic < M; ic++) {
+              int it = s->iwctype[ic];
+              double ri = r_en[i + N * ic], rj = r_en[j + N * ic];
+              double dd7, dd8, dd9, dd10;
+              scale_dist2(*s, ri, rri[1], dd7, dd9);
+              scale_dist2(*s, rj, rrj[1], dd8, dd10);
+              if (rri[1] == s->asymp_r && rrj[1] == s->asymp_r) continue;
+              rri[1] = 1 - s->scalek * rri[1]; dd7 = -s->scalek * dd7; dd9 = -s->scalek * dd9;
+              rrj[1] = 1 - s->scalek * rrj[1]; dd8 = -s->scalek * dd8; dd10 = -s->scalek * dd10;
+              double sgs = ri + rj, tgs = ri - rj;
+              double u2pst = rij * rij + sgs * tgs, u2mst = rij * rij - sgs * tgs;
+              for (int iord = 1; iord <= s->nordc; iord++) {
+                rri[iord] = rri[1] * rri[iord - 1];
+                rrj[iord] = rrj[1] * rrj[iord - 1];
+                ss[iord] = rri[iord] + rrj[iord];
+                tt[iord] = rri[iord] * rrj[iord];
+              }
+              Een e = een_terms(uu, ss, tt, rri, rrj, it, true);
+              double fuu = e.fuu * dd1 * dd1 + e.fu * dd2;
+              double fu = e.fu * dd1 / rij;
+              double fui = e.fui * dd1 * dd7, fuj = e.fuj * dd1 * dd8;
+              double fii = e.fii * dd7 * dd7 + e.fi * dd9, fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
+              double fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
+              fso[FI(i, j, N)] += e.fc;
+              for (int k = 0; k < 3; k++) {
+                fijo[FIJ(k, i, j, N)] += fi * rvec_en[k + 3 * (i + N * ic)] + fu * rvec_ee[k + 3 * ij];
+                fijo[FIJ(k, j, i, N)] += fj * rvec_en[k + 3 * (j + N * ic)] - fu * rvec_ee[k + 3 * ij];
+              }
+              d2ijo[FI(i, j, N)] += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rij) + fuj * u2mst / (rj * rij) +
+                                    fii + 2 * fi + fjj + 2 * fj;
+            }
+          }
+          fsumo += fso[FI(i, j, N)];
+          for (int k = 0; k < 3; k++) {
+            fjo[k + 3 * i] += fijo[FIJ(k, i, j, N)];
+            fjo[k + 3 * j] += fijo[FIJ(k, j, i, N)];
+          }
+          d2o += d2ijo[FI(i, j, N)];
+        }
+    }
+    for (int i = 0; i < N; i++) {
+      fso[FI(i, i, N)] = 0;
+      for (int k = 0; k < 3; k++) fijo[FIJ(k, i, i, N)] = 0;
+      d2ijo[FI(i, i, N)] = 0;
+      for (int ic = 0; ic < M; ic++) {
+        int it = s->iwctype[ic];
+        double ri = r_en[i + N * ic], dd7, dd9;
+        scale_dist2(*s, ri, rri[1], dd7, dd9);
+        if (rri[1] == s->asymp_r) continue;
+        double top = s->A4(0, it) * rri[1], topi = s->A4(0, it), topii = 0;
+        double bot = 1 + s->A4(1, it) * rri[1], boti = s->A4(1, it), botii = 0, bot2 = bot * bot;
+        double fen = top / bot - s->asymp_jasa[it];
+        double feni = topi / bot - boti * top / bot2;
+        double fenii = topii - (botii * top + 2 * boti * topi) / bot + 2 * boti * boti * top / bot2;
+        fenii = fenii / bot;
+        for (int iord = 2; iord <= s->norda; iord++) {
+          rri[iord] = std::pow(rri[1], iord);
+          fen += s->A4(iord, it) * rri[iord];
+          feni += s->A4(iord, it) * iord * rri[iord - 1];
+          fenii += s->A4(iord, it) * iord * (iord - 1) * rri[iord - 2];
+        }
+        fenii = fenii * dd7 * dd7 + feni * dd9;
+        feni = feni * dd7 / ri;
+        fso[FI(i, i, N)] += fen;
+        for (int k = 0; k < 3; k++) fijo[FIJ(k, i, i, N)] += feni * rvec_en[k + 3 * (i + N * ic)];
+        d2ijo[FI(i, i, N)] += fenii + 2 * feni;
+      }
+      fsumo += fso[FI(i, i, N)];
+      for (int k = 0; k < 3; k++) fjo[k + 3 * i] += fijo[FIJ(k, i, i, N)];
+      d2o += d2ijo[FI(i, i, N)];
+    }
+  }
+
+  // ---- jastrow4e (vmc/jastrow4e.f90:3), iflag 0 (no Laplacian) or 1 ----
+  void jastrow4e(int iel, int iflag) {
+    const int nordj = std::max(std::max(s->norda, s->nordb), s->nordc);
+    vector<double> UU(nordj + 4, 0), SS(nordj + 4, 0), TT(nordj + 4, 0), RI(nordj + 4, 0), RJ(nordj + 4, 0);
+    double *uu = &UU[3], *ss = &SS[3], *tt = &TT[3], *rri = &RI[3], *rrj = &RJ[3];
+    uu[0] = 1; ss[0] = 2; tt[0] = 1; rri[0] = 1; rrj[0] = 1;
+    const bool second = iflag > 0;
+    if (N >= 2) {
+      fjn = fjo;
+      fsumn = fsumo;
+      d2n = d2o;
+      for (int jj = 0; jj < N; jj++) {
+        if (jj == iel) continue;
+        int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
+        int ij = i * (i - 1) / 2 + j;
+        for (int k = 0; k < 3; k++) fijn[FIJ(k, i, j, N)] = fijn[FIJ(k, j, i, N)] = 0;
+        fsn[FI(i, j, N)] = 0;
+        d2ijn[FI(i, j, N)] = 0;
+        double sspinn = 1;
+        int ipar = 0, isb = 0;
+        if (i < s->nup || j >= s->nup) {
+          if (s->nspin2b == 2) isb = 1;
+          else if (s->nocuspb == 0) sspinn = 0.5;
+          ipar = 1;
+        }
+        double rij = r_ee[ij], dd1, dd2 = 0;
+        if (!second) scale_dist1(*s, rij, uu[1], dd1);
+        else scale_dist2(*s, rij, uu[1], dd1, dd2);
+        if (uu[1] != s->asymp_r) {
+          double top = sspinn * s->B(0, isb) * uu[1], topu = sspinn * s->B(0, isb);
+          double bot = 1 + s->B(1, isb) * uu[1], botu = s->B(1, isb), bot2 = bot * bot;
+          double fee = top / bot - s->asymp_jasb[ipar];
+          double feeu = topu / bot - botu * top / bot2;
+          for (int iord = 2; iord <= s->nordb; iord++) {
+            uu[iord] = uu[1] * uu[iord - 1];
+            fee += s->B(iord, isb) * uu[iord];
+            feeu += s->B(iord, isb) * iord * uu[iord - 1];
+          }
+          double feeuu = 0;
+          if (second) {
+            double topuu = 0, botuu = 0;
+            feeuu = topuu - (botuu * top + 2 * botu * topu) / bot + 2 * botu * botu * top / bot2;
+            feeuu = feeuu / bot;
+            for (int iord = 2; iord <= s->nordb; iord++) feeuu += s->B(iord, isb) * iord * (iord - 1) * uu[iord - 2];
+            feeuu = feeuu * dd1 * dd1 + feeu * dd2;
+          }
+          feeu = feeu * dd1 / rij;
+          fsn[FI(i, j, N)] += fee;
+          for (int k = 0; k < 3; k++) {
+            fijn[FIJ(k, i, j, N)] += feeu * rvec_ee[k + 3 * ij];
+            fijn[FIJ(k, j, i, N)] -= feeu * rvec_ee[k + 3 * ij];
+          }
+          if (second) d2ijn[FI(i, j, N)] += 2 * (feeuu + 2 * feeu);
+        }
+        if (s->nordc > 1) {
+          uu[1] = 1 - s->scalek * uu[1];
+          dd1 = -s->scalek * dd1;
+          if (second) dd2 = -s->scalek * dd2;
+          for (int iord = 2; iord <= s->nordc; iord++) uu[iord] = uu[1] * uu[iord - 1];
+          for (int ic = 0; ic < M; ic++) {
+            int it = s->iwctype[ic];
+            double ri = r_en[i + N * ic], rj = r_en[j + N * ic];
+            double dd7, dd8, dd9 = 0, dd10 = 0;
+            if (!second) {
+              scale_dist1(*s, ri, rri[1], dd7);
+              scale_dist1(*s, rj, rrj[1], dd8);
+            } else {
+              scale_dist2(*s, ri, rri[1], dd7, dd9);
+              scale_dist2(*s, rj, rrj[1], dd8, dd10);
+            }
+            if (rri[1] == s->asymp_r && rrj[1] == s->asymp_r) continue;
+            rri[1] = 1 - s->scalek * rri[1]; dd7 = -s->scalek * dd7;
+            rrj[1] = 1 - s->scalek * rrj[1]; dd8 = -s->scalek * dd8;
+            if (second) { dd9 = -s->scalek * dd9; dd10 = -s->scalek * dd10; }
+            for (int iord = 1; iord <= s->nordc; iord++) {
+              rri[iord] = rri[1] * rri[iord - 1];
+              rrj[iord] = rrj[1] * rrj[iord - 1];
+              ss[iord] = rri[iord] + rrj[iord];
+              tt[iord] = rri[iord] * rrj[iord];
+            }
+            Een e = een_terms(uu, ss, tt, rri, rrj, it, second);
+            double fuu = 0, fui = 0, fuj = 0, fii = 0, fjj = 0, u2pst = 0, u2mst = 0;
+            if (second) {
+              double sgs = ri + rj, tgs = ri - rj;
+              u2pst = rij * rij + sgs * tgs;
+              u2mst = rij * rij - sgs * tgs;
+              fuu = e.fuu * dd1 * dd1 + e.fu * dd2;
+              fui = e.fui * dd1 * dd7;
+              fuj = e.fuj * dd1 * dd8;
+              fii = e.fii * dd7 * dd7 + e.fi * dd9;
+              fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
+            }
+            double fu = e.fu * dd1 / rij, fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
+            fsn[FI(i, j, N)] += e.fc;
+            for (int k = 0; k < 3; k++) {
+              fijn[FIJ(k, i, j, N)] += fi * rvec_en[k + 3 * (i + N * ic)] + fu * rvec_ee[k + 3 * ij];
+              fijn[FIJ(k, j, i, N)] += fj * rvec_en[k + 3 * (j + N * ic)] - fu * rvec_ee[k + 3 * ij];
+            }
+            if (second)
+              d2ijn[FI(i, j, N)] += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rij) + fuj * u2mst / (rj * rij) + fii +
+                                    2 * fi + fjj + 2 * fj;
+          }
+        }
+        fsumn = fsumn + fsn[FI(i, j, N)] - fso[FI(i, j, N)];
+        for (int k = 0; k < 3; k++) {
+          fjn[k + 3 * i] = fjn[k + 3 * i] + fijn[FIJ(k, i, j, N)] - fijo[FIJ(k, i, j, N)];
+          fjn[k + 3 * j] = fjn[k + 3 * j] + fijn[FIJ(k, j, i, N)] - fijo[FIJ(k, j, i, N)];
+        }
+        d2n = d2n + d2ijn[FI(i, j, N)] - d2ijo[FI(i, j, N)];
+      }
+    }
+    // e-n part (label 65)
+    for (int k = 0; k < 3; k++) fijn[FIJ(k, iel, iel, N)] = 0;
+    fsn[FI(iel, iel, N)] = 0;
+    d2ijn[FI(iel, iel, N)] = 0;
+    for (int ic = 0; ic < M; ic++) {
+      int it = s->iwctype[ic];
+      double ri = r_en[iel + N * ic], dd7, dd9 = 0;
+      if (!second) scale_dist1(*s, ri, rri[1], dd7);
+      else scale_dist2(*s, ri, rri[1], dd7, dd9);
+      if (rri[1] == s->asymp_r) continue;
+      double top = s->A4(0, it) * rri[1], topi = s->A4(0, it);
+      double bot = s->A4(1, it) * rri[1], boti = s->A4(1, it);
+      bot = 1 + bot;
+      double bot2 = bot * bot;
+      double fen = top / bot - s->asymp_jasa[it];
+      double feni = topi / bot - boti * top / bot2;
+      for (int iord = 2; iord <= s->norda; iord++) {
+        rri[iord] = std::pow(rri[1], iord);
+        fen += s->A4(iord, it) * rri[iord];
+        feni += s->A4(iord, it) * iord * rri[iord - 1];
+      }
+      double fenii = 0;
+      if (second) {
+        double topii = 0, botii = 0;
+        fenii = topii - (botii * top + 2 * boti * topi) / bot + 2 * boti * boti * top / bot2;
+        fenii = fenii / bot;
+        for (int iord = 2; iord <= s->norda; iord++) fenii += s->A4(iord, it) * iord * (iord - 1) * rri[iord - 2];
+        fenii = fenii * dd7 * dd7 + feni * dd9;
+      }
+      feni = feni * dd7 / ri;
+      fsn[FI(iel, iel, N)] += fen;
+      for (int k = 0; k < 3; k++) fijn[FIJ(k, iel, iel, N)] += feni * rvec_en[k + 3 * (iel + N * ic)];
+      if (second) d2ijn[FI(iel, iel, N)] += fenii + 2 * feni;
+    }
+    fsumn = fsumn + fsn[FI(iel, iel, N)] - fso[FI(iel, iel, N)];
+    for (int k = 0; k < 3; k++)
+      fjn[k + 3 * iel] = fjn[k + 3 * iel] + fijn[FIJ(k, iel, iel, N)] - fijo[FIJ(k, iel, iel, N)];
+    d2n = d2n + d2ijn[FI(iel, iel, N)] - d2ijo[FI(iel, iel, N)];
+  }
+
+  // jastrowe (vmc/jastrowe.f90:3): v = fjn, psij = fsumn
+  void jastrowe(int iel, int iflag) {
+    jastrow4e(iel, iflag);
+    vjn = fjn;
+  }
+  // jassav (vmc/jassav.f90:3)
+  void jassav(int iel, int iflag) {
+    fsumo = fsumn;
+    fjo = fjn;
+    for (int j = 0; j <= iel; j++) fso[FI(iel, j, N)] = fsn[FI(iel, j, N)];
+    for (int j = iel + 1; j < N; j++) fso[FI(j, iel, N)] = fsn[FI(j, iel, N)];
+    for (int j = 0; j < N; j++)
+      for (int k = 0; k < 3; k++) {
+        fijo[FIJ(k, iel, j, N)] = fijn[FIJ(k, iel, j, N)];
+        fijo[FIJ(k, j, iel, N)] = fijn[FIJ(k, j, iel, N)];
+      }
+    if (iflag > 0) {
+      d2o = d2n;
+      for (int j = 0; j <= iel; j++) d2ijo[FI(iel, j, N)] = d2ijn[FI(iel, j, N)];
+      for (int j = iel + 1; j < N; j++) d2ijo[FI(j, iel, N)] = d2ijn[FI(j, iel, N)];
+    }
+    vj = vjn;
+  }
+
+  // ---- orbitals (vmc/orbitals_no_qmckl.f90:19): all electrons, ider=2 ----
+  void orbitals_all() {
+    basis_fns(*s, 0, N, N, rvec_en.data(), r_en.data(), 2, phin.data(), dphin.data(), d2phin.data());
+    for (int i = 0; i < N; i++)
+      for (int iorb = 0; iorb < O; iorb++) {
+        double a = 0, d1 = 0, d2 = 0, d3 = 0, dd = 0;
+        for (int m = 0; m < K; m++) {
+          double cm = s->COEF(m, iorb);
+          a += cm * phin[m + K * i];
+          d1 += cm * dphin[m + K * (i + N * 0)];
+          d2 += cm * dphin[m + K * (i + N * 1)];
+          d3 += cm * dphin[m + K * (i + N * 2)];
+          dd += cm * d2phin[m + K * i];
+        }
+        orb[i + N * iorb] = a;
+        dorb[iorb + O * (i + N * 0)] = d1;
+        dorb[iorb + O * (i + N * 1)] = d2;
+        dorb[iorb + O * (i + N * 2)] = d3;
+        ddorb[iorb + O * i] = dd;
+      }
+  }
+  // orbitalse (vmc/orbitals_no_qmckl.f90:195): one electron, ider=1 or 2
+  void orbitalse(int iel, int iflag) {
+    int ider = iflag > 0 ? 2 : 1;
+    basis_fns(*s, iel, iel + 1, N, rvec_en.data(), r_en.data(), ider, phin.data(), dphin.data(), d2phin.data());
+    for (int iorb = 0; iorb < O; iorb++) {
+      double a = 0, d1 = 0, d2 = 0, d3 = 0, dd = 0;
+      for (int m = 0; m < K; m++) {
+        double cm = s->COEF(m, iorb);
+        a += cm * phin[m + K * iel];
+        d1 += cm * dphin[m + K * (iel + N * 0)];
+        d2 += cm * dphin[m + K * (iel + N * 1)];
+        d3 += cm * dphin[m + K * (iel + N * 2)];
+        if (ider == 2) dd += cm * d2phin[m + K * iel];
+      }
+      orbn[iorb] = a;
+      dorbn[iorb + O * 0] = d1;
+      dorbn[iorb + O * 1] = d2;
+      dorbn[iorb + O * 2] = d3;
+      if (ider == 2) ddorbn[iorb] = dd;
+    }
+  }
+
+  int nel_of(int iab) const { return iab == 0 ? s->nup : s->ndn; }
+  int occ(int jslot) const { return s->iworbd[jslot] - 1; }  // iworbd(j,kref), 0-based orbital
+
+  // ---- determinant (vmc/determinant.f90:9) + matinv ----
+  bool determinant() {
+    orbitals_all();
+    for (int iab = 0; iab < 2; iab++) {
+      int ish = iab == 0 ? 0 : s->nup, nel = nel_of(iab);
+      detiab[iab] = 1.0;
+      vector<double> &sl = slmi[iab];
+      for (int j = 0; j < nel; j++) {
+        int jorb = occ(j + ish);
+        int jk = nel * j;
+        for (int e = 0; e < nel; e++) {
+          sl[jk + e] = orb[(ish + e) + N * jorb];
+          // fp(k, j, iab) with stride nel*3 over electrons: fp(k, j + nel*e)
+          for (int k = 0; k < 3; k++) fp[iab][k + 3 * (j + nel * e)] = dorb[jorb + O * ((ish + e) + N * k)];
+          fpp[iab][j + nel * e] = ddorb[jorb + O * (ish + e)];
+        }
+      }
+      if (nel > 0) {
+        if (or_matinv(sl.data(), nel, &detiab[iab]) != 0) return false;
+      }
+      for (int i = 0; i < nel; i++) {
+        int ik = nel * i;
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int j = 0; j < nel; j++) {
+          a0 += sl[j + ik] * fp[iab][0 + 3 * (j + ik)];
+          a1 += sl[j + ik] * fp[iab][1 + 3 * (j + ik)];
+          a2 += sl[j + ik] * fp[iab][2 + 3 * (j + ik)];
+          a3 += sl[j + ik] * fpp[iab][j + ik];
+        }
+        ddx[0 + 3 * (i + ish)] = a0;
+        ddx[1 + 3 * (i + ish)] = a1;
+        ddx[2 + 3 * (i + ish)] = a2;
+        d2dx2[i + ish] = a3;
+      }
+    }
+    return true;
+  }
+
+  // ---- determinante (vmc/determinante.f90:3): ratio + eager SM update ----
+  void determinante(int iel, int iflag) {
+    orbitalse(iel, iflag);
+    int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
+    int ikel = nel * (iel - ish);
+    const vector<double> &sl = slmi[iab];
+    double ratio = 0;
+    for (int j = 0; j < nel; j++) ratio += sl[j + ikel] * orbn[occ(j + ish)];
+    detn = detiab[iab] * ratio;
+    if (ratio == 0.0) return;
+    for (int i = 0; i < nel; i++) {
+      if (i + ish == iel) continue;
+      int ik = nel * i;
+      double sum = 0;
+      for (int j = 0; j < nel; j++) sum += sl[j + ik] * orbn[occ(j + ish)];
+      sum = sum / ratio;
+      for (int j = 0; j < nel; j++) slmin[j + ik] = sl[j + ik] - sl[j + ikel] * sum;
+    }
+    for (int j = 0; j < nel; j++) slmin[j + ikel] = sl[j + ikel] / ratio;
+  }
+  // detsav (vmc/detsav.f90:3), single determinant
+  void detsav(int iel) {
+    int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab);
+    for (int j = 0; j < nel * nel; j++) slmi[iab][j] = slmin[j];
+    detiab[iab] = detn;
+    for (int iorb = 0; iorb < O; iorb++) {
+      orb[iel + N * iorb] = orbn[iorb];
+      for (int k = 0; k < 3; k++) dorb[iorb + O * (iel + N * k)] = dorbn[iorb + O * k];
+    }
+  }
+  // determinante_ref_grad (vmc/determinante.f90:285) with the given slmi column
+  void ref_grad(int iel, const double *sl, const double *dorbv /* dorb(norb,3) */, int ldo, double *v) {
+    int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
+    int ik = (iel - ish) * nel;
+    v[0] = v[1] = v[2] = 0;
+    for (int j = 0; j < nel; j++) {
+      int o = occ(j + ish);
+      v[0] += sl[j + ik] * dorbv[o + ldo * 0];
+      v[1] += sl[j + ik] * dorbv[o + ldo * 1];
+      v[2] += sl[j + ik] * dorbv[o + ldo * 2];
+    }
+  }
+  // compute_determinante_grad (vmc/determinante.f90:69), single det, iflag_move 1 or 0
+  void grad(int iel, int iflag_move, double *vd) {
+    if (iflag_move == 1) {
+      int iab = iel < s->nup ? 0 : 1;
+      double *dt = dorb_tmp.data();
+      for (int k = 0; k < 3; k++)
+        for (int iorb = 0; iorb < O; iorb++) dt[iorb + O * k] = dorb[iorb + O * (iel + N * k)];
+      double vref[3];
+      ref_grad(iel, slmi[iab].data(), dt, O, vref);
+      for (int k = 0; k < 3; k++) vd[k] = 0.0 + vref[k] + vj[k + 3 * iel];
+    } else {
+      double vref[3];
+      ref_grad(iel, slmin.data(), dorbn.data(), O, vref);
+      for (int k = 0; k < 3; k++) vd[k] = 0.0 + vref[k] + vjn[k + 3 * iel];
+    }
+  }
+
+  // ---- psie (vmc/hpsie.f90:3), single det; returns psid ----
+  double psie(int iel, const double *x, double &psij, int iflag) {
+    distances(iel, x);
+    jastrowe(iel, iflag);
+    psij = fsumn;
+    determinante(iel, iflag);
+    if (detn == 0.0) return 0.0;
+    int iab = iel < s->nup ? 0 : 1;
+    return detn * detiab[1 - iab] * s->cdet[0];
+  }
+
+  // ---- ECP: gauss_pot / getvps_gauss (vmc/readps_gauss.f90:6-92) ----
+  void gauss_pot(double r, int l /*1-based CHAMP channel*/, int ict, double &vpot, double &dvpot) const {
+    double v = 0, dv = 0, rsq = r * r;
+    int nt = s->necp_term[ict * CW_MPS_L + (l - 1)];
+    for (int i = 0; i < nt; i++) {
+      int idx = (ict * CW_MPS_L + (l - 1)) * CW_MGAUSS + i;
+      int pw = s->necp_power[idx];
+      double p, dpv;
+      if (pw != 2) {
+        p = std::pow(r, pw - 2);
+        dpv = (pw - 2) * p / r;
+      } else {
+        p = 1.0;
+        dpv = 0.0;
+      }
+      double e;
+      if (s->ecp_exponent[idx] * rsq > 7.0e2) e = 0.0;
+      else e = s->ecp_coef[idx] * std::exp(-s->ecp_exponent[idx] * rsq);
+      v += p * e;
+      dv += (dpv - 2 * p * s->ecp_exponent[idx] * r) * e;
+    }
+    vpot = v;
+    dvpot = dv;
+  }
+  void getvps_gauss(int iel) {
+    for (int ic = 0; ic < M; ic++) {
+      int ict = s->iwctype[ic];
+      double r = std::max(1.0e-10, r_en[iel + N * ic]);
+      double ri = 1.0 / r;
+      double vpot, dvpot;
+      int lp = s->lpot[ict];
+      gauss_pot(r, lp, ict, vpot, dvpot);
+      vpot = vpot - s->znuc[ict] * ri;
+      vps[iel + N * (ic + M * (lp - 1))] = vpot;
+      for (int l = 1; l <= lp - 1; l++) {
+        gauss_pot(r, l, ict, vpot, dvpot);
+        vps[iel + N * (ic + M * (l - 1))] = vpot;
+      }
+    }
+  }
+  static double yl0(int l, double costh) {
+    if (l == 1) return 1.0;
+    if (l == 2) return 3.0 * costh;
+    if (l == 3) return 2.5 * (3 * costh * costh - 1);
+    return 3.5 * (5 * costh * costh * costh - 3 * costh);
+  }
+  // psinl / psianl / psibnl (vmc/nonlpsi.f90), ijas=4
+  double psinl(double u, double rri, double rrj, int it) const {
+    if (rri == s->asymp_r && rrj == s->asymp_r) return 0.0;
+    const int nordj = std::max(std::max(s->norda, s->nordb), s->nordc);
+    double uu[16], ri[16], rj[16], ss[16], tt[16];
+    (void)nordj;
+    uu[1] = 1 - s->scalek * u;
+    ri[1] = 1 - s->scalek * rri;
+    rj[1] = 1 - s->scalek * rrj;
+    uu[0] = 1; ri[0] = 1; rj[0] = 1; ss[0] = 2; tt[0] = 1;
+    for (int jp = 1; jp <= s->nordc; jp++) {
+      uu[jp] = uu[1] * uu[jp - 1];
+      ri[jp] = ri[1] * ri[jp - 1];
+      rj[jp] = rj[1] * rj[jp - 1];
+      ss[jp] = ri[jp] + rj[jp];
+      tt[jp] = ri[jp] * rj[jp];
+    }
+    double v = 0;
+    int ll = 0;
+    for (int n = 2; n <= s->nordc; n++)
+      for (int k = n - 1; k >= 0; k--) {
+        int l_hi = (k == 0) ? n - k - 2 : n - k;
+        for (int l = l_hi; l >= 0; l--) {
+          int m = (n - k - l) / 2;
+          if (2 * m == n - k - l) {
+            v += s->C(ll, it) * uu[k] * ss[l] * tt[m];
+            ll++;
+          }
+        }
+      }
+    return v;
+  }
+  double psianl(double rri, int it) const {
+    if (rri == s->asymp_r) return 0.0;
+    double v = s->A4(0, it) * rri / (1.0 + s->A4(1, it) * rri) - s->asymp_jasa[it];
+    double rrip = rri;
+    for (int i = 2; i <= s->norda; i++) {
+      rrip *= rri;
+      v += s->A4(i, it) * rrip;
+    }
+    return v;
+  }
+  double psibnl(double u, int isb, int ipar, double sspinn) const {
+    if (u == s->asymp_r) return 0.0;
+    double fee = s->B(0, isb) * u / (1 + s->B(1, isb) * u);
+    double v = sspinn * fee - s->asymp_jasb[ipar];
+    double uu = u;
+    for (int i = 2; i <= s->nordb; i++) {
+      uu *= u;
+      v += s->B(i, isb) * uu;
+    }
+    return v;
+  }
+
+  // ---- nonloc_pot + nonloc (vmc/nonloc_pot.f90:3, vmc/nonloc.f90:5) ----
+  void nonloc_pot(const double *x, double &pe, double *vpsp_det) {
+    for (int i = 0; i < N; i++) getvps_gauss(i);
+    for (int ic = 0; ic < M; ic++)
+      for (int i = 0; i < N; i++) pe += vps[i + N * (ic + M * (s->lpot[s->iwctype[ic]] - 1))];
+    nonloc(x, vpsp_det);
+  }
+  void nonloc(const double *x, double *vpsp_det) {
+    vpsp_det[0] = vpsp_det[1] = 0;
+    // enumerate quadrature points (iel outer, ic middle, iq inner)
+    struct QP { int iel, ic, iq; double costh, x[3]; };
+    vector<QP> qp;
+    for (int i = 0; i < N; i++)
+      for (int ic = 0; ic < M; ic++) {
+        int ict = s->iwctype[ic];
+        int iskip = 1;
+        for (int l = 1; l <= s->lpot[ict] - 1; l++)
+          if (std::fabs(vps[i + N * (ic + M * (l - 1))]) > 1.0e-4) iskip = 0;
+        if (iskip) continue;
+        double ri = 1.0 / r_en[i + N * ic];
+        for (int iq = 0; iq < s->nquad; iq++) {
+          QP p;
+          p.iel = i; p.ic = ic; p.iq = iq;
+          p.costh = rvec_en[0 + 3 * (i + N * ic)] * xq[iq] + rvec_en[1 + 3 * (i + N * ic)] * yq[iq] +
+                    rvec_en[2 + 3 * (i + N * ic)] * zq[iq];
+          p.costh = p.costh * ri;
+          p.x[0] = r_en[i + N * ic] * xq[iq] + s->cent[0 + 3 * ic];
+          p.x[1] = r_en[i + N * ic] * yq[iq] + s->cent[1 + 3 * ic];
+          p.x[2] = r_en[i + N * ic] * zq[iq] + s->cent[2 + 3 * ic];
+          qp.push_back(p);
+        }
+      }
+    int nxq = (int)qp.size();
+    if (nxq == 0) return;
+    // distance_quad (vmc/nonloc.f90:364) + r_en_quad(nxquad,ic)=r_en(i,ic)
+    vector<double> rq((size_t)nxq * M), rvq((size_t)3 * nxq * M);
+    for (int q = 0; q < nxq; q++)
+      for (int jc = 0; jc < M; jc++) {
+        double rr = 0;
+        for (int k = 0; k < 3; k++) {
+          double d = qp[q].x[k] - s->cent[k + 3 * jc];
+          rvq[k + 3 * (q + (size_t)nxq * jc)] = d;
+        }
+        for (int k = 0; k < 3; k++) rr += rvq[k + 3 * (q + (size_t)nxq * jc)] * rvq[k + 3 * (q + (size_t)nxq * jc)];
+        rq[q + (size_t)nxq * jc] = std::sqrt(rr);
+      }
+    for (int q = 0; q < nxq; q++) rq[q + (size_t)nxq * qp[q].ic] = r_en[qp[q].iel + N * qp[q].ic];
+    // orbitals_quad (ider=0) + nonlocd_quad
+    vector<double> ph((size_t)K * nxq);
+    basis_fns(*s, 0, nxq, nxq, rvq.data(), rq.data(), 0, ph.data(), nullptr, nullptr);
+    vector<double> det_ratio(nxq), orbq(O);
+    for (int q = 0; q < nxq; q++) {
+      for (int iorb = 0; iorb < O; iorb++) {
+        double a = 0;
+        for (int m = 0; m < K; m++) a += s->COEF(m, iorb) * ph[m + (size_t)K * q];
+        orbq[iorb] = a;
+      }
+      int iel = qp[q].iel;
+      int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
+      int ikel = nel * (iel - ish);
+      double r = 0;
+      for (int j = 0; j < nel; j++) r += slmi[iab][j + ikel] * orbq[occ(j + ish)];
+      det_ratio[q] = r;
+    }
+    // nonlocj_quad4 (vmc/nonloc.f90:656)
+    vector<double> rr_en((size_t)N * M), rr_en_quad(M), ratio_jn(nxq);
+    for (int ic = 0; ic < M; ic++)
+      for (int i = 0; i < N; i++) scale_dist0(*s, r_en[i + N * ic], rr_en[i + N * ic]);
+    for (int q = 0; q < nxq; q++) {
+      int iel = qp[q].iel;
+      for (int ic = 0; ic < M; ic++) scale_dist0(*s, rq[q + (size_t)nxq * ic], rr_en_quad[ic]);
+      double fsum = 0;
+      if (N >= 2) {
+        for (int jj = 0; jj < N; jj++) {
+          if (jj == iel) continue;
+          int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
+          double sspinn = 1;
+          int ipar = 0, isb = 0;
+          if (i < s->nup || j >= s->nup) {
+            if (s->nspin2b == 2) isb = 1;
+            else if (s->nocuspb == 0) sspinn = 0.5;
+            ipar = 1;
+          }
+          double dx[3], rij = 0;
+          for (int k = 0; k < 3; k++) dx[k] = x[k + 3 * jj] - qp[q].x[k];
+          for (int k = 0; k < 3; k++) rij += dx[k] * dx[k];
+          rij = std::sqrt(rij);
+          double u;
+          scale_dist0(*s, rij, u);
+          double f = psibnl(u, isb, ipar, sspinn);
+          if (s->nordc > 1)
+            for (int ic = 0; ic < M; ic++) f += psinl(u, rr_en_quad[ic], rr_en[jj + N * ic], s->iwctype[ic]);
+          fsum = fsum + f - fso[FI(i, j, N)];
+        }
+      }
+      double fen = 0;
+      for (int ic = 0; ic < M; ic++) fen += psianl(rr_en_quad[ic], s->iwctype[ic]);
+      fsum = fsum + fen - fso[FI(iel, iel, N)];
+      ratio_jn[q] = fsum;
+    }
+    for (int q = 0; q < nxq; q++) {
+      int iel = qp[q].iel, ic = qp[q].ic, ict = s->iwctype[ic];
+      int iab = iel < s->nup ? 0 : 1;
+      double term = 0;
+      for (int l = 1; l <= s->lpot[ict] - 1; l++) term += yl0(l, qp[q].costh) * vps[iel + N * (ic + M * (l - 1))];
+      double trj = term * s->wq[qp[q].iq] * std::exp(ratio_jn[q]);
+      vpsp_det[iab] += trj * det_ratio[q];
+    }
+  }
+
+  // pot_local (vmc/pot_local.f90:3)
+  double pot_local() const {
+    double pe = s->pecent;
+    if (s->nloc == 0)
+      for (int i = 0; i < N; i++)
+        for (int ic = 0; ic < M; ic++) pe += -s->znuc[s->iwctype[ic]] / r_en[i + N * ic];
+    int ij = 0;
+    for (int i = 1; i < N; i++)
+      for (int j = 0; j < i; j++, ij++) pe += 1 / r_ee[ij];
+    return pe;
+  }
+
+  // ---- hpsi (vmc/hpsi.f90:3), single det; returns false if singular ----
+  bool hpsi(const double *coord, double &psid, double &psij, double &ekin, double &energy,
+            double *extra = nullptr) {
+    const double hb = 0.5;
+    distances(-1, coord);
+    double pe = pot_local();
+    jastrow_factor4();
+    vj = fjo;
+    double d2j = d2o;
+    psij = fsumo;
+    if (!determinant()) return false;
+    double vpsp[2] = {0, 0};
+    if (s->nloc > 0) nonloc_pot(coord, pe, vpsp);
+    double ekin_det[2], eloc_det[2];
+    for (int iab = 0; iab < 2; iab++) {
+      int nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
+      ekin_det[iab] = 0;
+      for (int i = 0; i < nel; i++) {
+        int e = i + ish;
+        double tmp = -hb * (d2dx2[e] + 2.0 * (vj[0 + 3 * e] * ddx[0 + 3 * e] + vj[1 + 3 * e] * ddx[1 + 3 * e] +
+                                              vj[2 + 3 * e] * ddx[2 + 3 * e]));
+        ekin_det[iab] += tmp;
+      }
+      eloc_det[iab] = ekin_det[iab] + vpsp[iab];
+    }
+    double ekin_other = -hb * d2j;
+    for (int i = 0; i < N; i++)
+      ekin_other += -hb * (vj[0 + 3 * i] * vj[0 + 3 * i] + vj[1 + 3 * i] * vj[1 + 3 * i] + vj[2 + 3 * i] * vj[2 + 3 * i]);
+    double e_other = ekin_other + pe;
+    psid = detiab[0] * detiab[1] * s->cdet[0];
+    double denergy = 0, dekin = 0;
+    energy = denergy + eloc_det[0] + eloc_det[1] + e_other;
+    ekin = dekin + ekin_det[0] + ekin_det[1] + ekin_other;
+    if (extra) {
+      extra[0] = pe;
+      extra[1] = vpsp[0] + vpsp[1];
+    }
+    return true;
+  }
+
+  // rotqua (vmc/rotqua.f90:357)
+  void rotqua() {
+    double x1, x2, x3, xsum;
+    do {
+      x1 = 1.0 - 2.0 * rng.uniform();
+      x2 = 1.0 - 2.0 * rng.uniform();
+      xsum = x1 * x1 + x2 * x2;
+    } while (xsum >= 1.0);
+    double xsum2 = 2.0 * std::sqrt(std::fabs(1.0 - xsum));
+    x1 = x1 * xsum2;
+    x2 = x2 * xsum2;
+    x3 = 1.0 - 2.0 * xsum;
+    double theta = std::acos(x3), sthet = std::sin(theta), cfi, sfi;
+    if (sthet < 1.0e-05) {
+      cfi = 1; sfi = 0; x1 = 0; x2 = 0; x3 = 1; sthet = 0;
+    } else {
+      cfi = x1 / sthet;
+      sfi = x2 / sthet;
+    }
+    double yy1 = x3 * cfi, yy2 = x3 * sfi, yy3 = -sthet;
+    double zz1 = -sfi, zz2 = cfi, zz3 = 0.0;
+    double u1, u2, usum;
+    do {
+      u1 = rng.uniform() * 2.0 - 1.0;
+      u2 = rng.uniform() * 2.0 - 1.0;
+      usum = u1 * u1 + u2 * u2;
+    } while (usum >= 1.0);
+    double uu = std::sqrt(usum);
+    u1 = u1 / uu;
+    u2 = u2 / uu;
+    double y1 = yy1 * u1 + zz1 * u2, y2 = yy2 * u1 + zz2 * u2, y3 = yy3 * u1 + zz3 * u2;
+    double z1 = yy1 * u2 - zz1 * u1, z2 = yy2 * u2 - zz2 * u1, z3 = yy3 * u2 - zz3 * u1;
+    for (int iq = 0; iq < s->nquad; iq++) {
+      xq[iq] = s->xq0[iq] * x1 + s->yq0[iq] * y1 + s->zq0[iq] * z1;
+      yq[iq] = s->xq0[iq] * x2 + s->yq0[iq] * y2 + s->zq0[iq] * z2;
+      zq[iq] = s->xq0[iq] * x3 + s->yq0[iq] * y3 + s->zq0[iq] * z3;
+    }
+  }
+
+  // zerest (vmc/acuest.f90:179): initial hpsi with the unrotated grid
+  bool zerest() {
+    zero_estimators();
+    xq = s->xq0; yq = s->yq0; zq = s->zq0;
+    double psid, psij, ekin, e;
+    if (!hpsi(xold.data(), psid, psij, ekin, e)) return false;
+    psido = psid; psijo = psij; eold = e; ekino = ekin;
+    psi2o = 2 * (std::log(std::fabs(psido)) + psijo);
+    distances(-1, xold.data());
+    for (int i = 0; i < N; i++) {
+      rmino[i] = 99.0e9;
+      for (int ic = 0; ic < M; ic++)
+        if (r_en[i + N * ic] < rmino[i]) {
+          rmino[i] = r_en[i + N * ic];
+          nearesto[i] = ic;
+        }
+      for (int k = 0; k < 3; k++) rvmino[k + 3 * i] = rvec_en[k + 3 * (i + N * nearesto[i])];
+    }
+    xnew = xold;
+    return true;
+  }
+
+  double thetamx(double r, double z) const {
+    return s->deltat + (2.0 - s->deltat) / (1.0 + (z * r) * (z * r));
+  }
+
+  // ---- metrop6 (vmc/metrop_mov1_slat.f90:3) ----
+  bool metrop6();
+};
+
+// gammai (vmc/gammai.f90:3)
+double gammai(double a, double x, double xae, int &iflag) {
+  if (x < a + 4) {
+    iflag = 1;
+    double ap = a, sum = 1 / a, del = sum;
+    int iter = (int)(21 + 3 * (x - a));
+    for (int n = 1; n <= iter; n++) {
+      ap = ap + 1;
+      del = del * x / ap;
+      sum = sum + del;
+    }
+    return sum * xae;
+  } else {
+    iflag = -1;
+    double a0 = 1, a1 = x, b0 = 0, b1 = 1, fac = 1, g = 0;
+    int iter = std::max(20 + (int)std::lround(a - x), 7);
+    for (int n = 1; n <= iter; n++) {
+      double an = (double)n, ana = an - a;
+      a0 = (a1 + a0 * ana) * fac;
+      b0 = (b1 + b0 * ana) * fac;
+      double anf = an * fac;
+      a1 = x * a0 + anf * a1;
+      b1 = x * b0 + anf * b1;
+      fac = 1 / a1;
+      g = b1 * fac;
+    }
+    return -(g * xae);
+  }
+}
+
+// Transition-area integral used twice in metrop6 (forward and reverse).
+double t_area(double zeta, double co, double rbot, double rtop, double bot) {
+  const double d5b2 = 2.5, d2b3 = .666666666666667, g5b2 = 1.329340388179137;
+  double rzero = -1.0 / co;
+  double zrbot = zeta * rbot, zrtop = zeta * rtop;
+  double zebot = std::sqrt(zrbot * zrbot * zrbot) * std::exp(-zrbot);
+  double zetop = std::sqrt(zrtop * zrtop * zrtop) * std::exp(-zrtop);
+  int iflagb, iflagt, iflagz;
+  double g52bot = gammai(d5b2, zrbot, zrbot * zebot, iflagb);
+  double g52top = gammai(d5b2, zrtop, zrtop * zetop, iflagt);
+  if (rzero < rbot || rzero > rtop) {
+    double g52dif = (iflagb * iflagt == 1) ? g52top - g52bot : g52top - g52bot + g5b2;
+    double g32dif = d2b3 * (g52dif + zetop - zebot);
+    return std::fabs(g32dif + co * g52dif / zeta) / (bot * std::sqrt(zeta * zeta * zeta));
+  }
+  double zrzer = zeta * rzero;
+  double zezer = std::sqrt(zrzer * zrzer * zrzer) * std::exp(-zrzer);
+  double g52zer = gammai(d5b2, zrzer, zrzer * zezer, iflagz);
+  double g52dif1 = (iflagb * iflagz == 1) ? g52zer - g52bot : g52zer - g52bot + g5b2;
+  double g32dif1 = d2b3 * (g52dif1 + zezer - zebot);
+  double g52dif2 = (iflagt * iflagz == 1) ? g52top - g52zer : g52top - g52zer + g5b2;
+  double g32dif2 = d2b3 * (g52dif2 + zetop - zezer);
+  return (std::fabs(g32dif1 + co * g52dif1 / zeta) + std::fabs(g32dif2 + co * g52dif2 / zeta)) /
+         (bot * std::sqrt(zeta * zeta * zeta));
+}
+
+bool Walker::metrop6() {
+  const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, d3b2 = 1.5, eps = 1.0e-10;
+  const double deltar = s->deltar, fbias = s->fbias;
+  double deltri = one / deltar;
+  for (int i = 0; i < N; i++) {
+    double *vo = &vold[3 * i];
+    grad(i, 1, vo);
+    double fxop = one;
+    int nearo = nearesto[i];
+    double zcusp = (s->nloc == 0) ? s->znuc[s->iwctype[nearo]] : zero;
+    rmino[i] = std::sqrt(rvmino[0 + 3 * i] * rvmino[0 + 3 * i] + rvmino[1 + 3 * i] * rvmino[1 + 3 * i] +
+                         rvmino[2 + 3 * i] * rvmino[2 + 3 * i]);
+    double rbot = rmino[i] * deltri, rtop = rmino[i] * deltar;
+    double voldr = zero;
+    for (int ic = 0; ic < 3; ic++) voldr += vo[ic] * rvmino[ic + 3 * i];
+    voldr = voldr / rmino[i];
+    double voldp = zero, xaxis[3], yaxis[3], zaxis[3];
+    for (int ic = 0; ic < 3; ic++) {
+      zaxis[ic] = rvmino[ic + 3 * i] / rmino[i];
+      xaxis[ic] = vo[ic] - voldr * zaxis[ic];
+      voldp += xaxis[ic] * xaxis[ic];
+    }
+    voldp = std::sqrt(voldp);
+    if (voldp < eps) {
+      xaxis[0] = eps * (one - zaxis[0] * zaxis[0]);
+      xaxis[1] = eps * (-zaxis[0] * zaxis[1]);
+      xaxis[2] = eps * (-zaxis[0] * zaxis[2]);
+      voldp = eps * std::sqrt(one - zaxis[0] * zaxis[0]);
+    }
+    for (int ic = 0; ic < 3; ic++) xaxis[ic] = xaxis[ic] / voldp;
+    double znear = s->znuc[s->iwctype[nearo]];
+    voldr = std::max(voldr, -2 * znear);
+    yaxis[0] = zaxis[1] * xaxis[2] - zaxis[2] * xaxis[1];
+    yaxis[1] = zaxis[2] * xaxis[0] - zaxis[0] * xaxis[2];
+    yaxis[2] = zaxis[0] * xaxis[1] - zaxis[1] * xaxis[0];
+    voldp = voldp * fbias;
+    double root = (zcusp + voldr) * (zcusp + voldr - four / rmino[i]), zeta;
+    if (root >= zero) {
+      root = std::sqrt(root);
+      zeta = half * (zcusp - voldr - root);
+      if (zeta <= zero) zeta = half * (zcusp - voldr + root);
+      if (zeta <= zero) zeta = eps;
+    } else {
+      zeta = (voldr < zero) ? -voldr - eps : one;
+    }
+    double co = (zeta + voldr) / (one - (zeta + voldr) * rmino[i]);
+    root = std::sqrt((d3b2 * co - zeta) * (d3b2 * co - zeta) + two * zeta * co);
+    double rmax1 = (d3b2 * co - zeta + root) / (two * zeta * co);
+    if (rmax1 < rbot) rmax1 = rbot;
+    if (rmax1 > rtop) rmax1 = rtop;
+    double fmax = std::sqrt(rmax1) * std::fabs(one + co * rmax1) * std::exp(-zeta * rmax1);
+    if (co < zero) {
+      double rmax2 = (d3b2 * co - zeta - root) / (two * zeta * co);
+      if (rmax2 < rbot) rmax2 = rbot;
+      if (rmax2 > rtop) rmax2 = rtop;
+      double fmax2 = std::sqrt(rmax2) * std::fabs(one + co * rmax2) * std::exp(-zeta * rmax2);
+      fmax = std::max(fmax, fmax2);
+    }
+    double bot = std::sqrt(rmino[i]) * std::fabs(one + co * rmino[i]) * std::exp(-zeta * rmino[i]);
+    double rtry, top;
+    for (;;) {
+      rtry = ((deltar - deltri) * rng.uniform() + deltri) * rmino[i];
+      top = std::sqrt(rtry) * std::fabs(one + co * rtry) * std::exp(-zeta * rtry);
+      double ratio = top / fmax;
+      if (ratio > rng.uniform()) break;
+    }
+    fxop = fxop * top / bot;
+    double areao = t_area(zeta, co, rbot, rtop, bot);
+    double raver = half * (rmino[i] + rtry);
+    double deltt = thetamx(raver, znear);
+    double costht = one - deltt * rng.uniform();
+    double zprime = rtry * costht;
+    double sintht = std::sqrt(one - costht * costht);
+    areao = areao * deltt;
+    double term = std::min(voldp * raver * sintht, one);
+    fmax = one + term;
+    double phitry, cosphi;
+    for (;;) {
+      phitry = PI * rng.uniform();
+      cosphi = std::cos(phitry);
+      top = one + term * cosphi;
+      if (top > rng.uniform() * fmax) break;
+    }
+    fxop = fxop * top;
+    double xprime = rtry * sintht * std::cos(phitry);
+    double yprime = std::sqrt(std::max(zero, rtry * rtry - xprime * xprime - zprime * zprime));
+    if (rng.uniform() < half) yprime = -yprime;
+    for (int ic = 0; ic < 3; ic++) {
+      rvminno[ic + 3 * i] = xaxis[ic] * xprime + yaxis[ic] * yprime + zaxis[ic] * zprime;
+      xnew[ic + 3 * i] = rvminno[ic + 3 * i] + s->cent[ic + 3 * nearo];
+    }
+    rminno[i] = rtry;
+    // geometrical rejection
+    rminn[i] = 99.0e9;
+    for (int j = 0; j < M; j++) {
+      double dist = zero;
+      for (int ic = 0; ic < 3; ic++) dist += (xnew[ic + 3 * i] - s->cent[ic + 3 * j]) * (xnew[ic + 3 * i] - s->cent[ic + 3 * j]);
+      if (dist < rminn[i]) {
+        rminn[i] = dist;
+        nearestn[i] = j;
+      }
+    }
+    int nearn = nearestn[i];
+    rminn[i] = std::sqrt(rminn[i]);
+    rminon[i] = zero;
+    double dot = zero;
+    for (int ic = 0; ic < 3; ic++) {
+      rvminn[ic + 3 * i] = xnew[ic + 3 * i] - s->cent[ic + 3 * nearn];
+      rvminon[ic + 3 * i] = xold[ic + 3 * i] - s->cent[ic + 3 * nearn];
+      rminon[i] += rvminon[ic + 3 * i] * rvminon[ic + 3 * i];
+      dot += rvminn[ic + 3 * i] * rvminon[ic + 3 * i];
+    }
+    rminon[i] = std::sqrt(rminon[i]);
+    dot = dot / (rminn[i] * rminon[i]);
+    costht = dot;
+    sintht = std::sqrt(one - costht * costht);
+    double ravern = half * (rminn[i] + rminon[i]);
+    delttn[i] = thetamx(ravern, s->znuc[s->iwctype[nearn]]);
+    int igeometrical = 0;
+    double p = zero, psi2n = 0, psidn = 0, psijn = 0;
+    double vn[3] = {0, 0, 0};
+    if (rminon[i] > rminn[i] * deltar || dot < one - delttn[i]) {
+      igeometrical = 1;
+      p = zero;
+    } else {
+      double rratio = rminno[i] / rminon[i];
+      psidn = psie(i, xnew.data(), psijn, 0);
+      if (psidn == 0.0) {
+        // psi2g computed as 1 (iguiding=0): only psid==0 (detn==0) rejects
+      }
+      bool zero_psi = (detn == 0.0);
+      if (zero_psi) {
+        p = zero;
+      } else {
+        grad(i, 0, vn);
+        for (int k = 0; k < 3; k++) vnew[k + 3 * i] = vn[k];
+        psi2n = std::log(std::fabs(1.0)) + 2 * (std::log(std::fabs(psidn)) + psijn);
+        double fxnp = one;
+        rbot = rminn[i] * deltri;
+        rtop = rminn[i] * deltar;
+        double vnewr = zero;
+        for (int ic = 0; ic < 3; ic++) vnewr += vn[ic] * rvminn[ic + 3 * i];
+        vnewr = vnewr / rminn[i];
+        double vnewp = zero;
+        for (int ic = 0; ic < 3; ic++) {
+          xaxis[ic] = vn[ic] - vnewr * rvminn[ic + 3 * i] / rminn[i];
+          vnewp += xaxis[ic] * xaxis[ic];
+        }
+        vnewp = std::sqrt(vnewp);
+        if (vnewp < eps) {
+          xaxis[0] = eps * (one - rvminn[0 + 3 * i] * rvminn[0 + 3 * i]);
+          xaxis[1] = eps * (-rvminn[0 + 3 * i] * rvminn[1 + 3 * i]);
+          xaxis[2] = eps * (-rvminn[0 + 3 * i] * rvminn[2 + 3 * i]);
+          vnewp = eps * std::sqrt(one - rvminn[0 + 3 * i] * rvminn[0 + 3 * i] * (two - rminn[i] * rminn[i]));
+        }
+        for (int ic = 0; ic < 3; ic++) xaxis[ic] = xaxis[ic] / vnewp;
+        double zc = (s->nloc == 0) ? s->znuc[s->iwctype[nearn]] : zero;
+        vnewr = std::max(vnewr, -2 * s->znuc[s->iwctype[nearn]]);
+        vnewp = vnewp * fbias;
+        root = (zc + vnewr) * (zc + vnewr - four / rminn[i]);
+        if (root >= zero) {
+          root = std::sqrt(root);
+          zeta = half * (zc - vnewr - root);
+          if (zeta <= zero) zeta = half * (zc - vnewr + root);
+          if (zeta <= zero) zeta = eps;
+        } else {
+          zeta = (vnewr < zero) ? -vnewr - eps : one;
+        }
+        co = (zeta + vnewr) / (one - (zeta + vnewr) * rminn[i]);
+        bot = std::sqrt(rminn[i]) * std::fabs(one + co * rminn[i]) * std::exp(-zeta * rminn[i]);
+        top = std::sqrt(rminon[i]) * std::fabs(one + co * rminon[i]) * std::exp(-zeta * rminon[i]);
+        fxnp = fxnp * top / bot;
+        double arean = t_area(zeta, co, rbot, rtop, bot);
+        arean = arean * delttn[i];
+        term = std::min(vnewp * ravern * sintht, one);
+        cosphi = zero;
+        double rnorm = zero;
+        for (int ic = 0; ic < 3; ic++) {
+          double term2 = rvminon[ic + 3 * i] / rminon[i] - costht * rvminn[ic + 3 * i] / rminn[i];
+          rnorm += term2 * term2;
+          cosphi += term2 * xaxis[ic];
+        }
+        cosphi = cosphi / std::sqrt(rnorm);
+        fxnp = fxnp * (one + term * cosphi);
+        p = rratio * rratio * std::exp(psi2n - psi2o) * std::fabs((fxnp * areao) / (fxop * arean));
+        p = std::min(one, p);
+      }
+    }
+    if (rng.uniform() < p) {
+      rmino[i] = rminn[i];
+      nearesto[i] = nearestn[i];
+      psi2o = psi2n;
+      for (int ic = 0; ic < 3; ic++) {
+        xold[ic + 3 * i] = xnew[ic + 3 * i];
+        rvmino[ic + 3 * i] = rvminn[ic + 3 * i];
+      }
+      psido = psidn;
+      psijo = psijn;
+      acc = acc + one;
+      jassav(i, 0);
+      detsav(i);
+    } else {
+      for (int ic = 0; ic < 3; ic++) xnew[ic + 3 * i] = xold[ic + 3 * i];
+      if (igeometrical == 0) distancese_restore(i);
+    }
+  }
+  // primary configuration: full recompute
+  double ekin, e;
+  if (!hpsi(xold.data(), psido, psijo, ekin, e)) return false;
+  eold = e;
+  ekino = ekin;
+  psi2o = 2 * (std::log(std::fabs(psido)) + psijo);
+  double wtg_sqrt = psido / psido * std::exp(psijo - psijo) / std::sqrt(1.0);
+  double wtg = wtg_sqrt * wtg_sqrt;
+  esum1 = eold;
+  wsum += wtg;
+  esum += eold * wtg;
+  pesum += (eold - ekino) * wtg;
+  tpbsum += ekino * wtg;
+  // acues1 + acusig
+  ecum1 += esum1 * wtg;
+  ecm21 += esum1 * esum1 * wtg;
+  ecum1s += eold * wtg;
+  ecm21s += eold * eold * wtg;
+  return true;
+}
+
+struct Walkers {
+  const Sys *s;
+  vector<Walker> w;
+  // global (rank-0) cumulative estimators after acuest_reduce
+  double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
+  double ecum1 = 0, ecm21 = 0, ecum1s = 0, ecm21s = 0;
+  long iblk = 0, passes = 0;
+  int nstep_last = 0;
+  bool failed = false;
+};
+
+}  // namespace
+
+// ===========================================================================
+// C API
+// ===========================================================================
+extern "C" {
+
+int or_nterms4(int nordc) { return nterms4(nordc); }
+
+void *or_sys_create(const cw_system_desc *d) {
+  Sys *s = new Sys();
+  s->N = d->nelec; s->nup = d->nup; s->ndn = d->nelec - d->nup;
+  s->M = d->ncent; s->nctype = d->nctype;
+  s->iwctype.assign(d->iwctype, d->iwctype + d->ncent);
+  s->cent.assign(d->cent, d->cent + 3 * d->ncent);
+  s->znuc.assign(d->znuc, d->znuc + d->nctype);
+  s->pecent = d->pecent;
+  s->mrwf = d->mrwf; s->mpts = d->mrwf_pts;
+  s->nrbas.assign(d->nrbas, d->nrbas + d->nctype);
+  s->igrid.assign(d->igrid, d->igrid + d->nctype);
+  s->nr.assign(d->nr, d->nr + d->nctype);
+  s->arg.assign(d->arg, d->arg + d->nctype);
+  s->r0.assign(d->r0, d->r0 + d->nctype);
+  size_t nt = (size_t)d->nctype * d->mrwf;
+  s->rwf.assign(d->rwf, d->rwf + nt * d->mrwf_pts);
+  s->d2rwf.assign(d->d2rwf, d->d2rwf + nt * d->mrwf_pts);
+  s->ce.assign(d->ce, d->ce + nt * CW_NCOEF);
+  s->ae.assign(d->ae, d->ae + nt * 2);
+  s->rmaxwf.assign(d->rmaxwf, d->rmaxwf + nt);
+  s->mbastyp = d->mbastyp;
+  s->nbastyp.assign(d->nbastyp, d->nbastyp + d->nctype);
+  s->iwlbas.assign(d->iwlbas, d->iwlbas + (size_t)d->nctype * d->mbastyp);
+  s->iwrwf.assign(d->iwrwf, d->iwrwf + (size_t)d->nctype * d->mbastyp);
+  s->K = d->nbasis; s->O = d->norb; s->ndet = d->ndet;
+  s->coef.assign(d->coef, d->coef + (size_t)d->nbasis * d->norb);
+  s->cdet.assign(d->cdet, d->cdet + d->ndet);
+  s->iworbd.assign(d->iworbd, d->iworbd + d->nelec);
+  s->norda = d->norda; s->nordb = d->nordb; s->nordc = d->nordc;
+  s->isc = d->isc; s->nspin2b = d->nspin2b; s->nocuspb = d->nocuspb;
+  s->scalek = d->scalek;
+  s->nterms = nterms4(d->nordc);
+  s->a4.assign(d->a4, d->a4 + (size_t)(d->norda + 1) * d->nctype);
+  s->b.assign(d->b, d->b + (size_t)(d->nordb + 1) * d->nspin2b);
+  if (s->nterms > 0) s->c.assign(d->c, d->c + (size_t)s->nterms * d->nctype);
+  s->nloc = d->nloc;
+  if (d->nloc > 0) {
+    s->lpot.assign(d->lpot, d->lpot + d->nctype);
+    s->necp_term.assign(d->necp_term, d->necp_term + (size_t)d->nctype * CW_MPS_L);
+    size_t ng = (size_t)d->nctype * CW_MPS_L * CW_MGAUSS;
+    s->necp_power.assign(d->necp_power, d->necp_power + ng);
+    s->ecp_exponent.assign(d->ecp_exponent, d->ecp_exponent + ng);
+    s->ecp_coef.assign(d->ecp_coef, d->ecp_coef + ng);
+    s->nquad = d->nquad;
+    s->xq0.assign(d->xq0, d->xq0 + d->nquad);
+    s->yq0.assign(d->yq0, d->yq0 + d->nquad);
+    s->zq0.assign(d->zq0, d->zq0 + d->nquad);
+    s->wq.assign(d->wq, d->wq + d->nquad);
+  } else {
+    s->nquad = 0;
+  }
+  s->deltar = d->deltar; s->deltat = d->deltat; s->fbias = d->fbias;
+  set_scale_dist(*s);
+  return s;
+}
+
+void or_sys_destroy(void *sys) { delete (Sys *)sys; }
+
+double or_pot_nn(int ncent, const double *cent, const double *znuc, const int32_t *iwctype) {
+  // pot_nn: sum_{i<j} Z_i Z_j / r_ij, i outer 2..ncent, j inner 1..i-1
+  double pe = 0;
+  for (int i = 1; i < ncent; i++)
+    for (int j = 0; j < i; j++) {
+      double r = 0;
+      for (int k = 0; k < 3; k++) r += (cent[k + 3 * i] - cent[k + 3 * j]) * (cent[k + 3 * i] - cent[k + 3 * j]);
+      r = std::sqrt(r);
+      pe += znuc[iwctype[i]] * znuc[iwctype[j]] / r;
+    }
+  return pe;
+}
+
+int or_matinv(double *a, int n, double *determinant) {
+  // matinv (vmc/matinv.f90:22). n<=2 closed forms; else partial-pivot LU
+  // (pivot = first entry of maximal |a| in the column, as idamax) with the
+  // base-10 scaled determinant product, then the inverse from the LU factors.
+  if (n == 0) return 0;
+  if (n == 1) {
+    *determinant = a[0];
+    a[0] = 1.0 / a[0];
+    return 0;
+  }
+  if (n == 2) {
+    *determinant = a[0] * a[3] - a[2] * a[1];
+    double deti = 1.0 / *determinant;
+    double aux = a[0];
+    a[0] = a[3] * deti;
+    a[3] = aux * deti;
+    a[1] = -a[1] * deti;
+    a[2] = -a[2] * deti;
+    return 0;
+  }
+  auto A = [&](int i, int j) -> double & { return a[i + n * j]; };
+  vector<int> ipvt(n);
+  for (int k = 0; k < n; k++) {
+    int p = k;
+    double amax = std::fabs(A(k, k));
+    for (int i = k + 1; i < n; i++)
+      if (std::fabs(A(i, k)) > amax) {
+        amax = std::fabs(A(i, k));
+        p = i;
+      }
+    ipvt[k] = p;
+    if (A(p, k) == 0.0) return 1;
+    if (p != k)
+      for (int j = 0; j < n; j++) std::swap(A(k, j), A(p, j));
+    double piv = 1.0 / A(k, k);
+    for (int i = k + 1; i < n; i++) A(i, k) *= piv;
+    for (int j = k + 1; j < n; j++) {
+      double akj = A(k, j);
+      if (akj != 0.0)
+        for (int i = k + 1; i < n; i++) A(i, j) -= A(i, k) * akj;
+    }
+  }
+  double det1 = 1.0, det2 = 0.0;
+  const double ten = 10.0;
+  for (int i = 0; i < n; i++) {
+    if (ipvt[i] != i) det1 = -det1;
+    det1 = A(i, i) * det1;
+    if (det1 == 0.0) break;
+    while (std::fabs(det1) < 1.0) { det1 = ten * det1; det2 = det2 - 1.0; }
+    while (std::fabs(det1) >= ten) { det1 = det1 / ten; det2 = det2 + 1.0; }
+  }
+  *determinant = det1 * std::pow(10.0, det2);
+  // inverse: inv(U) in place, then solve inv(A)*L = inv(U), then column swaps
+  vector<double> col(n);
+  for (int j = 0; j < n; j++) {
+    A(j, j) = 1.0 / A(j, j);
+    double ajj = -A(j, j);
+    // column j of inv(U): inv(U)(0:j-1,0:j-1) * U(0:j-1,j) * (-1/U(j,j))
+    for (int i = 0; i < j; i++) {
+      double sum = 0;
+      for (int k = i; k < j; k++) sum += A(i, k) * A(k, j);
+      col[i] = sum;
+    }
+    for (int i = 0; i < j; i++) A(i, j) = col[i] * ajj;
+  }
+  vector<double> work(n);
+  for (int j = n - 2; j >= 0; j--) {
+    for (int i = j + 1; i < n; i++) {
+      work[i] = A(i, j);
+      A(i, j) = 0.0;
+    }
+    for (int i = 0; i < n; i++) {
+      double sum = 0;
+      for (int k = j + 1; k < n; k++) sum += A(i, k) * work[k];
+      A(i, j) -= sum;
+    }
+  }
+  for (int j = n - 2; j >= 0; j--) {
+    int jp = ipvt[j];
+    if (jp != j)
+      for (int i = 0; i < n; i++) std::swap(A(i, j), A(i, jp));
+  }
+  return 0;
+}
+
+void or_rng_states(const int32_t *irn8, int nwalk, uint64_t *out) {
+  Rng r;
+  std::memcpy(r.s, irn8, 32);
+  for (int w = 0; w < nwalk; w++) {
+    std::memcpy(out + 4 * w, r.s, 32);
+    r.jump();
+  }
+}
+
+void or_rng_uniform(uint64_t *state, int n, double *out) {
+  Rng r;
+  std::memcpy(r.s, state, 32);
+  for (int i = 0; i < n; i++) out[i] = r.uniform();
+  std::memcpy(state, r.s, 32);
+}
+
+void or_gesqua(int *nq, double *xq, double *yq, double *zq, double *wq) {
+  // gesqua (vmc/rotqua.f90:3), cases needed here: 4 (tetrahedron), 6, 18, 26
+  // (octahedron family); other orders fall back to the closest of these.
+  static const int iqs[4] = {4, 6, 18, 26};
+  int best = 0;
+  for (int c = 1; c < 4; c++)
+    if (std::abs(*nq - iqs[c]) < std::abs(*nq - iqs[best])) best = c;
+  int n = iqs[best];
+  *nq = n;
+  for (int j = 0; j < n; j++) xq[j] = yq[j] = zq[j] = wq[j] = 0;
+  double p = 1.0 / std::sqrt(2.0), q = 1.0 / std::sqrt(3.0);
+  if (n == 4) {
+    for (int j = 0; j < 4; j++) {
+      wq[j] = 0.25;
+      xq[j] = (j + 1 > 2) ? -q : q;
+      yq[j] = (j + 1 == 2 || j + 1 == 4) ? -q : q;
+      zq[j] = (j + 1 == 2 || j + 1 == 3) ? -q : q;
+    }
+    return;
+  }
+  // weights ww(icase,k) for icase 2 (6), 4 (18), 5 (26) and octa counts 6,12,8
+  double w1, w2, w3;
+  if (n == 6) { w1 = 1.0 / 6.0; w2 = 0; w3 = 0; }
+  else if (n == 18) { w1 = 1.0 / 30.0; w2 = 1.0 / 15.0; w3 = 0; }
+  else { w1 = 1.0 / 21.0; w2 = 4.0 / 105.0; w3 = 27.0 / 840.0; }
+  for (int j = 0; j < n; j++) wq[j] = j < 6 ? w1 : (j < 18 ? w2 : w3);
+  int ip = 0, lp = 0;
+  double si = -1.0;
+  for (int ii = 0; ii < 2; ii++) {
+    si = -si;
+    xq[ii] = si;
+    yq[2 + ii] = si;
+    zq[4 + ii] = si;
+    if (n > 6) {
+      double sj = -1.0;
+      for (int jj = 0; jj < 2; jj++) {
+        sj = -sj;
+        ip++;
+        xq[5 + ip] = si * p;
+        yq[5 + ip] = sj * p;
+        yq[9 + ip] = si * p;
+        zq[9 + ip] = sj * p;
+        zq[13 + ip] = si * p;
+        xq[13 + ip] = sj * p;
+        if (n > 18) {
+          double sk = -1.0;
+          for (int kk = 0; kk < 2; kk++) {
+            sk = -sk;
+            lp++;
+            xq[17 + lp] = si * q;
+            yq[17 + lp] = sj * q;
+            zq[17 + lp] = sk * q;
+          }
+        }
+      }
+    }
+  }
+}
+
+void or_sites(void *sysp, uint64_t *state, double *x) {
+  const Sys &s = *(const Sys *)sysp;
+  Rng r;
+  std::memcpy(r.s, state, 32);
+  // nsite rule of mc_configs_start (vmc/mc_configs.f90:75-94), no charged atom
+  vector<int> nsite(s.M);
+  int l = 0;
+  for (int i = 0; i < s.M; i++) {
+    nsite[i] = (int)(s.znuc[s.iwctype[i]] + 0.5);
+    l += nsite[i];
+    if (l > s.N) {
+      nsite[i] -= (l - s.N);
+      l = s.N;
+    }
+  }
+  if (l < s.N) nsite[0] += (s.N - l);
+  // sites (vmc/sites.f90:3)
+  l = 0;
+  for (int ispin = 1; ispin <= 2; ispin++)
+    for (int i = 0; i < s.M && l < s.N; i++) {
+      int ju = (nsite[i] + 2 - ispin) / 2;
+      for (int j = 1; j <= ju; j++) {
+        l++;
+        if (l > s.N) break;
+        double z = s.znuc[s.iwctype[i]], sitsca;
+        if (j == 1) sitsca = 1 / z;
+        else if (j <= 5) sitsca = 2 / (z - 2);
+        else sitsca = 3 / (z - 10);
+        for (int ic = 0; ic < 3; ic++) {
+          double site = -std::log(r.uniform());
+          double sg = r.uniform() - 0.5;
+          site = sg >= 0 ? std::fabs(site) : -std::fabs(site);
+          x[ic + 3 * (l - 1)] = sitsca * site + s.cent[ic + 3 * i];
+        }
+      }
+    }
+  std::memcpy(state, r.s, 32);
+}
+
+void or_orbitals(void *sys, const double *x, double *orb, double *dorb, double *ddorb) {
+  Walker w((const Sys *)sys);
+  w.distances(-1, x);
+  w.orbitals_all();
+  if (orb) std::memcpy(orb, w.orb.data(), sizeof(double) * w.orb.size());
+  if (dorb) std::memcpy(dorb, w.dorb.data(), sizeof(double) * w.dorb.size());
+  if (ddorb) std::memcpy(ddorb, w.ddorb.data(), sizeof(double) * w.ddorb.size());
+}
+
+void or_jastrow(void *sys, const double *x, double *psij, double *v, double *d2j) {
+  Walker w((const Sys *)sys);
+  w.distances(-1, x);
+  w.jastrow_factor4();
+  if (psij) *psij = w.fsumo;
+  if (v) std::memcpy(v, w.fjo.data(), sizeof(double) * w.fjo.size());
+  if (d2j) *d2j = w.d2o;
+}
+
+int or_slater(void *sys, const double *x, double *slmi, double *det) {
+  const Sys *s = (const Sys *)sys;
+  Walker w(s);
+  w.distances(-1, x);
+  if (!w.determinant()) return 1;
+  int nmax = std::max(s->nup, s->ndn);
+  for (int iab = 0; iab < 2; iab++) {
+    int nel = iab == 0 ? s->nup : s->ndn;
+    if (slmi)
+      for (int j = 0; j < nel * nel; j++) slmi[iab * nmax * nmax + j] = w.slmi[iab][j];
+    if (det) det[iab] = w.detiab[iab];
+  }
+  return 0;
+}
+
+int or_hpsi(void *sys, const double *x, const double *xq, const double *yq, const double *zq, double *out) {
+  const Sys *s = (const Sys *)sys;
+  Walker w(s);
+  if (xq) {
+    w.xq.assign(xq, xq + s->nquad);
+    w.yq.assign(yq, yq + s->nquad);
+    w.zq.assign(zq, zq + s->nquad);
+  }
+  double psid, psij, ekin, e, extra[2];
+  if (!w.hpsi(x, psid, psij, ekin, e, extra)) return 1;
+  out[0] = e; out[1] = psid; out[2] = psij; out[3] = ekin; out[4] = extra[0]; out[5] = extra[1];
+  return 0;
+}
+
+void *or_walkers_create(void *sysp, int nwalk, const double *x, const uint64_t *rng) {
+  const Sys *s = (const Sys *)sysp;
+  Walkers *ws = new Walkers();
+  ws->s = s;
+  ws->w.reserve(nwalk);
+  for (int k = 0; k < nwalk; k++) {
+    ws->w.emplace_back(s);
+    Walker &w = ws->w.back();
+    std::memcpy(w.rng.s, rng + 4 * k, 32);
+    std::memcpy(w.xold.data(), x + (size_t)3 * s->N * k, sizeof(double) * 3 * s->N);
+    if (!w.zerest()) ws->failed = true;
+  }
+  return ws;
+}
+
+void or_walkers_destroy(void *ws) { delete (Walkers *)ws; }
+
+int or_zerest(void *wsp) {
+  // zerest (vmc/acuest.f90:179) on every walker + the rank-0 cumulative sums
+  Walkers *ws = (Walkers *)wsp;
+  int bad = 0;
+  for (Walker &w : ws->w)
+    if (!w.zerest()) bad = 1;
+  ws->ecum = ws->ecm2 = ws->wcum = ws->pecum = ws->tpbcum = ws->pecm2 = ws->tpbcm2 = ws->acc = 0;
+  ws->ecum1 = ws->ecm21 = ws->ecum1s = ws->ecm21s = 0;
+  ws->iblk = 0;
+  ws->passes = 0;
+  return bad;
+}
+
+int or_vmc_steps(void *wsp, int nstep, int nthreads) {
+  Walkers *ws = (Walkers *)wsp;
+  int W = (int)ws->w.size();
+  if (nthreads < 1) nthreads = 1;
+  vector<int> bad(W, 0);
+  auto work = [&](int t) {
+    for (int k = t; k < W; k += nthreads) {
+      Walker &w = ws->w[k];
+      for (int st = 0; st < nstep; st++) {
+        if (ws->s->nloc > 0) w.rotqua();
+        if (!w.metrop6()) { bad[k] = 1; break; }
+      }
+    }
+  };
+  if (nthreads == 1) work(0);
+  else {
+    vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work, t);
+    for (auto &t : th) t.join();
+  }
+  ws->passes += nstep;
+  ws->nstep_last = nstep;
+  for (int k = 0; k < W; k++)
+    if (bad[k]) return 1;
+  return 0;
+}
+
+void or_end_block(void *wsp, double *block_energy) {
+  // acuest (vmc/acuest.f90:61) per walker then acuest_reduce's sum over ranks
+  Walkers *ws = (Walkers *)wsp;
+  double es = 0, wsm = 0;
+  for (Walker &w : ws->w) {
+    double enow = w.esum / w.wsum;
+    ws->wcum += w.wsum;
+    ws->ecum += w.esum;
+    ws->ecm2 += w.esum * enow;
+    double penow = w.pesum / w.wsum, tpbnow = w.tpbsum / w.wsum;
+    ws->pecm2 += w.pesum * penow;
+    ws->tpbcm2 += w.tpbsum * tpbnow;
+    ws->pecum += w.pesum;
+    ws->tpbcum += w.tpbsum;
+    ws->acc += w.acc;
+    ws->ecum1 += w.ecum1; ws->ecm21 += w.ecm21; ws->ecum1s += w.ecum1s; ws->ecm21s += w.ecm21s;
+    es += w.esum;
+    wsm += w.wsum;
+    w.esum = w.wsum = w.pesum = w.tpbsum = 0;
+    w.acc = 0;
+    w.ecum1 = w.ecm21 = w.ecum1s = w.ecm21s = 0;
+  }
+  ws->iblk += (long)ws->w.size();
+  if (block_energy) *block_energy = es / wsm;
+}
+
+void or_results(void *wsp, double *out) {
+  // finwrt (vmc/finwrt.f90:75-187) with the reduced (all-rank) sums
+  Walkers *ws = (Walkers *)wsp;
+  int W = (int)ws->w.size();
+  double passes = (double)ws->passes * W;  // passes summed over ranks (finwrt uses nproc*passes)
+  double efin = ws->ecum / ws->wcum;
+  auto err = [&](double x, double x2) {
+    return std::sqrt(std::fabs(x2 / ws->wcum - (x / ws->wcum) * (x / ws->wcum)) / (double)ws->iblk);
+  };
+  auto err1 = [&](double x, double x2) {
+    return std::sqrt(std::fabs(x2 / ws->wcum - (x / ws->wcum) * (x / ws->wcum)) / passes);
+  };
+  double eerr = err(ws->ecum, ws->ecm2);
+  double eerr1s = err1(ws->ecum1s, ws->ecm21s);
+  double rtpass = std::sqrt(passes);
+  double tcsq = eerr1s == 0 ? 0 : eerr / eerr1s;
+  out[0] = efin;
+  out[1] = eerr;
+  out[2] = eerr1s * rtpass;
+  out[3] = tcsq * tcsq;
+  out[4] = ws->acc / (passes * ws->s->N);
+  out[5] = ws->pecum / ws->wcum;
+  out[6] = ws->tpbcum / ws->wcum;
+  out[7] = (double)ws->iblk;
+}
+
+void or_get_walkers(void *wsp, double *x, uint64_t *rng) {
+  Walkers *ws = (Walkers *)wsp;
+  int N = ws->s->N;
+  for (size_t k = 0; k < ws->w.size(); k++) {
+    if (x) std::memcpy(x + 3 * N * k, ws->w[k].xold.data(), sizeof(double) * 3 * N);
+    if (rng) std::memcpy(rng + 4 * k, ws->w[k].rng.s, 32);
+  }
+}
+
+void or_get_sums(void *wsp, double *out) {
+  Walkers *ws = (Walkers *)wsp;
+  for (size_t k = 0; k < ws->w.size(); k++) {
+    const Walker &w = ws->w[k];
+    out[5 * k + 0] = w.wsum;
+    out[5 * k + 1] = w.esum;
+    out[5 * k + 2] = w.pesum;
+    out[5 * k + 3] = w.tpbsum;
+    out[5 * k + 4] = w.acc;
+  }
+}
+
+void or_get_state(void *wsp, double *eold, double *psido, double *psijo) {
+  Walkers *ws = (Walkers *)wsp;
+  for (size_t k = 0; k < ws->w.size(); k++) {
+    if (eold) eold[k] = ws->w[k].eold;
+    if (psido) psido[k] = ws->w[k].psido;
+    if (psijo) psijo[k] = ws->w[k].psijo;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and bench.py's
+CPU-baseline leg.  The engine package never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_RNG = os.path.join(HERE, "_ref", "libxoshiro_ref.so")
+
+_dp = C.POINTER(C.c_double)
+_u64 = C.POINTER(C.c_uint64)
+_i32 = C.POINTER(C.c_int32)
+
+
+def build(force: bool = False):
+    if force or not os.path.exists(LIB):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        V = C.c_void_p
+        L.or_sys_create.restype = V
+        L.or_sys_create.argtypes = [C.c_void_p]
+        L.or_sys_destroy.argtypes = [V]
+        L.or_nterms4.argtypes = [C.c_int]
+        L.or_pot_nn.restype = C.c_double
+        L.or_pot_nn.argtypes = [C.c_int, _dp, _dp, _i32]
+        L.or_matinv.argtypes = [_dp, C.c_int, _dp]
+        L.or_rng_states.argtypes = [_i32, C.c_int, _u64]
+        L.or_rng_uniform.argtypes = [_u64, C.c_int, _dp]
+        L.or_gesqua.argtypes = [C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
+        L.or_sites.argtypes = [V, _u64, _dp]
+        L.or_orbitals.argtypes = [V, _dp, _dp, _dp, _dp]
+        L.or_jastrow.argtypes = [V, _dp, _dp, _dp, _dp]
+        L.or_slater.argtypes = [V, _dp, _dp, _dp]
+        L.or_hpsi.argtypes = [V, _dp, _dp, _dp, _dp, _dp]
+        L.or_walkers_create.restype = V
+        L.or_walkers_create.argtypes = [V, C.c_int, _dp, _u64]
+        L.or_walkers_destroy.argtypes = [V]
+        L.or_vmc_steps.argtypes = [V, C.c_int, C.c_int]
+        L.or_zerest.argtypes = [V]
+        L.or_end_block.argtypes = [V, _dp]
+        L.or_results.argtypes = [V, _dp]
+        L.or_get_walkers.argtypes = [V, _dp, _u64]
+        L.or_get_sums.argtypes = [V, _dp]
+        L.or_get_state.argtypes = [V, _dp, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def dp(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def u64(a):
+    return a.ctypes.data_as(_u64)
+
+
+DEFAULT_SEED = "18123437465549275475255231234865"  # CHAMP default, vmc/parser.f90:315
+
+
+def seed_ints(cseed: str = DEFAULT_SEED):
+    """read(cseed,'(8i4)') irn (vmc/parser.f90:651)."""
+    return np.array([int(cseed[4 * i:4 * i + 4]) for i in range(8)], np.int32)
+
+
+def rng_states(nwalk: int, cseed: str = DEFAULT_SEED):
+    out = np.zeros((nwalk, 4), np.uint64)
+    irn = seed_ints(cseed)
+    lib().or_rng_states(irn.ctypes.data_as(_i32), nwalk, u64(out))
+    return out
+
+
+class OracleSystem:
+    def __init__(self, system):
+        self.system = system
+        self._desc = system.desc()
+        self.h = lib().or_sys_create(C.addressof(self._desc))
+        self.N = system.nelec
+
+    def __del__(self):
+        try:
+            lib().or_sys_destroy(self.h)
+        except Exception:
+            pass
+
+    def orbitals(self, x):
+        s = self.system
+        orb = np.zeros((s.norb, s.nelec))
+        dorb = np.zeros((3, s.nelec, s.norb))
+        ddorb = np.zeros((s.nelec, s.norb))
+        lib().or_orbitals(self.h, dp(np.ascontiguousarray(x, float)), dp(orb), dp(dorb), dp(ddorb))
+        return orb, dorb, ddorb
+
+    def jastrow(self, x):
+        psij = np.zeros(1)
+        v = np.zeros((self.N, 3))
+        d2 = np.zeros(1)
+        lib().or_jastrow(self.h, dp(np.ascontiguousarray(x, float)), dp(psij), dp(v), dp(d2))
+        return psij[0], v, d2[0]
+
+    def slater(self, x):
+        s = self.system
+        nmax = max(s.nup, s.ndn)
+        slmi = np.zeros((2, nmax * nmax))
+        det = np.zeros(2)
+        rc = lib().or_slater(self.h, dp(np.ascontiguousarray(x, float)), dp(slmi), dp(det))
+        if rc:
+            raise RuntimeError("singular Slater matrix")
+        return slmi, det
+
+    def hpsi(self, x, quad=None):
+        out = np.zeros(6)
+        if quad is None:
+            rc = lib().or_hpsi(self.h, dp(np.ascontiguousarray(x, float)), None, None, None, dp(out))
+        else:
+            xq, yq, zq = (np.ascontiguousarray(q, float) for q in quad)
+            rc = lib().or_hpsi(self.h, dp(np.ascontiguousarray(x, float)), dp(xq), dp(yq), dp(zq), dp(out))
+        if rc:
+            raise RuntimeError("singular Slater matrix")
+        return dict(energy=out[0], psid=out[1], psij=out[2], ekin=out[3], pe_local=out[4], vpsp=out[5])
+
+    def sites(self, state):
+        x = np.zeros((self.N, 3))
+        st = np.ascontiguousarray(state, np.uint64).copy()
+        lib().or_sites(self.h, u64(st), dp(x))
+        return x, st
+
+
+class OracleWalkers:
+    def __init__(self, osys: OracleSystem, x, rng):
+        self.osys = osys
+        x = np.ascontiguousarray(x, float)
+        rng = np.ascontiguousarray(rng, np.uint64)
+        self.W = rng.shape[0]
+        self.h = lib().or_walkers_create(osys.h, self.W, dp(x), u64(rng))
+
+    def __del__(self):
+        try:
+            lib().or_walkers_destroy(self.h)
+        except Exception:
+            pass
+
+    def steps(self, nstep, nthreads=1):
+        rc = lib().or_vmc_steps(self.h, nstep, nthreads)
+        if rc:
+            raise RuntimeError("oracle walker failed (singular matrix)")
+
+    def zerest(self):
+        lib().or_zerest(self.h)
+
+    def end_block(self):
+        e = np.zeros(1)
+        lib().or_end_block(self.h, dp(e))
+        return e[0]
+
+    def results(self):
+        out = np.zeros(8)
+        lib().or_results(self.h, dp(out))
+        return dict(energy=out[0], err=out[1], sigma=out[2], tcorr=out[3], accept=out[4], pe=out[5],
+                    ke=out[6], nblocks=out[7])
+
+    def walkers(self):
+        x = np.zeros((self.W, self.osys.N, 3))
+        r = np.zeros((self.W, 4), np.uint64)
+        lib().or_get_walkers(self.h, dp(x), u64(r))
+        return x, r
+
+    def sums(self):
+        out = np.zeros((self.W, 5))
+        lib().or_get_sums(self.h, dp(out))
+        return out
+
+    def state(self):
+        e = np.zeros(self.W)
+        p = np.zeros(self.W)
+        j = np.zeros(self.W)
+        lib().or_get_state(self.h, dp(e), dp(p), dp(j))
+        return e, p, j
