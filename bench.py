@@ -1,0 +1,320 @@
+"""Throughput benchmark of the B200 walker engine (VMC, electron-moves/s).
+
+A step is one metrop6 sweep (vmc/metrop_mov1_slat.f90:3): every electron of
+every walker offered one accelerated-Metropolis move, then the full local
+energy (hpsi) and the weighted sums.  Default workload: the 120-electron,
+30-centre, 540-Gaussian synthetic molecule with 8192 walkers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times CHAMP's own CPU algorithm for the same workload.  The
+CHAMP Fortran build needs gfortran/MPI, absent on this image, so the timed CPU
+implementation is the FP64 C++ restatement in oracle/ (kind "port") run with
+one walker per host thread, as CHAMP runs one walker per MPI rank.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: (synthetic config, walkers, description)
+    "c1": ("c1", 8192, "vmc-c1: 30 centres (15 C-like Z=4 with BFD-form ECP, 15 H-like), 120 electrons "
+                       "(60/60), 540 Gaussians, 60 orbitals, order-5 Jastrow, 8192 walkers"),
+    "c0": ("c0", 1024, "vmc-c0: 3 centres (Z 6/1/1, ECP on the heavy atom), 8 electrons (4/4), 60 Gaussians, "
+                       "4 orbitals, order-5 Jastrow, 1024 walkers"),
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def algorithmic(system, W):
+    """Work per launch of the move-stage kernels (FP64 reference algorithm)."""
+    N, M, K, O = system.nelec, system.ncent, system.nbasis, system.norb
+    T = system.c.shape[1] if system.c.ndim == 2 else 0
+    ns = max(system.nup, system.ndn)
+    f_jastrow_move = 8 * (N - 1) * M * T + 8 * (N - 1) * system.nordb + 8 * M * system.norda
+    f_move = 2 * 4 * K * O + 30 * K + 2 * ns + 2 * ns * ns + f_jastrow_move + 6 * ns
+    b_move = 8 * (2 * ns * ns + 6 * N + 8 * (N - 1) + 4 * O)
+    f_jastrow_full = 9 * N * (N - 1) * M * T
+    return dict(f_jastrow_move=W * f_jastrow_move, f_move=W * f_move, b_move=W * b_move,
+                f_jastrow_full=W * f_jastrow_full)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in (self.out or "").splitlines():
+            p = [v.strip() for v in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                smax.append(float(p[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(ngpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=None)
+        pg = dist
+    return rank, world, local, pg
+
+
+def max_over_ranks(v, pg, local):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    import torch
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize(local)
+
+
+def cpu_port_rate(system, walkers_cpu, nthreads, min_seconds=10.0, max_steps=4, seed_offset=0):
+    """Oracle (FP64 C++ restatement of CHAMP) on host threads: electron-moves/s."""
+    from oracle import oracle
+    oracle.build()
+    o = oracle.OracleSystem(system)
+    rng = oracle.rng_states(walkers_cpu + seed_offset)[seed_offset:].copy()
+    xs = []
+    for w in range(walkers_cpu):
+        x, rng[w] = o.sites(rng[w])
+        xs.append(x)
+    ow = oracle.OracleWalkers(o, np.array(xs), rng)
+    ow.steps(1, nthreads)  # warm-up sweep
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps:
+        ow.steps(1, nthreads)
+        steps += 1
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return walkers_cpu * system.nelec * steps / dt, steps, dt
+
+
+def run_reference(args):
+    rank, world, local, pg = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    from champ_b200.system import make_synthetic
+    cfg, W, desc = CONFIGS[args.config]
+    system = make_synthetic(cfg)
+    nthreads = os.cpu_count() or 1
+    rates = []
+    for _ in range(max(1, args.steps)):
+        rate, steps, dt = cpu_port_rate(system, nthreads, nthreads, min_seconds=5.0, max_steps=2)
+        rates.append(rate)
+    v = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": "electron-moves/s", "value": v, "unit": "electron-moves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "walkers": W, "walkers_cpu": nthreads, "precision": "fp64"},
+        "cpu_baseline": {"value": v, "unit": "electron-moves/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{nthreads} walkers (one per host thread, as one per CHAMP MPI rank), "
+                                   f"1-2 metrop6 sweeps per sample after one warm-up sweep"},
+        "e2e": {"value": v, "unit": "electron-moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.system import make_synthetic
+    cfg, W, desc = CONFIGS[args.config]
+    if args.walkers:
+        W = args.walkers
+    system = make_synthetic(cfg)
+    # replica r runs its own walkers: streams r*W .. r*W+W-1 of the default seed
+    rng_all = rng_states(W * (rank + 1))
+    rng = rng_all[rank * W:].copy()
+    x = initial_configs(system, rng)
+    eng = Engine(system, device=local, precision=args.precision)
+    eng.set_walkers(x, rng)
+    for _ in range(args.warmup):
+        eng.vmc_steps(1)
+    # --- timed region: K steps, walkers resident in HBM -------------------
+    with ClockSampler(local) as clk:
+        barrier(pg, local)
+        eng.vmc_steps(args.steps)
+        barrier(pg, local)
+    ms_dev = eng.last_ms()
+    launches = eng.launches()
+    ms_max = max_over_ranks(ms_dev, pg, local)
+    moves = W * system.nelec * args.steps * world
+    value = moves / (ms_max * 1e-3)
+    # --- per-stage timing pass (CUDA events around every launch) ----------
+    eng.profile(True)
+    eng.vmc_steps(1)
+    stages = eng.stage_times()
+    eng.profile(False)
+    # --- e2e: the C-ABI calls of a caller that keeps walkers in host memory
+    x_h = torch.empty((W, system.nelec, 3), dtype=torch.float64, pin_memory=True).numpy()
+    r_h = torch.empty((W, 4), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    xx, rr = eng.walkers()
+    x_h[...] = xx
+    r_h[...] = rr
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.set_walkers(x_h, r_h)          # H2D: positions + streams (zerest recompute)
+        eng.vmc_steps(1)
+        xx, rr = eng.walkers()             # D2H: positions + streams
+        x_h[...] = xx
+        r_h[...] = rr
+        eng.end_block()                    # D2H: per-walker sums
+    barrier(pg, local)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, pg, local)
+    e2e = W * system.nelec * e2e_steps * world / e2e_s
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
+    peaks, peak_kind = load_peaks()
+    fp64_peak = None
+    try:
+        import ctypes as C
+        from champ_b200.abi import load_engine
+        t = np.zeros(1)
+        if load_engine().cw_fma_peak(local, 1, t.ctypes.data_as(C.POINTER(C.c_double))) == 0:
+            fp64_peak = float(t[0])
+    except Exception:
+        fp64_peak = None
+    alg = algorithmic(system, W)
+    ms_jm, n_jm = stages["jastrow_move"]
+    ms_acc, n_acc = stages["accept"]
+    total_stage = sum(v[0] for v in stages.values())
+    top = max(stages.items(), key=lambda kv: kv[1][0])
+    jm_tflops = alg["f_jastrow_move"] / (ms_jm / n_jm * 1e-3) / 1e12
+    roof = {"kernel": "k_jastrow_move (jastrow4e, one electron, all walkers)", "bound": "fp64-simt",
+            "achieved": jm_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": (jm_tflops / fp64_peak) if fp64_peak else None,
+            "peak_source": "measured FP64 FMA probe (cw_fma_peak) on this GPU",
+            "traffic": None, "share_of_step": ms_jm / total_stage,
+            "work_per_launch": "8*(N-1)*M*T + 8*(N-1)*nordb + 8*M*norda FLOP per walker (T=23 e-e-n terms)"}
+    acc_gbs = alg["b_move"] / (ms_acc / n_acc * 1e-3) / 1e9
+    roof_hbm = {"kernel": "k_accept (ratio, accept, Sherman-Morrison commit)", "bound": "hbm",
+                "achieved": acc_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                "frac": acc_gbs / peaks.get("hbm_gbs"), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                "work_per_launch": "8*(2 n^2 + 6N + 8(N-1) + 4 O) bytes per walker-move"}
+    cpu_rate, cpu_steps, cpu_dt = cpu_port_rate(system, os.cpu_count() or 1, os.cpu_count() or 1,
+                                                min_seconds=10.0, max_steps=3)
+    h2d = W * system.nelec * 3 * 8 + W * 32
+    d2h = h2d + W * 8 * 8
+    line = {
+        "metric": "electron-moves/s", "value": value, "unit": "electron-moves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "mixed",
+        "data": "synthetic",
+        "config": {"workload": desc, "walkers": W, "electrons": system.nelec, "basis": system.nbasis,
+                   "orbitals": system.norb, "centres": system.ncent, "precision": args.precision,
+                   "l2": "per-walker state (3.8 GB of Jastrow pair tables alone) exceeds the 126 MB L2",
+                   "parallelism": f"replicas x{world} (independent walker populations, no data-path collective)"},
+        "e2e": {"value": e2e, "unit": "electron-moves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "cw_set_walkers (pinned host x, rng) + cw_vmc_steps(1) + cw_get_walkers + cw_end_block"},
+        "roofline": roof, "roofline_hbm": roof_hbm,
+        "top_stage": {"name": top[0], "ms": top[1][0], "launches": top[1][1]},
+        "stages_ms_per_step": {k: round(v[0], 3) for k, v in stages.items()},
+        "cpu_baseline": {"value": cpu_rate, "unit": "electron-moves/s", "cores": os.cpu_count() or 1, "kind": "port",
+                         "sample": f"{os.cpu_count()} walkers x {cpu_steps} sweeps ({cpu_dt:.1f} s), "
+                                   "oracle C++ FP64 restatement, one walker per host thread"},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
+    ap.add_argument("--walkers", type=int, default=0)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

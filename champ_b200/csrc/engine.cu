@@ -15,6 +15,7 @@
 #include "gemm.cuh"
 #include "hpsi.cuh"
 #include "move.cuh"
+#include "peak.cuh"
 
 
 using namespace cw;
@@ -39,6 +40,14 @@ struct cw_ctx {
   double ecum1s = 0, ecm21s = 0;
   long iblk = 0, passes = 0;
   double last_ms = 0;
+  // launch accounting and optional per-stage event timing
+  long launches = 0;
+  bool prof = false;
+  std::vector<cudaEvent_t> evpool;
+  std::vector<int> evstage;      // stage of event pair k
+  size_t evused = 0;
+  double stage_ms[CW_NSTAGE] = {0};
+  long stage_n[CW_NSTAGE] = {0};
 };
 
 namespace {
@@ -94,6 +103,39 @@ int dalloc(cw_ctx *c, std::vector<void *> &list, T **p, size_t n) {
 void free_list(std::vector<void *> &l) {
   for (void *p : l) cudaFree(p);
   l.clear();
+}
+
+// Bracket a launch with CUDA events when profiling; count it either way.
+void stage_begin(cw_ctx *c, int stage) {
+  c->launches++;
+  if (!c->prof) return;
+  const size_t k = c->evused;
+  if (2 * k + 2 > c->evpool.size()) {
+    for (int i = 0; i < 256; i++) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      c->evpool.push_back(e);
+    }
+    c->evstage.resize(c->evpool.size() / 2);
+  }
+  c->evstage[k] = stage;
+  cudaEventRecord(c->evpool[2 * k], c->stream);
+}
+void stage_end(cw_ctx *c) {
+  if (!c->prof) return;
+  cudaEventRecord(c->evpool[2 * c->evused + 1], c->stream);
+  c->evused++;
+}
+void stage_collect(cw_ctx *c) {
+  if (!c->prof) return;
+  cudaStreamSynchronize(c->stream);
+  for (size_t k = 0; k < c->evused; k++) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->evpool[2 * k], c->evpool[2 * k + 1]);
+    c->stage_ms[c->evstage[k]] += ms;
+    c->stage_n[c->evstage[k]]++;
+  }
+  c->evused = 0;
 }
 
 int launch_check(cw_ctx *c, const char *what) {
@@ -158,31 +200,47 @@ int nord_attrs(cw_ctx *c) {
 int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullptr) {
   const CSys &h = c->h;
   const int W = c->W, N = h.N, M = h.M;
+  stage_begin(c, CW_ST_JASTROW_FULL);
   NORD_DISPATCH(launch_jfull, c);
+  stage_end(c);
   LCHK("k_jastrow_full");
   // orbitals in electron chunks
   const int ec = c->hb.chunk;
   for (int e0 = 0; e0 < N; e0 += ec) {
     const int ne = std::min(ec, N - e0);
     const long nt = (long)W * ne * M;
+    stage_begin(c, CW_ST_BASIS_ALL);
     k_basis_all<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    stage_end(c);
     LCHK("k_basis_all");
+    stage_begin(c, CW_ST_LCAO_ALL);
     dgemm(c->stream, W * ne * 5, h.Oa, h.K, c->hb.phi, c->g.coefT, c->hb.orball);
+    stage_end(c);
     LCHK("dgemm(all)");
     const long ns = (long)W * ne * h.nmax;
+    stage_begin(c, CW_ST_SCATTER);
     k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    stage_end(c);
     LCHK("k_scatter_orbs");
   }
+  stage_begin(c, CW_ST_SLATER_INV);
   k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->st, c->hb);
+  stage_end(c);
   LCHK("k_slater_inv");
   if (h.nloc > 0) {
     const int nchunk = (h.K + 63) / 64;
+    stage_begin(c, CW_ST_CTILDE);
     k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->st, c->hb, c->g);
+    stage_end(c);
     LCHK("k_ctilde");
+    stage_begin(c, CW_ST_ECP);
     NORD_DISPATCH(launch_ecp, c);
+    stage_end(c);
     LCHK("k_ecp");
   }
+  stage_begin(c, CW_ST_ENERGY);
   k_energy<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->hb, mode, d_e, d_ekin);
+  stage_end(c);
   LCHK("k_energy");
   return CW_OK;
 }
@@ -444,6 +502,7 @@ void cw_destroy(cw_ctx *c) {
   free_list(c->sys_allocs);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -457,6 +516,28 @@ int cw_sync(cw_ctx *c) {
 }
 
 double cw_last_ms(const cw_ctx *c) { return c ? c->last_ms : 0.0; }
+
+long cw_launches(const cw_ctx *c) { return c ? c->launches : 0; }
+
+int cw_profile(cw_ctx *c, int enable) {
+  if (!c) return CW_ERR_ARG;
+  c->prof = enable != 0;
+  for (int k = 0; k < CW_NSTAGE; k++) {
+    c->stage_ms[k] = 0;
+    c->stage_n[k] = 0;
+  }
+  c->evused = 0;
+  return CW_OK;
+}
+
+int cw_stage_times(cw_ctx *c, double *ms, long *launches) {
+  if (!c) return CW_ERR_ARG;
+  for (int k = 0; k < CW_NSTAGE; k++) {
+    if (ms) ms[k] = c->stage_ms[k];
+    if (launches) launches[k] = c->stage_n[k];
+  }
+  return CW_OK;
+}
 
 int cw_set_walkers(cw_ctx *c, int nwalk, const double *x, const uint64_t *rng) {
   if (!c || nwalk <= 0 || !x || !rng) return fail(c, CW_ERR_ARG, "cw_set_walkers: bad arguments");
@@ -500,27 +581,41 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
   CK(cudaSetDevice(c->device));
   const CSys &h = c->h;
   const int W = c->W;
+  c->launches = 0;
   CK(cudaEventRecord(c->ev0, c->stream));
   for (int s = 0; s < nstep; s++) {
     if (h.nloc > 0) {
+      stage_begin(c, CW_ST_ROTQUA);
       k_rotqua<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st);
+      stage_end(c);
       LCHK("k_rotqua");
     }
     for (int i = 0; i < h.N; i++) {
+      stage_begin(c, CW_ST_PROPOSE);
       k_propose<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->mb, i);
+      stage_end(c);
       LCHK("k_propose");
+      stage_begin(c, CW_ST_JASTROW_MOVE);
       NORD_DISPATCH(launch_jmove, c, i);
+      stage_end(c);
       LCHK("k_jastrow_move");
       const long nt = (long)W * h.M;
+      stage_begin(c, CW_ST_BASIS_MOVE);
       k_basis_move<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->mb, c->g);
+      stage_end(c);
       LCHK("k_basis_move");
+      stage_begin(c, CW_ST_LCAO_MOVE);
       dgemm(c->stream, W * 4, h.Oa, h.K, c->mb.phi, c->g.coefT, c->mb.orbn);
+      stage_end(c);
       LCHK("dgemm(move)");
+      stage_begin(c, CW_ST_ACCEPT);
       k_accept<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+      stage_end(c);
       LCHK("k_accept");
     }
     int rc = run_hpsi(c, 1);
     if (rc) return rc;
+    if (c->prof && c->evused > 4096) stage_collect(c);
   }
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));
@@ -528,6 +623,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
   c->passes += nstep;
+  stage_collect(c);
   return check_status(c);
 }
 
@@ -683,6 +779,38 @@ int cw_slater(cw_ctx *c, double *slmi, double *det) {
   const int W = c->W, nmax = c->h.nmax;
   if (slmi) CK(cudaMemcpy(slmi, c->st.slmi, sizeof(double) * W * 2 * nmax * nmax, cudaMemcpyDeviceToHost));
   if (det) CK(cudaMemcpy(det, c->st.detiab, sizeof(double) * W * 2, cudaMemcpyDeviceToHost));
+  return CW_OK;
+}
+
+int cw_fma_peak(int device, int fp64, double *tflops) {
+  if (!tflops) return CW_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return CW_ERR_CUDA;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  void *out = nullptr;
+  if (cudaMalloc(&out, 64) != cudaSuccess) return CW_ERR_OOM;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = nsm * 8, threads = 256, iters = fp64 ? 8192 : 32768;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(e0);
+    if (fp64) k_fma_peak<double><<<blocks, threads>>>((double *)out, iters, 0.999999, 1e-7);
+    else k_fma_peak<float><<<blocks, threads>>>((float *)out, iters, 0.999999f, 1e-7f);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (err != cudaSuccess) return CW_ERR_CUDA;
+  const double flops = 2.0 * 8 * (double)iters * blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
   return CW_OK;
 }
 

@@ -109,6 +109,19 @@ class Engine:
     def last_ms(self) -> float:
         return float(self.lib.cw_last_ms(self.h))
 
+    def launches(self) -> int:
+        return int(self.lib.cw_launches(self.h))
+
+    def profile(self, enable: bool = True):
+        self._check(self.lib.cw_profile(self.h, 1 if enable else 0), "cw_profile")
+
+    def stage_times(self) -> dict:
+        from .abi import STAGES
+        ms = np.zeros(len(STAGES))
+        n = (C.c_long * len(STAGES))()
+        self._check(self.lib.cw_stage_times(self.h, dptr(ms), n), "cw_stage_times")
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(STAGES)}
+
     def end_block(self) -> float:
         e = np.zeros(1)
         self._check(self.lib.cw_end_block(self.h, dptr(e)), "cw_end_block")

@@ -185,6 +185,27 @@ int cw_get_state(cw_ctx *ctx, double *eold, double *psido, double *psijo);
  * engine stream). */
 double cw_last_ms(const cw_ctx *ctx);
 
+/* Kernel launches issued by the last cw_vmc_steps call. */
+long cw_launches(const cw_ctx *ctx);
+
+/* Per-stage device timing.  enable=1 brackets every launch of the following
+ * cw_vmc_steps calls with CUDA events on the engine stream (adds event
+ * overhead; leave off for throughput runs).  cw_stage_times fills, for each
+ * of the CW_NSTAGE stages below, the accumulated milliseconds and launch
+ * counts since profiling was enabled. */
+enum {
+  CW_ST_ROTQUA = 0, CW_ST_PROPOSE, CW_ST_JASTROW_MOVE, CW_ST_BASIS_MOVE, CW_ST_LCAO_MOVE,
+  CW_ST_ACCEPT, CW_ST_JASTROW_FULL, CW_ST_BASIS_ALL, CW_ST_LCAO_ALL, CW_ST_SCATTER,
+  CW_ST_SLATER_INV, CW_ST_CTILDE, CW_ST_ECP, CW_ST_ENERGY, CW_NSTAGE
+};
+int cw_profile(cw_ctx *ctx, int enable);
+int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
+
+/* Diagnostics: measured FMA throughput of the CUDA cores of `device`
+ * (fp64=1: FP64, else FP32), TFLOP/s — the roofline denominator of the
+ * CUDA-core bound stages.  No counterpart in CHAMP. */
+int cw_fma_peak(int device, int fp64, double *tflops);
+
 /* ------------------------------------------------------------------------ */
 /* Host-only helpers (no GPU needed)                                        */
 /* ------------------------------------------------------------------------ */
