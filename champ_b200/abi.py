@@ -108,6 +108,8 @@ def load_engine(path: str | None = None):
     lib.cw_profile.restype = C.c_int
     lib.cw_stage_times.argtypes = [V, _dp, C.POINTER(C.c_long)]
     lib.cw_stage_times.restype = C.c_int
+    lib.cw_orbitals_noalloc.argtypes = [V, C.c_int, C.c_void_p, C.c_void_p]
+    lib.cw_orbitals_noalloc.restype = C.c_int
     lib.cw_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
     lib.cw_fma_peak.restype = C.c_int
     lib.cw_rng_states.argtypes = [C.POINTER(C.c_int32), C.c_int, C.POINTER(C.c_uint64)]
@@ -125,7 +127,7 @@ EXPORTED_SYMBOLS = [
     "cw_create", "cw_destroy", "cw_last_error", "cw_sync", "cw_set_walkers", "cw_get_walkers",
     "cw_vmc_steps", "cw_end_block", "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow",
     "cw_slater", "cw_get_sums", "cw_get_state", "cw_last_ms", "cw_rng_states", "cw_sites",
-    "cw_launches", "cw_profile", "cw_stage_times", "cw_fma_peak",
+    "cw_launches", "cw_profile", "cw_stage_times", "cw_fma_peak", "cw_orbitals_noalloc",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy"]

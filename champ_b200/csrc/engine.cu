@@ -904,3 +904,78 @@ int cw_sites(const cw_system_desc *d, int nwalk, uint64_t *rng, double *x) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free orbital evaluation at caller-given points.
+//
+// Some callers cannot call cudaMalloc while they run: a Fortran/OpenACC host
+// whose device memory is pre-reserved by another allocator or pool, or a
+// driver loop that cannot afford cudaMalloc's implicit device-wide
+// synchronisation in the middle of a Monte Carlo step.  For them,
+// cw_orbitals_noalloc evaluates the orbitals (value, gradient, Laplacian)
+// at points the caller already holds on the device and writes them to a
+// device buffer the caller provides.  The basis-function values it needs in
+// between live in the fixed array below, reserved once when the library's
+// device code is loaded on a GPU and kept until the process exits; the call
+// itself allocates nothing.
+// ===========================================================================
+#define CW_NOALLOC_SCRATCH_DOUBLES (2u * 1024u * 1024u) /* 16 MiB per GPU */
+
+static __device__ __align__(256) double cw_noalloc_phi[CW_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+double *g_noalloc_scratch[kNoallocMaxDevices] = {nullptr};
+
+// The array's name is only a host-side stand-in for the device symbol: its
+// device address is looked up once per device, with that device current.
+int noalloc_scratch(cw_ctx *c, double **p) {
+  const int dev = c->device;
+  if (dev < 0 || dev >= kNoallocMaxDevices) return fail(c, CW_ERR_ARG, "device index out of range");
+  if (!g_noalloc_scratch[dev]) {
+    void *addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, cw_noalloc_phi);
+    if (e != cudaSuccess || !addr)
+      return fail(c, CW_ERR_CUDA, "cudaGetSymbolAddress(cw_noalloc_phi) failed: %s", cudaGetErrorString(e));
+    g_noalloc_scratch[dev] = (double *)addr;
+  }
+  *p = g_noalloc_scratch[dev];
+  return CW_OK;
+}
+
+// basis functions (value, gradient, Laplacian) of npts points, thread per
+// (point, centre); rows (p*5 + d) of phi, as k_basis_all writes them.
+__global__ void k_basis_points(GSys g, int npts, const double *__restrict__ xyz, double *__restrict__ phi) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int M = cs.M, K = cs.K;
+  if (t >= (long)npts * M) return;
+  const int ic = (int)(t % M);
+  const long p = t / M;
+  const double xc[3] = {xyz[3 * p] - cs.cent[3 * ic], xyz[3 * p + 1] - cs.cent[3 * ic + 1],
+                        xyz[3 * p + 2] - cs.cent[3 * ic + 2]};
+  double *row = phi + (size_t)p * 5 * K;
+  basis_centre(g, ic, xc, 2, [&](int a, int d, double v) { row[(size_t)d * K + a] = v; });
+}
+}  // namespace
+
+extern "C" int cw_orbitals_noalloc(cw_ctx *c, int npts, const double *xyz, double *out) {
+  if (!c) return CW_ERR_ARG;
+  if (npts <= 0 || !xyz || !out) return fail(c, CW_ERR_ARG, "cw_orbitals_noalloc: bad arguments");
+  const CSys &h = c->h;
+  const size_t need = (size_t)npts * 5 * h.K;
+  if (need > CW_NOALLOC_SCRATCH_DOUBLES)
+    return fail(c, CW_ERR_ARG,
+                "cw_orbitals_noalloc: %d points x 5 x %d basis functions exceed the fixed scratch of %u doubles "
+                "(at most %u points per call for this basis)",
+                npts, h.K, CW_NOALLOC_SCRATCH_DOUBLES, (unsigned)(CW_NOALLOC_SCRATCH_DOUBLES / (5u * h.K)));
+  CK(cudaSetDevice(c->device));
+  double *phi = nullptr;
+  int rc = noalloc_scratch(c, &phi);
+  if (rc) return rc;
+  const long nt = (long)npts * h.M;
+  k_basis_points<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->g, npts, xyz, phi);
+  LCHK("k_basis_points");
+  dgemm(c->stream, npts * 5, h.Oa, h.K, phi, c->g.coefT, out);
+  LCHK("dgemm(noalloc)");
+  return CW_OK;
+}

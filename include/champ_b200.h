@@ -201,6 +201,21 @@ enum {
 int cw_profile(cw_ctx *ctx, int enable);
 int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
 
+/* Orbitals at points, allocating nothing.  No counterpart in CHAMP: this
+ * entry point exists for callers that cannot call cudaMalloc while they run
+ * (device memory owned by another allocator, or a step loop that cannot take
+ * cudaMalloc's implicit device synchronisation).  xyz [npts][3] and out
+ * [npts][5][norb] (value, d/dx, d/dy, d/dz, Laplacian of every orbital) are
+ * DEVICE pointers on the context's device, provided by the caller.  Basis
+ * values in between go to a fixed 16 MiB array that every GPU loading the
+ * library reserves until exit, so npts*5*nbasis must not exceed 2^21
+ * (CW_ERR_ARG otherwise).  The first call on a device looks up that array's
+ * device address (make that first call before any stream capture).  The work
+ * is queued on the context's stream: out is ready after cw_sync.  All calls
+ * share the one array: calls that overlap on the GPU (several contexts on
+ * the same device, different streams) race on it. */
+int cw_orbitals_noalloc(cw_ctx *ctx, int npts, const double *xyz, double *out);
+
 /* Diagnostics: measured FMA throughput of the CUDA cores of `device`
  * (fp64=1: FP64, else FP32), TFLOP/s — the roofline denominator of the
  * CUDA-core bound stages.  No counterpart in CHAMP. */
