@@ -130,4 +130,4 @@ EXPORTED_SYMBOLS = [
     "cw_launches", "cw_profile", "cw_stage_times", "cw_fma_peak", "cw_orbitals_noalloc",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
-          "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy"]
+          "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit"]

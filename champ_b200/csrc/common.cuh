@@ -94,7 +94,8 @@ struct MoveScratch {
   double rminn, rminon, rminno, delttn, fxop, areao, rratio;
   int nearestn, igeo;
   double rvminon[3];
-  double pad;
+  double ratio;       // determinant ratio of the proposed move (k_decide)
+  int acc, pad;       // accepted? (k_decide)
 };
 
 struct MoveBuf {
@@ -240,6 +241,230 @@ __device__ __forceinline__ EenOut<T> een_poly(const T *__restrict__ cc, T u1, T 
               e.fuj += c * T(k) * ukm * gj;
             }
           }
+        }
+      }
+    }
+  }
+  return e;
+}
+
+
+// ---------------------------------------------------------------------------
+// Folded e-e-n polynomial.  With x, y, z the switched scaled distances of
+// electron i and j to one centre and of the pair, every e-e-n term is
+//   c * z^k * (x^(l+m) y^m + x^m y^(l+m)),
+// so for a fixed x the polynomial is  sum_k z^k sum_p B[k][p](x) y^p  with
+//   B[k][m]   += c x^(l+m),   B[k][l+m] += c x^m.
+// Only (k,p) with 1 <= p <= NORD-1 (k = 0) or 0 <= p <= NORD-k (k >= 1) can
+// be non-zero; they are stored packed (18 of 30 entries at order 5).
+// een_fold builds B and dB/dx once per (moved electron, centre); een_apply*
+// then cost O(nB) per partner instead of O(nterms * NORD).  Same polynomial
+// as jastrow4e / psinl, summed in a different order.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int een_pmin(int k) { return k == 0 ? 1 : 0; }
+__host__ __device__ constexpr int een_pmax(int nord, int k) { return k == 0 ? nord - 1 : nord - k; }
+__host__ __device__ constexpr int een_off(int nord, int k) {
+  int o = 0;
+  for (int kk = 0; kk < k; kk++) o += een_pmax(nord, kk) - een_pmin(kk) + 1;
+  return o;
+}
+__host__ __device__ constexpr int een_nb(int nord) { return nord <= 1 ? 1 : een_off(nord, nord); }
+
+// B and dB/dx interleaved: BD[2*t] = B_t, BD[2*t+1] = dB_t (t = packed index)
+template <int NORD, typename T>
+__device__ __forceinline__ void een_fold(const T *__restrict__ cc, T x, T *BD) {
+  T xp[NORD + 1], dxp[NORD + 1];
+  xp[0] = 1;
+  dxp[0] = 0;
+#pragma unroll
+  for (int q = 1; q <= NORD; q++) {
+    xp[q] = xp[q - 1] * x;
+    dxp[q] = T(q) * xp[q - 1];
+  }
+  T B[een_nb(NORD)], dB[een_nb(NORD)];
+#pragma unroll
+  for (int t = 0; t < een_nb(NORD); t++) {
+    B[t] = 0;
+    dB[t] = 0;
+  }
+  int ll = 0;
+#pragma unroll
+  for (int n = 2; n <= NORD; n++) {
+#pragma unroll
+    for (int k = n - 1; k >= 0; k--) {
+      const int l_hi = (k == 0) ? n - k - 2 : n - k;
+#pragma unroll
+      for (int l = l_hi; l >= 0; l--) {
+        const int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) {
+          const T c = cc[ll];
+          ll++;
+          const int t1 = een_off(NORD, k) + m - een_pmin(k);
+          const int t2 = een_off(NORD, k) + l + m - een_pmin(k);
+          B[t1] += c * xp[l + m];
+          B[t2] += c * xp[m];
+          dB[t1] += c * dxp[l + m];
+          dB[t2] += c * dxp[m];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < een_nb(NORD); t++) {
+    BD[2 * t] = B[t];
+    BD[2 * t + 1] = dB[t];
+  }
+}
+
+// value and first derivatives (d/dz, d/dx, d/dy) of the folded polynomial;
+// BD in shared memory, 16-byte aligned (one vector load per (B, dB) pair)
+template <int NORD>
+__device__ __forceinline__ void een_apply1(const double *__restrict__ BD, double y, double z, double &fc,
+                                           double &fu, double &fi, double &fj) {
+  double yp[NORD + 1], dyp[NORD + 1];
+  yp[0] = 1;
+  dyp[0] = 0;
+#pragma unroll
+  for (int p = 1; p <= NORD; p++) {
+    yp[p] = yp[p - 1] * y;
+    dyp[p] = double(p) * yp[p - 1];
+  }
+  const double2 *bd = reinterpret_cast<const double2 *>(BD);
+  fc = 0; fu = 0; fi = 0; fj = 0;
+  double zk = 1, zkm = 0;  // z^k, k z^(k-1)
+#pragma unroll
+  for (int k = 0; k < NORD; k++) {
+    double a = 0, ax = 0, ay = 0;
+#pragma unroll
+    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
+      const double2 v = bd[een_off(NORD, k) + p - een_pmin(k)];
+      a += v.x * yp[p];
+      ax += v.y * yp[p];
+      ay += v.x * dyp[p];
+    }
+    fc += zk * a;
+    fu += zkm * a;
+    fi += zk * ax;
+    fj += zk * ay;
+    zkm = double(k + 1) * zk;
+    zk *= z;
+  }
+}
+
+// value-only fold, packed B (padded to an even count for vector loads)
+template <int NORD, typename T>
+__device__ __forceinline__ void een_fold0(const T *__restrict__ cc, T x, T *Bout) {
+  T xp[NORD + 1];
+  xp[0] = 1;
+#pragma unroll
+  for (int q = 1; q <= NORD; q++) xp[q] = xp[q - 1] * x;
+  T B[een_nb(NORD) + 1];
+#pragma unroll
+  for (int t = 0; t <= een_nb(NORD); t++) B[t] = 0;
+  int ll = 0;
+#pragma unroll
+  for (int n = 2; n <= NORD; n++) {
+#pragma unroll
+    for (int k = n - 1; k >= 0; k--) {
+      const int l_hi = (k == 0) ? n - k - 2 : n - k;
+#pragma unroll
+      for (int l = l_hi; l >= 0; l--) {
+        const int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) {
+          const T c = cc[ll];
+          ll++;
+          B[een_off(NORD, k) + m - een_pmin(k)] += c * xp[l + m];
+          B[een_off(NORD, k) + l + m - een_pmin(k)] += c * xp[m];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 2 * ((een_nb(NORD) + 1) / 2); t++) Bout[t] = B[t];
+}
+
+template <int NORD>
+__device__ __forceinline__ double een_apply0(const double *__restrict__ Bp, double y, double z) {
+  constexpr int NB2 = (een_nb(NORD) + 1) / 2;
+  double Bv[2 * NB2];
+  const double2 *b2 = reinterpret_cast<const double2 *>(Bp);
+#pragma unroll
+  for (int t = 0; t < NB2; t++) {
+    const double2 v = b2[t];
+    Bv[2 * t] = v.x;
+    Bv[2 * t + 1] = v.y;
+  }
+  double yp[NORD + 1];
+  yp[0] = 1;
+#pragma unroll
+  for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
+  double fc = 0, zk = 1;
+#pragma unroll
+  for (int k = 0; k < NORD; k++) {
+    double a = 0;
+#pragma unroll
+    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) a += Bv[een_off(NORD, k) + p - een_pmin(k)] * yp[p];
+    fc += zk * a;
+    zk *= z;
+  }
+  return fc;
+}
+
+// e-e-n term of one pair and centre with first and second derivatives (the
+// full-Jastrow case of jastrow4.f90): per term only P = x^(l+m) y^m +
+// x^m y^(l+m) and its x/y derivatives, scaled by the z factors of its k.
+template <int NORD, typename T>
+__device__ __forceinline__ EenOut<T> een_pair2(const T *__restrict__ cc, T z, T x, T y) {
+  // only the power tables of x, y and z stay live; derivative factors are
+  // compile-time constants of each unrolled term
+  T xp[NORD + 1], yp[NORD + 1], zk[NORD];
+  xp[0] = 1; yp[0] = 1; zk[0] = 1;
+#pragma unroll
+  for (int q = 1; q <= NORD; q++) {
+    xp[q] = xp[q - 1] * x;
+    yp[q] = yp[q - 1] * y;
+  }
+#pragma unroll
+  for (int k = 1; k < NORD; k++) zk[k] = zk[k - 1] * z;
+  EenOut<T> e{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int ll = 0;
+#pragma unroll
+  for (int n = 2; n <= NORD; n++) {
+#pragma unroll
+    for (int k = n - 1; k >= 0; k--) {
+      const int l_hi = (k == 0) ? n - k - 2 : n - k;
+#pragma unroll
+      for (int l = l_hi; l >= 0; l--) {
+        const int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) {
+          const T c = cc[ll];
+          ll++;
+          const int a = l + m, b = m;
+          const T xa1 = a >= 1 ? T(a) * xp[a >= 1 ? a - 1 : 0] : T(0);
+          const T xb1 = b >= 1 ? T(b) * xp[b >= 1 ? b - 1 : 0] : T(0);
+          const T ya1 = a >= 1 ? T(a) * yp[a >= 1 ? a - 1 : 0] : T(0);
+          const T yb1 = b >= 1 ? T(b) * yp[b >= 1 ? b - 1 : 0] : T(0);
+          const T xa2 = a >= 2 ? T(a * (a - 1)) * xp[a >= 2 ? a - 2 : 0] : T(0);
+          const T xb2 = b >= 2 ? T(b * (b - 1)) * xp[b >= 2 ? b - 2 : 0] : T(0);
+          const T ya2 = a >= 2 ? T(a * (a - 1)) * yp[a >= 2 ? a - 2 : 0] : T(0);
+          const T yb2 = b >= 2 ? T(b * (b - 1)) * yp[b >= 2 ? b - 2 : 0] : T(0);
+          const T P = xp[a] * yp[b] + xp[b] * yp[a];
+          const T Px = xa1 * yp[b] + xb1 * yp[a];
+          const T Py = xp[a] * yb1 + xp[b] * ya1;
+          const T Pxx = xa2 * yp[b] + xb2 * yp[a];
+          const T Pyy = xp[a] * yb2 + xp[b] * ya2;
+          const T cz = c * zk[k];
+          const T cdz = k >= 1 ? c * T(k) * zk[k >= 1 ? k - 1 : 0] : T(0);
+          const T cd2z = k >= 2 ? c * T(k * (k - 1)) * zk[k >= 2 ? k - 2 : 0] : T(0);
+          e.fc += cz * P;
+          e.fu += cdz * P;
+          e.fuu += cd2z * P;
+          e.fi += cz * Px;
+          e.fii += cz * Pxx;
+          e.fui += cdz * Px;
+          e.fj += cz * Py;
+          e.fjj += cz * Pyy;
+          e.fuj += cdz * Py;
         }
       }
     }
@@ -436,38 +661,42 @@ __device__ __forceinline__ void slm_eval(int l, double x, double y, double z, do
 // (d=1..3, ider>=1) and Laplacian (d=4, ider>=2).
 template <typename Store>
 __device__ __forceinline__ void basis_centre(const GSys &g, int ic, const double *xc, int ider, Store out) {
+  // Radial functions are evaluated one at a time and combined at once with
+  // every AO that uses them (iwrwf), so no per-thread array of spline values
+  // is needed (it would live in local memory).
   const int it = cs.iwctype[ic];
   const double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
   const double ri = 1.0 / r;
-  double wfv[CW_MAX_RWF][4];
   const int nrb = cs.nrbas[it];
-  for (int irb = 0; irb < nrb; irb++) {
-    if (r <= cs.rmaxwf[it * CW_MAX_RWF + irb]) {
-      splfit_d(g, r, irb, it, wfv[irb], ider);
-    } else {
-      wfv[irb][0] = wfv[irb][1] = wfv[irb][2] = wfv[irb][3] = 0.0;
-    }
-  }
   const int nbt = cs.nbastyp[it];
   const int m0 = cs.ao_first[ic];
   const double xcri[3] = {xc[0] * ri, xc[1] * ri, xc[2] * ri};
-  for (int ib = 0; ib < nbt; ib++) {
-    const int l = __ldg(g.iwlbas + it * cs.mbastyp + ib);
-    const int irb = __ldg(g.iwrwf + it * cs.mbastyp + ib) - 1;
-    double y, dy[3], lap;
-    slm_eval(l, xc[0], xc[1], xc[2], y, dy, lap);
-    const double *w = wfv[irb];
-    out(m0 + ib, 0, y * w[0]);
-    if (ider >= 1) {
-      double dum = 0;
-      for (int jj = 0; jj < 3; jj++) {
-        out(m0 + ib, 1 + jj, y * xcri[jj] * w[1] + dy[jj] * w[0]);
-        dum += dy[jj] * xcri[jj];
-      }
-      if (ider >= 2) {
-        double d2 = y * w[2] + y * 2.0 * ri * w[1] + lap * w[0];
-        d2 += 2.0 * dum * w[1];
-        out(m0 + ib, 4, d2);
+  const int *iwl = g.iwlbas + it * cs.mbastyp;
+  const int *iwr = g.iwrwf + it * cs.mbastyp;
+  for (int irb = 0; irb < nrb; irb++) {
+    double w[4];
+    if (r <= cs.rmaxwf[it * CW_MAX_RWF + irb]) {
+      splfit_d(g, r, irb, it, w, ider);
+    } else {
+      w[0] = w[1] = w[2] = w[3] = 0.0;
+    }
+    for (int ib = 0; ib < nbt; ib++) {
+      if (__ldg(iwr + ib) - 1 != irb) continue;
+      const int l = __ldg(iwl + ib);
+      double y, dy[3], lap;
+      slm_eval(l, xc[0], xc[1], xc[2], y, dy, lap);
+      out(m0 + ib, 0, y * w[0]);
+      if (ider >= 1) {
+        double dum = 0;
+        for (int jj = 0; jj < 3; jj++) {
+          out(m0 + ib, 1 + jj, y * xcri[jj] * w[1] + dy[jj] * w[0]);
+          dum += dy[jj] * xcri[jj];
+        }
+        if (ider >= 2) {
+          double d2 = y * w[2] + y * 2.0 * ri * w[1] + lap * w[0];
+          d2 += 2.0 * dum * w[1];
+          out(m0 + ib, 4, d2);
+        }
       }
     }
   }

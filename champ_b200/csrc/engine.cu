@@ -482,11 +482,18 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(cudaMemcpy(slot, so.data(), so.size() * sizeof(int), cudaMemcpyHostToDevice));
   c->g.rwf = rwf; c->g.d2rwf = d2rwf; c->g.iwlbas = iwl; c->g.iwrwf = iwr; c->g.coefT = coefT; c->g.slot_orb = slot;
   // dynamic shared memory sizes
-  c->smem_jmove = sizeof(double) * 4 * 6 * (size_t)h.M;
+  {
+    const int nord = h.nordc <= 1 ? 1 : h.nordc;
+    c->smem_jmove = sizeof(double) * 4 * (size_t)h.M * (6 + 2 * een_nb(nord));
+  }
   c->smem_jfull = sizeof(double) * 3 * (size_t)h.N;
   c->smem_sinv = sizeof(double) * ((size_t)nmax * nmax + nmax);
   c->smem_ctil = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64);
-  c->smem_ecp = sizeof(double) * ((size_t)h.N * h.M + 3 * h.N + 4 * h.M + (size_t)h.nquad * h.K + (size_t)h.nquad * h.M);
+  {
+    const int nord = h.nordc <= 1 ? 1 : h.nordc;
+    c->smem_ecp = sizeof(double) * ((size_t)h.N * h.M + 3 * h.N + 4 * h.M + (size_t)h.nquad * h.K +
+                                    (size_t)h.nquad * h.M + (size_t)h.nquad * h.M * 2 * ((een_nb(nord) + 1) / 2) + 1);
+  }
   CK(cudaFuncSetAttribute(k_slater_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_sinv));
   CK(cudaFuncSetAttribute(k_ctilde, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ctil));
   int rc = nord_attrs(c);
@@ -592,7 +599,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
     }
     for (int i = 0; i < h.N; i++) {
       stage_begin(c, CW_ST_PROPOSE);
-      k_propose<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->mb, i);
+      k_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, i);
       stage_end(c);
       LCHK("k_propose");
       stage_begin(c, CW_ST_JASTROW_MOVE);
@@ -609,9 +616,13 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
       stage_end(c);
       LCHK("dgemm(move)");
       stage_begin(c, CW_ST_ACCEPT);
-      k_accept<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+      k_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, i);
       stage_end(c);
-      LCHK("k_accept");
+      LCHK("k_decide");
+      stage_begin(c, CW_ST_COMMIT);
+      k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+      stage_end(c);
+      LCHK("k_commit");
     }
     int rc = run_hpsi(c, 1);
     if (rc) return rc;

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(256) k_jastrow_full(WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *sx = smem;            // [3][N]
   __shared__ double red[8];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(256) k_jastrow_full(WState st, HBuf hb) {
         scale2<double>(rj, rrj, dd8, dd10);
         if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
         dd7 = -kap * dd7; dd9 = -kap * dd9; dd8 = -kap * dd8; dd10 = -kap * dd10;
-        const EenOut<double> e = een_poly<NORD, 2, double>(&cs.c[it * CW_MAX_TERMS], u1, 1 - kap * rri, 1 - kap * rrj);
+        const EenOut<double> e = een_pair2<NORD, double>(&cs.c[it * CW_MAX_TERMS], u1, 1 - kap * rri, 1 - kap * rrj);
         const double sgs = ri + rj, tgs = ri - rj;
         const double u2pst = rij * rij + sgs * tgs, u2mst = rij * rij - sgs * tgs;
         const double fuu = e.fuu * du1 * du1 + e.fu * du2;
@@ -226,7 +226,7 @@ __global__ void k_slater_inv(WState st, HBuf hb) {
   const int N = cs.N, nmax = cs.nmax;
   const int nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
   const int n = nel;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *A = smem;              // n*n column-major: A(e,j) = orb of slot j at electron e
   double *col = smem + n * n;    // n
   __shared__ int ipvt[256];
@@ -386,7 +386,7 @@ __global__ void k_ctilde(WState st, HBuf hb, GSys g) {
   const int nmax = cs.nmax, K = cs.K, Oa = cs.Oa, N = cs.N;
   const int nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
   if (nel == 0) return;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *S = smem;                 // nel*nel
   double *Co = smem + nel * nel;    // [nel][64]
   const double *slmi = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
@@ -445,12 +445,17 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M, K = cs.K, NQ = cs.nquad;
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;  // warp q <-> quadrature point q
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *rr_en = smem;                 // [N][M] scaled e-n distances
   double *sx = rr_en + N * M;           // [3][N]
   double *vps = sx + 3 * N;             // [M][4] channel potentials of the current electron
   double *phiq = vps + 4 * M;           // [NQ][K]
   double *rrq = phiq + (size_t)NQ * K;  // [NQ][M]
+  constexpr int NB = 2 * ((een_nb(NORD) + 1) / 2);
+  // [NQ][M][NB] folded e-e-n coefficients of the point; 16-byte aligned for
+  // the vector loads of een_apply0 (NB is even)
+  const size_t bq_off = (((size_t)(rrq - smem) + (size_t)NQ * M) + 1) & ~(size_t)1;
+  double *bq = smem + bq_off;
   __shared__ int s_act[CW_MAX_CENT];
   __shared__ int s_nact;
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
@@ -508,6 +513,9 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
         double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
         if (jc == ic) r = rin;  // r_en_quad(iq,ic) = r_en(i,ic)
         rq[jc] = scale0<double>(r);
+        if (NORD > 1)
+          een_fold0<NORD, double>(&cs.c[cs.iwctype[jc] * CW_MAX_TERMS], 1 - cs.scalek * rq[jc],
+                                  bq + ((size_t)q * M + jc) * NB);
         basis_centre(g, jc, xc, 0, [&](int m, int d, double v) { if (d == 0) ph[m] = v; });
       }
       __syncwarp();
@@ -528,8 +536,15 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
         const double rij = sqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
         const double u = scale0<double>(rij);
         double f = psibnl_d(u, isb, ipar, sspinn);
-        if (NORD > 1)
-          for (int jc = 0; jc < M; jc++) f += psinl_d<NORD>(u, rq[jc], rr_en[jj * M + jc], cs.iwctype[jc]);
+        if (NORD > 1) {
+          // psinl (vmc/nonlpsi.f90:4) through the folded coefficients of the point
+          const double z = 1 - cs.scalek * u;
+          for (int jc = 0; jc < M; jc++) {
+            const double rrj = rr_en[jj * M + jc];
+            if (rq[jc] == cs.asymp_r && rrj == cs.asymp_r) continue;
+            f += een_apply0<NORD>(bq + ((size_t)q * M + jc) * NB, 1 - cs.scalek * rrj, z);
+          }
+        }
         fsum += f - fso[(size_t)i * N + jj];
       }
       double fen = 0;

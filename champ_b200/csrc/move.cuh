@@ -1,13 +1,14 @@
 // move.cuh — single-electron accelerated-Metropolis move, batched over walkers.
 //
-// One move of electron `iel` for all walkers is five launches:
+// One move of electron `iel` for all walkers is six launches:
 //   k_propose       metrop6 proposal (vmc/metrop_mov1_slat.f90:131-361)
 //   k_jastrow_move  jastrow4e iflag=0 (vmc/jastrow4e.f90:3)
 //   k_basis_move    basis_fns for the moved electron (vmc/basis_fns.f90:8)
 //   gemm            LCAO contraction (vmc/orbitals_no_qmckl.f90:195)
-//   k_accept        ratio + drift at the new point, reverse transition
-//                   probability, accept/reject, and on accept the commit of
-//                   determinante/detsav (Sherman–Morrison) and jassav.
+//   k_decide        ratio + drift at the new point, reverse transition
+//                   probability, accept/reject (thread per walker)
+//   k_commit        on accept: determinante/detsav (Sherman–Morrison) and
+//                   jassav (CTA per walker)
 #pragma once
 #include "common.cuh"
 
@@ -78,30 +79,29 @@ __device__ __forceinline__ void spin_of(int iel, int &iab, int &nel, int &ish) {
 }
 
 // ---------------------------------------------------------------------------
-// Proposal: warp per walker.  Lanes form the drift at the old position
-// (compute_determinante_grad iflag_move=1: slmi column · dorb + vj), lane 0
-// then samples the move exactly as metrop6 does.
+// Proposal: thread per walker (the sampling is a serial chain of dependent
+// FP64 operations; 32 walkers share a warp instead of one).  The drift at the
+// old position is compute_determinante_grad iflag_move=1: slmi column · dorb
+// + vj.
 // ---------------------------------------------------------------------------
 __global__ void k_propose(WState st, MoveBuf mb, int iel) {
-  const int lane = threadIdx.x & 31;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, nmax = cs.nmax;
   int iab, nel, ish;
   spin_of(iel, iab, nel, ish);
   const int iloc = iel - ish;
   const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * iloc;
+  const double *d0p = st.dorbs + (((size_t)w * 3 + 0) * N + iel) * nmax;
+  const double *d1p = st.dorbs + (((size_t)w * 3 + 1) * N + iel) * nmax;
+  const double *d2p = st.dorbs + (((size_t)w * 3 + 2) * N + iel) * nmax;
   double g0 = 0, g1 = 0, g2 = 0;
-  for (int j = lane; j < nel; j += 32) {
+  for (int j = 0; j < nel; j++) {
     const double s = sl[j];
-    g0 += s * st.dorbs[(((size_t)w * 3 + 0) * N + iel) * nmax + j];
-    g1 += s * st.dorbs[(((size_t)w * 3 + 1) * N + iel) * nmax + j];
-    g2 += s * st.dorbs[(((size_t)w * 3 + 2) * N + iel) * nmax + j];
+    g0 += s * d0p[j];
+    g1 += s * d1p[j];
+    g2 += s * d2p[j];
   }
-  g0 = warp_sum(g0);
-  g1 = warp_sum(g1);
-  g2 = warp_sum(g2);
-  if (lane != 0) return;
 
   const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, d3b2 = 1.5, eps = 1.0e-10;
   const double deltar = cs.deltar, deltri = one / deltar, fbias = cs.fbias;
@@ -250,13 +250,16 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
 // ---------------------------------------------------------------------------
 template <int NORD>
 __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
+  constexpr int NB = een_nb(NORD);        // folded coefficients per centre
+  constexpr int PER = 6 + 2 * NB;         // shared doubles per centre
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int M = cs.M, N = cs.N;
-  double *sh = smem + (size_t)wib * M * 6;  // per centre: rvec(3), r, scaled r, dd1
-  double *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M;
+  double *sh = smem + (size_t)wib * M * PER;
+  // per centre ic: rvec(3), r, scaled r, dd1, then B[NB], dB[NB]
+  double *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M, *sh_B = sh + 6 * M;
   const bool active = (w < st.W);
   int igeo = 1;
   double xi[3] = {0, 0, 0};
@@ -266,6 +269,7 @@ __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
     xi[0] = m.xnew[0]; xi[1] = m.xnew[1]; xi[2] = m.xnew[2];
   }
   if (!active || igeo) return;  // whole warp leaves together (same walker)
+  const double kap = cs.scalek;
   for (int ic = lane; ic < M; ic += 32) {
     double r2 = 0;
     for (int k = 0; k < 3; k++) {
@@ -279,9 +283,9 @@ __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
     scale2<double>(r, rr, dd1, dd2);
     sh_s[ic] = rr;
     sh_d[ic] = dd1;
+    if (NORD > 1) een_fold<NORD, double>(&cs.c[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sh_B + (size_t)ic * 2 * NB);
   }
   __syncwarp();
-  const double kap = cs.scalek;
   const double *xw = st.x + (size_t)w * 3 * N;
   const double *fso_i = st.fso + ((size_t)w * N + iel) * N;
   double dfs = 0, dv0 = 0, dv1 = 0, dv2 = 0;
@@ -308,10 +312,9 @@ __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
       }
     }
     if (NORD > 1) {
-      const double u1 = 1 - kap * u;
+      const double z = 1 - kap * u;
       const double du = -kap * dd1;
       for (int ic = 0; ic < M; ic++) {
-        const int it = cs.iwctype[ic];
         const double rj_v[3] = {xj[0] - cs.cent[3 * ic], xj[1] - cs.cent[3 * ic + 1], xj[2] - cs.cent[3 * ic + 2]};
         const double rj = sqrt(rj_v[0] * rj_v[0] + rj_v[1] * rj_v[1] + rj_v[2] * rj_v[2]);
         double rrj, dd8, dd10;
@@ -320,11 +323,12 @@ __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
         if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
         const double ri = sh_r[ic];
         const double dd7 = sh_d[ic];
-        const EenOut<double> e = een_poly<NORD, 1, double>(&cs.c[it * CW_MAX_TERMS], u1, 1 - kap * rri, 1 - kap * rrj);
-        const double fu = e.fu * du / rij;
-        const double fi = e.fi * (-kap * dd7) / ri;
-        const double fj = e.fj * (-kap * dd8) / rj;
-        fs += e.fc;
+        double fc, fu_, fi_, fj_;
+        een_apply1<NORD>(sh_B + (size_t)ic * 2 * NB, 1 - kap * rrj, z, fc, fu_, fi_, fj_);
+        const double fu = fu_ * du / rij;
+        const double fi = fi_ * (-kap * dd7) / ri;
+        const double fj = fj_ * (-kap * dd8) / rj;
+        fs += fc;
         for (int k = 0; k < 3; k++) {
           gi[k] += fi * sh_rv[k * M + ic] + fu * rvee[k];
           gj[k] += fj * rj_v[k] - fu * rvee[k];
@@ -404,159 +408,160 @@ __global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
 }
 
 // ---------------------------------------------------------------------------
-// Accept / reject and commit: CTA per walker.
+// Accept / reject: thread per walker.  Ratio and drift at the new point
+// (determinante :40-46 + compute_determinante_grad iflag_move=0), the
+// reverse transition probability (metrop6 :435-560) and the accept draw.
+// Scalar state of accepted moves is committed here; k_commit applies the
+// matrix and table updates.
 // ---------------------------------------------------------------------------
-__global__ void k_accept(WState st, MoveBuf mb, GSys g, int iel) {
+__global__ void k_decide(WState st, MoveBuf mb, GSys g, int iel) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
+  int iab, nel, ish;
+  spin_of(iel, iab, nel, ish);
+  const int iloc = iel - ish;
+  MoveScratch &m = mb.ms[w];
+  const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * iloc;
+  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const int *slot = g.slot_orb + iab * nmax;
+  const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, eps = 1.0e-10;
+  DRng rng;
+  rng.load(st.rng + 4 * (size_t)w);
+  double p = zero, psidn = 0, psi2n = 0, ratio = 0;
+  const double fsumn = mb.fsumn[w];
+  if (!m.igeo) {
+    for (int j = 0; j < nel; j++) ratio += sl[j] * orbn[slot[j]];
+    const double detn = st.detiab[2 * w + iab] * ratio;
+    psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
+    if (detn != 0.0) {
+      double v0 = 0, v1 = 0, v2 = 0;
+      for (int j = 0; j < nel; j++) {
+        const double sc = sl[j] / ratio;
+        v0 += sc * orbn[1 * Oa + slot[j]];
+        v1 += sc * orbn[2 * Oa + slot[j]];
+        v2 += sc * orbn[3 * Oa + slot[j]];
+      }
+      const double vn[3] = {0.0 + v0 + mb.vjn[3 * w + 0], 0.0 + v1 + mb.vjn[3 * w + 1],
+                            0.0 + v2 + mb.vjn[3 * w + 2]};
+      psi2n = log(fabs(1.0)) + 2 * (log(fabs(psidn)) + fsumn);
+      const double deltar = cs.deltar, deltri = one / deltar;
+      const double rminn = m.rminn, rminon = m.rminon;
+      const double rbot = rminn * deltri, rtop = rminn * deltar;
+      double vnewr = zero;
+      for (int ic = 0; ic < 3; ic++) vnewr += vn[ic] * m.rvminn[ic];
+      vnewr = vnewr / rminn;
+      double vnewp = zero, xaxis[3];
+      for (int ic = 0; ic < 3; ic++) {
+        xaxis[ic] = vn[ic] - vnewr * m.rvminn[ic] / rminn;
+        vnewp += xaxis[ic] * xaxis[ic];
+      }
+      vnewp = sqrt(vnewp);
+      if (vnewp < eps) {
+        xaxis[0] = eps * (one - m.rvminn[0] * m.rvminn[0]);
+        xaxis[1] = eps * (-m.rvminn[0] * m.rvminn[1]);
+        xaxis[2] = eps * (-m.rvminn[0] * m.rvminn[2]);
+        vnewp = eps * sqrt(one - m.rvminn[0] * m.rvminn[0] * (two - rminn * rminn));
+      }
+      for (int ic = 0; ic < 3; ic++) xaxis[ic] = xaxis[ic] / vnewp;
+      const double zn = cs.znuc[cs.iwctype[m.nearestn]];
+      const double zc = (cs.nloc == 0) ? zn : zero;
+      vnewr = fmax(vnewr, -2 * zn);
+      vnewp = vnewp * cs.fbias;
+      double root = (zc + vnewr) * (zc + vnewr - four / rminn), zeta;
+      if (root >= zero) {
+        root = sqrt(root);
+        zeta = half * (zc - vnewr - root);
+        if (zeta <= zero) zeta = half * (zc - vnewr + root);
+        if (zeta <= zero) zeta = eps;
+      } else {
+        zeta = (vnewr < zero) ? -vnewr - eps : one;
+      }
+      const double co = (zeta + vnewr) / (one - (zeta + vnewr) * rminn);
+      const double bot = sqrt(rminn) * fabs(one + co * rminn) * exp(-zeta * rminn);
+      const double top = sqrt(rminon) * fabs(one + co * rminon) * exp(-zeta * rminon);
+      double fxnp = one * top / bot;
+      double arean = t_area_d(zeta, co, rbot, rtop, bot);
+      arean = arean * m.delttn;
+      double dot = 0;
+      for (int ic = 0; ic < 3; ic++) dot += m.rvminn[ic] * m.rvminon[ic];
+      dot = dot / (rminn * rminon);
+      const double costht = dot;
+      const double sintht = sqrt(one - costht * costht);
+      const double ravern = half * (rminn + rminon);
+      const double term = fmin(vnewp * ravern * sintht, one);
+      double cosphi = zero, rnorm = zero;
+      for (int ic = 0; ic < 3; ic++) {
+        const double term2 = m.rvminon[ic] / rminon - costht * m.rvminn[ic] / rminn;
+        rnorm += term2 * term2;
+        cosphi += term2 * xaxis[ic];
+      }
+      cosphi = cosphi / sqrt(rnorm);
+      fxnp = fxnp * (one + term * cosphi);
+      p = m.rratio * m.rratio * exp(psi2n - st.psi2o[w]) * fabs((fxnp * m.areao) / (m.fxop * arean));
+      p = fmin(one, p);
+    }
+  }
+  const int acc = (rng.uniform() < p) ? 1 : 0;
+  rng.store(st.rng + 4 * (size_t)w);
+  m.acc = acc;
+  m.ratio = ratio;
+  if (acc) {
+    st.psi2o[w] = psi2n;
+    st.psido[w] = psidn;
+    st.psijo[w] = fsumn;
+    st.fsumo[w] = fsumn;
+    st.detiab[2 * w + iab] = st.detiab[2 * w + iab] * ratio;
+    st.sums[(size_t)w * 8 + 4] += 1.0;
+    st.rmino[(size_t)w * N + iel] = m.rminn;
+    st.nearesto[(size_t)w * N + iel] = m.nearestn;
+    for (int k = 0; k < 3; k++) {
+      st.rvmino[((size_t)w * 3 + k) * N + iel] = m.rvminn[k];
+      st.x[((size_t)w * 3 + k) * N + iel] = m.xnew[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Commit of an accepted move: detsav (Sherman–Morrison, determinante :47-62)
+// and jassav.  CTA per walker; rejected walkers return at once.
+// ---------------------------------------------------------------------------
+__global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
+  if (!mb.ms[w].acc) return;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
   spin_of(iel, iab, nel, ish);
   const int iloc = iel - ish;
-  __shared__ double s_col[256];     // slmin column iel (= slmi column / ratio)
-  __shared__ double s_orb[256];     // new orbital values of the Slater columns
-  __shared__ int s_acc;
-  __shared__ double s_ratio;
-  const MoveScratch m = mb.ms[w];
+  __shared__ double s_orb[256];
+  __shared__ double s_col[256];
+  const double ratio = mb.ms[w].ratio;
   double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
   const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
   const int *slot = g.slot_orb + iab * nmax;
-  if (wid == 0) {
-    double ratio = 0;
-    if (!m.igeo) {
-      for (int j = lane; j < nel; j += 32) {
-        const double o = orbn[slot[j]];
-        s_orb[j] = o;
-        ratio += sl[(size_t)nel * iloc + j] * o;
-      }
-      ratio = warp_sum(ratio);
-    }
-    double v0 = 0, v1 = 0, v2 = 0;
-    if (!m.igeo && ratio != 0.0) {
-      for (int j = lane; j < nel; j += 32) {
-        const double sc = sl[(size_t)nel * iloc + j] / ratio;
-        s_col[j] = sc;
-        v0 += sc * orbn[1 * Oa + slot[j]];
-        v1 += sc * orbn[2 * Oa + slot[j]];
-        v2 += sc * orbn[3 * Oa + slot[j]];
-      }
-      v0 = warp_sum(v0);
-      v1 = warp_sum(v1);
-      v2 = warp_sum(v2);
-    }
-    if (lane == 0) {
-      const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, eps = 1.0e-10;
-      DRng rng;
-      rng.load(st.rng + 4 * (size_t)w);
-      double p = zero, psidn = 0, psi2n = 0;
-      const double fsumn = mb.fsumn[w];
-      if (!m.igeo) {
-        const double detn = st.detiab[2 * w + iab] * ratio;
-        psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
-        if (detn != 0.0) {
-          const double vn[3] = {0.0 + v0 + mb.vjn[3 * w + 0], 0.0 + v1 + mb.vjn[3 * w + 1],
-                                0.0 + v2 + mb.vjn[3 * w + 2]};
-          psi2n = log(fabs(1.0)) + 2 * (log(fabs(psidn)) + fsumn);
-          const double deltar = cs.deltar, deltri = one / deltar;
-          const double rminn = m.rminn, rminon = m.rminon;
-          double rbot = rminn * deltri, rtop = rminn * deltar;
-          double vnewr = zero;
-          for (int ic = 0; ic < 3; ic++) vnewr += vn[ic] * m.rvminn[ic];
-          vnewr = vnewr / rminn;
-          double vnewp = zero, xaxis[3];
-          for (int ic = 0; ic < 3; ic++) {
-            xaxis[ic] = vn[ic] - vnewr * m.rvminn[ic] / rminn;
-            vnewp += xaxis[ic] * xaxis[ic];
-          }
-          vnewp = sqrt(vnewp);
-          if (vnewp < eps) {
-            xaxis[0] = eps * (one - m.rvminn[0] * m.rvminn[0]);
-            xaxis[1] = eps * (-m.rvminn[0] * m.rvminn[1]);
-            xaxis[2] = eps * (-m.rvminn[0] * m.rvminn[2]);
-            vnewp = eps * sqrt(one - m.rvminn[0] * m.rvminn[0] * (two - rminn * rminn));
-          }
-          for (int ic = 0; ic < 3; ic++) xaxis[ic] = xaxis[ic] / vnewp;
-          const double zn = cs.znuc[cs.iwctype[m.nearestn]];
-          const double zc = (cs.nloc == 0) ? zn : zero;
-          vnewr = fmax(vnewr, -2 * zn);
-          vnewp = vnewp * cs.fbias;
-          double root = (zc + vnewr) * (zc + vnewr - four / rminn), zeta;
-          if (root >= zero) {
-            root = sqrt(root);
-            zeta = half * (zc - vnewr - root);
-            if (zeta <= zero) zeta = half * (zc - vnewr + root);
-            if (zeta <= zero) zeta = eps;
-          } else {
-            zeta = (vnewr < zero) ? -vnewr - eps : one;
-          }
-          const double co = (zeta + vnewr) / (one - (zeta + vnewr) * rminn);
-          const double bot = sqrt(rminn) * fabs(one + co * rminn) * exp(-zeta * rminn);
-          const double top = sqrt(rminon) * fabs(one + co * rminon) * exp(-zeta * rminon);
-          double fxnp = one * top / bot;
-          double arean = t_area_d(zeta, co, rbot, rtop, bot);
-          arean = arean * m.delttn;
-          // costht/sintht of the reverse move (geometric block of metrop6)
-          double dot = 0;
-          for (int ic = 0; ic < 3; ic++) dot += m.rvminn[ic] * m.rvminon[ic];
-          dot = dot / (rminn * rminon);
-          const double costht = dot;
-          const double sintht = sqrt(one - costht * costht);
-          const double ravern = half * (rminn + rminon);
-          const double term = fmin(vnewp * ravern * sintht, one);
-          double cosphi = zero, rnorm = zero;
-          for (int ic = 0; ic < 3; ic++) {
-            const double term2 = m.rvminon[ic] / rminon - costht * m.rvminn[ic] / rminn;
-            rnorm += term2 * term2;
-            cosphi += term2 * xaxis[ic];
-          }
-          cosphi = cosphi / sqrt(rnorm);
-          fxnp = fxnp * (one + term * cosphi);
-          p = m.rratio * m.rratio * exp(psi2n - st.psi2o[w]) * fabs((fxnp * m.areao) / (m.fxop * arean));
-          p = fmin(one, p);
-        }
-      }
-      const int acc = (rng.uniform() < p) ? 1 : 0;
-      rng.store(st.rng + 4 * (size_t)w);
-      if (acc) {
-        st.psi2o[w] = psi2n;
-        st.psido[w] = psidn;
-        st.psijo[w] = fsumn;
-        st.fsumo[w] = fsumn;
-        st.detiab[2 * w + iab] = st.detiab[2 * w + iab] * ratio;
-        st.sums[(size_t)w * 8 + 4] += 1.0;
-        st.rmino[(size_t)w * N + iel] = m.rminn;
-        st.nearesto[(size_t)w * N + iel] = m.nearestn;
-        for (int k = 0; k < 3; k++) {
-          st.rvmino[((size_t)w * 3 + k) * N + iel] = m.rvminn[k];
-          st.x[((size_t)w * 3 + k) * N + iel] = m.xnew[k];
-        }
-      }
-      s_acc = acc;
-      s_ratio = ratio;
-    }
+  for (int j = tid; j < nel; j += blockDim.x) {
+    s_orb[j] = orbn[slot[j]];
+    s_col[j] = sl[(size_t)nel * iloc + j];
   }
   __syncthreads();
-  if (!s_acc) return;
-  const double ratio = s_ratio;
-  // --- detsav: Sherman–Morrison update of the spin block (determinante :47-62)
   // rows k != iloc: slmi(:,k) -= slmi(:,iloc) * (slmi(:,k)·orb_new)/ratio
   for (int k = wid; k < nel; k += nwarp) {
     if (k == iloc) continue;
     double s = 0;
     for (int j = lane; j < nel; j += 32) s += sl[(size_t)nel * k + j] * s_orb[j];
     s = warp_sum(s) / ratio;
-    for (int j = lane; j < nel; j += 32) sl[(size_t)nel * k + j] = sl[(size_t)nel * k + j] - sl[(size_t)nel * iloc + j] * s;
+    for (int j = lane; j < nel; j += 32) sl[(size_t)nel * k + j] = sl[(size_t)nel * k + j] - s_col[j] * s;
   }
-  __syncthreads();
-  for (int j = tid; j < nel; j += blockDim.x) sl[(size_t)nel * iloc + j] = s_col[j];
+  for (int j = tid; j < nel; j += blockDim.x) sl[(size_t)nel * iloc + j] = s_col[j] / ratio;
   // orbital rows of the moved electron
   for (int j = tid; j < nel; j += blockDim.x) {
     st.orbs[((size_t)w * N + iel) * nmax + j] = s_orb[j];
     for (int k = 0; k < 3; k++)
       st.dorbs[(((size_t)w * 3 + k) * N + iel) * nmax + j] = orbn[(1 + k) * Oa + slot[j]];
   }
-  // --- jassav: pair tables and per-electron gradients
+  // jassav: pair tables and per-electron gradients
   double *fso = st.fso + (size_t)w * N * N;
   for (int jj = tid; jj < N; jj += blockDim.x) {
     const double fsn = mb.fsn[(size_t)w * N + jj];

@@ -196,7 +196,7 @@ long cw_launches(const cw_ctx *ctx);
 enum {
   CW_ST_ROTQUA = 0, CW_ST_PROPOSE, CW_ST_JASTROW_MOVE, CW_ST_BASIS_MOVE, CW_ST_LCAO_MOVE,
   CW_ST_ACCEPT, CW_ST_JASTROW_FULL, CW_ST_BASIS_ALL, CW_ST_LCAO_ALL, CW_ST_SCATTER,
-  CW_ST_SLATER_INV, CW_ST_CTILDE, CW_ST_ECP, CW_ST_ENERGY, CW_NSTAGE
+  CW_ST_SLATER_INV, CW_ST_CTILDE, CW_ST_ECP, CW_ST_ENERGY, CW_ST_COMMIT, CW_NSTAGE
 };
 int cw_profile(cw_ctx *ctx, int enable);
 int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
