@@ -56,6 +56,7 @@ __constant__ CSys cs;
 // Global-memory tables of the system.
 struct GSys {
   const double *rwf, *d2rwf;      // [nctype][mrwf][mpts]
+  const double *gridpow;          // [nctype][mpts+1]  r0*arg^(jx-1), jx = 0..mpts
   const int *iwlbas, *iwrwf;      // [nctype][mbastyp]
   const double *coefT;            // [K][Oa]  (active orbitals)
   const int *slot_orb;            // [2][nmax] active-orbital index of Slater column j, spin s
@@ -472,6 +473,89 @@ __device__ __forceinline__ EenOut<T> een_pair2(const T *__restrict__ cc, T z, T 
   return e;
 }
 
+
+// Fold with first and second x-derivatives: BD3[3*t .. 3*t+2] = B, dB, d2B
+template <int NORD, typename T>
+__device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD3) {
+  T xp[NORD + 1];
+  xp[0] = 1;
+#pragma unroll
+  for (int q = 1; q <= NORD; q++) xp[q] = xp[q - 1] * x;
+  T B[een_nb(NORD)], dB[een_nb(NORD)], d2B[een_nb(NORD)];
+#pragma unroll
+  for (int t = 0; t < een_nb(NORD); t++) B[t] = dB[t] = d2B[t] = 0;
+  int ll = 0;
+#pragma unroll
+  for (int n = 2; n <= NORD; n++) {
+#pragma unroll
+    for (int k = n - 1; k >= 0; k--) {
+      const int l_hi = (k == 0) ? n - k - 2 : n - k;
+#pragma unroll
+      for (int l = l_hi; l >= 0; l--) {
+        const int m = (n - k - l) / 2;
+        if (2 * m == n - k - l) {
+          const T c = cc[ll];
+          ll++;
+          const int a = l + m, b = m;
+          const int t1 = een_off(NORD, k) + b - een_pmin(k);   // y^m   gets c x^(l+m)
+          const int t2 = een_off(NORD, k) + a - een_pmin(k);   // y^(l+m) gets c x^m
+          B[t1] += c * xp[a];
+          B[t2] += c * xp[b];
+          if (a >= 1) dB[t1] += c * T(a) * xp[a >= 1 ? a - 1 : 0];
+          if (b >= 1) dB[t2] += c * T(b) * xp[b >= 1 ? b - 1 : 0];
+          if (a >= 2) d2B[t1] += c * T(a * (a - 1)) * xp[a >= 2 ? a - 2 : 0];
+          if (b >= 2) d2B[t2] += c * T(b * (b - 1)) * xp[b >= 2 ? b - 2 : 0];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < een_nb(NORD); t++) {
+    BD3[3 * t] = B[t];
+    BD3[3 * t + 1] = dB[t];
+    BD3[3 * t + 2] = d2B[t];
+  }
+}
+
+// all nine value/derivative sums of the e-e-n term (jastrow4.f90 fc, fu,
+// fuu, fi, fii, fj, fjj, fui, fuj) from the folded row coefficients
+template <int NORD>
+__device__ __forceinline__ EenOut<double> een_apply2(const double *__restrict__ BD3, double y, double z) {
+  double yp[NORD + 1];
+  yp[0] = 1;
+#pragma unroll
+  for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
+  EenOut<double> e{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double zk = 1, dzk = 0, d2zk = 0;
+#pragma unroll
+  for (int k = 0; k < NORD; k++) {
+    double a = 0, ax = 0, axx = 0, ay = 0, ayy = 0;
+#pragma unroll
+    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
+      const int t = een_off(NORD, k) + p - een_pmin(k);
+      const double b0 = BD3[3 * t], b1 = BD3[3 * t + 1], b2 = BD3[3 * t + 2];
+      a += b0 * yp[p];
+      ax += b1 * yp[p];
+      axx += b2 * yp[p];
+      if (p >= 1) ay += b0 * (double(p) * yp[p >= 1 ? p - 1 : 0]);
+      if (p >= 2) ayy += b0 * (double(p * (p - 1)) * yp[p >= 2 ? p - 2 : 0]);
+    }
+    e.fc += zk * a;
+    e.fu += dzk * a;
+    e.fuu += d2zk * a;
+    e.fi += zk * ax;
+    e.fii += zk * axx;
+    e.fui += dzk * ax;
+    e.fj += zk * ay;
+    e.fjj += zk * ayy;
+    e.fuj += dzk * ay;
+    d2zk = double(k + 1) * dzk;
+    dzk = double(k + 1) * zk;
+    zk *= z;
+  }
+  return e;
+}
+
 // Padé + polynomial e-e term (jastrow4.f90 ee part) at scaled u:
 // returns fee, d fee/du, d2 fee/du2 (MODE>=2)
 template <int MODE, typename T>
@@ -515,80 +599,6 @@ __device__ __forceinline__ void en_term(int it, T r, T &fen, T &feni, T &fenii) 
     if (MODE >= 2) fenii += ac * T(iord * (iord - 1)) * rpm;
     rpm = rp;
     rp = rord;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// splfit (vmc/splfit.f90:3-94)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void splfit_d(const GSys &g, double r, int irb, int it, double *wfv, int ider) {
-  const int ig = cs.igrid[it];
-  const double arg = cs.arg[it], r0 = cs.r0[it];
-  double xr, ref0, ref1, delh;
-  int jx;
-  if (ig == 1) {
-    xr = (r - r0) / arg + 1;
-    jx = (int)xr;
-    ref0 = r0 + arg * (jx - 1);
-    ref1 = ref0 + arg;
-    delh = arg;
-  } else if (ig == 2) {
-    double dlrad0 = log(r0), dlogag = log(arg);
-    xr = (log(r) - dlrad0) / dlogag + 1;
-    jx = (int)xr;
-    ref0 = r0 * pow(arg, (double)(jx - 1));
-    ref1 = ref0 * arg;
-    delh = ref1 - ref0;
-  } else {
-    double dlogag = log(arg);
-    xr = (log((r + r0) / r0)) / dlogag + 1.0;
-    jx = (int)xr;
-    ref0 = r0 * pow(arg, (double)(jx - 1)) - r0;
-    ref1 = (ref0 + r0) * arg - r0;
-    delh = ref1 - ref0;
-  }
-  const int tb = irb + cs.mrwf * it;
-  if (jx < 1) {
-    const double *ce = &cs.ce[(it * CW_MAX_RWF + irb) * 5];
-    const double rpow[5] = {1.0, r, r * r, r * r * r, r * r * r * r};
-    double v = ce[0];
-    for (int ii = 2; ii <= 5; ii++) v += ce[ii - 1] * rpow[ii - 1];
-    wfv[0] = v;
-    if (ider >= 1) {
-      double p1 = 0, p2 = 0, p3 = 0;
-      for (int ii = 2; ii <= 5; ii++) {
-        const double c = ce[ii - 1];
-        p1 += (ii - 1) * c * rpow[ii - 2];
-        if (ii >= 3) p2 += (ii - 1) * (ii - 2) * c * rpow[ii - 3];
-        if (ii >= 4) p3 += (ii - 1) * (ii - 2) * (ii - 3) * c * rpow[ii - 4];
-      }
-      wfv[1] = p1; wfv[2] = p2; wfv[3] = p3;
-    }
-  } else if (jx >= cs.nr[it]) {
-    const double *ae = &cs.ae[(it * CW_MAX_RWF + irb) * 2];
-    wfv[0] = ae[0] * exp(-ae[1] * r);
-    if (ider >= 1) {
-      wfv[1] = -ae[1] * wfv[0];
-      wfv[2] = -ae[1] * wfv[1];
-      wfv[3] = -ae[1] * wfv[2];
-    }
-  } else {
-    const double *y = g.rwf + (size_t)tb * cs.mpts;
-    const double *y2 = g.d2rwf + (size_t)tb * cs.mpts;
-    const double y0 = __ldg(y + jx - 1), y1 = __ldg(y + jx);
-    const double d0 = __ldg(y2 + jx - 1), d1 = __ldg(y2 + jx);
-    const double sixth = 1.0 / 6.0;
-    const double delhi = 1.0 / delh;
-    const double bb = (r - ref0) * delhi;
-    const double aa = (ref1 - r) * delhi;
-    const double cc = aa * (aa * aa - 1.0) * delh * delh * sixth;
-    const double dd = bb * (bb * bb - 1.0) * delh * delh * sixth;
-    wfv[0] = aa * y0 + bb * y1 + cc * d0 + dd * d1;
-    if (ider >= 1) {
-      wfv[1] = (y1 - y0) * delhi + (-(3.0 * aa * aa - 1.0) * d0 + (3.0 * bb * bb - 1.0) * d1) * delh * sixth;
-      wfv[2] = aa * d0 + bb * d1;
-      wfv[3] = (-d0 + d1) * delhi;
-    }
   }
 }
 
@@ -661,9 +671,12 @@ __device__ __forceinline__ void slm_eval(int l, double x, double y, double z, do
 // (d=1..3, ider>=1) and Laplacian (d=4, ider>=2).
 template <typename Store>
 __device__ __forceinline__ void basis_centre(const GSys &g, int ic, const double *xc, int ider, Store out) {
-  // Radial functions are evaluated one at a time and combined at once with
-  // every AO that uses them (iwrwf), so no per-thread array of spline values
-  // is needed (it would live in local memory).
+  // basis_fns + splfit (vmc/splfit.f90:3-94) for every radial function of
+  // the centre.  The grid interval (jx, ref0, ref1) depends only on r and
+  // the atom type, so it is located once per centre; r0*arg^(jx-1) comes
+  // from a per-type table instead of pow().  Radial functions are then
+  // evaluated one at a time and combined with every AO that uses them
+  // (iwrwf), so no per-thread array of spline values is needed.
   const int it = cs.iwctype[ic];
   const double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
   const double ri = 1.0 / r;
@@ -673,10 +686,75 @@ __device__ __forceinline__ void basis_centre(const GSys &g, int ic, const double
   const double xcri[3] = {xc[0] * ri, xc[1] * ri, xc[2] * ri};
   const int *iwl = g.iwlbas + it * cs.mbastyp;
   const int *iwr = g.iwrwf + it * cs.mbastyp;
+  // grid location (splfit :33-55)
+  const int ig = cs.igrid[it];
+  const double arg = cs.arg[it], r0 = cs.r0[it];
+  const double *gp = g.gridpow + (size_t)it * (cs.mpts + 1);
+  double xr, ref0 = 0, ref1 = 0, delh = 1;
+  int jx;
+  if (ig == 1) {
+    xr = (r - r0) / arg + 1;
+    jx = (int)xr;
+    ref0 = r0 + arg * (jx - 1);
+    ref1 = ref0 + arg;
+    delh = arg;
+  } else if (ig == 2) {
+    xr = (log(r) - log(r0)) / log(arg) + 1;
+    jx = (int)xr;
+    if (jx >= 1 && jx <= cs.mpts) {
+      ref0 = __ldg(gp + jx);
+      ref1 = ref0 * arg;
+      delh = ref1 - ref0;
+    }
+  } else {
+    xr = (log((r + r0) / r0)) / log(arg) + 1.0;
+    jx = (int)xr;
+    if (jx >= 1 && jx <= cs.mpts) {
+      ref0 = __ldg(gp + jx) - r0;
+      ref1 = (ref0 + r0) * arg - r0;
+      delh = ref1 - ref0;
+    }
+  }
+  const int spline = (jx >= 1 && jx < cs.nr[it]);
+  const double sixth = 1.0 / 6.0;
+  const double delhi = 1.0 / delh;
+  const double bb = (r - ref0) * delhi;
+  const double aa = (ref1 - r) * delhi;
+  const double cc = aa * (aa * aa - 1.0) * delh * delh * sixth;
+  const double dd = bb * (bb * bb - 1.0) * delh * delh * sixth;
+  const double t1 = (3.0 * aa * aa - 1.0) * delh * sixth, t2 = (3.0 * bb * bb - 1.0) * delh * sixth;
   for (int irb = 0; irb < nrb; irb++) {
     double w[4];
     if (r <= cs.rmaxwf[it * CW_MAX_RWF + irb]) {
-      splfit_d(g, r, irb, it, w, ider);
+      if (spline) {
+        const size_t tb = (size_t)(irb + cs.mrwf * it) * cs.mpts;
+        const double y0 = __ldg(g.rwf + tb + jx - 1), y1 = __ldg(g.rwf + tb + jx);
+        const double d0 = __ldg(g.d2rwf + tb + jx - 1), d1 = __ldg(g.d2rwf + tb + jx);
+        w[0] = aa * y0 + bb * y1 + cc * d0 + dd * d1;
+        w[1] = (y1 - y0) * delhi + (-t1 * d0 + t2 * d1);
+        w[2] = aa * d0 + bb * d1;
+        w[3] = (-d0 + d1) * delhi;
+      } else if (jx < 1) {
+        const double *ce = &cs.ce[(it * CW_MAX_RWF + irb) * 5];
+        const double rpow[5] = {1.0, r, r * r, r * r * r, r * r * r * r};
+        double v = ce[0];
+        for (int ii = 2; ii <= 5; ii++) v += ce[ii - 1] * rpow[ii - 1];
+        w[0] = v;
+        double p1 = 0, p2 = 0, p3 = 0;
+        for (int ii = 2; ii <= 5; ii++) {
+          const double c = ce[ii - 1];
+          p1 += (ii - 1) * c * rpow[ii - 2];
+          if (ii >= 3) p2 += (ii - 1) * (ii - 2) * c * rpow[ii - 3];
+          if (ii >= 4) p3 += (ii - 1) * (ii - 2) * (ii - 3) * c * rpow[ii - 4];
+        }
+        w[1] = p1; w[2] = p2; w[3] = p3;
+      } else {
+        const double *ae = &cs.ae[(it * CW_MAX_RWF + irb) * 2];
+        w[0] = ae[0] * exp(-ae[1] * r);
+        w[1] = -ae[1] * w[0];
+        w[2] = -ae[1] * w[1];
+        w[3] = -ae[1] * w[2];
+      }
     } else {
       w[0] = w[1] = w[2] = w[3] = 0.0;
     }

@@ -158,7 +158,7 @@ void launch_jmove(cw_ctx *c, int iel) {
 }
 template <int NORD>
 void launch_jfull(cw_ctx *c) {
-  k_jastrow_full<NORD><<<c->W, 256, c->smem_jfull, c->stream>>>(c->st, c->hb);
+  k_jastrow_full<NORD><<<c->W, 128, c->smem_jfull, c->stream>>>(c->st, c->hb);
 }
 template <int NORD>
 void launch_ecp(cw_ctx *c) {
@@ -310,6 +310,7 @@ int alloc_walkers(cw_ctx *c, int W) {
   DALLOC(L, b.phi, (size_t)W * chunk * 5 * K);
   DALLOC(L, b.orball, (size_t)W * chunk * 5 * Oa);
   if (h.nloc > 0) DALLOC(L, b.ctilde, (size_t)W * N * K);
+  DALLOC(L, b.entab, (size_t)W * M * N * 8);
   CK(cudaMemsetAsync(s.status, 0, sizeof(int) * W, c->stream));
   CK(cudaMemsetAsync(s.sums, 0, sizeof(double) * W * 8, c->stream));
   c->W = W;
@@ -480,13 +481,25 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     if (v < 0 || v >= d->norb) return fail(c, CW_ERR_ARG, "iworbd entry out of range");
   DALLOC(L, slot, so.size());
   CK(cudaMemcpy(slot, so.data(), so.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // r0*arg^(jx-1) of every grid point (splfit's ref0 for igrid 2 and 3)
+  std::vector<double> gpw((size_t)d->nctype * (d->mrwf_pts + 1), 0.0);
+  for (int it = 0; it < d->nctype; it++)
+    for (int jx = 1; jx <= d->mrwf_pts; jx++)
+      gpw[(size_t)it * (d->mrwf_pts + 1) + jx] = d->r0[it] * std::pow(d->arg[it], jx - 1);
+  double *gridpow;
+  DALLOC(L, gridpow, gpw.size());
+  CK(cudaMemcpy(gridpow, gpw.data(), gpw.size() * sizeof(double), cudaMemcpyHostToDevice));
   c->g.rwf = rwf; c->g.d2rwf = d2rwf; c->g.iwlbas = iwl; c->g.iwrwf = iwr; c->g.coefT = coefT; c->g.slot_orb = slot;
+  c->g.gridpow = gridpow;
   // dynamic shared memory sizes
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
     c->smem_jmove = sizeof(double) * 4 * (size_t)h.M * (6 + 2 * een_nb(nord));
   }
-  c->smem_jfull = sizeof(double) * 3 * (size_t)h.N;
+  {
+    const int nord = h.nordc <= 1 ? 1 : h.nordc;
+    c->smem_jfull = sizeof(double) * (3 * (size_t)h.N + 1 + 2 * (size_t)h.M * 3 * een_nb(nord));
+  }
   c->smem_sinv = sizeof(double) * ((size_t)nmax * nmax + nmax);
   c->smem_ctil = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64);
   {

@@ -25,6 +25,7 @@ struct HBuf {
   double *phi;      // [rows][K] chunk basis
   double *orball;   // [rows][Oa] chunk orbitals
   double *ctilde;   // [W][N][K]
+  double *entab;    // [W][M][N][8] e-n table of the full Jastrow: rr, dd1, dd2, r, rvec(3)
   int chunk;        // electrons per chunk
 };
 
@@ -51,104 +52,137 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 // ---------------------------------------------------------------------------
-// jastrow_factor4: CTA per walker, threads over pairs.
+// jastrow_factor4 (vmc/jastrow4.f90:3): CTA per walker.
+//  1. e-n table of every (electron, centre): scaled distance and its
+//     derivatives, the distance and its vector (L2-resident scratch);
+//  2. pair rows i and N-1-i together (N-1 pairs per batch): the row
+//     electron's e-e-n coefficients are folded per centre (value, d/dx,
+//     d2/dx2) into shared memory, then threads over the batch's pairs
+//     evaluate every centre from the folded coefficients;
+//  3. e-n terms, per-electron gradient sums, block sums.
 // ---------------------------------------------------------------------------
 template <int NORD>
-__global__ void __launch_bounds__(256) k_jastrow_full(WState st, HBuf hb) {
+__global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M;
+  constexpr int NB = een_nb(NORD);
   extern __shared__ __align__(16) double smem[];
-  double *sx = smem;            // [3][N]
-  __shared__ double red[8];
+  double *sx = smem;                      // [3][N]
+  double *sB = smem + 3 * N + (3 * N & 1);  // [2][M][3*NB] folded rows
+  __shared__ double red[4];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
   __syncthreads();
   const double kap = cs.scalek;
+  double *tab = hb.entab + (size_t)w * M * N * 8;
+  for (int t = threadIdx.x; t < M * N; t += blockDim.x) {
+    const int ic = t / N, e = t % N;
+    const double v0 = sx[e] - cs.cent[3 * ic], v1 = sx[N + e] - cs.cent[3 * ic + 1], v2 = sx[2 * N + e] - cs.cent[3 * ic + 2];
+    const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    double rr, dd1, dd2;
+    scale2<double>(r, rr, dd1, dd2);
+    double *q = tab + (size_t)t * 8;
+    q[0] = rr; q[1] = dd1; q[2] = dd2; q[3] = r; q[4] = v0; q[5] = v1; q[6] = v2; q[7] = 0;
+  }
   double *fso = st.fso + (size_t)w * N * N;
   double *fij0 = st.fijo + ((size_t)w * 3 + 0) * N * N;
   double *fij1 = st.fijo + ((size_t)w * 3 + 1) * N * N;
   double *fij2 = st.fijo + ((size_t)w * 3 + 2) * N * N;
   double fsum = 0, d2sum = 0, pee = 0;
-  const long npair = (long)N * (N - 1) / 2;
-  for (long p = threadIdx.x; p < npair; p += blockDim.x) {
-    int i, j;
-    pair_of(p, i, j);
-    int isb, ipar;
-    double sspinn;
-    pair_spin(i, j, isb, ipar, sspinn);
-    const double rv[3] = {sx[i] - sx[j], sx[N + i] - sx[N + j], sx[2 * N + i] - sx[2 * N + j]};
-    const double rij = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
-    pee += 1 / rij;
-    double u, dd1, dd2;
-    scale2<double>(rij, u, dd1, dd2);
-    double fs = 0, d2 = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
-    if (u != cs.asymp_r) {
-      double fee, feeu, feeuu;
-      ee_term<2, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
-      feeuu = feeuu * dd1 * dd1 + feeu * dd2;
-      feeu = feeu * dd1 / rij;
-      fs += fee;
-      for (int k = 0; k < 3; k++) {
-        gi[k] += feeu * rv[k];
-        gj[k] -= feeu * rv[k];
-      }
-      d2 += 2 * (feeuu + 2 * feeu);
-    }
+  const int nbatch = N / 2;  // rows (b, N-1-b); the middle row of odd N joins batch 0 below
+  for (int bt = 0; bt < (N + 1) / 2; bt++) {
+    const int ia = bt, ib = N - 1 - bt;  // ia == ib only for the middle row of odd N
+    const int npa = ia, npb = (ib != ia) ? ib : 0;
+    __syncthreads();  // previous batch done with sB; table written
     if (NORD > 1) {
-      const double u1 = 1 - kap * u, du1 = -kap * dd1, du2 = -kap * dd2;
-      for (int ic = 0; ic < M; ic++) {
-        const int it = cs.iwctype[ic];
-        const double *cc = &cs.cent[3 * ic];
-        const double ri_v[3] = {sx[i] - cc[0], sx[N + i] - cc[1], sx[2 * N + i] - cc[2]};
-        const double rj_v[3] = {sx[j] - cc[0], sx[N + j] - cc[1], sx[2 * N + j] - cc[2]};
-        const double ri = sqrt(ri_v[0] * ri_v[0] + ri_v[1] * ri_v[1] + ri_v[2] * ri_v[2]);
-        const double rj = sqrt(rj_v[0] * rj_v[0] + rj_v[1] * rj_v[1] + rj_v[2] * rj_v[2]);
-        double rri, dd7, dd9, rrj, dd8, dd10;
-        scale2<double>(ri, rri, dd7, dd9);
-        scale2<double>(rj, rrj, dd8, dd10);
-        if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
-        dd7 = -kap * dd7; dd9 = -kap * dd9; dd8 = -kap * dd8; dd10 = -kap * dd10;
-        const EenOut<double> e = een_pair2<NORD, double>(&cs.c[it * CW_MAX_TERMS], u1, 1 - kap * rri, 1 - kap * rrj);
-        const double sgs = ri + rj, tgs = ri - rj;
-        const double u2pst = rij * rij + sgs * tgs, u2mst = rij * rij - sgs * tgs;
-        const double fuu = e.fuu * du1 * du1 + e.fu * du2;
-        const double fu = e.fu * du1 / rij;
-        const double fui = e.fui * du1 * dd7, fuj = e.fuj * du1 * dd8;
-        const double fii = e.fii * dd7 * dd7 + e.fi * dd9, fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
-        const double fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
-        fs += e.fc;
-        for (int k = 0; k < 3; k++) {
-          gi[k] += fi * ri_v[k] + fu * rv[k];
-          gj[k] += fj * rj_v[k] - fu * rv[k];
-        }
-        d2 += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rij) + fuj * u2mst / (rj * rij) + fii + 2 * fi + fjj + 2 * fj;
+      for (int t = threadIdx.x; t < 2 * M; t += blockDim.x) {
+        const int row = t / M, ic = t % M;
+        const int i = row == 0 ? ia : ib;
+        const double rr = tab[((size_t)ic * N + i) * 8];
+        een_fold2<NORD, double>(&cs.c[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sB + ((size_t)row * M + ic) * 3 * NB);
       }
     }
-    fso[(size_t)i * N + j] = fs;
-    fso[(size_t)j * N + i] = fs;
-    fij0[(size_t)i * N + j] = gi[0]; fij0[(size_t)j * N + i] = gj[0];
-    fij1[(size_t)i * N + j] = gi[1]; fij1[(size_t)j * N + i] = gj[1];
-    fij2[(size_t)i * N + j] = gi[2]; fij2[(size_t)j * N + i] = gj[2];
-    fsum += fs;
-    d2sum += d2;
+    __syncthreads();
+    for (int t = threadIdx.x; t < npa + npb; t += blockDim.x) {
+      const int row = t < npa ? 0 : 1;
+      const int i = row == 0 ? ia : ib, j = row == 0 ? t : t - npa;
+      int isb, ipar;
+      double sspinn;
+      pair_spin(i, j, isb, ipar, sspinn);
+      const double rv[3] = {sx[i] - sx[j], sx[N + i] - sx[N + j], sx[2 * N + i] - sx[2 * N + j]};
+      const double rij = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+      pee += 1 / rij;
+      double u, dd1, dd2;
+      scale2<double>(rij, u, dd1, dd2);
+      double fs = 0, d2 = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
+      if (u != cs.asymp_r) {
+        double fee, feeu, feeuu;
+        ee_term<2, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+        feeuu = feeuu * dd1 * dd1 + feeu * dd2;
+        feeu = feeu * dd1 / rij;
+        fs += fee;
+        for (int k = 0; k < 3; k++) {
+          gi[k] += feeu * rv[k];
+          gj[k] -= feeu * rv[k];
+        }
+        d2 += 2 * (feeuu + 2 * feeu);
+      }
+      if (NORD > 1) {
+        const double z = 1 - kap * u, du1 = -kap * dd1, du2 = -kap * dd2;
+        const double *Brow = sB + (size_t)row * M * 3 * NB;
+        for (int ic = 0; ic < M; ic++) {
+          const double *qi = tab + ((size_t)ic * N + i) * 8;
+          const double *qj = tab + ((size_t)ic * N + j) * 8;
+          const double rri = qi[0], rrj = qj[0];
+          if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
+          const double dd7 = -kap * qi[1], dd9 = -kap * qi[2], ri = qi[3];
+          const double dd8 = -kap * qj[1], dd10 = -kap * qj[2], rj = qj[3];
+          const EenOut<double> e = een_apply2<NORD>(Brow + (size_t)ic * 3 * NB, 1 - kap * rrj, z);
+          const double sgs = ri + rj, tgs = ri - rj;
+          const double u2pst = rij * rij + sgs * tgs, u2mst = rij * rij - sgs * tgs;
+          const double fuu = e.fuu * du1 * du1 + e.fu * du2;
+          const double fu = e.fu * du1 / rij;
+          const double fui = e.fui * du1 * dd7, fuj = e.fuj * du1 * dd8;
+          const double fii = e.fii * dd7 * dd7 + e.fi * dd9, fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
+          const double fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
+          fs += e.fc;
+          gi[0] += fi * qi[4] + fu * rv[0];
+          gi[1] += fi * qi[5] + fu * rv[1];
+          gi[2] += fi * qi[6] + fu * rv[2];
+          gj[0] += fj * qj[4] - fu * rv[0];
+          gj[1] += fj * qj[5] - fu * rv[1];
+          gj[2] += fj * qj[6] - fu * rv[2];
+          d2 += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rij) + fuj * u2mst / (rj * rij) + fii + 2 * fi + fjj + 2 * fj;
+        }
+      }
+      fso[(size_t)i * N + j] = fs;
+      fso[(size_t)j * N + i] = fs;
+      fij0[(size_t)i * N + j] = gi[0]; fij0[(size_t)j * N + i] = gj[0];
+      fij1[(size_t)i * N + j] = gi[1]; fij1[(size_t)j * N + i] = gj[1];
+      fij2[(size_t)i * N + j] = gi[2]; fij2[(size_t)j * N + i] = gj[2];
+      fsum += fs;
+      d2sum += d2;
+    }
   }
+  (void)nbatch;
+  __syncthreads();
   // e-n terms
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     double fs = 0, d2 = 0, g[3] = {0, 0, 0};
     for (int ic = 0; ic < M; ic++) {
       const int it = cs.iwctype[ic];
-      const double *cc = &cs.cent[3 * ic];
-      const double rvv[3] = {sx[i] - cc[0], sx[N + i] - cc[1], sx[2 * N + i] - cc[2]};
-      const double ri = sqrt(rvv[0] * rvv[0] + rvv[1] * rvv[1] + rvv[2] * rvv[2]);
-      double rri, dd7, dd9;
-      scale2<double>(ri, rri, dd7, dd9);
+      const double *q = tab + ((size_t)ic * N + i) * 8;
+      const double rri = q[0];
       if (rri == cs.asymp_r) continue;
+      const double dd7 = q[1], dd9 = q[2], ri = q[3];
       double fen, feni, fenii;
       en_term<2, double>(it, rri, fen, feni, fenii);
       fenii = fenii * dd7 * dd7 + feni * dd9;
       feni = feni * dd7 / ri;
       fs += fen;
-      for (int k = 0; k < 3; k++) g[k] += feni * rvv[k];
+      g[0] += feni * q[4];
+      g[1] += feni * q[5];
+      g[2] += feni * q[6];
       d2 += fenii + 2 * feni;
     }
     fso[(size_t)i * N + i] = fs;
@@ -170,9 +204,9 @@ __global__ void __launch_bounds__(256) k_jastrow_full(WState st, HBuf hb) {
     st.fjo[((size_t)w * 3 + 1) * N + i] = a1;
     st.fjo[((size_t)w * 3 + 2) * N + i] = a2;
   }
-  const double tf = block_sum<256>(fsum, red);
-  const double td = block_sum<256>(d2sum, red);
-  const double tp = block_sum<256>(pee, red);
+  const double tf = block_sum<128>(fsum, red);
+  const double td = block_sum<128>(d2sum, red);
+  const double tp = block_sum<128>(pee, red);
   if (threadIdx.x == 0) {
     st.fsumo[w] = tf;
     hb.d2o[w] = td;
