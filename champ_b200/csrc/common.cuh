@@ -48,6 +48,9 @@ struct CSys {
   double ecp_exponent[CW_MAX_TYPES * 4 * 16];
   double ecp_coef[CW_MAX_TYPES * 4 * 16];
   double xq0[CW_MAX_QUAD], yq0[CW_MAX_QUAD], zq0[CW_MAX_QUAD], wq[CW_MAX_QUAD];
+  // Slm (vmc/slm.f90) as monomials: exponents of x, y, z and the constant
+  int slm_a[36], slm_b[36], slm_c[36];
+  double slm_k[36];
 };
 
 // the one system block of the engine translation unit
@@ -60,6 +63,7 @@ struct GSys {
   const int *iwlbas, *iwrwf;      // [nctype][mbastyp]
   const double *coefT;            // [K][Oa]  (active orbitals)
   const int *slot_orb;            // [2][nmax] active-orbital index of Slater column j, spin s
+  const int4 *ao;                 // [K] per AO: centre, radial function (0-based), atom type, Slm index
 };
 
 // ---------------------------------------------------------------------------
@@ -776,6 +780,131 @@ __device__ __forceinline__ void basis_centre(const GSys &g, int ic, const double
           out(m0 + ib, 4, d2);
         }
       }
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Warp-cooperative basis evaluation of one point for all K AOs.
+// Lanes first stage per-centre data (displacement, powers, spline interval
+// and weights) in shared memory, then run over AOs: every lane follows the
+// same code (table-driven Slm monomials), and consecutive lanes write
+// consecutive AOs.  Same arithmetic as basis_centre/splfit.
+// ---------------------------------------------------------------------------
+constexpr int kCenRec = 28;  // doubles per centre record
+
+template <int IDER>
+__device__ __forceinline__ void warp_basis_prepass(const GSys &g, const double *x, double *rec, int lane) {
+  for (int ic = lane; ic < cs.M; ic += 32) {
+    double *q = rec + (size_t)ic * kCenRec;
+    const int it = cs.iwctype[ic];
+    const double xc0 = x[0] - cs.cent[3 * ic], xc1 = x[1] - cs.cent[3 * ic + 1], xc2 = x[2] - cs.cent[3 * ic + 2];
+    const double r = sqrt(xc0 * xc0 + xc1 * xc1 + xc2 * xc2);
+    const double ri = 1.0 / r;
+    const int ig = cs.igrid[it];
+    const double arg = cs.arg[it], r0 = cs.r0[it];
+    const double *gp = g.gridpow + (size_t)it * (cs.mpts + 1);
+    double xr, ref0 = 0, ref1 = 0, delh = 1;
+    int jx;
+    if (ig == 1) {
+      xr = (r - r0) / arg + 1;
+      jx = (int)xr;
+      ref0 = r0 + arg * (jx - 1);
+      ref1 = ref0 + arg;
+      delh = arg;
+    } else if (ig == 2) {
+      xr = (log(r) - log(r0)) / log(arg) + 1;
+      jx = (int)xr;
+      if (jx >= 1 && jx <= cs.mpts) {
+        ref0 = __ldg(gp + jx);
+        ref1 = ref0 * arg;
+        delh = ref1 - ref0;
+      }
+    } else {
+      xr = (log((r + r0) / r0)) / log(arg) + 1.0;
+      jx = (int)xr;
+      if (jx >= 1 && jx <= cs.mpts) {
+        ref0 = __ldg(gp + jx) - r0;
+        ref1 = (ref0 + r0) * arg - r0;
+        delh = ref1 - ref0;
+      }
+    }
+    const double sixth = 1.0 / 6.0, delhi = 1.0 / delh;
+    const double bb = (r - ref0) * delhi, aa = (ref1 - r) * delhi;
+    q[0] = xc0; q[1] = xc1; q[2] = xc2; q[3] = r; q[4] = ri;
+    q[5] = (double)jx;
+    q[6] = aa; q[7] = bb;
+    q[8] = aa * (aa * aa - 1.0) * delh * delh * sixth;
+    q[9] = bb * (bb * bb - 1.0) * delh * delh * sixth;
+    q[10] = (3.0 * aa * aa - 1.0) * delh * sixth;
+    q[11] = (3.0 * bb * bb - 1.0) * delh * sixth;
+    q[12] = delhi;
+    double px = 1, py = 1, pz = 1;
+#pragma unroll
+    for (int p = 0; p < 5; p++) {
+      q[13 + p] = px; q[18 + p] = py; q[23 + p] = pz;
+      px *= xc0; py *= xc1; pz *= xc2;
+    }
+  }
+}
+
+// value (d=0), gradient (d=1..3, IDER>=1), Laplacian (d=4, IDER>=2) of AO m
+template <int IDER, typename Store>
+__device__ __forceinline__ void warp_basis_ao(const GSys &g, const double *rec, int m, Store out) {
+  const int4 a4 = __ldg(g.ao + m);
+  const int ic = a4.x, irb = a4.y, it = a4.z, l = a4.w;
+  const double *q = rec + (size_t)ic * kCenRec;
+  const double r = q[3], ri = q[4];
+  const int jx = (int)q[5];
+  double w0 = 0, w1 = 0, w2 = 0;
+  if (r <= cs.rmaxwf[it * CW_MAX_RWF + irb]) {
+    if (jx >= 1 && jx < cs.nr[it]) {
+      const size_t tb = (size_t)(irb + cs.mrwf * it) * cs.mpts;
+      const double y0 = __ldg(g.rwf + tb + jx - 1), y1 = __ldg(g.rwf + tb + jx);
+      const double d0 = __ldg(g.d2rwf + tb + jx - 1), d1 = __ldg(g.d2rwf + tb + jx);
+      w0 = q[6] * y0 + q[7] * y1 + q[8] * d0 + q[9] * d1;
+      w1 = (y1 - y0) * q[12] + (-q[10] * d0 + q[11] * d1);
+      w2 = q[6] * d0 + q[7] * d1;
+    } else if (jx < 1) {
+      const double *ce = &cs.ce[(it * CW_MAX_RWF + irb) * 5];
+      const double rpow[5] = {1.0, r, r * r, r * r * r, r * r * r * r};
+      w0 = ce[0];
+      for (int ii = 2; ii <= 5; ii++) w0 += ce[ii - 1] * rpow[ii - 1];
+      for (int ii = 2; ii <= 5; ii++) {
+        const double c = ce[ii - 1];
+        w1 += (ii - 1) * c * rpow[ii - 2];
+        if (ii >= 3) w2 += (ii - 1) * (ii - 2) * c * rpow[ii - 3];
+      }
+    } else {
+      const double *ae = &cs.ae[(it * CW_MAX_RWF + irb) * 2];
+      w0 = ae[0] * exp(-ae[1] * r);
+      w1 = -ae[1] * w0;
+      w2 = -ae[1] * w1;
+    }
+  }
+  const int ea = cs.slm_a[l], eb = cs.slm_b[l], ec = cs.slm_c[l];
+  const double k = cs.slm_k[l];
+  const double *X = q + 13, *Y = q + 18, *Z = q + 23;
+  const double y = k * X[ea] * Y[eb] * Z[ec];
+  out(m, 0, y * w0);
+  if (IDER >= 1) {
+    const double dy0 = ea ? k * ea * X[ea - 1] * Y[eb] * Z[ec] : 0.0;
+    const double dy1 = eb ? k * eb * X[ea] * Y[eb - 1] * Z[ec] : 0.0;
+    const double dy2 = ec ? k * ec * X[ea] * Y[eb] * Z[ec - 1] : 0.0;
+    const double xr0 = q[0] * ri, xr1 = q[1] * ri, xr2 = q[2] * ri;
+    out(m, 1, y * xr0 * w1 + dy0 * w0);
+    out(m, 2, y * xr1 * w1 + dy1 * w0);
+    out(m, 3, y * xr2 * w1 + dy2 * w0);
+    if (IDER >= 2) {
+      double lap = 0;
+      if (ea >= 2) lap += k * ea * (ea - 1) * X[ea - 2] * Y[eb] * Z[ec];
+      if (eb >= 2) lap += k * eb * (eb - 1) * X[ea] * Y[eb - 2] * Z[ec];
+      if (ec >= 2) lap += k * ec * (ec - 1) * X[ea] * Y[eb] * Z[ec - 2];
+      const double dum = dy0 * xr0 + dy1 * xr1 + dy2 * xr2;
+      double d2 = y * w2 + y * 2.0 * ri * w1 + lap * w0;
+      d2 += 2.0 * dum * w1;
+      out(m, 4, d2);
     }
   }
 }

@@ -34,7 +34,8 @@ struct cw_ctx {
   MoveBuf mb{};
   HBuf hb{};
   std::vector<void *> w_allocs;
-  size_t smem_jmove = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0;
+  size_t smem_jmove = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
+  int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
   double ecum1s = 0, ecm21s = 0;
@@ -208,9 +209,10 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
   const int ec = c->hb.chunk;
   for (int e0 = 0; e0 < N; e0 += ec) {
     const int ne = std::min(ec, N - e0);
-    const long nt = (long)W * ne * M;
+    const long nwarps = (long)W * ne;
+    const int bw = c->basis_warps;
     stage_begin(c, CW_ST_BASIS_ALL);
-    k_basis_all<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->hb, c->g, e0, ne);
     stage_end(c);
     LCHK("k_basis_all");
     stage_begin(c, CW_ST_LCAO_ALL);
@@ -453,6 +455,28 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     for (int iord = 2; iord <= d->nordb; iord++) v += bb[iord] * std::pow(h.asymp_r, iord);
     h.asymp_jasb[i] = v;
   }
+  {
+    // Slm monomials (vmc/slm.f90 index table)
+    static const int A[36] = {0, 0, 1, 0, 0, 2, 1, 1, 0, 0, 0, 3, 2, 2, 1, 1, 1, 0, 0, 0, 0,
+                              4, 3, 3, 2, 2, 2, 1, 1, 1, 1, 0, 0, 0, 0, 0};
+    static const int B[36] = {0, 0, 0, 1, 0, 0, 1, 0, 2, 1, 0, 0, 1, 0, 2, 1, 0, 3, 2, 1, 0,
+                              0, 1, 0, 2, 1, 0, 3, 2, 1, 0, 4, 3, 2, 1, 0};
+    static const int Cz[36] = {0, 0, 0, 0, 1, 0, 0, 1, 0, 1, 2, 0, 0, 1, 0, 1, 2, 0, 1, 2, 3,
+                               0, 0, 1, 0, 1, 2, 0, 1, 2, 3, 0, 1, 2, 3, 4};
+    const double cs_ = 0.28209479177387814, cp = 0.48860251190291992, cd1 = 0.630783130505040,
+                 cd2 = 1.092548430592079, cf = 0.74635266518023078, cf2 = 1.66889529453113635,
+                 cf3 = 2.89061144264055405, cg = 0.8462843753216345, cg2 = 2.2390579955406924,
+                 cg3 = 2.890611442640554, cg4 = 5.006685883593409;
+    const double K_[36] = {0,   cs_, cp,  cp,  cp,  cd1, cd2, cd2, cd1, cd2, cd1, cf,
+                           cf2, cf2, cf2, cf3, cf2, cf,  cf2, cf2, cf,  cg,  cg2, cg2,
+                           cg3, cg4, cg3, cg2, cg4, cg4, cg2, cg,  cg2, cg3, cg2, cg};
+    for (int l = 0; l < 36; l++) {
+      h.slm_a[l] = A[l];
+      h.slm_b[l] = B[l];
+      h.slm_c[l] = Cz[l];
+      h.slm_k[l] = K_[l];
+    }
+  }
   CK(cudaMemcpyToSymbol(cs, &h, sizeof(CSys)));
   // global tables
   auto &L = c->sys_allocs;
@@ -491,6 +515,20 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(cudaMemcpy(gridpow, gpw.data(), gpw.size() * sizeof(double), cudaMemcpyHostToDevice));
   c->g.rwf = rwf; c->g.d2rwf = d2rwf; c->g.iwlbas = iwl; c->g.iwrwf = iwr; c->g.coefT = coefT; c->g.slot_orb = slot;
   c->g.gridpow = gridpow;
+  std::vector<int4> aot(d->nbasis);
+  for (int ic = 0; ic < d->ncent; ic++) {
+    const int it = d->iwctype[ic];
+    for (int ib = 0; ib < d->nbastyp[it]; ib++) {
+      const int mm = h.ao_first[ic] + ib;
+      aot[mm] = make_int4(ic, d->iwrwf[it * d->mbastyp + ib] - 1, it, d->iwlbas[it * d->mbastyp + ib]);
+      if (aot[mm].w < 1 || aot[mm].w > 35 || aot[mm].y < 0 || aot[mm].y >= d->nrbas[it])
+        return fail(c, CW_ERR_ARG, "basis pointer out of range (centre %d, AO %d)", ic, ib);
+    }
+  }
+  int4 *aodev;
+  DALLOC(L, aodev, aot.size());
+  CK(cudaMemcpy(aodev, aot.data(), aot.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  c->g.ao = aodev;
   // dynamic shared memory sizes
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
@@ -504,9 +542,15 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   c->smem_ctil = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64);
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
-    c->smem_ecp = sizeof(double) * ((size_t)h.N * h.M + 3 * h.N + 4 * h.M + (size_t)h.nquad * h.K +
-                                    (size_t)h.nquad * h.M + (size_t)h.nquad * h.M * 2 * ((een_nb(nord) + 1) / 2) + 1);
+    c->smem_ecp = sizeof(double) * ((size_t)h.N * h.M + 3 * h.N + 4 * h.M + (size_t)h.nquad * h.M +
+                                    (size_t)h.nquad * h.M * 2 * ((een_nb(nord) + 1) / 2) + 1 +
+                                    (size_t)h.nquad * h.M * kCenRec);
   }
+  // warp-per-point basis kernels: as many warps per block as 4 records fit
+  c->basis_warps = (int)std::max<size_t>(1, std::min<size_t>(4, (160 * 1024) / ((size_t)h.M * kCenRec * sizeof(double))));
+  c->smem_basis = (size_t)c->basis_warps * h.M * kCenRec * sizeof(double);
+  CK(cudaFuncSetAttribute(k_basis_move, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_basis));
+  CK(cudaFuncSetAttribute(k_basis_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_basis));
   CK(cudaFuncSetAttribute(k_slater_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_sinv));
   CK(cudaFuncSetAttribute(k_ctilde, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ctil));
   int rc = nord_attrs(c);
@@ -619,9 +663,9 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
       NORD_DISPATCH(launch_jmove, c, i);
       stage_end(c);
       LCHK("k_jastrow_move");
-      const long nt = (long)W * h.M;
+      const int bw = c->basis_warps;
       stage_begin(c, CW_ST_BASIS_MOVE);
-      k_basis_move<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->mb, c->g);
+      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
       stage_end(c);
       LCHK("k_basis_move");
       stage_begin(c, CW_ST_LCAO_MOVE);
@@ -753,8 +797,9 @@ int cw_orbitals(cw_ctx *c, double *orb, double *dorb, double *ddorb) {
   std::vector<double> buf;
   for (int e0 = 0; e0 < N; e0 += ec) {
     const int ne = std::min(ec, N - e0);
-    const long nt = (long)W * ne * M;
-    k_basis_all<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    const long nwarps = (long)W * ne;
+    const int bw = c->basis_warps;
+    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->hb, c->g, e0, ne);
     LCHK("k_basis_all");
     dgemm(c->stream, W * ne * 5, Oa, K, c->hb.phi, c->g.coefT, c->hb.orball);
     LCHK("dgemm(all)");

@@ -215,23 +215,24 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
 }
 
 // ---------------------------------------------------------------------------
-// basis functions with Laplacian for electrons [e0, e0+ne): thread per
-// (walker, electron, centre); rows ((w*ne + e)*5 + d).
+// basis functions with Laplacian for electrons [e0, e0+ne): warp per
+// (walker, electron); rows ((w*ne + e)*5 + d).
 // ---------------------------------------------------------------------------
 __global__ void k_basis_all(WState st, HBuf hb, GSys g, int e0, int ne) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int M = cs.M, K = cs.K, N = cs.N;
-  if (t >= (long)st.W * ne * M) return;
-  const int ic = (int)(t % M);
-  const long we = t / M;
-  const int el = (int)(we % ne);
-  const int w = (int)(we / ne);
-  const int e = e0 + el;
-  const double xc[3] = {st.x[((size_t)w * 3 + 0) * N + e] - cs.cent[3 * ic],
-                        st.x[((size_t)w * 3 + 1) * N + e] - cs.cent[3 * ic + 1],
-                        st.x[((size_t)w * 3 + 2) * N + e] - cs.cent[3 * ic + 2]};
-  double *phi = hb.phi + ((size_t)we * 5) * K;
-  basis_centre(g, ic, xc, 2, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
+  extern __shared__ __align__(16) double smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int K = cs.K, N = cs.N;
+  if (gw >= (long)st.W * ne) return;
+  const int el = (int)(gw % ne), w = (int)(gw / ne), e = e0 + el;
+  const double x[3] = {st.x[((size_t)w * 3 + 0) * N + e], st.x[((size_t)w * 3 + 1) * N + e],
+                       st.x[((size_t)w * 3 + 2) * N + e]};
+  double *rec = smem + (size_t)wib * cs.M * kCenRec;
+  warp_basis_prepass<2>(g, x, rec, lane);
+  __syncwarp();
+  double *phi = hb.phi + ((size_t)gw * 5) * K;
+  for (int m = lane; m < K; m += 32)
+    warp_basis_ao<2>(g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
 }
 
 __global__ void k_scatter_orbs(WState st, HBuf hb, GSys g, int e0, int ne) {
@@ -483,13 +484,13 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
   double *rr_en = smem;                 // [N][M] scaled e-n distances
   double *sx = rr_en + N * M;           // [3][N]
   double *vps = sx + 3 * N;             // [M][4] channel potentials of the current electron
-  double *phiq = vps + 4 * M;           // [NQ][K]
-  double *rrq = phiq + (size_t)NQ * K;  // [NQ][M]
+  double *rrq = vps + 4 * M;            // [NQ][M]
   constexpr int NB = 2 * ((een_nb(NORD) + 1) / 2);
   // [NQ][M][NB] folded e-e-n coefficients of the point; 16-byte aligned for
   // the vector loads of een_apply0 (NB is even)
   const size_t bq_off = (((size_t)(rrq - smem) + (size_t)NQ * M) + 1) & ~(size_t)1;
   double *bq = smem + bq_off;
+  double *recq = bq + (size_t)NQ * M * NB;  // [NQ][M][kCenRec] basis prepass of the point
   __shared__ int s_act[CW_MAX_CENT];
   __shared__ int s_nact;
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
@@ -539,24 +540,27 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
       const double xqq = xqw[q], yqq = xqw[NQ + q], zqq = xqw[2 * NQ + q];
       const double costh = (ri_v[0] * xqq + ri_v[1] * yqq + ri_v[2] * zqq) * (1.0 / rin);
       const double xp[3] = {rin * xqq + cs.cent[3 * ic], rin * yqq + cs.cent[3 * ic + 1], rin * zqq + cs.cent[3 * ic + 2]};
-      double *ph = phiq + (size_t)q * K;
       double *rq = rrq + (size_t)q * M;
-      // distance_quad + basis values at the quadrature point (ider=0)
+      double *rec = recq + (size_t)q * M * kCenRec;
+      // distance_quad (r_en_quad(iq,ic) = r_en(i,ic)) and the folded e-e-n
+      // coefficients of the point
       for (int jc = lane; jc < M; jc += 32) {
         double xc[3] = {xp[0] - cs.cent[3 * jc], xp[1] - cs.cent[3 * jc + 1], xp[2] - cs.cent[3 * jc + 2]};
         double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
-        if (jc == ic) r = rin;  // r_en_quad(iq,ic) = r_en(i,ic)
+        if (jc == ic) r = rin;
         rq[jc] = scale0<double>(r);
         if (NORD > 1)
           een_fold0<NORD, double>(&cs.c[cs.iwctype[jc] * CW_MAX_TERMS], 1 - cs.scalek * rq[jc],
                                   bq + ((size_t)q * M + jc) * NB);
-        basis_centre(g, jc, xc, 0, [&](int m, int d, double v) { if (d == 0) ph[m] = v; });
       }
+      warp_basis_prepass<0>(g, xp, rec, lane);
       __syncwarp();
-      // determinant ratio (nonlocd_quad) via c~
+      // determinant ratio (nonlocd_quad) via c~: basis values (ider=0) of the
+      // point contracted on the fly
       const double *ct = hb.ctilde + ((size_t)w * N + i) * K;
       double dr = 0;
-      for (int m = lane; m < K; m += 32) dr += ph[m] * ct[m];
+      for (int m = lane; m < K; m += 32)
+        warp_basis_ao<0>(g, rec, m, [&](int, int, double v) { dr += v * ct[m]; });
       dr = warp_sum(dr);
       // Jastrow ratio (nonlocj_quad4)
       double fsum = 0;

@@ -387,24 +387,28 @@ __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
 }
 
 // ---------------------------------------------------------------------------
-// Basis functions of the moved electron: thread per (walker, centre).
+// Basis functions of the moved electron (basis_fns ider=1): warp per walker,
+// per-centre prepass then lanes over AOs.
 // ---------------------------------------------------------------------------
 __global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int M = cs.M, K = cs.K;
-  if (t >= (long)st.W * M) return;
-  const int w = (int)(t / M), ic = (int)(t % M);
-  const MoveScratch &m = mb.ms[w];
+  extern __shared__ __align__(16) double smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= st.W) return;
+  const int K = cs.K;
+  const MoveScratch &mv = mb.ms[w];
   double *phi = mb.phi + (size_t)w * 4 * K;
-  if (m.igeo) {
+  if (mv.igeo) {
     // the GEMM still reads these rows: keep them finite
-    const int m0 = cs.ao_first[ic], m1 = cs.ao_first[ic + 1];
-    for (int a = m0; a < m1; a++)
-      for (int d = 0; d < 4; d++) phi[(size_t)d * K + a] = 0.0;
+    for (int t = lane; t < 4 * K; t += 32) phi[t] = 0.0;
     return;
   }
-  const double xc[3] = {m.xnew[0] - cs.cent[3 * ic], m.xnew[1] - cs.cent[3 * ic + 1], m.xnew[2] - cs.cent[3 * ic + 2]};
-  basis_centre(g, ic, xc, 1, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
+  double *rec = smem + (size_t)wib * cs.M * kCenRec;
+  const double x[3] = {mv.xnew[0], mv.xnew[1], mv.xnew[2]};
+  warp_basis_prepass<1>(g, x, rec, lane);
+  __syncwarp();
+  for (int m = lane; m < K; m += 32)
+    warp_basis_ao<1>(g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
 }
 
 // ---------------------------------------------------------------------------
