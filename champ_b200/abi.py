@@ -114,7 +114,14 @@ def load_engine(path: str | None = None):
     lib.cw_fma_peak.restype = C.c_int
     lib.cw_rng_states.argtypes = [C.POINTER(C.c_int32), C.c_int, C.POINTER(C.c_uint64)]
     lib.cw_sites.argtypes = [C.POINTER(CwSystemDesc), C.c_int, C.POINTER(C.c_uint64), _dp]
-    for f in ("cw_rng_states", "cw_sites", "cw_sync", "cw_set_walkers", "cw_get_walkers", "cw_vmc_steps", "cw_end_block",
+    lib.cw_dmc_init.argtypes = [V, C.c_int, C.c_int, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                C.c_double, C.c_double, C.c_int]
+    lib.cw_dmc_steps.argtypes = [V, C.c_int]
+    lib.cw_dmc_end_block.argtypes = [V]
+    lib.cw_dmc_results.argtypes = [V, _dp]
+    lib.cw_dmc_walkers.argtypes = [V, C.POINTER(C.c_int), _dp, _dp, _dp, C.POINTER(C.c_uint64)]
+    for f in ("cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
+              "cw_rng_states", "cw_sites", "cw_sync", "cw_set_walkers", "cw_get_walkers", "cw_vmc_steps", "cw_end_block",
               "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow", "cw_slater",
               "cw_get_sums", "cw_get_state"):
         getattr(lib, f).restype = C.c_int
@@ -128,6 +135,7 @@ EXPORTED_SYMBOLS = [
     "cw_vmc_steps", "cw_end_block", "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow",
     "cw_slater", "cw_get_sums", "cw_get_state", "cw_last_ms", "cw_rng_states", "cw_sites",
     "cw_launches", "cw_profile", "cw_stage_times", "cw_fma_peak", "cw_orbitals_noalloc",
+    "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
-          "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit"]
+          "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj"]

@@ -131,7 +131,7 @@ __device__ __forceinline__ float warp_sumf(float v) {
 // xoshiro256** (CHAMP vmc/xoroshiro256starstar.c next / next_uniform_double)
 struct DRng {
   uint64_t s0, s1, s2, s3;
-  __device__ __forceinline__ uint64_t next() {
+  __host__ __device__ __forceinline__ uint64_t next() {
     const uint64_t r1 = s1 * 5;
     const uint64_t result = ((r1 << 7) | (r1 >> 57)) * 9;
     const uint64_t t = s1 << 17;
@@ -143,9 +143,9 @@ struct DRng {
     s3 = (s3 << 45) | (s3 >> 19);
     return result;
   }
-  __device__ __forceinline__ double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }
-  __device__ void load(const uint64_t *p) { s0 = p[0]; s1 = p[1]; s2 = p[2]; s3 = p[3]; }
-  __device__ void store(uint64_t *p) const { p[0] = s0; p[1] = s1; p[2] = s2; p[3] = s3; }
+  __host__ __device__ __forceinline__ double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }
+  __host__ __device__ void load(const uint64_t *p) { s0 = p[0]; s1 = p[1]; s2 = p[2]; s3 = p[3]; }
+  __host__ __device__ void store(uint64_t *p) const { p[0] = s0; p[1] = s1; p[2] = s2; p[3] = s3; }
 };
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,249 @@
+// dmc.cuh — diffusion Monte Carlo step of every walker: dmc_ps
+// (dmc/dmc_ps_mov1.f90:4) with the reweighting of dmc/branching.f90 (icut_e=0,
+// icut_br=0: the ECP branch of dmc_eloc_cutoff, fratio-scaled energies).
+//
+//   k_dmc_propose   drift-diffusion proposal of electron iel (:293-318)
+//   (k_jastrow_move, k_basis_move, LCAO GEMM and k_commit are shared with VMC)
+//   k_dmc_decide    Green-function acceptance, node crossings, age boost
+//                   (:340-435)
+//   k_dmc_weights   drift of every electron after hpsi (:516), fratio,
+//                   reweight, per-walker sums of the step (:520-673)
+//   k_set_quad      the step's quadrature rotation, shared by the population
+//   k_walker_copy   walker copies of splitj (dmc/splitj.f90), CTA per copy
+#pragma once
+#include "common.cuh"
+
+namespace cw {
+
+struct DmcBuf {
+  double *vold;     // [cap][3][N] drift of every electron (vold_dmc)
+  double *wt;       // [cap]
+  double *fratio;   // [cap]
+  int *iage;        // [cap]
+  double *eprev;    // [cap] eold at the start of the step
+  double *acc;      // [cap][DA_NA] per-walker sums of one step
+  int *copy_src;    // [cap]
+  int *copy_dst;    // [cap]
+};
+
+// per-walker sums of one step (reduced on the host in walker order)
+enum {
+  DA_DFUS2AC = 0, DA_DFUS2UN, DA_DFUS2O, DA_IACCEPT, DA_ACC, DA_TRY, DA_NACC, DA_NODECR,
+  DA_WSUM1, DA_ESUM1, DA_PESUM, DA_TPBSUM, DA_TAUSUM, DA_NA = 16
+};
+
+struct DmcScalars {
+  double tau, etrial, eest, ffi, fprod;
+};
+
+__device__ __forceinline__ double gauss_d(DRng &r) {
+  // gauss (vmc/gauss.f90:3): one normal deviate, the cosine draw first
+  const double twopi = 6.283185307179586231995926937088370323181152343750;
+  const double g = cos(twopi * r.uniform());
+  return g * sqrt(-2 * log(r.uniform()));
+}
+
+// drift of electron e: slmi row · dorbs + vj (compute_determinante_grad
+// iflag_move=1)
+__device__ __forceinline__ void drift_old(const WState &st, int w, int e, double v[3]) {
+  const int N = cs.N, nmax = cs.nmax;
+  const int iab = e < cs.nup ? 0 : 1, nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
+  const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * (e - ish);
+  double g0 = 0, g1 = 0, g2 = 0;
+  for (int j = 0; j < nel; j++) {
+    const double s = sl[j];
+    g0 += s * st.dorbs[(((size_t)w * 3 + 0) * N + e) * nmax + j];
+    g1 += s * st.dorbs[(((size_t)w * 3 + 1) * N + e) * nmax + j];
+    g2 += s * st.dorbs[(((size_t)w * 3 + 2) * N + e) * nmax + j];
+  }
+  const double *fjo = st.fjo + (size_t)w * 3 * N;
+  v[0] = 0.0 + g0 + fjo[e];
+  v[1] = 0.0 + g1 + fjo[N + e];
+  v[2] = 0.0 + g2 + fjo[2 * N + e];
+}
+
+// thread per walker: drift + Gaussian diffusion of electron iel
+__global__ void k_dmc_propose(WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, int iel) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N;
+  double vo[3];
+  drift_old(st, w, iel, vo);
+  for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + iel] = vo[k];
+  const double tau = sc.tau, rttau = sqrt(tau), adrift = 0.5;
+  const double v2old = vo[0] * vo[0] + vo[1] * vo[1] + vo[2] * vo[2];
+  const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2old * tau) - 1.0) / (adrift * v2old);
+  DRng rng;
+  rng.load(st.rng + 4 * (size_t)w);
+  double dfus2o = 0;
+  MoveScratch &m = mb.ms[w];
+  for (int k = 0; k < 3; k++) {
+    const double drift = vavvt * vo[k];
+    const double dfus = gauss_d(rng) * rttau;
+    const double dx = drift + dfus;
+    dfus2o += dfus * dfus;
+    m.xnew[k] = st.x[((size_t)w * 3 + k) * N + iel] + dx;
+  }
+  rng.store(st.rng + 4 * (size_t)w);
+  m.igeo = 0;
+  db.acc[(size_t)w * DA_NA + DA_DFUS2O] = dfus2o;
+}
+
+// thread per walker: ratio and drift at the new point, reverse diffusion,
+// acceptance p = |psi_n/psi_o|^2 G(o<-n)/G(n<-o) with the age boost
+__global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalars sc, int iel) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
+  const int iab = iel < cs.nup ? 0 : 1, nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
+  MoveScratch &m = mb.ms[w];
+  const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * (iel - ish);
+  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const int *slot = g.slot_orb + iab * nmax;
+  double *acc = db.acc + (size_t)w * DA_NA;
+  const double tau = sc.tau, adrift = 0.5;
+  double ratio = 0;
+  for (int j = 0; j < nel; j++) ratio += sl[j] * orbn[slot[j]];
+  const double detn = st.detiab[2 * w + iab] * ratio;
+  const double psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
+  const double psijn = mb.fsumn[w];
+  double vn[3] = {0, 0, 0};
+  if (detn != 0.0) {
+    double v0 = 0, v1 = 0, v2 = 0;
+    for (int j = 0; j < nel; j++) {
+      const double s = sl[j] / ratio;
+      v0 += s * orbn[1 * Oa + slot[j]];
+      v1 += s * orbn[2 * Oa + slot[j]];
+      v2 += s * orbn[3 * Oa + slot[j]];
+    }
+    vn[0] = 0.0 + v0 + mb.vjn[3 * w + 0];
+    vn[1] = 0.0 + v1 + mb.vjn[3 * w + 1];
+    vn[2] = 0.0 + v2 + mb.vjn[3 * w + 2];
+  }
+  const double psido = st.psido[w], psijo = st.psijo[w];
+  if (psidn * psido <= 0.0) acc[DA_NODECR] += 1;  // icross=1: counted, the move is not refused
+  const double v2new = vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2];
+  const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2new * tau) - 1.0) / (adrift * v2new);
+  double dfus2n = 0;
+  for (int k = 0; k < 3; k++) {
+    const double xbac = m.xnew[k] + vavvt * vn[k];
+    const double dfus = xbac - st.x[((size_t)w * 3 + k) * N + iel];
+    dfus2n += dfus * dfus;
+  }
+  const double dfus2o = acc[DA_DFUS2O];
+  double p = (psidn / psido) * (psidn / psido) * exp(2 * (psijn - psijo)) * exp((dfus2o - dfus2n) / (2.0 * tau)) * 1.0;
+  const int age = db.iage[w];
+  if (age > 50) p = p * pow(1.1, (double)(age - 50));
+  p = fmin(1.0, p);
+  acc[DA_ACC] += p;
+  acc[DA_TRY] += 1;
+  acc[DA_DFUS2AC] += p * dfus2o;
+  acc[DA_DFUS2UN] += dfus2o;
+  DRng rng;
+  rng.load(st.rng + 4 * (size_t)w);
+  const int a = (rng.uniform() < p) ? 1 : 0;
+  rng.store(st.rng + 4 * (size_t)w);
+  m.acc = a;
+  m.ratio = ratio;
+  if (a) {
+    acc[DA_IACCEPT] = 1;
+    acc[DA_NACC] += 1;
+    db.iage[w] = 0;
+    for (int k = 0; k < 3; k++) st.x[((size_t)w * 3 + k) * N + iel] = m.xnew[k];
+    st.psido[w] = psidn;
+    st.psijo[w] = psijn;
+    st.fsumo[w] = psijn;
+    st.detiab[2 * w + iab] = detn;
+  }
+}
+
+// Warp per walker, after hpsi: drift of every electron, fratio
+// (dmc_eloc_cutoff, nloc>0 branch), and for mode 1 the reweighting
+// (calculate_reweight) and the walker's sums of the step.
+__global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= st.W) return;
+  const int N = cs.N;
+  const double tau = sc.tau, adrift = 0.5;
+  double vav2sum = 0, v2sum = 0;
+  for (int e = lane; e < N; e += 32) {
+    double v[3];
+    drift_old(st, w, e, v);
+    for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + e] = v[k];
+    const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2 * tau * 1.0) - 1.0) / (adrift * v2);
+    const double vavvn = vavvt / (tau * 1.0);
+    vav2sum += vavvn * vavvn * v2;
+    v2sum += v2;
+  }
+  vav2sum = warp_sum(vav2sum);
+  v2sum = warp_sum(v2sum);
+  if (lane != 0) return;
+  const double fration = sqrt(vav2sum / v2sum);
+  if (mode == 0) {
+    db.fratio[w] = fration;
+    return;
+  }
+  double *acc = db.acc + (size_t)w * DA_NA;
+  const double taunow = tau * acc[DA_DFUS2AC] / acc[DA_DFUS2UN] * 1.0;
+  const double enew = st.eold[w];  // hpsi of this step
+  const double eold = db.eprev[w];
+  const double deo = sc.eest - eold, den = sc.eest - enew;
+  const double ewto = sc.eest - deo * db.fratio[w];
+  const double ewtn = sc.eest - den * fration;
+  double dwt = exp((sc.etrial - 0.5 * (ewto + ewtn)) * taunow);
+  dwt = dwt * sc.ffi;
+  const double wt = db.wt[w] * dwt;
+  db.wt[w] = wt;
+  const double wtg = wt * sc.fprod;
+  acc[DA_TAUSUM] = wtg * taunow;
+  db.fratio[w] = fration;
+  if (acc[DA_IACCEPT] == 0) db.iage[w] += 1;
+  const double ekino = st.ekino[w];
+  acc[DA_WSUM1] = wt;
+  acc[DA_ESUM1] = wt * enew;
+  acc[DA_PESUM] = wtg * (enew - ekino);
+  acc[DA_TPBSUM] = wtg * ekino;
+}
+
+struct QuadRot {
+  double x[CW_MAX_QUAD], y[CW_MAX_QUAD], z[CW_MAX_QUAD];
+};
+
+__global__ void k_set_quad(WState st, QuadRot q) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  const int NQ = cs.nquad;
+  double *xq = st.xq + (size_t)w * 3 * NQ;
+  for (int i = 0; i < NQ; i++) {
+    xq[i] = q.x[i];
+    xq[NQ + i] = q.y[i];
+    xq[2 * NQ + i] = q.z[i];
+  }
+}
+
+// Per-walker fields of a splitj copy: every array the next step reads
+// (configuration, wave-function tables, drift, fratio) except the random
+// stream, which stays with its slot.
+struct WalkerRec {
+  int nfield;
+  double *ptr[20];
+  long len[20];  // doubles per walker
+};
+
+// CTA per copy: walker copy_src[c] -> slot copy_dst[c].  The host guarantees
+// that no source slot is also a destination, so copies run concurrently.
+__global__ void k_walker_copy(WalkerRec rec, DmcBuf db, int ncopy) {
+  const int c = blockIdx.x;
+  if (c >= ncopy) return;
+  const int src = db.copy_src[c], dst = db.copy_dst[c];
+  for (int f = 0; f < rec.nfield; f++) {
+    const long n = rec.len[f];
+    const double *p = rec.ptr[f] + (size_t)src * n;
+    double *q = rec.ptr[f] + (size_t)dst * n;
+    for (long t = threadIdx.x; t < n; t += blockDim.x) q[t] = p[t];
+  }
+}
+
+}  // namespace cw

@@ -15,10 +15,31 @@
 #include "gemm.cuh"
 #include "hpsi.cuh"
 #include "move.cuh"
+#include "dmc.cuh"
 #include "peak.cuh"
 
 
 using namespace cw;
+
+// Host side of a DMC population (one CHAMP rank's dmc arrays and scalars).
+struct DmcHost {
+  bool on = false;
+  int mwalk = 0, nconf = 0, nfprod = 100;
+  double tau = 0, etrial = 0;
+  DRng pop{};                       // rotqua + splitj stream
+  double eest = 0, eigv = 1, wdsumo = 0, fprod = 1;
+  std::vector<double> ff;           // ff(0:nfprod-1)
+  long ipass = 0;
+  double wsum1 = 0, esum1 = 0, pesum = 0, tpbsum = 0, tausum = 0;
+  double wgsum = 0, egsum = 0, wgcum = 0, egcum = 0, wgcm2 = 0, egcm2 = 0, taucum = 0;
+  double pecum = 0, tpbcum = 0, acc = 0, trymove = 0;
+  long nacc = 0, nodecr = 0, nbrnch = 0, iblk = 0;
+  DmcBuf db{};
+  std::vector<void *> allocs;
+  double *h_acc = nullptr, *h_wt = nullptr;   // pinned, [mwalk][DA_NA] and [mwalk]
+  int *h_iage = nullptr, *h_copy = nullptr;   // pinned, [mwalk] and [2][mwalk]
+  WalkerRec rec{};
+};
 
 struct cw_ctx {
   int device = 0, precision = 0;
@@ -49,6 +70,7 @@ struct cw_ctx {
   size_t evused = 0;
   double stage_ms[CW_NSTAGE] = {0};
   long stage_n[CW_NSTAGE] = {0};
+  DmcHost dmc;
 };
 
 namespace {
@@ -258,7 +280,16 @@ int check_status(cw_ctx *c) {
   return CW_OK;
 }
 
+void free_dmc(cw_ctx *c) {
+  DmcHost &d = c->dmc;
+  free_list(d.allocs);
+  for (void *p : {(void *)d.h_acc, (void *)d.h_wt, (void *)d.h_iage, (void *)d.h_copy})
+    if (p) cudaFreeHost(p);
+  d = DmcHost();
+}
+
 int alloc_walkers(cw_ctx *c, int W) {
+  free_dmc(c);
   free_list(c->w_allocs);
   const CSys &h = c->h;
   const int N = h.N, M = h.M, K = h.K, Oa = h.Oa, nmax = h.nmax, NQ = std::max(h.nquad, 1);
@@ -562,6 +593,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
 void cw_destroy(cw_ctx *c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  free_dmc(c);
   free_list(c->w_allocs);
   free_list(c->sys_allocs);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1046,5 +1078,352 @@ extern "C" int cw_orbitals_noalloc(cw_ctx *c, int npts, const double *xyz, doubl
   LCHK("k_basis_points");
   dgemm(c->stream, npts * 5, h.Oa, h.K, phi, c->g.coefT, out);
   LCHK("dgemm(noalloc)");
+  return CW_OK;
+}
+
+// ===========================================================================
+// Diffusion Monte Carlo: one population per context (CHAMP's per-rank dmc
+// arrays).  Walker slots 0..mwalk-1 live in the walker arrays allocated for
+// mwalk; kernels run over the nwalk active ones.
+// ===========================================================================
+namespace {
+
+// splitj (dmc/splitj.f90:3) on the host weights and ages: pairs small
+// weights, splits weights >= 2 and compacts the population.  Appends the
+// (source, destination) slot copies in CHAMP's order; returns the new nwalk
+// or -1 when mwalk would be exceeded.
+int splitj_host(DmcHost &d, int nwalk, std::vector<std::pair<int, int>> &copies) {
+  double *wt = d.h_wt;
+  int *iage = d.h_iage;
+  std::vector<int> iwundr;
+  int ipair = 0, iw2 = 0;
+  for (int iw = 0; iw < nwalk; iw++) {
+    if (wt[iw] < 0.5) {
+      if (wt[iw] == 0.0) {
+        d.nbrnch++;
+        iwundr.push_back(iw);
+      } else if (ipair == 0) {
+        ipair = 1;
+        iw2 = iw;
+      } else {
+        d.nbrnch++;
+        ipair = 0;
+        const double wttot = wt[iw] + wt[iw2];
+        if (d.pop.uniform() > (wt[iw] / wttot)) {
+          wt[iw2] = wttot;
+          iwundr.push_back(iw);
+        } else {
+          wt[iw] = wttot;
+          iwundr.push_back(iw2);
+        }
+      }
+    }
+  }
+  int nwalk2 = nwalk;
+  for (int iw = 0; iw < nwalk; iw++) {
+    if (wt[iw] >= 2.0) {
+      d.nbrnch++;
+      int dst;
+      if (!iwundr.empty()) {
+        dst = iwundr.back();
+        iwundr.pop_back();
+      } else {
+        dst = nwalk2++;
+        if (nwalk2 > d.mwalk) return -1;
+      }
+      wt[iw] = wt[iw] * 0.5;
+      wt[dst] = wt[iw];
+      iage[dst] = iage[iw];
+      copies.emplace_back(iw, dst);
+    }
+  }
+  for (int j = (int)iwundr.size() - 1; j >= 0; j--) {
+    const int dst = iwundr[j], src = nwalk2 - 1;
+    nwalk2--;
+    wt[dst] = wt[src];
+    iage[dst] = iage[src];
+    copies.emplace_back(src, dst);
+  }
+  return nwalk2;
+}
+
+void add_field(WalkerRec &r, double *p, long len) {
+  r.ptr[r.nfield] = p;
+  r.len[r.nfield] = len;
+  r.nfield++;
+}
+
+}  // namespace
+
+extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, const uint64_t *rng,
+                           const uint64_t *pop_rng, double tau, double etrial, int nfprod) {
+  if (!c || nwalk <= 0 || mwalk < nwalk || !x || !rng || !pop_rng || !(tau > 0) || nfprod < 1)
+    return fail(c, CW_ERR_ARG, "cw_dmc_init: bad arguments");
+  if (c->h.nloc == 0)
+    return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: all-electron DMC (dmc_ae) is not implemented; nloc > 0 required");
+  CK(cudaSetDevice(c->device));
+  int rc = alloc_walkers(c, mwalk);
+  if (rc) return rc;
+  const CSys &h = c->h;
+  const int N = h.N, nmax = h.nmax;
+  DmcHost &d = c->dmc;
+  DmcBuf &b = d.db;
+  DALLOC(d.allocs, b.vold, (size_t)mwalk * 3 * N);
+  DALLOC(d.allocs, b.wt, mwalk);
+  DALLOC(d.allocs, b.fratio, mwalk);
+  DALLOC(d.allocs, b.iage, mwalk);
+  DALLOC(d.allocs, b.eprev, mwalk);
+  DALLOC(d.allocs, b.acc, (size_t)mwalk * DA_NA);
+  DALLOC(d.allocs, b.copy_src, mwalk);
+  DALLOC(d.allocs, b.copy_dst, mwalk);
+  CK(cudaMallocHost((void **)&d.h_acc, sizeof(double) * mwalk * DA_NA));
+  CK(cudaMallocHost((void **)&d.h_wt, sizeof(double) * mwalk));
+  CK(cudaMallocHost((void **)&d.h_iage, sizeof(int) * mwalk));
+  CK(cudaMallocHost((void **)&d.h_copy, sizeof(int) * 2 * mwalk));
+  // active population
+  c->W = nwalk;
+  c->st.W = nwalk;
+  std::vector<double> xt((size_t)nwalk * 3 * N);
+  for (int w = 0; w < nwalk; w++)
+    for (int e = 0; e < N; e++)
+      for (int k = 0; k < 3; k++) xt[((size_t)w * 3 + k) * N + e] = x[((size_t)w * N + e) * 3 + k];
+  CK(cudaMemcpyAsync(c->st.x, xt.data(), sizeof(double) * xt.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->st.rng, rng, sizeof(uint64_t) * 4 * mwalk, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->st.status, 0, sizeof(int) * mwalk, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // init: hpsi with the unrotated grid, then drift and fratio of every walker
+  rc = zerest(c);
+  if (rc) return rc;
+  d.tau = tau;
+  d.etrial = etrial;
+  d.mwalk = mwalk;
+  d.nconf = nwalk;
+  d.nfprod = nfprod;
+  d.pop.load(pop_rng);
+  d.ff.assign(nfprod, 1.0);
+  d.eigv = 1.0;
+  d.eest = etrial;
+  d.fprod = 1.0;
+  d.wdsumo = nwalk;
+  const DmcScalars sc{tau, etrial, d.eest, 1.0, 1.0};
+  k_dmc_weights<<<(nwalk + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 0);
+  LCHK("k_dmc_weights(init)");
+  for (int w = 0; w < nwalk; w++) d.h_wt[w] = 1.0;
+  CK(cudaMemcpyAsync(b.wt, d.h_wt, sizeof(double) * nwalk, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(b.iage, 0, sizeof(int) * mwalk, c->stream));
+  // walker record of splitj copies
+  WalkerRec &r = d.rec;
+  r.nfield = 0;
+  add_field(r, c->st.x, 3L * N);
+  add_field(r, c->st.psido, 1);
+  add_field(r, c->st.psijo, 1);
+  add_field(r, c->st.psi2o, 1);
+  add_field(r, c->st.eold, 1);
+  add_field(r, c->st.ekino, 1);
+  add_field(r, c->st.slmi, 2L * nmax * nmax);
+  add_field(r, c->st.detiab, 2);
+  add_field(r, c->st.orbs, (long)N * nmax);
+  add_field(r, c->st.dorbs, 3L * N * nmax);
+  add_field(r, c->st.fso, (long)N * N);
+  add_field(r, c->st.fijo, 3L * N * N);
+  add_field(r, c->st.fjo, 3L * N);
+  add_field(r, c->st.fsumo, 1);
+  add_field(r, b.vold, 3L * N);
+  add_field(r, b.fratio, 1);
+  CK(cudaStreamSynchronize(c->stream));
+  d.on = true;
+  return CW_OK;
+}
+
+extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
+  if (!c || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_steps: no DMC population (cw_dmc_init)");
+  CK(cudaSetDevice(c->device));
+  const CSys &h = c->h;
+  DmcHost &d = c->dmc;
+  DmcBuf &b = d.db;
+  c->launches = 0;
+  double total_ms = 0;
+  std::vector<std::pair<int, int>> copies;
+  std::vector<int> origin(d.mwalk), is_src(d.mwalk);
+  for (int s = 0; s < nstep; s++) {
+    const int W = c->W;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    d.ipass++;
+    if (h.nloc > 0) {
+      double f[9];
+      rotqua_frame(d.pop, f);
+      QuadRot q;
+      for (int iq = 0; iq < h.nquad; iq++) {
+        q.x[iq] = h.xq0[iq] * f[0] + h.yq0[iq] * f[3] + h.zq0[iq] * f[6];
+        q.y[iq] = h.xq0[iq] * f[1] + h.yq0[iq] * f[4] + h.zq0[iq] * f[7];
+        q.z[iq] = h.xq0[iq] * f[2] + h.yq0[iq] * f[5] + h.zq0[iq] * f[8];
+      }
+      stage_begin(c, CW_ST_ROTQUA);
+      k_set_quad<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st, q);
+      stage_end(c);
+      LCHK("k_set_quad");
+    }
+    // population control factor (dmc_ps :148-160)
+    const int ipmod = (int)(d.ipass % d.nfprod);
+    const double ginv = std::min(1.0, d.tau);
+    const double ffn = d.eigv * std::pow(d.wdsumo / d.nconf, ginv);
+    const double ffi = 1.0 / ffn;
+    d.fprod = d.fprod * ffn / d.ff[ipmod];
+    d.ff[ipmod] = ffn;
+    const DmcScalars sc{d.tau, d.etrial, d.eest, ffi, d.fprod};
+    CK(cudaMemsetAsync(b.acc, 0, sizeof(double) * W * DA_NA, c->stream));
+    CK(cudaMemcpyAsync(b.eprev, c->st.eold, sizeof(double) * W, cudaMemcpyDeviceToDevice, c->stream));
+    for (int i = 0; i < h.N; i++) {
+      stage_begin(c, CW_ST_PROPOSE);
+      k_dmc_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, b, sc, i);
+      stage_end(c);
+      LCHK("k_dmc_propose");
+      stage_begin(c, CW_ST_JASTROW_MOVE);
+      NORD_DISPATCH(launch_jmove, c, i);
+      stage_end(c);
+      LCHK("k_jastrow_move");
+      const int bw = c->basis_warps;
+      stage_begin(c, CW_ST_BASIS_MOVE);
+      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+      stage_end(c);
+      LCHK("k_basis_move");
+      stage_begin(c, CW_ST_LCAO_MOVE);
+      dgemm(c->stream, W * 4, h.Oa, h.K, c->mb.phi, c->g.coefT, c->mb.orbn);
+      stage_end(c);
+      LCHK("dgemm(move)");
+      stage_begin(c, CW_ST_ACCEPT);
+      k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, b, sc, i);
+      stage_end(c);
+      LCHK("k_dmc_decide");
+      stage_begin(c, CW_ST_COMMIT);
+      k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+      stage_end(c);
+      LCHK("k_commit");
+    }
+    int rc = run_hpsi(c, 0);
+    if (rc) return rc;
+    stage_begin(c, CW_ST_DMC_WEIGHTS);
+    k_dmc_weights<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 1);
+    stage_end(c);
+    LCHK("k_dmc_weights");
+    CK(cudaMemcpyAsync(d.h_acc, b.acc, sizeof(double) * W * DA_NA, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(d.h_wt, b.wt, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(d.h_iage, b.iage, sizeof(int) * W, cudaMemcpyDeviceToHost, c->stream));
+    rc = check_status(c);  // synchronises the stream
+    if (rc) return rc;
+    // the step's sums, in walker order
+    for (int w = 0; w < W; w++) {
+      const double *a = d.h_acc + (size_t)w * DA_NA;
+      d.wsum1 += a[DA_WSUM1];
+      d.esum1 += a[DA_ESUM1];
+      d.pesum += a[DA_PESUM];
+      d.tpbsum += a[DA_TPBSUM];
+      d.tausum += a[DA_TAUSUM];
+      d.acc += a[DA_ACC];
+      d.trymove += a[DA_TRY];
+      d.nacc += (long)a[DA_NACC];
+      d.nodecr += (long)a[DA_NODECR];
+    }
+    const double wgsum1 = d.wsum1 * d.fprod, egsum1 = d.esum1 * d.fprod;
+    // splitj: weights on the host, walker copies on the device
+    copies.clear();
+    const int nwalk2 = splitj_host(d, W, copies);
+    if (nwalk2 < 0) return fail(c, CW_ERR_STATE, "SPLITJ: MWALK exceeded (mwalk=%d)", d.mwalk);
+    for (int k = 0; k < d.mwalk; k++) {
+      origin[k] = k;
+      is_src[k] = 0;
+    }
+    for (auto &cp : copies) origin[cp.second] = origin[cp.first];
+    int ncopy = 0;
+    for (int k = 0; k < nwalk2; k++)
+      if (origin[k] != k) {
+        d.h_copy[ncopy] = origin[k];
+        d.h_copy[d.mwalk + ncopy] = k;
+        is_src[origin[k]] = 1;
+        ncopy++;
+      }
+    for (int k = 0; k < ncopy; k++)
+      if (is_src[d.h_copy[d.mwalk + k]])
+        return fail(c, CW_ERR_STATE, "splitj: slot %d is both a copy source and a destination", d.h_copy[d.mwalk + k]);
+    CK(cudaMemcpyAsync(b.wt, d.h_wt, sizeof(double) * nwalk2, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(b.iage, d.h_iage, sizeof(int) * nwalk2, cudaMemcpyHostToDevice, c->stream));
+    if (ncopy > 0) {
+      CK(cudaMemcpyAsync(b.copy_src, d.h_copy, sizeof(int) * ncopy, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(b.copy_dst, d.h_copy + d.mwalk, sizeof(int) * ncopy, cudaMemcpyHostToDevice, c->stream));
+      stage_begin(c, CW_ST_SPLITJ);
+      k_walker_copy<<<ncopy, 256, 0, c->stream>>>(d.rec, b, ncopy);
+      stage_end(c);
+      LCHK("k_walker_copy");
+    }
+    c->W = nwalk2;
+    c->st.W = nwalk2;
+    // acues1 (dmc/acues1.f90:3)
+    d.wgsum += wgsum1;
+    d.egsum += egsum1;
+    d.eest = (d.egcum + d.egsum) / (d.wgcum + d.wgsum);
+    d.eigv = std::exp((d.etrial - d.eest) * (d.taucum + d.tausum) / (d.wgcum + d.wgsum));
+    d.wdsumo = d.wsum1;
+    d.wsum1 = 0;
+    d.esum1 = 0;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    total_ms += ms;
+    if (c->prof) stage_collect(c);
+  }
+  c->last_ms = total_ms;
+  c->passes += nstep;
+  return CW_OK;
+}
+
+extern "C" int cw_dmc_end_block(cw_ctx *c) {
+  if (!c || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_end_block: no DMC population");
+  DmcHost &d = c->dmc;
+  // acuest (dmc/acuest.f90:112-255): block sums into the cumulative ones
+  const double egnow = d.egsum / d.wgsum;
+  d.egcm2 += d.egsum * egnow;
+  d.wgcm2 += d.wgsum * d.wgsum;
+  d.egcum += d.egsum;
+  d.wgcum += d.wgsum;
+  d.taucum += d.tausum;
+  d.pecum += d.pesum;
+  d.tpbcum += d.tpbsum;
+  d.egsum = d.wgsum = d.tausum = d.pesum = d.tpbsum = 0;
+  d.iblk++;
+  return CW_OK;
+}
+
+extern "C" int cw_dmc_results(cw_ctx *c, double *out) {
+  if (!c || !out || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_results: no DMC population");
+  const DmcHost &d = c->dmc;
+  if (d.iblk == 0) return fail(c, CW_ERR_STATE, "cw_dmc_results: no completed blocks");
+  // finwrt (dmc/finwrt.f90): error with the effective number of blocks
+  const double egave = d.egcum / d.wgcum;
+  const double rn = d.wgcum * d.wgcum / d.wgcm2;
+  const double err = std::sqrt(std::max((d.egcm2 / d.wgcum - egave * egave) / (rn - 1), 0.0));
+  out[0] = egave;
+  out[1] = d.iblk > 1 ? err : 0.0;
+  out[2] = c->W;
+  out[3] = d.eest;
+  out[4] = d.acc / std::max(d.trymove, 1.0);
+  out[5] = d.taucum / d.wgcum;
+  out[6] = d.pecum / d.wgcum;
+  out[7] = d.tpbcum / d.wgcum;
+  out[8] = (double)d.iblk;
+  out[9] = d.fprod;
+  out[10] = d.eigv;
+  out[11] = d.wdsumo;
+  return CW_OK;
+}
+
+extern "C" int cw_dmc_walkers(cw_ctx *c, int *nwalk, double *x, double *wt, double *eold, uint64_t *rng) {
+  if (!c || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_walkers: no DMC population");
+  const int W = c->W;
+  if (nwalk) *nwalk = W;
+  int rc = cw_get_walkers(c, x, rng);
+  if (rc) return rc;
+  if (wt) CK(cudaMemcpy(wt, c->dmc.db.wt, sizeof(double) * W, cudaMemcpyDeviceToHost));
+  if (eold) CK(cudaMemcpy(eold, c->st.eold, sizeof(double) * W, cudaMemcpyDeviceToHost));
   return CW_OK;
 }

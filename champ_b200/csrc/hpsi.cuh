@@ -673,12 +673,11 @@ __global__ void k_energy(WState st, HBuf hb, int mode, double *out_e, double *ou
   }
 }
 
-// rotqua (vmc/rotqua.f90:357): thread per walker
-__global__ void k_rotqua(WState st) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= st.W) return;
-  DRng rng;
-  rng.load(st.rng + 4 * (size_t)w);
+// rotqua (vmc/rotqua.f90:357): random rotation frame (x, y, z axes) of the
+// quadrature grid drawn from one stream.  Host and device share it: VMC draws
+// per walker on the device, DMC draws once per step from the population
+// stream on the host.
+__host__ __device__ inline void rotqua_frame(DRng &rng, double f[9]) {
   double x1, x2, x3, xsum;
   int guard = 0;
   do {
@@ -709,14 +708,24 @@ __global__ void k_rotqua(WState st) {
   const double uu = sqrt(usum);
   u1 = u1 / uu;
   u2 = u2 / uu;
-  const double y1 = yy1 * u1 + zz1 * u2, y2 = yy2 * u1 + zz2 * u2, y3 = yy3 * u1 + zz3 * u2;
-  const double z1 = yy1 * u2 - zz1 * u1, z2 = yy2 * u2 - zz2 * u1, z3 = yy3 * u2 - zz3 * u1;
+  f[0] = x1; f[1] = x2; f[2] = x3;
+  f[3] = yy1 * u1 + zz1 * u2; f[4] = yy2 * u1 + zz2 * u2; f[5] = yy3 * u1 + zz3 * u2;
+  f[6] = yy1 * u2 - zz1 * u1; f[7] = yy2 * u2 - zz2 * u1; f[8] = yy3 * u2 - zz3 * u1;
+}
+
+__global__ void k_rotqua(WState st) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  DRng rng;
+  rng.load(st.rng + 4 * (size_t)w);
+  double f[9];
+  rotqua_frame(rng, f);
   const int NQ = cs.nquad;
   double *xq = st.xq + (size_t)w * 3 * NQ;
   for (int iq = 0; iq < NQ; iq++) {
-    xq[iq] = cs.xq0[iq] * x1 + cs.yq0[iq] * y1 + cs.zq0[iq] * z1;
-    xq[NQ + iq] = cs.xq0[iq] * x2 + cs.yq0[iq] * y2 + cs.zq0[iq] * z2;
-    xq[2 * NQ + iq] = cs.xq0[iq] * x3 + cs.yq0[iq] * y3 + cs.zq0[iq] * z3;
+    xq[iq] = cs.xq0[iq] * f[0] + cs.yq0[iq] * f[3] + cs.zq0[iq] * f[6];
+    xq[NQ + iq] = cs.xq0[iq] * f[1] + cs.yq0[iq] * f[4] + cs.zq0[iq] * f[7];
+    xq[2 * NQ + iq] = cs.xq0[iq] * f[2] + cs.yq0[iq] * f[5] + cs.zq0[iq] * f[8];
   }
   rng.store(st.rng + 4 * (size_t)w);
 }

@@ -13,6 +13,10 @@ names and argument meaning:
 * ``orbitals``, ``jastrow``, ``slater`` — orbitals / jastrow_factor /
   determinant parity hooks.
 
+``Dmc`` drives a diffusion Monte Carlo population over the same context:
+``init`` (dmc/init.f90), ``steps`` (rotqua + dmc_ps + splitj + acues1,
+dmc/dmc.f90:88-107), ``end_block`` (acuest) and ``results`` (finwrt).
+
 Every call goes through the C ABI of include/champ_b200.h; a nonzero status
 raises ``EngineError`` carrying cw_last_error, the way CHAMP's fatal_error
 aborts (module/m_error.f90:31).
@@ -176,3 +180,50 @@ class Engine:
         det = np.zeros((self.W, 2))
         self._check(self.lib.cw_slater(self.h, dptr(slmi), dptr(det)), "cw_slater")
         return slmi, det
+
+
+class Dmc:
+    """One DMC population (one CHAMP rank's walkers) on an ``Engine``."""
+
+    def __init__(self, engine: Engine, x, rng, pop_rng, tau: float, etrial: float, mwalk: int | None = None,
+                 nfprod: int = 100):
+        self.e = engine
+        x = np.ascontiguousarray(x, np.float64)
+        W = x.shape[0]
+        self.mwalk = int(mwalk or int(1.5 * W) + 1)
+        rng = np.ascontiguousarray(rng, np.uint64)
+        if rng.shape[0] < self.mwalk:
+            raise ValueError(f"rng holds {rng.shape[0]} streams, mwalk={self.mwalk} slots need one each")
+        pop = np.ascontiguousarray(pop_rng, np.uint64).reshape(4)
+        rc = engine.lib.cw_dmc_init(engine.h, W, self.mwalk, dptr(x), u64ptr(rng), u64ptr(pop), float(tau),
+                                    float(etrial), int(nfprod))
+        engine._check(rc, "cw_dmc_init")
+        engine.W = W
+
+    def steps(self, n: int):
+        self.e._check(self.e.lib.cw_dmc_steps(self.e.h, n), "cw_dmc_steps")
+
+    def end_block(self):
+        self.e._check(self.e.lib.cw_dmc_end_block(self.e.h), "cw_dmc_end_block")
+
+    def results(self) -> dict:
+        o = np.zeros(12)
+        self.e._check(self.e.lib.cw_dmc_results(self.e.h, dptr(o)), "cw_dmc_results")
+        return dict(energy=o[0], err=o[1], nwalk=int(o[2]), eest=o[3], accept=o[4], taueff=o[5], pe=o[6],
+                    ke=o[7], nblocks=o[8], fprod=o[9], eigv=o[10], wdsumo=o[11])
+
+    def walkers(self):
+        N = self.e.system.nelec
+        n = C.c_int()
+        x = np.zeros((self.mwalk, N, 3))
+        wt = np.zeros(self.mwalk)
+        eo = np.zeros(self.mwalk)
+        r = np.zeros((self.mwalk, 4), np.uint64)
+        self.e._check(self.e.lib.cw_dmc_walkers(self.e.h, C.byref(n), dptr(x), dptr(wt), dptr(eo), u64ptr(r)),
+                      "cw_dmc_walkers")
+        k = n.value
+        self.e.W = k
+        return x[:k], wt[:k], eo[:k], r[:k]
+
+    def last_ms(self) -> float:
+        return self.e.last_ms()

@@ -565,4 +565,47 @@ def make_synthetic(config: str, seed: int = 20261203) -> System:
         hyd = dict(z=1.0, lpot=1, a1=-1.0,
                    basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 1)]), 1.0, 4))
         return _assemble("tiny", rng, cent, [0, 1], [heavy, hyd], 5, 3, 4, 3, 2)
+    if config == "he":
+        return _helium()
     raise ValueError(f"unknown synthetic config {config!r}")
+
+
+HE_EXACT = -2.903724377  # non-relativistic ground state of He, Hartree
+
+
+def _helium() -> System:
+    """He atom through the ECP code path (a bare-Coulomb local channel, no
+    nonlocal channel), one 1s orbital for both spins: a nodeless trial
+    function, so DMC converges to the exact ground-state energy HE_EXACT.
+
+    The orbital is a non-negative combination of six s Gaussians fitted to
+    exp(-zeta r) / exp(J_en(r)) so that orbital times the electron-nucleus
+    Jastrow factor (a1 = -2: the nuclear cusp) is close to the hydrogenic
+    1s with zeta = 27/16; the electron-electron term carries the 1/2 cusp.
+    """
+    from scipy.optimize import nnls
+    kappa, zeta = 0.6, 27.0 / 16.0
+    ex = np.array([0.08, 0.25, 0.8, 2.5, 8.0, 25.0])
+    r = np.linspace(0.0, 8.0, 801)
+    target = np.exp(-zeta * r + 2.0 * (1.0 - np.exp(-kappa * r)) / kappa)
+    A = np.stack([gnorm(e, 0) * np.exp(-e * r * r) for e in ex], axis=1)
+    wts = (r + 0.05)
+    co, _ = nnls(A * wts[:, None], target * wts)
+    keep = co > 0
+    shells = [(0, ex[keep], co[keep])]
+    he = dict(z=2.0, lpot=1, a1=-2.0, basis=_type_from_shells(shells, 2.0, 4))
+    basis = assemble_basis([he["basis"]])
+    rng = np.random.default_rng(7)
+    a4 = np.zeros((1, 6))
+    a4[0, 0] = -2.0
+    b = np.zeros((1, 6))
+    b[0, 0] = 0.5
+    c = np.zeros((1, nterms4(5)))
+    nterm, power, expo, ecoef = _bfd_like_ecp(rng, 2.0, 1)
+    xq, yq, zq, wq = gesqua(6)
+    return System(name="he", nelec=2, nup=1, iwctype=np.array([0], np.int32), cent=np.zeros((1, 3)),
+                  znuc=np.array([2.0]), coef=np.ones((1, 1)), iworbd=np.array([[1, 1]], np.int32),
+                  cdet=np.array([1.0]), norda=5, nordb=5, nordc=5, scalek=kappa, a4=a4, b=b, c=c,
+                  nloc=4, lpot=np.array([1], np.int32), necp_term=nterm[None], necp_power=power[None],
+                  ecp_exponent=expo[None], ecp_coef=ecoef[None], nquad=6, xq0=xq, yq0=yq, zq0=zq, wq=wq,
+                  **basis)

@@ -196,7 +196,8 @@ long cw_launches(const cw_ctx *ctx);
 enum {
   CW_ST_ROTQUA = 0, CW_ST_PROPOSE, CW_ST_JASTROW_MOVE, CW_ST_BASIS_MOVE, CW_ST_LCAO_MOVE,
   CW_ST_ACCEPT, CW_ST_JASTROW_FULL, CW_ST_BASIS_ALL, CW_ST_LCAO_ALL, CW_ST_SCATTER,
-  CW_ST_SLATER_INV, CW_ST_CTILDE, CW_ST_ECP, CW_ST_ENERGY, CW_ST_COMMIT, CW_NSTAGE
+  CW_ST_SLATER_INV, CW_ST_CTILDE, CW_ST_ECP, CW_ST_ENERGY, CW_ST_COMMIT, CW_ST_DMC_WEIGHTS,
+  CW_ST_SPLITJ, CW_NSTAGE
 };
 int cw_profile(cw_ctx *ctx, int enable);
 int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
@@ -215,6 +216,43 @@ int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
  * share the one array: calls that overlap on the GPU (several contexts on
  * the same device, different streams) race on it. */
 int cw_orbitals_noalloc(cw_ctx *ctx, int npts, const double *xyz, double *out);
+
+/* ------------------------------------------------------------------------ */
+/* Diffusion Monte Carlo (idmc=2, nloc>0: dmc/dmc.f90:88-111)                */
+/* ------------------------------------------------------------------------ */
+
+/* Start a DMC population of nwalk walkers (capacity mwalk = CHAMP's MWALK)
+ * from x [nwalk][nelec][3]: init (dmc/init.f90:60-150) — hpsi of every
+ * walker with the unrotated quadrature, drift and fratio, wt=1, eest=eigv
+ * start values, fprod=1.  rng [mwalk][4]: the move stream of every walker
+ * slot (a slot keeps its stream through splitj copies); pop_rng [4]: the
+ * population stream that rotqua and splitj draw from (CHAMP's per-rank
+ * stream).  tau, etrial, nfprod as in the dmc input.  Replaces the walkers
+ * of any earlier cw_set_walkers. */
+int cw_dmc_init(cw_ctx *ctx, int nwalk, int mwalk, const double *x, const uint64_t *rng,
+                const uint64_t *pop_rng, double tau, double etrial, int nfprod);
+
+/* `nstep` DMC steps of the population, the body of dmc.f90's j loop:
+ * rotqua (dmc.f90:94, one rotation for all walkers), dmc_ps
+ * (dmc/dmc_ps_mov1.f90:4: per electron drift-diffusion move with the
+ * Green-function acceptance; hpsi; fratio and reweighting,
+ * dmc/branching.f90:27,111; population factor fprod), splitj
+ * (dmc/splitj.f90:3) and acues1 (dmc/acues1.f90:3).  The population size
+ * changes; CW_ERR_STATE if it would exceed mwalk ("SPLITJ: MWALK exceeded"). */
+int cw_dmc_steps(cw_ctx *ctx, int nstep);
+
+/* Close a DMC block: the cumulative sums of acuest (dmc/acuest.f90). */
+int cw_dmc_end_block(cw_ctx *ctx);
+
+/* DMC estimates, finwrt (dmc/finwrt.f90): out[0]=egave (mixed estimator),
+ * out[1]=its error (rn_eff of the block weights), out[2]=nwalk,
+ * out[3]=eest, out[4]=acceptance, out[5]=taueff, out[6]=PE, out[7]=KE,
+ * out[8]=blocks, out[9]=fprod, out[10]=eigv, out[11]=wdsumo. */
+int cw_dmc_results(cw_ctx *ctx, double *out);
+
+/* Current population: *nwalk, and (any may be NULL) x [nwalk][nelec][3],
+ * wt [nwalk], eold [nwalk], rng [nwalk][4]; the arrays must hold mwalk. */
+int cw_dmc_walkers(cw_ctx *ctx, int *nwalk, double *x, double *wt, double *eold, uint64_t *rng);
 
 /* Diagnostics: measured FMA throughput of the CUDA cores of `device`
  * (fp64=1: FP64, else FP32), TFLOP/s — the roofline denominator of the

@@ -1599,6 +1599,300 @@ struct Walkers {
   bool failed = false;
 };
 
+
+// ===========================================================================
+// DMC: dmc_ps (dmc/dmc_ps_mov1.f90:4), calculate_fratio / calculate_reweight
+// (dmc/branching.f90:27,111), splitj (dmc/splitj.f90:3), acues1
+// (dmc/acues1.f90:3) and the block sums of acuest (dmc/acuest.f90).
+// One population, as one CHAMP rank in dmc_one_mpi1.  Each walker slot owns
+// a random stream for its moves; rotqua and splitj draw from the population
+// stream, as CHAMP's rank does.
+// ===========================================================================
+struct DmcParams {
+  double tau, etrial;
+  int nconf, mwalk, nfprod;
+};
+
+struct DmcPop {
+  const Sys *s;
+  DmcParams prm;
+  vector<Walker> w;          // slots 0..mwalk-1, active 0..nwalk-1
+  int nwalk;
+  Rng pop;
+  double eest, eigv, wdsumo, fprod;
+  vector<double> ff;
+  vector<double> wt, fratio;
+  vector<int> iage;
+  long ipass = 0;
+  // per-step and per-block sums
+  double wsum1 = 0, esum1 = 0, pesum = 0, tpbsum = 0, tausum = 0;
+  double wgsum = 0, egsum = 0, wgcum = 0, egcum = 0, wgcm2 = 0, egcm2 = 0, taucum = 0;
+  double pecum = 0, tpbcum = 0;
+  double acc = 0, trymove = 0;
+  long nacc = 0, nodecr = 0, nbrnch = 0, iblk = 0;
+  bool failed = false;
+};
+
+double gauss_draw(Rng &r) {
+  // gauss (vmc/gauss.f90:3): one normal from two uniforms, cos draw first
+  double g = std::cos(2 * PI * r.uniform());
+  return g * std::sqrt(-2 * std::log(r.uniform()));
+}
+
+// grad for every electron after hpsi (dmc_ps :516): vold(3,nelec)
+void vold_all(Walker &w) {
+  for (int i = 0; i < w.N; i++) w.grad(i, 1, &w.vold[3 * i]);
+}
+
+// dmc_eloc_cutoff, nloc>0 branch (dmc/branching.f90:221-241) -> fratio (icut_e=0)
+double fratio_of(const Walker &w, double tau, double tratio) {
+  const double adrift = 0.5;
+  double vav2sum = 0, v2sum = 0;
+  for (int i = 0; i < w.N; i++) {
+    const double *v = &w.vold[3 * i];
+    double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    double vavvt = (std::sqrt(1.0 + 2.0 * adrift * v2 * tau * tratio) - 1.0) / (adrift * v2);
+    double vavvn = vavvt / (tau * tratio);
+    vav2sum += vavvn * vavvn * v2;
+    v2sum += v2;
+  }
+  return std::sqrt(vav2sum / v2sum);
+}
+
+// one walker of dmc_ps: electron moves, hpsi, weight; returns false if singular
+bool dmc_walker(DmcPop &P, int iw, double ffi, double &wsum1, double &esum1, double &pesum, double &tpbsum,
+                double &tausum, double &acc, double &trymove, long &nacc, long &nodecr) {
+  Walker &w = P.w[iw];
+  const Sys *s = P.s;
+  const double tau = P.prm.tau, rttau = std::sqrt(tau), adrift = 0.5, one = 1, two = 2, zero = 0;
+  double dfus2ac = 0, dfus2un = 0, drifdif = 0, pp = 1;
+  int iaccept = 0;
+  for (int i = 0; i < w.N; i++) {
+    double *vo = &w.vold[3 * i];
+    w.grad(i, 1, vo);
+    double v2old = vo[0] * vo[0] + vo[1] * vo[1] + vo[2] * vo[2];
+    double vavvt = (std::sqrt(one + two * adrift * v2old * tau) - one) / (adrift * v2old);
+    double dfus2o = zero, xnew[3];
+    for (int k = 0; k < 3; k++) {
+      double drift = vavvt * vo[k];
+      double dfus = gauss_draw(w.rng) * rttau;
+      double dx = drift + dfus;
+      dfus2o += dfus * dfus;
+      xnew[k] = w.xold[k + 3 * i] + dx;
+    }
+    for (int k = 0; k < 3; k++) w.xnew[k + 3 * i] = xnew[k];
+    double psijn;
+    double psidn = w.psie(i, w.xnew.data(), psijn, 0);
+    double vn[3];
+    if (w.detn != 0.0) w.grad(i, 0, vn);
+    else vn[0] = vn[1] = vn[2] = 0;
+    if (psidn * w.psido <= zero) nodecr++;  // icross=1: counted, not rejected
+    double v2new = vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2];
+    vavvt = (std::sqrt(one + two * adrift * v2new * tau) - one) / (adrift * v2new);
+    double dfus2n = zero;
+    for (int k = 0; k < 3; k++) {
+      double drift = vavvt * vn[k];
+      double xbac = xnew[k] + drift;
+      double dfus = xbac - w.xold[k + 3 * i];
+      dfus2n += dfus * dfus;
+    }
+    double p = (psidn / w.psido) * (psidn / w.psido) * std::exp(2 * (psijn - w.psijo)) *
+               std::exp((dfus2o - dfus2n) / (two * tau)) * 1.0;
+    if (P.iage[iw] > 50) p = p * std::pow(1.1, P.iage[iw] - 50);
+    pp = pp * p;
+    p = std::min(one, p);
+    acc += p;
+    trymove += 1;
+    dfus2ac += p * dfus2o;
+    dfus2un += dfus2o;
+    if (w.rng.uniform() < p) {
+      iaccept = 1;
+      nacc++;
+      P.iage[iw] = 0;
+      for (int k = 0; k < 3; k++) {
+        drifdif += (w.xold[k + 3 * i] - xnew[k]) * (w.xold[k + 3 * i] - xnew[k]);
+        w.xold[k + 3 * i] = xnew[k];
+      }
+      w.psido = psidn;
+      w.psijo = psijn;
+      w.jassav(i, 0);
+      w.detsav(i);
+    } else {
+      for (int k = 0; k < 3; k++) w.xnew[k + 3 * i] = w.xold[k + 3 * i];
+      w.distancese_restore(i);
+    }
+  }
+  double tauprim = tau * dfus2ac / dfus2un;
+  double psidn, psijn, ekino, enew;
+  if (!w.hpsi(w.xold.data(), psidn, psijn, ekino, enew)) return false;
+  vold_all(w);
+  double taunow = tauprim * 1.0;
+  double fration = fratio_of(w, tau, one);
+  // calculate_reweight (icut_e=0, icut_br=0)
+  double deo = P.eest - w.eold, den = P.eest - enew;
+  double ewto = P.eest - deo * P.fratio[iw];
+  double ewtn = P.eest - den * fration;
+  double expon = (P.prm.etrial - 0.5 * (ewto + ewtn)) * taunow;
+  double dwt = std::exp(expon);
+  dwt = dwt * ffi;
+  P.wt[iw] = P.wt[iw] * dwt;
+  double wtnow = P.wt[iw];
+  double wtg = wtnow * P.fprod;
+  tausum += wtg * taunow;
+  w.eold = enew;
+  w.ekino = ekino;
+  w.psido = psidn;
+  w.psijo = psijn;
+  P.fratio[iw] = fration;
+  if (iaccept == 0) P.iage[iw]++;
+  wsum1 += wtnow;
+  esum1 += wtnow * w.eold;
+  pesum += wtg * (w.eold - ekino);
+  tpbsum += wtg * ekino;
+  (void)pp;
+  (void)drifdif;
+  return true;
+}
+
+// copy walker iw into slot iw2 (splitjdet/splitjjas and the dmc arrays);
+// the slot keeps its own random stream
+void copy_walker(DmcPop &P, int iw, int iw2) {
+  Rng keep = P.w[iw2].rng;
+  P.w[iw2] = P.w[iw];
+  P.w[iw2].rng = keep;
+  P.fratio[iw2] = P.fratio[iw];
+}
+
+// splitj (dmc/splitj.f90:3)
+void splitj(DmcPop &P) {
+  const double zero = 0, two = 2, half = 0.5;
+  vector<int> iwundr;
+  int ipair = 0, iw2 = 0;
+  for (int iw = 0; iw < P.nwalk; iw++) {
+    if (P.wt[iw] < half) {
+      if (P.wt[iw] == zero) {
+        P.nbrnch++;
+        iwundr.push_back(iw);
+      } else if (ipair == 0) {
+        ipair = 1;
+        iw2 = iw;
+      } else {
+        P.nbrnch++;
+        ipair = 0;
+        double wttot = P.wt[iw] + P.wt[iw2];
+        if (P.pop.uniform() > (P.wt[iw] / wttot)) {
+          P.wt[iw2] = wttot;
+          iwundr.push_back(iw);
+        } else {
+          P.wt[iw] = wttot;
+          iwundr.push_back(iw2);
+        }
+      }
+    }
+  }
+  int nwalk2 = P.nwalk;
+  for (int iw = 0; iw < P.nwalk; iw++) {
+    if (P.wt[iw] >= two) {
+      P.nbrnch++;
+      int dst;
+      if (!iwundr.empty()) {
+        dst = iwundr.back();
+        iwundr.pop_back();
+      } else {
+        dst = nwalk2++;
+        if (nwalk2 > P.prm.mwalk) { P.failed = true; return; }
+      }
+      P.wt[iw] = P.wt[iw] * half;
+      P.wt[dst] = P.wt[iw];
+      P.iage[dst] = P.iage[iw];
+      copy_walker(P, iw, dst);
+    }
+  }
+  for (int j = (int)iwundr.size() - 1; j >= 0; j--) {
+    int dst = iwundr[j];
+    int src = nwalk2 - 1;
+    nwalk2--;
+    P.wt[dst] = P.wt[src];
+    P.iage[dst] = P.iage[src];
+    copy_walker(P, src, dst);
+  }
+  P.nwalk = nwalk2;
+}
+
+bool dmc_step(DmcPop &P, int nthreads) {
+  const Sys *s = P.s;
+  P.ipass++;
+  if (s->nloc > 0) {
+    // rotqua with the population stream, shared by every walker
+    Walker tmp(s);
+    tmp.rng = P.pop;
+    tmp.rotqua();
+    P.pop = tmp.rng;
+    for (int iw = 0; iw < P.nwalk; iw++) {
+      P.w[iw].xq = tmp.xq;
+      P.w[iw].yq = tmp.yq;
+      P.w[iw].zq = tmp.zq;
+    }
+  }
+  const int ipmod = (int)(P.ipass % P.prm.nfprod);
+  const double ginv = std::min(1.0, P.prm.tau);
+  const double ffn = P.eigv * std::pow(P.wdsumo / P.prm.nconf, ginv);
+  const double ffi = 1.0 / ffn;
+  P.fprod = P.fprod * ffn / P.ff[ipmod];
+  P.ff[ipmod] = ffn;
+  const int W = P.nwalk;
+  vector<double> a_w(W), a_e(W), a_pe(W), a_tpb(W), a_tau(W), a_acc(W), a_try(W);
+  vector<long> a_nacc(W), a_nod(W);
+  vector<int> bad(W, 0);
+  auto work = [&](int t) {
+    for (int iw = t; iw < W; iw += nthreads) {
+      double ws = 0, es = 0, pes = 0, tps = 0, tas = 0, ac = 0, tr = 0;
+      long na = 0, nd = 0;
+      if (!dmc_walker(P, iw, ffi, ws, es, pes, tps, tas, ac, tr, na, nd)) bad[iw] = 1;
+      a_w[iw] = ws; a_e[iw] = es; a_pe[iw] = pes; a_tpb[iw] = tps; a_tau[iw] = tas;
+      a_acc[iw] = ac; a_try[iw] = tr; a_nacc[iw] = na; a_nod[iw] = nd;
+    }
+  };
+  if (nthreads <= 1) work(0);
+  else {
+    vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work, t);
+    for (auto &t : th) t.join();
+  }
+  for (int iw = 0; iw < W; iw++) {
+    if (bad[iw]) return false;
+    P.wsum1 += a_w[iw]; P.esum1 += a_e[iw]; P.pesum += a_pe[iw]; P.tpbsum += a_tpb[iw];
+    P.tausum += a_tau[iw]; P.acc += a_acc[iw]; P.trymove += a_try[iw]; P.nacc += a_nacc[iw];
+    P.nodecr += a_nod[iw];
+  }
+  const double wgsum1 = P.wsum1 * P.fprod, egsum1 = P.esum1 * P.fprod;
+  splitj(P);
+  if (P.failed) return false;
+  // acues1 (idmc=2)
+  P.wgsum += wgsum1;
+  P.egsum += egsum1;
+  P.eest = (P.egcum + P.egsum) / (P.wgcum + P.wgsum);
+  P.eigv = std::exp((P.prm.etrial - P.eest) * (P.taucum + P.tausum) / (P.wgcum + P.wgsum));
+  P.wdsumo = P.wsum1;
+  P.wsum1 = 0;
+  P.esum1 = 0;
+  return true;
+}
+
+void dmc_end_block(DmcPop &P) {
+  // acuest (dmc/acuest.f90:112-255): block sums into the cumulative ones
+  const double egnow = P.egsum / P.wgsum;
+  P.egcm2 += P.egsum * egnow;
+  P.wgcm2 += P.wgsum * P.wgsum;
+  P.egcum += P.egsum;
+  P.wgcum += P.wgsum;
+  P.taucum += P.tausum;
+  P.pecum += P.pesum;
+  P.tpbcum += P.tpbsum;
+  P.egsum = P.wgsum = P.tausum = P.pesum = P.tpbsum = 0;
+  P.iblk++;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -2062,6 +2356,81 @@ void or_get_state(void *wsp, double *eold, double *psido, double *psijo) {
     if (psido) psido[k] = ws->w[k].psido;
     if (psijo) psijo[k] = ws->w[k].psijo;
   }
+}
+
+
+// ----------------------------------------------------------------------------
+// DMC
+// ----------------------------------------------------------------------------
+void *or_dmc_create(void *sysp, int nwalk, const double *x, const uint64_t *rng, const uint64_t *pop_rng,
+                    double tau, double etrial, int mwalk, int nfprod) {
+  const Sys *s = (const Sys *)sysp;
+  DmcPop *P = new DmcPop();
+  P->s = s;
+  P->prm = DmcParams{tau, etrial, nwalk, std::max(mwalk, nwalk), nfprod};
+  P->nwalk = nwalk;
+  std::memcpy(P->pop.s, pop_rng, 32);
+  P->w.reserve(P->prm.mwalk);
+  for (int k = 0; k < P->prm.mwalk; k++) {
+    P->w.emplace_back(s);
+    std::memcpy(P->w[k].rng.s, rng + 4 * k, 32);
+  }
+  P->wt.assign(P->prm.mwalk, 0.0);
+  P->fratio.assign(P->prm.mwalk, 0.0);
+  P->iage.assign(P->prm.mwalk, 0);
+  P->ff.assign(nfprod, 1.0);
+  // init (dmc/init.f90:60-150)
+  P->eigv = 1.0;
+  P->eest = etrial;
+  P->fprod = 1.0;
+  P->wdsumo = nwalk;
+  for (int iw = 0; iw < nwalk; iw++) {
+    Walker &w = P->w[iw];
+    std::memcpy(w.xold.data(), x + (size_t)3 * s->N * iw, sizeof(double) * 3 * s->N);
+    w.xq = s->xq0; w.yq = s->yq0; w.zq = s->zq0;
+    double psid, psij, ekin, e;
+    if (!w.hpsi(w.xold.data(), psid, psij, ekin, e)) P->failed = true;
+    w.psido = psid; w.psijo = psij; w.eold = e; w.ekino = ekin;
+    vold_all(w);
+    w.xnew = w.xold;
+    P->wt[iw] = 1.0;
+    // first call of dmc_ps: fratio with tratio=1
+    P->fratio[iw] = fratio_of(w, tau, 1.0);
+  }
+  return P;
+}
+void or_dmc_destroy(void *p) { delete (DmcPop *)p; }
+int or_dmc_steps(void *p, int nstep, int nthreads) {
+  DmcPop *P = (DmcPop *)p;
+  if (P->failed) return 1;
+  for (int k = 0; k < nstep; k++)
+    if (!dmc_step(*P, nthreads)) return 1;
+  return 0;
+}
+void or_dmc_end_block(void *p) { dmc_end_block(*(DmcPop *)p); }
+// out: [0] egave, [1] err, [2] nwalk, [3] eest, [4] acceptance, [5] taueff,
+//      [6] pe, [7] ke, [8] nblocks, [9] fprod, [10] eigv, [11] wdsumo
+void or_dmc_results(void *p, double *out) {
+  DmcPop *P = (DmcPop *)p;
+  double egave = P->egcum / P->wgcum;
+  double rn = P->wgcum * P->wgcum / P->wgcm2;
+  double err = std::sqrt(std::max((P->egcm2 / P->wgcum - egave * egave) / (rn - 1), 0.0));
+  out[0] = egave; out[1] = P->iblk > 1 ? err : 0.0; out[2] = P->nwalk; out[3] = P->eest;
+  out[4] = P->acc / std::max(P->trymove, 1.0); out[5] = P->taucum / P->wgcum;
+  out[6] = P->pecum / P->wgcum; out[7] = P->tpbcum / P->wgcum; out[8] = (double)P->iblk;
+  out[9] = P->fprod; out[10] = P->eigv; out[11] = P->wdsumo;
+}
+// walkers: x [nwalk][N][3], wt [nwalk], eold [nwalk]; returns nwalk
+int or_dmc_walkers(void *p, double *x, double *wt, double *eold, uint64_t *rng) {
+  DmcPop *P = (DmcPop *)p;
+  int N = P->s->N;
+  for (int iw = 0; iw < P->nwalk; iw++) {
+    if (x) std::memcpy(x + (size_t)3 * N * iw, P->w[iw].xold.data(), sizeof(double) * 3 * N);
+    if (wt) wt[iw] = P->wt[iw];
+    if (eold) eold[iw] = P->w[iw].eold;
+    if (rng) std::memcpy(rng + 4 * iw, P->w[iw].rng.s, 32);
+  }
+  return P->nwalk;
 }
 
 }  // extern "C"

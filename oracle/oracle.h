@@ -56,6 +56,17 @@ void or_get_walkers(void *ws, double *x, uint64_t *rng);
 void or_get_sums(void *ws, double *out);
 void or_get_state(void *ws, double *eold, double *psido, double *psijo);
 
+/* DMC population (dmc_ps, branching, splitj, acues1/acuest), one CHAMP rank:
+ * walker slot k owns move stream rng[k] (mwalk slots), pop_rng drives
+ * rotqua and splitj. */
+void *or_dmc_create(void *sys, int nwalk, const double *x, const uint64_t *rng, const uint64_t *pop_rng,
+                    double tau, double etrial, int mwalk, int nfprod);
+void or_dmc_destroy(void *dmc);
+int or_dmc_steps(void *dmc, int nstep, int nthreads);
+void or_dmc_end_block(void *dmc);
+void or_dmc_results(void *dmc, double *out);
+int or_dmc_walkers(void *dmc, double *x, double *wt, double *eold, uint64_t *rng);
+
 #ifdef __cplusplus
 }
 #endif

@@ -192,3 +192,53 @@ class OracleWalkers:
         j = np.zeros(self.W)
         lib().or_get_state(self.h, dp(e), dp(p), dp(j))
         return e, p, j
+
+
+class OracleDmc:
+    """DMC population of the oracle (dmc_ps + branching + splitj)."""
+
+    def __init__(self, osys: OracleSystem, x, rng, pop_rng, tau, etrial, mwalk=None, nfprod=100):
+        L = lib()
+        L.or_dmc_create.restype = C.c_void_p
+        L.or_dmc_create.argtypes = [C.c_void_p, C.c_int, _dp, _u64, _u64, C.c_double, C.c_double, C.c_int, C.c_int]
+        L.or_dmc_destroy.argtypes = [C.c_void_p]
+        L.or_dmc_steps.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.or_dmc_end_block.argtypes = [C.c_void_p]
+        L.or_dmc_results.argtypes = [C.c_void_p, _dp]
+        L.or_dmc_walkers.argtypes = [C.c_void_p, _dp, _dp, _dp, _u64]
+        self.osys = osys
+        x = np.ascontiguousarray(x, float)
+        W = x.shape[0]
+        self.mwalk = mwalk or int(1.5 * W) + 1
+        rng = np.ascontiguousarray(rng, np.uint64)
+        assert rng.shape[0] >= self.mwalk
+        pop = np.ascontiguousarray(pop_rng, np.uint64)
+        self.h = L.or_dmc_create(osys.h, W, dp(x), u64(rng), u64(pop), tau, etrial, self.mwalk, nfprod)
+
+    def __del__(self):
+        try:
+            lib().or_dmc_destroy(self.h)
+        except Exception:
+            pass
+
+    def steps(self, n, nthreads=1):
+        if lib().or_dmc_steps(self.h, n, nthreads):
+            raise RuntimeError("oracle DMC failed")
+
+    def end_block(self):
+        lib().or_dmc_end_block(self.h)
+
+    def results(self):
+        o = np.zeros(12)
+        lib().or_dmc_results(self.h, dp(o))
+        return dict(energy=o[0], err=o[1], nwalk=int(o[2]), eest=o[3], accept=o[4], taueff=o[5], pe=o[6],
+                    ke=o[7], nblocks=o[8], fprod=o[9], eigv=o[10], wdsumo=o[11])
+
+    def walkers(self):
+        N = self.osys.N
+        x = np.zeros((self.mwalk, N, 3))
+        wt = np.zeros(self.mwalk)
+        e = np.zeros(self.mwalk)
+        r = np.zeros((self.mwalk, 4), np.uint64)
+        n = lib().or_dmc_walkers(self.h, dp(x), dp(wt), dp(e), u64(r))
+        return x[:n], wt[:n], e[:n], r[:n]
