@@ -138,7 +138,7 @@ def barrier(pg, local):
     torch.cuda.synchronize(local)
 
 
-def cpu_port_rate(system, walkers_cpu, nthreads, min_seconds=10.0, max_steps=4, seed_offset=0):
+def cpu_port_rate(system, walkers_cpu, nthreads, min_seconds=10.0, max_steps=4, seed_offset=0, warm_sweeps=1):
     """Oracle (FP64 C++ restatement of CHAMP) on host threads: electron-moves/s."""
     from oracle import oracle
     oracle.build()
@@ -149,7 +149,7 @@ def cpu_port_rate(system, walkers_cpu, nthreads, min_seconds=10.0, max_steps=4, 
         x, rng[w] = o.sites(rng[w])
         xs.append(x)
     ow = oracle.OracleWalkers(o, np.array(xs), rng)
-    ow.steps(1, nthreads)  # warm-up sweep
+    ow.steps(warm_sweeps, nthreads)  # untimed warm-up sweeps
     t0 = time.perf_counter()
     steps = 0
     while steps < max_steps:
@@ -170,8 +170,9 @@ def run_reference(args):
     system = make_synthetic(cfg)
     nthreads = os.cpu_count() or 1
     rates = []
-    for _ in range(max(1, args.steps)):
-        rate, steps, dt = cpu_port_rate(system, nthreads, nthreads, min_seconds=5.0, max_steps=2)
+    for k in range(max(1, args.steps)):
+        rate, steps, dt = cpu_port_rate(system, nthreads, nthreads, min_seconds=5.0, max_steps=100,
+                                        warm_sweeps=max(1, args.warmup) if k == 0 else 1)
         rates.append(rate)
     v = statistics.median(rates)
     line = {
@@ -181,7 +182,7 @@ def run_reference(args):
         "config": {"workload": desc, "walkers": W, "walkers_cpu": nthreads, "precision": "fp64"},
         "cpu_baseline": {"value": v, "unit": "electron-moves/s", "cores": nthreads, "kind": "port",
                          "sample": f"{nthreads} walkers (one per host thread, as one per CHAMP MPI rank), "
-                                   f"1-2 metrop6 sweeps per sample after one warm-up sweep"},
+                                   f"metrop6 sweeps for >=5 s per step, median over {len(rates)} steps"},
         "e2e": {"value": v, "unit": "electron-moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -216,6 +217,12 @@ def run_ours(args):
     ms_max = max_over_ranks(ms_dev, pg, local)
     moves = W * system.nelec * args.steps * world
     value = moves / (ms_max * 1e-3)
+    # efficiency 1/(err^2 t): the timed steps form one block whose walker
+    # means give the error of the mean energy (finwrt's err with walkers as
+    # ranks); t is the device time of the timed steps
+    eng.end_block()
+    res = eng.results()
+    eff = 1.0 / (res["err"] ** 2 * ms_dev * 1e-3) if res["err"] > 0 else None
     # --- per-stage timing pass (CUDA events around every launch) ----------
     eng.profile(True)
     eng.vmc_steps(1)
@@ -266,13 +273,18 @@ def run_ours(args):
             "peak_source": "measured FP64 FMA probe (cw_fma_peak) on this GPU",
             "traffic": None, "share_of_step": ms_jm / total_stage,
             "work_per_launch": "8*(N-1)*M*T + 8*(N-1)*nordb + 8*M*norda FLOP per walker (T=23 e-e-n terms)"}
-    acc_gbs = alg["b_move"] / (ms_acc / n_acc * 1e-3) / 1e9
-    roof_hbm = {"kernel": "k_accept (ratio, accept, Sherman-Morrison commit)", "bound": "hbm",
-                "achieved": acc_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                "frac": acc_gbs / peaks.get("hbm_gbs"), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+    # HBM-bound move update: k_decide (ratio, drift, accept) + k_commit
+    # (Sherman-Morrison rows, orbital rows, Jastrow pair rows); the
+    # algorithmic bytes are the per-move B_move of the reference algorithm
+    ms_cm, n_cm = stages["commit"]
+    upd_ms = ms_acc / n_acc + ms_cm / n_cm
+    upd_gbs = alg["b_move"] / (upd_ms * 1e-3) / 1e9
+    roof_hbm = {"kernel": "k_decide + k_commit (ratio, accept, Sherman-Morrison and table commit)", "bound": "hbm",
+                "achieved": upd_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                "frac": upd_gbs / peaks.get("hbm_gbs"), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                 "work_per_launch": "8*(2 n^2 + 6N + 8(N-1) + 4 O) bytes per walker-move"}
     cpu_rate, cpu_steps, cpu_dt = cpu_port_rate(system, os.cpu_count() or 1, os.cpu_count() or 1,
-                                                min_seconds=10.0, max_steps=3)
+                                                min_seconds=10.0, max_steps=1000)
     h2d = W * system.nelec * 3 * 8 + W * 32
     d2h = h2d + W * 8 * 8
     line = {
@@ -287,6 +299,10 @@ def run_ours(args):
         "e2e": {"value": e2e, "unit": "electron-moves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "cw_set_walkers (pinned host x, rng) + cw_vmc_steps(1) + cw_get_walkers + cw_end_block"},
         "roofline": roof, "roofline_hbm": roof_hbm,
+        "efficiency": {"value": eff, "unit": "1/(Ha^2 s)", "energy": res["energy"], "err": res["err"],
+                       "sigma": res["sigma"], "t_s": ms_dev * 1e-3,
+                       "note": "one block of the timed steps, walkers in the role of CHAMP ranks; "
+                               "walkers only warmed up, not equilibrated"},
         "top_stage": {"name": top[0], "ms": top[1][0], "launches": top[1][1]},
         "stages_ms_per_step": {k: round(v[0], 3) for k, v in stages.items()},
         "cpu_baseline": {"value": cpu_rate, "unit": "electron-moves/s", "cores": os.cpu_count() or 1, "kind": "port",
