@@ -87,6 +87,9 @@ struct WState {
   double *fijo;       // [W][3][N][N] fijo(k,i,j) -> [k][i][j]
   double *fjo;        // [W][3][N]
   double *fsumo;      // [W]
+  double *enm;        // [W][2][M][N] e-n table of every electron: scaled distance
+                      // rr and dd1/r (rebuilt by hpsi, row of a moved electron
+                      // replaced on commit)
   // estimators [W][8]: wsum esum pesum tpbsum acc ecum1s ecm21s (spare)
   double *sums;
   int *status;        // [W] nonzero: singular matrix / NaN
@@ -112,6 +115,7 @@ struct MoveBuf {
   double *vjn;        // [W][3]
   double *phi;        // [W][4][K]  basis at xnew (value, dx, dy, dz)
   double *orbn;       // [W][4][Oa]
+  double *enn;        // [W][2][M]  e-n row (rr, dd1/r) of the moved electron at xnew
 };
 
 // ---------------------------------------------------------------------------

@@ -315,6 +315,7 @@ int alloc_walkers(cw_ctx *c, int W) {
   DALLOC(L, s.fijo, (size_t)W * 3 * N * N);
   DALLOC(L, s.fjo, (size_t)W * 3 * N);
   DALLOC(L, s.fsumo, W);
+  DALLOC(L, s.enm, (size_t)W * 2 * M * N);
   DALLOC(L, s.sums, (size_t)W * 8);
   DALLOC(L, s.status, W);
   MoveBuf &m = c->mb;
@@ -326,6 +327,7 @@ int alloc_walkers(cw_ctx *c, int W) {
   DALLOC(L, m.vjn, (size_t)W * 3);
   DALLOC(L, m.phi, (size_t)W * 4 * K);
   DALLOC(L, m.orbn, (size_t)W * 4 * Oa);
+  DALLOC(L, m.enn, (size_t)W * 2 * M);
   HBuf &b = c->hb;
   DALLOC(L, b.d2o, W);
   DALLOC(L, b.pe_ee, W);
@@ -1228,6 +1230,7 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   add_field(r, c->st.fijo, 3L * N * N);
   add_field(r, c->st.fjo, 3L * N);
   add_field(r, c->st.fsumo, 1);
+  add_field(r, c->st.enm, 2L * h.M * N);
   add_field(r, b.vold, 3L * N);
   add_field(r, b.fratio, 1);
   CK(cudaStreamSynchronize(c->stream));

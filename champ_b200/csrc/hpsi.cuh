@@ -83,6 +83,8 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
     scale2<double>(r, rr, dd1, dd2);
     double *q = tab + (size_t)t * 8;
     q[0] = rr; q[1] = dd1; q[2] = dd2; q[3] = r; q[4] = v0; q[5] = v1; q[6] = v2; q[7] = 0;
+    st.enm[(size_t)w * 2 * M * N + t] = rr;
+    st.enm[((size_t)w * 2 + 1) * M * N + t] = dd1 / r;
   }
   double *fso = st.fso + (size_t)w * N * N;
   double *fij0 = st.fijo + ((size_t)w * 3 + 0) * N * N;

@@ -249,7 +249,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
 // Per-centre quantities of the moved electron are staged in shared memory.
 // ---------------------------------------------------------------------------
 template <int NORD>
-__global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
+__global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) double smem[];
   constexpr int NB = een_nb(NORD);        // folded coefficients per centre
   constexpr int PER = 6 + 2 * NB;         // shared doubles per centre
@@ -283,6 +283,8 @@ __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
     scale2<double>(r, rr, dd1, dd2);
     sh_s[ic] = rr;
     sh_d[ic] = dd1;
+    mb.enn[((size_t)w * 2 + 0) * M + ic] = rr;
+    mb.enn[((size_t)w * 2 + 1) * M + ic] = dd1 / r;
     if (NORD > 1) een_fold<NORD, double>(&cs.c[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sh_B + (size_t)ic * 2 * NB);
   }
   __syncwarp();
@@ -314,20 +316,21 @@ __global__ void k_jastrow_move(WState st, MoveBuf mb, int iel) {
     if (NORD > 1) {
       const double z = 1 - kap * u;
       const double du = -kap * dd1;
+      // partner's e-n values from the walker's table (coalesced over lanes)
+      const double *en_rr = st.enm + (size_t)w * 2 * M * N + jj;
+      const double *en_h = en_rr + (size_t)M * N;
       for (int ic = 0; ic < M; ic++) {
-        const double rj_v[3] = {xj[0] - cs.cent[3 * ic], xj[1] - cs.cent[3 * ic + 1], xj[2] - cs.cent[3 * ic + 2]};
-        const double rj = sqrt(rj_v[0] * rj_v[0] + rj_v[1] * rj_v[1] + rj_v[2] * rj_v[2]);
-        double rrj, dd8, dd10;
-        scale2<double>(rj, rrj, dd8, dd10);
+        const double rrj = en_rr[(size_t)ic * N], hj = en_h[(size_t)ic * N];
         const double rri = sh_s[ic];
         if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
+        const double rj_v[3] = {xj[0] - cs.cent[3 * ic], xj[1] - cs.cent[3 * ic + 1], xj[2] - cs.cent[3 * ic + 2]};
         const double ri = sh_r[ic];
         const double dd7 = sh_d[ic];
         double fc, fu_, fi_, fj_;
         een_apply1<NORD>(sh_B + (size_t)ic * 2 * NB, 1 - kap * rrj, z, fc, fu_, fi_, fj_);
         const double fu = fu_ * du / rij;
         const double fi = fi_ * (-kap * dd7) / ri;
-        const double fj = fj_ * (-kap * dd8) / rj;
+        const double fj = fj_ * (-kap) * hj;
         fs += fc;
         for (int k = 0; k < 3; k++) {
           gi[k] += fi * sh_rv[k * M + ic] + fu * rvee[k];
@@ -564,6 +567,12 @@ __global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
     st.orbs[((size_t)w * N + iel) * nmax + j] = s_orb[j];
     for (int k = 0; k < 3; k++)
       st.dorbs[(((size_t)w * 3 + k) * N + iel) * nmax + j] = orbn[(1 + k) * Oa + slot[j]];
+  }
+  // e-n table row of the moved electron
+  const int M = cs.M;
+  for (int t = tid; t < 2 * M; t += blockDim.x) {
+    const int pl = t / M, ic = t % M;
+    st.enm[(((size_t)w * 2 + pl) * M + ic) * N + iel] = mb.enn[((size_t)w * 2 + pl) * M + ic];
   }
   // jassav: pair tables and per-electron gradients
   double *fso = st.fso + (size_t)w * N * N;
