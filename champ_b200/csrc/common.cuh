@@ -116,11 +116,23 @@ struct MoveBuf {
   double *phi;        // [W][4][K]  basis at xnew (value, dx, dy, dz)
   double *orbn;       // [W][4][Oa]
   double *enn;        // [W][2][M]  e-n row (rr, dd1/r) of the moved electron at xnew
+  float *phi_hi, *phi_lo;  // mixed precision: [W*4][kp] split basis rows (null in FP64)
+  int kp;                  // row pitch of phi_hi/phi_lo (K rounded up to 32)
 };
 
 // ---------------------------------------------------------------------------
 // small helpers
 // ---------------------------------------------------------------------------
+// FP64 -> (hi, lo) FP32 pair, hi exactly TF32-representable (round to
+// nearest, ties away), lo the FP32 remainder: the operand split of the
+// tensor-core LCAO contraction.
+__device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"((float)x));
+  hi = __uint_as_float(h);
+  lo = (float)(x - (double)hi);
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

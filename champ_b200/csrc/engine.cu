@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/champ_b200.h"
 #include "common.cuh"
 #include "gemm.cuh"
@@ -17,6 +19,7 @@
 #include "move.cuh"
 #include "dmc.cuh"
 #include "peak.cuh"
+#include "umma.cuh"
 
 
 using namespace cw;
@@ -71,6 +74,13 @@ struct cw_ctx {
   double stage_ms[CW_NSTAGE] = {0};
   long stage_n[CW_NSTAGE] = {0};
   DmcHost dmc;
+  // mixed precision: tensor-core LCAO (TF32 x3) operands and tensor maps
+  bool mixed = false;
+  int kp = 0, np = 0, umma_st = 0;
+  size_t smem_umma = 0;
+  float *coef_hi = nullptr, *coef_lo = nullptr;   // [Oa][kp]
+  int *d_err = nullptr;                            // tensor-core stage error flags
+  CUtensorMap tm_b_hi{}, tm_b_lo{}, tm_mv_hi{}, tm_mv_lo{}, tm_all_hi{}, tm_all_lo{};
 };
 
 namespace {
@@ -219,6 +229,61 @@ int nord_attrs(cw_ctx *c) {
   }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// 2-D FP32 tensor map over rows x K (row pitch kp floats), box 32 x box_rows,
+// 128-byte swizzle; elements past K or past the last row read as zero.
+int make_map(cw_ctx *c, CUtensorMap *map, const float *base, int K, long rows, int kp, int box_rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return fail(c, CW_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  cuuint64_t gdim[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  cuuint64_t gstr[1] = {(cuuint64_t)kp * sizeof(float)};
+  cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
+  cuuint32_t est[2] = {1u, 1u};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, gdim, gstr, box, est,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(c, CW_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return CW_OK;
+}
+
+__global__ void k_split_rows(const double *src, int rows, int K, float *hi, float *lo, int kp) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)rows * kp) return;
+  const int r = (int)(t / kp), k = (int)(t % kp);
+  float h = 0.0f, l = 0.0f;
+  if (k < K) split_tf32(src[(size_t)r * K + k], h, l);
+  hi[t] = h;
+  lo[t] = l;
+}
+
+// LCAO contraction of M basis rows: tensor cores (TF32 x3) in the mixed
+// path, FP64 CUDA-core GEMM otherwise.
+int lcao(cw_ctx *c, bool move, int M, const double *phi64, double *out) {
+  const CSys &h = c->h;
+  if (!c->mixed) {
+    dgemm(c->stream, M, h.Oa, h.K, phi64, c->g.coefT, out);
+    return launch_check(c, "dgemm");
+  }
+  const CUtensorMap &ahi = move ? c->tm_mv_hi : c->tm_all_hi;
+  const CUtensorMap &alo = move ? c->tm_mv_lo : c->tm_all_lo;
+  k_lcao_tf32x3<<<(M + 127) / 128, 128, c->smem_umma, c->stream>>>(ahi, alo, c->tm_b_hi, c->tm_b_lo, M, h.K, c->np,
+                                                                   h.Oa, c->umma_st, out, h.Oa, c->d_err);
+  return launch_check(c, "k_lcao_tf32x3");
+}
+
 // Full local energy of every walker (hpsi).  mode 1 also adds metrop6's sums.
 int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullptr) {
   const CSys &h = c->h;
@@ -238,9 +303,11 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     stage_end(c);
     LCHK("k_basis_all");
     stage_begin(c, CW_ST_LCAO_ALL);
-    dgemm(c->stream, W * ne * 5, h.Oa, h.K, c->hb.phi, c->g.coefT, c->hb.orball);
-    stage_end(c);
-    LCHK("dgemm(all)");
+    {
+      int rc = lcao(c, false, W * ne * 5, c->hb.phi, c->hb.orball);
+      stage_end(c);
+      if (rc) return rc;
+    }
     const long ns = (long)W * ne * h.nmax;
     stage_begin(c, CW_ST_SCATTER);
     k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
@@ -270,6 +337,12 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
 }
 
 int check_status(cw_ctx *c) {
+  if (c->mixed) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (e) return fail(c, CW_ERR_CUDA, "tensor-core LCAO stage: a pipeline wait timed out (flags %d)", e);
+  }
   std::vector<int> s(c->W);
   CK(cudaMemcpyAsync(s.data(), c->st.status, sizeof(int) * c->W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -344,6 +417,21 @@ int alloc_walkers(cw_ctx *c, int W) {
   b.chunk = chunk;
   DALLOC(L, b.phi, (size_t)W * chunk * 5 * K);
   DALLOC(L, b.orball, (size_t)W * chunk * 5 * Oa);
+  m.phi_hi = m.phi_lo = nullptr;
+  b.phi_hi = b.phi_lo = nullptr;
+  if (c->mixed) {
+    const int kp = c->kp;
+    m.kp = b.kp = kp;
+    DALLOC(L, m.phi_hi, (size_t)W * 4 * kp);
+    DALLOC(L, m.phi_lo, (size_t)W * 4 * kp);
+    DALLOC(L, b.phi_hi, (size_t)W * chunk * 5 * kp);
+    DALLOC(L, b.phi_lo, (size_t)W * chunk * 5 * kp);
+    int rc = make_map(c, &c->tm_mv_hi, m.phi_hi, K, (long)W * 4, kp, 128);
+    if (!rc) rc = make_map(c, &c->tm_mv_lo, m.phi_lo, K, (long)W * 4, kp, 128);
+    if (!rc) rc = make_map(c, &c->tm_all_hi, b.phi_hi, K, (long)W * chunk * 5, kp, 128);
+    if (!rc) rc = make_map(c, &c->tm_all_lo, b.phi_lo, K, (long)W * chunk * 5, kp, 128);
+    if (rc) return rc;
+  }
   if (h.nloc > 0) DALLOC(L, b.ctilde, (size_t)W * N * K);
   DALLOC(L, b.entab, (size_t)W * M * N * 8);
   CK(cudaMemsetAsync(s.status, 0, sizeof(int) * W, c->stream));
@@ -589,6 +677,30 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   int rc = nord_attrs(c);
   if (rc) return rc;
   if (c->smem_ecp > 227 * 1024 && h.nloc) return fail(c, CW_ERR_UNSUPPORTED, "ECP stage shared memory too large");
+  if (precision == CW_PREC_MIXED) {
+    // tensor-core LCAO: coefficients split once into TF32 hi/lo, [Oa][kp]
+    c->mixed = true;
+    c->kp = (h.K + 31) / 32 * 32;
+    c->np = (h.Oa + 15) / 16 * 16;
+    if (c->np > 256) return fail(c, CW_ERR_UNSUPPORTED, "mixed precision: more than 256 orbitals");
+    c->umma_st = umma_stages(c->np);
+    c->smem_umma = umma_smem_bytes(c->np);
+    CK(cudaFuncSetAttribute(k_lcao_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_umma));
+    double *cA;
+    DALLOC(L, cA, (size_t)h.Oa * h.K);
+    CK(cudaMemcpy(cA, d->coef, sizeof(double) * (size_t)h.Oa * h.K, cudaMemcpyHostToDevice));
+    DALLOC(L, c->coef_hi, (size_t)h.Oa * c->kp);
+    DALLOC(L, c->coef_lo, (size_t)h.Oa * c->kp);
+    const long n = (long)h.Oa * c->kp;
+    k_split_rows<<<(unsigned)((n + 255) / 256), 256>>>(cA, h.Oa, h.K, c->coef_hi, c->coef_lo, c->kp);
+    LCHK("k_split_rows");
+    CK(cudaDeviceSynchronize());
+    DALLOC(L, c->d_err, 1);
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    rc = make_map(c, &c->tm_b_hi, c->coef_hi, h.K, h.Oa, c->kp, c->np);
+    if (!rc) rc = make_map(c, &c->tm_b_lo, c->coef_lo, h.K, h.Oa, c->kp, c->np);
+    if (rc) return rc;
+  }
   return CW_OK;
 }
 
@@ -703,9 +815,11 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
       stage_end(c);
       LCHK("k_basis_move");
       stage_begin(c, CW_ST_LCAO_MOVE);
-      dgemm(c->stream, W * 4, h.Oa, h.K, c->mb.phi, c->g.coefT, c->mb.orbn);
-      stage_end(c);
-      LCHK("dgemm(move)");
+      {
+        int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn);
+        stage_end(c);
+        if (rc) return rc;
+      }
       stage_begin(c, CW_ST_ACCEPT);
       k_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, i);
       stage_end(c);
@@ -835,8 +949,10 @@ int cw_orbitals(cw_ctx *c, double *orb, double *dorb, double *ddorb) {
     const int bw = c->basis_warps;
     k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->hb, c->g, e0, ne);
     LCHK("k_basis_all");
-    dgemm(c->stream, W * ne * 5, Oa, K, c->hb.phi, c->g.coefT, c->hb.orball);
-    LCHK("dgemm(all)");
+    {
+      int rc = lcao(c, false, W * ne * 5, c->hb.phi, c->hb.orball);
+      if (rc) return rc;
+    }
     buf.resize((size_t)W * ne * 5 * Oa);
     CK(cudaMemcpyAsync(buf.data(), c->hb.orball, sizeof(double) * buf.size(), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -1291,9 +1407,11 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       stage_end(c);
       LCHK("k_basis_move");
       stage_begin(c, CW_ST_LCAO_MOVE);
-      dgemm(c->stream, W * 4, h.Oa, h.K, c->mb.phi, c->g.coefT, c->mb.orbn);
-      stage_end(c);
-      LCHK("dgemm(move)");
+      {
+        int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn);
+        stage_end(c);
+        if (rc) return rc;
+      }
       stage_begin(c, CW_ST_ACCEPT);
       k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, b, sc, i);
       stage_end(c);

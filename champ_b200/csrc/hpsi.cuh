@@ -27,6 +27,8 @@ struct HBuf {
   double *ctilde;   // [W][N][K]
   double *entab;    // [W][M][N][8] e-n table of the full Jastrow: rr, dd1, dd2, r, rvec(3)
   int chunk;        // electrons per chunk
+  float *phi_hi, *phi_lo;  // mixed precision: [rows][kp] split chunk basis (null in FP64)
+  int kp;
 };
 
 __device__ __forceinline__ void pair_of(long p, int &i, int &j) {
@@ -232,6 +234,18 @@ __global__ void k_basis_all(WState st, HBuf hb, GSys g, int e0, int ne) {
   double *rec = smem + (size_t)wib * cs.M * kCenRec;
   warp_basis_prepass<2>(g, x, rec, lane);
   __syncwarp();
+  if (hb.phi_hi) {
+    const int kp = hb.kp;
+    float *hi = hb.phi_hi + ((size_t)gw * 5) * kp, *lo = hb.phi_lo + ((size_t)gw * 5) * kp;
+    for (int m = lane; m < K; m += 32)
+      warp_basis_ao<2>(g, rec, m, [&](int a, int d, double v) {
+        float h, l;
+        split_tf32(v, h, l);
+        hi[(size_t)d * kp + a] = h;
+        lo[(size_t)d * kp + a] = l;
+      });
+    return;
+  }
   double *phi = hb.phi + ((size_t)gw * 5) * K;
   for (int m = lane; m < K; m += 32)
     warp_basis_ao<2>(g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });

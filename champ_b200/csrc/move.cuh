@@ -401,15 +401,35 @@ __global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
   const int K = cs.K;
   const MoveScratch &mv = mb.ms[w];
   double *phi = mb.phi + (size_t)w * 4 * K;
+  const int kp = mb.kp;
+  float *hi = mb.phi_hi ? mb.phi_hi + (size_t)w * 4 * kp : nullptr;
+  float *lo = mb.phi_lo ? mb.phi_lo + (size_t)w * 4 * kp : nullptr;
   if (mv.igeo) {
     // the GEMM still reads these rows: keep them finite
-    for (int t = lane; t < 4 * K; t += 32) phi[t] = 0.0;
+    if (hi) {
+      for (int t = lane; t < 4 * K; t += 32) {
+        hi[(size_t)(t / K) * kp + t % K] = 0.0f;
+        lo[(size_t)(t / K) * kp + t % K] = 0.0f;
+      }
+    } else {
+      for (int t = lane; t < 4 * K; t += 32) phi[t] = 0.0;
+    }
     return;
   }
   double *rec = smem + (size_t)wib * cs.M * kCenRec;
   const double x[3] = {mv.xnew[0], mv.xnew[1], mv.xnew[2]};
   warp_basis_prepass<1>(g, x, rec, lane);
   __syncwarp();
+  if (hi) {
+    for (int m = lane; m < K; m += 32)
+      warp_basis_ao<1>(g, rec, m, [&](int a, int d, double v) {
+        float h, l;
+        split_tf32(v, h, l);
+        hi[(size_t)d * kp + a] = h;
+        lo[(size_t)d * kp + a] = l;
+      });
+    return;
+  }
   for (int m = lane; m < K; m += 32)
     warp_basis_ao<1>(g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
 }

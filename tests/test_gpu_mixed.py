@@ -1,0 +1,99 @@
+"""Mixed-precision path (cw_create(..., CW_PREC_MIXED)) against the FP64
+oracle.  The LCAO contraction runs on the tensor cores with TF32 x3 split
+operands and FP32 accumulation; everything downstream stays FP64.  Stated
+bounds (relative to the largest entry of each compared array):
+orbitals and derivatives 2e-6, local energy 5e-5 * max(1, |E|),
+determinant 2e-3 (the random orthonormal orbitals of these synthetic
+systems make ill-conditioned Slater matrices that amplify the FP32
+accumulation error), and the
+accept/reject decisions of a few VMC steps identical."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+TOL_ORB = 2e-6
+TOL_E = 5e-5
+TOL_DET = 2e-3
+
+
+def _setup(oracle_mod, config, W):
+    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.system import make_synthetic
+    s = make_synthetic(config)
+    rng = rng_states(W)
+    x = initial_configs(s, rng)
+    eng = Engine(s, precision="mixed")
+    eng.set_walkers(x, rng)
+    return s, eng, oracle_mod.OracleSystem(s), x, rng
+
+
+@pytest.mark.parametrize("config,W", [("tiny", 8), ("c0", 8), ("c1", 2)])
+def test_mixed_orbitals(oracle_mod, config, W):
+    s, eng, o, x, _ = _setup(oracle_mod, config, W)
+    orb, dorb, ddorb = eng.orbitals()
+    worst = 0.0
+    for w in range(W):
+        ro, rd, rdd = o.orbitals(x[w])
+        e = max(rel_err(orb[w], ro), rel_err(dorb[w], rd), rel_err(ddorb[w], rdd))
+        worst = max(worst, e)
+    print(f"{config}: max relative orbital error {worst:.2e}")
+    assert worst < TOL_ORB
+
+
+@pytest.mark.parametrize("config,W", [("tiny", 8), ("c0", 8), ("c1", 2)])
+def test_mixed_hpsi(oracle_mod, config, W):
+    s, eng, o, x, _ = _setup(oracle_mod, config, W)
+    h = eng.hpsi()
+    worst, worst_d = 0.0, 0.0
+    for w in range(W):
+        r = o.hpsi(x[w])
+        worst = max(worst, abs(h["energy"][w] - r["energy"]) / max(1.0, abs(r["energy"])))
+        worst_d = max(worst_d, abs(h["psid"][w] - r["psid"]) / abs(r["psid"]))
+    print(f"{config}: max relative local-energy error {worst:.2e}, determinant {worst_d:.2e}")
+    assert worst <= TOL_E
+    assert worst_d <= TOL_DET
+
+
+def test_mixed_vmc_decisions(oracle_mod):
+    for config in ("tiny", "c0"):
+        s, eng, o, x, rng = _setup(oracle_mod, config, 16)
+        ow = oracle_mod.OracleWalkers(o, x, rng)
+        for step in range(3):
+            eng.vmc_steps(1)
+            ow.steps(1)
+            xg, rg = eng.walkers()
+            xo, ro = ow.walkers()
+            assert np.array_equal(rg, ro), f"{config}: random streams diverged at step {step}"
+            assert rel_err(xg, xo) < 1e-5
+            sg, so = eng.sums(), ow.sums()
+            assert np.array_equal(sg[:, 4], so[:, 4]), "acceptance counts differ"
+
+
+def test_mixed_mean_energy(oracle_mod):
+    """Same walkers and streams through the FP64 and the mixed engine: the
+    acceptance agrees and the mean energies differ by a small fraction of
+    the statistical error (samples near a node of the determinant, where
+    the local energy is large and ill-conditioned, carry most of the
+    difference)."""
+    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.system import make_synthetic
+    s = make_synthetic("c0")
+    W = 512
+    rng = rng_states(W)
+    x = initial_configs(s, rng)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        e = Engine(s, precision=prec)
+        e.set_walkers(x, rng)
+        for _ in range(4):
+            e.vmc_steps(5)
+            e.end_block()
+        res[prec] = e.results()
+        e.close()
+    d = abs(res["mixed"]["energy"] - res["fp64"]["energy"])
+    print(f"c0 mean energy fp64 {res['fp64']['energy']:.6f} +- {res['fp64']['err']:.4f}, "
+          f"mixed {res['mixed']['energy']:.6f}, |diff| {d:.2e} Ha")
+    assert res["mixed"]["accept"] == res["fp64"]["accept"]
+    assert d <= 0.05 * res["fp64"]["err"]
