@@ -40,6 +40,7 @@ struct CSys {
   double a4[CW_MAX_TYPES * (CW_MAX_NORD + 1)];
   double b[2 * (CW_MAX_NORD + 1)];
   double c[CW_MAX_TYPES * CW_MAX_TERMS];
+  float cf[CW_MAX_TYPES * CW_MAX_TERMS];   // FP32 copy of c (mixed-precision Jastrow)
   double asymp_jasa[CW_MAX_TYPES];
   // ECP
   int lpot[CW_MAX_TYPES];
@@ -334,6 +335,40 @@ __device__ __forceinline__ void een_fold(const T *__restrict__ cc, T x, T *BD) {
   for (int t = 0; t < een_nb(NORD); t++) {
     BD[2 * t] = B[t];
     BD[2 * t + 1] = dB[t];
+  }
+}
+
+// FP32 twin of een_apply1 (mixed-precision Jastrow): BD 8-byte aligned
+template <int NORD>
+__device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float y, float z, float &fc, float &fu,
+                                            float &fi, float &fj) {
+  float yp[NORD + 1], dyp[NORD + 1];
+  yp[0] = 1;
+  dyp[0] = 0;
+#pragma unroll
+  for (int p = 1; p <= NORD; p++) {
+    yp[p] = yp[p - 1] * y;
+    dyp[p] = float(p) * yp[p - 1];
+  }
+  const float2 *bd = reinterpret_cast<const float2 *>(BD);
+  fc = 0; fu = 0; fi = 0; fj = 0;
+  float zk = 1, zkm = 0;
+#pragma unroll
+  for (int k = 0; k < NORD; k++) {
+    float a = 0, ax = 0, ay = 0;
+#pragma unroll
+    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
+      const float2 v = bd[een_off(NORD, k) + p - een_pmin(k)];
+      a += v.x * yp[p];
+      ax += v.y * yp[p];
+      ay += v.x * dyp[p];
+    }
+    fc += zk * a;
+    fu += zkm * a;
+    fi += zk * ax;
+    fj += zk * ay;
+    zkm = float(k + 1) * zk;
+    zk *= z;
   }
 }
 

@@ -58,7 +58,7 @@ struct cw_ctx {
   MoveBuf mb{};
   HBuf hb{};
   std::vector<void *> w_allocs;
-  size_t smem_jmove = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
+  size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
   int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
@@ -187,7 +187,10 @@ template <int NORD>
 void launch_jmove(cw_ctx *c, int iel) {
   const int warps = 4;
   dim3 grid((c->W + warps - 1) / warps);
-  k_jastrow_move<NORD><<<grid, 32 * warps, c->smem_jmove, c->stream>>>(c->st, c->mb, iel);
+  if (c->mixed)
+    k_jastrow_move_f32<NORD><<<grid, 32 * warps, c->smem_jmove_f32, c->stream>>>(c->st, c->mb, iel);
+  else
+    k_jastrow_move<NORD><<<grid, 32 * warps, c->smem_jmove, c->stream>>>(c->st, c->mb, iel);
 }
 template <int NORD>
 void launch_jfull(cw_ctx *c) {
@@ -200,6 +203,8 @@ void launch_ecp(cw_ctx *c) {
 template <int NORD>
 int set_attrs(cw_ctx *c) {
   CK(cudaFuncSetAttribute(k_jastrow_move<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_jmove));
+  CK(cudaFuncSetAttribute(k_jastrow_move_f32<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)c->smem_jmove_f32));
   CK(cudaFuncSetAttribute(k_jastrow_full<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_jfull));
   if (c->h.nloc > 0)
     CK(cudaFuncSetAttribute(k_ecp<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
@@ -539,7 +544,10 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
       for (int k = 0; k < 2; k++) h.ae[(it * CW_MAX_RWF + irb) * 2 + k] = d->ae[src * 2 + k];
     }
     for (int k = 0; k <= d->norda; k++) h.a4[it * (d->norda + 1) + k] = d->a4[it * (d->norda + 1) + k];
-    for (int k = 0; k < h.nterms; k++) h.c[it * CW_MAX_TERMS + k] = d->c[it * h.nterms + k];
+    for (int k = 0; k < h.nterms; k++) {
+      h.c[it * CW_MAX_TERMS + k] = d->c[it * h.nterms + k];
+      h.cf[it * CW_MAX_TERMS + k] = (float)d->c[it * h.nterms + k];
+    }
     if (d->nloc) {
       h.lpot[it] = d->lpot[it];
       for (int l = 0; l < CW_MPS_L; l++) {
@@ -654,6 +662,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
     c->smem_jmove = sizeof(double) * 4 * (size_t)h.M * (6 + 2 * een_nb(nord));
+    c->smem_jmove_f32 = sizeof(float) * 4 * (size_t)h.M * (6 + 2 * een_nb(nord));
   }
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;

@@ -390,6 +390,151 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
 }
 
 // ---------------------------------------------------------------------------
+// Mixed-precision jastrow4e: the same warp-per-walker kernel with the pair
+// and e-e-n polynomial sums in FP32 (folded coefficients, scaled distances,
+// per-pair value and gradients); coordinates differ in FP64 before the cast,
+// and the row sums against the stored FP64 tables (dfs, dv) stay FP64.
+// ---------------------------------------------------------------------------
+template <int NORD>
+__global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf mb, int iel) {
+  extern __shared__ __align__(16) float smemf[];
+  constexpr int NB = een_nb(NORD);
+  constexpr int PER = 6 + 2 * NB;         // shared floats per centre
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int M = cs.M, N = cs.N;
+  float *sh = smemf + (size_t)wib * M * PER;
+  float *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M, *sh_B = sh + 6 * M;
+  const bool active = (w < st.W);
+  int igeo = 1;
+  double xi[3] = {0, 0, 0};
+  if (active) {
+    const MoveScratch &m = mb.ms[w];
+    igeo = m.igeo;
+    xi[0] = m.xnew[0]; xi[1] = m.xnew[1]; xi[2] = m.xnew[2];
+  }
+  if (!active || igeo) return;
+  const float kap = (float)cs.scalek;
+  const float asym = (float)cs.asymp_r;
+  for (int ic = lane; ic < M; ic += 32) {
+    float r2 = 0;
+    for (int k = 0; k < 3; k++) {
+      const float d = (float)(xi[k] - cs.cent[3 * ic + k]);
+      sh_rv[k * M + ic] = d;
+      r2 += d * d;
+    }
+    const float r = sqrtf(r2);
+    sh_r[ic] = r;
+    float rr, dd1, dd2;
+    scale2<float>(r, rr, dd1, dd2);
+    sh_s[ic] = rr;
+    sh_d[ic] = dd1;
+    mb.enn[((size_t)w * 2 + 0) * M + ic] = rr;
+    mb.enn[((size_t)w * 2 + 1) * M + ic] = dd1 / r;
+    if (NORD > 1) een_fold<NORD, float>(&cs.cf[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sh_B + (size_t)ic * 2 * NB);
+  }
+  __syncwarp();
+  const double *xw = st.x + (size_t)w * 3 * N;
+  const double *fso_i = st.fso + ((size_t)w * N + iel) * N;
+  double dfs = 0, dv0 = 0, dv1 = 0, dv2 = 0;
+  for (int jj = lane; jj < N; jj += 32) {
+    if (jj == iel) continue;
+    const double xj[3] = {xw[jj], xw[N + jj], xw[2 * N + jj]};
+    const int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
+    int isb, ipar;
+    double sspinn_d;
+    pair_spin(i, j, isb, ipar, sspinn_d);
+    const float sspinn = (float)sspinn_d;
+    const float rvee[3] = {(float)(xi[0] - xj[0]), (float)(xi[1] - xj[1]), (float)(xi[2] - xj[2])};
+    const float rij = sqrtf(rvee[0] * rvee[0] + rvee[1] * rvee[1] + rvee[2] * rvee[2]);
+    float u, dd1, dd2;
+    scale2<float>(rij, u, dd1, dd2);
+    float fs = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
+    if (u != asym) {
+      float fee, feeu, feeuu;
+      ee_term<1, float>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+      feeu = feeu * dd1 / rij;
+      fs += fee;
+      for (int k = 0; k < 3; k++) {
+        gi[k] += feeu * rvee[k];
+        gj[k] -= feeu * rvee[k];
+      }
+    }
+    if (NORD > 1) {
+      const float z = 1 - kap * u;
+      const float du = -kap * dd1;
+      const float du_r = du / rij;
+      const double *en_rr = st.enm + (size_t)w * 2 * M * N + jj;
+      const double *en_h = en_rr + (size_t)M * N;
+      for (int ic = 0; ic < M; ic++) {
+        const float rrj = (float)en_rr[(size_t)ic * N], hj = (float)en_h[(size_t)ic * N];
+        const float rri = sh_s[ic];
+        if (rri == asym && rrj == asym) continue;
+        const float rj_v[3] = {(float)(xj[0] - cs.cent[3 * ic]), (float)(xj[1] - cs.cent[3 * ic + 1]),
+                               (float)(xj[2] - cs.cent[3 * ic + 2])};
+        float fc, fu_, fi_, fj_;
+        een_apply1f<NORD>(sh_B + (size_t)ic * 2 * NB, 1 - kap * rrj, z, fc, fu_, fi_, fj_);
+        const float fu = fu_ * du_r;
+        const float fi = fi_ * (-kap * sh_d[ic]) / sh_r[ic];
+        const float fj = fj_ * (-kap) * hj;
+        fs += fc;
+        for (int k = 0; k < 3; k++) {
+          gi[k] += fi * sh_rv[k * M + ic] + fu * rvee[k];
+          gj[k] += fj * rj_v[k] - fu * rvee[k];
+        }
+      }
+    }
+    mb.fsn[(size_t)w * N + jj] = fs;
+    for (int k = 0; k < 3; k++) {
+      mb.fijn_i[((size_t)w * 3 + k) * N + jj] = gi[k];
+      mb.fijn_j[((size_t)w * 3 + k) * N + jj] = gj[k];
+    }
+    dfs += (double)fs - fso_i[jj];
+    dv0 += (double)gi[0] - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + jj];
+    dv1 += (double)gi[1] - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + jj];
+    dv2 += (double)gi[2] - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + jj];
+  }
+  // e-n part of the moved electron
+  float fen_s = 0, ge0 = 0, ge1 = 0, ge2 = 0;
+  for (int ic = lane; ic < M; ic += 32) {
+    const int it = cs.iwctype[ic];
+    const float rri = sh_s[ic];
+    if (rri == asym) continue;
+    float fen, feni, fenii;
+    en_term<1, float>(it, rri, fen, feni, fenii);
+    feni = feni * sh_d[ic] / sh_r[ic];
+    fen_s += fen;
+    ge0 += feni * sh_rv[0 * M + ic];
+    ge1 += feni * sh_rv[1 * M + ic];
+    ge2 += feni * sh_rv[2 * M + ic];
+  }
+  fen_s = warp_sumf(fen_s);
+  ge0 = warp_sumf(ge0);
+  ge1 = warp_sumf(ge1);
+  ge2 = warp_sumf(ge2);
+  dfs = warp_sum(dfs);
+  dv0 = warp_sum(dv0);
+  dv1 = warp_sum(dv1);
+  dv2 = warp_sum(dv2);
+  if (lane == 0) {
+    mb.fsn[(size_t)w * N + iel] = fen_s;
+    mb.fijn_i[((size_t)w * 3 + 0) * N + iel] = ge0;
+    mb.fijn_i[((size_t)w * 3 + 1) * N + iel] = ge1;
+    mb.fijn_i[((size_t)w * 3 + 2) * N + iel] = ge2;
+    dfs += (double)fen_s - fso_i[iel];
+    dv0 += (double)ge0 - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + iel];
+    dv1 += (double)ge1 - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + iel];
+    dv2 += (double)ge2 - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + iel];
+    mb.fsumn[w] = st.fsumo[w] + dfs;
+    const double *fjo = st.fjo + (size_t)w * 3 * N;
+    mb.vjn[3 * w + 0] = fjo[0 * N + iel] + dv0;
+    mb.vjn[3 * w + 1] = fjo[1 * N + iel] + dv1;
+    mb.vjn[3 * w + 2] = fjo[2 * N + iel] + dv2;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Basis functions of the moved electron (basis_fns ider=1): warp per walker,
 // per-centre prepass then lanes over AOs.
 // ---------------------------------------------------------------------------

@@ -1,6 +1,7 @@
 """Mixed-precision path (cw_create(..., CW_PREC_MIXED)) against the FP64
 oracle.  The LCAO contraction runs on the tensor cores with TF32 x3 split
-operands and FP32 accumulation; everything downstream stays FP64.  Stated
+operands and FP32 accumulation, the move Jastrow sums in FP32; Slater
+algebra, local energy and estimator sums stay FP64.  Stated
 bounds (relative to the largest entry of each compared array):
 orbitals and derivatives 2e-6, local energy 5e-5 * max(1, |E|),
 determinant 2e-3 (the random orthonormal orbitals of these synthetic
@@ -73,7 +74,8 @@ def test_mixed_vmc_decisions(oracle_mod):
 
 def test_mixed_mean_energy(oracle_mod):
     """Same walkers and streams through the FP64 and the mixed engine: the
-    acceptance agrees and the mean energies differ by a small fraction of
+    acceptance agrees (up to near-threshold decisions) and the mean
+    energies differ by a small fraction of
     the statistical error (samples near a node of the determinant, where
     the local energy is large and ill-conditioned, carry most of the
     difference)."""
@@ -95,5 +97,7 @@ def test_mixed_mean_energy(oracle_mod):
     d = abs(res["mixed"]["energy"] - res["fp64"]["energy"])
     print(f"c0 mean energy fp64 {res['fp64']['energy']:.6f} +- {res['fp64']['err']:.4f}, "
           f"mixed {res['mixed']['energy']:.6f}, |diff| {d:.2e} Ha")
-    assert res["mixed"]["accept"] == res["fp64"]["accept"]
+    # 512 walkers x 8 electrons x 20 steps = 81920 decisions: a few may
+    # flip where the FP64 acceptance probability lies within ~1e-6 of the draw
+    assert abs(res["mixed"]["accept"] - res["fp64"]["accept"]) <= 2e-4
     assert d <= 0.05 * res["fp64"]["err"]
