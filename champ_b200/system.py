@@ -609,3 +609,57 @@ def _helium() -> System:
                   nloc=4, lpot=np.array([1], np.int32), necp_term=nterm[None], necp_power=power[None],
                   ecp_exponent=expo[None], ecp_coef=ecoef[None], nquad=6, xq0=xq, yq0=yq, zq0=zq, wq=wq,
                   **basis)
+
+
+def rotation_expansion(s: System, rots, extra_orbitals: int = 0, seed: int = 11, permute: bool = True):
+    """Multideterminant system built from orbital rotations, and its single-
+    determinant twin.
+
+    Each rotation (spin, slot, orbital, t) replaces the reference orbital of
+    that electron slot by phi_ref + t * phi_orbital (0-based orbital, a
+    virtual one).  The product over rotations of (reference + t * excitation)
+    is a multideterminant expansion with 2**len(rots) determinants whose
+    value equals the single determinant of the rotated orbitals; the twin
+    holds those rotated orbitals as extra LCAO rows.  With permute=True some
+    determinants list their orbitals in a swapped order with the sign folded
+    into cdet, as CHAMP inputs may.  Returns (multidet system, twin).
+    """
+    import dataclasses
+    import itertools
+    rng = np.random.default_rng(seed)
+    coef = np.asarray(s.coef, float)
+    if extra_orbitals:
+        extra = rng.normal(size=(extra_orbitals, coef.shape[1])) * 0.3
+        coef = np.vstack([coef, extra])
+    ref = np.asarray(s.iworbd[0], np.int32)
+    slots = [(sp, sl) for sp, sl, _, _ in rots]
+    if len(set(slots)) != len(slots):
+        raise ValueError("one rotation per electron slot")
+    dets, cdets = [], []
+    for mask in itertools.product([0, 1], repeat=len(rots)):
+        occ = ref.copy()
+        c = 1.0
+        for (sp, sl, orb, t), m in zip(rots, mask):
+            if m:
+                occ[sl + (0 if sp == 0 else s.nup)] = orb + 1
+                c *= t
+        if permute and len(dets) % 3 == 1 and s.nup >= 2:
+            occ[0], occ[1] = occ[1], occ[0]
+            c = -c
+        dets.append(occ)
+        cdets.append(c)
+    md = dataclasses.replace(s, name=s.name + "_md", coef=coef, iworbd=np.array(dets, np.int32),
+                             cdet=np.array(cdets, float), _keep=[])
+    # twin: rotated orbitals appended as new rows, the up and down slots point at them
+    rows = [coef]
+    occ1 = ref.copy()
+    nextra = coef.shape[0]
+    for sp, sl, orb, t in rots:
+        e = sl + (0 if sp == 0 else s.nup)
+        o = occ1[e] - 1
+        rows.append((coef[o] + t * coef[orb])[None, :])
+        occ1[e] = nextra + 1
+        nextra += 1
+    twin = dataclasses.replace(s, name=s.name + "_twin", coef=np.vstack(rows), iworbd=occ1[None, :].astype(np.int32),
+                               cdet=np.array([1.0]), _keep=[])
+    return md, twin

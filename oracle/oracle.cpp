@@ -66,8 +66,18 @@ struct Sys {
   int mbastyp;
   vector<int> nbastyp, iwlbas, iwrwf;
   int K, O, ndet;
-  vector<double> coef, cdet;
+  vector<double> coef, cdet;   // cdet: sign-adjusted by multideterminants_define
   vector<int> iworbd;  // iworbd(j) for kref=1, 1-based orbital
+  vector<int> iworbd_all;      // [ndet][N] 1-based, reordered as multideterminants_define does
+  // compact multideterminant tables per spin (multideterminants_define,
+  // vmc/set_input_data.f90:46), all indices 0-based, kref = determinant 0
+  struct MdSpin {
+    int ivirt = 0, iactv = 0;          // first virtual orbital, first active slot
+    int nuniq = 0, nsingle = 0, ndouble = 0;
+    vector<int> numrep;                // [nuniq]
+    vector<int> irepcol, ireporb;      // [nuniq][MEXCIT] replaced slot / new orbital
+    vector<int> kdet2, kaux2;          // full determinants not kref-equivalent and their unique index
+  } md[2];
   int norda, nordb, nordc, isc, nspin2b, nocuspb, nterms;
   double scalek;
   vector<double> a4, b, c;
@@ -103,6 +113,135 @@ int nterms4(int nord) {
       }
     }
   return i;
+}
+
+constexpr int MEXCIT = 10;  // vmc_mod MEXCIT (module/m_vmc.f90:99)
+
+// multideterminants_define (vmc/set_input_data.f90:46-414) with kref = 1:
+// per spin, the excitation of every determinant relative to kref (replaced
+// reference slots irepcol in slot order, new orbitals ireporb in the
+// determinant's order), the permutation sign folded into cdet, the unique
+// spin-determinants (first occurrence of each excitation) ordered singles,
+// doubles, then the rest, and the (determinant, unique index) lists of the
+// determinants whose spin part differs from kref.  The reference reorders
+// the unique list by pairwise swaps; a stable partition is used here, which
+// changes only the summation order of the Y-matrix accumulation.
+bool multideterminants_define(Sys &s) {
+  const int N = s.N, nd = s.ndet;
+  vector<int> numrep((size_t)nd * 2, 0), irc((size_t)nd * 2 * N, 0), iro((size_t)nd * 2 * N, 0);
+  vector<int> itot(nd, 0);
+  auto IW = [&](int k, int i) -> int & { return s.iworbd_all[(size_t)k * N + i]; };
+  for (int k = 1; k < nd; k++) {
+    for (int iab = 0; iab < 2; iab++) {
+      const int nel = iab == 0 ? s.nup : s.ndn, ish = iab == 0 ? 0 : s.nup;
+      int &nr = numrep[k * 2 + iab];
+      nr = 0;
+      for (int iref = 0; iref < nel; iref++) {
+        const int iwref = IW(0, iref + ish);
+        bool in = false;
+        for (int i = 0; i < nel; i++)
+          if (IW(k, i + ish) == iwref) in = true;
+        if (!in) irc[((size_t)k * 2 + iab) * N + nr++] = iref;
+      }
+      int isub = 0;
+      for (int i = 0; i < nel; i++) {
+        const int iw = IW(k, i + ish);
+        bool in = false;
+        for (int iref = 0; iref < nel; iref++)
+          if (iw == IW(0, iref + ish)) in = true;
+        if (!in) iro[((size_t)k * 2 + iab) * N + isub++] = iw - 1;
+      }
+      if (isub != nr) return false;
+      vector<int> sw(nel);
+      for (int i = 0; i < nel; i++) sw[i] = IW(0, i + ish);
+      for (int r = 0; r < nr; r++) sw[irc[((size_t)k * 2 + iab) * N + r]] = iro[((size_t)k * 2 + iab) * N + r] + 1;
+      int iphase = 0;
+      for (int i = 0; i < nel; i++) {
+        if (IW(k, i + ish) != sw[i]) {
+          for (int l = i + 1; l < nel; l++) {
+            if (sw[l] == IW(k, i + ish)) {
+              std::swap(sw[i], sw[l]);
+              iphase++;
+            }
+          }
+        }
+      }
+      itot[k] += iphase;
+    }
+    if (itot[k] % 2) s.cdet[k] = -s.cdet[k];
+  }
+  for (int k = 1; k < nd; k++) {
+    for (int i = 0; i < N; i++) IW(k, i) = IW(0, i);
+    for (int iab = 0; iab < 2; iab++) {
+      const int ish = iab == 0 ? 0 : s.nup;
+      for (int r = 0; r < numrep[k * 2 + iab]; r++)
+        IW(k, irc[((size_t)k * 2 + iab) * N + r] + ish) = iro[((size_t)k * 2 + iab) * N + r] + 1;
+    }
+  }
+  for (int iab = 0; iab < 2; iab++) {
+    Sys::MdSpin &m = s.md[iab];
+    const int nel = iab == 0 ? s.nup : s.ndn;
+    m = Sys::MdSpin();
+    m.iactv = nel;
+    m.ivirt = s.nup;  // ivirt(1)=nup+1 and ivirt(2)=ndn+1 in CHAMP's 1-based numbering
+    if (iab == 1) m.ivirt = s.ndn;
+    for (int k = 1; k < nd; k++)
+      for (int r = 0; r < numrep[k * 2 + iab]; r++) {
+        m.iactv = std::min(m.iactv, irc[((size_t)k * 2 + iab) * N + r]);
+        m.ivirt = std::min(m.ivirt, iro[((size_t)k * 2 + iab) * N + r]);
+      }
+    auto same = [&](int a, int b) {
+      if (numrep[a * 2 + iab] != numrep[b * 2 + iab]) return false;
+      for (int r = 0; r < numrep[a * 2 + iab]; r++) {
+        if (irc[((size_t)a * 2 + iab) * N + r] != irc[((size_t)b * 2 + iab) * N + r]) return false;
+        if (iro[((size_t)a * 2 + iab) * N + r] != iro[((size_t)b * 2 + iab) * N + r]) return false;
+      }
+      return true;
+    };
+    // iwundet: kref if no excitation, else the first determinant with the same excitation
+    vector<int> iwun(nd, 0);
+    for (int i = 1; i < nd; i++) {
+      if (numrep[i * 2 + iab] == 0) { iwun[i] = 0; continue; }
+      int j = 0;
+      while (j != i && !same(j, i)) j++;
+      iwun[i] = j;
+    }
+    vector<int> uniq;
+    for (int k = 1; k < nd; k++)
+      if (iwun[k] == k) uniq.push_back(k);
+    vector<int> order;
+    for (int pass = 0; pass < 3; pass++)
+      for (int k : uniq) {
+        const int nr = numrep[k * 2 + iab];
+        if ((pass == 0 && nr == 1) || (pass == 1 && nr == 2) || (pass == 2 && nr > 2)) order.push_back(k);
+      }
+    m.nuniq = (int)order.size();
+    m.numrep.assign(m.nuniq, 0);
+    m.irepcol.assign((size_t)m.nuniq * MEXCIT, 0);
+    m.ireporb.assign((size_t)m.nuniq * MEXCIT, 0);
+    vector<int> kidx(nd, -1);
+    for (int kk = 0; kk < m.nuniq; kk++) {
+      const int k = order[kk];
+      kidx[k] = kk;
+      const int nr = numrep[k * 2 + iab];
+      if (nr > MEXCIT) return false;
+      m.numrep[kk] = nr;
+      if (nr == 1) m.nsingle++;
+      else if (nr == 2) m.ndouble++;
+      for (int r = 0; r < nr; r++) {
+        m.irepcol[(size_t)kk * MEXCIT + r] = irc[((size_t)k * 2 + iab) * N + r];
+        m.ireporb[(size_t)kk * MEXCIT + r] = iro[((size_t)k * 2 + iab) * N + r];
+      }
+    }
+    for (int k = 1; k < nd; k++) {
+      const int kun = iwun[k];
+      if (kun != 0) {
+        m.kdet2.push_back(k);
+        m.kaux2.push_back(kidx[kun]);
+      }
+    }
+  }
+  return true;
 }
 
 // set_scale_dist (vmc/scale_dist.f90:3-55)
@@ -379,6 +518,15 @@ struct Walker {
   // slater
   vector<double> slmi[2], slmin, fp[2], fpp[2], ddx, d2dx2, dorb_tmp;
   double detiab[2], detn;
+  // multideterminant state (multimat, multislater, ycompact and their "n" twins)
+  vector<double> aa[2], aan;          // [n][O] column-major aa(irep,jrep) = [irep + n*jrep]
+  vector<double> wfmat[2], wfmatn;    // [nuniq][MEXCIT^2]
+  vector<double> ddet[2], ddetn;      // [nuniq] excitation ratios
+  vector<double> detall[2], detalln;  // [ndet] detiab(k,iab)
+  vector<double> ymat[2], ymatn;      // [O][n] ymat(jrep,irep) = [jrep + O*irep]
+  vector<double> bmat;                // [N][O] b(iorb,i) = [iorb + O*i] (kinetic + nonlocal)
+  vector<double> bkin;                // [N][O]
+  double psidn_md = 0;                // psid at the proposed position (multideterminant)
   // quadrature (qua), rotated per step
   vector<double> xq, yq, zq;
   // ecp
@@ -414,6 +562,24 @@ struct Walker {
     fpp[0].assign(std::max(n1 * n1, 1), 0); fpp[1].assign(std::max(n2 * n2, 1), 0);
     ddx.assign(3 * N, 0); d2dx2.assign(N, 0); dorb_tmp.assign(3 * O, 0);
     detiab[0] = detiab[1] = detn = 0;
+    if (s->ndet > 1) {
+      int nmx = std::max(std::max(n1, n2), 1);
+      for (int iab = 0; iab < 2; iab++) {
+        int nel = std::max(iab == 0 ? n1 : n2, 1);
+        aa[iab].assign((size_t)nel * O, 0);
+        wfmat[iab].assign((size_t)std::max(s->md[iab].nuniq, 1) * MEXCIT * MEXCIT, 0);
+        ddet[iab].assign(std::max(s->md[iab].nuniq, 1), 0);
+        detall[iab].assign(s->ndet, 0);
+        ymat[iab].assign((size_t)O * nel, 0);
+      }
+      aan.assign((size_t)nmx * O, 0);
+      wfmatn.assign((size_t)std::max(std::max(s->md[0].nuniq, s->md[1].nuniq), 1) * MEXCIT * MEXCIT, 0);
+      ddetn.assign(std::max(std::max(s->md[0].nuniq, s->md[1].nuniq), 1), 0);
+      detalln.assign(s->ndet, 0);
+      ymatn.assign((size_t)O * nmx, 0);
+    }
+    bmat.assign((size_t)N * O, 0);
+    bkin.assign((size_t)N * O, 0);
     xq = s->xq0; yq = s->yq0; zq = s->zq0;
     vps.assign((size_t)N * M * CW_MPS_L, 0);
     zero_estimators();
@@ -928,11 +1094,139 @@ struct Walker {
   void detsav(int iel) {
     int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab);
     for (int j = 0; j < nel * nel; j++) slmi[iab][j] = slmin[j];
+    if (s->ndet > 1) {
+      // detsav (vmc/detsav.f90:41-82): ymat, aa (virtual columns), wfmat, detiab
+      const Sys::MdSpin &m = s->md[iab];
+      for (int j = m.ivirt; j < O; j++)
+        for (int i = 0; i < nel; i++) {
+          ymat[iab][j + (size_t)O * i] = ymatn[j + (size_t)O * i];
+          aa[iab][i + (size_t)nel * j] = aan[i + (size_t)nel * j];
+        }
+      for (int kk = 0; kk < m.nuniq; kk++) {
+        const int nr = m.numrep[kk];
+        for (int t = 0; t < nr * nr; t++)
+          wfmat[iab][(size_t)kk * MEXCIT * MEXCIT + t] = wfmatn[(size_t)kk * MEXCIT * MEXCIT + t];
+        ddet[iab][kk] = ddetn[kk];
+      }
+      for (int k = 0; k < s->ndet; k++) detall[iab][k] = detalln[k];
+    }
     detiab[iab] = detn;
     for (int iorb = 0; iorb < O; iorb++) {
       orb[iel + N * iorb] = orbn[iorb];
       for (int k = 0; k < 3; k++) dorb[iorb + O * (iel + N * k)] = dorbn[iorb + O * k];
     }
+  }
+
+  // ---- multideterminant pieces ----
+  // Excitation determinants of the unique spin-determinants of spin iab
+  // from aa: ratio dd(kk) and the inverse of the excitation matrix in wf
+  // (multideterminante.f90:69-124, multideterminant.f90:119-215).
+  bool md_tables(int iab, const double *aav, double *wf, double *dd) const {
+    const Sys::MdSpin &m = s->md[iab];
+    const int nel = nel_of(iab);
+    for (int kk = 0; kk < m.nuniq; kk++) {
+      const int nr = m.numrep[kk];
+      const int *rc = &m.irepcol[(size_t)kk * MEXCIT], *ro = &m.ireporb[(size_t)kk * MEXCIT];
+      double *w = wf + (size_t)kk * MEXCIT * MEXCIT;
+      if (nr == 1) {
+        dd[kk] = aav[rc[0] + (size_t)nel * ro[0]];
+        w[0] = 1.0 / dd[kk];
+      } else if (nr == 2) {
+        w[0] = aav[rc[0] + (size_t)nel * ro[0]];
+        w[1] = aav[rc[1] + (size_t)nel * ro[0]];
+        w[2] = aav[rc[0] + (size_t)nel * ro[1]];
+        w[3] = aav[rc[1] + (size_t)nel * ro[1]];
+        dd[kk] = w[0] * w[3] - w[2] * w[1];
+        const double deti = 1.0 / dd[kk], aux = w[0];
+        w[0] = w[3] * deti;
+        w[1] = -w[1] * deti;
+        w[2] = -w[2] * deti;
+        w[3] = aux * deti;
+      } else {
+        for (int jr = 0; jr < nr; jr++)
+          for (int ir = 0; ir < nr; ir++) w[ir + nr * jr] = aav[rc[ir] + (size_t)nel * ro[jr]];
+        if (or_matinv(w, nr, &dd[kk]) != 0) return false;
+      }
+    }
+    return true;
+  }
+  // detiab(k,iab) of every determinant from the reference value and the ratios
+  void md_unroll(int iab, double dref, const double *dd, double *dall) const {
+    const Sys::MdSpin &m = s->md[iab];
+    for (int k = 0; k < s->ndet; k++) dall[k] = dref;
+    for (size_t t = 0; t < m.kdet2.size(); t++) dall[m.kdet2[t]] = dall[m.kdet2[t]] * dd[m.kaux2[t]];
+  }
+  // compute_ymat (vmc/multideterminant.f90:258)
+  void compute_ymat(int iab, const double *du, const double *dd_, const double *wf, double *y) const {
+    const Sys::MdSpin &m = s->md[iab];
+    const int nel = nel_of(iab);
+    const double detrefi = 1.0 / (du[0] * dd_[0]);
+    std::fill(y, y + (size_t)O * nel, 0.0);
+    vector<double> ceq(std::max(m.nuniq, 1), 0.0);
+    for (size_t t = 0; t < m.kdet2.size(); t++) {
+      const int k = m.kdet2[t], kw = m.kaux2[t];
+      const double detall_k = detrefi * du[k] * dd_[k] * s->cdet[k];
+      ceq[kw] = ceq[kw] + detall_k;
+    }
+    for (int kk = 0; kk < m.nuniq; kk++) {
+      const int nr = m.numrep[kk];
+      const int *rc = &m.irepcol[(size_t)kk * MEXCIT], *ro = &m.ireporb[(size_t)kk * MEXCIT];
+      const double *w = wf + (size_t)kk * MEXCIT * MEXCIT;
+      for (int ir = 0; ir < nr; ir++)
+        for (int jr = 0; jr < nr; jr++) y[ro[jr] + (size_t)O * rc[ir]] += ceq[kk] * w[jr + nr * ir];
+    }
+  }
+  // multideterminante_grad (vmc/multideterminante.f90:149): velocity from Y
+  void md_grad(int iel, const double *b, int ldb, double detratio, const double *sl, const double *aav,
+               const double *y, double *vel) const {
+    vel[0] = vel[1] = vel[2] = 0;
+    if (s->ndet == 1) return;
+    const int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup, jel = iel - ish;
+    const Sys::MdSpin &m = s->md[iab];
+    vector<double> gmat((size_t)nel * O * 3, 0.0);
+    for (int kk = 0; kk < 3; kk++)
+      for (int jrep = m.ivirt; jrep < O; jrep++) {
+        double dum = 0.0;
+        for (int j = 0; j < nel; j++) dum += b[occ(j + ish) + (size_t)ldb * kk] * aav[j + (size_t)nel * jrep];
+        dum = b[jrep + (size_t)ldb * kk] - dum;
+        for (int irep = m.iactv; irep < nel; irep++)
+          gmat[irep + (size_t)nel * (jrep + (size_t)O * kk)] = dum * sl[irep + (size_t)nel * jel];
+      }
+    for (int kk = 0; kk < 3; kk++) {
+      double dum = 0;
+      for (int jrep = m.ivirt; jrep < O; jrep++)
+        for (int irep = m.iactv; irep < nel; irep++)
+          dum += y[jrep + (size_t)O * irep] * gmat[irep + (size_t)nel * (jrep + (size_t)O * kk)];
+      vel[kk] = dum * detratio;
+    }
+  }
+  // multideterminante (vmc/multideterminante.f90:3): tables at the proposed
+  // position from the updated inverse slmin and the new orbital row
+  bool multideterminante(int iel) {
+    const int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
+    const Sys::MdSpin &m = s->md[iab];
+    for (int jrep = m.ivirt; jrep < O; jrep++)
+      for (int irep = 0; irep < nel; irep++) {
+        double dum = 0.0;
+        for (int i = 0; i < nel; i++) {
+          const double o = (i + ish == iel) ? orbn[jrep] : orb[(i + ish) + (size_t)N * jrep];
+          dum += slmin[irep + (size_t)nel * i] * o;
+        }
+        aan[irep + (size_t)nel * jrep] = dum;
+      }
+    if (!md_tables(iab, aan.data(), wfmatn.data(), ddetn.data())) return false;
+    md_unroll(iab, detn, ddetn.data(), detalln.data());
+    if (iab == 0) compute_ymat(0, detalln.data(), detall[1].data(), wfmatn.data(), ymatn.data());
+    else compute_ymat(1, detall[0].data(), detalln.data(), wfmatn.data(), ymatn.data());
+    return true;
+  }
+  // update_ymat (vmc/multideterminant.f90:562): after the last electron of a
+  // spin has been offered its move, the other spin's Y sees the new dets
+  void update_ymat(int iel) {
+    if (s->ndet == 1) return;
+    if ((iel != s->nup - 1 && iel != N - 1) || s->ndn == 0) return;
+    const int iab = (iel == s->nup - 1) ? 1 : 0;
+    compute_ymat(iab, detall[0].data(), detall[1].data(), wfmat[iab].data(), ymat[iab].data());
   }
   // determinante_ref_grad (vmc/determinante.f90:285) with the given slmi column
   void ref_grad(int iel, const double *sl, const double *dorbv /* dorb(norb,3) */, int ldo, double *v) {
@@ -948,18 +1242,27 @@ struct Walker {
   }
   // compute_determinante_grad (vmc/determinante.f90:69), single det, iflag_move 1 or 0
   void grad(int iel, int iflag_move, double *vd) {
+    const int iab = iel < s->nup ? 0 : 1;
+    double vel[3] = {0, 0, 0};
     if (iflag_move == 1) {
-      int iab = iel < s->nup ? 0 : 1;
       double *dt = dorb_tmp.data();
       for (int k = 0; k < 3; k++)
         for (int iorb = 0; iorb < O; iorb++) dt[iorb + O * k] = dorb[iorb + O * (iel + N * k)];
       double vref[3];
       ref_grad(iel, slmi[iab].data(), dt, O, vref);
-      for (int k = 0; k < 3; k++) vd[k] = 0.0 + vref[k] + vj[k + 3 * iel];
+      if (s->ndet > 1) {
+        const double detratio = detiab[0] * detiab[1] / psido;
+        md_grad(iel, dt, O, detratio, slmi[iab].data(), aa[iab].data(), ymat[iab].data(), vel);
+      }
+      for (int k = 0; k < 3; k++) vd[k] = vel[k] + vref[k] + vj[k + 3 * iel];
     } else {
       double vref[3];
       ref_grad(iel, slmin.data(), dorbn.data(), O, vref);
-      for (int k = 0; k < 3; k++) vd[k] = 0.0 + vref[k] + vjn[k + 3 * iel];
+      if (s->ndet > 1) {
+        const double detratio = (iab == 0 ? detn * detiab[1] : detiab[0] * detn) / psidn_md;
+        md_grad(iel, dorbn.data(), O, detratio, slmin.data(), aan.data(), ymatn.data(), vel);
+      }
+      for (int k = 0; k < 3; k++) vd[k] = vel[k] + vref[k] + vjn[k + 3 * iel];
     }
   }
 
@@ -971,7 +1274,16 @@ struct Walker {
     determinante(iel, iflag);
     if (detn == 0.0) return 0.0;
     int iab = iel < s->nup ? 0 : 1;
-    return detn * detiab[1 - iab] * s->cdet[0];
+    if (s->ndet == 1) return detn * detiab[1 - iab] * s->cdet[0];
+    if (!multideterminante(iel)) {
+      singular = true;
+      return 0.0;
+    }
+    // determinante_psit (vmc/determinante_psit.f90:4)
+    double determ = 0.0;
+    for (int k = 0; k < s->ndet; k++) determ += detalln[k] * detall[1 - iab][k] * s->cdet[k];
+    psidn_md = determ;
+    return determ;
   }
 
   // ---- ECP: gauss_pot / getvps_gauss (vmc/readps_gauss.f90:6-92) ----
@@ -1124,13 +1436,14 @@ struct Walker {
     // orbitals_quad (ider=0) + nonlocd_quad
     vector<double> ph((size_t)K * nxq);
     basis_fns(*s, 0, nxq, nxq, rvq.data(), rq.data(), 0, ph.data(), nullptr, nullptr);
-    vector<double> det_ratio(nxq), orbq(O);
+    vector<double> det_ratio(nxq), orbq(O), orbq_all(s->ndet > 1 ? (size_t)nxq * O : 0);
     for (int q = 0; q < nxq; q++) {
       for (int iorb = 0; iorb < O; iorb++) {
         double a = 0;
         for (int m = 0; m < K; m++) a += s->COEF(m, iorb) * ph[m + (size_t)K * q];
         orbq[iorb] = a;
       }
+      if (s->ndet > 1) std::copy(orbq.begin(), orbq.end(), orbq_all.begin() + (size_t)O * q);
       int iel = qp[q].iel;
       int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
       int ikel = nel * (iel - ish);
@@ -1181,6 +1494,9 @@ struct Walker {
       for (int l = 1; l <= s->lpot[ict] - 1; l++) term += yl0(l, qp[q].costh) * vps[iel + N * (ic + M * (l - 1))];
       double trj = term * s->wq[qp[q].iq] * std::exp(ratio_jn[q]);
       vpsp_det[iab] += trj * det_ratio[q];
+      // pseudopotential contribution to the B matrix (nonloc.f90:271-273)
+      if (s->ndet > 1)
+        for (int iorb = 0; iorb < O; iorb++) bmat[iorb + (size_t)O * iel] += trj * orbq_all[iorb + (size_t)O * q];
     }
   }
 
@@ -1196,6 +1512,80 @@ struct Walker {
     return pe;
   }
 
+  // multideterminant_hpsi (vmc/multideterminant.f90:3) with bxmatrix
+  // (vmc/bxmatrices.f90:3) and the Y-matrix energy of hpsi (vmc/hpsi.f90:220-238):
+  // aa = A^-1 Phi, tildem = A^-1 B - X Phi with X = A^-1 B_occ A^-1, the
+  // excitation tables, every detiab, both Y matrices, psid and the energy
+  // corrections denergy / dekin.
+  bool multideterminant_hpsi(double &psid, double &denergy, double &dekin) {
+    vector<double> tild[2], tildk[2];
+    for (int iab = 0; iab < 2; iab++) {
+      const int nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
+      tild[iab].assign((size_t)std::max(nel, 1) * O, 0.0);
+      tildk[iab].assign((size_t)std::max(nel, 1) * O, 0.0);
+      if (nel == 0) continue;
+      const vector<double> &sl = slmi[iab];
+      // xmat from B restricted to the reference orbitals (multiply_slmi_mderiv_simple)
+      auto xmat_of = [&](const vector<double> &bb, vector<double> &xm) {
+        vector<double> bt((size_t)nel * nel), work(nel);
+        for (int i = 0; i < nel; i++)
+          for (int j = 0; j < nel; j++) bt[j + (size_t)nel * i] = bb[occ(j + ish) + (size_t)O * (i + ish)];
+        xm.assign((size_t)nel * nel, 0.0);
+        for (int mm = 0; mm < nel; mm++) {
+          for (int j = 0; j < nel; j++) {
+            work[j] = 0;
+            for (int i = 0; i < nel; i++) work[j] = work[j] + bt[i + (size_t)nel * j] * sl[i + (size_t)nel * mm];
+          }
+          for (int n = 0; n < nel; n++) {
+            double x = 0;
+            for (int j = 0; j < nel; j++) x = x + work[j] * sl[n + (size_t)nel * j];
+            xm[mm + (size_t)nel * n] = x;
+          }
+        }
+      };
+      vector<double> xm, xmk;
+      xmat_of(bmat, xm);
+      xmat_of(bkin, xmk);
+      for (int jrep = 0; jrep < O; jrep++)
+        for (int irep = 0; irep < nel; irep++) {
+          double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
+          for (int i = 0; i < nel; i++) {
+            const double o = orb[(i + ish) + (size_t)N * jrep];
+            d1 += sl[irep + (size_t)nel * i] * o;
+            d2 += sl[irep + (size_t)nel * i] * bmat[jrep + (size_t)O * (i + ish)];
+            d3 += xm[i + (size_t)nel * irep] * o;
+            d4 += sl[irep + (size_t)nel * i] * bkin[jrep + (size_t)O * (i + ish)];
+            d5 += xmk[i + (size_t)nel * irep] * o;
+          }
+          aa[iab][irep + (size_t)nel * jrep] = d1;
+          tild[iab][irep + (size_t)nel * jrep] = d2 - d3;
+          tildk[iab][irep + (size_t)nel * jrep] = d4 - d5;
+        }
+    }
+    for (int iab = 0; iab < 2; iab++) {
+      if (!md_tables(iab, aa[iab].data(), wfmat[iab].data(), ddet[iab].data())) return false;
+      md_unroll(iab, detiab[iab], ddet[iab].data(), detall[iab].data());
+    }
+    compute_ymat(0, detall[0].data(), detall[1].data(), wfmat[0].data(), ymat[0].data());
+    if (s->ndn > 0) compute_ymat(1, detall[0].data(), detall[1].data(), wfmat[1].data(), ymat[1].data());
+    psid = 0.0;
+    for (int k = 0; k < s->ndet; k++) psid = psid + detall[0][k] * detall[1][k] * s->cdet[k];
+    denergy = 0;
+    dekin = 0;
+    for (int iab = 0; iab < 2; iab++) {
+      const int nel = nel_of(iab);
+      const Sys::MdSpin &m = s->md[iab];
+      for (int jrep = m.ivirt; jrep < O; jrep++)
+        for (int irep = m.iactv; irep < nel; irep++) {
+          denergy = denergy + ymat[iab][jrep + (size_t)O * irep] * tild[iab][irep + (size_t)nel * jrep];
+          dekin = dekin + ymat[iab][jrep + (size_t)O * irep] * tildk[iab][irep + (size_t)nel * jrep];
+        }
+    }
+    denergy = denergy * detiab[0] * detiab[1] / psid;
+    dekin = dekin * detiab[0] * detiab[1] / psid;
+    return true;
+  }
+
   // ---- hpsi (vmc/hpsi.f90:3), single det; returns false if singular ----
   bool hpsi(const double *coord, double &psid, double &psij, double &ekin, double &energy,
             double *extra = nullptr) {
@@ -1207,6 +1597,17 @@ struct Walker {
     double d2j = d2o;
     psij = fsumo;
     if (!determinant()) return false;
+    if (s->ndet > 1) {
+      // compute_bmatrices_kin (vmc/determinant.f90:196): B of the kinetic operator
+      for (int i = 0; i < N; i++)
+        for (int iorb = 0; iorb < O; iorb++) {
+          const double bk = -hb * (ddorb[iorb + O * i] + 2 * (vj[0 + 3 * i] * dorb[iorb + O * (i + N * 0)] +
+                                                            vj[1 + 3 * i] * dorb[iorb + O * (i + N * 1)] +
+                                                            vj[2 + 3 * i] * dorb[iorb + O * (i + N * 2)]));
+          bkin[iorb + (size_t)O * i] = bk;
+          bmat[iorb + (size_t)O * i] = bk;
+        }
+    }
     double vpsp[2] = {0, 0};
     if (s->nloc > 0) nonloc_pot(coord, pe, vpsp);
     double ekin_det[2], eloc_det[2];
@@ -1225,8 +1626,12 @@ struct Walker {
     for (int i = 0; i < N; i++)
       ekin_other += -hb * (vj[0 + 3 * i] * vj[0 + 3 * i] + vj[1 + 3 * i] * vj[1 + 3 * i] + vj[2 + 3 * i] * vj[2 + 3 * i]);
     double e_other = ekin_other + pe;
-    psid = detiab[0] * detiab[1] * s->cdet[0];
     double denergy = 0, dekin = 0;
+    if (s->ndet == 1) {
+      psid = detiab[0] * detiab[1] * s->cdet[0];
+    } else {
+      if (!multideterminant_hpsi(psid, denergy, dekin)) return false;
+    }
     energy = denergy + eloc_det[0] + eloc_det[1] + e_other;
     ekin = dekin + ekin_det[0] + ekin_det[1] + ekin_other;
     if (extra) {
@@ -1566,6 +1971,8 @@ bool Walker::metrop6() {
       for (int ic = 0; ic < 3; ic++) xnew[ic + 3 * i] = xold[ic + 3 * i];
       if (igeometrical == 0) distancese_restore(i);
     }
+    update_ymat(i);
+    if (singular) return false;
   }
   // primary configuration: full recompute
   double ekin, e;
@@ -1721,10 +2128,13 @@ bool dmc_walker(DmcPop &P, int iw, double ffi, double &wsum1, double &esum1, dou
       for (int k = 0; k < 3; k++) w.xnew[k + 3 * i] = w.xold[k + 3 * i];
       w.distancese_restore(i);
     }
+    w.update_ymat(i);
+    if (w.singular) return false;
   }
   double tauprim = tau * dfus2ac / dfus2un;
   double psidn, psijn, ekino, enew;
   if (!w.hpsi(w.xold.data(), psidn, psijn, ekino, enew)) return false;
+  w.psido = psidn;  // dmc_ps :516 drifts with the hpsi value of psid
   vold_all(w);
   double taunow = tauprim * 1.0;
   double fration = fratio_of(w, tau, one);
@@ -1930,6 +2340,11 @@ void *or_sys_create(const cw_system_desc *d) {
   s->coef.assign(d->coef, d->coef + (size_t)d->nbasis * d->norb);
   s->cdet.assign(d->cdet, d->cdet + d->ndet);
   s->iworbd.assign(d->iworbd, d->iworbd + d->nelec);
+  s->iworbd_all.assign(d->iworbd, d->iworbd + (size_t)d->ndet * d->nelec);
+  if (d->ndet > 1 && !multideterminants_define(*s)) {
+    delete s;
+    return nullptr;
+  }
   s->norda = d->norda; s->nordb = d->nordb; s->nordc = d->nordc;
   s->isc = d->isc; s->nspin2b = d->nspin2b; s->nocuspb = d->nocuspb;
   s->scalek = d->scalek;
