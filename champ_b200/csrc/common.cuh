@@ -41,6 +41,8 @@ struct CSys {
   double b[2 * (CW_MAX_NORD + 1)];
   double c[CW_MAX_TYPES * CW_MAX_TERMS];
   float cf[CW_MAX_TYPES * CW_MAX_TERMS];   // FP32 copy of c (mixed-precision Jastrow)
+  // multideterminant expansion (ndet > 1)
+  int ndet, md_nuniq[2], md_ivirt[2], md_iactv[2];
   double asymp_jasa[CW_MAX_TYPES];
   // ECP
   int lpot[CW_MAX_TYPES];
@@ -119,6 +121,10 @@ struct MoveBuf {
   double *enn;        // [W][2][M]  e-n row (rr, dd1/r) of the moved electron at xnew
   float *phi_hi, *phi_lo;  // mixed precision: [W*4][kp] split basis rows (null in FP64)
   int kp;                  // row pitch of phi_hi/phi_lo (K rounded up to 32)
+  // multideterminant terms of the move (null for one determinant)
+  const double *md_velo;   // [W][3] drift correction at the old position
+  const double *md_veln;   // [W][3] drift correction at the proposed position
+  const double *md_psidn;  // [W]    psi_D at the proposed position
 };
 
 // ---------------------------------------------------------------------------

@@ -45,7 +45,8 @@ __device__ __forceinline__ double gauss_d(DRng &r) {
 
 // drift of electron e: slmi row · dorbs + vj (compute_determinante_grad
 // iflag_move=1)
-__device__ __forceinline__ void drift_old(const WState &st, int w, int e, double v[3]) {
+__device__ __forceinline__ void drift_old(const WState &st, int w, int e, double v[3],
+                                          const double *md_vel = nullptr) {
   const int N = cs.N, nmax = cs.nmax;
   const int iab = e < cs.nup ? 0 : 1, nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
   const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * (e - ish);
@@ -57,9 +58,9 @@ __device__ __forceinline__ void drift_old(const WState &st, int w, int e, double
     g2 += s * st.dorbs[(((size_t)w * 3 + 2) * N + e) * nmax + j];
   }
   const double *fjo = st.fjo + (size_t)w * 3 * N;
-  v[0] = 0.0 + g0 + fjo[e];
-  v[1] = 0.0 + g1 + fjo[N + e];
-  v[2] = 0.0 + g2 + fjo[2 * N + e];
+  v[0] = (md_vel ? md_vel[0] : 0.0) + g0 + fjo[e];
+  v[1] = (md_vel ? md_vel[1] : 0.0) + g1 + fjo[N + e];
+  v[2] = (md_vel ? md_vel[2] : 0.0) + g2 + fjo[2 * N + e];
 }
 
 // thread per walker: drift + Gaussian diffusion of electron iel
@@ -68,7 +69,7 @@ __global__ void k_dmc_propose(WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, i
   if (w >= st.W) return;
   const int N = cs.N;
   double vo[3];
-  drift_old(st, w, iel, vo);
+  drift_old(st, w, iel, vo, mb.md_velo ? mb.md_velo + 3 * w : nullptr);
   for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + iel] = vo[k];
   const double tau = sc.tau, rttau = sqrt(tau), adrift = 0.5;
   const double v2old = vo[0] * vo[0] + vo[1] * vo[1] + vo[2] * vo[2];
@@ -105,7 +106,7 @@ __global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalar
   double ratio = 0;
   for (int j = 0; j < nel; j++) ratio += sl[j] * orbn[slot[j]];
   const double detn = st.detiab[2 * w + iab] * ratio;
-  const double psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
+  const double psidn = mb.md_psidn ? mb.md_psidn[w] : detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
   const double psijn = mb.fsumn[w];
   double vn[3] = {0, 0, 0};
   if (detn != 0.0) {
@@ -116,9 +117,10 @@ __global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalar
       v1 += s * orbn[2 * Oa + slot[j]];
       v2 += s * orbn[3 * Oa + slot[j]];
     }
-    vn[0] = 0.0 + v0 + mb.vjn[3 * w + 0];
-    vn[1] = 0.0 + v1 + mb.vjn[3 * w + 1];
-    vn[2] = 0.0 + v2 + mb.vjn[3 * w + 2];
+    const double *mv = mb.md_veln ? mb.md_veln + 3 * w : nullptr;
+    vn[0] = (mv ? mv[0] : 0.0) + v0 + mb.vjn[3 * w + 0];
+    vn[1] = (mv ? mv[1] : 0.0) + v1 + mb.vjn[3 * w + 1];
+    vn[2] = (mv ? mv[2] : 0.0) + v2 + mb.vjn[3 * w + 2];
   }
   const double psido = st.psido[w], psijo = st.psijo[w];
   if (psidn * psido <= 0.0) acc[DA_NODECR] += 1;  // icross=1: counted, the move is not refused
@@ -160,7 +162,7 @@ __global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalar
 // Warp per walker, after hpsi: drift of every electron, fratio
 // (dmc_eloc_cutoff, nloc>0 branch), and for mode 1 the reweighting
 // (calculate_reweight) and the walker's sums of the step.
-__global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode) {
+__global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode, const double *md_vall) {
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= st.W) return;
@@ -169,7 +171,7 @@ __global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode) {
   double vav2sum = 0, v2sum = 0;
   for (int e = lane; e < N; e += 32) {
     double v[3];
-    drift_old(st, w, e, v);
+    drift_old(st, w, e, v, md_vall ? md_vall + ((size_t)w * N + e) * 3 : nullptr);
     for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + e] = v[k];
     const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
     const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2 * tau * 1.0) - 1.0) / (adrift * v2);
@@ -228,8 +230,8 @@ __global__ void k_set_quad(WState st, QuadRot q) {
 // stream, which stays with its slot.
 struct WalkerRec {
   int nfield;
-  double *ptr[20];
-  long len[20];  // doubles per walker
+  double *ptr[24];
+  long len[24];  // doubles per walker
 };
 
 // CTA per copy: walker copy_src[c] -> slot copy_dst[c].  The host guarantees

@@ -18,6 +18,7 @@
 #include "hpsi.cuh"
 #include "move.cuh"
 #include "dmc.cuh"
+#include "mdet.cuh"
 #include "peak.cuh"
 #include "umma.cuh"
 
@@ -74,6 +75,12 @@ struct cw_ctx {
   double stage_ms[CW_NSTAGE] = {0};
   long stage_n[CW_NSTAGE] = {0};
   DmcHost dmc;
+  // multideterminant expansion
+  bool md_on = false;
+  MdTab mdt{};
+  MdBuf md{};
+  double *md_vall = nullptr;     // [W][N][3] drift corrections of every electron (DMC)
+  size_t smem_md_hpsi = 0, smem_md_phase = 0, smem_md_move = 0;
   // mixed precision: tensor-core LCAO (TF32 x3) operands and tensor maps
   bool mixed = false;
   int kp = 0, np = 0, umma_st = 0;
@@ -234,6 +241,111 @@ int nord_attrs(cw_ctx *c) {
   }
 }
 
+// multideterminants_define (vmc/set_input_data.f90:46-414), kref = the
+// first determinant: per spin the excitation (replaced reference slots in
+// slot order, new orbitals in the determinant's order) of every
+// determinant, the permutation sign folded into the coefficient, the unique
+// spin-determinants ordered singles, doubles, rest (stable within each
+// class), and for every determinant the unique index of each spin part
+// (-1: the same as the reference).
+int md_define(cw_ctx *c, const cw_system_desc *d, std::vector<int> &exc, std::vector<int> &kw,
+              std::vector<double> &cdet, int nuniq[2], int ivirt[2], int iactv[2], int &numax) {
+  const int N = d->nelec, nd = d->ndet, nup = d->nup, ndn = N - nup;
+  auto IW = [&](int k, int i) { return d->iworbd[(size_t)k * N + i]; };
+  for (size_t t = 0; t < (size_t)nd * N; t++)
+    if (d->iworbd[t] < 1 || d->iworbd[t] > d->norb) return fail(c, CW_ERR_ARG, "iworbd entry out of range");
+  std::vector<int> numrep((size_t)nd * 2, 0), irc((size_t)nd * 2 * N, 0), iro((size_t)nd * 2 * N, 0);
+  cdet.assign(d->cdet, d->cdet + nd);
+  for (int k = 1; k < nd; k++) {
+    int itot = 0;
+    for (int iab = 0; iab < 2; iab++) {
+      const int nel = iab == 0 ? nup : ndn, ish = iab == 0 ? 0 : nup;
+      int nr = 0;
+      for (int iref = 0; iref < nel; iref++) {
+        bool in = false;
+        for (int i = 0; i < nel; i++)
+          if (IW(k, i + ish) == IW(0, iref + ish)) in = true;
+        if (!in) irc[((size_t)k * 2 + iab) * N + nr++] = iref;
+      }
+      int isub = 0;
+      for (int i = 0; i < nel; i++) {
+        bool in = false;
+        for (int iref = 0; iref < nel; iref++)
+          if (IW(k, i + ish) == IW(0, iref + ish)) in = true;
+        if (!in) iro[((size_t)k * 2 + iab) * N + isub++] = IW(k, i + ish) - 1;
+      }
+      if (isub != nr) return fail(c, CW_ERR_ARG, "determinant %d: inconsistent excitation", k + 1);
+      numrep[k * 2 + iab] = nr;
+      std::vector<int> sw(nel);
+      for (int i = 0; i < nel; i++) sw[i] = IW(0, i + ish);
+      for (int r = 0; r < nr; r++) sw[irc[((size_t)k * 2 + iab) * N + r]] = iro[((size_t)k * 2 + iab) * N + r] + 1;
+      for (int i = 0; i < nel; i++)
+        if (IW(k, i + ish) != sw[i])
+          for (int l = i + 1; l < nel; l++)
+            if (sw[l] == IW(k, i + ish)) {
+              std::swap(sw[i], sw[l]);
+              itot++;
+            }
+    }
+    if (itot % 2) cdet[k] = -cdet[k];
+  }
+  kw.assign((size_t)nd * 2, -1);
+  std::vector<std::vector<int>> order(2);
+  for (int iab = 0; iab < 2; iab++) {
+    const int nel = iab == 0 ? nup : ndn;
+    iactv[iab] = nel;
+    ivirt[iab] = iab == 0 ? nup : ndn;
+    for (int k = 1; k < nd; k++)
+      for (int r = 0; r < numrep[k * 2 + iab]; r++) {
+        iactv[iab] = std::min(iactv[iab], irc[((size_t)k * 2 + iab) * N + r]);
+        ivirt[iab] = std::min(ivirt[iab], iro[((size_t)k * 2 + iab) * N + r]);
+      }
+    auto same = [&](int a, int b) {
+      if (numrep[a * 2 + iab] != numrep[b * 2 + iab]) return false;
+      for (int r = 0; r < numrep[a * 2 + iab]; r++)
+        if (irc[((size_t)a * 2 + iab) * N + r] != irc[((size_t)b * 2 + iab) * N + r] ||
+            iro[((size_t)a * 2 + iab) * N + r] != iro[((size_t)b * 2 + iab) * N + r])
+          return false;
+      return true;
+    };
+    std::vector<int> iwun(nd, 0), uniq;
+    for (int i = 1; i < nd; i++) {
+      if (numrep[i * 2 + iab] == 0) continue;
+      int j = 0;
+      while (j != i && !same(j, i)) j++;
+      iwun[i] = j;
+      if (j == i) uniq.push_back(i);
+    }
+    for (int pass = 0; pass < 3; pass++)
+      for (int k : uniq) {
+        const int nr = numrep[k * 2 + iab];
+        if ((pass == 0 && nr == 1) || (pass == 1 && nr == 2) || (pass == 2 && nr > 2)) order[iab].push_back(k);
+      }
+    std::vector<int> kidx(nd, -1);
+    for (size_t kk = 0; kk < order[iab].size(); kk++) kidx[order[iab][kk]] = (int)kk;
+    for (int k = 1; k < nd; k++)
+      if (numrep[k * 2 + iab] > 0) kw[(size_t)k * 2 + iab] = kidx[iwun[k]];
+    nuniq[iab] = (int)order[iab].size();
+  }
+  numax = std::max(1, std::max(nuniq[0], nuniq[1]));
+  const int stride = 1 + 2 * CW_MD_MEX;
+  exc.assign((size_t)2 * numax * stride, 0);
+  for (int iab = 0; iab < 2; iab++)
+    for (int kk = 0; kk < nuniq[iab]; kk++) {
+      const int k = order[iab][kk], nr = numrep[k * 2 + iab];
+      if (nr > CW_MD_MEX)
+        return fail(c, CW_ERR_UNSUPPORTED, "determinant %d: %d-fold excitation (at most %d supported)", k + 1, nr,
+                    CW_MD_MEX);
+      int *e = &exc[((size_t)iab * numax + kk) * stride];
+      e[0] = nr;
+      for (int r = 0; r < nr; r++) {
+        e[1 + r] = irc[((size_t)k * 2 + iab) * N + r];
+        e[1 + CW_MD_MEX + r] = iro[((size_t)k * 2 + iab) * N + r];
+      }
+    }
+  return CW_OK;
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -289,6 +401,43 @@ int lcao(cw_ctx *c, bool move, int M, const double *phi64, double *out) {
   return launch_check(c, "k_lcao_tf32x3");
 }
 
+// Multideterminant steps of a single-electron move (no-ops for one
+// determinant): before the proposal (spin-phase G and Y, drift at the old
+// position), after the LCAO (tables at the proposed position), after the
+// commit (tables of an accepted move).
+int md_before_propose(cw_ctx *c, int iel) {
+  if (!c->md_on) return CW_OK;
+  const CSys &h = c->h;
+  const int W = c->W;
+  if (iel == 0 || (iel == h.nup && h.ndn > 0)) {
+    stage_begin(c, CW_ST_MDET);
+    k_md_phase<<<W, 128, c->smem_md_phase, c->stream>>>(c->st, c->md, c->mdt, iel == 0 ? 0 : 1);
+    stage_end(c);
+    LCHK("k_md_phase");
+  }
+  stage_begin(c, CW_ST_MDET);
+  k_md_drift_old<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->md, c->g, iel);
+  stage_end(c);
+  LCHK("k_md_drift_old");
+  return CW_OK;
+}
+int md_after_lcao(cw_ctx *c, int iel) {
+  if (!c->md_on) return CW_OK;
+  stage_begin(c, CW_ST_MDET);
+  k_md_move<<<c->W, 128, c->smem_md_move, c->stream>>>(c->st, c->mb, c->md, c->mdt, c->g, iel);
+  stage_end(c);
+  LCHK("k_md_move");
+  return CW_OK;
+}
+int md_after_commit(cw_ctx *c, int iel) {
+  if (!c->md_on) return CW_OK;
+  stage_begin(c, CW_ST_MDET);
+  k_md_commit<<<c->W, 128, 0, c->stream>>>(c->st, c->mb, c->md, c->mdt, iel);
+  stage_end(c);
+  LCHK("k_md_commit");
+  return CW_OK;
+}
+
 // Full local energy of every walker (hpsi).  mode 1 also adds metrop6's sums.
 int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullptr) {
   const CSys &h = c->h;
@@ -313,6 +462,13 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
       stage_end(c);
       if (rc) return rc;
     }
+    if (c->md_on) {
+      const long nt = (long)W * ne * h.Oa;
+      stage_begin(c, CW_ST_SCATTER);
+      k_md_scatter<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->md, c->hb.orball, e0, ne);
+      stage_end(c);
+      LCHK("k_md_scatter");
+    }
     const long ns = (long)W * ne * h.nmax;
     stage_begin(c, CW_ST_SCATTER);
     k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
@@ -323,6 +479,11 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
   k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->st, c->hb);
   stage_end(c);
   LCHK("k_slater_inv");
+  if (h.nloc > 0 && c->md_on) {
+    const size_t np = (size_t)W * N * h.K;
+    k_md_zero<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(c->md.P, np);
+    LCHK("k_md_zero");
+  }
   if (h.nloc > 0) {
     const int nchunk = (h.K + 63) / 64;
     stage_begin(c, CW_ST_CTILDE);
@@ -333,6 +494,19 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     NORD_DISPATCH(launch_ecp, c);
     stage_end(c);
     LCHK("k_ecp");
+    if (c->md_on) {
+      // pseudopotential B matrix of every orbital: P x coef
+      stage_begin(c, CW_ST_LCAO_ALL);
+      dgemm(c->stream, W * N, h.Oa, h.K, c->md.P, c->g.coefT, c->md.bnl);
+      stage_end(c);
+      LCHK("dgemm(bnl)");
+    }
+  }
+  if (c->md_on) {
+    stage_begin(c, CW_ST_MDET);
+    k_md_hpsi<<<W, 128, c->smem_md_hpsi, c->stream>>>(c->st, c->md, c->mdt, c->g);
+    stage_end(c);
+    LCHK("k_md_hpsi");
   }
   stage_begin(c, CW_ST_ENERGY);
   k_energy<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->hb, mode, d_e, d_ekin);
@@ -438,6 +612,40 @@ int alloc_walkers(cw_ctx *c, int W) {
     if (rc) return rc;
   }
   if (h.nloc > 0) DALLOC(L, b.ctilde, (size_t)W * N * K);
+  m.md_velo = m.md_veln = m.md_psidn = nullptr;
+  b.md_P = nullptr;
+  b.md_den = b.md_S = nullptr;
+  c->md_vall = nullptr;
+  if (c->md_on) {
+    MdBuf &d = c->md;
+    const int nu = c->mdt.numax;
+    DALLOC(L, d.aa, (size_t)W * 2 * nmax * Oa);
+    DALLOC(L, d.ymat, (size_t)W * 2 * nmax * Oa);
+    DALLOC(L, d.dd, (size_t)W * 2 * nu);
+    DALLOC(L, d.G, (size_t)W * (nu + 1));
+    DALLOC(L, d.S, W);
+    DALLOC(L, d.orbA, (size_t)W * N * Oa);
+    DALLOC(L, d.dorbA, (size_t)W * 3 * N * Oa);
+    DALLOC(L, d.bkin, (size_t)W * N * Oa);
+    DALLOC(L, d.bnl, (size_t)W * N * Oa);
+    CK(cudaMemsetAsync(d.bnl, 0, sizeof(double) * (size_t)W * N * Oa, c->stream));
+    if (h.nloc > 0) DALLOC(L, d.P, (size_t)W * N * K);
+    DALLOC(L, d.den, (size_t)W * 2);
+    DALLOC(L, d.aan, (size_t)W * nmax * Oa);
+    DALLOC(L, d.yn, (size_t)W * nmax * Oa);
+    DALLOC(L, d.ddn, (size_t)W * nu);
+    DALLOC(L, d.Sn, W);
+    DALLOC(L, d.psidn, W);
+    DALLOC(L, d.veln, (size_t)W * 3);
+    DALLOC(L, d.velo, (size_t)W * 3);
+    DALLOC(L, c->md_vall, (size_t)W * N * 3);
+    m.md_velo = d.velo;
+    m.md_veln = d.veln;
+    m.md_psidn = d.psidn;
+    b.md_P = d.P;
+    b.md_den = d.den;
+    b.md_S = d.S;
+  }
   DALLOC(L, b.entab, (size_t)W * M * N * 8);
   CK(cudaMemsetAsync(s.status, 0, sizeof(int) * W, c->stream));
   CK(cudaMemsetAsync(s.sums, 0, sizeof(double) * W * 8, c->stream));
@@ -493,7 +701,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   if (d->nctype > CW_MAX_TYPES) return bad("nctype exceeds CW_MAX_TYPES");
   if (d->mrwf > CW_MAX_RWF) return bad("mrwf exceeds CW_MAX_RWF");
   if (d->nordc > CW_MAX_NORD || d->norda > CW_MAX_NORD || d->nordb > CW_MAX_NORD) return bad("Jastrow order > 7");
-  if (d->ndet != 1) return bad("this engine version evaluates single-determinant wave functions (ndet=1)");
+  if (d->ndet < 1) return bad("ndet must be at least 1");
   if (d->nloc != 0 && d->nloc != 4) return bad("nloc must be 0 or 4");
   if (d->nquad > 32) return bad("nquad > 32 not supported");
   if (d->isc < 2 || d->isc > 5) return bad("isc must be 2..5");
@@ -686,6 +894,42 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   int rc = nord_attrs(c);
   if (rc) return rc;
   if (c->smem_ecp > 227 * 1024 && h.nloc) return fail(c, CW_ERR_UNSUPPORTED, "ECP stage shared memory too large");
+  if (d->ndet > 1) {
+    // compact multideterminant tables (multideterminants_define)
+    std::vector<int> exc, kw;
+    std::vector<double> cdet;
+    int nuniq[2], ivirt[2], iactv[2], numax = 1;
+    rc = md_define(c, d, exc, kw, cdet, nuniq, ivirt, iactv, numax);
+    if (rc) return rc;
+    h.ndet = d->ndet;
+    for (int s2 = 0; s2 < 2; s2++) {
+      h.md_nuniq[s2] = nuniq[s2];
+      h.md_ivirt[s2] = ivirt[s2];
+      h.md_iactv[s2] = iactv[s2];
+    }
+    CK(cudaMemcpyToSymbol(cs, &h, sizeof(CSys)));
+    int *dexc, *dkw;
+    double *dcd;
+    DALLOC(L, dexc, exc.size());
+    DALLOC(L, dkw, kw.size());
+    DALLOC(L, dcd, cdet.size());
+    CK(cudaMemcpy(dexc, exc.data(), sizeof(int) * exc.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dkw, kw.data(), sizeof(int) * kw.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dcd, cdet.data(), sizeof(double) * cdet.size(), cudaMemcpyHostToDevice));
+    c->mdt = MdTab{dexc, dkw, dcd, numax};
+    c->md_on = true;
+    const size_t O = h.Oa;
+    c->smem_md_hpsi = sizeof(double) * (4 * (size_t)nmax * nmax + (size_t)nmax * O + numax + 1);
+    c->smem_md_phase = sizeof(double) * ((size_t)nmax * O + numax + 1);
+    c->smem_md_move = sizeof(double) * (2 * (size_t)nmax + O + 2 * (size_t)nmax * O + numax);
+    const size_t lim = 227 * 1024;
+    if (c->smem_md_hpsi > lim || c->smem_md_move > lim)
+      return fail(c, CW_ERR_UNSUPPORTED, "multideterminant tables exceed shared memory (nmax %d, norb %d, %d unique)",
+                  nmax, h.Oa, numax);
+    CK(cudaFuncSetAttribute(k_md_hpsi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_hpsi));
+    CK(cudaFuncSetAttribute(k_md_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_phase));
+    CK(cudaFuncSetAttribute(k_md_move, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_move));
+  }
   if (precision == CW_PREC_MIXED) {
     // tensor-core LCAO: coefficients split once into TF32 hi/lo, [Oa][kp]
     c->mixed = true;
@@ -810,6 +1054,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
       LCHK("k_rotqua");
     }
     for (int i = 0; i < h.N; i++) {
+      if (int rc = md_before_propose(c, i)) return rc;
       stage_begin(c, CW_ST_PROPOSE);
       k_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, i);
       stage_end(c);
@@ -829,6 +1074,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
         stage_end(c);
         if (rc) return rc;
       }
+      if (int rc = md_after_lcao(c, i)) return rc;
       stage_begin(c, CW_ST_ACCEPT);
       k_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, i);
       stage_end(c);
@@ -837,6 +1083,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
       k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
       stage_end(c);
       LCHK("k_commit");
+      if (int rc = md_after_commit(c, i)) return rc;
     }
     int rc = run_hpsi(c, 1);
     if (rc) return rc;
@@ -1333,7 +1580,11 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   d.fprod = 1.0;
   d.wdsumo = nwalk;
   const DmcScalars sc{tau, etrial, d.eest, 1.0, 1.0};
-  k_dmc_weights<<<(nwalk + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 0);
+  if (c->md_on) {
+    k_md_drift_all<<<(unsigned)(((long)nwalk * N + 3) / 4), 128, 0, c->stream>>>(c->st, c->md, c->g, c->md_vall);
+    LCHK("k_md_drift_all");
+  }
+  k_dmc_weights<<<(nwalk + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 0, c->md_vall);
   LCHK("k_dmc_weights(init)");
   for (int w = 0; w < nwalk; w++) d.h_wt[w] = 1.0;
   CK(cudaMemcpyAsync(b.wt, d.h_wt, sizeof(double) * nwalk, cudaMemcpyHostToDevice, c->stream));
@@ -1356,6 +1607,13 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   add_field(r, c->st.fjo, 3L * N);
   add_field(r, c->st.fsumo, 1);
   add_field(r, c->st.enm, 2L * h.M * N);
+  if (c->md_on) {
+    add_field(r, c->md.aa, 2L * nmax * h.Oa);
+    add_field(r, c->md.ymat, 2L * nmax * h.Oa);
+    add_field(r, c->md.dd, 2L * c->mdt.numax);
+    add_field(r, c->md.S, 1);
+    add_field(r, c->md.dorbA, 3L * N * h.Oa);
+  }
   add_field(r, b.vold, 3L * N);
   add_field(r, b.fratio, 1);
   CK(cudaStreamSynchronize(c->stream));
@@ -1402,6 +1660,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
     CK(cudaMemsetAsync(b.acc, 0, sizeof(double) * W * DA_NA, c->stream));
     CK(cudaMemcpyAsync(b.eprev, c->st.eold, sizeof(double) * W, cudaMemcpyDeviceToDevice, c->stream));
     for (int i = 0; i < h.N; i++) {
+      if (int rc = md_before_propose(c, i)) return rc;
       stage_begin(c, CW_ST_PROPOSE);
       k_dmc_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, b, sc, i);
       stage_end(c);
@@ -1421,6 +1680,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
         stage_end(c);
         if (rc) return rc;
       }
+      if (int rc = md_after_lcao(c, i)) return rc;
       stage_begin(c, CW_ST_ACCEPT);
       k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, b, sc, i);
       stage_end(c);
@@ -1429,11 +1689,18 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
       stage_end(c);
       LCHK("k_commit");
+      if (int rc = md_after_commit(c, i)) return rc;
     }
     int rc = run_hpsi(c, 0);
     if (rc) return rc;
+    if (c->md_on) {
+      stage_begin(c, CW_ST_MDET);
+      k_md_drift_all<<<(unsigned)(((long)W * h.N + 3) / 4), 128, 0, c->stream>>>(c->st, c->md, c->g, c->md_vall);
+      stage_end(c);
+      LCHK("k_md_drift_all");
+    }
     stage_begin(c, CW_ST_DMC_WEIGHTS);
-    k_dmc_weights<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 1);
+    k_dmc_weights<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 1, c->md_vall);
     stage_end(c);
     LCHK("k_dmc_weights");
     CK(cudaMemcpyAsync(d.h_acc, b.acc, sizeof(double) * W * DA_NA, cudaMemcpyDeviceToHost, c->stream));

@@ -29,6 +29,10 @@ struct HBuf {
   int chunk;        // electrons per chunk
   float *phi_hi, *phi_lo;  // mixed precision: [rows][kp] split chunk basis (null in FP64)
   int kp;
+  // multideterminant (null for one determinant)
+  double *md_P;            // [W][N][K] pseudopotential quadrature basis sums
+  const double *md_den;    // [W][2] energy / kinetic corrections
+  const double *md_S;      // [W]    psi_D / (D_ref^up D_ref^dn)
 };
 
 __device__ __forceinline__ void pair_of(long p, int &i, int &j) {
@@ -606,7 +610,15 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
       fsum = warp_sum(fsum) + (warp_sum(fen) - fso[(size_t)i * N + i]);
       double term = 0;
       for (int l = 1; l <= cs.lpot[ict] - 1; l++) term += yl0_d(l, costh) * vps[4 * ic + (l - 1)];
-      vp_acc[iab] += term * cs.wq[q] * exp(fsum) * dr;
+      const double trj = term * cs.wq[q] * exp(fsum);
+      vp_acc[iab] += trj * dr;
+      if (hb.md_P) {
+        // pseudopotential B matrix of every orbital (nonloc.f90:271): the
+        // basis values of the point weighted by trj, contracted with coef later
+        double *P = hb.md_P + ((size_t)w * N + i) * K;
+        for (int m = lane; m < K; m += 32)
+          warp_basis_ao<0>(g, rec, m, [&](int, int, double v) { atomicAdd(&P[m], trj * v); });
+      }
       __syncwarp();
     }
   }
@@ -664,9 +676,11 @@ __global__ void k_energy(WState st, HBuf hb, int mode, double *out_e, double *ou
   const double vp0 = cs.nloc ? hb.vpsp[2 * w] : 0.0, vp1 = cs.nloc ? hb.vpsp[2 * w + 1] : 0.0;
   const double ekin_other = -hb_ * hb.d2o[w] + v2;
   const double e_other = ekin_other + pe;
-  const double energy = 0.0 + (ek[0] + vp0) + (ek[1] + vp1) + e_other;
-  const double ekin = 0.0 + ek[0] + ek[1] + ekin_other;
-  const double psid = st.detiab[2 * w] * st.detiab[2 * w + 1] * cs.cdet;
+  const double dener = hb.md_den ? hb.md_den[2 * w] : 0.0, dekin = hb.md_den ? hb.md_den[2 * w + 1] : 0.0;
+  const double energy = dener + (ek[0] + vp0) + (ek[1] + vp1) + e_other;
+  const double ekin = dekin + ek[0] + ek[1] + ekin_other;
+  const double psid = hb.md_S ? st.detiab[2 * w] * st.detiab[2 * w + 1] * hb.md_S[w]
+                             : st.detiab[2 * w] * st.detiab[2 * w + 1] * cs.cdet;
   const double psij = st.fsumo[w];
   st.eold[w] = energy;
   st.ekino[w] = ekin;

@@ -1,0 +1,524 @@
+// mdet.cuh — multideterminant wave functions, psi_D = sum_k c_k D_k^up D_k^dn
+// with determinants given as excitations of a reference (CHAMP's compact
+// table method: vmc/multideterminant.f90, vmc/multideterminante.f90,
+// vmc/set_input_data.f90:46).
+//
+// Per spin s, with A the reference Slater matrix and Phi the values of all
+// orbitals at the electrons of spin s:
+//   aa = A^-1 Phi                        (n x O, only columns >= ivirt used)
+//   d_s[kk] = det(aa[irepcol_kk, ireporb_kk])   excitation ratio of unique
+//                                        spin-determinant kk
+//   S = sum_k c_k d_up(k) d_dn(k)        (d = 1 for a kref-equivalent part)
+//   psi_D = D_ref^up D_ref^dn S
+// Y matrix of spin s: Y[irep][v] = sum_kk ceq[kk] (M_kk^-1)[jr][ir] at
+// (v, irep) = (ireporb[jr], irepcol[ir]), ceq[kk] = d_s[kk] G_s[kk] with
+//   G_s[kk] = sum_{k: spin-s part of k is kk} c_k d_other(k),
+// which depends only on the other spin.  During the moves of spin s the
+// other spin is frozen, so G_s is formed once per spin phase and each move
+// costs O(unique spin-determinants), not O(ndet).
+//
+//   k_md_scatter    orbital values / gradients of every orbital and the
+//                   kinetic B matrix (compute_bmatrices_kin) from hpsi's LCAO
+//   k_md_ecp_b      pseudopotential B matrix: quadrature basis sums x coef
+//   k_md_hpsi       aa, excitation ratios, S, Y of both spins, the energy
+//                   corrections (multideterminant_hpsi + hpsi :220-238)
+//   k_md_phase      G_s and Y_s at the start of the moves of spin s
+//                   (update_ymat, vmc/multideterminant.f90:562)
+//   k_md_drift_old  multideterminante_grad at the old position
+//   k_md_move       multideterminante at the proposed position: rank-1
+//                   update of aa, ratios, S, psi_D, Y, drift
+#pragma once
+#include "common.cuh"
+
+namespace cw {
+
+#define CW_MD_MEX 4   // largest excitation order handled on the GPU
+
+struct MdTab {
+  const int *exc;     // [2][nuniq_max][1 + 2*CW_MD_MEX]: numrep, irepcol[], ireporb[]
+  const int *kw;      // [ndet][2] unique index of each spin part, -1 = kref-equivalent
+  const double *cdet; // [ndet] sign-adjusted coefficients
+  int numax;          // nuniq_max
+};
+
+struct MdBuf {
+  double *aa;     // [W][2][nmax][O]
+  double *ymat;   // [W][2][nmax][O]  Y(v, irep) at [irep][v]
+  double *dd;     // [W][2][numax]
+  double *G;      // [W][numax + 1]  phase weights of the moving spin, [numax] = kref-equivalent part
+  double *S;      // [W]
+  double *orbA;   // [W][N][O]
+  double *dorbA;  // [W][3][N][O]
+  double *bkin;   // [W][N][O]
+  double *bnl;    // [W][N][O]
+  double *P;      // [W][N][K] quadrature basis sums of the pseudopotential
+  double *den;    // [W][2]  denergy, dekin
+  // move outputs (spin of the moved electron)
+  double *aan;    // [W][nmax][O]
+  double *yn;     // [W][nmax][O]
+  double *ddn;    // [W][numax]
+  double *Sn;     // [W]
+  double *psidn;  // [W]
+  double *veln;   // [W][3]
+  double *velo;   // [W][3]
+};
+
+__device__ __forceinline__ const int *md_exc(const MdTab &t, int s, int kk) {
+  return t.exc + ((size_t)s * t.numax + kk) * (1 + 2 * CW_MD_MEX);
+}
+
+// determinant and inverse of the excitation matrix M[ir][jr] =
+// aa[rc[ir]][ro[jr]] (aa row stride ld); inverse stored column-major as
+// CHAMP's wfmat: inv[jr + nr*ir] = (M^-1)(jr, ir)
+__device__ __forceinline__ double md_small_inv(const double *aa, int ld, const int *e, double *inv) {
+  const int nr = e[0];
+  const int *rc = e + 1, *ro = e + 1 + CW_MD_MEX;
+  if (nr == 1) {
+    const double d = aa[(size_t)rc[0] * ld + ro[0]];
+    inv[0] = 1.0 / d;
+    return d;
+  }
+  if (nr == 2) {
+    const double w0 = aa[(size_t)rc[0] * ld + ro[0]], w1 = aa[(size_t)rc[1] * ld + ro[0]];
+    const double w2 = aa[(size_t)rc[0] * ld + ro[1]], w3 = aa[(size_t)rc[1] * ld + ro[1]];
+    const double d = w0 * w3 - w2 * w1, di = 1.0 / d;
+    inv[0] = w3 * di;
+    inv[1] = -w1 * di;
+    inv[2] = -w2 * di;
+    inv[3] = w0 * di;
+    return d;
+  }
+  // Gauss-Jordan with partial pivoting on the column-major copy
+  double a[CW_MD_MEX * CW_MD_MEX], b[CW_MD_MEX * CW_MD_MEX];
+  for (int jr = 0; jr < nr; jr++)
+    for (int ir = 0; ir < nr; ir++) {
+      a[ir + nr * jr] = aa[(size_t)rc[ir] * ld + ro[jr]];
+      b[ir + nr * jr] = (ir == jr) ? 1.0 : 0.0;
+    }
+  double det = 1.0;
+  for (int c = 0; c < nr; c++) {
+    int p = c;
+    for (int r = c + 1; r < nr; r++)
+      if (fabs(a[r + nr * c]) > fabs(a[p + nr * c])) p = r;
+    if (p != c) {
+      det = -det;
+      for (int k = 0; k < nr; k++) {
+        double t = a[c + nr * k]; a[c + nr * k] = a[p + nr * k]; a[p + nr * k] = t;
+        t = b[c + nr * k]; b[c + nr * k] = b[p + nr * k]; b[p + nr * k] = t;
+      }
+    }
+    const double piv = a[c + nr * c];
+    det *= piv;
+    const double pinv = 1.0 / piv;
+    for (int k = 0; k < nr; k++) {
+      a[c + nr * k] *= pinv;
+      b[c + nr * k] *= pinv;
+    }
+    for (int r = 0; r < nr; r++) {
+      if (r == c) continue;
+      const double f = a[r + nr * c];
+      if (f == 0.0) continue;
+      for (int k = 0; k < nr; k++) {
+        a[r + nr * k] -= f * a[c + nr * k];
+        b[r + nr * k] -= f * b[c + nr * k];
+      }
+    }
+  }
+  for (int t = 0; t < nr * nr; t++) inv[t] = b[t];
+  return det;
+}
+
+template <int BS>
+__device__ __forceinline__ double md_block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double r = 0;
+  for (int k = 0; k < BS / 32; k++) r += red[k];
+  __syncthreads();
+  return r;  // valid on every thread
+}
+
+// orbital rows of every orbital and the kinetic B of one electron chunk
+__global__ void k_md_scatter(WState st, MdBuf md, const double *orball, int e0, int ne) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = cs.N, O = cs.Oa;
+  if (t >= (long)st.W * ne * O) return;
+  const int o = (int)(t % O);
+  const long we = t / O;
+  const int el = (int)(we % ne), w = (int)(we / ne), e = e0 + el;
+  const double *ob = orball + (size_t)we * 5 * O;
+  const double v = ob[o], d0 = ob[O + o], d1 = ob[2 * O + o], d2 = ob[3 * O + o], lap = ob[4 * O + o];
+  md.orbA[((size_t)w * N + e) * O + o] = v;
+  md.dorbA[(((size_t)w * 3 + 0) * N + e) * O + o] = d0;
+  md.dorbA[(((size_t)w * 3 + 1) * N + e) * O + o] = d1;
+  md.dorbA[(((size_t)w * 3 + 2) * N + e) * O + o] = d2;
+  const double vx = st.fjo[((size_t)w * 3 + 0) * N + e], vy = st.fjo[((size_t)w * 3 + 1) * N + e],
+               vz = st.fjo[((size_t)w * 3 + 2) * N + e];
+  md.bkin[((size_t)w * N + e) * O + o] = -0.5 * (lap + 2 * (vx * d0 + vy * d1 + vz * d2));
+}
+
+// G_s (and its kref-equivalent part) from the other spin's ratios; smem-free
+__device__ void md_form_G(const MdTab &tab, const MdBuf &md, int w, int s, double *G, double *red) {
+  const int NU = cs.md_nuniq[s];
+  for (int kk = threadIdx.x; kk <= NU; kk += blockDim.x) G[kk] = 0.0;
+  __syncthreads();
+  const double *dother = md.dd + ((size_t)w * 2 + (1 - s)) * tab.numax;
+  double gref = 0.0;
+  for (int k = threadIdx.x; k < cs.ndet; k += blockDim.x) {
+    const int kws = tab.kw[2 * k + s], kwo = tab.kw[2 * k + (1 - s)];
+    const double v = tab.cdet[k] * (kwo >= 0 ? dother[kwo] : 1.0);
+    if (kws >= 0) atomicAdd(&G[kws], v);
+    else gref += v;
+  }
+  gref = md_block_sum<128>(gref, red);
+  if (threadIdx.x == 0) G[NU] = gref;
+  __syncthreads();
+}
+
+// Y_s into shared memory Y[n][O] from aa (row stride O), ratios dd and G
+__device__ void md_form_Y(const MdTab &tab, int s, const double *aa, const double *dd, const double *G, double *Y) {
+  const int n = s == 0 ? cs.nup : cs.ndn, O = cs.Oa, NU = cs.md_nuniq[s];
+  for (int t = threadIdx.x; t < n * O; t += blockDim.x) Y[t] = 0.0;
+  __syncthreads();
+  for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
+    const int *e = md_exc(tab, s, kk);
+    double inv[CW_MD_MEX * CW_MD_MEX];
+    md_small_inv(aa, O, e, inv);
+    const double ceq = dd[kk] * G[kk];
+    const int nr = e[0];
+    for (int ir = 0; ir < nr; ir++)
+      for (int jr = 0; jr < nr; jr++) atomicAdd(&Y[e[1 + ir] * O + e[1 + CW_MD_MEX + jr]], ceq * inv[jr + nr * ir]);
+  }
+  __syncthreads();
+}
+
+// multideterminante_grad: velocity of electron e (spin s, slot jel) from
+// the drift operands: column c of A^-1 (c[irep] = slmi[irep + n*jel]),
+// gradients b_k[v] of every orbital at the electron, aa and Y (row stride
+// O); lanes of one warp over the virtual orbitals.  Returns the
+// detratio-scaled sum on every lane.
+__device__ void md_velocity_warp(int s, const double *c, const double *b0, const double *b1, const double *b2,
+                                 int bstride_slot /*1*/, const double *aa, const double *Y, const int *slot_orb,
+                                 double detratio, double vel[3]) {
+  const int n = s == 0 ? cs.nup : cs.ndn, O = cs.Oa;
+  const int ivirt = cs.md_ivirt[s], iactv = cs.md_iactv[s];
+  const int lane = threadIdx.x & 31;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int v = ivirt + lane; v < O; v += 32) {
+    double u = 0;
+    for (int irep = iactv; irep < n; irep++) u += Y[irep * O + v] * c[irep];
+    double t0 = 0, t1 = 0, t2 = 0;
+    for (int j = 0; j < n; j++) {
+      const double a = aa[j * O + v];
+      const int oj = slot_orb[j];
+      t0 += b0[oj] * a;
+      t1 += b1[oj] * a;
+      t2 += b2[oj] * a;
+    }
+    a0 += (b0[v] - t0) * u;
+    a1 += (b1[v] - t1) * u;
+    a2 += (b2[v] - t2) * u;
+  }
+  (void)bstride_slot;
+  vel[0] = warp_sum(a0) * detratio;
+  vel[1] = warp_sum(a1) * detratio;
+  vel[2] = warp_sum(a2) * detratio;
+}
+
+// ---------------------------------------------------------------------------
+// hpsi part: CTA (128 threads) per walker.  Shared: slmi of one spin (n*n),
+// X and X_kin (n*n each), Y (n*O), G (numax+1), reduction scratch.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab, GSys g) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
+  extern __shared__ __align__(16) double smem[];
+  double *Sl = smem;                       // nmax*nmax
+  double *X = Sl + nmax * nmax;            // nmax*nmax
+  double *Xk = X + nmax * nmax;            // nmax*nmax
+  double *T = Xk + nmax * nmax;            // nmax*nmax work
+  double *Y = T + nmax * nmax;             // nmax*O
+  double *G = Y + (size_t)nmax * O;        // numax+1
+  __shared__ double red[4];
+  // 1. aa and excitation ratios of both spins
+  for (int s = 0; s < 2; s++) {
+    const int n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+    if (n == 0) continue;
+    const double *slmi = st.slmi + ((size_t)w * 2 + s) * nmax * nmax;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) Sl[t] = slmi[t];
+    __syncthreads();
+    double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+    for (int t = threadIdx.x; t < n * O; t += blockDim.x) {
+      const int irep = t / O, v = t % O;
+      double d = 0;
+      for (int e = 0; e < n; e++) d += Sl[irep + n * e] * md.orbA[((size_t)w * N + ish + e) * O + v];
+      aa[t] = d;
+    }
+    __syncthreads();
+    double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
+    for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) {
+      double inv[CW_MD_MEX * CW_MD_MEX];
+      dd[kk] = md_small_inv(aa, O, md_exc(tab, s, kk), inv);
+    }
+  }
+  __syncthreads();
+  // 2. S
+  double sp = 0;
+  for (int k = threadIdx.x; k < cs.ndet; k += blockDim.x) {
+    const int k0 = tab.kw[2 * k], k1 = tab.kw[2 * k + 1];
+    const double d0 = k0 >= 0 ? md.dd[((size_t)w * 2 + 0) * tab.numax + k0] : 1.0;
+    const double d1 = k1 >= 0 ? md.dd[((size_t)w * 2 + 1) * tab.numax + k1] : 1.0;
+    sp += d0 * d1 * tab.cdet[k];
+  }
+  const double Ssum = md_block_sum<128>(sp, red);
+  // 3. per spin: Y, then the energy corrections sum_{irep>=iactv, v>=ivirt} Y tildem
+  double den = 0, dek = 0;
+  for (int s = 0; s < 2; s++) {
+    const int n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+    if (n == 0) continue;
+    const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+    const double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
+    md_form_G(tab, md, w, s, G, red);
+    md_form_Y(tab, s, aa, dd, G, Y);
+    double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
+    for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
+    // X = A^-1 B_occ A^-1 (bxmatrix) for B = bkin + bnl and for bkin
+    const double *slmi = st.slmi + ((size_t)w * 2 + s) * nmax * nmax;
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) Sl[t] = slmi[t];
+    __syncthreads();
+    for (int pass = 0; pass < 2; pass++) {
+      double *Xo = pass == 0 ? X : Xk;
+      // T[j][m] = sum_i B(occ_i, e_j) slmi[i + n m]
+      for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        const int j = t / n, m = t % n;
+        double a = 0;
+        for (int i = 0; i < n; i++) {
+          const int oi = g.slot_orb[s * nmax + i];
+          const size_t bi = ((size_t)w * N + ish + j) * O + oi;
+          const double bv = pass == 0 ? md.bkin[bi] + md.bnl[bi] : md.bkin[bi];
+          a += bv * Sl[i + n * m];
+        }
+        T[t] = a;
+      }
+      __syncthreads();
+      // X[m][np] (CHAMP xmat(m + n*np)) = sum_j T[j][m] slmi[np + n j]
+      for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        const int m = t / n, np = t % n;
+        double a = 0;
+        for (int j = 0; j < n; j++) a += T[j * n + m] * Sl[np + n * j];
+        Xo[m * n + np] = a;
+      }
+      __syncthreads();
+    }
+    const int ivirt = cs.md_ivirt[s], iactv = cs.md_iactv[s];
+    const int nv = O - ivirt, na = n - iactv;
+    for (int t = threadIdx.x; t < nv * na; t += blockDim.x) {
+      const int irep = iactv + t / nv, v = ivirt + t % nv;
+      double d2 = 0, d3 = 0, d4 = 0, d5 = 0;
+      for (int e = 0; e < n; e++) {
+        const size_t bi = ((size_t)w * N + ish + e) * O + v;
+        const double ov = md.orbA[bi];
+        const double sl = Sl[irep + n * e];
+        d2 += sl * (md.bkin[bi] + md.bnl[bi]);
+        d3 += X[e * n + irep] * ov;
+        d4 += sl * md.bkin[bi];
+        d5 += Xk[e * n + irep] * ov;
+      }
+      const double y = Y[irep * O + v];
+      den += y * (d2 - d3);
+      dek += y * (d4 - d5);
+    }
+    __syncthreads();
+  }
+  den = md_block_sum<128>(den, red);
+  dek = md_block_sum<128>(dek, red);
+  if (threadIdx.x == 0) {
+    md.S[w] = Ssum;
+    md.den[2 * w] = den / Ssum;
+    md.den[2 * w + 1] = dek / Ssum;
+  }
+}
+
+// pseudopotential B matrix: bnl[w][e][o] = sum_m P[w][e][m] coef(m, o) is
+// a GEMM launched by the host; this kernel only clears P before k_ecp
+__global__ void k_md_zero(double *p, size_t n) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) p[t] = 0.0;
+}
+
+// G_s and Y_s before the moves of spin s: CTA (128) per walker
+__global__ void __launch_bounds__(128) k_md_phase(WState st, MdBuf md, MdTab tab, int s) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int O = cs.Oa, nmax = cs.nmax, n = s == 0 ? cs.nup : cs.ndn;
+  extern __shared__ __align__(16) double smem[];
+  double *Y = smem;                  // nmax*O
+  double *G = Y + (size_t)nmax * O;  // numax+1
+  __shared__ double red[4];
+  md_form_G(tab, md, w, s, G, red);
+  double *gG = md.G + (size_t)w * (tab.numax + 1);
+  for (int kk = threadIdx.x; kk <= cs.md_nuniq[s]; kk += blockDim.x) gG[kk] = G[kk];
+  const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+  const double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
+  md_form_Y(tab, s, aa, dd, G, Y);
+  double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
+  for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
+}
+
+// multideterminante_grad at the old position of electron iel: warp per walker
+__global__ void k_md_drift_old(WState st, MdBuf md, GSys g, int iel) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= st.W) return;
+  const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
+  const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+  const double *c = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
+  const double *b0 = md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O;
+  const double *b1 = md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O;
+  const double *b2 = md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O;
+  const double detratio = st.detiab[2 * w] * st.detiab[2 * w + 1] / st.psido[w];
+  double vel[3];
+  md_velocity_warp(s, c, b0, b1, b2, 1, md.aa + ((size_t)w * 2 + s) * nmax * O,
+                   md.ymat + ((size_t)w * 2 + s) * nmax * O, g.slot_orb + s * nmax, detratio, vel);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; k++) md.velo[3 * w + k] = vel[k];
+}
+
+// drift correction of every electron at the current configuration (after
+// hpsi, dmc_ps :516): warp per (walker, electron); vall [W][N][3]
+__global__ void k_md_drift_all(WState st, MdBuf md, GSys g, double *vall) {
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
+  if (gw >= (long)st.W * N) return;
+  const int w = (int)(gw / N), e = (int)(gw % N);
+  const int s = e < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+  const double *c = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (e - ish);
+  const double *b0 = md.dorbA + (((size_t)w * 3 + 0) * N + e) * O;
+  const double *b1 = md.dorbA + (((size_t)w * 3 + 1) * N + e) * O;
+  const double *b2 = md.dorbA + (((size_t)w * 3 + 2) * N + e) * O;
+  const double detratio = st.detiab[2 * w] * st.detiab[2 * w + 1] / st.psido[w];
+  double vel[3];
+  md_velocity_warp(s, c, b0, b1, b2, 1, md.aa + ((size_t)w * 2 + s) * nmax * O,
+                   md.ymat + ((size_t)w * 2 + s) * nmax * O, g.slot_orb + s * nmax, detratio, vel);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; k++) vall[((size_t)w * N + e) * 3 + k] = vel[k];
+}
+
+// multideterminante at the proposed position of electron iel: CTA (128)
+// per walker.  Shared: c (nmax), slot values (nmax), w (O), aan (nmax*O),
+// Yn (nmax*O), ratios (numax).
+__global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md, MdTab tab, GSys g, int iel) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int O = cs.Oa, Oa = cs.Oa, nmax = cs.nmax;
+  const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+  const int ivirt = cs.md_ivirt[s], NU = cs.md_nuniq[s];
+  extern __shared__ __align__(16) double smem[];
+  double *c = smem;                       // nmax
+  double *ps = c + nmax;                  // nmax  new values of the slot orbitals
+  double *wv = ps + nmax;                 // O
+  double *An = wv + O;                    // nmax*O
+  double *Yn = An + (size_t)nmax * O;     // nmax*O
+  double *dn = Yn + (size_t)nmax * O;     // numax
+  __shared__ double red[4];
+  __shared__ double s_R;
+  if (mb.ms[w].igeo) {
+    if (threadIdx.x == 0) md.psidn[w] = 0.0;
+    return;
+  }
+  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    c[j] = sl[j];
+    ps[j] = orbn[g.slot_orb[s * nmax + j]];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0;
+    for (int j = 0; j < n; j++) r += c[j] * ps[j];
+    s_R = r;
+  }
+  __syncthreads();
+  const double R = s_R;
+  if (R == 0.0) {
+    if (threadIdx.x == 0) md.psidn[w] = 0.0;
+    return;
+  }
+  const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+  // w[v] = (psi_new[v] - sum_i phi_new(slot i) aa[i][v]) / R, aan = aa + c (x) w
+  for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) {
+    double t = 0;
+    for (int i = 0; i < n; i++) t += ps[i] * aa[i * O + v];
+    wv[v] = (orbn[v] - t) / R;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < n * O; t += blockDim.x) {
+    const int i = t / O, v = t % O;
+    An[t] = v >= ivirt ? aa[t] + c[i] * wv[v] : 0.0;
+  }
+  __syncthreads();
+  // ratios of the moving spin, S at the new position
+  const double *G = md.G + (size_t)w * (tab.numax + 1);
+  double sp = 0;
+  for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
+    double inv[CW_MD_MEX * CW_MD_MEX];
+    const double d = md_small_inv(An, O, md_exc(tab, s, kk), inv);
+    dn[kk] = d;
+    sp += d * G[kk];
+  }
+  const double Sn = md_block_sum<128>(sp, red) + G[NU];
+  md_form_Y(tab, s, An, dn, G, Yn);
+  const double detn_ref = st.detiab[2 * w + s] * R;
+  const double psidn = (s == 0 ? detn_ref * st.detiab[2 * w + 1] : st.detiab[2 * w] * detn_ref) * Sn;
+  // drift at the new position: column iel of the updated inverse is c / R
+  for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = c[j] / R;
+  __syncthreads();
+  const double detratio = (s == 0 ? detn_ref * st.detiab[2 * w + 1] : st.detiab[2 * w] * detn_ref) / psidn;
+  if (threadIdx.x < 32) {
+    double vel[3];
+    md_velocity_warp(s, c, orbn + Oa, orbn + 2 * Oa, orbn + 3 * Oa, 1, An, Yn, g.slot_orb + s * nmax, detratio, vel);
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < 3; k++) md.veln[3 * w + k] = vel[k];
+      md.psidn[w] = psidn;
+      md.Sn[w] = Sn;
+    }
+  }
+  double *aan = md.aan + (size_t)w * nmax * O;
+  double *yn = md.yn + (size_t)w * nmax * O;
+  for (int t = threadIdx.x; t < n * O; t += blockDim.x) {
+    aan[t] = An[t];
+    yn[t] = Yn[t];
+  }
+  double *ddn = md.ddn + (size_t)w * tab.numax;
+  for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) ddn[kk] = dn[kk];
+}
+
+// commit of an accepted move (with k_commit): aa, Y, ratios, S of the moved
+// spin and the gradient row of the moved electron
+__global__ void k_md_commit(WState st, MoveBuf mb, MdBuf md, MdTab tab, int iel) {
+  const int w = blockIdx.x;
+  if (w >= st.W || !mb.ms[w].acc) return;
+  const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
+  const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn;
+  const int ivirt = cs.md_ivirt[s];
+  double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+  double *y = md.ymat + ((size_t)w * 2 + s) * nmax * O;
+  const double *aan = md.aan + (size_t)w * nmax * O;
+  const double *yn = md.yn + (size_t)w * nmax * O;
+  for (int t = threadIdx.x; t < n * O; t += blockDim.x) {
+    if (t % O >= ivirt) aa[t] = aan[t];
+    y[t] = yn[t];
+  }
+  double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
+  for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) dd[kk] = md.ddn[(size_t)w * tab.numax + kk];
+  const double *orbn = mb.orbn + (size_t)w * 4 * O;
+  for (int o = threadIdx.x; o < O; o += blockDim.x)
+    for (int k = 0; k < 3; k++) md.dorbA[(((size_t)w * 3 + k) * N + iel) * O + o] = orbn[(1 + k) * O + o];
+  if (threadIdx.x == 0) md.S[w] = md.Sn[w];
+}
+
+}  // namespace cw

@@ -106,7 +106,9 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, d3b2 = 1.5, eps = 1.0e-10;
   const double deltar = cs.deltar, deltri = one / deltar, fbias = cs.fbias;
   const double *fjo = st.fjo + (size_t)w * 3 * N;
-  double vo[3] = {0.0 + g0 + fjo[0 * N + iel], 0.0 + g1 + fjo[1 * N + iel], 0.0 + g2 + fjo[2 * N + iel]};
+  const double m0 = mb.md_velo ? mb.md_velo[3 * w] : 0.0, m1 = mb.md_velo ? mb.md_velo[3 * w + 1] : 0.0,
+               m2 = mb.md_velo ? mb.md_velo[3 * w + 2] : 0.0;
+  double vo[3] = {m0 + g0 + fjo[0 * N + iel], m1 + g1 + fjo[1 * N + iel], m2 + g2 + fjo[2 * N + iel]};
   DRng rng;
   rng.load(st.rng + 4 * (size_t)w);
   MoveScratch m;
@@ -605,7 +607,7 @@ __global__ void k_decide(WState st, MoveBuf mb, GSys g, int iel) {
   if (!m.igeo) {
     for (int j = 0; j < nel; j++) ratio += sl[j] * orbn[slot[j]];
     const double detn = st.detiab[2 * w + iab] * ratio;
-    psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
+    psidn = mb.md_psidn ? mb.md_psidn[w] : detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
     if (detn != 0.0) {
       double v0 = 0, v1 = 0, v2 = 0;
       for (int j = 0; j < nel; j++) {
@@ -614,8 +616,9 @@ __global__ void k_decide(WState st, MoveBuf mb, GSys g, int iel) {
         v1 += sc * orbn[2 * Oa + slot[j]];
         v2 += sc * orbn[3 * Oa + slot[j]];
       }
-      const double vn[3] = {0.0 + v0 + mb.vjn[3 * w + 0], 0.0 + v1 + mb.vjn[3 * w + 1],
-                            0.0 + v2 + mb.vjn[3 * w + 2]};
+      const double *mv = mb.md_veln ? mb.md_veln + 3 * w : nullptr;
+      const double vn[3] = {(mv ? mv[0] : 0.0) + v0 + mb.vjn[3 * w + 0], (mv ? mv[1] : 0.0) + v1 + mb.vjn[3 * w + 1],
+                            (mv ? mv[2] : 0.0) + v2 + mb.vjn[3 * w + 2]};
       psi2n = log(fabs(1.0)) + 2 * (log(fabs(psidn)) + fsumn);
       const double deltar = cs.deltar, deltri = one / deltar;
       const double rminn = m.rminn, rminon = m.rminon;

@@ -82,9 +82,9 @@ typedef struct cw_system_desc {
   /* --- orbitals and determinants (slater, dorb_m) --- */
   int32_t nbasis, norb;
   const double *coef;          /* [norb][nbasis] = Fortran coef(nbasis,norb)          */
-  int32_t ndet;                /* this engine version: ndet == 1                      */
+  int32_t ndet;                /* determinants; kref = the first one                  */
   const int32_t *iworbd;       /* [ndet][nelec] 1-based orbital of each electron slot */
-  const double *cdet;          /* [ndet]                                              */
+  const double *cdet;          /* [ndet] (excitations up to 4-fold per spin on the GPU) */
 
   /* --- Jastrow ijas=4 (jastrow, bparm; read_jastrow_file) --- */
   int32_t norda, nordb, nordc;
@@ -197,7 +197,7 @@ enum {
   CW_ST_ROTQUA = 0, CW_ST_PROPOSE, CW_ST_JASTROW_MOVE, CW_ST_BASIS_MOVE, CW_ST_LCAO_MOVE,
   CW_ST_ACCEPT, CW_ST_JASTROW_FULL, CW_ST_BASIS_ALL, CW_ST_LCAO_ALL, CW_ST_SCATTER,
   CW_ST_SLATER_INV, CW_ST_CTILDE, CW_ST_ECP, CW_ST_ENERGY, CW_ST_COMMIT, CW_ST_DMC_WEIGHTS,
-  CW_ST_SPLITJ, CW_NSTAGE
+  CW_ST_SPLITJ, CW_ST_MDET, CW_NSTAGE
 };
 int cw_profile(cw_ctx *ctx, int enable);
 int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);

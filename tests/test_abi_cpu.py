@@ -57,9 +57,15 @@ def test_create_rejects_bad_input_without_gpu(lib):
     from champ_b200.abi import CW_PREC_FP64
     s = make_synthetic("tiny")
     d = s.desc()
-    d.ndet = 3
+    d.ndet = 0
     h = C.c_void_p()
     rc = lib.cw_create(C.byref(h), C.byref(d), 0, CW_PREC_FP64)
     assert rc == 1
-    assert b"single-determinant" in lib.cw_last_error(h)
+    assert b"ndet" in lib.cw_last_error(h)
+    lib.cw_destroy(h)
+    d = s.desc()
+    d.nquad = 40
+    h = C.c_void_p()
+    assert lib.cw_create(C.byref(h), C.byref(d), 0, CW_PREC_FP64) == 1
+    assert b"nquad" in lib.cw_last_error(h)
     lib.cw_destroy(h)
