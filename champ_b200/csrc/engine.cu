@@ -80,7 +80,7 @@ struct cw_ctx {
   MdTab mdt{};
   MdBuf md{};
   double *md_vall = nullptr;     // [W][N][3] drift corrections of every electron (DMC)
-  size_t smem_md_hpsi = 0, smem_md_phase = 0, smem_md_move = 0;
+  size_t smem_md_hpsi = 0, smem_md_phase = 0, smem_md_move = 0, smem_md_drift = 0;
   // mixed precision: tensor-core LCAO (TF32 x3) operands and tensor maps
   bool mixed = false;
   int kp = 0, np = 0, umma_st = 0;
@@ -416,7 +416,7 @@ int md_before_propose(cw_ctx *c, int iel) {
     LCHK("k_md_phase");
   }
   stage_begin(c, CW_ST_MDET);
-  k_md_drift_old<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->md, c->g, iel);
+  k_md_drift_old<<<W, 128, c->smem_md_drift, c->stream>>>(c->st, c->md, c->mdt, c->g, iel);
   stage_end(c);
   LCHK("k_md_drift_old");
   return CW_OK;
@@ -631,8 +631,8 @@ int alloc_walkers(cw_ctx *c, int W) {
     CK(cudaMemsetAsync(d.bnl, 0, sizeof(double) * (size_t)W * N * Oa, c->stream));
     if (h.nloc > 0) DALLOC(L, d.P, (size_t)W * N * K);
     DALLOC(L, d.den, (size_t)W * 2);
-    DALLOC(L, d.aan, (size_t)W * nmax * Oa);
-    DALLOC(L, d.yn, (size_t)W * nmax * Oa);
+    DALLOC(L, d.cvec, (size_t)W * nmax);
+    DALLOC(L, d.wvec, (size_t)W * Oa);
     DALLOC(L, d.ddn, (size_t)W * nu);
     DALLOC(L, d.Sn, W);
     DALLOC(L, d.psidn, W);
@@ -920,8 +920,9 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     c->md_on = true;
     const size_t O = h.Oa;
     c->smem_md_hpsi = sizeof(double) * (4 * (size_t)nmax * nmax + (size_t)nmax * O + numax + 1);
-    c->smem_md_phase = sizeof(double) * ((size_t)nmax * O + numax + 1);
-    c->smem_md_move = sizeof(double) * (2 * (size_t)nmax + O + 2 * (size_t)nmax * O + numax);
+    c->smem_md_phase = sizeof(double) * ((size_t)numax + 1);
+    c->smem_md_move = sizeof(double) * (2 * (size_t)nmax + 4 * O + (size_t)nmax * O);
+    c->smem_md_drift = sizeof(double) * ((size_t)nmax + 3 * O + (size_t)nmax * O);
     const size_t lim = 227 * 1024;
     if (c->smem_md_hpsi > lim || c->smem_md_move > lim)
       return fail(c, CW_ERR_UNSUPPORTED, "multideterminant tables exceed shared memory (nmax %d, norb %d, %d unique)",
@@ -929,6 +930,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     CK(cudaFuncSetAttribute(k_md_hpsi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_hpsi));
     CK(cudaFuncSetAttribute(k_md_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_phase));
     CK(cudaFuncSetAttribute(k_md_move, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_move));
+    CK(cudaFuncSetAttribute(k_md_drift_old, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_drift));
   }
   if (precision == CW_PREC_MIXED) {
     // tensor-core LCAO: coefficients split once into TF32 hi/lo, [Oa][kp]
@@ -1609,7 +1611,6 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   add_field(r, c->st.enm, 2L * h.M * N);
   if (c->md_on) {
     add_field(r, c->md.aa, 2L * nmax * h.Oa);
-    add_field(r, c->md.ymat, 2L * nmax * h.Oa);
     add_field(r, c->md.dd, 2L * c->mdt.numax);
     add_field(r, c->md.S, 1);
     add_field(r, c->md.dorbA, 3L * N * h.Oa);

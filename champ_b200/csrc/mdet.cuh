@@ -22,11 +22,15 @@
 //   k_md_ecp_b      pseudopotential B matrix: quadrature basis sums x coef
 //   k_md_hpsi       aa, excitation ratios, S, Y of both spins, the energy
 //                   corrections (multideterminant_hpsi + hpsi :220-238)
-//   k_md_phase      G_s and Y_s at the start of the moves of spin s
-//                   (update_ymat, vmc/multideterminant.f90:562)
+//   k_md_phase      G_s at the start of the moves of spin s (the role of
+//                   update_ymat, vmc/multideterminant.f90:562)
 //   k_md_drift_old  multideterminante_grad at the old position
 //   k_md_move       multideterminante at the proposed position: rank-1
-//                   update of aa, ratios, S, psi_D, Y, drift
+//                   update of aa, ratios, S, psi_D, drift
+// The moves never form Y: the drift needs only its contraction with one
+// inverse column, sum_{v,irep} Y[irep][v] t[v] c[irep], which regrouped per
+// excitation is sum_kk d_kk G_kk t[ro_kk] . M_kk^-1 c[rc_kk]; Y itself is
+// built once per sweep for the energy (k_md_hpsi) and the post-hpsi drifts.
 #pragma once
 #include "common.cuh"
 
@@ -54,8 +58,8 @@ struct MdBuf {
   double *P;      // [W][N][K] quadrature basis sums of the pseudopotential
   double *den;    // [W][2]  denergy, dekin
   // move outputs (spin of the moved electron)
-  double *aan;    // [W][nmax][O]
-  double *yn;     // [W][nmax][O]
+  double *cvec;   // [W][nmax] inverse column of the moved electron (before the move)
+  double *wvec;   // [W][O]    rank-1 factor of aa
   double *ddn;    // [W][numax]
   double *Sn;     // [W]
   double *psidn;  // [W]
@@ -126,6 +130,95 @@ __device__ __forceinline__ double md_small_inv(const double *aa, int ld, const i
   }
   for (int t = 0; t < nr * nr; t++) inv[t] = b[t];
   return det;
+}
+
+// det(M) and z = M^-1 b for the excitation matrix M[ir][jr] =
+// aa[rc[ir]][ro[jr]] and b[ir] = cvec[rc[ir]]: Gaussian elimination with
+// partial pivoting, fully unrolled in registers for NR <= 4.
+template <int NR>
+__device__ __forceinline__ double md_solve_nr(const double *aa, int ld, const int *rc, const int *ro,
+                                             const double *cvec, double *z) {
+  double a[NR][NR], b[NR];
+#pragma unroll
+  for (int ir = 0; ir < NR; ir++) {
+#pragma unroll
+    for (int jr = 0; jr < NR; jr++) a[ir][jr] = aa[(size_t)rc[ir] * ld + ro[jr]];
+    b[ir] = cvec[rc[ir]];
+  }
+  // M z = b with M[ir][jr]: eliminate over columns jr (unknown z[jr])
+  double det = 1.0;
+#pragma unroll
+  for (int c = 0; c < NR; c++) {
+    int p = c;
+#pragma unroll
+    for (int r = c + 1; r < NR; r++)
+      if (fabs(a[r][c]) > fabs(a[p][c])) p = r;
+    if (p != c) {
+      det = -det;
+#pragma unroll
+      for (int k = 0; k < NR; k++) {
+        // swap rows p and c without dynamic indexing: select per element
+        double tc = a[c][k], tp = 0;
+#pragma unroll
+        for (int r = c + 1; r < NR; r++)
+          if (r == p) tp = a[r][k];
+        a[c][k] = tp;
+#pragma unroll
+        for (int r = c + 1; r < NR; r++)
+          if (r == p) a[r][k] = tc;
+      }
+      double tc = b[c], tp = 0;
+#pragma unroll
+      for (int r = c + 1; r < NR; r++)
+        if (r == p) tp = b[r];
+      b[c] = tp;
+#pragma unroll
+      for (int r = c + 1; r < NR; r++)
+        if (r == p) b[r] = tc;
+    }
+    det *= a[c][c];
+    const double pinv = 1.0 / a[c][c];
+#pragma unroll
+    for (int r = c + 1; r < NR; r++) {
+      const double f = a[r][c] * pinv;
+#pragma unroll
+      for (int k = c; k < NR; k++) a[r][k] -= f * a[c][k];
+      b[r] -= f * b[c];
+    }
+  }
+#pragma unroll
+  for (int c = NR - 1; c >= 0; c--) {
+    double v = b[c];
+#pragma unroll
+    for (int k = c + 1; k < NR; k++) v -= a[c][k] * z[k];
+    z[c] = v / a[c][c];
+  }
+  return det;
+}
+
+// excitation ratio d = det(M) and the drift contraction sum_jr t[ro[jr]] z[jr]
+// with z = M^-1 cvec[rc] (t: 3 components, row stride tstride)
+__device__ __forceinline__ double md_ratio_contract(const double *aa, int ld, const int *e, const double *cvec,
+                                                    const double *t, int tstride, double g[3]) {
+  const int nr = e[0];
+  const int *rc = e + 1, *ro = e + 1 + CW_MD_MEX;
+  double z[CW_MD_MEX], d;
+  switch (nr) {
+    case 1: d = md_solve_nr<1>(aa, ld, rc, ro, cvec, z); break;
+    case 2: d = md_solve_nr<2>(aa, ld, rc, ro, cvec, z); break;
+    case 3: d = md_solve_nr<3>(aa, ld, rc, ro, cvec, z); break;
+    default: d = md_solve_nr<4>(aa, ld, rc, ro, cvec, z); break;
+  }
+  g[0] = g[1] = g[2] = 0;
+#pragma unroll
+  for (int jr = 0; jr < CW_MD_MEX; jr++) {
+    if (jr >= nr) break;
+    const int v = ro[jr];
+    g[0] += t[v] * z[jr];
+    g[1] += t[tstride + v] * z[jr];
+    g[2] += t[2 * tstride + v] * z[jr];
+  }
+  return d;
 }
 
 template <int BS>
@@ -351,45 +444,29 @@ __global__ void k_md_zero(double *p, size_t n) {
   if (t < n) p[t] = 0.0;
 }
 
-// G_s and Y_s before the moves of spin s: CTA (128) per walker
-__global__ void __launch_bounds__(128) k_md_phase(WState st, MdBuf md, MdTab tab, int s) {
-  const int w = blockIdx.x;
-  if (w >= st.W) return;
-  const int O = cs.Oa, nmax = cs.nmax, n = s == 0 ? cs.nup : cs.ndn;
-  extern __shared__ __align__(16) double smem[];
-  double *Y = smem;                  // nmax*O
-  double *G = Y + (size_t)nmax * O;  // numax+1
-  __shared__ double red[4];
-  md_form_G(tab, md, w, s, G, red);
-  double *gG = md.G + (size_t)w * (tab.numax + 1);
-  for (int kk = threadIdx.x; kk <= cs.md_nuniq[s]; kk += blockDim.x) gG[kk] = G[kk];
-  const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
-  const double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
-  md_form_Y(tab, s, aa, dd, G, Y);
-  double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
-  for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
+// drift operands t_k[v] = b_k[v] - sum_j b_k[occ_j] aa[j][v] of one
+// electron (multideterminante_grad's gmat without the slmi factor), shared
+__device__ __forceinline__ void md_form_t(int s, const double *b0, const double *b1, const double *b2,
+                                          const double *aa, const int *slot_orb, double *t) {
+  const int n = s == 0 ? cs.nup : cs.ndn, O = cs.Oa, ivirt = cs.md_ivirt[s];
+  for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) {
+    double t0 = 0, t1 = 0, t2 = 0;
+    for (int j = 0; j < n; j++) {
+      const double a = aa[j * O + v];
+      const int oj = slot_orb[j];
+      t0 += b0[oj] * a;
+      t1 += b1[oj] * a;
+      t2 += b2[oj] * a;
+    }
+    t[v] = b0[v] - t0;
+    t[O + v] = b1[v] - t1;
+    t[2 * O + v] = b2[v] - t2;
+  }
 }
 
-// multideterminante_grad at the old position of electron iel: warp per walker
-__global__ void k_md_drift_old(WState st, MdBuf md, GSys g, int iel) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= st.W) return;
-  const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
-  const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
-  const double *c = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
-  const double *b0 = md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O;
-  const double *b1 = md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O;
-  const double *b2 = md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O;
-  const double detratio = st.detiab[2 * w] * st.detiab[2 * w + 1] / st.psido[w];
-  double vel[3];
-  md_velocity_warp(s, c, b0, b1, b2, 1, md.aa + ((size_t)w * 2 + s) * nmax * O,
-                   md.ymat + ((size_t)w * 2 + s) * nmax * O, g.slot_orb + s * nmax, detratio, vel);
-  if ((threadIdx.x & 31) == 0)
-    for (int k = 0; k < 3; k++) md.velo[3 * w + k] = vel[k];
-}
-
-// drift correction of every electron at the current configuration (after
-// hpsi, dmc_ps :516): warp per (walker, electron); vall [W][N][3]
+// drift correction of every electron at the current configuration right
+// after hpsi (dmc_ps :516), from the Y matrix hpsi just built: warp per
+// (walker, electron); vall [W][N][3]
 __global__ void k_md_drift_all(WState st, MdBuf md, GSys g, double *vall) {
   const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
@@ -408,29 +485,85 @@ __global__ void k_md_drift_all(WState st, MdBuf md, GSys g, double *vall) {
     for (int k = 0; k < 3; k++) vall[((size_t)w * N + e) * 3 + k] = vel[k];
 }
 
+// G_s before the moves of spin s: CTA (128) per walker
+__global__ void __launch_bounds__(128) k_md_phase(WState st, MdBuf md, MdTab tab, int s) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  extern __shared__ __align__(16) double smem[];
+  double *G = smem;  // numax+1
+  __shared__ double red[4];
+  md_form_G(tab, md, w, s, G, red);
+  double *gG = md.G + (size_t)w * (tab.numax + 1);
+  for (int kk = threadIdx.x; kk <= cs.md_nuniq[s]; kk += blockDim.x) gG[kk] = G[kk];
+}
+
+// multideterminante_grad at the old position of electron iel, without the Y
+// matrix: vel = detratio * sum_kk d_kk G_kk sum_jr t[ro_jr] (M_kk^-1 c)[jr]
+// with c the column of A^-1 of the electron (the Y contraction regrouped per
+// excitation).  CTA (128) per walker; shared: c (nmax), t (3*O), aa (nmax*O).
+__global__ void __launch_bounds__(128) k_md_drift_old(WState st, MdBuf md, MdTab tab, GSys g, int iel) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
+  const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+  extern __shared__ __align__(16) double smem[];
+  double *c = smem;              // nmax
+  double *t = c + nmax;          // 3*O
+  double *A = t + 3 * O;         // nmax*O
+  __shared__ double red[4];
+  const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
+  const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = sl[j];
+  for (int q = threadIdx.x; q < n * O; q += blockDim.x) A[q] = aa[q];
+  __syncthreads();
+  md_form_t(s, md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O, md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O,
+            md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O, A, g.slot_orb + s * nmax, t);
+  __syncthreads();
+  const double *G = md.G + (size_t)w * (tab.numax + 1);
+  double v0 = 0, v1 = 0, v2 = 0;
+  for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) {
+    double gv[3];
+    const double d = md_ratio_contract(A, O, md_exc(tab, s, kk), c, t, O, gv);
+    const double ce = d * G[kk];
+    v0 += ce * gv[0];
+    v1 += ce * gv[1];
+    v2 += ce * gv[2];
+  }
+  v0 = md_block_sum<128>(v0, red);
+  v1 = md_block_sum<128>(v1, red);
+  v2 = md_block_sum<128>(v2, red);
+  if (threadIdx.x == 0) {
+    const double detratio = st.detiab[2 * w] * st.detiab[2 * w + 1] / st.psido[w];
+    md.velo[3 * w] = v0 * detratio;
+    md.velo[3 * w + 1] = v1 * detratio;
+    md.velo[3 * w + 2] = v2 * detratio;
+  }
+}
+
 // multideterminante at the proposed position of electron iel: CTA (128)
-// per walker.  Shared: c (nmax), slot values (nmax), w (O), aan (nmax*O),
-// Yn (nmax*O), ratios (numax).
+// per walker.  aa_new = aa + c (x) w with w[v] = (psi_new[v] - sum_i
+// phi_new(occ_i) aa[i][v]) / R (the Sherman-Morrison form of
+// slmin * orb_new), the excitation ratios, S, psi_D and the drift at the new
+// point.  Shared: c, slot values (nmax each), w (O), t (3*O), aa_new (nmax*O).
 __global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md, MdTab tab, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
-  const int O = cs.Oa, Oa = cs.Oa, nmax = cs.nmax;
+  const int O = cs.Oa, nmax = cs.nmax;
   const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
   const int ivirt = cs.md_ivirt[s], NU = cs.md_nuniq[s];
   extern __shared__ __align__(16) double smem[];
   double *c = smem;                       // nmax
-  double *ps = c + nmax;                  // nmax  new values of the slot orbitals
+  double *ps = c + nmax;                  // nmax
   double *wv = ps + nmax;                 // O
-  double *An = wv + O;                    // nmax*O
-  double *Yn = An + (size_t)nmax * O;     // nmax*O
-  double *dn = Yn + (size_t)nmax * O;     // numax
+  double *t = wv + O;                     // 3*O
+  double *An = t + 3 * O;                 // nmax*O
   __shared__ double red[4];
   __shared__ double s_R;
   if (mb.ms[w].igeo) {
     if (threadIdx.x == 0) md.psidn[w] = 0.0;
     return;
   }
-  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const double *orbn = mb.orbn + (size_t)w * 4 * O;
   const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     c[j] = sl[j];
@@ -449,56 +582,59 @@ __global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md
     return;
   }
   const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
-  // w[v] = (psi_new[v] - sum_i phi_new(slot i) aa[i][v]) / R, aan = aa + c (x) w
   for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) {
-    double t = 0;
-    for (int i = 0; i < n; i++) t += ps[i] * aa[i * O + v];
-    wv[v] = (orbn[v] - t) / R;
+    double tt = 0;
+    for (int i = 0; i < n; i++) tt += ps[i] * aa[i * O + v];
+    wv[v] = (orbn[v] - tt) / R;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < n * O; t += blockDim.x) {
-    const int i = t / O, v = t % O;
-    An[t] = v >= ivirt ? aa[t] + c[i] * wv[v] : 0.0;
+  for (int q = threadIdx.x; q < n * O; q += blockDim.x) {
+    const int i = q / O, v = q % O;
+    An[q] = v >= ivirt ? aa[q] + c[i] * wv[v] : 0.0;
   }
   __syncthreads();
-  // ratios of the moving spin, S at the new position
-  const double *G = md.G + (size_t)w * (tab.numax + 1);
-  double sp = 0;
-  for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
-    double inv[CW_MD_MEX * CW_MD_MEX];
-    const double d = md_small_inv(An, O, md_exc(tab, s, kk), inv);
-    dn[kk] = d;
-    sp += d * G[kk];
-  }
-  const double Sn = md_block_sum<128>(sp, red) + G[NU];
-  md_form_Y(tab, s, An, dn, G, Yn);
-  const double detn_ref = st.detiab[2 * w + s] * R;
-  const double psidn = (s == 0 ? detn_ref * st.detiab[2 * w + 1] : st.detiab[2 * w] * detn_ref) * Sn;
-  // drift at the new position: column iel of the updated inverse is c / R
+  // column iel of the updated inverse is c / R; drift operands at the new point
+  md_form_t(s, orbn + O, orbn + 2 * O, orbn + 3 * O, An, g.slot_orb + s * nmax, t);
+  __syncthreads();
   for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = c[j] / R;
   __syncthreads();
-  const double detratio = (s == 0 ? detn_ref * st.detiab[2 * w + 1] : st.detiab[2 * w] * detn_ref) / psidn;
-  if (threadIdx.x < 32) {
-    double vel[3];
-    md_velocity_warp(s, c, orbn + Oa, orbn + 2 * Oa, orbn + 3 * Oa, 1, An, Yn, g.slot_orb + s * nmax, detratio, vel);
-    if (threadIdx.x == 0) {
-      for (int k = 0; k < 3; k++) md.veln[3 * w + k] = vel[k];
-      md.psidn[w] = psidn;
-      md.Sn[w] = Sn;
-    }
-  }
-  double *aan = md.aan + (size_t)w * nmax * O;
-  double *yn = md.yn + (size_t)w * nmax * O;
-  for (int t = threadIdx.x; t < n * O; t += blockDim.x) {
-    aan[t] = An[t];
-    yn[t] = Yn[t];
-  }
+  const double *G = md.G + (size_t)w * (tab.numax + 1);
   double *ddn = md.ddn + (size_t)w * tab.numax;
-  for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) ddn[kk] = dn[kk];
+  double sp = 0, v0 = 0, v1 = 0, v2 = 0;
+  for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
+    double gv[3];
+    const double d = md_ratio_contract(An, O, md_exc(tab, s, kk), c, t, O, gv);
+    ddn[kk] = d;
+    const double ce = d * G[kk];
+    sp += ce;
+    v0 += ce * gv[0];
+    v1 += ce * gv[1];
+    v2 += ce * gv[2];
+  }
+  const double Sn = md_block_sum<128>(sp, red) + G[NU];
+  v0 = md_block_sum<128>(v0, red);
+  v1 = md_block_sum<128>(v1, red);
+  v2 = md_block_sum<128>(v2, red);
+  if (threadIdx.x == 0) {
+    const double detn_ref = st.detiab[2 * w + s] * R;
+    const double dpair = s == 0 ? detn_ref * st.detiab[2 * w + 1] : st.detiab[2 * w] * detn_ref;
+    const double psidn = dpair * Sn;
+    const double detratio = dpair / psidn;
+    md.veln[3 * w] = v0 * detratio;
+    md.veln[3 * w + 1] = v1 * detratio;
+    md.veln[3 * w + 2] = v2 * detratio;
+    md.psidn[w] = psidn;
+    md.Sn[w] = Sn;
+  }
+  // rank-1 factors for the commit (the inverse column before the move)
+  double *cv = md.cvec + (size_t)w * nmax;
+  double *wg = md.wvec + (size_t)w * O;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) cv[j] = c[j] * R;
+  for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) wg[v] = wv[v];
 }
 
-// commit of an accepted move (with k_commit): aa, Y, ratios, S of the moved
-// spin and the gradient row of the moved electron
+// commit of an accepted move (after k_commit): aa += c (x) w on the
+// virtual columns, ratios, S, and the gradient row of the moved electron
 __global__ void k_md_commit(WState st, MoveBuf mb, MdBuf md, MdTab tab, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W || !mb.ms[w].acc) return;
@@ -506,12 +642,11 @@ __global__ void k_md_commit(WState st, MoveBuf mb, MdBuf md, MdTab tab, int iel)
   const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn;
   const int ivirt = cs.md_ivirt[s];
   double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
-  double *y = md.ymat + ((size_t)w * 2 + s) * nmax * O;
-  const double *aan = md.aan + (size_t)w * nmax * O;
-  const double *yn = md.yn + (size_t)w * nmax * O;
-  for (int t = threadIdx.x; t < n * O; t += blockDim.x) {
-    if (t % O >= ivirt) aa[t] = aan[t];
-    y[t] = yn[t];
+  const double *cv = md.cvec + (size_t)w * nmax;
+  const double *wg = md.wvec + (size_t)w * O;
+  for (int q = threadIdx.x; q < n * O; q += blockDim.x) {
+    const int i = q / O, v = q % O;
+    if (v >= ivirt) aa[q] = aa[q] + cv[i] * wg[v];
   }
   double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
   for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) dd[kk] = md.ddn[(size_t)w * tab.numax + kk];

@@ -533,6 +533,9 @@ def make_synthetic(config: str, seed: int = 20261203) -> System:
     c1: 30 nuclei on a zig-zag chain alternating C-like (Z=4, ECP) and H-like
         (Z=1) centres, 120 electrons (60/60), 540 Gaussians, 60 orbitals.
     tiny: 2 nuclei, 6 electrons, small basis (fast parity cases).
+    c2: 12 nuclei, 40 electrons, 300 Gaussians, 80 orbitals, 10^4
+        determinants (multideterminant DMC).
+    he: He atom through the ECP path (DMC reaches the exact energy).
     """
     rng = np.random.default_rng(seed)
     if config == "c0":
@@ -567,7 +570,80 @@ def make_synthetic(config: str, seed: int = 20261203) -> System:
         return _assemble("tiny", rng, cent, [0, 1], [heavy, hyd], 5, 3, 4, 3, 2)
     if config == "he":
         return _helium()
+    if config == "c2":
+        return _c2(rng)
     raise ValueError(f"unknown synthetic config {config!r}")
+
+
+def ci_expansion(rng, nup, ndn, norb, ndet, pools=(150, 500, 300, 120), nact_occ=8, nact_virt=30,
+                 level_p=(0.1, 0.45, 0.3, 0.15)):
+    """Seeded CI expansion of single to quadruple excitations of the aufbau
+    reference (orbitals 1..nup / 1..ndn).
+
+    Spin strings come from per-level pools (excitations from the top
+    nact_occ occupied slots into the lowest nact_virt virtual orbitals), as
+    selected-CI expansions reuse spin strings; each determinant pairs an up
+    and a down string whose levels add up to 1..4.  Coefficients decay as
+    |c_k| = k**-1.5 with random signs, c_1 = 1 for the reference.
+    Returns (iworbd [ndet][nup+ndn] 1-based, cdet [ndet]).
+    """
+    def pool(nel, lev, size):
+        out, seen = [], set()
+        occ_slots = list(range(max(0, nel - nact_occ), nel))
+        virt = list(range(nel + 1, min(norb, nel + nact_virt) + 1))
+        tries = 0
+        while len(out) < size and tries < 50 * size:
+            tries += 1
+            slots = tuple(sorted(rng.choice(occ_slots, size=lev, replace=False)))
+            orbs = tuple(rng.choice(virt, size=lev, replace=False))
+            key = (slots, tuple(sorted(orbs)))
+            if key in seen:
+                continue
+            seen.add(key)
+            occ = list(range(1, nel + 1))
+            for sl, o in zip(slots, orbs):
+                occ[sl] = int(o)
+            out.append(tuple(occ))
+        return out
+    ref = (tuple(range(1, nup + 1)), tuple(range(1, ndn + 1)))
+    pu = {lev: pool(nup, lev, sz) for lev, sz in zip((1, 2, 3, 4), pools)}
+    pd = {lev: pool(ndn, lev, sz) for lev, sz in zip((1, 2, 3, 4), pools)}
+    dets, seen = [ref], {ref}
+    while len(dets) < ndet:
+        L = int(rng.choice([1, 2, 3, 4], p=list(level_p)))
+        lu = int(rng.integers(0, L + 1))
+        ld = L - lu
+        up = ref[0] if lu == 0 else pu[lu][int(rng.integers(len(pu[lu])))]
+        dn = ref[1] if ld == 0 else pd[ld][int(rng.integers(len(pd[ld])))]
+        if (up, dn) in seen:
+            continue
+        seen.add((up, dn))
+        dets.append((up, dn))
+    iworbd = np.array([list(u) + list(d) for u, d in dets], np.int32)
+    k = np.arange(1, ndet + 1, dtype=float)
+    cdet = k ** -1.5 * np.where(rng.random(ndet) < 0.5, -1.0, 1.0)
+    cdet[0] = 1.0
+    return iworbd, cdet
+
+
+def _c2(rng) -> System:
+    """Config 2: 12 centres (9 C-like Z=4 with BFD-form ECP, 3 H-like), 40
+    electrons (20/20; the valence charges add up to 39, so one extra
+    electron), 300 Gaussians (C-like s4p5d1, H-like s4p7), 80 orbitals,
+    order-5 Jastrow, 10^4 determinants (ci_expansion)."""
+    nat = 12
+    types = [0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1]
+    cent = np.zeros((nat, 3))
+    for i in range(nat):
+        cent[i] = (1.35 * i + rng.normal(0, 0.05), 0.8 * (i % 2) + rng.normal(0, 0.05), 0.4 * ((i // 2) % 2) +
+                   rng.normal(0, 0.05))
+    heavy = dict(z=4.0, lpot=2, a1=0.0,
+                 basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 5), (2, 1)]), 4.0, 4))
+    hyd = dict(z=1.0, lpot=1, a1=-1.0,
+               basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 7)]), 1.0, 4))
+    s = _assemble("c2", rng, cent, types, [heavy, hyd], 40, 20, 80, 20, 20)
+    s.iworbd, s.cdet = ci_expansion(rng, 20, 20, 80, 10000)
+    return s
 
 
 HE_EXACT = -2.903724377  # non-relativistic ground state of He, Hartree

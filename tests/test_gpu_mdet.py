@@ -77,3 +77,20 @@ def test_mdet_dmc_parity(oracle_mod):
         assert rel_err(a[0], b[0]) < 1e-9
         assert rel_err(a[1], b[1]) < 1e-9
         assert rel_err(a[2], b[2]) < 1e-9
+
+
+def test_c2_hpsi(oracle_mod):
+    """The 10^4-determinant, 40-electron, 300-Gaussian, 80-orbital molecule."""
+    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.system import make_synthetic
+    s = make_synthetic("c2")
+    rng = rng_states(2)
+    x = initial_configs(s, rng)
+    eng = Engine(s)
+    eng.set_walkers(x, rng)
+    h = eng.hpsi()
+    o = oracle_mod.OracleSystem(s)
+    for w in range(2):
+        r = o.hpsi(x[w])
+        assert abs(h["psid"][w] - r["psid"]) <= 1e-9 * abs(r["psid"])
+        assert abs(h["energy"][w] - r["energy"]) <= TOL * max(1.0, abs(r["energy"]))
