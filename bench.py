@@ -33,6 +33,9 @@ CONFIGS = {
                        "(60/60), 540 Gaussians, 60 orbitals, order-5 Jastrow, 8192 walkers"),
     "c0": ("c0", 1024, "vmc-c0: 3 centres (Z 6/1/1, ECP on the heavy atom), 8 electrons (4/4), 60 Gaussians, "
                        "4 orbitals, order-5 Jastrow, 1024 walkers"),
+    "c2": ("c2", 16384, "dmc-c2: 12 centres (9 C-like Z=4 with BFD-form ECP, 3 H-like), 40 electrons (20/20), "
+                        "300 Gaussians, 80 orbitals, 10^4 determinants (1-4-fold excitations, |c_k|~k^-1.5), "
+                        "order-5 Jastrow, 16384 walkers, tau=0.01, branching on"),
 }
 
 
@@ -189,6 +192,104 @@ def run_reference(args):
     return 0
 
 
+def cpu_port_dmc_rate(system, nwalk_cpu, nthreads, min_seconds=10.0, max_steps=200):
+    """Oracle DMC (dmc_ps + branching + splitj) on host threads: electron-moves/s."""
+    from oracle import oracle
+    oracle.build()
+    o = oracle.OracleSystem(system)
+    mw = 4 * nwalk_cpu + 1
+    rng = oracle.rng_states(mw + 1)
+    xs = []
+    for w in range(nwalk_cpu):
+        x, rng[w] = o.sites(rng[w])
+        xs.append(x)
+    e0 = float(np.median([o.hpsi(x)["energy"] for x in xs]))
+    d = oracle.OracleDmc(o, np.array(xs), rng[:mw], rng[mw], tau=0.01, etrial=e0, mwalk=mw)
+    d.steps(1, nthreads)
+    t0 = time.perf_counter()
+    moves = 0
+    steps = 0
+    while steps < max_steps:
+        nw = d.results()["nwalk"]
+        d.steps(1, nthreads)
+        moves += nw * system.nelec
+        steps += 1
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return moves / dt, steps, dt
+
+
+def run_dmc(args):
+    """DMC workload (config c2): electron-moves/s of dmc_ps steps."""
+    import torch
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from champ_b200.engine import Dmc, Engine, initial_configs, rng_states
+    from champ_b200.system import make_synthetic
+    cfg, W, desc = CONFIGS[args.config]
+    if args.walkers:
+        W = args.walkers
+    system = make_synthetic(cfg)
+    mw = 3 * W + 1   # capacity for the branching of a crude (random-orbital) trial function
+    rng_all = rng_states((mw + 1) * (rank + 1))
+    rng = rng_all[rank * (mw + 1):].copy()
+    x = initial_configs(system, rng[:W].copy())
+    eng = Engine(system, device=local, precision=args.precision)
+    eng.set_walkers(x, rng[:W].copy())
+    eng.vmc_steps(2)
+    xv, _ = eng.walkers()
+    e0 = float(np.median(eng.state()[0]))   # robust against the heavy tails of E_L near nodes
+    dmc = Dmc(eng, xv, rng[:mw], rng[mw], tau=0.01, etrial=e0, mwalk=mw)
+    for _ in range(args.warmup):
+        dmc.steps(1)
+    moves = 0
+    ms = 0.0
+    launches = 0
+    with ClockSampler(local) as clk:
+        barrier(pg, local)
+        for _ in range(args.steps):
+            nw = dmc.population()
+            dmc.steps(1)
+            ms += dmc.last_ms()
+            launches += eng.launches()
+            moves += nw * system.nelec
+        barrier(pg, local)
+    ms_max = max_over_ranks(ms, pg, local)
+    value = moves * world / (ms_max * 1e-3)
+    eng.profile(True)
+    dmc.steps(1)
+    stages = eng.stage_times()
+    eng.profile(False)
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
+    cpu_rate, cpu_steps, cpu_dt = cpu_port_dmc_rate(system, os.cpu_count() or 1, os.cpu_count() or 1)
+    top = max(stages.items(), key=lambda kv: kv[1][0])
+    line = {
+        "metric": "electron-moves/s", "value": value, "unit": "electron-moves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "mixed", "data": "synthetic",
+        "config": {"workload": desc, "walkers": W, "mwalk": mw, "electrons": system.nelec,
+                   "determinants": int(system.iworbd.shape[0]), "precision": args.precision,
+                   "l2": "per-walker state (about 0.7 MB per walker) exceeds the 126 MB L2",
+                   "parallelism": f"replicas x{world} (independent populations)"},
+        "top_stage": {"name": top[0], "ms": top[1][0], "launches": top[1][1]},
+        "stages_ms_per_step": {k: round(v[0], 3) for k, v in stages.items() if v[1]},
+        "cpu_baseline": {"value": cpu_rate, "unit": "electron-moves/s", "cores": os.cpu_count() or 1,
+                         "kind": "port", "sample": f"oracle DMC, {os.cpu_count()} walkers on {os.cpu_count()} threads, "
+                                                   f"{cpu_steps} steps ({cpu_dt:.1f} s)"},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
     rank, world, local, pg = dist_setup(args.gpus)
@@ -329,6 +430,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c2":
+        return run_dmc(args)
     return run_ours(args)
 
 

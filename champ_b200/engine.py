@@ -227,3 +227,8 @@ class Dmc:
 
     def last_ms(self) -> float:
         return self.e.last_ms()
+
+    def population(self) -> int:
+        n = C.c_int()
+        self.e._check(self.e.lib.cw_dmc_walkers(self.e.h, C.byref(n), None, None, None, None), "cw_dmc_walkers")
+        return int(n.value)
