@@ -321,8 +321,14 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
       // partner's e-n values from the walker's table (coalesced over lanes)
       const double *en_rr = st.enm + (size_t)w * 2 * M * N + jj;
       const double *en_h = en_rr + (size_t)M * N;
+      // table values of the next centre are loaded one iteration ahead
+      double nrr = en_rr[0], nh = en_h[0];
       for (int ic = 0; ic < M; ic++) {
-        const double rrj = en_rr[(size_t)ic * N], hj = en_h[(size_t)ic * N];
+        const double rrj = nrr, hj = nh;
+        if (ic + 1 < M) {
+          nrr = en_rr[(size_t)(ic + 1) * N];
+          nh = en_h[(size_t)(ic + 1) * N];
+        }
         const double rri = sh_s[ic];
         if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
         const double rj_v[3] = {xj[0] - cs.cent[3 * ic], xj[1] - cs.cent[3 * ic + 1], xj[2] - cs.cent[3 * ic + 2]};
@@ -469,8 +475,13 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
       const float du_r = du / rij;
       const double *en_rr = st.enm + (size_t)w * 2 * M * N + jj;
       const double *en_h = en_rr + (size_t)M * N;
+      double nrr = en_rr[0], nh = en_h[0];
       for (int ic = 0; ic < M; ic++) {
-        const float rrj = (float)en_rr[(size_t)ic * N], hj = (float)en_h[(size_t)ic * N];
+        const float rrj = (float)nrr, hj = (float)nh;
+        if (ic + 1 < M) {
+          nrr = en_rr[(size_t)(ic + 1) * N];
+          nh = en_h[(size_t)(ic + 1) * N];
+        }
         const float rri = sh_s[ic];
         if (rri == asym && rrj == asym) continue;
         const float rj_v[3] = {(float)(xj[0] - cs.cent[3 * ic]), (float)(xj[1] - cs.cent[3 * ic + 1]),

@@ -117,16 +117,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 // Shared-memory bytes of one launch (stages of A_hi, A_lo, B_hi, B_lo plus
 // alignment slack and barriers).
 __host__ __device__ inline size_t umma_stage_bytes(int np) { return 2u * 128u * 128u + 2u * (size_t)np * 128u; }
+// two CTAs per SM (each up to ~110 KB of stages), at least 2 stages: the
+// tiles of a launch then fit one wave instead of 1.7 at one CTA per SM
 __host__ inline int umma_stages(int np) {
   const size_t sb = umma_stage_bytes(np);
-  int s = (int)((200u * 1024u) / sb);
+  int s = (int)((110u * 1024u) / sb);
   return s > 4 ? 4 : (s < 2 ? 2 : s);
 }
 __host__ inline size_t umma_smem_bytes(int np) {
   return 1024 + (size_t)umma_stages(np) * umma_stage_bytes(np) + 256;
 }
 
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
     k_lcao_tf32x3(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
                   const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo, int M, int K,
                   int np, int nc, int stages, double *__restrict__ C, int ldc, int *err) {
