@@ -445,6 +445,34 @@ __device__ __forceinline__ void een_fold0(const T *__restrict__ cc, T x, T *Bout
   for (int t = 0; t < 2 * ((een_nb(NORD) + 1) / 2); t++) Bout[t] = B[t];
 }
 
+// FP32 twin of een_apply0 (mixed path): Bp 8-byte aligned
+template <int NORD>
+__device__ __forceinline__ float een_apply0f(const float *__restrict__ Bp, float y, float z) {
+  constexpr int NB2 = (een_nb(NORD) + 1) / 2;
+  float Bv[2 * NB2];
+  const float2 *b2 = reinterpret_cast<const float2 *>(Bp);
+#pragma unroll
+  for (int t = 0; t < NB2; t++) {
+    const float2 v = b2[t];
+    Bv[2 * t] = v.x;
+    Bv[2 * t + 1] = v.y;
+  }
+  float yp[NORD + 1];
+  yp[0] = 1;
+#pragma unroll
+  for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
+  float fc = 0, zk = 1;
+#pragma unroll
+  for (int k = 0; k < NORD; k++) {
+    float a = 0;
+#pragma unroll
+    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) a += Bv[een_off(NORD, k) + p - een_pmin(k)] * yp[p];
+    fc += zk * a;
+    zk *= z;
+  }
+  return fc;
+}
+
 template <int NORD>
 __device__ __forceinline__ double een_apply0(const double *__restrict__ Bp, double y, double z) {
   constexpr int NB2 = (een_nb(NORD) + 1) / 2;
@@ -580,26 +608,26 @@ __device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD3)
 
 // all nine value/derivative sums of the e-e-n term (jastrow4.f90 fc, fu,
 // fuu, fi, fii, fj, fjj, fui, fuj) from the folded row coefficients
-template <int NORD>
-__device__ __forceinline__ EenOut<double> een_apply2(const double *__restrict__ BD3, double y, double z) {
-  double yp[NORD + 1];
+template <int NORD, typename T = double>
+__device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD3, T y, T z) {
+  T yp[NORD + 1];
   yp[0] = 1;
 #pragma unroll
   for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
-  EenOut<double> e{0, 0, 0, 0, 0, 0, 0, 0, 0};
-  double zk = 1, dzk = 0, d2zk = 0;
+  EenOut<T> e{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  T zk = 1, dzk = 0, d2zk = 0;
 #pragma unroll
   for (int k = 0; k < NORD; k++) {
-    double a = 0, ax = 0, axx = 0, ay = 0, ayy = 0;
+    T a = 0, ax = 0, axx = 0, ay = 0, ayy = 0;
 #pragma unroll
     for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
       const int t = een_off(NORD, k) + p - een_pmin(k);
-      const double b0 = BD3[3 * t], b1 = BD3[3 * t + 1], b2 = BD3[3 * t + 2];
+      const T b0 = BD3[3 * t], b1 = BD3[3 * t + 1], b2 = BD3[3 * t + 2];
       a += b0 * yp[p];
       ax += b1 * yp[p];
       axx += b2 * yp[p];
-      if (p >= 1) ay += b0 * (double(p) * yp[p >= 1 ? p - 1 : 0]);
-      if (p >= 2) ayy += b0 * (double(p * (p - 1)) * yp[p >= 2 ? p - 2 : 0]);
+      if (p >= 1) ay += b0 * (T(p) * yp[p >= 1 ? p - 1 : 0]);
+      if (p >= 2) ayy += b0 * (T(p * (p - 1)) * yp[p >= 2 ? p - 2 : 0]);
     }
     e.fc += zk * a;
     e.fu += dzk * a;
@@ -610,12 +638,20 @@ __device__ __forceinline__ EenOut<double> een_apply2(const double *__restrict__ 
     e.fj += zk * ay;
     e.fjj += zk * ayy;
     e.fuj += dzk * ay;
-    d2zk = double(k + 1) * dzk;
-    dzk = double(k + 1) * zk;
+    d2zk = T(k + 1) * dzk;
+    dzk = T(k + 1) * zk;
     zk *= z;
   }
   return e;
 }
+
+// e-e-n coefficients of atom type it in the compute precision
+template <typename T>
+__device__ __forceinline__ const T *een_coef(int it);
+template <>
+__device__ __forceinline__ const double *een_coef<double>(int it) { return &cs.c[it * CW_MAX_TERMS]; }
+template <>
+__device__ __forceinline__ const float *een_coef<float>(int it) { return &cs.cf[it * CW_MAX_TERMS]; }
 
 // Padé + polynomial e-e term (jastrow4.f90 ee part) at scaled u:
 // returns fee, d fee/du, d2 fee/du2 (MODE>=2)

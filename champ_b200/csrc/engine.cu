@@ -201,20 +201,32 @@ void launch_jmove(cw_ctx *c, int iel) {
 }
 template <int NORD>
 void launch_jfull(cw_ctx *c) {
-  k_jastrow_full<NORD><<<c->W, 128, c->smem_jfull, c->stream>>>(c->st, c->hb);
+  if (c->mixed)
+    k_jastrow_full<NORD, float><<<c->W, 128, c->smem_jfull, c->stream>>>(c->st, c->hb);
+  else
+    k_jastrow_full<NORD, double><<<c->W, 128, c->smem_jfull, c->stream>>>(c->st, c->hb);
 }
 template <int NORD>
 void launch_ecp(cw_ctx *c) {
-  k_ecp<NORD><<<c->W, 32 * c->h.nquad, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+  if (c->mixed)
+    k_ecp<NORD, float><<<c->W, 32 * c->h.nquad, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+  else
+    k_ecp<NORD, double><<<c->W, 32 * c->h.nquad, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
 }
 template <int NORD>
 int set_attrs(cw_ctx *c) {
   CK(cudaFuncSetAttribute(k_jastrow_move<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_jmove));
   CK(cudaFuncSetAttribute(k_jastrow_move_f32<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)c->smem_jmove_f32));
-  CK(cudaFuncSetAttribute(k_jastrow_full<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_jfull));
+  CK(cudaFuncSetAttribute(k_jastrow_full<NORD, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)c->smem_jfull));
+  CK(cudaFuncSetAttribute(k_jastrow_full<NORD, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)c->smem_jfull));
   if (c->h.nloc > 0)
-    CK(cudaFuncSetAttribute(k_ecp<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
+  {
+    CK(cudaFuncSetAttribute(k_ecp<NORD, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
+    CK(cudaFuncSetAttribute(k_ecp<NORD, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
+  }
   return CW_OK;
 }
 

@@ -67,7 +67,10 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 //     evaluate every centre from the folded coefficients;
 //  3. e-n terms, per-electron gradient sums, block sums.
 // ---------------------------------------------------------------------------
-template <int NORD>
+// T is the arithmetic of the pair and e-e-n terms (double: parity path,
+// float: mixed path); distances, 1/r_ij, the tables and the sums over
+// pairs stay FP64.
+template <int NORD, typename T>
 __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
   constexpr int NB = een_nb(NORD);
   extern __shared__ __align__(16) double smem[];
   double *sx = smem;                      // [3][N]
-  double *sB = smem + 3 * N + (3 * N & 1);  // [2][M][3*NB] folded rows
+  T *sB = reinterpret_cast<T *>(smem + 3 * N + (3 * N & 1));  // [2][M][3*NB] folded rows
   __shared__ double red[4];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
   __syncthreads();
@@ -107,7 +110,7 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
         const int row = t / M, ic = t % M;
         const int i = row == 0 ? ia : ib;
         const double rr = tab[((size_t)ic * N + i) * 8];
-        een_fold2<NORD, double>(&cs.c[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sB + ((size_t)row * M + ic) * 3 * NB);
+        een_fold2<NORD, T>(een_coef<T>(cs.iwctype[ic]), T(1 - kap * rr), sB + ((size_t)row * M + ic) * 3 * NB);
       }
     }
     __syncthreads();
@@ -120,47 +123,49 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
       const double rv[3] = {sx[i] - sx[j], sx[N + i] - sx[N + j], sx[2 * N + i] - sx[2 * N + j]};
       const double rij = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
       pee += 1 / rij;
-      double u, dd1, dd2;
-      scale2<double>(rij, u, dd1, dd2);
-      double fs = 0, d2 = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
-      if (u != cs.asymp_r) {
-        double fee, feeu, feeuu;
-        ee_term<2, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+      const T rijT = (T)rij, kT = (T)kap, asym = (T)cs.asymp_r;
+      const T rvT[3] = {(T)rv[0], (T)rv[1], (T)rv[2]};
+      T u, dd1, dd2;
+      scale2<T>(rijT, u, dd1, dd2);
+      T fs = 0, d2 = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
+      if (u != asym) {
+        T fee, feeu, feeuu;
+        ee_term<2, T>(isb, ipar, (T)sspinn, u, fee, feeu, feeuu);
         feeuu = feeuu * dd1 * dd1 + feeu * dd2;
-        feeu = feeu * dd1 / rij;
+        feeu = feeu * dd1 / rijT;
         fs += fee;
         for (int k = 0; k < 3; k++) {
-          gi[k] += feeu * rv[k];
-          gj[k] -= feeu * rv[k];
+          gi[k] += feeu * rvT[k];
+          gj[k] -= feeu * rvT[k];
         }
         d2 += 2 * (feeuu + 2 * feeu);
       }
       if (NORD > 1) {
-        const double z = 1 - kap * u, du1 = -kap * dd1, du2 = -kap * dd2;
-        const double *Brow = sB + (size_t)row * M * 3 * NB;
+        const T z = 1 - kT * u, du1 = -kT * dd1, du2 = -kT * dd2;
+        const T *Brow = sB + (size_t)row * M * 3 * NB;
         for (int ic = 0; ic < M; ic++) {
           const double *qi = tab + ((size_t)ic * N + i) * 8;
           const double *qj = tab + ((size_t)ic * N + j) * 8;
-          const double rri = qi[0], rrj = qj[0];
-          if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
-          const double dd7 = -kap * qi[1], dd9 = -kap * qi[2], ri = qi[3];
-          const double dd8 = -kap * qj[1], dd10 = -kap * qj[2], rj = qj[3];
-          const EenOut<double> e = een_apply2<NORD>(Brow + (size_t)ic * 3 * NB, 1 - kap * rrj, z);
-          const double sgs = ri + rj, tgs = ri - rj;
-          const double u2pst = rij * rij + sgs * tgs, u2mst = rij * rij - sgs * tgs;
-          const double fuu = e.fuu * du1 * du1 + e.fu * du2;
-          const double fu = e.fu * du1 / rij;
-          const double fui = e.fui * du1 * dd7, fuj = e.fuj * du1 * dd8;
-          const double fii = e.fii * dd7 * dd7 + e.fi * dd9, fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
-          const double fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
+          const T rri = (T)qi[0], rrj = (T)qj[0];
+          if (rri == asym && rrj == asym) continue;
+          const T dd7 = -kT * (T)qi[1], dd9 = -kT * (T)qi[2], ri = (T)qi[3];
+          const T dd8 = -kT * (T)qj[1], dd10 = -kT * (T)qj[2], rj = (T)qj[3];
+          const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 3 * NB, 1 - kT * rrj, z);
+          const T sgs = ri + rj, tgs = ri - rj;
+          const T u2pst = rijT * rijT + sgs * tgs, u2mst = rijT * rijT - sgs * tgs;
+          const T fuu = e.fuu * du1 * du1 + e.fu * du2;
+          const T fu = e.fu * du1 / rijT;
+          const T fui = e.fui * du1 * dd7, fuj = e.fuj * du1 * dd8;
+          const T fii = e.fii * dd7 * dd7 + e.fi * dd9, fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
+          const T fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
           fs += e.fc;
-          gi[0] += fi * qi[4] + fu * rv[0];
-          gi[1] += fi * qi[5] + fu * rv[1];
-          gi[2] += fi * qi[6] + fu * rv[2];
-          gj[0] += fj * qj[4] - fu * rv[0];
-          gj[1] += fj * qj[5] - fu * rv[1];
-          gj[2] += fj * qj[6] - fu * rv[2];
-          d2 += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rij) + fuj * u2mst / (rj * rij) + fii + 2 * fi + fjj + 2 * fj;
+          gi[0] += fi * (T)qi[4] + fu * rvT[0];
+          gi[1] += fi * (T)qi[5] + fu * rvT[1];
+          gi[2] += fi * (T)qi[6] + fu * rvT[2];
+          gj[0] += fj * (T)qj[4] - fu * rvT[0];
+          gj[1] += fj * (T)qj[5] - fu * rvT[1];
+          gj[2] += fj * (T)qj[6] - fu * rvT[2];
+          d2 += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rijT) + fuj * u2mst / (rj * rijT) + fii + 2 * fi + fjj + 2 * fj;
         }
       }
       fso[(size_t)i * N + j] = fs;
@@ -481,20 +486,27 @@ __device__ __forceinline__ double psianl_d(double rri, int it) {
   }
   return v;
 }
-__device__ __forceinline__ double psibnl_d(double u, int isb, int ipar, double sspinn) {
-  if (u == cs.asymp_r) return 0.0;
+template <typename T>
+__device__ __forceinline__ T psibnl_t(T u, int isb, int ipar, T sspinn) {
+  if (u == (T)cs.asymp_r) return 0;
   const int nb = cs.nordb + 1;
-  double fee = cs.b[isb * nb] * u / (1 + cs.b[isb * nb + 1] * u);
-  double v = sspinn * fee - cs.asymp_jasb[ipar];
-  double uu = u;
+  T fee = (T)cs.b[isb * nb] * u / (1 + (T)cs.b[isb * nb + 1] * u);
+  T v = sspinn * fee - (T)cs.asymp_jasb[ipar];
+  T uu = u;
   for (int i = 2; i <= cs.nordb; i++) {
     uu *= u;
-    v += cs.b[isb * nb + i] * uu;
+    v += (T)cs.b[isb * nb + i] * uu;
   }
   return v;
 }
+__device__ __forceinline__ double psibnl_d(double u, int isb, int ipar, double sspinn) {
+  return psibnl_t<double>(u, isb, ipar, sspinn);
+}
 
-template <int NORD>
+// T: arithmetic of the quadrature points' Jastrow ratio terms (double:
+// parity path, float: mixed path); the ratio sums, potentials, basis values
+// and the determinant ratio stay FP64.
+template <int NORD, typename T>
 __global__ void k_ecp(WState st, HBuf hb, GSys g) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
@@ -509,8 +521,8 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
   // [NQ][M][NB] folded e-e-n coefficients of the point; 16-byte aligned for
   // the vector loads of een_apply0 (NB is even)
   const size_t bq_off = (((size_t)(rrq - smem) + (size_t)NQ * M) + 1) & ~(size_t)1;
-  double *bq = smem + bq_off;
-  double *recq = bq + (size_t)NQ * M * NB;  // [NQ][M][kCenRec] basis prepass of the point
+  T *bq = reinterpret_cast<T *>(smem + bq_off);
+  double *recq = smem + bq_off + (size_t)NQ * M * NB;  // [NQ][M][kCenRec] basis prepass of the point
   __shared__ int s_act[CW_MAX_CENT];
   __shared__ int s_nact;
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
@@ -570,8 +582,7 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
         if (jc == ic) r = rin;
         rq[jc] = scale0<double>(r);
         if (NORD > 1)
-          een_fold0<NORD, double>(&cs.c[cs.iwctype[jc] * CW_MAX_TERMS], 1 - cs.scalek * rq[jc],
-                                  bq + ((size_t)q * M + jc) * NB);
+          een_fold0<NORD, T>(een_coef<T>(cs.iwctype[jc]), T(1 - cs.scalek * rq[jc]), bq + ((size_t)q * M + jc) * NB);
       }
       warp_basis_prepass<0>(g, xp, rec, lane);
       __syncwarp();
@@ -592,18 +603,21 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
         pair_spin(pi, pj, isb, ipar, sspinn);
         const double dx0 = sx[jj] - xp[0], dx1 = sx[N + jj] - xp[1], dx2 = sx[2 * N + jj] - xp[2];
         const double rij = sqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
-        const double u = scale0<double>(rij);
-        double f = psibnl_d(u, isb, ipar, sspinn);
+        const T u = scale0<T>((T)rij);
+        T f = psibnl_t<T>(u, isb, ipar, (T)sspinn);
         if (NORD > 1) {
           // psinl (vmc/nonlpsi.f90:4) through the folded coefficients of the point
-          const double z = 1 - cs.scalek * u;
+          const T kT = (T)cs.scalek, z = 1 - kT * u;
           for (int jc = 0; jc < M; jc++) {
             const double rrj = rr_en[jj * M + jc];
             if (rq[jc] == cs.asymp_r && rrj == cs.asymp_r) continue;
-            f += een_apply0<NORD>(bq + ((size_t)q * M + jc) * NB, 1 - cs.scalek * rrj, z);
+            if constexpr (sizeof(T) == 8)
+              f += een_apply0<NORD>((const double *)(bq + ((size_t)q * M + jc) * NB), 1 - cs.scalek * rrj, (double)z);
+            else
+              f += een_apply0f<NORD>((const float *)(bq + ((size_t)q * M + jc) * NB), 1 - kT * (T)rrj, (float)z);
           }
         }
-        fsum += f - fso[(size_t)i * N + jj];
+        fsum += (double)f - fso[(size_t)i * N + jj];
       }
       double fen = 0;
       for (int jc = lane; jc < M; jc += 32) fen += psianl_d(rq[jc], cs.iwctype[jc]);
