@@ -178,6 +178,35 @@ void stage_collect(cw_ctx *c) {
   c->evused = 0;
 }
 
+// The system constants live in one __constant__ block per device.  Every
+// entry point that launches kernels binds its context first: when another
+// context's constants are loaded, that context's queued work is waited for
+// and this context's constants are uploaded.  Contexts of different systems
+// on one device therefore serialise; contexts on different devices do not.
+cw_ctx *g_const_owner[64] = {nullptr};
+
+int bind(cw_ctx *c) {
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  const int dev = c->device & 63;
+  cw_ctx *o = g_const_owner[dev];
+  if (o == c) return CW_OK;
+  if (o && o->stream) {
+    e = cudaStreamSynchronize(o->stream);
+    if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "waiting for another context: %s", cudaGetErrorString(e));
+  }
+  e = cudaMemcpyToSymbol(cs, &c->h, sizeof(CSys));
+  if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "constant upload: %s", cudaGetErrorString(e));
+  g_const_owner[dev] = c;
+  return CW_OK;
+}
+
+#define BIND(c)                 \
+  do {                          \
+    int rc_b = bind(c);         \
+    if (rc_b) return rc_b;      \
+  } while (0)
+
 int launch_check(cw_ctx *c, const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
@@ -826,7 +855,13 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
       h.slm_k[l] = K_[l];
     }
   }
+  {
+    // another context's queued kernels may still read the constant block
+    cw_ctx *o = g_const_owner[device & 63];
+    if (o && o->stream) CK(cudaStreamSynchronize(o->stream));
+  }
   CK(cudaMemcpyToSymbol(cs, &h, sizeof(CSys)));
+  g_const_owner[device & 63] = c;
   // global tables
   auto &L = c->sys_allocs;
   const size_t nt = (size_t)d->nctype * d->mrwf * d->mrwf_pts;
@@ -973,6 +1008,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
 
 void cw_destroy(cw_ctx *c) {
   if (!c) return;
+  if (g_const_owner[c->device & 63] == c) g_const_owner[c->device & 63] = nullptr;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_dmc(c);
   free_list(c->w_allocs);
@@ -1018,7 +1054,7 @@ int cw_stage_times(cw_ctx *c, double *ms, long *launches) {
 
 int cw_set_walkers(cw_ctx *c, int nwalk, const double *x, const uint64_t *rng) {
   if (!c || nwalk <= 0 || !x || !rng) return fail(c, CW_ERR_ARG, "cw_set_walkers: bad arguments");
-  CK(cudaSetDevice(c->device));
+  BIND(c);
   if (nwalk != c->W) {
     int rc = alloc_walkers(c, nwalk);
     if (rc) return rc;
@@ -1055,7 +1091,7 @@ int cw_get_walkers(cw_ctx *c, double *x, uint64_t *rng) {
 
 int cw_vmc_steps(cw_ctx *c, int nstep) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
-  CK(cudaSetDevice(c->device));
+  BIND(c);
   const CSys &h = c->h;
   const int W = c->W;
   c->launches = 0;
@@ -1166,6 +1202,7 @@ int cw_results(cw_ctx *c, double *out) {
 int cw_hpsi(cw_ctx *c, const double *xq, const double *yq, const double *zq, double *energy, double *psid,
             double *psij, double *ekin) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  BIND(c);
   const CSys &h = c->h;
   const int W = c->W, NQ = h.nquad;
   if (NQ > 0) {
@@ -1209,6 +1246,7 @@ int cw_get_sums(cw_ctx *c, double *out) {
 
 int cw_orbitals(cw_ctx *c, double *orb, double *dorb, double *ddorb) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  BIND(c);
   const CSys &h = c->h;
   const int W = c->W, N = h.N, M = h.M, Oa = h.Oa, K = h.K;
   const int ec = c->hb.chunk;
@@ -1243,6 +1281,7 @@ int cw_orbitals(cw_ctx *c, double *orb, double *dorb, double *ddorb) {
 
 int cw_jastrow(cw_ctx *c, double *psij, double *v, double *d2j) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  BIND(c);
   NORD_DISPATCH(launch_jfull, c);
   LCHK("k_jastrow_full");
   const int W = c->W, N = c->h.N;
@@ -1261,6 +1300,7 @@ int cw_jastrow(cw_ctx *c, double *psij, double *v, double *d2j) {
 
 int cw_slater(cw_ctx *c, double *slmi, double *det) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  BIND(c);
   int rc = run_hpsi(c, 0);
   if (rc) return rc;
   rc = check_status(c);
@@ -1457,7 +1497,7 @@ extern "C" int cw_orbitals_noalloc(cw_ctx *c, int npts, const double *xyz, doubl
                 "cw_orbitals_noalloc: %d points x 5 x %d basis functions exceed the fixed scratch of %u doubles "
                 "(at most %u points per call for this basis)",
                 npts, h.K, CW_NOALLOC_SCRATCH_DOUBLES, (unsigned)(CW_NOALLOC_SCRATCH_DOUBLES / (5u * h.K)));
-  CK(cudaSetDevice(c->device));
+  BIND(c);
   double *phi = nullptr;
   int rc = noalloc_scratch(c, &phi);
   if (rc) return rc;
@@ -1549,7 +1589,7 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
     return fail(c, CW_ERR_ARG, "cw_dmc_init: bad arguments");
   if (c->h.nloc == 0)
     return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: all-electron DMC (dmc_ae) is not implemented; nloc > 0 required");
-  CK(cudaSetDevice(c->device));
+  BIND(c);
   int rc = alloc_walkers(c, mwalk);
   if (rc) return rc;
   const CSys &h = c->h;
@@ -1636,7 +1676,7 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
 
 extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
   if (!c || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_steps: no DMC population (cw_dmc_init)");
-  CK(cudaSetDevice(c->device));
+  BIND(c);
   const CSys &h = c->h;
   DmcHost &d = c->dmc;
   DmcBuf &b = d.db;

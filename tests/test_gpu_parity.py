@@ -133,3 +133,26 @@ def test_c1_hpsi(oracle_mod):
         assert abs(h["energy"][w] - r["energy"]) <= TOL * max(1.0, abs(r["energy"]))
         assert abs(h["psid"][w] - r["psid"]) <= 1e-9 * abs(r["psid"])
         assert abs(h["psij"][w] - r["psij"]) <= TOL * max(1.0, abs(r["psij"]))
+
+
+def test_two_systems_interleaved(oracle_mod):
+    """Two contexts of different molecules in one process, calls interleaved:
+    each keeps computing its own system."""
+    s1, e1, o1, x1, r1 = _setup(oracle_mod, "tiny", 8)
+    s2, e2, o2, x2, r2 = _setup(oracle_mod, "c0", 8)
+    w1 = oracle_mod.OracleWalkers(o1, x1, r1)
+    w2 = oracle_mod.OracleWalkers(o2, x2, r2)
+    for _ in range(2):
+        h1 = e1.hpsi()
+        h2 = e2.hpsi()
+        xa, _ = e1.walkers()
+        xb, _ = e2.walkers()
+        for w in range(8):
+            assert abs(h1["energy"][w] - o1.hpsi(xa[w])["energy"]) <= TOL * max(1.0, abs(h1["energy"][w]))
+            assert abs(h2["energy"][w] - o2.hpsi(xb[w])["energy"]) <= TOL * max(1.0, abs(h2["energy"][w]))
+        e1.vmc_steps(1)
+        e2.vmc_steps(1)
+        w1.steps(1)
+        w2.steps(1)
+        assert rel_err(e1.walkers()[0], w1.walkers()[0]) < 1e-9
+        assert rel_err(e2.walkers()[0], w2.walkers()[0]) < 1e-9
