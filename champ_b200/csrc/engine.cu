@@ -1583,6 +1583,8 @@ void add_field(WalkerRec &r, double *p, long len) {
 
 }  // namespace
 
+int dmc_alloc(cw_ctx *c, int mwalk);
+
 extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, const uint64_t *rng,
                            const uint64_t *pop_rng, double tau, double etrial, int nfprod) {
   if (!c || nwalk <= 0 || mwalk < nwalk || !x || !rng || !pop_rng || !(tau > 0) || nfprod < 1)
@@ -1590,24 +1592,12 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   if (c->h.nloc == 0)
     return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: all-electron DMC (dmc_ae) is not implemented; nloc > 0 required");
   BIND(c);
-  int rc = alloc_walkers(c, mwalk);
+  int rc = dmc_alloc(c, mwalk);
   if (rc) return rc;
   const CSys &h = c->h;
-  const int N = h.N, nmax = h.nmax;
+  const int N = h.N;
   DmcHost &d = c->dmc;
   DmcBuf &b = d.db;
-  DALLOC(d.allocs, b.vold, (size_t)mwalk * 3 * N);
-  DALLOC(d.allocs, b.wt, mwalk);
-  DALLOC(d.allocs, b.fratio, mwalk);
-  DALLOC(d.allocs, b.iage, mwalk);
-  DALLOC(d.allocs, b.eprev, mwalk);
-  DALLOC(d.allocs, b.acc, (size_t)mwalk * DA_NA);
-  DALLOC(d.allocs, b.copy_src, mwalk);
-  DALLOC(d.allocs, b.copy_dst, mwalk);
-  CK(cudaMallocHost((void **)&d.h_acc, sizeof(double) * mwalk * DA_NA));
-  CK(cudaMallocHost((void **)&d.h_wt, sizeof(double) * mwalk));
-  CK(cudaMallocHost((void **)&d.h_iage, sizeof(int) * mwalk));
-  CK(cudaMallocHost((void **)&d.h_copy, sizeof(int) * 2 * mwalk));
   // active population
   c->W = nwalk;
   c->st.W = nwalk;
@@ -1643,6 +1633,33 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   for (int w = 0; w < nwalk; w++) d.h_wt[w] = 1.0;
   CK(cudaMemcpyAsync(b.wt, d.h_wt, sizeof(double) * nwalk, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(b.iage, 0, sizeof(int) * mwalk, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  d.on = true;
+  return CW_OK;
+}
+
+// Walker storage for mwalk slots plus the DMC arrays, pinned host buffers
+// and the walker record of splitj copies.
+int dmc_alloc(cw_ctx *c, int mwalk) {
+  int rc = alloc_walkers(c, mwalk);
+  if (rc) return rc;
+  const CSys &h = c->h;
+  const int N = h.N, nmax = h.nmax;
+  DmcHost &d = c->dmc;
+  DmcBuf &b = d.db;
+  d.mwalk = mwalk;
+  DALLOC(d.allocs, b.vold, (size_t)mwalk * 3 * N);
+  DALLOC(d.allocs, b.wt, mwalk);
+  DALLOC(d.allocs, b.fratio, mwalk);
+  DALLOC(d.allocs, b.iage, mwalk);
+  DALLOC(d.allocs, b.eprev, mwalk);
+  DALLOC(d.allocs, b.acc, (size_t)mwalk * DA_NA);
+  DALLOC(d.allocs, b.copy_src, mwalk);
+  DALLOC(d.allocs, b.copy_dst, mwalk);
+  CK(cudaMallocHost((void **)&d.h_acc, sizeof(double) * mwalk * DA_NA));
+  CK(cudaMallocHost((void **)&d.h_wt, sizeof(double) * mwalk));
+  CK(cudaMallocHost((void **)&d.h_iage, sizeof(int) * mwalk));
+  CK(cudaMallocHost((void **)&d.h_copy, sizeof(int) * 2 * mwalk));
   // walker record of splitj copies
   WalkerRec &r = d.rec;
   r.nfield = 0;
@@ -1669,8 +1686,6 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   }
   add_field(r, b.vold, 3L * N);
   add_field(r, b.fratio, 1);
-  CK(cudaStreamSynchronize(c->stream));
-  d.on = true;
   return CW_OK;
 }
 
@@ -1876,4 +1891,228 @@ extern "C" int cw_dmc_walkers(cw_ctx *c, int *nwalk, double *x, double *wt, doub
   if (wt) CK(cudaMemcpy(wt, c->dmc.db.wt, sizeof(double) * W, cudaMemcpyDeviceToHost));
   if (eold) CK(cudaMemcpy(eold, c->st.eold, sizeof(double) * W, cudaMemcpyDeviceToHost));
   return CW_OK;
+}
+
+// ===========================================================================
+// Checkpoint / restart of the walker population and the accumulators: the
+// role of CHAMP's dumper / startr (vmc/dumper.f90:51-106, dmc/dumper.f90:3,
+// dmc/restart.f90:3).  The buffer holds what the Markov chain needs to
+// continue — configurations, random streams, the rotated quadrature, the
+// walkers' block sums and the global accumulators (for DMC: population,
+// weights, ages, fratio, the population stream and the branching scalars);
+// every derived table is rebuilt by hpsi on restore, so a restored run
+// continues exactly as the uninterrupted one.
+// ===========================================================================
+namespace {
+
+const char kCkMagic[8] = {'C', 'W', 'C', 'K', 'P', 'T', '0', '1'};
+
+struct CkWriter {
+  std::vector<uint8_t> b;
+  template <typename T>
+  void put(const T &v) {
+    const uint8_t *p = reinterpret_cast<const uint8_t *>(&v);
+    b.insert(b.end(), p, p + sizeof(T));
+  }
+  template <typename T>
+  void put(const T *v, size_t n) {
+    const uint8_t *p = reinterpret_cast<const uint8_t *>(v);
+    b.insert(b.end(), p, p + n * sizeof(T));
+  }
+};
+struct CkReader {
+  const uint8_t *p;
+  size_t n, off = 0;
+  bool ok = true;
+  template <typename T>
+  T get() {
+    T v{};
+    if (off + sizeof(T) > n) { ok = false; return v; }
+    std::memcpy(&v, p + off, sizeof(T));
+    off += sizeof(T);
+    return v;
+  }
+  template <typename T>
+  void get(T *v, size_t cnt) {
+    if (off + cnt * sizeof(T) > n) { ok = false; return; }
+    std::memcpy(v, p + off, cnt * sizeof(T));
+    off += cnt * sizeof(T);
+  }
+};
+
+template <typename T>
+int d2h(cw_ctx *c, std::vector<T> &v, const T *src, size_t n) {
+  v.resize(n);
+  CK(cudaMemcpyAsync(v.data(), src, sizeof(T) * n, cudaMemcpyDeviceToHost, c->stream));
+  return CW_OK;
+}
+
+int ck_serialize(cw_ctx *c, std::vector<uint8_t> &out) {
+  if (c->W == 0) return fail(c, CW_ERR_STATE, "checkpoint: no walkers");
+  BIND(c);
+  const CSys &h = c->h;
+  const int W = c->W, N = h.N, NQ = std::max(h.nquad, 0);
+  const bool dmc = c->dmc.on;
+  const int slots = dmc ? c->dmc.mwalk : W;
+  CkWriter o;
+  o.put(kCkMagic, 8);
+  const int64_t hdr[12] = {1, dmc ? 1 : 0, N, h.nup, h.K, h.Oa, h.M, h.ndet, NQ, W, slots, c->precision};
+  o.put(hdr, 12);
+  std::vector<double> x, xq, sums;
+  std::vector<uint64_t> rng;
+  int rc = d2h(c, x, c->st.x, (size_t)W * 3 * N);
+  if (!rc) rc = d2h(c, rng, c->st.rng, (size_t)slots * 4);
+  if (!rc && NQ > 0) rc = d2h(c, xq, c->st.xq, (size_t)W * 3 * NQ);
+  if (!rc) rc = d2h(c, sums, c->st.sums, (size_t)W * 8);
+  if (rc) return rc;
+  std::vector<double> wt, fratio;
+  std::vector<int> iage;
+  if (dmc) {
+    rc = d2h(c, wt, c->dmc.db.wt, (size_t)W);
+    if (!rc) rc = d2h(c, fratio, c->dmc.db.fratio, (size_t)W);
+    if (!rc) rc = d2h(c, iage, c->dmc.db.iage, (size_t)W);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  o.put(x.data(), x.size());
+  o.put(rng.data(), rng.size());
+  o.put(xq.data(), xq.size());
+  o.put(sums.data(), sums.size());
+  const double vg[10] = {c->ecum, c->ecm2, c->wcum, c->pecum, c->tpbcum, c->pecm2, c->tpbcm2, c->acc, c->ecum1s, c->ecm21s};
+  o.put(vg, 10);
+  const int64_t vi[2] = {c->iblk, c->passes};
+  o.put(vi, 2);
+  if (dmc) {
+    const DmcHost &d = c->dmc;
+    o.put(wt.data(), wt.size());
+    o.put(fratio.data(), fratio.size());
+    o.put(iage.data(), iage.size());
+    uint64_t pop[4];
+    d.pop.store(pop);
+    o.put(pop, 4);
+    const double ds[21] = {d.tau, d.etrial, d.eest, d.eigv, d.wdsumo, d.fprod, d.wsum1, d.esum1, d.pesum, d.tpbsum,
+                           d.tausum, d.wgsum, d.egsum, d.wgcum, d.egcum, d.wgcm2, d.egcm2, d.taucum, d.pecum,
+                           d.tpbcum, d.acc};
+    o.put(ds, 21);
+    const int64_t di[8] = {d.nconf, d.nfprod, d.ipass, d.nacc, d.nodecr, d.nbrnch, d.iblk, (int64_t)d.ff.size()};
+    o.put(di, 8);
+    o.put(d.trymove);
+    o.put(d.ff.data(), d.ff.size());
+  }
+  out.swap(o.b);
+  return CW_OK;
+}
+
+int ck_restore(cw_ctx *c, const uint8_t *buf, size_t n) {
+  const CSys &h = c->h;
+  CkReader r{buf, n};
+  char mg[8];
+  r.get(mg, 8);
+  if (!r.ok || std::memcmp(mg, kCkMagic, 8) != 0) return fail(c, CW_ERR_ARG, "restore: not a checkpoint buffer");
+  int64_t hdr[12];
+  r.get(hdr, 12);
+  if (!r.ok || hdr[0] != 1) return fail(c, CW_ERR_ARG, "restore: unsupported checkpoint version");
+  const bool dmc = hdr[1] == 1;
+  if (hdr[2] != h.N || hdr[3] != h.nup || hdr[4] != h.K || hdr[5] != h.Oa || hdr[6] != h.M || hdr[7] != h.ndet ||
+      hdr[8] != std::max(h.nquad, 0))
+    return fail(c, CW_ERR_ARG, "restore: checkpoint of a different system");
+  const int W = (int)hdr[9], slots = (int)hdr[10], N = h.N, NQ = std::max(h.nquad, 0);
+  if (W <= 0 || slots < W) return fail(c, CW_ERR_ARG, "restore: bad walker counts");
+  std::vector<double> x((size_t)W * 3 * N), xq((size_t)W * 3 * NQ), sums((size_t)W * 8);
+  std::vector<uint64_t> rng((size_t)slots * 4);
+  r.get(x.data(), x.size());
+  r.get(rng.data(), rng.size());
+  r.get(xq.data(), xq.size());
+  r.get(sums.data(), sums.size());
+  double vg[10];
+  int64_t vi[2];
+  r.get(vg, 10);
+  r.get(vi, 2);
+  std::vector<double> wt, fratio, ds(21), ff;
+  std::vector<int> iage;
+  uint64_t pop[4] = {0, 0, 0, 0};
+  int64_t di[8] = {0};
+  double trymove = 0;
+  if (dmc) {
+    wt.resize(W);
+    fratio.resize(W);
+    iage.resize(W);
+    r.get(wt.data(), W);
+    r.get(fratio.data(), W);
+    r.get(iage.data(), W);
+    r.get(pop, 4);
+    r.get(ds.data(), 21);
+    r.get(di, 8);
+    trymove = r.get<double>();
+    if (di[7] < 1 || di[7] > (1 << 20)) return fail(c, CW_ERR_ARG, "restore: bad nfprod");
+    ff.resize((size_t)di[7]);
+    r.get(ff.data(), ff.size());
+  }
+  if (!r.ok || r.off != n) return fail(c, CW_ERR_ARG, "restore: truncated or oversized checkpoint buffer");
+  BIND(c);
+  int rc = dmc ? dmc_alloc(c, slots) : alloc_walkers(c, W);
+  if (rc) return rc;
+  c->W = W;
+  c->st.W = W;
+  CK(cudaMemcpyAsync(c->st.x, x.data(), sizeof(double) * x.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->st.rng, rng.data(), sizeof(uint64_t) * rng.size(), cudaMemcpyHostToDevice, c->stream));
+  if (NQ > 0) CK(cudaMemcpyAsync(c->st.xq, xq.data(), sizeof(double) * xq.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->st.status, 0, sizeof(int) * slots, c->stream));
+  // derived state: every table of the current configurations
+  rc = run_hpsi(c, 0);
+  if (rc) return rc;
+  const long nt = (long)W * N;
+  k_nearest<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st);
+  LCHK("k_nearest");
+  CK(cudaMemcpyAsync(c->st.sums, sums.data(), sizeof(double) * sums.size(), cudaMemcpyHostToDevice, c->stream));
+  c->ecum = vg[0]; c->ecm2 = vg[1]; c->wcum = vg[2]; c->pecum = vg[3]; c->tpbcum = vg[4];
+  c->pecm2 = vg[5]; c->tpbcm2 = vg[6]; c->acc = vg[7]; c->ecum1s = vg[8]; c->ecm21s = vg[9];
+  c->iblk = vi[0];
+  c->passes = vi[1];
+  if (dmc) {
+    DmcHost &d = c->dmc;
+    DmcBuf &b = d.db;
+    for (int w = 0; w < W; w++) {
+      d.h_wt[w] = wt[w];
+      d.h_iage[w] = iage[w];
+    }
+    CK(cudaMemcpyAsync(b.wt, d.h_wt, sizeof(double) * W, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(b.iage, d.h_iage, sizeof(int) * W, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(b.fratio, fratio.data(), sizeof(double) * W, cudaMemcpyHostToDevice, c->stream));
+    d.pop.load(pop);
+    d.tau = ds[0]; d.etrial = ds[1]; d.eest = ds[2]; d.eigv = ds[3]; d.wdsumo = ds[4]; d.fprod = ds[5];
+    d.wsum1 = ds[6]; d.esum1 = ds[7]; d.pesum = ds[8]; d.tpbsum = ds[9]; d.tausum = ds[10]; d.wgsum = ds[11];
+    d.egsum = ds[12]; d.wgcum = ds[13]; d.egcum = ds[14]; d.wgcm2 = ds[15]; d.egcm2 = ds[16]; d.taucum = ds[17];
+    d.pecum = ds[18]; d.tpbcum = ds[19]; d.acc = ds[20];
+    d.nconf = (int)di[0]; d.nfprod = (int)di[1]; d.ipass = di[2]; d.nacc = di[3]; d.nodecr = di[4];
+    d.nbrnch = di[5]; d.iblk = di[6];
+    d.trymove = trymove;
+    d.ff = ff;
+    d.on = true;
+  }
+  return check_status(c);
+}
+
+}  // namespace
+
+extern "C" long cw_checkpoint_bytes(cw_ctx *c) {
+  if (!c) return -1;
+  std::vector<uint8_t> b;
+  if (ck_serialize(c, b)) return -1;
+  return (long)b.size();
+}
+
+extern "C" int cw_checkpoint(cw_ctx *c, void *buf, long bytes) {
+  if (!c || !buf) return fail(c, CW_ERR_ARG, "cw_checkpoint: bad arguments");
+  std::vector<uint8_t> b;
+  int rc = ck_serialize(c, b);
+  if (rc) return rc;
+  if ((long)b.size() > bytes) return fail(c, CW_ERR_ARG, "cw_checkpoint: buffer of %ld bytes, %zu needed", bytes, b.size());
+  std::memcpy(buf, b.data(), b.size());
+  return CW_OK;
+}
+
+extern "C" int cw_restore(cw_ctx *c, const void *buf, long bytes) {
+  if (!c || !buf || bytes <= 0) return fail(c, CW_ERR_ARG, "cw_restore: bad arguments");
+  return ck_restore(c, static_cast<const uint8_t *>(buf), (size_t)bytes);
 }

@@ -147,6 +147,24 @@ class Engine:
         self._check(self.lib.cw_get_state(self.h, dptr(e), dptr(p), dptr(j)), "cw_get_state")
         return e, p, j
 
+    # -- checkpoint / restart (dumper / startr) ---------------------------
+    def checkpoint(self) -> bytes:
+        n = int(self.lib.cw_checkpoint_bytes(self.h))
+        if n < 0:
+            self._check(1, "cw_checkpoint_bytes")
+        buf = C.create_string_buffer(n)
+        self._check(self.lib.cw_checkpoint(self.h, buf, n), "cw_checkpoint")
+        return buf.raw
+
+    def restore(self, data: bytes):
+        buf = C.create_string_buffer(data, len(data))
+        self._check(self.lib.cw_restore(self.h, buf, len(data)), "cw_restore")
+        n = C.c_int()
+        if self.lib.cw_dmc_walkers(self.h, C.byref(n), None, None, None, None) == 0:
+            self.W = int(n.value)
+        else:
+            self.W = int(np.frombuffer(data[8 + 9 * 8:8 + 10 * 8], np.int64)[0])
+
     # -- per-walker routines ----------------------------------------------
     def hpsi(self, quad=None) -> dict:
         W = self.W
@@ -199,6 +217,14 @@ class Dmc:
                                     float(etrial), int(nfprod))
         engine._check(rc, "cw_dmc_init")
         engine.W = W
+
+    @classmethod
+    def attach(cls, engine: "Engine", mwalk: int):
+        """Wrap the DMC population of an engine restored from a checkpoint."""
+        d = cls.__new__(cls)
+        d.e = engine
+        d.mwalk = int(mwalk)
+        return d
 
     def steps(self, n: int):
         self.e._check(self.e.lib.cw_dmc_steps(self.e.h, n), "cw_dmc_steps")

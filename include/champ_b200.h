@@ -254,6 +254,24 @@ int cw_dmc_results(cw_ctx *ctx, double *out);
  * wt [nwalk], eold [nwalk], rng [nwalk][4]; the arrays must hold mwalk. */
 int cw_dmc_walkers(cw_ctx *ctx, int *nwalk, double *x, double *wt, double *eold, uint64_t *rng);
 
+/* ------------------------------------------------------------------------ */
+/* Checkpoint / restart (dumper / startr)                                     */
+/* ------------------------------------------------------------------------ */
+
+/* Checkpoint of the walker population and the accumulators, the content of
+ * CHAMP's restart files (vmc/dumper.f90:51-106, dmc/dumper.f90:3,
+ * dmc/restart.f90:3): configurations, random streams, the current
+ * quadrature rotation, per-walker block sums and the global accumulators,
+ * and for a DMC population its weights, ages, fratio, the population stream
+ * and the branching scalars.  cw_checkpoint_bytes gives the size (-1 on
+ * error); cw_checkpoint fills a host buffer of at least that size.
+ * cw_restore loads a buffer made for the same system into a context
+ * (replacing its walkers), rebuilds every table with hpsi (startr's hpsi
+ * call) and continues the Markov chain exactly where it stopped. */
+long cw_checkpoint_bytes(cw_ctx *ctx);
+int cw_checkpoint(cw_ctx *ctx, void *buf, long bytes);
+int cw_restore(cw_ctx *ctx, const void *buf, long bytes);
+
 /* Diagnostics: measured FMA throughput of the CUDA cores of `device`
  * (fp64=1: FP64, else FP32), TFLOP/s — the roofline denominator of the
  * CUDA-core bound stages.  No counterpart in CHAMP. */
