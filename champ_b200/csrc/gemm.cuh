@@ -2,10 +2,12 @@
 //
 // A holds basis-function rows (value/gradient/Laplacian of one electron of
 // one walker per row), B the LCAO coefficients (basis x orbital), C the
-// orbitals.  128x64 output tile per CTA, 256 threads, 8x4 register tile,
-// 8-deep K slices staged in shared memory with a register prefetch of the
-// next slice.  FP64 SIMT: the B200 has no FP64 tensor-core path wider than
-// its FMA units.
+// orbitals.  128x64 output tile per CTA, 128 threads, 8x8 register tile (16
+// shared-memory doubles per 64 FMAs: the FP64 FMA rate of an SM needs at
+// most one shared double per 4 FMAs), 8-deep K slices staged in shared
+// memory (rows padded by 2 doubles: conflict-free transposed stores, 16-byte
+// aligned vector loads) with a register prefetch of the next slice.  FP64
+// SIMT: the B200 has no FP64 tensor-core path wider than its FMA units.
 #pragma once
 #include "common.cuh"
 
@@ -15,8 +17,8 @@ template <int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 k_dgemm(int M, int N, int K, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C) {
   constexpr int NT = (BM / TM) * (BN / TN);
-  __shared__ double As[2][BK][BM + 1];
-  __shared__ double Bs[2][BK][BN];
+  __shared__ __align__(16) double As[2][BK][BM + 2];
+  __shared__ __align__(16) double Bs[2][BK][BN];
   const int tid = threadIdx.x;
   const int tx = tid % (BN / TN), ty = tid / (BN / TN);
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
@@ -73,10 +75,27 @@ k_dgemm(int M, int N, int K, const double *__restrict__ A, const double *__restr
 #pragma unroll
     for (int kk = 0; kk < BK; kk++) {
       double a[TM], b[TN];
+      if constexpr (TM % 2 == 0 && TN % 2 == 0) {
+        const double2 *pa = reinterpret_cast<const double2 *>(&As[buf][kk][ty * TM]);
+        const double2 *pb = reinterpret_cast<const double2 *>(&Bs[buf][kk][tx * TN]);
 #pragma unroll
-      for (int i = 0; i < TM; i++) a[i] = As[buf][kk][ty * TM + i];
+        for (int i = 0; i < TM / 2; i++) {
+          const double2 v = pa[i];
+          a[2 * i] = v.x;
+          a[2 * i + 1] = v.y;
+        }
 #pragma unroll
-      for (int j = 0; j < TN; j++) b[j] = Bs[buf][kk][tx * TN + j];
+        for (int j = 0; j < TN / 2; j++) {
+          const double2 v = pb[j];
+          b[2 * j] = v.x;
+          b[2 * j + 1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < TM; i++) a[i] = As[buf][kk][ty * TM + i];
+#pragma unroll
+        for (int j = 0; j < TN; j++) b[j] = Bs[buf][kk][tx * TN + j];
+      }
 #pragma unroll
       for (int i = 0; i < TM; i++)
 #pragma unroll
@@ -106,7 +125,7 @@ inline void dgemm(cudaStream_t s, int M, int N, int K, const double *A, const do
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
     k_dgemm<BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, s>>>(M, N, K, A, B, C);
   } else {
-    constexpr int BM = 128, BN = 64, BK = 8, TM = 8, TN = 4;
+    constexpr int BM = 128, BN = 64, BK = 8, TM = 8, TN = 8;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
     k_dgemm<BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, s>>>(M, N, K, A, B, C);
   }
