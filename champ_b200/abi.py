@@ -120,11 +120,13 @@ def load_engine(path: str | None = None):
     lib.cw_dmc_end_block.argtypes = [V]
     lib.cw_dmc_results.argtypes = [V, _dp]
     lib.cw_dmc_walkers.argtypes = [V, C.POINTER(C.c_int), _dp, _dp, _dp, C.POINTER(C.c_uint64)]
+    lib.cw_dmc_set_tmoves.argtypes = [V, C.c_int]
+    lib.cw_dmc_counts.argtypes = [V, C.POINTER(C.c_long)]
     lib.cw_checkpoint_bytes.argtypes = [V]
     lib.cw_checkpoint_bytes.restype = C.c_long
     lib.cw_checkpoint.argtypes = [V, C.c_void_p, C.c_long]
     lib.cw_restore.argtypes = [V, C.c_void_p, C.c_long]
-    for f in ("cw_checkpoint", "cw_restore", "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
+    for f in ("cw_dmc_set_tmoves", "cw_dmc_counts", "cw_checkpoint", "cw_restore", "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
               "cw_rng_states", "cw_sites", "cw_sync", "cw_set_walkers", "cw_get_walkers", "cw_vmc_steps", "cw_end_block",
               "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow", "cw_slater",
               "cw_get_sums", "cw_get_state"):
@@ -140,7 +142,7 @@ EXPORTED_SYMBOLS = [
     "cw_slater", "cw_get_sums", "cw_get_state", "cw_last_ms", "cw_rng_states", "cw_sites",
     "cw_launches", "cw_profile", "cw_stage_times", "cw_fma_peak", "cw_orbitals_noalloc",
     "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
-    "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore",
+    "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore", "cw_dmc_set_tmoves", "cw_dmc_counts",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
-          "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet"]
+          "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

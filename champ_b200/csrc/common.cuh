@@ -106,7 +106,8 @@ struct MoveScratch {
   int nearestn, igeo;
   double rvminon[3];
   double ratio;       // determinant ratio of the proposed move (k_decide)
-  int acc, pad;       // accepted? (k_decide)
+  int acc;           // accepted? (k_decide)
+  int tel;           // electron of a T-move (moves whose launch gives no electron)
 };
 
 struct MoveBuf {

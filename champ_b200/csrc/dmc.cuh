@@ -29,7 +29,7 @@ struct DmcBuf {
 // per-walker sums of one step (reduced on the host in walker order)
 enum {
   DA_DFUS2AC = 0, DA_DFUS2UN, DA_DFUS2O, DA_IACCEPT, DA_ACC, DA_TRY, DA_NACC, DA_NODECR,
-  DA_WSUM1, DA_ESUM1, DA_PESUM, DA_TPBSUM, DA_TAUSUM, DA_NA = 16
+  DA_WSUM1, DA_ESUM1, DA_PESUM, DA_TPBSUM, DA_TAUSUM, DA_TMOVE, DA_NA = 16
 };
 
 struct DmcScalars {
@@ -207,6 +207,128 @@ __global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode, con
   acc[DA_ESUM1] = wt * enew;
   acc[DA_PESUM] = wtg * (enew - ekino);
   acc[DA_TPBSUM] = wtg * ekino;
+}
+
+// T-move choice of every walker (icasula = -1, nonloc_grid,
+// dmc/nonloc_grid.f90:3, over all electrons): warp per walker.  t_norm =
+// 1 + tau sum(-t) over the negative matrix elements; when some exist one
+// draw p from the walker's stream and the first (electron, point, centre),
+// in CHAMP's loop order, whose cumulative -tau t / t_norm exceeds p moves:
+// each lane sums a contiguous chunk, a warp scan finds the chunk, its lane
+// walks it.  The proposed point is r_en(e, ic) times the rotated quadrature
+// direction about the centre.
+__global__ void k_tmove_select(WState st, MoveBuf mb, const double *tv, DmcScalars sc) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= st.W) return;
+  const int N = cs.N, M = cs.M, NQ = cs.nquad;
+  const int L = N * NQ * M;
+  const double *t = tv + (size_t)w * L;
+  const int per = (L + 31) / 32, a = lane * per, b = min(L, a + per);
+  double sneg = 0;
+  for (int k = a; k < b; k++) {
+    const double v = t[k];
+    if (v < 0.0) sneg -= v;
+  }
+  const double tot = warp_sum(sneg);
+  const double tau = sc.tau;
+  const double t_norm = 1.0 + tot * tau;
+  MoveScratch &m = mb.ms[w];
+  if (t_norm == 1.0) {
+    if (lane == 0) m.igeo = 1;
+    return;
+  }
+  const double t_normi = 1.0 / t_norm;
+  double p = 0;
+  if (lane == 0) {
+    DRng rng;
+    rng.load(st.rng + 4 * (size_t)w);
+    p = rng.uniform();
+    rng.store(st.rng + 4 * (size_t)w);
+  }
+  p = __shfl_sync(0xffffffffu, p, 0);
+  double cl = 0;
+  for (int k = a; k < b; k++) {
+    const double v = t[k];
+    cl = cl - tau * (v < 0.0 ? v : 0.0) * t_normi;
+  }
+  double incl = cl;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += u;
+  }
+  const unsigned hit = __ballot_sync(0xffffffffu, incl > p && b > a);
+  if (hit == 0) {
+    if (lane == 0) m.igeo = 1;
+    return;
+  }
+  const int l0 = __ffs(hit) - 1;
+  if (lane != l0) return;
+  double t_cum = incl - cl;
+  int kk = -1, last_neg = -1;
+  for (int k = a; k < b; k++) {
+    const double v = t[k];
+    if (v < 0.0) last_neg = k;
+    t_cum = t_cum - tau * (v < 0.0 ? v : 0.0) * t_normi;
+    if (t_cum > p) {
+      kk = k;
+      break;
+    }
+  }
+  // rounding between the chunk sum and the walk: the chunk's last transition
+  if (kk < 0) kk = last_neg;
+  if (kk < 0) {
+    m.igeo = 1;
+    return;
+  }
+  const int e = kk / (NQ * M), iq = (kk / M) % NQ, ic = kk % M;
+  double d[3], r2 = 0;
+  for (int k = 0; k < 3; k++) {
+    d[k] = st.x[((size_t)w * 3 + k) * N + e] - cs.cent[3 * ic + k];
+    r2 += d[k] * d[k];
+  }
+  const double r = sqrt(r2);
+  const double *xq = st.xq + (size_t)w * 3 * NQ;
+  for (int k = 0; k < 3; k++) m.xnew[k] = r * xq[k * NQ + iq] + cs.cent[3 * ic + k];
+  m.igeo = 0;
+  m.tel = e;
+}
+
+// T-move of the chosen electron, always accepted (icasula = -1): ratio at
+// the point, psi_D, psi_J, commit of the scalars; k_commit applies the
+// matrix and table updates.  Thread per walker.
+__global__ void k_tmove_accept(WState st, MoveBuf mb, GSys g, DmcBuf db) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  MoveScratch &m = mb.ms[w];
+  if (m.igeo) {
+    m.acc = 0;
+    return;
+  }
+  const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa, iel = m.tel;
+  const int iab = iel < cs.nup ? 0 : 1, nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
+  const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * (iel - ish);
+  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const int *slot = g.slot_orb + iab * nmax;
+  double ratio = 0;
+  for (int j = 0; j < nel; j++) ratio += sl[j] * orbn[slot[j]];
+  const double detn = st.detiab[2 * w + iab] * ratio;
+  const double psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
+  if (detn == 0.0) {
+    st.status[w] |= 1;
+    m.acc = 0;
+    return;
+  }
+  m.acc = 1;
+  m.ratio = ratio;
+  for (int k = 0; k < 3; k++) st.x[((size_t)w * 3 + k) * N + iel] = m.xnew[k];
+  st.psido[w] = psidn;
+  st.psijo[w] = mb.fsumn[w];
+  st.fsumo[w] = mb.fsumn[w];
+  st.detiab[2 * w + iab] = detn;
+  db.iage[w] = 0;
+  db.acc[(size_t)w * DA_NA + DA_TMOVE] = 1;
 }
 
 struct QuadRot {

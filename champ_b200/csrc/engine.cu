@@ -38,6 +38,8 @@ struct DmcHost {
   double wgsum = 0, egsum = 0, wgcum = 0, egcum = 0, wgcm2 = 0, egcm2 = 0, taucum = 0;
   double pecum = 0, tpbcum = 0, acc = 0, trymove = 0;
   long nacc = 0, nodecr = 0, nbrnch = 0, iblk = 0;
+  int icasula = 0;                  // 0: no T-moves, -1: one per walker and step
+  long nmove_casula = 0;
   DmcBuf db{};
   std::vector<void *> allocs;
   double *h_acc = nullptr, *h_wt = nullptr;   // pinned, [mwalk][DA_NA] and [mwalk]
@@ -654,6 +656,7 @@ int alloc_walkers(cw_ctx *c, int W) {
   }
   if (h.nloc > 0) DALLOC(L, b.ctilde, (size_t)W * N * K);
   m.md_velo = m.md_veln = m.md_psidn = nullptr;
+  b.tvpsp = nullptr;
   b.md_P = nullptr;
   b.md_den = b.md_S = nullptr;
   c->md_vall = nullptr;
@@ -1759,6 +1762,8 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       LCHK("k_commit");
       if (int rc = md_after_commit(c, i)) return rc;
     }
+    if (d.icasula == -1)
+      CK(cudaMemsetAsync(c->hb.tvpsp, 0, sizeof(double) * (size_t)W * h.N * h.nquad * h.M, c->stream));
     int rc = run_hpsi(c, 0);
     if (rc) return rc;
     if (c->md_on) {
@@ -1771,6 +1776,36 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
     k_dmc_weights<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 1, c->md_vall);
     stage_end(c);
     LCHK("k_dmc_weights");
+    if (d.icasula == -1) {
+      // T-moves (dmc_ps :701-735): choice, then the forced move of each walker's electron
+      stage_begin(c, CW_ST_TMOVE);
+      k_tmove_select<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->mb, c->hb.tvpsp, sc);
+      stage_end(c);
+      LCHK("k_tmove_select");
+      stage_begin(c, CW_ST_JASTROW_MOVE);
+      NORD_DISPATCH(launch_jmove, c, -1);
+      stage_end(c);
+      LCHK("k_jastrow_move(tmove)");
+      const int bw = c->basis_warps;
+      stage_begin(c, CW_ST_BASIS_MOVE);
+      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+      stage_end(c);
+      LCHK("k_basis_move(tmove)");
+      stage_begin(c, CW_ST_LCAO_MOVE);
+      {
+        int rc2 = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn);
+        stage_end(c);
+        if (rc2) return rc2;
+      }
+      stage_begin(c, CW_ST_TMOVE);
+      k_tmove_accept<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, b);
+      stage_end(c);
+      LCHK("k_tmove_accept");
+      stage_begin(c, CW_ST_COMMIT);
+      k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, -1);
+      stage_end(c);
+      LCHK("k_commit(tmove)");
+    }
     CK(cudaMemcpyAsync(d.h_acc, b.acc, sizeof(double) * W * DA_NA, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(d.h_wt, b.wt, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(d.h_iage, b.iage, sizeof(int) * W, cudaMemcpyDeviceToHost, c->stream));
@@ -1788,6 +1823,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       d.trymove += a[DA_TRY];
       d.nacc += (long)a[DA_NACC];
       d.nodecr += (long)a[DA_NODECR];
+      d.nmove_casula += (long)a[DA_TMOVE];
     }
     const double wgsum1 = d.wsum1 * d.fprod, egsum1 = d.esum1 * d.fprod;
     // splitj: weights on the host, walker copies on the device
@@ -1994,8 +2030,9 @@ int ck_serialize(cw_ctx *c, std::vector<uint8_t> &out) {
                            d.tausum, d.wgsum, d.egsum, d.wgcum, d.egcum, d.wgcm2, d.egcm2, d.taucum, d.pecum,
                            d.tpbcum, d.acc};
     o.put(ds, 21);
-    const int64_t di[8] = {d.nconf, d.nfprod, d.ipass, d.nacc, d.nodecr, d.nbrnch, d.iblk, (int64_t)d.ff.size()};
-    o.put(di, 8);
+    const int64_t di[10] = {d.nconf, d.nfprod, d.ipass, d.nacc, d.nodecr, d.nbrnch, d.iblk, (int64_t)d.ff.size(),
+                            d.icasula, d.nmove_casula};
+    o.put(di, 10);
     o.put(d.trymove);
     o.put(d.ff.data(), d.ff.size());
   }
@@ -2031,7 +2068,7 @@ int ck_restore(cw_ctx *c, const uint8_t *buf, size_t n) {
   std::vector<double> wt, fratio, ds(21), ff;
   std::vector<int> iage;
   uint64_t pop[4] = {0, 0, 0, 0};
-  int64_t di[8] = {0};
+  int64_t di[10] = {0};
   double trymove = 0;
   if (dmc) {
     wt.resize(W);
@@ -2042,7 +2079,7 @@ int ck_restore(cw_ctx *c, const uint8_t *buf, size_t n) {
     r.get(iage.data(), W);
     r.get(pop, 4);
     r.get(ds.data(), 21);
-    r.get(di, 8);
+    r.get(di, 10);
     trymove = r.get<double>();
     if (di[7] < 1 || di[7] > (1 << 20)) return fail(c, CW_ERR_ARG, "restore: bad nfprod");
     ff.resize((size_t)di[7]);
@@ -2089,6 +2126,11 @@ int ck_restore(cw_ctx *c, const uint8_t *buf, size_t n) {
     d.trymove = trymove;
     d.ff = ff;
     d.on = true;
+    if (di[8] != 0) {
+      rc = cw_dmc_set_tmoves(c, (int)di[8]);
+      if (rc) return rc;
+    }
+    d.nmove_casula = di[9];
   }
   return check_status(c);
 }
@@ -2115,4 +2157,30 @@ extern "C" int cw_checkpoint(cw_ctx *c, void *buf, long bytes) {
 extern "C" int cw_restore(cw_ctx *c, const void *buf, long bytes) {
   if (!c || !buf || bytes <= 0) return fail(c, CW_ERR_ARG, "cw_restore: bad arguments");
   return ck_restore(c, static_cast<const uint8_t *>(buf), (size_t)bytes);
+}
+
+extern "C" int cw_dmc_set_tmoves(cw_ctx *c, int icasula) {
+  if (!c || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_set_tmoves: no DMC population");
+  if (icasula != 0 && icasula != -1) return fail(c, CW_ERR_UNSUPPORTED, "T-moves: icasula %d (0 or -1 supported)", icasula);
+  if (icasula != 0 && c->h.nloc == 0) return fail(c, CW_ERR_ARG, "T-moves need a pseudopotential (nloc > 0)");
+  if (icasula != 0 && c->md_on)
+    return fail(c, CW_ERR_UNSUPPORTED, "T-moves of multideterminant wave functions are not implemented");
+  BIND(c);
+  DmcHost &d = c->dmc;
+  if (icasula != 0 && !c->hb.tvpsp) {
+    const CSys &h = c->h;
+    DALLOC(d.allocs, c->hb.tvpsp, (size_t)d.mwalk * h.N * h.nquad * h.M);
+  }
+  d.icasula = icasula;
+  return CW_OK;
+}
+
+extern "C" int cw_dmc_counts(cw_ctx *c, long *out) {
+  if (!c || !out || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_counts: no DMC population");
+  const DmcHost &d = c->dmc;
+  out[0] = d.nacc;
+  out[1] = d.nodecr;
+  out[2] = d.nbrnch;
+  out[3] = d.nmove_casula;
+  return CW_OK;
 }

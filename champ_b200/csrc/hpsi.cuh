@@ -29,6 +29,7 @@ struct HBuf {
   int chunk;        // electrons per chunk
   float *phi_hi, *phi_lo;  // mixed precision: [rows][kp] split chunk basis (null in FP64)
   int kp;
+  double *tvpsp;           // [W][N][nquad][M] T-move matrix elements (null without T-moves)
   // multideterminant (null for one determinant)
   double *md_P;            // [W][N][K] pseudopotential quadrature basis sums
   const double *md_den;    // [W][2] energy / kinetic corrections
@@ -626,6 +627,8 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
       for (int l = 1; l <= cs.lpot[ict] - 1; l++) term += yl0_d(l, costh) * vps[4 * ic + (l - 1)];
       const double trj = term * cs.wq[q] * exp(fsum);
       vp_acc[iab] += trj * dr;
+      if (hb.tvpsp && lane == 0)  // transition matrix element of a T-move (nonloc.f90:296)
+        hb.tvpsp[(((size_t)w * N + i) * NQ + q) * M + ic] = dr * trj;
       if (hb.md_P) {
         // pseudopotential B matrix of every orbital (nonloc.f90:271): the
         // basis values of the point weighted by trj, contracted with coef later

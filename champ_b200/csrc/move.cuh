@@ -241,7 +241,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   m.areao = areao;
   m.rratio = m.rminno / rminon;
   m.nearestn = nearn;
-  m.pad = 0;
+  m.tel = iel;
   mb.ms[w] = m;
   rng.store(st.rng + 4 * (size_t)w);
 }
@@ -271,6 +271,7 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
     xi[0] = m.xnew[0]; xi[1] = m.xnew[1]; xi[2] = m.xnew[2];
   }
   if (!active || igeo) return;  // whole warp leaves together (same walker)
+  if (iel < 0) iel = mb.ms[w].tel;
   const double kap = cs.scalek;
   for (int ic = lane; ic < M; ic += 32) {
     double r2 = 0;
@@ -423,6 +424,7 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
     xi[0] = m.xnew[0]; xi[1] = m.xnew[1]; xi[2] = m.xnew[2];
   }
   if (!active || igeo) return;
+  if (iel < 0) iel = mb.ms[w].tel;
   const float kap = (float)cs.scalek;
   const float asym = (float)cs.asymp_r;
   for (int ic = lane; ic < M; ic += 32) {
@@ -716,6 +718,7 @@ __global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   if (!mb.ms[w].acc) return;
+  if (iel < 0) iel = mb.ms[w].tel;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;

@@ -254,6 +254,14 @@ class Dmc:
     def last_ms(self) -> float:
         return self.e.last_ms()
 
+    def set_tmoves(self, icasula: int):
+        self.e._check(self.e.lib.cw_dmc_set_tmoves(self.e.h, int(icasula)), "cw_dmc_set_tmoves")
+
+    def counts(self) -> dict:
+        o = (C.c_long * 4)()
+        self.e._check(self.e.lib.cw_dmc_counts(self.e.h, o), "cw_dmc_counts")
+        return dict(accepted=o[0], node_crossings=o[1], branchings=o[2], tmoves=o[3])
+
     def population(self) -> int:
         n = C.c_int()
         self.e._check(self.e.lib.cw_dmc_walkers(self.e.h, C.byref(n), None, None, None, None), "cw_dmc_walkers")

@@ -197,7 +197,7 @@ enum {
   CW_ST_ROTQUA = 0, CW_ST_PROPOSE, CW_ST_JASTROW_MOVE, CW_ST_BASIS_MOVE, CW_ST_LCAO_MOVE,
   CW_ST_ACCEPT, CW_ST_JASTROW_FULL, CW_ST_BASIS_ALL, CW_ST_LCAO_ALL, CW_ST_SCATTER,
   CW_ST_SLATER_INV, CW_ST_CTILDE, CW_ST_ECP, CW_ST_ENERGY, CW_ST_COMMIT, CW_ST_DMC_WEIGHTS,
-  CW_ST_SPLITJ, CW_ST_MDET, CW_NSTAGE
+  CW_ST_SPLITJ, CW_ST_MDET, CW_ST_TMOVE, CW_NSTAGE
 };
 int cw_profile(cw_ctx *ctx, int enable);
 int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
@@ -249,6 +249,17 @@ int cw_dmc_end_block(cw_ctx *ctx);
  * out[3]=eest, out[4]=acceptance, out[5]=taueff, out[6]=PE, out[7]=KE,
  * out[8]=blocks, out[9]=fprod, out[10]=eigv, out[11]=wdsumo. */
 int cw_dmc_results(cw_ctx *ctx, double *out);
+
+/* T-moves (Casula), icasula of the dmc input (dmc_ps :701-795,
+ * dmc/nonloc_grid.f90:3): 0 off (default), -1 after each step's reweighting
+ * one T-move per walker, chosen over every electron and quadrature point
+ * from the negative nonlocal matrix elements of the step's hpsi and always
+ * accepted.  Single-determinant wave functions with a pseudopotential. */
+int cw_dmc_set_tmoves(cw_ctx *ctx, int icasula);
+
+/* DMC move counts: out[0]=accepted drift-diffusion moves, out[1]=node
+ * crossings, out[2]=branching events (nbrnch), out[3]=T-moves. */
+int cw_dmc_counts(cw_ctx *ctx, long *out);
 
 /* Current population: *nwalk, and (any may be NULL) x [nwalk][nelec][3],
  * wt [nwalk], eold [nwalk], rng [nwalk][4]; the arrays must hold mwalk. */

@@ -531,6 +531,7 @@ struct Walker {
   vector<double> xq, yq, zq;
   // ecp
   vector<double> vps;  // vps(i,ic,l) [i + N*(ic + M*l)]
+  vector<double> tvpsp;  // t_vpsp(ic,iq,i) [(i*nquad + iq)*M + ic] of the last hpsi (T-moves)
   // estimators (estsum, forcewt, est*)
   double esum, wsum, pesum, tpbsum, acc, esum1;
   double ecum, ecm2, wcum, pecum, tpbcum, pecm2, tpbcm2, ecum1, ecm21, ecum1s, ecm21s;
@@ -582,6 +583,7 @@ struct Walker {
     bkin.assign((size_t)N * O, 0);
     xq = s->xq0; yq = s->yq0; zq = s->zq0;
     vps.assign((size_t)N * M * CW_MPS_L, 0);
+    tvpsp.assign((size_t)N * std::max(s->nquad, 1) * M, 0.0);
     zero_estimators();
   }
   void zero_estimators() {
@@ -1395,6 +1397,7 @@ struct Walker {
   }
   void nonloc(const double *x, double *vpsp_det) {
     vpsp_det[0] = vpsp_det[1] = 0;
+    std::fill(tvpsp.begin(), tvpsp.end(), 0.0);
     // enumerate quadrature points (iel outer, ic middle, iq inner)
     struct QP { int iel, ic, iq; double costh, x[3]; };
     vector<QP> qp;
@@ -1494,6 +1497,8 @@ struct Walker {
       for (int l = 1; l <= s->lpot[ict] - 1; l++) term += yl0(l, qp[q].costh) * vps[iel + N * (ic + M * (l - 1))];
       double trj = term * s->wq[qp[q].iq] * std::exp(ratio_jn[q]);
       vpsp_det[iab] += trj * det_ratio[q];
+      // transition matrix element of a T-move to this point (nonloc.f90:296-298)
+      tvpsp[((size_t)iel * s->nquad + qp[q].iq) * M + ic] = det_ratio[q] * trj;
       // pseudopotential contribution to the B matrix (nonloc.f90:271-273)
       if (s->ndet > 1)
         for (int iorb = 0; iorb < O; iorb++) bmat[iorb + (size_t)O * iel] += trj * orbq_all[iorb + (size_t)O * q];
@@ -2018,6 +2023,7 @@ struct Walkers {
 struct DmcParams {
   double tau, etrial;
   int nconf, mwalk, nfprod;
+  int icasula = 0;  // 0: no T-moves, -1: one T-move per walker and step (dmc_ps :701-795)
 };
 
 struct DmcPop {
@@ -2036,9 +2042,12 @@ struct DmcPop {
   double wgsum = 0, egsum = 0, wgcum = 0, egcum = 0, wgcm2 = 0, egcm2 = 0, taucum = 0;
   double pecum = 0, tpbcum = 0;
   double acc = 0, trymove = 0;
-  long nacc = 0, nodecr = 0, nbrnch = 0, iblk = 0;
+  long nacc = 0, nodecr = 0, nbrnch = 0, iblk = 0, nmove_casula = 0;
+  vector<int> tmoved;  // [mwalk] walker made a T-move in this step
   bool failed = false;
 };
+
+bool tmove_walker(DmcPop &P, int iw);
 
 double gauss_draw(Rng &r) {
   // gauss (vmc/gauss.f90:3): one normal from two uniforms, cos draw first
@@ -2161,6 +2170,61 @@ bool dmc_walker(DmcPop &P, int iw, double ffi, double &wsum1, double &esum1, dou
   tpbsum += wtg * ekino;
   (void)pp;
   (void)drifdif;
+  if (P.prm.icasula == -1 && s->nloc > 0) return tmove_walker(P, iw);
+  return true;
+}
+
+// T-move of one walker (icasula = -1): nonloc_grid (dmc/nonloc_grid.f90:3)
+// over every electron with the matrix elements of the last hpsi, then the
+// move of the chosen electron to its quadrature point, always accepted
+// (dmc_ps :701-735).  Returns false if the new point is singular.
+bool tmove_walker(DmcPop &P, int iw) {
+  Walker &w = P.w[iw];
+  const Sys *s = P.s;
+  const int N = w.N, M = w.M, NQ = s->nquad;
+  const double tauprim = P.prm.tau;
+  double t_norm = 0.0;
+  for (int i = 0; i < N; i++)
+    for (int iq = 0; iq < NQ; iq++)
+      for (int ic = 0; ic < M; ic++) {
+        double &t = w.tvpsp[((size_t)i * NQ + iq) * M + ic];
+        if (t > 0.0) t = 0.0;
+        t_norm = t_norm - t;
+      }
+  t_norm = 1.0 + t_norm * tauprim;
+  if (t_norm == 1.0) return true;
+  const double t_normi = 1.0 / t_norm;
+  double t_cum = 0.0;
+  const double p = w.rng.uniform();
+  int iel = -1, icg = -1, iqg = -1;
+  for (int i = 0; i < N && iel < 0; i++)
+    for (int iq = 0; iq < NQ && iel < 0; iq++)
+      for (int ic = 0; ic < M; ic++) {
+        t_cum = t_cum - tauprim * w.tvpsp[((size_t)i * NQ + iq) * M + ic] * t_normi;
+        if (t_cum > p) {
+          iel = i;
+          icg = ic;
+          iqg = iq;
+          break;
+        }
+      }
+  if (iel < 0) return true;
+  // distances of the walker at its current configuration (r_en of electron iel)
+  w.distances(iel, w.xold.data());
+  const double r = w.r_en[iel + N * icg];
+  double xn[3] = {r * w.xq[iqg] + s->cent[0 + 3 * icg], r * w.yq[iqg] + s->cent[1 + 3 * icg],
+                  r * w.zq[iqg] + s->cent[2 + 3 * icg]};
+  for (int k = 0; k < 3; k++) w.xnew[k + 3 * iel] = xn[k];
+  double psijn;
+  const double psidn = w.psie(iel, w.xnew.data(), psijn, 0);
+  if (w.singular) return false;
+  for (int k = 0; k < 3; k++) w.xold[k + 3 * iel] = xn[k];
+  w.psido = psidn;
+  w.psijo = psijn;
+  w.jassav(iel, 0);
+  w.detsav(iel);
+  P.iage[iw] = 0;
+  P.tmoved[iw] = 1;
   return true;
 }
 
@@ -2251,6 +2315,7 @@ bool dmc_step(DmcPop &P, int nthreads) {
   P.fprod = P.fprod * ffn / P.ff[ipmod];
   P.ff[ipmod] = ffn;
   const int W = P.nwalk;
+  std::fill(P.tmoved.begin(), P.tmoved.end(), 0);
   vector<double> a_w(W), a_e(W), a_pe(W), a_tpb(W), a_tau(W), a_acc(W), a_try(W);
   vector<long> a_nacc(W), a_nod(W);
   vector<int> bad(W, 0);
@@ -2269,6 +2334,7 @@ bool dmc_step(DmcPop &P, int nthreads) {
     for (int t = 0; t < nthreads; t++) th.emplace_back(work, t);
     for (auto &t : th) t.join();
   }
+  for (int iw = 0; iw < W; iw++) P.nmove_casula += P.tmoved[iw];
   for (int iw = 0; iw < W; iw++) {
     if (bad[iw]) return false;
     P.wsum1 += a_w[iw]; P.esum1 += a_e[iw]; P.pesum += a_pe[iw]; P.tpbsum += a_tpb[iw];
@@ -2791,6 +2857,7 @@ void *or_dmc_create(void *sysp, int nwalk, const double *x, const uint64_t *rng,
     std::memcpy(P->w[k].rng.s, rng + 4 * k, 32);
   }
   P->wt.assign(P->prm.mwalk, 0.0);
+  P->tmoved.assign(P->prm.mwalk, 0);
   P->fratio.assign(P->prm.mwalk, 0.0);
   P->iage.assign(P->prm.mwalk, 0);
   P->ff.assign(nfprod, 1.0);
@@ -2815,6 +2882,16 @@ void *or_dmc_create(void *sysp, int nwalk, const double *x, const uint64_t *rng,
   return P;
 }
 void or_dmc_destroy(void *p) { delete (DmcPop *)p; }
+// T-moves (icasula, dmc_ps :701): 0 off, -1 one T-move per walker and step;
+// returns 1 for an unsupported value or a multideterminant wave function
+int or_dmc_set_tmoves(void *p, int icasula) {
+  DmcPop *P = (DmcPop *)p;
+  if (icasula != 0 && icasula != -1) return 1;
+  if (icasula != 0 && (P->s->ndet > 1 || P->s->nloc == 0)) return 1;
+  P->prm.icasula = icasula;
+  return 0;
+}
+long or_dmc_tmoves(void *p) { return ((DmcPop *)p)->nmove_casula; }
 int or_dmc_steps(void *p, int nstep, int nthreads) {
   DmcPop *P = (DmcPop *)p;
   if (P->failed) return 1;

@@ -66,6 +66,8 @@ int or_dmc_steps(void *dmc, int nstep, int nthreads);
 void or_dmc_end_block(void *dmc);
 void or_dmc_results(void *dmc, double *out);
 int or_dmc_walkers(void *dmc, double *x, double *wt, double *eold, uint64_t *rng);
+int or_dmc_set_tmoves(void *dmc, int icasula);
+long or_dmc_tmoves(void *dmc);
 
 #ifdef __cplusplus
 }

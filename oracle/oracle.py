@@ -225,6 +225,18 @@ class OracleDmc:
         if lib().or_dmc_steps(self.h, n, nthreads):
             raise RuntimeError("oracle DMC failed")
 
+    def set_tmoves(self, icasula: int):
+        L = lib()
+        L.or_dmc_set_tmoves.argtypes = [C.c_void_p, C.c_int]
+        if L.or_dmc_set_tmoves(self.h, icasula):
+            raise ValueError("unsupported T-move setting")
+
+    def tmoves(self) -> int:
+        L = lib()
+        L.or_dmc_tmoves.argtypes = [C.c_void_p]
+        L.or_dmc_tmoves.restype = C.c_long
+        return int(L.or_dmc_tmoves(self.h))
+
     def end_block(self):
         lib().or_dmc_end_block(self.h)
 

@@ -86,3 +86,22 @@ def test_dmc_mwalk_exceeded(oracle_mod):
     dg = Dmc(eng, x, rng, pop, tau=0.05, etrial=e0 + 50.0, mwalk=33)
     with pytest.raises(EngineError, match="MWALK"):
         dg.steps(20)
+
+
+@pytest.mark.parametrize("config,W", [("tiny", 32), ("c0", 24)])
+def test_dmc_tmove_parity(oracle_mod, config, W):
+    """T-moves (icasula = -1): same choices, same moved electrons, same
+    populations as the oracle."""
+    from champ_b200.engine import Dmc, Engine
+    mw = 4 * W
+    s, o, e0, x, rng, pop = _vmc_start(oracle_mod, config, W, mw, 10)
+    eng = Engine(s)
+    dg = Dmc(eng, x, rng, pop, tau=0.02, etrial=e0, mwalk=mw)
+    dg.set_tmoves(-1)
+    do = oracle_mod.OracleDmc(o, x, rng, pop, tau=0.02, etrial=e0, mwalk=mw)
+    do.set_tmoves(-1)
+    for step in range(5):
+        dg.steps(1)
+        do.steps(1, 8)
+        _compare(dg, do)
+    assert dg.counts()["tmoves"] == do.tmoves() > 0

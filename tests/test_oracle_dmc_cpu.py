@@ -100,3 +100,31 @@ def test_dmc_branching_population(oracle_mod):
         assert 0 < len(wt) <= 4 * W
         assert np.all(wt >= 0) and np.all(np.isfinite(eo))
     assert len(set(sizes)) > 1, "population never changed: branching not exercised"
+
+
+def test_tmoves_oracle(oracle_mod):
+    """T-moves move electrons when the pseudopotential has negative matrix
+    elements, reproducibly, and are refused where unsupported."""
+    from champ_b200.system import make_synthetic, rotation_expansion
+    s = make_synthetic("c0")
+    o = oracle_mod.OracleSystem(s)
+    W = 16
+    st = oracle_mod.rng_states(4 * W + 1)
+    xs = []
+    for w in range(W):
+        x, st[w] = o.sites(st[w])
+        xs.append(x)
+    e0 = float(np.median([o.hpsi(x)["energy"] for x in xs]))
+    runs = []
+    for _ in range(2):
+        d = oracle_mod.OracleDmc(o, np.array(xs), st[:4 * W], st[4 * W], tau=0.02, etrial=e0, mwalk=4 * W)
+        d.set_tmoves(-1)
+        d.steps(4, 4)
+        runs.append((d.tmoves(), d.walkers()[0]))
+    assert runs[0][0] == runs[1][0] > 0
+    assert np.array_equal(runs[0][1], runs[1][1])
+    md, _ = rotation_expansion(make_synthetic("tiny"), [(0, 2, 3, 0.3)], extra_orbitals=2)
+    om = oracle_mod.OracleSystem(md)
+    dm = oracle_mod.OracleDmc(om, np.array([om.sites(st[0])[0]]), st[:4], st[4], tau=0.01, etrial=0.0, mwalk=4)
+    with pytest.raises(ValueError):
+        dm.set_tmoves(-1)
