@@ -113,32 +113,18 @@ class ClockSampler:
 
 
 def dist_setup(ngpus):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=None)
-        pg = dist
-    return rank, world, local, pg
+    """One process per GPU (torchrun): the replica plumbing of champ_b200.replicas."""
+    from champ_b200.replicas import Replicas
+    rep = Replicas()
+    return rep.rank, rep.world, rep.local, rep
 
 
-def max_over_ranks(v, pg, local):
-    if pg is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+def max_over_ranks(v, rep, local):
+    return rep.max(v)
 
 
-def barrier(pg, local):
-    import torch
-    if pg is not None:
-        pg.barrier()
-    torch.cuda.synchronize(local)
+def barrier(rep, local):
+    rep.barrier()
 
 
 def cpu_port_rate(system, walkers_cpu, nthreads, min_seconds=10.0, max_steps=4, seed_offset=0, warm_sweeps=1):
@@ -167,6 +153,7 @@ def cpu_port_rate(system, walkers_cpu, nthreads, min_seconds=10.0, max_steps=4, 
 def run_reference(args):
     rank, world, local, pg = dist_setup(args.gpus)
     if rank != 0:
+        pg.close()
         return 0
     from champ_b200.system import make_synthetic
     cfg, W, desc = CONFIGS[args.config]
@@ -189,6 +176,7 @@ def run_reference(args):
         "e2e": {"value": v, "unit": "electron-moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    pg.close()
     return 0
 
 
@@ -262,8 +250,7 @@ def run_dmc(args):
     stages = eng.stage_times()
     eng.profile(False)
     if rank != 0:
-        if pg is not None:
-            pg.destroy_process_group()
+        pg.close()
         return 0
     cpu_rate, cpu_steps, cpu_dt = cpu_port_dmc_rate(system, os.cpu_count() or 1, os.cpu_count() or 1)
     top = max(stages.items(), key=lambda kv: kv[1][0])
@@ -285,8 +272,7 @@ def run_dmc(args):
         "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    pg.close()
     return 0
 
 
@@ -301,8 +287,8 @@ def run_ours(args):
         W = args.walkers
     system = make_synthetic(cfg)
     # replica r runs its own walkers: streams r*W .. r*W+W-1 of the default seed
-    rng_all = rng_states(W * (rank + 1))
-    rng = rng_all[rank * W:].copy()
+    from champ_b200.replicas import rank_streams
+    rng = rank_streams(rank, W, rng_states)
     x = initial_configs(system, rng)
     eng = Engine(system, device=local, precision=args.precision)
     eng.set_walkers(x, rng)
@@ -349,8 +335,7 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0, pg, local)
     e2e = W * system.nelec * e2e_steps * world / e2e_s
     if rank != 0:
-        if pg is not None:
-            pg.destroy_process_group()
+        pg.close()
         return 0
     peaks, peak_kind = load_peaks()
     fp64_peak = None
@@ -413,8 +398,7 @@ def run_ours(args):
         "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    pg.close()
     return 0
 
 
