@@ -62,6 +62,7 @@ struct cw_ctx {
   HBuf hb{};
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
+  int ecp_warps = 1, ecp_naov = 0;
   int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
@@ -240,9 +241,9 @@ void launch_jfull(cw_ctx *c) {
 template <int NORD>
 void launch_ecp(cw_ctx *c) {
   if (c->mixed)
-    k_ecp<NORD, float><<<c->W, 32 * c->h.nquad, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+    k_ecp<NORD, float><<<c->W, 32 * c->ecp_warps, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
   else
-    k_ecp<NORD, double><<<c->W, 32 * c->h.nquad, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+    k_ecp<NORD, double><<<c->W, 32 * c->ecp_warps, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
 }
 template <int NORD>
 int set_attrs(cw_ctx *c) {
@@ -253,8 +254,30 @@ int set_attrs(cw_ctx *c) {
                           (int)c->smem_jfull));
   CK(cudaFuncSetAttribute(k_jastrow_full<NORD, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)c->smem_jfull));
-  if (c->h.nloc > 0)
-  {
+  if (c->h.nloc > 0) {
+    // warps per ECP block: the most resident warps per SM under the shared
+    // memory (228 KB), register (64 K) and warp (64) limits; ties go to the
+    // larger block (fewer list passes)
+    cudaFuncAttributes fa;
+    CK(c->mixed ? cudaFuncGetAttributes(&fa, k_ecp<NORD, float>) : cudaFuncGetAttributes(&fa, k_ecp<NORD, double>));
+    const int tbytes = c->mixed ? 4 : 8, nb = 2 * ((een_nb(NORD) + 1) / 2);
+    const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+    const int naov = c->ecp_naov;
+    int best = 0;
+    for (int nw = 4; nw <= kEcpMaxWarps; nw++) {
+      const size_t bytes = sizeof(double) * (ecp_base_doubles(c->h.N, c->h.M, 32 * nw) +
+                                             (size_t)nw * ecp_warp_doubles(c->h.M, nb, tbytes, naov)) +
+                           fa.sharedSizeBytes;
+      if (bytes > 227 * 1024) continue;
+      const int blocks = (int)std::min<size_t>({(size_t)(64 / nw), (228 * 1024) / (bytes + 1024),
+                                                (size_t)(65536 / (regs_warp * nw))});
+      if (blocks * nw >= best && blocks > 0) {
+        best = blocks * nw;
+        c->ecp_warps = nw;
+        c->smem_ecp = bytes - fa.sharedSizeBytes;
+      }
+    }
+    if (best == 0) return fail(c, CW_ERR_UNSUPPORTED, "ECP stage shared memory too large");
     CK(cudaFuncSetAttribute(k_ecp<NORD, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
     CK(cudaFuncSetAttribute(k_ecp<NORD, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
   }
@@ -930,9 +953,6 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   c->smem_ctil = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64);
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
-    c->smem_ecp = sizeof(double) * ((size_t)h.N * h.M + 3 * h.N + 4 * h.M + (size_t)h.nquad * h.M +
-                                    (size_t)h.nquad * h.M * 2 * ((een_nb(nord) + 1) / 2) + 1 +
-                                    (size_t)h.nquad * h.M * kCenRec);
   }
   // warp-per-point basis kernels: as many warps per block as 4 records fit
   c->basis_warps = (int)std::max<size_t>(1, std::min<size_t>(4, (160 * 1024) / ((size_t)h.M * kCenRec * sizeof(double))));
@@ -941,9 +961,10 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(cudaFuncSetAttribute(k_basis_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_basis));
   CK(cudaFuncSetAttribute(k_slater_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_sinv));
   CK(cudaFuncSetAttribute(k_ctilde, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ctil));
+  c->mixed = precision == CW_PREC_MIXED;
+  c->ecp_naov = d->ndet > 1 ? h.K : 0;  // the ECP stage keeps the point's basis values for the B matrix
   int rc = nord_attrs(c);
   if (rc) return rc;
-  if (c->smem_ecp > 227 * 1024 && h.nloc) return fail(c, CW_ERR_UNSUPPORTED, "ECP stage shared memory too large");
   if (d->ndet > 1) {
     // compact multideterminant tables (multideterminants_define)
     std::vector<int> exc, kw;
@@ -968,6 +989,8 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     CK(cudaMemcpy(dcd, cdet.data(), sizeof(double) * cdet.size(), cudaMemcpyHostToDevice));
     c->mdt = MdTab{dexc, dkw, dcd, numax};
     c->md_on = true;
+    if (h.nloc > 0 && c->ecp_naov != h.K)  // the ECP block's basis-value rows must be sized
+      return fail(c, CW_ERR_STATE, "ECP stage sized without multideterminant basis rows");
     const size_t O = h.Oa;
     c->smem_md_hpsi = sizeof(double) * (4 * (size_t)nmax * nmax + (size_t)nmax * O + numax + 1);
     c->smem_md_phase = sizeof(double) * ((size_t)numax + 1);

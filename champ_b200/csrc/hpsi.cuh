@@ -468,7 +468,7 @@ __global__ void k_ctilde(WState st, HBuf hb, GSys g) {
 }
 
 // ---------------------------------------------------------------------------
-// Pseudopotential: CTA per walker, one warp per quadrature point.
+// Pseudopotential: CTA per walker, warps over (pair, quadrature point).
 // ---------------------------------------------------------------------------
 template <int NORD>
 __device__ __forceinline__ double psinl_d(double u, double rri, double rrj, int it) {
@@ -504,77 +504,122 @@ __device__ __forceinline__ double psibnl_d(double u, int isb, int ipar, double s
   return psibnl_t<double>(u, isb, ipar, sspinn);
 }
 
+// Shared-memory plan of k_ecp (in doubles, every region 16-byte aligned):
+//   rr_en [N][M] scaled e-n distances, sx [3][N], the pair list (channel
+//   potentials [cap][3], packed i*M+ic [cap] ints), then per warp: the
+//   point's scaled e-n distances [M], its folded e-e-n coefficients [M][NB],
+//   its basis prepass [M][kCenRec] and, for multideterminant wave functions,
+//   its basis values [K] (reused by the pseudopotential B matrix).
+constexpr int kEcpMaxWarps = 16;
+__host__ __device__ inline size_t ecp_base_doubles(int N, int M, int cap) {
+  const size_t b = (size_t)N * M + 3 * (size_t)N + 3 * (size_t)cap + (size_t)(cap + 1) / 2;
+  return b + (b & 1);
+}
+__host__ __device__ inline size_t ecp_warp_doubles(int M, int nb, int tbytes, int naov) {
+  size_t bq = ((size_t)M * nb * tbytes + 7) / 8;
+  bq += bq & 1;
+  return (size_t)(M + (M & 1)) + bq + (size_t)M * kCenRec + (size_t)(naov + (naov & 1));
+}
+
 // T: arithmetic of the quadrature points' Jastrow ratio terms (double:
 // parity path, float: mixed path); the ratio sums, potentials, basis values
 // and the determinant ratio stay FP64.
+//
+// CTA per walker.  getvps_gauss (vmc/nonloc_pot.f90:3) runs for every
+// (electron, centre) pair in parallel; the pairs whose non-local channels
+// pass the reference's 1e-4 test are listed in (electron, centre) order, and
+// each warp then evaluates (pair, quadrature point) units round-robin: the
+// point's determinant ratio (nonlocd_quad through c~), its Jastrow ratio
+// (nonlocj_quad4) and the weighted Legendre sum (vmc/nonloc.f90:5).  The list
+// holds at most blockDim entries; a walker with more active pairs is
+// processed in several passes, in the same order.
 template <int NORD, typename T>
-__global__ void k_ecp(WState st, HBuf hb, GSys g) {
+__global__ void __launch_bounds__(32 * kEcpMaxWarps) k_ecp(WState st, HBuf hb, GSys g) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
-  const int N = cs.N, M = cs.M, K = cs.K, NQ = cs.nquad;
-  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;  // warp q <-> quadrature point q
-  extern __shared__ __align__(16) double smem[];
-  double *rr_en = smem;                 // [N][M] scaled e-n distances
-  double *sx = rr_en + N * M;           // [3][N]
-  double *vps = sx + 3 * N;             // [M][4] channel potentials of the current electron
-  double *rrq = vps + 4 * M;            // [NQ][M]
+  const int N = cs.N, M = cs.M, K = cs.K, NQ = cs.nquad, NM = N * M;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5, cap = blockDim.x;
   constexpr int NB = 2 * ((een_nb(NORD) + 1) / 2);
-  // [NQ][M][NB] folded e-e-n coefficients of the point; 16-byte aligned for
-  // the vector loads of een_apply0 (NB is even)
-  const size_t bq_off = (((size_t)(rrq - smem) + (size_t)NQ * M) + 1) & ~(size_t)1;
-  T *bq = reinterpret_cast<T *>(smem + bq_off);
-  double *recq = smem + bq_off + (size_t)NQ * M * NB;  // [NQ][M][kCenRec] basis prepass of the point
-  __shared__ int s_act[CW_MAX_CENT];
-  __shared__ int s_nact;
+  extern __shared__ __align__(16) double smem[];
+  double *rr_en = smem;                         // [N][M]
+  double *sx = rr_en + NM;                      // [3][N]
+  double *lst_v = sx + 3 * N;                   // [cap][3] non-local channel potentials
+  int *lst_ie = reinterpret_cast<int *>(lst_v + 3 * cap);  // [cap] i*M + ic
+  const int naov = hb.md_P ? K : 0;
+  const size_t wsd = ecp_warp_doubles(M, NB, (int)sizeof(T), naov);
+  double *wsp = smem + ecp_base_doubles(N, M, cap) + (size_t)wid * wsd;
+  double *rq = wsp;                             // [M]
+  T *bq = reinterpret_cast<T *>(wsp + M + (M & 1));  // [M][NB]
+  double *aov = wsp + wsd - (naov + (naov & 1));      // [K] basis values (multideterminant)
+  double *rec = aov - (size_t)M * kCenRec;            // [M][kCenRec]
+  __shared__ int s_wcnt[kEcpMaxWarps];
+  __shared__ int s_total;
+  __shared__ double s_red[kEcpMaxWarps][3];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
+  if (threadIdx.x == 0) s_total = 0;
   __syncthreads();
-  for (int t = threadIdx.x; t < N * M; t += blockDim.x) {
+  for (int t = threadIdx.x; t < NM; t += blockDim.x) {
     const int jj = t / M, jc = t % M;
     const double d0 = sx[jj] - cs.cent[3 * jc], d1 = sx[N + jj] - cs.cent[3 * jc + 1], d2 = sx[2 * N + jj] - cs.cent[3 * jc + 2];
     rr_en[t] = scale0<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2));
   }
   const double *xqw = st.xq + (size_t)w * 3 * NQ;
   const double *fso = st.fso + (size_t)w * N * N;
-  double vp_acc[2] = {0, 0};
-  double vloc = 0;
-  for (int i = 0; i < N; i++) {
-    __syncthreads();
-    // vps of electron i for every centre (getvps_gauss)
-    for (int ic = threadIdx.x; ic < M; ic += blockDim.x) {
-      const int ict = cs.iwctype[ic];
-      const double d0 = sx[i] - cs.cent[3 * ic], d1 = sx[N + i] - cs.cent[3 * ic + 1], d2 = sx[2 * N + i] - cs.cent[3 * ic + 2];
-      const double r = fmax(1.0e-10, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
-      const int lp = cs.lpot[ict];
-      vps[4 * ic + (lp - 1)] = gauss_pot_d(r, lp, ict) - cs.znuc[ict] * (1.0 / r);
-      for (int l = 1; l <= lp - 1; l++) vps[4 * ic + (l - 1)] = gauss_pot_d(r, l, ict);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int na = 0;
-      for (int ic = 0; ic < M; ic++) {
-        const int ict = cs.iwctype[ic];
-        vloc += vps[4 * ic + cs.lpot[ict] - 1];
-        int skip = 1;
-        for (int l = 1; l <= cs.lpot[ict] - 1; l++)
-          if (fabs(vps[4 * ic + l - 1]) > 1.0e-4) skip = 0;
-        if (!skip) s_act[na++] = ic;
+  double vp0 = 0, vp1 = 0, vloc = 0;
+  int cursor = 0;
+  for (;;) {
+    // ---- list the active (electron, centre) pairs from `cursor` on
+    while (cursor < NM) {
+      const int t = cursor + threadIdx.x;
+      int flag = 0;
+      double v[3] = {0, 0, 0}, vl = 0;
+      if (t < NM) {
+        const int i = t / M, ic = t % M, ict = cs.iwctype[ic];
+        const double d0 = sx[i] - cs.cent[3 * ic], d1 = sx[N + i] - cs.cent[3 * ic + 1], d2 = sx[2 * N + i] - cs.cent[3 * ic + 2];
+        const double r = fmax(1.0e-10, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+        const int lp = cs.lpot[ict];
+        vl = gauss_pot_d(r, lp, ict) - cs.znuc[ict] * (1.0 / r);
+#pragma unroll
+        for (int l = 1; l <= 3; l++) {
+          if (l <= lp - 1) {
+            v[l - 1] = gauss_pot_d(r, l, ict);
+            if (fabs(v[l - 1]) > 1.0e-4) flag = 1;
+          }
+        }
       }
-      s_nact = na;
+      const unsigned bal = __ballot_sync(0xffffffffu, flag);
+      if (lane == 0) s_wcnt[wid] = __popc(bal);
+      __syncthreads();
+      int off = 0, tot = 0;
+      for (int k = 0; k < nw; k++) {
+        const int c = s_wcnt[k];
+        off += k < wid ? c : 0;
+        tot += c;
+      }
+      const int base = s_total;
+      __syncthreads();  // s_wcnt and s_total read by every thread
+      if (base + tot > cap) break;  // uniform: this chunk opens the next pass
+      if (flag) {
+        const int pos = base + off + __popc(bal & ((1u << lane) - 1u));
+        lst_ie[pos] = t;
+        lst_v[3 * pos] = v[0]; lst_v[3 * pos + 1] = v[1]; lst_v[3 * pos + 2] = v[2];
+      }
+      vloc += vl;
+      if (threadIdx.x == 0) s_total = base + tot;
+      cursor += blockDim.x;
+      __syncthreads();
     }
-    __syncthreads();
-    const int na = s_nact;
-    if (q >= NQ) continue;
-    const int iab = i < cs.nup ? 0 : 1;
-    for (int a = 0; a < na; a++) {
-      const int ic = s_act[a];
+    const int nlist = s_total;
+    // ---- (pair, quadrature point) units, round-robin over warps
+    for (int u = wid; u < nlist * NQ; u += nw) {
+      const int a = u / NQ, q = u - a * NQ;
+      const int pt = lst_ie[a], i = pt / M, ic = pt - (pt / M) * M;
       const int ict = cs.iwctype[ic];
       const double ri_v[3] = {sx[i] - cs.cent[3 * ic], sx[N + i] - cs.cent[3 * ic + 1], sx[2 * N + i] - cs.cent[3 * ic + 2]};
       const double rin = sqrt(ri_v[0] * ri_v[0] + ri_v[1] * ri_v[1] + ri_v[2] * ri_v[2]);
       const double xqq = xqw[q], yqq = xqw[NQ + q], zqq = xqw[2 * NQ + q];
       const double costh = (ri_v[0] * xqq + ri_v[1] * yqq + ri_v[2] * zqq) * (1.0 / rin);
       const double xp[3] = {rin * xqq + cs.cent[3 * ic], rin * yqq + cs.cent[3 * ic + 1], rin * zqq + cs.cent[3 * ic + 2]};
-      double *rq = rrq + (size_t)q * M;
-      double *rec = recq + (size_t)q * M * kCenRec;
       // distance_quad (r_en_quad(iq,ic) = r_en(i,ic)) and the folded e-e-n
       // coefficients of the point
       for (int jc = lane; jc < M; jc += 32) {
@@ -583,7 +628,7 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
         if (jc == ic) r = rin;
         rq[jc] = scale0<double>(r);
         if (NORD > 1)
-          een_fold0<NORD, T>(een_coef<T>(cs.iwctype[jc]), T(1 - cs.scalek * rq[jc]), bq + ((size_t)q * M + jc) * NB);
+          een_fold0<NORD, T>(een_coef<T>(cs.iwctype[jc]), T(1 - cs.scalek * rq[jc]), bq + (size_t)jc * NB);
       }
       warp_basis_prepass<0>(g, xp, rec, lane);
       __syncwarp();
@@ -592,7 +637,10 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
       const double *ct = hb.ctilde + ((size_t)w * N + i) * K;
       double dr = 0;
       for (int m = lane; m < K; m += 32)
-        warp_basis_ao<0>(g, rec, m, [&](int, int, double v) { dr += v * ct[m]; });
+        warp_basis_ao<0>(g, rec, m, [&](int, int, double v) {
+          dr += v * ct[m];
+          if (naov) aov[m] = v;
+        });
       dr = warp_sum(dr);
       // Jastrow ratio (nonlocj_quad4)
       double fsum = 0;
@@ -613,9 +661,9 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
             const double rrj = rr_en[jj * M + jc];
             if (rq[jc] == cs.asymp_r && rrj == cs.asymp_r) continue;
             if constexpr (sizeof(T) == 8)
-              f += een_apply0<NORD>((const double *)(bq + ((size_t)q * M + jc) * NB), 1 - cs.scalek * rrj, (double)z);
+              f += een_apply0<NORD>((const double *)(bq + (size_t)jc * NB), 1 - cs.scalek * rrj, (double)z);
             else
-              f += een_apply0f<NORD>((const float *)(bq + ((size_t)q * M + jc) * NB), 1 - kT * (T)rrj, (float)z);
+              f += een_apply0f<NORD>((const float *)(bq + (size_t)jc * NB), 1 - kT * (T)rrj, (float)z);
           }
         }
         fsum += (double)f - fso[(size_t)i * N + jj];
@@ -624,34 +672,37 @@ __global__ void k_ecp(WState st, HBuf hb, GSys g) {
       for (int jc = lane; jc < M; jc += 32) fen += psianl_d(rq[jc], cs.iwctype[jc]);
       fsum = warp_sum(fsum) + (warp_sum(fen) - fso[(size_t)i * N + i]);
       double term = 0;
-      for (int l = 1; l <= cs.lpot[ict] - 1; l++) term += yl0_d(l, costh) * vps[4 * ic + (l - 1)];
+      for (int l = 1; l <= cs.lpot[ict] - 1; l++) term += yl0_d(l, costh) * lst_v[3 * a + (l - 1)];
       const double trj = term * cs.wq[q] * exp(fsum);
-      vp_acc[iab] += trj * dr;
+      if (i < cs.nup) vp0 += trj * dr;
+      else vp1 += trj * dr;
       if (hb.tvpsp && lane == 0)  // transition matrix element of a T-move (nonloc.f90:296)
         hb.tvpsp[(((size_t)w * N + i) * NQ + q) * M + ic] = dr * trj;
       if (hb.md_P) {
         // pseudopotential B matrix of every orbital (nonloc.f90:271): the
         // basis values of the point weighted by trj, contracted with coef later
         double *P = hb.md_P + ((size_t)w * N + i) * K;
-        for (int m = lane; m < K; m += 32)
-          warp_basis_ao<0>(g, rec, m, [&](int, int, double v) { atomicAdd(&P[m], trj * v); });
+        for (int m = lane; m < K; m += 32) atomicAdd(&P[m], trj * aov[m]);
       }
       __syncwarp();
     }
+    __syncthreads();  // list consumed
+    if (cursor >= NM) break;
+    if (threadIdx.x == 0) s_total = 0;
   }
-  __syncthreads();
-  __shared__ double s_vp[32][2];
-  if (lane == 0 && q < 32) {
-    s_vp[q][0] = vp_acc[0];
-    s_vp[q][1] = vp_acc[1];
+  vloc = warp_sum(vloc);
+  if (lane == 0) {
+    s_red[wid][0] = vp0;
+    s_red[wid][1] = vp1;
+    s_red[wid][2] = vloc;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double a = 0, b = 0;
-    for (int k = 0; k < NQ; k++) { a += s_vp[k][0]; b += s_vp[k][1]; }
+    double a = 0, b = 0, c = 0;
+    for (int k = 0; k < nw; k++) { a += s_red[k][0]; b += s_red[k][1]; c += s_red[k][2]; }
     hb.vpsp[2 * w] = a;
     hb.vpsp[2 * w + 1] = b;
-    hb.pe_ecp[w] = vloc;
+    hb.pe_ecp[w] = c;
   }
 }
 
