@@ -73,6 +73,64 @@ __device__ double t_area_d(double zeta, double co, double rbot, double rtop, dou
          (bot * sqrt(zeta * zeta * zeta));
 }
 
+// One candidate of metrop6's radial rejection loop (vmc/metrop_mov1_slat.f90:236-240):
+// rtry from the first draw, accepted when top/fmax exceeds the second.
+__device__ __forceinline__ bool radial_candidate(DRng &r, double rmin, double deltar, double deltri, double co,
+                                                 double zeta, double fmx, double &rtry, double &top) {
+  rtry = ((deltar - deltri) * r.uniform() + deltri) * rmin;
+  top = sqrt(rtry) * fabs(1.0 + co * rtry) * exp(-zeta * rtry);
+  const double ratio = top / fmx;
+  return ratio > r.uniform();
+}
+
+// The radial rejection loop with the reference's draw order.  Each lane first
+// tries kRadialSerial candidates of its own walker; the walkers still pending
+// are then taken one at a time by the whole warp, lane L testing candidate L
+// of the next 32 (its copy of the stream advanced by 2L draws).  The first
+// accepted candidate, and the stream state after it, are those of the serial
+// loop.  Every lane of the warp must call it.  Returns true when the loop gave
+// up (more than ~10^6 candidates: a non-finite walker).
+constexpr int kRadialSerial = 16;
+__device__ __noinline__ bool radial_sample(DRng &rng, bool live, double rmin, double deltar, double deltri,
+                                           double co, double zeta, double fmx, double &rtry, double &top) {
+  bool done = !live, gave_up = false;
+  for (int k = 0; k < kRadialSerial && !done; k++) done = radial_candidate(rng, rmin, deltar, deltri, co, zeta, fmx, rtry, top);
+  const int lane = threadIdx.x & 31;
+  int rounds = 0;
+  unsigned pend = __ballot_sync(0xffffffffu, !done);
+  while (pend) {
+    const int p = __ffs(pend) - 1;
+    DRng r;
+    r.s0 = __shfl_sync(0xffffffffu, rng.s0, p);
+    r.s1 = __shfl_sync(0xffffffffu, rng.s1, p);
+    r.s2 = __shfl_sync(0xffffffffu, rng.s2, p);
+    r.s3 = __shfl_sync(0xffffffffu, rng.s3, p);
+    const double rm = __shfl_sync(0xffffffffu, rmin, p), cp = __shfl_sync(0xffffffffu, co, p);
+    const double zp = __shfl_sync(0xffffffffu, zeta, p), fp = __shfl_sync(0xffffffffu, fmx, p);
+    for (int k = 0; k < 2 * lane; k++) r.next();
+    double rt, tp;
+    const bool ok = radial_candidate(r, rm, deltar, deltri, cp, zp, fp, rt, tp);
+    const unsigned am = __ballot_sync(0xffffffffu, ok);
+    const int ks = am ? __ffs(am) - 1 : 31;
+    const uint64_t n0 = __shfl_sync(0xffffffffu, r.s0, ks), n1 = __shfl_sync(0xffffffffu, r.s1, ks);
+    const uint64_t n2 = __shfl_sync(0xffffffffu, r.s2, ks), n3 = __shfl_sync(0xffffffffu, r.s3, ks);
+    const double rtk = __shfl_sync(0xffffffffu, rt, ks), tpk = __shfl_sync(0xffffffffu, tp, ks);
+    if (lane == p) {
+      rng.s0 = n0; rng.s1 = n1; rng.s2 = n2; rng.s3 = n3;
+      if (am) {
+        rtry = rtk;
+        top = tpk;
+        done = true;
+      } else if (++rounds > 32768) {
+        gave_up = true;
+        done = true;
+      }
+    }
+    pend = __ballot_sync(0xffffffffu, !done);
+  }
+  return gave_up;
+}
+
 __device__ __forceinline__ void spin_of(int iel, int &iab, int &nel, int &ish) {
   if (iel < cs.nup) { iab = 0; nel = cs.nup; ish = 0; }
   else { iab = 1; nel = cs.ndn; ish = cs.nup; }
@@ -85,8 +143,11 @@ __device__ __forceinline__ void spin_of(int iel, int &iab, int &nel, int &ish) {
 // + vj.
 // ---------------------------------------------------------------------------
 __global__ void k_propose(WState st, MoveBuf mb, int iel) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= st.W) return;
+  // Every lane runs to the end (the radial sampling below is warp-cooperative);
+  // lanes past the population mirror the last walker and store nothing.
+  const int wt = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = wt < st.W;
+  const int w = live ? wt : st.W - 1;
   const int N = cs.N, nmax = cs.nmax;
   int iab, nel, ish;
   spin_of(iel, iab, nel, ish);
@@ -119,7 +180,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   double rv[3];
   for (int k = 0; k < 3; k++) rv[k] = st.rvmino[((size_t)w * 3 + k) * N + iel];
   const double rmin = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
-  st.rmino[(size_t)w * N + iel] = rmin;
+  if (live) st.rmino[(size_t)w * N + iel] = rmin;
   double rbot = rmin * deltri, rtop = rmin * deltar;
   double voldr = zero;
   for (int ic = 0; ic < 3; ic++) voldr += vo[ic] * rv[ic];
@@ -167,14 +228,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   }
   double bot = sqrt(rmin) * fabs(one + co * rmin) * exp(-zeta * rmin);
   double rtry, top;
-  // rejection sampling of r; bounded so that a non-finite walker cannot spin
-  for (int guard = 0;; guard++) {
-    rtry = ((deltar - deltri) * rng.uniform() + deltri) * rmin;
-    top = sqrt(rtry) * fabs(one + co * rtry) * exp(-zeta * rtry);
-    double ratio = top / fmx;
-    if (ratio > rng.uniform()) break;
-    if (guard > 1000000) { st.status[w] |= 4; break; }
-  }
+  if (radial_sample(rng, live, rmin, deltar, deltri, co, zeta, fmx, rtry, top) && live) st.status[w] |= 4;
   fxop = fxop * top / bot;
   double areao = t_area_d(zeta, co, rbot, rtop, bot);
   double raver = half * (rmin + rtry);
@@ -242,6 +296,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   m.rratio = m.rminno / rminon;
   m.nearestn = nearn;
   m.tel = iel;
+  if (!live) return;
   mb.ms[w] = m;
   rng.store(st.rng + 4 * (size_t)w);
 }
