@@ -25,7 +25,7 @@ struct HBuf {
   double *phi;      // [rows][K] chunk basis
   double *orball;   // [rows][Oa] chunk orbitals
   double *ctilde;   // [W][N][K]
-  double *entab;    // [W][M][N][8] e-n table of the full Jastrow: rr, dd1, dd2, r, rvec(3)
+  double *entab;    // [W][5][M][N] e-n table of the full Jastrow (k_jastrow_full)
   int chunk;        // electrons per chunk
   float *phi_hi, *phi_lo;  // mixed precision: [rows][kp] split chunk basis (null in FP64)
   int kp;
@@ -60,59 +60,93 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 
 // ---------------------------------------------------------------------------
 // jastrow_factor4 (vmc/jastrow4.f90:3): CTA per walker.
-//  1. e-n table of every (electron, centre): scaled distance and its
-//     derivatives, the distance and its vector (L2-resident scratch);
+//  1. thread per electron over the centres: the e-n table (scaled distance,
+//     its derivative factors, r^2) in structure-of-arrays form, the move
+//     kernels' e-n table, and the e-n terms;
 //  2. pair rows i and N-1-i together (N-1 pairs per batch): the row
 //     electron's e-e-n coefficients are folded per centre (value, d/dx,
-//     d2/dx2) into shared memory, then threads over the batch's pairs
-//     evaluate every centre from the folded coefficients;
-//  3. e-n terms, per-electron gradient sums, block sums.
+//     d2/dx2) into shared memory with its table entries, then threads over
+//     the batch's pairs evaluate every centre from the folded coefficients;
+//     the table stores d rr/dr divided by r, so the pair-centre loop has no
+//     division;
+//  3. per-electron gradient sums (warp per row) and block sums.
 // ---------------------------------------------------------------------------
+// e-n table fields ([W][kEnFields][M][N]): scaled distance rr, -kappa rr',
+// -kappa rr'', -kappa rr'/r, r^2
+constexpr int kEnFields = 5;
+
 // T is the arithmetic of the pair and e-e-n terms (double: parity path,
 // float: mixed path); distances, 1/r_ij, the tables and the sums over
 // pairs stay FP64.
 template <int NORD, typename T>
-__global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jastrow_full(WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
-  const int N = cs.N, M = cs.M;
+  const int N = cs.N, M = cs.M, MN = M * N;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   constexpr int NB = een_nb(NORD);
   extern __shared__ __align__(16) double smem[];
   double *sx = smem;                      // [3][N]
-  T *sB = reinterpret_cast<T *>(smem + 3 * N + (3 * N & 1));  // [2][M][3*NB] folded rows
+  double *sI = sx + 3 * N;                // [2][M][8] table entries and e-n vectors of the batch's rows
+  T *sB = reinterpret_cast<T *>(sI + 2 * M * 8);  // [2][M][3*NB] folded rows
   __shared__ double red[4];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
   __syncthreads();
-  const double kap = cs.scalek;
-  double *tab = hb.entab + (size_t)w * M * N * 8;
-  for (int t = threadIdx.x; t < M * N; t += blockDim.x) {
-    const int ic = t / N, e = t % N;
-    const double v0 = sx[e] - cs.cent[3 * ic], v1 = sx[N + e] - cs.cent[3 * ic + 1], v2 = sx[2 * N + e] - cs.cent[3 * ic + 2];
-    const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-    double rr, dd1, dd2;
-    scale2<double>(r, rr, dd1, dd2);
-    double *q = tab + (size_t)t * 8;
-    q[0] = rr; q[1] = dd1; q[2] = dd2; q[3] = r; q[4] = v0; q[5] = v1; q[6] = v2; q[7] = 0;
-    st.enm[(size_t)w * 2 * M * N + t] = rr;
-    st.enm[((size_t)w * 2 + 1) * M * N + t] = dd1 / r;
-  }
+  const double kap = cs.scalek, asym = cs.asymp_r;
+  double *tab = hb.entab + (size_t)w * kEnFields * MN;
   double *fso = st.fso + (size_t)w * N * N;
   double *fij0 = st.fijo + ((size_t)w * 3 + 0) * N * N;
   double *fij1 = st.fijo + ((size_t)w * 3 + 1) * N * N;
   double *fij2 = st.fijo + ((size_t)w * 3 + 2) * N * N;
   double fsum = 0, d2sum = 0, pee = 0;
-  const int nbatch = N / 2;  // rows (b, N-1-b); the middle row of odd N joins batch 0 below
+  // 1. e-n table and e-n terms
+  for (int e = threadIdx.x; e < N; e += blockDim.x) {
+    double fs = 0, d2 = 0, g[3] = {0, 0, 0};
+    for (int ic = 0; ic < M; ic++) {
+      const double v0 = sx[e] - cs.cent[3 * ic], v1 = sx[N + e] - cs.cent[3 * ic + 1], v2 = sx[2 * N + e] - cs.cent[3 * ic + 2];
+      const double r2 = v0 * v0 + v1 * v1 + v2 * v2, r = sqrt(r2);
+      double rr, dd1, dd2;
+      scale2<double>(r, rr, dd1, dd2);
+      const int t = ic * N + e;
+      tab[t] = rr;
+      tab[MN + t] = -kap * dd1;
+      tab[2 * MN + t] = -kap * dd2;
+      tab[3 * MN + t] = -kap * dd1 / r;
+      tab[4 * MN + t] = r2;
+      st.enm[(size_t)w * 2 * MN + t] = rr;
+      st.enm[((size_t)w * 2 + 1) * MN + t] = dd1 / r;
+      if (rr == asym) continue;
+      double fen, feni, fenii;
+      en_term<2, double>(cs.iwctype[ic], rr, fen, feni, fenii);
+      fenii = fenii * dd1 * dd1 + feni * dd2;
+      feni = feni * dd1 / r;
+      fs += fen;
+      g[0] += feni * v0;
+      g[1] += feni * v1;
+      g[2] += feni * v2;
+      d2 += fenii + 2 * feni;
+    }
+    fso[(size_t)e * N + e] = fs;
+    fij0[(size_t)e * N + e] = g[0];
+    fij1[(size_t)e * N + e] = g[1];
+    fij2[(size_t)e * N + e] = g[2];
+    fsum += fs;
+    d2sum += d2;
+  }
+  // 2. pairs
+  const T kT = (T)kap, asymT = (T)asym;
   for (int bt = 0; bt < (N + 1) / 2; bt++) {
     const int ia = bt, ib = N - 1 - bt;  // ia == ib only for the middle row of odd N
     const int npa = ia, npb = (ib != ia) ? ib : 0;
-    __syncthreads();  // previous batch done with sB; table written
-    if (NORD > 1) {
-      for (int t = threadIdx.x; t < 2 * M; t += blockDim.x) {
-        const int row = t / M, ic = t % M;
-        const int i = row == 0 ? ia : ib;
-        const double rr = tab[((size_t)ic * N + i) * 8];
-        een_fold2<NORD, T>(een_coef<T>(cs.iwctype[ic]), T(1 - kap * rr), sB + ((size_t)row * M + ic) * 3 * NB);
-      }
+    __syncthreads();  // previous batch done with sB / sI; table written
+    for (int t = threadIdx.x; t < 2 * M; t += blockDim.x) {
+      const int row = t / M, ic = t % M;
+      const int i = row == 0 ? ia : ib;
+      double *q = sI + (size_t)t * 8;
+#pragma unroll
+      for (int f = 0; f < kEnFields; f++) q[f] = tab[f * MN + ic * N + i];
+      for (int k = 0; k < 3; k++) q[kEnFields + k] = sx[k * N + i] - cs.cent[3 * ic + k];
+      if (NORD > 1) een_fold2<NORD, T>(een_coef<T>(cs.iwctype[ic]), T(1 - kap * q[0]), sB + (size_t)t * 3 * NB);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < npa + npb; t += blockDim.x) {
@@ -121,19 +155,21 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
       int isb, ipar;
       double sspinn;
       pair_spin(i, j, isb, ipar, sspinn);
-      const double rv[3] = {sx[i] - sx[j], sx[N + i] - sx[N + j], sx[2 * N + i] - sx[2 * N + j]};
-      const double rij = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
-      pee += 1 / rij;
-      const T rijT = (T)rij, kT = (T)kap, asym = (T)cs.asymp_r;
+      const double xj[3] = {sx[j], sx[N + j], sx[2 * N + j]};
+      const double rv[3] = {sx[i] - xj[0], sx[N + i] - xj[1], sx[2 * N + i] - xj[2]};
+      const double rij2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2], rij = sqrt(rij2);
+      const double irij = 1 / rij;
+      pee += irij;
+      const T rijT = (T)rij, irijT = (T)irij, rij2T = (T)rij2;
       const T rvT[3] = {(T)rv[0], (T)rv[1], (T)rv[2]};
       T u, dd1, dd2;
       scale2<T>(rijT, u, dd1, dd2);
       T fs = 0, d2 = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
-      if (u != asym) {
+      if (u != (T)cs.asymp_r) {
         T fee, feeu, feeuu;
         ee_term<2, T>(isb, ipar, (T)sspinn, u, fee, feeu, feeuu);
         feeuu = feeuu * dd1 * dd1 + feeu * dd2;
-        feeu = feeu * dd1 / rijT;
+        feeu = feeu * dd1 * irijT;
         fs += fee;
         for (int k = 0; k < 3; k++) {
           gi[k] += feeu * rvT[k];
@@ -142,31 +178,34 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
         d2 += 2 * (feeuu + 2 * feeu);
       }
       if (NORD > 1) {
-        const T z = 1 - kT * u, du1 = -kT * dd1, du2 = -kT * dd2;
+        const T z = 1 - kT * u, du1 = -kT * dd1, du2 = -kT * dd2, du1r = du1 * irijT;
         const T *Brow = sB + (size_t)row * M * 3 * NB;
+        const double *Irow = sI + (size_t)row * M * 8;
+        const double *tj = tab + j;
         for (int ic = 0; ic < M; ic++) {
-          const double *qi = tab + ((size_t)ic * N + i) * 8;
-          const double *qj = tab + ((size_t)ic * N + j) * 8;
-          const T rri = (T)qi[0], rrj = (T)qj[0];
+          const double *qi = Irow + ic * 8;
+          const double rri = qi[0], rrj = tj[ic * N];
           if (rri == asym && rrj == asym) continue;
-          const T dd7 = -kT * (T)qi[1], dd9 = -kT * (T)qi[2], ri = (T)qi[3];
-          const T dd8 = -kT * (T)qj[1], dd10 = -kT * (T)qj[2], rj = (T)qj[3];
-          const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 3 * NB, 1 - kT * rrj, z);
-          const T sgs = ri + rj, tgs = ri - rj;
-          const T u2pst = rijT * rijT + sgs * tgs, u2mst = rijT * rijT - sgs * tgs;
+          const T Ai = (T)qi[1], Bi = (T)qi[2], Gi = (T)qi[3], Si = (T)qi[4];
+          const T Aj = (T)tj[MN + ic * N], Bj = (T)tj[2 * MN + ic * N], Gj = (T)tj[3 * MN + ic * N],
+                  Sj = (T)tj[4 * MN + ic * N];
+          const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 3 * NB, T(1 - kap * rrj), z);
+          const T dS = Si - Sj;
           const T fuu = e.fuu * du1 * du1 + e.fu * du2;
-          const T fu = e.fu * du1 / rijT;
-          const T fui = e.fui * du1 * dd7, fuj = e.fuj * du1 * dd8;
-          const T fii = e.fii * dd7 * dd7 + e.fi * dd9, fjj = e.fjj * dd8 * dd8 + e.fj * dd10;
-          const T fi = e.fi * dd7 / ri, fj = e.fj * dd8 / rj;
+          const T fu = e.fu * du1r;
+          const T fii = e.fii * Ai * Ai + e.fi * Bi, fjj = e.fjj * Aj * Aj + e.fj * Bj;
+          const T fi = e.fi * Gi, fj = e.fj * Gj;
           fs += e.fc;
-          gi[0] += fi * (T)qi[4] + fu * rvT[0];
-          gi[1] += fi * (T)qi[5] + fu * rvT[1];
-          gi[2] += fi * (T)qi[6] + fu * rvT[2];
-          gj[0] += fj * (T)qj[4] - fu * rvT[0];
-          gj[1] += fj * (T)qj[5] - fu * rvT[1];
-          gj[2] += fj * (T)qj[6] - fu * rvT[2];
-          d2 += 2 * (fuu + 2 * fu) + fui * u2pst / (ri * rijT) + fuj * u2mst / (rj * rijT) + fii + 2 * fi + fjj + 2 * fj;
+          const T vj0 = (T)(xj[0] - cs.cent[3 * ic]), vj1 = (T)(xj[1] - cs.cent[3 * ic + 1]),
+                  vj2 = (T)(xj[2] - cs.cent[3 * ic + 2]);
+          gi[0] += fi * (T)qi[5] + fu * rvT[0];
+          gi[1] += fi * (T)qi[6] + fu * rvT[1];
+          gi[2] += fi * (T)qi[7] + fu * rvT[2];
+          gj[0] += fj * vj0 - fu * rvT[0];
+          gj[1] += fj * vj1 - fu * rvT[1];
+          gj[2] += fj * vj2 - fu * rvT[2];
+          d2 += 2 * (fuu + 2 * fu) + du1r * (e.fui * Gi * (rij2T + dS) + e.fuj * Gj * (rij2T - dS)) + fii + 2 * fi +
+                fjj + 2 * fj;
         }
       }
       fso[(size_t)i * N + j] = fs;
@@ -178,45 +217,24 @@ __global__ void __launch_bounds__(128) k_jastrow_full(WState st, HBuf hb) {
       d2sum += d2;
     }
   }
-  (void)nbatch;
+  (void)asymT;
   __syncthreads();
-  // e-n terms
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    double fs = 0, d2 = 0, g[3] = {0, 0, 0};
-    for (int ic = 0; ic < M; ic++) {
-      const int it = cs.iwctype[ic];
-      const double *q = tab + ((size_t)ic * N + i) * 8;
-      const double rri = q[0];
-      if (rri == cs.asymp_r) continue;
-      const double dd7 = q[1], dd9 = q[2], ri = q[3];
-      double fen, feni, fenii;
-      en_term<2, double>(it, rri, fen, feni, fenii);
-      fenii = fenii * dd7 * dd7 + feni * dd9;
-      feni = feni * dd7 / ri;
-      fs += fen;
-      g[0] += feni * q[4];
-      g[1] += feni * q[5];
-      g[2] += feni * q[6];
-      d2 += fenii + 2 * feni;
-    }
-    fso[(size_t)i * N + i] = fs;
-    fij0[(size_t)i * N + i] = g[0];
-    fij1[(size_t)i * N + i] = g[1];
-    fij2[(size_t)i * N + i] = g[2];
-    fsum += fs;
-    d2sum += d2;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+  // 3. per-electron gradient sums: warp per row, lanes over the partners
+  for (int i = wid; i < N; i += blockDim.x >> 5) {
     double a0 = 0, a1 = 0, a2 = 0;
-    for (int j = 0; j < N; j++) {
+    for (int j = lane; j < N; j += 32) {
       a0 += fij0[(size_t)i * N + j];
       a1 += fij1[(size_t)i * N + j];
       a2 += fij2[(size_t)i * N + j];
     }
-    st.fjo[((size_t)w * 3 + 0) * N + i] = a0;
-    st.fjo[((size_t)w * 3 + 1) * N + i] = a1;
-    st.fjo[((size_t)w * 3 + 2) * N + i] = a2;
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
+    if (lane == 0) {
+      st.fjo[((size_t)w * 3 + 0) * N + i] = a0;
+      st.fjo[((size_t)w * 3 + 1) * N + i] = a1;
+      st.fjo[((size_t)w * 3 + 2) * N + i] = a2;
+    }
   }
   const double tf = block_sum<128>(fsum, red);
   const double td = block_sum<128>(d2sum, red);
