@@ -63,6 +63,7 @@ struct cw_ctx {
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
   int ecp_warps = 1, ecp_naov = 0;
+  double *bocc = nullptr;  // [nmax][K] coefficients of the occupied orbitals (c~ GEMM)
   int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
@@ -553,7 +554,10 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
   if (h.nloc > 0) {
     const int nchunk = (h.K + 63) / 64;
     stage_begin(c, CW_ST_CTILDE);
-    k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->st, c->hb, c->g);
+    if (c->bocc)  // rows (walker, spin, slot) of slmi times the occupied coefficient rows
+      dgemm(c->stream, W * N, h.K, h.nmax, c->st.slmi, c->bocc, c->hb.ctilde);
+    else
+      k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->st, c->hb, c->g);
     stage_end(c);
     LCHK("k_ctilde");
     stage_begin(c, CW_ST_ECP);
@@ -915,6 +919,17 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     if (v < 0 || v >= d->norb) return fail(c, CW_ERR_ARG, "iworbd entry out of range");
   DALLOC(L, slot, so.size());
   CK(cudaMemcpy(slot, so.data(), so.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // c~ as one GEMM over all walkers and both spins (slmi rows x occupied
+  // coefficient rows) when both spins fill nmax slots with the same orbitals
+  bool same_occ = d->nup == nmax && ndn == nmax && nmax % 2 == 0 && d->nbasis % 2 == 0;
+  for (int j = 0; same_occ && j < nmax; j++) same_occ = so[j] == so[nmax + j];
+  if (same_occ && d->nloc) {
+    std::vector<double> bo((size_t)nmax * d->nbasis);
+    for (int j = 0; j < nmax; j++)
+      for (int mm = 0; mm < d->nbasis; mm++) bo[(size_t)j * d->nbasis + mm] = d->coef[(size_t)so[j] * d->nbasis + mm];
+    DALLOC(L, c->bocc, bo.size());
+    CK(cudaMemcpy(c->bocc, bo.data(), bo.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   // r0*arg^(jx-1) of every grid point (splfit's ref0 for igrid 2 and 3)
   std::vector<double> gpw((size_t)d->nctype * (d->mrwf_pts + 1), 0.0);
   for (int it = 0; it < d->nctype; it++)
@@ -942,8 +957,8 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   // dynamic shared memory sizes
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
-    c->smem_jmove = sizeof(double) * 4 * (size_t)h.M * (6 + 2 * een_nb(nord));
-    c->smem_jmove_f32 = sizeof(float) * 4 * (size_t)h.M * (6 + 2 * een_nb(nord));
+    c->smem_jmove = sizeof(double) * 4 * (size_t)h.M * (8 + 2 * een_nb(nord));
+    c->smem_jmove_f32 = sizeof(float) * 4 * (size_t)h.M * (8 + 2 * een_nb(nord));
   }
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
@@ -961,6 +976,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(cudaFuncSetAttribute(k_basis_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_basis));
   CK(cudaFuncSetAttribute(k_slater_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_sinv));
   CK(cudaFuncSetAttribute(k_ctilde, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ctil));
+  CK(cudaFuncSetAttribute(k_dgemm_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMmaSmem));
   c->mixed = precision == CW_PREC_MIXED;
   c->ecp_naov = d->ndet > 1 ? h.K : 0;  // the ECP stage keeps the point's basis values for the B matrix
   int rc = nord_attrs(c);

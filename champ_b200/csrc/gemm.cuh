@@ -6,8 +6,9 @@
 // shared-memory doubles per 64 FMAs: the FP64 FMA rate of an SM needs at
 // most one shared double per 4 FMAs), 8-deep K slices staged in shared
 // memory (rows padded by 2 doubles: conflict-free transposed stores, 16-byte
-// aligned vector loads) with a register prefetch of the next slice.  FP64
-// SIMT: the B200 has no FP64 tensor-core path wider than its FMA units.
+// aligned vector loads) with a register prefetch of the next slice.  This
+// SIMT kernel serves the shapes the FP64 tensor-core kernel below does not
+// (odd K or N, N <= 16).
 #pragma once
 #include "common.cuh"
 
@@ -119,8 +120,117 @@ k_dgemm(int M, int N, int K, const double *__restrict__ A, const double *__restr
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core variant (mma.sync m16n8k4 .f64; tcgen05 has no FP64 kind):
+// 128x64 output tile per CTA, 4 warps of 32x64 (2x8 m16n8 accumulators in
+// registers), 16-deep K slices in a 3-stage cp.async ring.  Shared rows are
+// padded (A: 20 doubles, B: 68) so that the fragment loads of a half-warp hit
+// 16 distinct 8-byte bank pairs.  Needs K and N even (16-byte row chunks);
+// out-of-range chunks are zero-filled by the copy.
+// ---------------------------------------------------------------------------
+constexpr int kMmaBM = 128, kMmaBN = 64, kMmaBK = 16, kMmaSA = kMmaBK + 4, kMmaSB = kMmaBN + 4, kMmaStages = 3;
+constexpr size_t kMmaSmem = sizeof(double) * (size_t)kMmaStages * (kMmaBM * kMmaSA + kMmaBK * kMmaSB);
+
+__device__ __forceinline__ void cp_async16(double *dst, const double *src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+}
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], const double (&a)[2], double b) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a[0]), "d"(a[1]), "d"(b));
+}
+
+__global__ void __launch_bounds__(128, 2)
+k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C) {
+  constexpr int BM = kMmaBM, BN = kMmaBN, BK = kMmaBK, SA = kMmaSA, SB = kMmaSB, ST = kMmaStages;
+  extern __shared__ __align__(16) double gsm[];
+  double *As = gsm;                          // [ST][BM][SA]
+  double *Bs = gsm + (size_t)ST * BM * SA;   // [ST][BK][SB]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nk = (K + BK - 1) / BK;
+  auto load_stage = [&](int kt, int s) {
+    const int k0 = kt * BK;
+#pragma unroll
+    for (int c = tid; c < BM * (BK / 2); c += 128) {
+      const int r = c / (BK / 2), kc = (c % (BK / 2)) * 2;
+      const int gm = m0 + r, gk = k0 + kc;
+      const bool ok = gm < M && gk < K;
+      cp_async16(As + ((size_t)s * BM + r) * SA + kc, ok ? A + (size_t)gm * K + gk : A, ok ? 16 : 0);
+    }
+#pragma unroll
+    for (int c = tid; c < BK * (BN / 2); c += 128) {
+      const int r = c / (BN / 2), nc = (c % (BN / 2)) * 2;
+      const int gk = k0 + r, gn = n0 + nc;
+      const bool ok = gk < K && gn < N;
+      cp_async16(Bs + ((size_t)s * BK + r) * SB + nc, ok ? B + (size_t)gk * N + gn : B, ok ? 16 : 0);
+    }
+  };
+  double acc[2][8][4];
+#pragma unroll
+  for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+    for (int ni = 0; ni < 8; ni++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[mi][ni][q] = 0.0;
+#pragma unroll
+  for (int s = 0; s < ST - 1; s++) {
+    if (s < nk) load_stage(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; kt++) {
+    cp_async_wait<ST - 2>();
+    __syncthreads();  // slice kt landed for every thread; slice kt-1's stage is free
+    if (kt + ST - 1 < nk) load_stage(kt + ST - 1, (kt + ST - 1) % ST);
+    cp_async_commit();
+    const double *as = As + ((size_t)(kt % ST) * BM + warp * 32) * SA;
+    const double *bs = Bs + (size_t)(kt % ST) * BK * SB;
+#pragma unroll
+    for (int k4 = 0; k4 < BK; k4 += 4) {
+      double a[2][2], b[8];
+#pragma unroll
+      for (int mi = 0; mi < 2; mi++) {
+        a[mi][0] = as[(mi * 16 + g) * SA + k4 + t];
+        a[mi][1] = as[(mi * 16 + g + 8) * SA + k4 + t];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 8; ni++) b[ni] = bs[(k4 + t) * SB + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 8; ni++) dmma_16x8x4(acc[mi][ni], a[mi], b[ni]);
+    }
+  }
+  cp_async_wait<0>();
+  // accumulator (mi, ni): rows m0 + warp*32 + mi*16 + g (+8), columns n0 + ni*8 + 2t (+1)
+#pragma unroll
+  for (int mi = 0; mi < 2; mi++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int gm = m0 + warp * 32 + mi * 16 + g + 8 * h;
+      if (gm >= M) continue;
+#pragma unroll
+      for (int ni = 0; ni < 8; ni++) {
+        const int gn = n0 + ni * 8 + 2 * t;
+        if (gn < N) *reinterpret_cast<double2 *>(C + (size_t)gm * N + gn) = make_double2(acc[mi][ni][2 * h], acc[mi][ni][2 * h + 1]);
+      }
+    }
+  }
+}
+
 inline void dgemm(cudaStream_t s, int M, int N, int K, const double *A, const double *B, double *C) {
-  if (N <= 16) {
+  const bool al16 = ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(C)) & 15) == 0;
+  if (N > 16 && (K % 2) == 0 && (N % 2) == 0 && al16) {
+    dim3 grid((M + kMmaBM - 1) / kMmaBM, (N + kMmaBN - 1) / kMmaBN);
+    k_dgemm_mma<<<grid, 128, kMmaSmem, s>>>(M, N, K, A, B, C);
+  } else if (N <= 16) {
     constexpr int BM = 64, BN = 16, BK = 16, TM = 4, TN = 1;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
     k_dgemm<BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, s>>>(M, N, K, A, B, C);
