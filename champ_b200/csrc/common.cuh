@@ -563,10 +563,26 @@ __device__ __forceinline__ EenOut<T> een_pair2(const T *__restrict__ cc, T z, T 
   return e;
 }
 
+// three of the four values of a 16-byte (float) / 32-byte (double) aligned
+// quadruple, in vector loads
+template <typename T>
+__device__ __forceinline__ void ld3(const T *p, T &a, T &b, T &c);
+template <>
+__device__ __forceinline__ void ld3<float>(const float *p, float &a, float &b, float &c) {
+  const float4 v = *reinterpret_cast<const float4 *>(p);
+  a = v.x; b = v.y; c = v.z;
+}
+template <>
+__device__ __forceinline__ void ld3<double>(const double *p, double &a, double &b, double &c) {
+  const double2 v = *reinterpret_cast<const double2 *>(p);
+  a = v.x; b = v.y;
+  c = p[2];
+}
 
-// Fold with first and second x-derivatives: BD3[3*t .. 3*t+2] = B, dB, d2B
+// Fold with first and second x-derivatives: BD4[4*t .. 4*t+2] = B, dB, d2B
+// (BD4[4*t+3] pads the quadruple for the vector loads of een_apply2)
 template <int NORD, typename T>
-__device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD3) {
+__device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD4) {
   T xp[NORD + 1];
   xp[0] = 1;
 #pragma unroll
@@ -601,16 +617,17 @@ __device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD3)
   }
 #pragma unroll
   for (int t = 0; t < een_nb(NORD); t++) {
-    BD3[3 * t] = B[t];
-    BD3[3 * t + 1] = dB[t];
-    BD3[3 * t + 2] = d2B[t];
+    BD4[4 * t] = B[t];
+    BD4[4 * t + 1] = dB[t];
+    BD4[4 * t + 2] = d2B[t];
+    BD4[4 * t + 3] = T(0);
   }
 }
 
 // all nine value/derivative sums of the e-e-n term (jastrow4.f90 fc, fu,
 // fuu, fi, fii, fj, fjj, fui, fuj) from the folded row coefficients
 template <int NORD, typename T = double>
-__device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD3, T y, T z) {
+__device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD4, T y, T z) {
   T yp[NORD + 1];
   yp[0] = 1;
 #pragma unroll
@@ -623,7 +640,8 @@ __device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD3, T y, 
 #pragma unroll
     for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
       const int t = een_off(NORD, k) + p - een_pmin(k);
-      const T b0 = BD3[3 * t], b1 = BD3[3 * t + 1], b2 = BD3[3 * t + 2];
+      T b0, b1, b2;
+      ld3<T>(BD4 + 4 * t, b0, b1, b2);
       a += b0 * yp[p];
       ax += b1 * yp[p];
       axx += b2 * yp[p];

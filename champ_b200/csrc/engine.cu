@@ -962,7 +962,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   }
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
-    c->smem_jfull = sizeof(double) * (3 * (size_t)h.N + 2 * (size_t)h.M * 8 + 2 * (size_t)h.M * 3 * een_nb(nord));
+    c->smem_jfull = sizeof(double) * (3 * (size_t)h.N + 1 + 2 * (size_t)h.M * 8 + 2 * (size_t)h.M * 4 * een_nb(nord));
   }
   c->smem_sinv = sizeof(double) * ((size_t)nmax * nmax + nmax);
   c->smem_ctil = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64);

@@ -79,7 +79,7 @@ constexpr int kEnFields = 5;
 // float: mixed path); distances, 1/r_ij, the tables and the sums over
 // pairs stay FP64.
 template <int NORD, typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jastrow_full(WState st, HBuf hb) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) k_jastrow_full(WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M, MN = M * N;
@@ -87,8 +87,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jastrow_full(WS
   constexpr int NB = een_nb(NORD);
   extern __shared__ __align__(16) double smem[];
   double *sx = smem;                      // [3][N]
-  double *sI = sx + 3 * N;                // [2][M][8] table entries and e-n vectors of the batch's rows
-  T *sB = reinterpret_cast<T *>(sI + 2 * M * 8);  // [2][M][3*NB] folded rows
+  double *sI = sx + 3 * N + (3 * N & 1);  // [2][M][8] table entries and e-n vectors of the batch's rows
+  T *sB = reinterpret_cast<T *>(sI + 2 * M * 8);  // [2][M][4*NB] folded rows (16-byte aligned)
   __shared__ double red[4];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
   __syncthreads();
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jastrow_full(WS
 #pragma unroll
       for (int f = 0; f < kEnFields; f++) q[f] = tab[f * MN + ic * N + i];
       for (int k = 0; k < 3; k++) q[kEnFields + k] = sx[k * N + i] - cs.cent[3 * ic + k];
-      if (NORD > 1) een_fold2<NORD, T>(een_coef<T>(cs.iwctype[ic]), T(1 - kap * q[0]), sB + (size_t)t * 3 * NB);
+      if (NORD > 1) een_fold2<NORD, T>(een_coef<T>(cs.iwctype[ic]), T(1 - kap * q[0]), sB + (size_t)t * 4 * NB);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < npa + npb; t += blockDim.x) {
@@ -179,17 +179,23 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jastrow_full(WS
       }
       if (NORD > 1) {
         const T z = 1 - kT * u, du1 = -kT * dd1, du2 = -kT * dd2, du1r = du1 * irijT;
-        const T *Brow = sB + (size_t)row * M * 3 * NB;
+        const T *Brow = sB + (size_t)row * M * 4 * NB;
         const double *Irow = sI + (size_t)row * M * 8;
         const double *tj = tab + j;
+        // the partner's table entries of the next centre are loaded one iteration ahead
+        double nr = tj[0], nA = tj[MN], nB = tj[2 * MN], nG = tj[3 * MN], nS = tj[4 * MN];
         for (int ic = 0; ic < M; ic++) {
+          const double rrj = nr;
+          const T Aj = (T)nA, Bj = (T)nB, Gj = (T)nG, Sj = (T)nS;
+          if (ic + 1 < M) {
+            const int o = (ic + 1) * N;
+            nr = tj[o]; nA = tj[MN + o]; nB = tj[2 * MN + o]; nG = tj[3 * MN + o]; nS = tj[4 * MN + o];
+          }
           const double *qi = Irow + ic * 8;
-          const double rri = qi[0], rrj = tj[ic * N];
+          const double rri = qi[0];
           if (rri == asym && rrj == asym) continue;
           const T Ai = (T)qi[1], Bi = (T)qi[2], Gi = (T)qi[3], Si = (T)qi[4];
-          const T Aj = (T)tj[MN + ic * N], Bj = (T)tj[2 * MN + ic * N], Gj = (T)tj[3 * MN + ic * N],
-                  Sj = (T)tj[4 * MN + ic * N];
-          const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 3 * NB, T(1 - kap * rrj), z);
+          const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 4 * NB, T(1 - kap * rrj), z);
           const T dS = Si - Sj;
           const T fuu = e.fuu * du1 * du1 + e.fu * du2;
           const T fu = e.fu * du1r;

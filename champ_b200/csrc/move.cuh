@@ -309,14 +309,14 @@ template <int NORD>
 __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) double smem[];
   constexpr int NB = een_nb(NORD);        // folded coefficients per centre
-  constexpr int PER = 6 + 2 * NB;         // shared doubles per centre
+  constexpr int PER = 8 + 2 * NB;         // shared doubles per centre (one pad keeps B 16-byte aligned)
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int M = cs.M, N = cs.N;
   double *sh = smem + (size_t)wib * M * PER;
-  // per centre ic: rvec(3), r, scaled r, dd1, then B[NB], dB[NB]
-  double *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M, *sh_B = sh + 6 * M;
+  // per centre ic: rvec(3), r, scaled r, dd1, -kappa dd1 / r, then B[NB], dB[NB]
+  double *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M, *sh_g = sh + 6 * M, *sh_B = sh + 8 * M;
   const bool active = (w < st.W);
   int igeo = 1;
   double xi[3] = {0, 0, 0};
@@ -341,6 +341,7 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
     scale2<double>(r, rr, dd1, dd2);
     sh_s[ic] = rr;
     sh_d[ic] = dd1;
+    sh_g[ic] = -kap * dd1 / r;
     mb.enn[((size_t)w * 2 + 0) * M + ic] = rr;
     mb.enn[((size_t)w * 2 + 1) * M + ic] = dd1 / r;
     if (NORD > 1) een_fold<NORD, double>(&cs.c[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sh_B + (size_t)ic * 2 * NB);
@@ -373,7 +374,7 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
     }
     if (NORD > 1) {
       const double z = 1 - kap * u;
-      const double du = -kap * dd1;
+      const double du_r = -kap * dd1 / rij;
       // partner's e-n values from the walker's table (coalesced over lanes)
       const double *en_rr = st.enm + (size_t)w * 2 * M * N + jj;
       const double *en_h = en_rr + (size_t)M * N;
@@ -388,12 +389,10 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
         const double rri = sh_s[ic];
         if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
         const double rj_v[3] = {xj[0] - cs.cent[3 * ic], xj[1] - cs.cent[3 * ic + 1], xj[2] - cs.cent[3 * ic + 2]};
-        const double ri = sh_r[ic];
-        const double dd7 = sh_d[ic];
         double fc, fu_, fi_, fj_;
         een_apply1<NORD>(sh_B + (size_t)ic * 2 * NB, 1 - kap * rrj, z, fc, fu_, fi_, fj_);
-        const double fu = fu_ * du / rij;
-        const double fi = fi_ * (-kap * dd7) / ri;
+        const double fu = fu_ * du_r;
+        const double fi = fi_ * sh_g[ic];
         const double fj = fj_ * (-kap) * hj;
         fs += fc;
         for (int k = 0; k < 3; k++) {
@@ -463,13 +462,13 @@ template <int NORD>
 __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) float smemf[];
   constexpr int NB = een_nb(NORD);
-  constexpr int PER = 6 + 2 * NB;         // shared floats per centre
+  constexpr int PER = 8 + 2 * NB;         // shared floats per centre (one pad keeps B 8-byte aligned)
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int M = cs.M, N = cs.N;
   float *sh = smemf + (size_t)wib * M * PER;
-  float *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M, *sh_B = sh + 6 * M;
+  float *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M, *sh_g = sh + 6 * M, *sh_B = sh + 8 * M;
   const bool active = (w < st.W);
   int igeo = 1;
   double xi[3] = {0, 0, 0};
@@ -495,6 +494,7 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
     scale2<float>(r, rr, dd1, dd2);
     sh_s[ic] = rr;
     sh_d[ic] = dd1;
+    sh_g[ic] = -kap * dd1 / r;
     mb.enn[((size_t)w * 2 + 0) * M + ic] = rr;
     mb.enn[((size_t)w * 2 + 1) * M + ic] = dd1 / r;
     if (NORD > 1) een_fold<NORD, float>(&cs.cf[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sh_B + (size_t)ic * 2 * NB);
@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
         float fc, fu_, fi_, fj_;
         een_apply1f<NORD>(sh_B + (size_t)ic * 2 * NB, 1 - kap * rrj, z, fc, fu_, fi_, fj_);
         const float fu = fu_ * du_r;
-        const float fi = fi_ * (-kap * sh_d[ic]) / sh_r[ic];
+        const float fi = fi_ * sh_g[ic];
         const float fj = fj_ * (-kap) * hj;
         fs += fc;
         for (int k = 0; k < 3; k++) {
