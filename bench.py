@@ -36,7 +36,22 @@ CONFIGS = {
     "c2": ("c2", 16384, "dmc-c2: 12 centres (9 C-like Z=4 with BFD-form ECP, 3 H-like), 40 electrons (20/20), "
                         "300 Gaussians, 80 orbitals, 10^4 determinants (1-4-fold excitations, |c_k|~k^-1.5), "
                         "order-5 Jastrow, 16384 walkers, tau=0.01, branching on"),
+    "c4": ("chain", 0, "serve-c4: seeded Poisson arrivals of VMC energy jobs, each a chain molecule of the "
+                       "batched distribution (8-200 electrons, ~4.5 x electrons Gaussians, C-like Z=4 with ECP "
+                       "and H-like centres), 256-1024 walkers, target error 0.5 mHa within a block budget, "
+                       "admitted against an HBM budget on one GPU"),
 }
+
+
+def jm_traffic(W):
+    """DRAM bytes per k_jastrow_move launch at W walkers, from the committed ncu
+    capture (per-walker traffic: the e-n table and pair rows of each walker)."""
+    p = os.path.join(ROOT, "profiles", "k_jastrow_move_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return (d["dram_bytes_read"] + d["dram_bytes_write"]) * W / d["walkers"]
 
 
 def load_peaks():
@@ -276,6 +291,61 @@ def run_dmc(args):
     return 0
 
 
+def run_serve(args):
+    """Serving loop (config c4): p50/p99 time-to-result of a Poisson stream of jobs."""
+    import torch
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from champ_b200 import serve
+    from champ_b200.system import make_chain
+    _, _, desc = CONFIGS[args.config]
+    njobs = max(16, args.steps)
+    rng = np.random.default_rng(4242 + rank)
+    nel = rng.integers(8, 201, size=njobs)
+    nwk = rng.integers(256, 1025, size=njobs)
+    arrivals = serve.poisson_arrivals(njobs, args.rate, 99 + rank)
+    budget = int(args.budget_gb * (1 << 30))
+
+    def jobs(n, t):
+        return [serve.Job(jid=i, system=make_chain(int(nel[i]), 1000 + i), nwalk=int(nwk[i]), target_err=5e-4,
+                          max_blocks=12, nstep=5, arrival=float(t[i]) if t is not None else 0.0,
+                          seed_offset=int(np.sum(nwk[:i]))) for i in range(n)]
+
+    # warm-up: the module loads and every kernel is compiled into the context once
+    serve.Server(budget, precision=args.precision, device=local).run(jobs(min(args.warmup, 2), None))
+    srv = serve.Server(budget, precision=args.precision, device=local)
+    with ClockSampler(local) as clk:
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        done = srv.run(jobs(njobs, arrivals))
+        torch.cuda.synchronize(local)
+        makespan = time.perf_counter() - t0
+        barrier(pg, local)
+    summ = serve.summary(done, makespan)
+    p50 = max_over_ranks(summ["p50_s"], pg, local)
+    if rank != 0:
+        pg.close()
+        return 0
+    line = {
+        "metric": "job time-to-result p50", "value": p50, "unit": "s", "n_gpus": world, "steps": njobs,
+        "warmup": args.warmup, "ms_per_step": 1e3 * makespan / njobs, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "mixed",
+        "data": "synthetic",
+        "config": {"workload": desc, "jobs": njobs, "rate_per_s": args.rate, "hbm_budget_gb": args.budget_gb,
+                   "precision": args.precision, "block": "5 sweeps", "max_blocks": 12,
+                   "parallelism": f"replicas x{world} (independent job streams)"},
+        "serving": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in summ.items()},
+        "peak_admitted_gb": round(srv.peak_bytes / (1 << 30), 3),
+        "e2e": {"value": p50, "unit": "s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "path": "host job specs -> engine contexts (walkers and streams uploaded) -> block results read back"},
+        "clocks": clk.summary(),
+        "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    pg.close()
+    return 0
+
+
 def run_ours(args):
     import torch
     rank, world, local, pg = dist_setup(args.gpus)
@@ -357,7 +427,9 @@ def run_ours(args):
             "achieved": jm_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
             "frac": (jm_tflops / fp64_peak) if fp64_peak else None,
             "peak_source": "measured FP64 FMA probe (cw_fma_peak) on this GPU",
-            "traffic": None, "share_of_step": ms_jm / total_stage,
+            "traffic": jm_traffic(W) if args.precision == "fp64" else None,
+            "traffic_source": "dram bytes of one ncu capture at 2048 walkers, scaled by the walker count",
+            "share_of_step": ms_jm / total_stage,
             "work_per_launch": "8*(N-1)*M*T + 8*(N-1)*nordb + 8*M*norda FLOP per walker (T=23 e-e-n terms)"}
     # HBM-bound move update: k_decide (ratio, drift, accept) + k_commit
     # (Sherman-Morrison rows, orbital rows, Jastrow pair rows); the
@@ -411,11 +483,18 @@ def main():
     ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
     ap.add_argument("--walkers", type=int, default=0)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--rate", type=float, default=4.0, help="c4: job arrivals per second")
+    ap.add_argument("--budget-gb", type=float, default=16.0, help="c4: HBM budget of the admitted jobs")
     args = ap.parse_args()
     if args.impl == "reference":
+        if args.config == "c4":
+            print(json.dumps({"impl": "reference", "unavailable": "CHAMP has no request loop (one job per run)"}))
+            return 0
         return run_reference(args)
     if args.config == "c2":
         return run_dmc(args)
+    if args.config == "c4":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -104,6 +104,8 @@ def load_engine(path: str | None = None):
     lib.cw_last_ms.restype = C.c_double
     lib.cw_launches.argtypes = [V]
     lib.cw_launches.restype = C.c_long
+    lib.cw_device_bytes.argtypes = [V]
+    lib.cw_device_bytes.restype = C.c_size_t
     lib.cw_profile.argtypes = [V, C.c_int]
     lib.cw_profile.restype = C.c_int
     lib.cw_stage_times.argtypes = [V, _dp, C.POINTER(C.c_long)]
@@ -143,6 +145,7 @@ EXPORTED_SYMBOLS = [
     "cw_launches", "cw_profile", "cw_stage_times", "cw_fma_peak", "cw_orbitals_noalloc",
     "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
     "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore", "cw_dmc_set_tmoves", "cw_dmc_counts",
+    "cw_device_bytes",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

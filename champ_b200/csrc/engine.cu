@@ -8,6 +8,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <map>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -63,6 +66,8 @@ struct cw_ctx {
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
   int ecp_warps = 1, ecp_naov = 0;
+  size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
+  std::unordered_map<void *, size_t> alloc_bytes;
   double *bocc = nullptr;  // [nmax][K] coefficients of the occupied orbitals (c~ GEMM)
   int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
@@ -134,6 +139,8 @@ int dalloc(cw_ctx *c, std::vector<void *> &list, T **p, size_t n) {
   if (e != cudaSuccess)
     return fail(c, CW_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
   list.push_back(q);
+  c->dev_bytes += std::max<size_t>(n, 1) * sizeof(T);
+  c->alloc_bytes[q] = std::max<size_t>(n, 1) * sizeof(T);
   *p = (T *)q;
   return CW_OK;
 }
@@ -144,9 +151,31 @@ int dalloc(cw_ctx *c, std::vector<void *> &list, T **p, size_t n) {
     if (rc_) return rc_;                           \
   } while (0)
 
-void free_list(std::vector<void *> &l) {
-  for (void *p : l) cudaFree(p);
+void free_list(cw_ctx *c, std::vector<void *> &l) {
+  for (void *p : l) {
+    cudaFree(p);
+    auto it = c->alloc_bytes.find(p);
+    if (it != c->alloc_bytes.end()) {
+      c->dev_bytes -= it->second;
+      c->alloc_bytes.erase(it);
+    }
+  }
   l.clear();
+}
+
+// The dynamic shared-memory limit of a kernel is a property of the function
+// on the device, shared by every context of the process; contexts of
+// different systems need different sizes, so the limit only ever grows.
+std::mutex g_smem_mu;
+std::map<std::pair<int, const void *>, size_t> g_smem_max;
+template <typename F>
+cudaError_t raise_smem(const cw_ctx *c, F *func, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_smem_mu);
+  size_t &cur = g_smem_max[{c->device, (const void *)func}];
+  if (bytes <= cur) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
 }
 
 // Bracket a launch with CUDA events when profiling; count it either way.
@@ -248,13 +277,10 @@ void launch_ecp(cw_ctx *c) {
 }
 template <int NORD>
 int set_attrs(cw_ctx *c) {
-  CK(cudaFuncSetAttribute(k_jastrow_move<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_jmove));
-  CK(cudaFuncSetAttribute(k_jastrow_move_f32<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)c->smem_jmove_f32));
-  CK(cudaFuncSetAttribute(k_jastrow_full<NORD, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)c->smem_jfull));
-  CK(cudaFuncSetAttribute(k_jastrow_full<NORD, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)c->smem_jfull));
+  CK(raise_smem(c, k_jastrow_move<NORD>, (size_t)(c->smem_jmove)));
+  CK(raise_smem(c, k_jastrow_move_f32<NORD>, (size_t)(c->smem_jmove_f32)));
+  CK(raise_smem(c, k_jastrow_full<NORD, double>, c->smem_jfull));
+  CK(raise_smem(c, k_jastrow_full<NORD, float>, c->smem_jfull));
   if (c->h.nloc > 0) {
     // warps per ECP block: the most resident warps per SM under the shared
     // memory (228 KB), register (64 K) and warp (64) limits; ties go to the
@@ -279,8 +305,8 @@ int set_attrs(cw_ctx *c) {
       }
     }
     if (best == 0) return fail(c, CW_ERR_UNSUPPORTED, "ECP stage shared memory too large");
-    CK(cudaFuncSetAttribute(k_ecp<NORD, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
-    CK(cudaFuncSetAttribute(k_ecp<NORD, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ecp));
+    CK(raise_smem(c, k_ecp<NORD, double>, c->smem_ecp));
+    CK(raise_smem(c, k_ecp<NORD, float>, c->smem_ecp));
   }
   return CW_OK;
 }
@@ -604,7 +630,7 @@ int check_status(cw_ctx *c) {
 
 void free_dmc(cw_ctx *c) {
   DmcHost &d = c->dmc;
-  free_list(d.allocs);
+  free_list(c, d.allocs);
   for (void *p : {(void *)d.h_acc, (void *)d.h_wt, (void *)d.h_iage, (void *)d.h_copy})
     if (p) cudaFreeHost(p);
   d = DmcHost();
@@ -612,7 +638,7 @@ void free_dmc(cw_ctx *c) {
 
 int alloc_walkers(cw_ctx *c, int W) {
   free_dmc(c);
-  free_list(c->w_allocs);
+  free_list(c, c->w_allocs);
   const CSys &h = c->h;
   const int N = h.N, M = h.M, K = h.K, Oa = h.Oa, nmax = h.nmax, NQ = std::max(h.nquad, 1);
   auto &L = c->w_allocs;
@@ -972,11 +998,11 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   // warp-per-point basis kernels: as many warps per block as 4 records fit
   c->basis_warps = (int)std::max<size_t>(1, std::min<size_t>(4, (160 * 1024) / ((size_t)h.M * kCenRec * sizeof(double))));
   c->smem_basis = (size_t)c->basis_warps * h.M * kCenRec * sizeof(double);
-  CK(cudaFuncSetAttribute(k_basis_move, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_basis));
-  CK(cudaFuncSetAttribute(k_basis_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_basis));
-  CK(cudaFuncSetAttribute(k_slater_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_sinv));
-  CK(cudaFuncSetAttribute(k_ctilde, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ctil));
-  CK(cudaFuncSetAttribute(k_dgemm_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMmaSmem));
+  CK(raise_smem(c, k_basis_move, (size_t)(c->smem_basis)));
+  CK(raise_smem(c, k_basis_all, (size_t)(c->smem_basis)));
+  CK(raise_smem(c, k_slater_inv, (size_t)(c->smem_sinv)));
+  CK(raise_smem(c, k_ctilde, (size_t)(c->smem_ctil)));
+  CK(raise_smem(c, k_dgemm_mma, (size_t)(kMmaSmem)));
   c->mixed = precision == CW_PREC_MIXED;
   c->ecp_naov = d->ndet > 1 ? h.K : 0;  // the ECP stage keeps the point's basis values for the B matrix
   int rc = nord_attrs(c);
@@ -1016,10 +1042,10 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     if (c->smem_md_hpsi > lim || c->smem_md_move > lim)
       return fail(c, CW_ERR_UNSUPPORTED, "multideterminant tables exceed shared memory (nmax %d, norb %d, %d unique)",
                   nmax, h.Oa, numax);
-    CK(cudaFuncSetAttribute(k_md_hpsi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_hpsi));
-    CK(cudaFuncSetAttribute(k_md_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_phase));
-    CK(cudaFuncSetAttribute(k_md_move, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_move));
-    CK(cudaFuncSetAttribute(k_md_drift_old, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_md_drift));
+    CK(raise_smem(c, k_md_hpsi, (size_t)(c->smem_md_hpsi)));
+    CK(raise_smem(c, k_md_phase, (size_t)(c->smem_md_phase)));
+    CK(raise_smem(c, k_md_move, (size_t)(c->smem_md_move)));
+    CK(raise_smem(c, k_md_drift_old, (size_t)(c->smem_md_drift)));
   }
   if (precision == CW_PREC_MIXED) {
     // tensor-core LCAO: coefficients split once into TF32 hi/lo, [Oa][kp]
@@ -1029,7 +1055,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     if (c->np > 256) return fail(c, CW_ERR_UNSUPPORTED, "mixed precision: more than 256 orbitals");
     c->umma_st = umma_stages(c->np);
     c->smem_umma = umma_smem_bytes(c->np);
-    CK(cudaFuncSetAttribute(k_lcao_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_umma));
+    CK(raise_smem(c, k_lcao_tf32x3, (size_t)(c->smem_umma)));
     double *cA;
     DALLOC(L, cA, (size_t)h.Oa * h.K);
     CK(cudaMemcpy(cA, d->coef, sizeof(double) * (size_t)h.Oa * h.K, cudaMemcpyHostToDevice));
@@ -1053,8 +1079,8 @@ void cw_destroy(cw_ctx *c) {
   if (g_const_owner[c->device & 63] == c) g_const_owner[c->device & 63] = nullptr;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_dmc(c);
-  free_list(c->w_allocs);
-  free_list(c->sys_allocs);
+  free_list(c, c->w_allocs);
+  free_list(c, c->sys_allocs);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -1063,6 +1089,7 @@ void cw_destroy(cw_ctx *c) {
 }
 
 const char *cw_last_error(const cw_ctx *c) { return c ? c->err.c_str() : "null context"; }
+size_t cw_device_bytes(const cw_ctx *c) { return c ? c->dev_bytes : 0; }
 
 int cw_sync(cw_ctx *c) {
   if (!c) return CW_ERR_ARG;

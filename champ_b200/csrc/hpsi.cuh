@@ -529,14 +529,15 @@ __device__ __forceinline__ double psibnl_d(double u, int isb, int ipar, double s
 }
 
 // Shared-memory plan of k_ecp (in doubles, every region 16-byte aligned):
-//   rr_en [N][M] scaled e-n distances, sx [3][N], the pair list (channel
+//   rr_en [N][M|1] scaled e-n distances (odd row stride: lanes over the
+//   electrons read them without bank conflicts), sx [3][N], the pair list (channel
 //   potentials [cap][3], packed i*M+ic [cap] ints), then per warp: the
 //   point's scaled e-n distances [M], its folded e-e-n coefficients [M][NB],
 //   its basis prepass [M][kCenRec] and, for multideterminant wave functions,
 //   its basis values [K] (reused by the pseudopotential B matrix).
 constexpr int kEcpMaxWarps = 16;
 __host__ __device__ inline size_t ecp_base_doubles(int N, int M, int cap) {
-  const size_t b = (size_t)N * M + 3 * (size_t)N + 3 * (size_t)cap + (size_t)(cap + 1) / 2;
+  const size_t b = (size_t)N * (M | 1) + 3 * (size_t)N + 3 * (size_t)cap + (size_t)(cap + 1) / 2;
   return b + (b & 1);
 }
 __host__ __device__ inline size_t ecp_warp_doubles(int M, int nb, int tbytes, int naov) {
@@ -565,8 +566,9 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps) k_ecp(WState st, HBuf hb, G
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5, cap = blockDim.x;
   constexpr int NB = 2 * ((een_nb(NORD) + 1) / 2);
   extern __shared__ __align__(16) double smem[];
-  double *rr_en = smem;                         // [N][M]
-  double *sx = rr_en + NM;                      // [3][N]
+  const int MS = M | 1;                         // row stride of rr_en
+  double *rr_en = smem;                         // [N][MS]
+  double *sx = rr_en + (size_t)N * MS;          // [3][N]
   double *lst_v = sx + 3 * N;                   // [cap][3] non-local channel potentials
   int *lst_ie = reinterpret_cast<int *>(lst_v + 3 * cap);  // [cap] i*M + ic
   const int naov = hb.md_P ? K : 0;
@@ -585,7 +587,7 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps) k_ecp(WState st, HBuf hb, G
   for (int t = threadIdx.x; t < NM; t += blockDim.x) {
     const int jj = t / M, jc = t % M;
     const double d0 = sx[jj] - cs.cent[3 * jc], d1 = sx[N + jj] - cs.cent[3 * jc + 1], d2 = sx[2 * N + jj] - cs.cent[3 * jc + 2];
-    rr_en[t] = scale0<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+    rr_en[jj * MS + jc] = scale0<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2));
   }
   const double *xqw = st.xq + (size_t)w * 3 * NQ;
   const double *fso = st.fso + (size_t)w * N * N;
@@ -682,7 +684,7 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps) k_ecp(WState st, HBuf hb, G
           // psinl (vmc/nonlpsi.f90:4) through the folded coefficients of the point
           const T kT = (T)cs.scalek, z = 1 - kT * u;
           for (int jc = 0; jc < M; jc++) {
-            const double rrj = rr_en[jj * M + jc];
+            const double rrj = rr_en[jj * MS + jc];
             if (rq[jc] == cs.asymp_r && rrj == cs.asymp_r) continue;
             if constexpr (sizeof(T) == 8)
               f += een_apply0<NORD>((const double *)(bq + (size_t)jc * NB), 1 - cs.scalek * rrj, (double)z);

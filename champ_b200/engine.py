@@ -116,6 +116,10 @@ class Engine:
     def launches(self) -> int:
         return int(self.lib.cw_launches(self.h))
 
+    def device_bytes(self) -> int:
+        """Bytes of device memory the context holds (tables, walkers, scratch)."""
+        return int(self.lib.cw_device_bytes(self.h))
+
     def profile(self, enable: bool = True):
         self._check(self.lib.cw_profile(self.h, 1 if enable else 0), "cw_profile")
 

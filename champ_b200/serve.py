@@ -1,0 +1,191 @@
+"""Request loop for VMC energy jobs on one GPU (continuous admission).
+
+A job is a system, a walker count, a target error bar and a block budget.
+Jobs arrive over time.  A job is admitted as soon as its device-memory
+estimate fits into what the HBM budget has left, first come first served (a
+job never overtakes an earlier one that does not fit yet).  From then on it
+keeps its engine context -- walker population, Slater inverses, Jastrow
+tables, accumulators -- resident on the device until it finishes.  The loop
+advances the admitted jobs one block at a time, round-robin (a block is
+``nstep`` sweeps followed by the block average, CHAMP's acuest), and admits
+newly arrived jobs between blocks.  A job finishes when its error bar reaches
+the target (after at least two blocks) or its block budget is spent; its
+context is then released and the jobs waiting for memory are admitted.
+
+Time-to-result of a job = completion time - arrival time.  Each job draws
+its walkers' streams from its own range (``seed_offset``), so a job's
+result does not depend on which other jobs share the device.
+
+The contexts of different molecules share the device's constant system
+block, so their kernels run one context at a time (the engine serialises
+them on the device); jobs overlap at block granularity, not inside a kernel.
+CHAMP itself has no request loop (one job per MPI run); this module is the
+serving layer the engine's C ABI is designed for.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import math
+import time
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Job:
+    jid: int
+    system: object
+    nwalk: int
+    target_err: float
+    max_blocks: int
+    nstep: int = 10
+    arrival: float = 0.0        # seconds after the loop starts
+    seed_offset: int = 0        # first random stream of the job's walkers
+    # filled in by the server
+    est_bytes: int = 0
+    device_bytes: int = 0
+    admitted: float = math.nan
+    done: float = math.nan
+    energy: float = math.nan
+    err: float = math.nan
+    blocks: int = 0
+    moves: int = 0
+    reached: bool = False
+    failed: str = ""
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def estimate_bytes(system, nwalk: int, precision: str = "fp64", chunk_bytes: int = 1 << 30) -> int:
+    """Device bytes a context of `system` with `nwalk` walkers allocates: the
+    walker state, move and local-energy scratch of the engine (the same
+    arrays, one value per element), plus the system tables (radial grids,
+    coefficients), with a 10% margin.  An upper bound of cw_device_bytes for
+    single-determinant jobs."""
+    N, M, K, O = system.nelec, system.ncent, system.nbasis, system.norb
+    nmax = max(system.nup, system.ndn)
+    NQ = max(int(getattr(system, "nquad", 0) or 0), 1)
+    W = nwalk
+    d = 8
+    walker = (3 * N + 4 + 3 * NQ + N + N + 3 * N + 5 + 2 * nmax * nmax + 2 + N * nmax + 3 * N * nmax
+              + N * N + 3 * N * N + 3 * N + 1 + 2 * M * N + 8 + 1)
+    move = 64 + N + 3 * N + 3 * N + 1 + 3 + 4 * K + 4 * O + 2 * M
+    hpsi = 1 + 1 + 1 + 2 + 4 * N + N * nmax + 5 * M * N
+    if getattr(system, "nloc", 0):
+        hpsi += N * K
+    per_e = W * 5 * (K + O) * d
+    chunk = min(max(1, chunk_bytes // max(per_e, 1)), N)
+    scratch = W * chunk * 5 * (K + O)
+    total = d * (W * (walker + move + hpsi) + scratch)
+    if precision == "mixed":
+        kp = (K + 31) // 32 * 32
+        total += 4 * (2 * W * 4 * kp + 2 * W * chunk * 5 * kp) + 8 * O * kp
+    rwf = np.asarray(system.rwf)
+    tables = 8 * (2 * rwf.size + rwf.shape[0] * (rwf.shape[-1] + 1) + K * O * 3 + nmax * K) + (1 << 20)
+    return int(1.10 * (total + tables))
+
+
+def _engine_for(job: Job, precision: str, device: int):
+    from .engine import Engine, initial_configs, rng_states
+    eng = Engine(job.system, device=device, precision=precision)
+    rng = rng_states(job.seed_offset + job.nwalk)[job.seed_offset:].copy()
+    x = initial_configs(job.system, rng)
+    eng.set_walkers(x, rng)
+    return eng
+
+
+class Server:
+    """One GPU, one HBM budget; `run` serves a list of jobs with arrival times."""
+
+    def __init__(self, budget_bytes: int, precision: str = "fp64", device: int = 0, engine_factory=None,
+                 clock=time.perf_counter, sleep=time.sleep):
+        self.budget = int(budget_bytes)
+        self.precision = precision
+        self.device = device
+        self.factory = engine_factory or (lambda job: _engine_for(job, precision, device))
+        self.clock = clock
+        self.sleep = sleep
+        self.peak_bytes = 0          # largest sum of admitted estimates
+        self.timeline = []           # (time, event, job id)
+
+    def run(self, jobs):
+        jobs = sorted(jobs, key=lambda j: (j.arrival, j.jid))
+        for j in jobs:
+            j.est_bytes = estimate_bytes(j.system, j.nwalk, self.precision)
+        pending = collections.deque(jobs)
+        waiting = collections.deque()
+        active = collections.deque()   # (job, engine) in round-robin order
+        used = 0
+        t0 = self.clock()
+
+        def now():
+            return self.clock() - t0
+
+        def arrive_and_admit():
+            nonlocal used
+            t = now()
+            while pending and pending[0].arrival <= t:
+                j = pending.popleft()
+                waiting.append(j)
+                self.timeline.append((t, "arrive", j.jid))
+            while waiting:
+                j = waiting[0]
+                if j.est_bytes > self.budget:      # can never fit: refuse, do not block the queue
+                    waiting.popleft()
+                    j.failed = f"needs {j.est_bytes} bytes, budget {self.budget}"
+                    j.done = now()
+                    self.timeline.append((j.done, "refuse", j.jid))
+                    continue
+                if used + j.est_bytes > self.budget:
+                    break
+                waiting.popleft()
+                eng = self.factory(j)
+                j.device_bytes = int(eng.device_bytes())
+                used += j.est_bytes
+                self.peak_bytes = max(self.peak_bytes, used)
+                j.admitted = now()
+                self.timeline.append((j.admitted, "admit", j.jid))
+                active.append((j, eng))
+
+        while pending or waiting or active:
+            arrive_and_admit()
+            if not active:
+                if pending:
+                    self.sleep(max(0.0, pending[0].arrival - now()))
+                continue
+            j, eng = active.popleft()
+            eng.vmc_steps(j.nstep)
+            eng.end_block()
+            r = eng.results()
+            j.blocks += 1
+            j.moves += j.nstep * j.nwalk * j.system.nelec
+            j.energy, j.err = float(r["energy"]), float(r["err"])
+            j.reached = j.blocks >= 2 and j.err <= j.target_err
+            if j.reached or j.blocks >= j.max_blocks:
+                j.done = now()
+                self.timeline.append((j.done, "done", j.jid))
+                eng.close()
+                used -= j.est_bytes
+            else:
+                active.append((j, eng))
+        return jobs
+
+
+def poisson_arrivals(n: int, rate: float, seed: int) -> np.ndarray:
+    """Arrival times (s) of n jobs of a Poisson stream with `rate` jobs/s."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def summary(jobs, makespan: float) -> dict:
+    """p50/p99 time-to-result of the finished jobs and aggregate throughput."""
+    ok = [j for j in jobs if not j.failed]
+    lat = np.array([j.latency for j in ok]) if ok else np.zeros(1)
+    moves = sum(j.moves for j in ok)
+    return dict(p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)),
+                mean_s=float(lat.mean()), jobs=len(jobs), finished=len(ok),
+                reached_target=sum(1 for j in ok if j.reached), refused=len(jobs) - len(ok),
+                moves_per_s=moves / makespan if makespan > 0 else 0.0, makespan_s=makespan)

@@ -575,6 +575,27 @@ def make_synthetic(config: str, seed: int = 20261203) -> System:
     raise ValueError(f"unknown synthetic config {config!r}")
 
 
+def make_chain(nelec: int, seed: int) -> System:
+    """Seeded chain molecule of the batched / serving job distribution: about
+    nelec/4 centres alternating C-like (Z=4, ECP, s/p/d basis) and H-like
+    (Z=1, s/p) as in c1, nelec electrons (ceil/floor halves), one occupied
+    orbital per up electron, basis about 4.5 x nelec Gaussians."""
+    if nelec < 2:
+        raise ValueError("a chain job needs at least 2 electrons")
+    rng = np.random.default_rng(seed)
+    nat = max(2, int(round(nelec / 4)))
+    cent = np.zeros((nat, 3))
+    for i in range(nat):
+        cent[i] = (1.30 * i + rng.normal(0, 0.05), 0.75 * (i % 2) + rng.normal(0, 0.05), rng.normal(0, 0.05))
+    heavy = dict(z=4.0, lpot=2, a1=0.0,
+                 basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 1)]), 4.0, 4))
+    hyd = dict(z=1.0, lpot=1, a1=-1.0,
+               basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 4)]), 1.0, 4))
+    types = [0 if i % 2 == 0 else 1 for i in range(nat)]
+    nup, ndn = (nelec + 1) // 2, nelec // 2
+    return _assemble(f"chain{nelec}", rng, cent, types, [heavy, hyd], nelec, nup, nup, nup, ndn)
+
+
 def ci_expansion(rng, nup, ndn, norb, ndet, pools=(150, 500, 300, 120), nact_occ=8, nact_virt=30,
                  level_p=(0.1, 0.45, 0.3, 0.15)):
     """Seeded CI expansion of single to quadruple excitations of the aufbau

@@ -188,6 +188,11 @@ double cw_last_ms(const cw_ctx *ctx);
 /* Kernel launches issued by the last cw_vmc_steps call. */
 long cw_launches(const cw_ctx *ctx);
 
+/* Device memory the context holds (bytes of its own allocations: system
+ * tables, walker state, scratch).  A serving loop admits jobs against an HBM
+ * budget with it; no reference counterpart (CHAMP runs one job per process). */
+size_t cw_device_bytes(const cw_ctx *ctx);
+
 /* Per-stage device timing.  enable=1 brackets every launch of the following
  * cw_vmc_steps calls with CUDA events on the engine stream (adds event
  * overhead; leave off for throughput runs).  cw_stage_times fills, for each
