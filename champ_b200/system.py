@@ -314,7 +314,16 @@ class System:
     deltar: float = 5.0
     deltat: float = 1.0
     fbias: float = 1.0
+    # several states sharing orbitals and Jastrow: [nstates][ndet] CI vectors
+    # (row 0 = cdet), guiding flag and weights
+    cdet_states: np.ndarray | None = None
+    iguiding: int = 0
+    weights_g: np.ndarray | None = None
     _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def nstates(self):
+        return 1 if self.cdet_states is None else int(np.asarray(self.cdet_states).shape[0])
 
     @property
     def ncent(self):
@@ -370,7 +379,18 @@ class System:
         d.nbasis, d.norb = self.nbasis, self.norb
         d.coef = D(self.coef)
         d.ndet = len(self.cdet)
-        d.iworbd, d.cdet = I(self.iworbd), D(self.cdet)
+        d.iworbd = I(self.iworbd)
+        cst = getattr(self, "cdet_states", None)
+        if cst is not None and len(cst) > 1:
+            cst = np.asarray(cst, float)
+            if cst.shape[1] != d.ndet or not np.array_equal(cst[0], np.asarray(self.cdet, float)):
+                raise ValueError("cdet_states must be [nstates][ndet] with state 1 equal to cdet")
+            d.cdet, d.nstates = D(cst), cst.shape[0]
+            d.iguiding = int(getattr(self, "iguiding", 0))
+            wg = getattr(self, "weights_g", None)
+            d.weights_g = D(wg if wg is not None else np.ones(cst.shape[0]))
+        else:
+            d.cdet, d.nstates = D(self.cdet), 1
         d.norda, d.nordb, d.nordc = self.norda, self.nordb, self.nordc
         d.isc, d.nspin2b, d.nocuspb = self.isc, self.nspin2b, self.nocuspb
         d.scalek = self.scalek

@@ -15,6 +15,7 @@
 #ifndef CHAMP_B200_H
 #define CHAMP_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -107,6 +108,15 @@ typedef struct cw_system_desc {
 
   /* --- metropolis (parser.f90:398-404) --- */
   double deltar, deltat, fbias;
+
+  /* --- several states sharing orbitals and Jastrow (csfs nstates,
+   *     mstates_ctrl iguiding, mstates3 weights_g; vmc/determinante.f90:134-230,
+   *     vmc/determinant_psig.f90:3).  nstates 0 or 1: one state; > 1 (VMC
+   *     only): cdet holds [nstates][ndet], the walk samples |psi_1|^2 and
+   *     state s is weighted by (psi_s/psi_1)^2 (iguiding = 0). --- */
+  int32_t nstates;
+  int32_t iguiding;            /* > 0 (guiding function) is refused: CW_ERR_UNSUPPORTED */
+  const double *weights_g;     /* [nstates] guiding weights (read only when iguiding > 0) */
 } cw_system_desc;
 
 typedef struct cw_ctx cw_ctx;
@@ -152,6 +162,17 @@ int cw_end_block(cw_ctx *ctx, double *block_energy);
  * out[2]=sigma, out[3]=Tcor, out[4]=acceptance, out[5]=PE, out[6]=KE,
  * out[7]=blocks so far (iblk). */
 int cw_results(cw_ctx *ctx, double *out);
+
+/* Results of state `istate` (0-based) of a multi-state wave function, from
+ * the reweighted block sums of that state (acuest / finwrt per istate):
+ * out[0] energy, out[1] its error, out[5] potential, out[6] kinetic energy,
+ * out[7] blocks; out[2..4] are NaN (sigma, Tcorr and acceptance are those of
+ * the sampled state, cw_results).  CW_ERR_ARG for istate outside [0, nstates). */
+int cw_results_state(cw_ctx *ctx, int istate, double *out);
+
+/* Per-walker local energies and psi_D of every state from the last hpsi:
+ * energy, psid [nwalk][nstates]. */
+int cw_state_energies(cw_ctx *ctx, double *energy, double *psid);
 
 /* Local energy of every walker at its current configuration, hpsi
  * (vmc/hpsi.f90:3) with the quadrature grid (xq,yq,zq)[nquad] given (NULL:

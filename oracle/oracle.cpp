@@ -67,6 +67,8 @@ struct Sys {
   vector<int> nbastyp, iwlbas, iwrwf;
   int K, O, ndet;
   vector<double> coef, cdet;   // cdet: sign-adjusted by multideterminants_define
+  int nstates = 1;             // CI vectors sharing orbitals and Jastrow (csfs nstates)
+  vector<double> cdet_st;      // [nstates][ndet], sign-adjusted like cdet; row 0 = cdet
   vector<int> iworbd;  // iworbd(j) for kref=1, 1-based orbital
   vector<int> iworbd_all;      // [ndet][N] 1-based, reordered as multideterminants_define does
   // compact multideterminant tables per spin (multideterminants_define,
@@ -168,7 +170,10 @@ bool multideterminants_define(Sys &s) {
       }
       itot[k] += iphase;
     }
-    if (itot[k] % 2) s.cdet[k] = -s.cdet[k];
+    if (itot[k] % 2) {
+      s.cdet[k] = -s.cdet[k];
+      for (int st = 0; st < s.nstates; st++) s.cdet_st[(size_t)st * nd + k] = -s.cdet_st[(size_t)st * nd + k];
+    }
   }
   for (int k = 1; k < nd; k++) {
     for (int i = 0; i < N; i++) IW(k, i) = IW(0, i);
@@ -534,6 +539,8 @@ struct Walker {
   vector<double> tvpsp;  // t_vpsp(ic,iq,i) [(i*nquad + iq)*M + ic] of the last hpsi (T-moves)
   // estimators (estsum, forcewt, est*)
   double esum, wsum, pesum, tpbsum, acc, esum1;
+  // several states: energies and psi_D of the last hpsi, block sums per state
+  vector<double> e_st, ekin_st, psid_st, wsum_st, esum_st, pesum_st, tpbsum_st;
   double ecum, ecm2, wcum, pecum, tpbcum, pecm2, tpbcm2, ecum1, ecm21, ecum1s, ecm21s;
   Rng rng;
   bool singular = false;
@@ -588,6 +595,8 @@ struct Walker {
   }
   void zero_estimators() {
     esum = wsum = pesum = tpbsum = acc = esum1 = 0;
+    for (auto *v : {&wsum_st, &esum_st, &pesum_st, &tpbsum_st}) v->assign(s->nstates, 0.0);
+    for (auto *v : {&e_st, &ekin_st, &psid_st}) v->resize(s->nstates, 0.0);
     ecum = ecm2 = wcum = pecum = tpbcum = pecm2 = tpbcm2 = ecum1 = ecm21 = ecum1s = ecm21s = 0;
   }
 
@@ -1159,7 +1168,9 @@ struct Walker {
     for (size_t t = 0; t < m.kdet2.size(); t++) dall[m.kdet2[t]] = dall[m.kdet2[t]] * dd[m.kaux2[t]];
   }
   // compute_ymat (vmc/multideterminant.f90:258)
-  void compute_ymat(int iab, const double *du, const double *dd_, const double *wf, double *y) const {
+  void compute_ymat(int iab, const double *du, const double *dd_, const double *wf, double *y,
+                    const double *cd = nullptr) const {
+    if (!cd) cd = s->cdet.data();
     const Sys::MdSpin &m = s->md[iab];
     const int nel = nel_of(iab);
     const double detrefi = 1.0 / (du[0] * dd_[0]);
@@ -1167,7 +1178,7 @@ struct Walker {
     vector<double> ceq(std::max(m.nuniq, 1), 0.0);
     for (size_t t = 0; t < m.kdet2.size(); t++) {
       const int k = m.kdet2[t], kw = m.kaux2[t];
-      const double detall_k = detrefi * du[k] * dd_[k] * s->cdet[k];
+      const double detall_k = detrefi * du[k] * dd_[k] * cd[k];
       ceq[kw] = ceq[kw] + detall_k;
     }
     for (int kk = 0; kk < m.nuniq; kk++) {
@@ -1588,8 +1599,38 @@ struct Walker {
     }
     denergy = denergy * detiab[0] * detiab[1] / psid;
     dekin = dekin * detiab[0] * detiab[1] / psid;
+    // further states (determinante.f90:134-230 with nstates > 1): the same
+    // excitation ratios and tildem, each state's own Y and psi_D
+    psid_st[0] = psid;
+    den_st[0] = denergy;
+    dek_st[0] = dekin;
+    for (int st = 1; st < s->nstates; st++) {
+      const double *cd = s->cdet_st.data() + (size_t)st * s->ndet;
+      vector<double> ys[2];
+      for (int iab = 0; iab < 2; iab++) {
+        ys[iab].assign((size_t)O * std::max(nel_of(iab), 1), 0.0);
+        if (nel_of(iab) > 0)
+          compute_ymat(iab, detall[0].data(), detall[1].data(), wfmat[iab].data(), ys[iab].data(), cd);
+      }
+      double ps = 0.0;
+      for (int k = 0; k < s->ndet; k++) ps = ps + detall[0][k] * detall[1][k] * cd[k];
+      double de = 0, dk = 0;
+      for (int iab = 0; iab < 2; iab++) {
+        const int nel = nel_of(iab);
+        const Sys::MdSpin &m = s->md[iab];
+        for (int jrep = m.ivirt; jrep < O; jrep++)
+          for (int irep = m.iactv; irep < nel; irep++) {
+            de = de + ys[iab][jrep + (size_t)O * irep] * tild[iab][irep + (size_t)nel * jrep];
+            dk = dk + ys[iab][jrep + (size_t)O * irep] * tildk[iab][irep + (size_t)nel * jrep];
+          }
+      }
+      psid_st[st] = ps;
+      den_st[st] = de * detiab[0] * detiab[1] / ps;
+      dek_st[st] = dk * detiab[0] * detiab[1] / ps;
+    }
     return true;
   }
+  vector<double> den_st = vector<double>(1), dek_st = vector<double>(1);
 
   // ---- hpsi (vmc/hpsi.f90:3), single det; returns false if singular ----
   bool hpsi(const double *coord, double &psid, double &psij, double &ekin, double &energy,
@@ -1635,10 +1676,21 @@ struct Walker {
     if (s->ndet == 1) {
       psid = detiab[0] * detiab[1] * s->cdet[0];
     } else {
+      den_st.resize(s->nstates);
+      dek_st.resize(s->nstates);
+      psid_st.resize(s->nstates);
       if (!multideterminant_hpsi(psid, denergy, dekin)) return false;
     }
     energy = denergy + eloc_det[0] + eloc_det[1] + e_other;
     ekin = dekin + ekin_det[0] + ekin_det[1] + ekin_other;
+    if (s->nstates > 1) {
+      e_st.resize(s->nstates);
+      ekin_st.resize(s->nstates);
+      for (int st = 0; st < s->nstates; st++) {
+        e_st[st] = den_st[st] + eloc_det[0] + eloc_det[1] + e_other;
+        ekin_st[st] = dek_st[st] + ekin_det[0] + ekin_det[1] + ekin_other;
+      }
+    }
     if (extra) {
       extra[0] = pe;
       extra[1] = vpsp[0] + vpsp[1];
@@ -1997,6 +2049,15 @@ bool Walker::metrop6() {
   ecm21 += esum1 * esum1 * wtg;
   ecum1s += eold * wtg;
   ecm21s += eold * eold * wtg;
+  // every state, reweighted to the sampled |psi_1|^2 (metrop6 :678-690, psi2g = 1)
+  for (int st = 0; s->nstates > 1 && st < s->nstates; st++) {
+    const double ws = psid_st[st] / psid_st[0] * std::exp(psijo - psijo) / std::sqrt(1.0);
+    const double wt = ws * ws;
+    wsum_st[st] += wt;
+    esum_st[st] += e_st[st] * wt;
+    pesum_st[st] += (e_st[st] - ekin_st[st]) * wt;
+    tpbsum_st[st] += ekin_st[st] * wt;
+  }
   return true;
 }
 
@@ -2006,6 +2067,7 @@ struct Walkers {
   // global (rank-0) cumulative estimators after acuest_reduce
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
   double ecum1 = 0, ecm21 = 0, ecum1s = 0, ecm21s = 0;
+  vector<double> wcum_st, ecum_st, ecm2_st, pecum_st, tpbcum_st;  // per state (acuest per istate)
   long iblk = 0, passes = 0;
   int nstep_last = 0;
   bool failed = false;
@@ -2405,6 +2467,12 @@ void *or_sys_create(const cw_system_desc *d) {
   s->K = d->nbasis; s->O = d->norb; s->ndet = d->ndet;
   s->coef.assign(d->coef, d->coef + (size_t)d->nbasis * d->norb);
   s->cdet.assign(d->cdet, d->cdet + d->ndet);
+  s->nstates = d->nstates > 1 ? d->nstates : 1;
+  s->cdet_st.assign(d->cdet, d->cdet + (size_t)s->nstates * d->ndet);
+  if (s->nstates > 1 && (d->iguiding > 0 || d->ndet < 2)) {
+    delete s;
+    return nullptr;
+  }
   s->iworbd.assign(d->iworbd, d->iworbd + d->nelec);
   s->iworbd_all.assign(d->iworbd, d->iworbd + (size_t)d->ndet * d->nelec);
   if (d->ndet > 1 && !multideterminants_define(*s)) {
@@ -2773,6 +2841,19 @@ void or_end_block(void *wsp, double *block_energy) {
     ws->tpbcum += w.tpbsum;
     ws->acc += w.acc;
     ws->ecum1 += w.ecum1; ws->ecm21 += w.ecm21; ws->ecum1s += w.ecum1s; ws->ecm21s += w.ecm21s;
+    const int ns = ws->s->nstates;
+    if (ns > 1) {
+      for (auto *v : {&ws->wcum_st, &ws->ecum_st, &ws->ecm2_st, &ws->pecum_st, &ws->tpbcum_st}) v->resize(ns, 0.0);
+      for (int st = 0; st < ns; st++) {
+        const double en = w.esum_st[st] / w.wsum_st[st];
+        ws->wcum_st[st] += w.wsum_st[st];
+        ws->ecum_st[st] += w.esum_st[st];
+        ws->ecm2_st[st] += w.esum_st[st] * en;
+        ws->pecum_st[st] += w.pesum_st[st];
+        ws->tpbcum_st[st] += w.tpbsum_st[st];
+        w.wsum_st[st] = w.esum_st[st] = w.pesum_st[st] = w.tpbsum_st[st] = 0;
+      }
+    }
     es += w.esum;
     wsm += w.wsum;
     w.esum = w.wsum = w.pesum = w.tpbsum = 0;
@@ -2807,6 +2888,36 @@ void or_results(void *wsp, double *out) {
   out[5] = ws->pecum / ws->wcum;
   out[6] = ws->tpbcum / ws->wcum;
   out[7] = (double)ws->iblk;
+}
+
+int or_results_state(void *wsp, int istate, double *out) {
+  // finwrt per state from the reweighted cumulative sums of that state
+  Walkers *ws = (Walkers *)wsp;
+  if (istate < 0 || istate >= ws->s->nstates) return 1;
+  if (ws->s->nstates == 1) {
+    or_results(wsp, out);
+    return 0;
+  }
+  const double wc = ws->wcum_st[istate], ec = ws->ecum_st[istate], e2 = ws->ecm2_st[istate];
+  const double nan = std::nan("");
+  out[0] = ec / wc;
+  out[1] = std::sqrt(std::fabs(e2 / wc - (ec / wc) * (ec / wc)) / (double)ws->iblk);
+  out[2] = out[3] = out[4] = nan;
+  out[5] = ws->pecum_st[istate] / wc;
+  out[6] = ws->tpbcum_st[istate] / wc;
+  out[7] = (double)ws->iblk;
+  return 0;
+}
+
+void or_state_energies(void *wsp, double *e, double *psid) {
+  Walkers *ws = (Walkers *)wsp;
+  const int ns = ws->s->nstates;
+  for (size_t k = 0; k < ws->w.size(); k++)
+    for (int st = 0; st < ns; st++) {
+      const Walker &w = ws->w[k];
+      e[k * ns + st] = ns > 1 ? w.e_st[st] : w.eold;
+      psid[k * ns + st] = ns > 1 ? w.psid_st[st] : w.psido;
+    }
 }
 
 void or_get_walkers(void *wsp, double *x, uint64_t *rng) {

@@ -52,6 +52,8 @@ int or_vmc_steps(void *ws, int nstep, int nthreads);
 int or_zerest(void *ws);
 void or_end_block(void *ws, double *block_energy);
 void or_results(void *ws, double *out);
+int or_results_state(void *ws, int istate, double *out);
+void or_state_energies(void *ws, double *e, double *psid);
 void or_get_walkers(void *ws, double *x, uint64_t *rng);
 void or_get_sums(void *ws, double *out);
 void or_get_state(void *ws, double *eold, double *psido, double *psijo);

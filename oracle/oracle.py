@@ -56,6 +56,9 @@ def lib():
         L.or_zerest.argtypes = [V]
         L.or_end_block.argtypes = [V, _dp]
         L.or_results.argtypes = [V, _dp]
+        L.or_results_state.argtypes = [V, C.c_int, _dp]
+        L.or_results_state.restype = C.c_int
+        L.or_state_energies.argtypes = [V, _dp, _dp]
         L.or_get_walkers.argtypes = [V, _dp, _u64]
         L.or_get_sums.argtypes = [V, _dp]
         L.or_get_state.argtypes = [V, _dp, _dp, _dp]
@@ -174,6 +177,18 @@ class OracleWalkers:
         lib().or_results(self.h, dp(out))
         return dict(energy=out[0], err=out[1], sigma=out[2], tcorr=out[3], accept=out[4], pe=out[5],
                     ke=out[6], nblocks=out[7])
+
+    def results_state(self, istate: int):
+        out = np.zeros(8)
+        if lib().or_results_state(self.h, istate, dp(out)):
+            raise ValueError(f"state {istate} out of range")
+        return dict(energy=out[0], err=out[1], pe=out[5], ke=out[6], nblocks=out[7])
+
+    def state_energies(self, nstates: int):
+        e = np.zeros((self.W, nstates))
+        p = np.zeros((self.W, nstates))
+        lib().or_state_energies(self.h, dp(e), dp(p))
+        return e, p
 
     def walkers(self):
         x = np.zeros((self.W, self.osys.N, 3))
