@@ -85,6 +85,53 @@ def read_det(path, nelec):
     return cdet, iworbd
 
 
+def expand_csf(ccsf, csfmap, ndet):
+    """Determinant coefficients of every state from CSF coefficients
+    (read_csfmap_file, vmc/read_data_parser.f90:1284): ccsf [nstates][ncsf],
+    csfmap[icsf] = [(det index 1-based, coefficient), ...];
+    cdet[k][jx] = sum_icsf ccsf[k][icsf] * c for every (jx, c) of csf icsf."""
+    ccsf = np.atleast_2d(np.asarray(ccsf, float))
+    if ccsf.shape[1] != len(csfmap):
+        raise ValueError("CSFMAP: wrong number of csf")
+    out = np.zeros((ccsf.shape[0], ndet))
+    for k in range(ccsf.shape[0]):
+        for icsf, terms in enumerate(csfmap):
+            for jd, c in terms:
+                if not 1 <= jd <= ndet:
+                    raise ValueError("id in CSFMAP larger than ndet")
+                out[k, jd - 1] += ccsf[k, icsf] * c
+    return out
+
+
+def read_det_states(path, nelec):
+    """.det file with optional csf / csfmap sections (read_csf_file,
+    read_csfmap_file): returns (cdet_states [nstates][ndet], iworbd).  Without
+    a csf section the file's determinant coefficients are the one state."""
+    cdet, iworbd = read_det(path, nelec)
+    ln = [l.split() for l in _lines(path) if l.strip() and not l.strip().startswith("#")]
+    heads = {t[0].lower(): i for i, t in enumerate(ln)}
+    if "csf" not in heads:
+        return cdet[None, :], iworbd
+    i = heads["csf"]
+    ncsf, nstates = int(ln[i][1]), int(ln[i][2])
+    ccsf = np.array([[float(v) for v in ln[i + 1 + k][:ncsf]] for k in range(nstates)])
+    if "csfmap" not in heads:                    # one determinant per CSF, in order
+        return expand_csf(ccsf, [[(j + 1, 1.0)] for j in range(ncsf)], len(cdet)), iworbd
+    i = heads["csfmap"]
+    ncsf_m, ndet_m, nmap = int(ln[i][1]), int(ln[i][2]), int(ln[i][3])
+    if ndet_m != len(cdet) or ncsf_m != ncsf:
+        raise ValueError("CSFMAP: wrong number of determinants or csf")
+    p = i + 1
+    csfmap = []
+    for _ in range(ncsf):
+        nterm = int(ln[p][0])
+        csfmap.append([(int(ln[p + 1 + t][0]), float(ln[p + 1 + t][1])) for t in range(nterm)])
+        p += 1 + nterm
+    if sum(len(t) for t in csfmap) != nmap:
+        raise ValueError("Error in CSFMAP:: not enough nmaps / file is corrupt")
+    return expand_csf(ccsf, csfmap, len(cdet)), iworbd
+
+
 def read_jastrow(path, nctype, nspin2b=1):
     ln = [l for l in _lines(path) if l.strip()]
     assert ln[0].split()[0] == "jastrow_parameter"

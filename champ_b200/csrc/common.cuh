@@ -14,6 +14,7 @@
 #define CW_MAX_TERMS 64
 #define CW_MAX_NORD 7
 #define CW_MAX_QUAD 86
+#define CW_MAX_STATES 8   // CI vectors of a multi-state wave function
 #define CW_MAX_ELEC 1024
 
 // ---------------------------------------------------------------------------
@@ -43,6 +44,9 @@ struct CSys {
   float cf[CW_MAX_TYPES * CW_MAX_TERMS];   // FP32 copy of c (mixed-precision Jastrow)
   // multideterminant expansion (ndet > 1)
   int ndet, md_nuniq[2], md_ivirt[2], md_iactv[2];
+  int nstates;  // CI vectors sharing orbitals and Jastrow (1 = one state)
+  int iguiding; // > 0: the walk samples the guiding function of the states
+  double wg[CW_MAX_STATES];  // guiding weights (weights_g, anormo = 1)
   double asymp_jasa[CW_MAX_TYPES];
   // ECP
   int lpot[CW_MAX_TYPES];
@@ -126,6 +130,7 @@ struct MoveBuf {
   const double *md_velo;   // [W][3] drift correction at the old position
   const double *md_veln;   // [W][3] drift correction at the proposed position
   const double *md_psidn;  // [W]    psi_D at the proposed position
+  const double *md_psi2g;  // [W]    guiding factor psi2g at the proposed position (null: 1)
 };
 
 // ---------------------------------------------------------------------------
@@ -139,6 +144,18 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"((float)x));
   hi = __uint_as_float(h);
   lo = (float)(x - (double)hi);
+}
+
+// determinant_psig (vmc/determinant_psig.f90:3) with anormo = 1 from the S
+// of every state (psi_i/psi_1 = S_i/S_1, one orbital set and Jastrow):
+// psi2g = w_1 + sum_{i>1} w_i (S_i/S_1)^2
+__device__ __forceinline__ double md_psig(const double *S, int ns) {
+  double g = cs.wg[0];
+  for (int i = 1; i < ns; i++) {
+    const double r = S[i] / S[0];
+    g = g + cs.wg[i] * r * r;
+  }
+  return g;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -65,13 +65,14 @@ struct cw_ctx {
   HBuf hb{};
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
-  int ecp_warps = 1, ecp_naov = 0;
+  int ecp_warps = 1, ecp_naov = 0, ecp_minb = 1;
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
   std::unordered_map<void *, size_t> alloc_bytes;
   double *bocc = nullptr;  // [nmax][K] coefficients of the occupied orbitals (c~ GEMM)
   int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
+  std::vector<double> st_cum;  // several states: [nstates][5] wcum, ecum, ecm2, pecum, tpbcum
   double ecum1s = 0, ecm21s = 0;
   long iblk = 0, passes = 0;
   double last_ms = 0;
@@ -270,10 +271,14 @@ void launch_jfull(cw_ctx *c) {
 }
 template <int NORD>
 void launch_ecp(cw_ctx *c) {
-  if (c->mixed)
-    k_ecp<NORD, float><<<c->W, 32 * c->ecp_warps, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
-  else
-    k_ecp<NORD, double><<<c->W, 32 * c->ecp_warps, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+  const dim3 grid(c->W), block(32 * c->ecp_warps);
+  if (c->mixed) {
+    if (c->ecp_minb == 2) k_ecp<NORD, float, 2><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+    else k_ecp<NORD, float, 1><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+  } else {
+    if (c->ecp_minb == 2) k_ecp<NORD, double, 2><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+    else k_ecp<NORD, double, 1><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+  }
 }
 template <int NORD>
 int set_attrs(cw_ctx *c) {
@@ -282,31 +287,43 @@ int set_attrs(cw_ctx *c) {
   CK(raise_smem(c, k_jastrow_full<NORD, double>, c->smem_jfull));
   CK(raise_smem(c, k_jastrow_full<NORD, float>, c->smem_jfull));
   if (c->h.nloc > 0) {
-    // warps per ECP block: the most resident warps per SM under the shared
-    // memory (228 KB), register (64 K) and warp (64) limits; ties go to the
-    // larger block (fewer list passes)
-    cudaFuncAttributes fa;
-    CK(c->mixed ? cudaFuncGetAttributes(&fa, k_ecp<NORD, float>) : cudaFuncGetAttributes(&fa, k_ecp<NORD, double>));
+    // warps per ECP block and register budget (two builds: one block per SM,
+    // or two with at most 64 registers): the most resident warps per SM under
+    // the shared memory (228 KB), register (64 K) and warp (64) limits; ties go
+    // to the larger register budget, then to the larger block (fewer passes)
     const int tbytes = c->mixed ? 4 : 8, nb = 2 * ((een_nb(NORD) + 1) / 2);
-    const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
     const int naov = c->ecp_naov;
     int best = 0;
-    for (int nw = 4; nw <= kEcpMaxWarps; nw++) {
-      const size_t bytes = sizeof(double) * (ecp_base_doubles(c->h.N, c->h.M, 32 * nw) +
-                                             (size_t)nw * ecp_warp_doubles(c->h.M, nb, tbytes, naov)) +
-                           fa.sharedSizeBytes;
-      if (bytes > 227 * 1024) continue;
-      const int blocks = (int)std::min<size_t>({(size_t)(64 / nw), (228 * 1024) / (bytes + 1024),
-                                                (size_t)(65536 / (regs_warp * nw))});
-      if (blocks * nw >= best && blocks > 0) {
-        best = blocks * nw;
-        c->ecp_warps = nw;
-        c->smem_ecp = bytes - fa.sharedSizeBytes;
+    for (int minb = 1; minb <= 2; minb++) {
+      cudaFuncAttributes fa;
+      if (c->mixed)
+        CK(minb == 2 ? cudaFuncGetAttributes(&fa, k_ecp<NORD, float, 2>) : cudaFuncGetAttributes(&fa, k_ecp<NORD, float, 1>));
+      else
+        CK(minb == 2 ? cudaFuncGetAttributes(&fa, k_ecp<NORD, double, 2>) : cudaFuncGetAttributes(&fa, k_ecp<NORD, double, 1>));
+      const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+      for (int nw = 4; nw <= kEcpMaxWarps; nw++) {
+        const size_t bytes = sizeof(double) * (ecp_base_doubles(c->h.N, c->h.M, 32 * nw) +
+                                               (size_t)nw * ecp_warp_doubles(c->h.M, nb, tbytes, naov)) +
+                             fa.sharedSizeBytes;
+        if (bytes > 227 * 1024) continue;
+        const int blocks = (int)std::min<size_t>({(size_t)(64 / nw), (228 * 1024) / (bytes + 1024),
+                                                  (size_t)(65536 / (regs_warp * nw))});
+        if (blocks > 0 && blocks * nw > best) {
+          best = blocks * nw;
+          c->ecp_warps = nw;
+          c->ecp_minb = minb;
+          c->smem_ecp = bytes - fa.sharedSizeBytes;
+        } else if (blocks > 0 && blocks * nw == best && minb == c->ecp_minb) {
+          c->ecp_warps = nw;
+          c->smem_ecp = bytes - fa.sharedSizeBytes;
+        }
       }
     }
     if (best == 0) return fail(c, CW_ERR_UNSUPPORTED, "ECP stage shared memory too large");
-    CK(raise_smem(c, k_ecp<NORD, double>, c->smem_ecp));
-    CK(raise_smem(c, k_ecp<NORD, float>, c->smem_ecp));
+    CK(raise_smem(c, k_ecp<NORD, double, 1>, c->smem_ecp));
+    CK(raise_smem(c, k_ecp<NORD, float, 1>, c->smem_ecp));
+    CK(raise_smem(c, k_ecp<NORD, double, 2>, c->smem_ecp));
+    CK(raise_smem(c, k_ecp<NORD, float, 2>, c->smem_ecp));
   }
   return CW_OK;
 }
@@ -348,7 +365,8 @@ int md_define(cw_ctx *c, const cw_system_desc *d, std::vector<int> &exc, std::ve
   for (size_t t = 0; t < (size_t)nd * N; t++)
     if (d->iworbd[t] < 1 || d->iworbd[t] > d->norb) return fail(c, CW_ERR_ARG, "iworbd entry out of range");
   std::vector<int> numrep((size_t)nd * 2, 0), irc((size_t)nd * 2 * N, 0), iro((size_t)nd * 2 * N, 0);
-  cdet.assign(d->cdet, d->cdet + nd);
+  const int ns = d->nstates > 1 ? d->nstates : 1;
+  cdet.assign(d->cdet, d->cdet + (size_t)ns * nd);  // [nstates][ndet]
   for (int k = 1; k < nd; k++) {
     int itot = 0;
     for (int iab = 0; iab < 2; iab++) {
@@ -380,7 +398,8 @@ int md_define(cw_ctx *c, const cw_system_desc *d, std::vector<int> &exc, std::ve
               itot++;
             }
     }
-    if (itot % 2) cdet[k] = -cdet[k];
+    if (itot % 2)
+      for (int st = 0; st < ns; st++) cdet[(size_t)st * nd + k] = -cdet[(size_t)st * nd + k];
   }
   kw.assign((size_t)nd * 2, -1);
   std::vector<std::vector<int>> order(2);
@@ -712,6 +731,10 @@ int alloc_walkers(cw_ctx *c, int W) {
   b.tvpsp = nullptr;
   b.md_P = nullptr;
   b.md_den = b.md_S = nullptr;
+  b.md_S_ms = b.md_den_ms = nullptr;
+  b.e_ms = b.psid_ms = b.sums_ms = nullptr;
+  c->md.S_ms = c->md.den_ms = c->md.Sn_ms = c->md.psi2gn = nullptr;
+  m.md_psi2g = nullptr;
   c->md_vall = nullptr;
   if (c->md_on) {
     MdBuf &d = c->md;
@@ -719,7 +742,7 @@ int alloc_walkers(cw_ctx *c, int W) {
     DALLOC(L, d.aa, (size_t)W * 2 * nmax * Oa);
     DALLOC(L, d.ymat, (size_t)W * 2 * nmax * Oa);
     DALLOC(L, d.dd, (size_t)W * 2 * nu);
-    DALLOC(L, d.G, (size_t)W * (nu + 1));
+    DALLOC(L, d.G, (size_t)W * (h.iguiding ? h.nstates : 1) * (nu + 1));
     DALLOC(L, d.S, W);
     DALLOC(L, d.orbA, (size_t)W * N * Oa);
     DALLOC(L, d.dorbA, (size_t)W * 3 * N * Oa);
@@ -742,6 +765,22 @@ int alloc_walkers(cw_ctx *c, int W) {
     b.md_P = d.P;
     b.md_den = d.den;
     b.md_S = d.S;
+    if (h.nstates > 1) {
+      const int ns = h.nstates;
+      DALLOC(L, d.S_ms, (size_t)W * ns);
+      DALLOC(L, d.den_ms, (size_t)W * ns * 2);
+      DALLOC(L, b.e_ms, (size_t)W * ns);
+      DALLOC(L, b.psid_ms, (size_t)W * ns);
+      DALLOC(L, b.sums_ms, (size_t)W * ns * 4);
+      CK(cudaMemsetAsync(b.sums_ms, 0, sizeof(double) * W * ns * 4, c->stream));
+      b.md_S_ms = d.S_ms;
+      b.md_den_ms = d.den_ms;
+      if (h.iguiding) {
+        DALLOC(L, d.Sn_ms, (size_t)W * ns);
+        DALLOC(L, d.psi2gn, W);
+        m.md_psi2g = d.psi2gn;
+      }
+    }
   }
   DALLOC(L, b.entab, (size_t)W * M * N * kEnFields);
   CK(cudaMemsetAsync(s.status, 0, sizeof(int) * W, c->stream));
@@ -772,6 +811,7 @@ int zerest(cw_ctx *c) {
   CK(cudaMemsetAsync(c->st.sums, 0, sizeof(double) * W * 8, c->stream));
   c->ecum = c->ecm2 = c->wcum = c->pecum = c->tpbcum = c->pecm2 = c->tpbcm2 = c->acc = 0;
   c->ecum1s = c->ecm21s = 0;
+  c->st_cum.assign(h.nstates > 1 ? (size_t)h.nstates * 5 : 0, 0.0);
   c->iblk = 0;
   c->passes = 0;
   return check_status(c);
@@ -827,6 +867,17 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   h.scalek = d->scalek;
   h.deltar = d->deltar; h.deltat = d->deltat; h.fbias = d->fbias; h.pecent = d->pecent;
   h.cdet = d->cdet[0];
+  h.nstates = d->nstates > 1 ? d->nstates : 1;
+  if (h.nstates > 1) {
+    if (d->ndet < 2) return fail(c, CW_ERR_UNSUPPORTED, "several states need a multideterminant expansion");
+    if (h.nstates > CW_MAX_STATES) return fail(c, CW_ERR_ARG, "at most %d states", CW_MAX_STATES);
+    h.iguiding = d->iguiding > 0 ? d->iguiding : 0;
+    if (h.iguiding) {
+      if (!d->weights_g) return fail(c, CW_ERR_ARG, "iguiding > 0 needs weights_g");
+      for (int i = 0; i < h.nstates; i++) h.wg[i] = d->weights_g[i];
+      if (!(h.wg[0] > 0)) return fail(c, CW_ERR_ARG, "weights_g of state 1 must be positive");
+    }
+  }
   h.mrwf = d->mrwf; h.mpts = d->mrwf_pts; h.mbastyp = d->mbastyp;
   int m = 0;
   for (int ic = 0; ic < d->ncent; ic++) {
@@ -1034,7 +1085,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     if (h.nloc > 0 && c->ecp_naov != h.K)  // the ECP block's basis-value rows must be sized
       return fail(c, CW_ERR_STATE, "ECP stage sized without multideterminant basis rows");
     const size_t O = h.Oa;
-    c->smem_md_hpsi = sizeof(double) * (4 * (size_t)nmax * nmax + (size_t)nmax * O + numax + 1);
+    c->smem_md_hpsi = sizeof(double) * (4 * (size_t)nmax * nmax + (h.nstates > 1 ? 3 : 1) * (size_t)nmax * O + numax + 1);
     c->smem_md_phase = sizeof(double) * ((size_t)numax + 1);
     c->smem_md_move = sizeof(double) * (2 * (size_t)nmax + 4 * O + (size_t)nmax * O);
     c->smem_md_drift = sizeof(double) * ((size_t)nmax + 3 * O + (size_t)nmax * O);
@@ -1243,8 +1294,58 @@ int cw_end_block(cw_ctx *c, double *block_energy) {
     es += v[1];
     wsm += v[0];
   }
+  if (c->hb.sums_ms) {
+    // acuest per state: the reweighted block sums of every walker
+    const int ns = c->h.nstates;
+    std::vector<double> q((size_t)W * ns * 4);
+    CK(cudaMemcpyAsync(q.data(), c->hb.sums_ms, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemsetAsync(c->hb.sums_ms, 0, sizeof(double) * q.size(), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int w = 0; w < W; w++)
+      for (int st = 0; st < ns; st++) {
+        const double *v = &q[((size_t)w * ns + st) * 4];
+        double *cu = &c->st_cum[(size_t)st * 5];
+        const double en = v[1] / v[0];
+        cu[0] += v[0];
+        cu[1] += v[1];
+        cu[2] += v[1] * en;
+        cu[3] += v[2];
+        cu[4] += v[3];
+      }
+  }
   c->iblk += W;
   if (block_energy) *block_energy = es / wsm;
+  return CW_OK;
+}
+
+int cw_results_state(cw_ctx *c, int istate, double *out) {
+  if (!c || !out) return fail(c, CW_ERR_ARG, "null argument");
+  if (istate < 0 || istate >= c->h.nstates) return fail(c, CW_ERR_ARG, "state %d of %d", istate, c->h.nstates);
+  if (c->h.nstates == 1) return cw_results(c, out);
+  if (c->iblk == 0) return fail(c, CW_ERR_STATE, "no completed blocks");
+  const double *cu = &c->st_cum[(size_t)istate * 5];
+  const double ef = cu[1] / cu[0];
+  out[0] = ef;
+  out[1] = std::sqrt(std::fabs(cu[2] / cu[0] - ef * ef) / (double)c->iblk);
+  out[2] = out[3] = out[4] = std::nan("");
+  out[5] = cu[3] / cu[0];
+  out[6] = cu[4] / cu[0];
+  out[7] = (double)c->iblk;
+  return CW_OK;
+}
+
+int cw_state_energies(cw_ctx *c, double *energy, double *psid) {
+  if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  BIND(c);
+  const int W = c->W, ns = c->h.nstates;
+  if (ns == 1) {
+    if (energy) CK(cudaMemcpyAsync(energy, c->st.eold, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+    if (psid) CK(cudaMemcpyAsync(psid, c->st.psido, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    if (energy) CK(cudaMemcpyAsync(energy, c->hb.e_ms, sizeof(double) * W * ns, cudaMemcpyDeviceToHost, c->stream));
+    if (psid) CK(cudaMemcpyAsync(psid, c->hb.psid_ms, sizeof(double) * W * ns, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
   return CW_OK;
 }
 
@@ -1660,6 +1761,8 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
     return fail(c, CW_ERR_ARG, "cw_dmc_init: bad arguments");
   if (c->h.nloc == 0)
     return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: all-electron DMC (dmc_ae) is not implemented; nloc > 0 required");
+  if (c->h.nstates > 1)
+    return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: several states are a VMC feature (dmc_ps samples one state)");
   BIND(c);
   int rc = dmc_alloc(c, mwalk);
   if (rc) return rc;
@@ -2102,6 +2205,14 @@ int ck_serialize(cw_ctx *c, std::vector<uint8_t> &out) {
     o.put(d.trymove);
     o.put(d.ff.data(), d.ff.size());
   }
+  if (h.nstates > 1) {
+    // several states: cumulative and current-block sums of every state
+    std::vector<double> q((size_t)W * h.nstates * 4);
+    CK(cudaMemcpyAsync(q.data(), c->hb.sums_ms, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    o.put(c->st_cum.data(), c->st_cum.size());
+    o.put(q.data(), q.size());
+  }
   out.swap(o.b);
   return CW_OK;
 }
@@ -2151,6 +2262,14 @@ int ck_restore(cw_ctx *c, const uint8_t *buf, size_t n) {
     ff.resize((size_t)di[7]);
     r.get(ff.data(), ff.size());
   }
+  // several states: cumulative and current-block sums of every state
+  std::vector<double> st_cum, st_q;
+  if (h.nstates > 1) {
+    st_cum.assign((size_t)h.nstates * 5, 0.0);
+    st_q.assign((size_t)W * h.nstates * 4, 0.0);
+    r.get(st_cum.data(), st_cum.size());
+    r.get(st_q.data(), st_q.size());
+  }
   if (!r.ok || r.off != n) return fail(c, CW_ERR_ARG, "restore: truncated or oversized checkpoint buffer");
   BIND(c);
   int rc = dmc ? dmc_alloc(c, slots) : alloc_walkers(c, W);
@@ -2197,6 +2316,11 @@ int ck_restore(cw_ctx *c, const uint8_t *buf, size_t n) {
       if (rc) return rc;
     }
     d.nmove_casula = di[9];
+  }
+  if (h.nstates > 1) {
+    c->st_cum = st_cum;
+    CK(cudaMemcpyAsync(c->hb.sums_ms, st_q.data(), sizeof(double) * st_q.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
   }
   return check_status(c);
 }

@@ -34,6 +34,11 @@ struct HBuf {
   double *md_P;            // [W][N][K] pseudopotential quadrature basis sums
   const double *md_den;    // [W][2] energy / kinetic corrections
   const double *md_S;      // [W]    psi_D / (D_ref^up D_ref^dn)
+  // several states (null for one): per state S, corrections, and outputs
+  const double *md_S_ms;   // [W][nstates]
+  const double *md_den_ms; // [W][nstates][2]
+  double *e_ms, *psid_ms;  // [W][nstates] local energy and psi_D of the last hpsi
+  double *sums_ms;         // [W][nstates][4] block sums: w, w E, w (E - T), w T
 };
 
 __device__ __forceinline__ void pair_of(long p, int &i, int &j) {
@@ -558,8 +563,8 @@ __host__ __device__ inline size_t ecp_warp_doubles(int M, int nb, int tbytes, in
 // (nonlocj_quad4) and the weighted Legendre sum (vmc/nonloc.f90:5).  The list
 // holds at most blockDim entries; a walker with more active pairs is
 // processed in several passes, in the same order.
-template <int NORD, typename T>
-__global__ void __launch_bounds__(32 * kEcpMaxWarps) k_ecp(WState st, HBuf hb, GSys g) {
+template <int NORD, typename T, int MINB>  // MINB: blocks per SM the register budget is set for
+__global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf hb, GSys g) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M, K = cs.K, NQ = cs.nquad, NM = N * M;
@@ -780,12 +785,37 @@ __global__ void k_energy(WState st, HBuf hb, int mode, double *out_e, double *ou
   st.ekino[w] = ekin;
   st.psido[w] = psid;
   st.psijo[w] = psij;
-  st.psi2o[w] = 2 * (log(fabs(psid)) + psij);
+  // guiding function (metrop6 :652-657, :732): psi2g from the S of every state
+  const double psi2g = (cs.iguiding > 0 && hb.md_S_ms) ? md_psig(hb.md_S_ms + (size_t)w * cs.nstates, cs.nstates) : 1.0;
+  st.psi2o[w] = log(fabs(psi2g)) + 2 * (log(fabs(psid)) + psij);
   if (!isfinite(energy)) st.status[w] |= 2;
   if (out_e) out_e[w] = energy;
   if (out_ekin) out_ekin[w] = ekin;
+  if (hb.md_S_ms) {
+    // every state: its own correction and psi_D, weighted by
+    // (psi_s/psi_1)^2 / psi2g for the sampled distribution (metrop6 :678-690)
+    const int ns = cs.nstates;
+    const double S1 = hb.md_S_ms[(size_t)w * ns];
+    for (int s = 0; s < ns; s++) {
+      const double *dn = hb.md_den_ms + ((size_t)w * ns + s) * 2;
+      const double Ss = hb.md_S_ms[(size_t)w * ns + s];
+      const double es = dn[0] + (ek[0] + vp0) + (ek[1] + vp1) + e_other;
+      const double ks = dn[1] + ek[0] + ek[1] + ekin_other;
+      hb.e_ms[(size_t)w * ns + s] = es;
+      hb.psid_ms[(size_t)w * ns + s] = st.detiab[2 * w] * st.detiab[2 * w + 1] * Ss;
+      if (mode == 1) {
+        const double ws = Ss / S1 * exp(psij - psij) / sqrt(psi2g);
+        const double wt = ws * ws;
+        double *q = hb.sums_ms + ((size_t)w * ns + s) * 4;
+        q[0] += wt;
+        q[1] += es * wt;
+        q[2] += (es - ks) * wt;
+        q[3] += ks * wt;
+      }
+    }
+  }
   if (mode == 1) {
-    const double wtg_sqrt = psid / psid * exp(psij - psij) / sqrt(1.0);
+    const double wtg_sqrt = psid / psid * exp(psij - psij) / sqrt(psi2g);
     const double wtg = wtg_sqrt * wtg_sqrt;
     double *s = st.sums + (size_t)w * 8;
     s[0] += wtg;

@@ -57,6 +57,12 @@ struct MdBuf {
   double *bnl;    // [W][N][O]
   double *P;      // [W][N][K] quadrature basis sums of the pseudopotential
   double *den;    // [W][2]  denergy, dekin
+  double *S_ms;   // [W][nstates] S of every state (null for one state)
+  double *den_ms; // [W][nstates][2] denergy, dekin of every state
+  // guiding function (null without): S of every state at the proposed point,
+  // psi2g there
+  double *Sn_ms;  // [W][nstates]
+  double *psi2gn; // [W]
   // move outputs (spin of the moved electron)
   double *cvec;   // [W][nmax] inverse column of the moved electron (before the move)
   double *wvec;   // [W][O]    rank-1 factor of aa
@@ -254,7 +260,8 @@ __global__ void k_md_scatter(WState st, MdBuf md, const double *orball, int e0, 
 }
 
 // G_s (and its kref-equivalent part) from the other spin's ratios; smem-free
-__device__ void md_form_G(const MdTab &tab, const MdBuf &md, int w, int s, double *G, double *red) {
+__device__ void md_form_G(const MdTab &tab, const MdBuf &md, int w, int s, double *G, double *red,
+                          const double *cdet) {
   const int NU = cs.md_nuniq[s];
   for (int kk = threadIdx.x; kk <= NU; kk += blockDim.x) G[kk] = 0.0;
   __syncthreads();
@@ -262,7 +269,7 @@ __device__ void md_form_G(const MdTab &tab, const MdBuf &md, int w, int s, doubl
   double gref = 0.0;
   for (int k = threadIdx.x; k < cs.ndet; k += blockDim.x) {
     const int kws = tab.kw[2 * k + s], kwo = tab.kw[2 * k + (1 - s)];
-    const double v = tab.cdet[k] * (kwo >= 0 ? dother[kwo] : 1.0);
+    const double v = cdet[k] * (kwo >= 0 ? dother[kwo] : 1.0);
     if (kws >= 0) atomicAdd(&G[kws], v);
     else gref += v;
   }
@@ -336,6 +343,8 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
   double *T = Xk + nmax * nmax;            // nmax*nmax work
   double *Y = T + nmax * nmax;             // nmax*O
   double *G = Y + (size_t)nmax * O;        // numax+1
+  double *Tm = G + tab.numax + 1;          // nmax*O tildem of B = bkin + bnl (several states only)
+  double *Tk = Tm + (size_t)nmax * O;      // nmax*O tildem of bkin
   __shared__ double red[4];
   // 1. aa and excitation ratios of both spins
   for (int s = 0; s < 2; s++) {
@@ -360,28 +369,35 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
     }
   }
   __syncthreads();
-  // 2. S
-  double sp = 0;
-  for (int k = threadIdx.x; k < cs.ndet; k += blockDim.x) {
-    const int k0 = tab.kw[2 * k], k1 = tab.kw[2 * k + 1];
-    const double d0 = k0 >= 0 ? md.dd[((size_t)w * 2 + 0) * tab.numax + k0] : 1.0;
-    const double d1 = k1 >= 0 ? md.dd[((size_t)w * 2 + 1) * tab.numax + k1] : 1.0;
-    sp += d0 * d1 * tab.cdet[k];
+  // 2. S of every state (state 0 drives the walk)
+  const int ns = cs.nstates;
+  __shared__ double s_S[CW_MAX_STATES], s_den[CW_MAX_STATES], s_dek[CW_MAX_STATES];
+  for (int stt = 0; stt < ns; stt++) {
+    const double *cd = tab.cdet + (size_t)stt * cs.ndet;
+    double sp = 0;
+    for (int k = threadIdx.x; k < cs.ndet; k += blockDim.x) {
+      const int k0 = tab.kw[2 * k], k1 = tab.kw[2 * k + 1];
+      const double d0 = k0 >= 0 ? md.dd[((size_t)w * 2 + 0) * tab.numax + k0] : 1.0;
+      const double d1 = k1 >= 0 ? md.dd[((size_t)w * 2 + 1) * tab.numax + k1] : 1.0;
+      sp += d0 * d1 * cd[k];
+    }
+    sp = md_block_sum<128>(sp, red);
+    if (threadIdx.x == 0) {
+      s_S[stt] = sp;
+      s_den[stt] = 0;
+      s_dek[stt] = 0;
+    }
   }
-  const double Ssum = md_block_sum<128>(sp, red);
-  // 3. per spin: Y, then the energy corrections sum_{irep>=iactv, v>=ivirt} Y tildem
-  double den = 0, dek = 0;
+  // 3. per spin: tildem = A^-1 B - X Phi (state-independent), then per state
+  //    G, Y and the energy corrections sum_{irep>=iactv, v>=ivirt} Y tildem
   for (int s = 0; s < 2; s++) {
     const int n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
     if (n == 0) continue;
     const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
     const double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
-    md_form_G(tab, md, w, s, G, red);
-    md_form_Y(tab, s, aa, dd, G, Y);
-    double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
-    for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
     // X = A^-1 B_occ A^-1 (bxmatrix) for B = bkin + bnl and for bkin
     const double *slmi = st.slmi + ((size_t)w * 2 + s) * nmax * nmax;
+    __syncthreads();
     for (int t = threadIdx.x; t < n * n; t += blockDim.x) Sl[t] = slmi[t];
     __syncthreads();
     for (int pass = 0; pass < 2; pass++) {
@@ -410,6 +426,14 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
     }
     const int ivirt = cs.md_ivirt[s], iactv = cs.md_iactv[s];
     const int nv = O - ivirt, na = n - iactv;
+    if (ns == 1) {
+      // one state: Y first, then tildem contracted with it on the fly
+      md_form_G(tab, md, w, s, G, red, tab.cdet);
+      md_form_Y(tab, s, aa, dd, G, Y);
+      double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
+      for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
+    }
+    double den1 = 0, dek1 = 0;
     for (int t = threadIdx.x; t < nv * na; t += blockDim.x) {
       const int irep = iactv + t / nv, v = ivirt + t % nv;
       double d2 = 0, d3 = 0, d4 = 0, d5 = 0;
@@ -422,18 +446,57 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
         d4 += sl * md.bkin[bi];
         d5 += Xk[e * n + irep] * ov;
       }
-      const double y = Y[irep * O + v];
-      den += y * (d2 - d3);
-      dek += y * (d4 - d5);
+      if (ns == 1) {
+        const double y = Y[irep * O + v];
+        den1 += y * (d2 - d3);
+        dek1 += y * (d4 - d5);
+      } else {
+        Tm[t] = d2 - d3;
+        Tk[t] = d4 - d5;
+      }
     }
-    __syncthreads();
+    if (ns == 1) {
+      den1 = md_block_sum<128>(den1, red);
+      dek1 = md_block_sum<128>(dek1, red);
+      if (threadIdx.x == 0) {
+        s_den[0] += den1;
+        s_dek[0] += dek1;
+      }
+      __syncthreads();
+      continue;
+    }
+    for (int stt = 0; stt < ns; stt++) {
+      md_form_G(tab, md, w, s, G, red, tab.cdet + (size_t)stt * cs.ndet);
+      md_form_Y(tab, s, aa, dd, G, Y);
+      if (stt == 0) {
+        double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
+        for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
+      }
+      double den = 0, dek = 0;
+      for (int t = threadIdx.x; t < nv * na; t += blockDim.x) {
+        const double y = Y[(iactv + t / nv) * O + ivirt + t % nv];
+        den += y * Tm[t];
+        dek += y * Tk[t];
+      }
+      den = md_block_sum<128>(den, red);
+      dek = md_block_sum<128>(dek, red);
+      if (threadIdx.x == 0) {
+        s_den[stt] += den;
+        s_dek[stt] += dek;
+      }
+      __syncthreads();
+    }
   }
-  den = md_block_sum<128>(den, red);
-  dek = md_block_sum<128>(dek, red);
   if (threadIdx.x == 0) {
-    md.S[w] = Ssum;
-    md.den[2 * w] = den / Ssum;
-    md.den[2 * w + 1] = dek / Ssum;
+    md.S[w] = s_S[0];
+    md.den[2 * w] = s_den[0] / s_S[0];
+    md.den[2 * w + 1] = s_dek[0] / s_S[0];
+    if (md.S_ms)
+      for (int stt = 0; stt < ns; stt++) {
+        md.S_ms[(size_t)w * ns + stt] = s_S[stt];
+        md.den_ms[((size_t)w * ns + stt) * 2] = s_den[stt] / s_S[stt];
+        md.den_ms[((size_t)w * ns + stt) * 2 + 1] = s_dek[stt] / s_S[stt];
+      }
   }
 }
 
@@ -492,9 +555,13 @@ __global__ void __launch_bounds__(128) k_md_phase(WState st, MdBuf md, MdTab tab
   extern __shared__ __align__(16) double smem[];
   double *G = smem;  // numax+1
   __shared__ double red[4];
-  md_form_G(tab, md, w, s, G, red);
-  double *gG = md.G + (size_t)w * (tab.numax + 1);
-  for (int kk = threadIdx.x; kk <= cs.md_nuniq[s]; kk += blockDim.x) gG[kk] = G[kk];
+  const int ng = cs.iguiding > 0 ? cs.nstates : 1;  // states whose G the moves need
+  for (int stt = 0; stt < ng; stt++) {
+    md_form_G(tab, md, w, s, G, red, tab.cdet + (size_t)stt * cs.ndet);
+    double *gG = md.G + ((size_t)w * ng + stt) * (tab.numax + 1);
+    for (int kk = threadIdx.x; kk <= cs.md_nuniq[s]; kk += blockDim.x) gG[kk] = G[kk];
+    __syncthreads();
+  }
 }
 
 // multideterminante_grad at the old position of electron iel, without the Y
@@ -519,7 +586,40 @@ __global__ void __launch_bounds__(128) k_md_drift_old(WState st, MdBuf md, MdTab
   md_form_t(s, md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O, md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O,
             md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O, A, g.slot_orb + s * nmax, t);
   __syncthreads();
-  const double *G = md.G + (size_t)w * (tab.numax + 1);
+  const double *G = md.G + (size_t)w * (cs.iguiding > 0 ? cs.nstates : 1) * (tab.numax + 1);
+  if (cs.iguiding > 0) {
+    // guiding (determinante.f90:150-171): sum_i w_i (S_i/S_1)^2 v_i / psi2g,
+    // v_i the velocity of state i (its own G, 1/S_i)
+    const int ns = cs.nstates;
+    const double *S = md.S_ms + (size_t)w * ns;
+    double vg[3] = {0, 0, 0};
+    for (int stt = 0; stt < ns; stt++) {
+      const double *Gs = G + (size_t)stt * (tab.numax + 1);
+      double a0 = 0, a1 = 0, a2 = 0;
+      for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) {
+        double gv[3];
+        const double d = md_ratio_contract(A, O, md_exc(tab, s, kk), c, t, O, gv);
+        const double ce = d * Gs[kk];
+        a0 += ce * gv[0];
+        a1 += ce * gv[1];
+        a2 += ce * gv[2];
+      }
+      a0 = md_block_sum<128>(a0, red);
+      a1 = md_block_sum<128>(a1, red);
+      a2 = md_block_sum<128>(a2, red);
+      const double r = S[stt] / S[0], f = cs.wg[stt] * r * r / S[stt];
+      vg[0] += f * a0;
+      vg[1] += f * a1;
+      vg[2] += f * a2;
+    }
+    if (threadIdx.x == 0) {
+      const double gi = 1.0 / md_psig(S, ns);
+      md.velo[3 * w] = vg[0] * gi;
+      md.velo[3 * w + 1] = vg[1] * gi;
+      md.velo[3 * w + 2] = vg[2] * gi;
+    }
+    return;
+  }
   double v0 = 0, v1 = 0, v2 = 0;
   for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) {
     double gv[3];
@@ -598,8 +698,57 @@ __global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md
   __syncthreads();
   for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = c[j] / R;
   __syncthreads();
-  const double *G = md.G + (size_t)w * (tab.numax + 1);
+  const double *G = md.G + (size_t)w * (cs.iguiding > 0 ? cs.nstates : 1) * (tab.numax + 1);
   double *ddn = md.ddn + (size_t)w * tab.numax;
+  if (cs.iguiding > 0) {
+    // guiding: S and velocity of every state at the proposed point, psi2g there
+    const int ns = cs.nstates;
+    __shared__ double s_Sn[CW_MAX_STATES], s_v[CW_MAX_STATES][3];
+    for (int stt = 0; stt < ns; stt++) {
+      const double *Gs = G + (size_t)stt * (tab.numax + 1);
+      double sp = 0, a0 = 0, a1 = 0, a2 = 0;
+      for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
+        double gv[3];
+        const double d = md_ratio_contract(An, O, md_exc(tab, s, kk), c, t, O, gv);
+        if (stt == 0) ddn[kk] = d;
+        const double ce = d * Gs[kk];
+        sp += ce;
+        a0 += ce * gv[0];
+        a1 += ce * gv[1];
+        a2 += ce * gv[2];
+      }
+      sp = md_block_sum<128>(sp, red) + Gs[NU];
+      a0 = md_block_sum<128>(a0, red);
+      a1 = md_block_sum<128>(a1, red);
+      a2 = md_block_sum<128>(a2, red);
+      if (threadIdx.x == 0) {
+        s_Sn[stt] = sp;
+        s_v[stt][0] = a0;
+        s_v[stt][1] = a1;
+        s_v[stt][2] = a2;
+      }
+    }
+    if (threadIdx.x == 0) {
+      const double detn_ref = st.detiab[2 * w + s] * R;
+      const double dpair = s == 0 ? detn_ref * st.detiab[2 * w + 1] : st.detiab[2 * w] * detn_ref;
+      const double g = md_psig(s_Sn, ns), gi = 1.0 / g;
+      double vg[3] = {0, 0, 0};
+      for (int stt = 0; stt < ns; stt++) {
+        const double r = s_Sn[stt] / s_Sn[0], f = cs.wg[stt] * r * r / s_Sn[stt];
+        for (int k = 0; k < 3; k++) vg[k] += f * s_v[stt][k];
+        md.Sn_ms[(size_t)w * ns + stt] = s_Sn[stt];
+      }
+      for (int k = 0; k < 3; k++) md.veln[3 * w + k] = vg[k] * gi;
+      md.psidn[w] = dpair * s_Sn[0];
+      md.Sn[w] = s_Sn[0];
+      md.psi2gn[w] = g;
+    }
+    double *cv = md.cvec + (size_t)w * nmax;
+    double *wgv = md.wvec + (size_t)w * O;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) cv[j] = c[j] * R;
+    for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) wgv[v] = wv[v];
+    return;
+  }
   double sp = 0, v0 = 0, v1 = 0, v2 = 0;
   for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
     double gv[3];
@@ -654,6 +803,9 @@ __global__ void k_md_commit(WState st, MoveBuf mb, MdBuf md, MdTab tab, int iel)
   for (int o = threadIdx.x; o < O; o += blockDim.x)
     for (int k = 0; k < 3; k++) md.dorbA[(((size_t)w * 3 + k) * N + iel) * O + o] = orbn[(1 + k) * O + o];
   if (threadIdx.x == 0) md.S[w] = md.Sn[w];
+  if (md.Sn_ms)
+    for (int stt = threadIdx.x; stt < cs.nstates; stt += blockDim.x)
+      md.S_ms[(size_t)w * cs.nstates + stt] = md.Sn_ms[(size_t)w * cs.nstates + stt];
 }
 
 }  // namespace cw

@@ -687,7 +687,7 @@ __global__ void k_decide(WState st, MoveBuf mb, GSys g, int iel) {
       const double *mv = mb.md_veln ? mb.md_veln + 3 * w : nullptr;
       const double vn[3] = {(mv ? mv[0] : 0.0) + v0 + mb.vjn[3 * w + 0], (mv ? mv[1] : 0.0) + v1 + mb.vjn[3 * w + 1],
                             (mv ? mv[2] : 0.0) + v2 + mb.vjn[3 * w + 2]};
-      psi2n = log(fabs(1.0)) + 2 * (log(fabs(psidn)) + fsumn);
+      psi2n = log(fabs(mb.md_psi2g ? mb.md_psi2g[w] : 1.0)) + 2 * (log(fabs(psidn)) + fsumn);
       const double deltar = cs.deltar, deltri = one / deltar;
       const double rminn = m.rminn, rminon = m.rminon;
       const double rbot = rminn * deltri, rtop = rminn * deltar;

@@ -141,6 +141,19 @@ class Engine:
         return dict(energy=o[0], err=o[1], sigma=o[2], tcorr=o[3], accept=o[4], pe=o[5], ke=o[6],
                     nblocks=o[7])
 
+    def results_state(self, istate: int) -> dict:
+        """Block results of state `istate` of a multi-state wave function."""
+        o = np.zeros(8)
+        self._check(self.lib.cw_results_state(self.h, istate, dptr(o)), "cw_results_state")
+        return dict(energy=o[0], err=o[1], pe=o[5], ke=o[6], nblocks=o[7])
+
+    def state_energies(self):
+        """Local energy and psi_D of every state at the last hpsi: [W][nstates] each."""
+        ns = self.system.nstates
+        e, p = np.zeros((self.W, ns)), np.zeros((self.W, ns))
+        self._check(self.lib.cw_state_energies(self.h, dptr(e), dptr(p)), "cw_state_energies")
+        return e, p
+
     def sums(self):
         out = np.zeros((self.W, 5))
         self._check(self.lib.cw_get_sums(self.h, dptr(out)), "cw_get_sums")

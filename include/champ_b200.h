@@ -112,10 +112,13 @@ typedef struct cw_system_desc {
   /* --- several states sharing orbitals and Jastrow (csfs nstates,
    *     mstates_ctrl iguiding, mstates3 weights_g; vmc/determinante.f90:134-230,
    *     vmc/determinant_psig.f90:3).  nstates 0 or 1: one state; > 1 (VMC
-   *     only): cdet holds [nstates][ndet], the walk samples |psi_1|^2 and
-   *     state s is weighted by (psi_s/psi_1)^2 (iguiding = 0). --- */
+   *     only, at most 8): cdet holds [nstates][ndet]; iguiding = 0: the walk
+   *     samples |psi_1|^2 and state s is weighted by (psi_s/psi_1)^2;
+   *     iguiding > 0: the walk samples psi2g |psi_1|^2 with
+   *     psi2g = sum_i weights_g[i] (psi_i/psi_1)^2 (anormo = 1) and state s
+   *     is weighted by (psi_s/psi_1)^2 / psi2g. --- */
   int32_t nstates;
-  int32_t iguiding;            /* > 0 (guiding function) is refused: CW_ERR_UNSUPPORTED */
+  int32_t iguiding;
   const double *weights_g;     /* [nstates] guiding weights (read only when iguiding > 0) */
 } cw_system_desc;
 

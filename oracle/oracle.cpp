@@ -68,6 +68,8 @@ struct Sys {
   int K, O, ndet;
   vector<double> coef, cdet;   // cdet: sign-adjusted by multideterminants_define
   int nstates = 1;             // CI vectors sharing orbitals and Jastrow (csfs nstates)
+  int iguiding = 0;            // > 0: sample the guiding function (mstates_ctrl)
+  vector<double> weights_g;    // [nstates] (mstates3; anormo = 1)
   vector<double> cdet_st;      // [nstates][ndet], sign-adjusted like cdet; row 0 = cdet
   vector<int> iworbd;  // iworbd(j) for kref=1, 1-based orbital
   vector<int> iworbd_all;      // [ndet][N] 1-based, reordered as multideterminants_define does
@@ -541,6 +543,10 @@ struct Walker {
   double esum, wsum, pesum, tpbsum, acc, esum1;
   // several states: energies and psi_D of the last hpsi, block sums per state
   vector<double> e_st, ekin_st, psid_st, wsum_st, esum_st, pesum_st, tpbsum_st;
+  // guiding function: psi_D of every state at the current and at the proposed
+  // configuration, and psi2g = sum_i w_i (psi_i/psi_1)^2 at the current one
+  vector<double> psid_cur, psidn_st;
+  double psi2g_o = 1.0;
   double ecum, ecm2, wcum, pecum, tpbcum, pecm2, tpbcm2, ecum1, ecm21, ecum1s, ecm21s;
   Rng rng;
   bool singular = false;
@@ -1254,7 +1260,65 @@ struct Walker {
     }
   }
   // compute_determinante_grad (vmc/determinante.f90:69), single det, iflag_move 1 or 0
+  // determinant_psig (vmc/determinant_psig.f90:3) with anormo = 1
+  double psig_of(const double *ps) const {
+    double g = s->weights_g[0];
+    for (int i = 1; i < s->nstates; i++) {
+      const double r = ps[i] / ps[0];
+      g = g + s->weights_g[i] * r * r;
+    }
+    return g;
+  }
+  // compute_determinante_grad with iguiding > 0 (vmc/determinante.f90:150-171,
+  // :196-229): sum_i w_i (psi_i/psi_1)^2 (vd_i + vref + vj) / psi2g with each
+  // state's multideterminant velocity from its own Y
+  void grad_guiding(int iel, int iflag_move, double *vd) {
+    const int iab = iel < s->nup ? 0 : 1, ns = s->nstates;
+    const double *ps = iflag_move == 1 ? psid_cur.data() : psidn_st.data();
+    vector<double> ys((size_t)O * std::max(nel_of(iab), 1));
+    double vref[3], vjv[3];
+    const double *b;
+    const double *sl;
+    const double *aav;
+    if (iflag_move == 1) {
+      double *dt = dorb_tmp.data();
+      for (int k = 0; k < 3; k++)
+        for (int iorb = 0; iorb < O; iorb++) dt[iorb + O * k] = dorb[iorb + O * (iel + N * k)];
+      ref_grad(iel, slmi[iab].data(), dt, O, vref);
+      b = dt;
+      sl = slmi[iab].data();
+      aav = aa[iab].data();
+      for (int k = 0; k < 3; k++) vjv[k] = vj[k + 3 * iel];
+    } else {
+      ref_grad(iel, slmin.data(), dorbn.data(), O, vref);
+      b = dorbn.data();
+      sl = slmin.data();
+      aav = aan.data();
+      for (int k = 0; k < 3; k++) vjv[k] = vjn[k + 3 * iel];
+    }
+    const double dpair = iflag_move == 1 ? detiab[0] * detiab[1] : (iab == 0 ? detn * detiab[1] : detiab[0] * detn);
+    const double psi2gi = 1.0 / psig_of(ps);
+    vd[0] = vd[1] = vd[2] = 0.0;
+    for (int i = 0; i < ns; i++) {
+      const double *cd = s->cdet_st.data() + (size_t)i * s->ndet;
+      if (iflag_move == 1)
+        compute_ymat(iab, detall[0].data(), detall[1].data(), wfmat[iab].data(), ys.data(), cd);
+      else if (iab == 0)
+        compute_ymat(0, detalln.data(), detall[1].data(), wfmatn.data(), ys.data(), cd);
+      else
+        compute_ymat(1, detall[0].data(), detalln.data(), wfmatn.data(), ys.data(), cd);
+      double vs[3];
+      md_grad(iel, b, O, dpair / ps[i], sl, aav, ys.data(), vs);
+      const double ratio = ps[i] / ps[0];
+      for (int k = 0; k < 3; k++) vd[k] = vd[k] + s->weights_g[i] * ratio * ratio * (vs[k] + vref[k] + vjv[k]);
+    }
+    for (int k = 0; k < 3; k++) vd[k] = vd[k] * psi2gi;
+  }
   void grad(int iel, int iflag_move, double *vd) {
+    if (s->iguiding > 0) {
+      grad_guiding(iel, iflag_move, vd);
+      return;
+    }
     const int iab = iel < s->nup ? 0 : 1;
     double vel[3] = {0, 0, 0};
     if (iflag_move == 1) {
@@ -1296,6 +1360,15 @@ struct Walker {
     double determ = 0.0;
     for (int k = 0; k < s->ndet; k++) determ += detalln[k] * detall[1 - iab][k] * s->cdet[k];
     psidn_md = determ;
+    if (s->iguiding > 0) {
+      psidn_st.resize(s->nstates);
+      for (int i = 0; i < s->nstates; i++) {
+        const double *cd = s->cdet_st.data() + (size_t)i * s->ndet;
+        double d = 0.0;
+        for (int k = 0; k < s->ndet; k++) d += detalln[k] * detall[1 - iab][k] * cd[k];
+        psidn_st[i] = d;
+      }
+    }
     return determ;
   }
 
@@ -1745,6 +1818,10 @@ struct Walker {
     if (!hpsi(xold.data(), psid, psij, ekin, e)) return false;
     psido = psid; psijo = psij; eold = e; ekino = ekin;
     psi2o = 2 * (std::log(std::fabs(psido)) + psijo);
+    if (s->iguiding > 0) {  // zerest after guiding (vmc/acuest.f90:273-278)
+      psid_cur = psid_st;
+      psi2o = std::log(std::fabs(psig_of(psid_cur.data()))) + 2 * (std::log(std::fabs(psido)) + psijo);
+    }
     distances(-1, xold.data());
     for (int i = 0; i < N; i++) {
       rmino[i] = 99.0e9;
@@ -1959,7 +2036,8 @@ bool Walker::metrop6() {
       } else {
         grad(i, 0, vn);
         for (int k = 0; k < 3; k++) vnew[k + 3 * i] = vn[k];
-        psi2n = std::log(std::fabs(1.0)) + 2 * (std::log(std::fabs(psidn)) + psijn);
+        const double psi2g = s->iguiding > 0 ? psig_of(psidn_st.data()) : 1.0;
+        psi2n = std::log(std::fabs(psi2g)) + 2 * (std::log(std::fabs(psidn)) + psijn);
         double fxnp = one;
         rbot = rminn[i] * deltri;
         rtop = rminn[i] * deltar;
@@ -2021,6 +2099,7 @@ bool Walker::metrop6() {
       }
       psido = psidn;
       psijo = psijn;
+      if (s->iguiding > 0) psid_cur = psidn_st;
       acc = acc + one;
       jassav(i, 0);
       detsav(i);
@@ -2037,7 +2116,13 @@ bool Walker::metrop6() {
   eold = e;
   ekino = ekin;
   psi2o = 2 * (std::log(std::fabs(psido)) + psijo);
-  double wtg_sqrt = psido / psido * std::exp(psijo - psijo) / std::sqrt(1.0);
+  double psi2g = 1.0;
+  if (s->iguiding > 0) {  // metrop6 :652-657, :732
+    psid_cur = psid_st;
+    psi2g = psig_of(psid_cur.data());
+    psi2o = std::log(std::fabs(psi2g)) + 2 * (std::log(std::fabs(psido)) + psijo);
+  }
+  double wtg_sqrt = psido / psido * std::exp(psijo - psijo) / std::sqrt(psi2g);
   double wtg = wtg_sqrt * wtg_sqrt;
   esum1 = eold;
   wsum += wtg;
@@ -2049,9 +2134,9 @@ bool Walker::metrop6() {
   ecm21 += esum1 * esum1 * wtg;
   ecum1s += eold * wtg;
   ecm21s += eold * eold * wtg;
-  // every state, reweighted to the sampled |psi_1|^2 (metrop6 :678-690, psi2g = 1)
+  // every state, reweighted to the sampled distribution (metrop6 :678-690)
   for (int st = 0; s->nstates > 1 && st < s->nstates; st++) {
-    const double ws = psid_st[st] / psid_st[0] * std::exp(psijo - psijo) / std::sqrt(1.0);
+    const double ws = psid_st[st] / psid_st[0] * std::exp(psijo - psijo) / std::sqrt(psi2g);
     const double wt = ws * ws;
     wsum_st[st] += wt;
     esum_st[st] += e_st[st] * wt;
@@ -2469,9 +2554,17 @@ void *or_sys_create(const cw_system_desc *d) {
   s->cdet.assign(d->cdet, d->cdet + d->ndet);
   s->nstates = d->nstates > 1 ? d->nstates : 1;
   s->cdet_st.assign(d->cdet, d->cdet + (size_t)s->nstates * d->ndet);
-  if (s->nstates > 1 && (d->iguiding > 0 || d->ndet < 2)) {
+  if (s->nstates > 1 && d->ndet < 2) {
     delete s;
     return nullptr;
+  }
+  s->iguiding = s->nstates > 1 ? d->iguiding : 0;
+  if (s->iguiding > 0) {
+    if (!d->weights_g) {
+      delete s;
+      return nullptr;
+    }
+    s->weights_g.assign(d->weights_g, d->weights_g + s->nstates);
   }
   s->iworbd.assign(d->iworbd, d->iworbd + d->nelec);
   s->iworbd_all.assign(d->iworbd, d->iworbd + (size_t)d->ndet * d->nelec);

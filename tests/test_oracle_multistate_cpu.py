@@ -105,3 +105,55 @@ def test_block_estimators_are_reweighted_averages(oracle_mod):
     assert ws.results_state(0)["energy"] == pytest.approx(ws.results()["energy"], rel=1e-12)
     with pytest.raises(ValueError):
         ws.results_state(3)
+
+
+def _guided(md, weights):
+    g = copy.copy(md)
+    g.iguiding = 1
+    g.weights_g = np.asarray(weights, float)
+    g._keep = []
+    return g
+
+
+def test_guiding_with_zero_weights_is_state1_walk(oracle_mod):
+    """weights (1, 0, 0): psi2g = 1 exactly, so the guided walk is the walk of
+    state 1, bitwise."""
+    md = _multistate()
+    o, xs, st = _walkers(oracle_mod, md, 4)
+    a = oracle_mod.OracleWalkers(o, xs, st.copy())
+    og = oracle_mod.OracleSystem(_guided(md, [1.0, 0.0, 0.0]))
+    b = oracle_mod.OracleWalkers(og, xs, st.copy())
+    for _ in range(2):
+        a.steps(2, 1)
+        b.steps(2, 1)
+        a.end_block()
+        b.end_block()
+    xa, ra = a.walkers()
+    xb, rb = b.walkers()
+    assert np.array_equal(ra, rb) and np.array_equal(xa, xb)
+    for s in range(3):
+        assert a.results_state(s) == b.results_state(s)
+
+
+def test_guiding_with_proportional_states_follows_state1(oracle_mod):
+    """States proportional to state 1 leave psi_g proportional to psi_1: the
+    guided walk is state 1's walk (to rounding) and every weight is 1/psi2g."""
+    from champ_b200.system import make_synthetic, rotation_expansion
+    md, _ = rotation_expansion(make_synthetic("tiny"), ROTS, extra_orbitals=4)
+    c1 = np.random.default_rng(5).normal(size=md.cdet.shape)
+    md.cdet = c1
+    md.cdet_states = np.stack([c1, 2.0 * c1, -0.5 * c1])
+    o, xs, st = _walkers(oracle_mod, md, 4)
+    a = oracle_mod.OracleWalkers(o, xs, st.copy())
+    b = oracle_mod.OracleWalkers(oracle_mod.OracleSystem(_guided(md, [1.0, 0.5, 2.0])), xs, st.copy())
+    for _ in range(2):
+        a.steps(2, 1)
+        b.steps(2, 1)
+    xa, ra = a.walkers()
+    xb, rb = b.walkers()
+    assert np.array_equal(ra, rb)
+    assert np.max(np.abs(xa - xb)) < 1e-10
+    a.end_block()
+    b.end_block()
+    for s in range(3):
+        assert b.results_state(s)["energy"] == pytest.approx(a.results_state(0)["energy"], rel=1e-10)
