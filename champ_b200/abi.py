@@ -109,6 +109,9 @@ def load_engine(path: str | None = None):
     lib.cw_device_bytes.restype = C.c_size_t
     lib.cw_results_state.argtypes = [V, C.c_int, _dp]
     lib.cw_state_energies.argtypes = [V, _dp, _dp]
+    lib.cw_opt_ci.argtypes = [V, C.c_int, C.c_int]
+    lib.cw_opt_ci_sums.argtypes = [V, _dp, _dp, _dp, _dp]
+    lib.cw_ci_o.argtypes = [V, _dp]
     lib.cw_profile.argtypes = [V, C.c_int]
     lib.cw_profile.restype = C.c_int
     lib.cw_stage_times.argtypes = [V, _dp, C.POINTER(C.c_long)]
@@ -134,7 +137,8 @@ def load_engine(path: str | None = None):
     for f in ("cw_dmc_set_tmoves", "cw_dmc_counts", "cw_checkpoint", "cw_restore", "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
               "cw_rng_states", "cw_sites", "cw_sync", "cw_set_walkers", "cw_get_walkers", "cw_vmc_steps", "cw_end_block",
               "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow", "cw_slater",
-              "cw_get_sums", "cw_get_state", "cw_results_state", "cw_state_energies"):
+              "cw_get_sums", "cw_get_state", "cw_results_state", "cw_state_energies", "cw_opt_ci",
+              "cw_opt_ci_sums", "cw_ci_o"):
         getattr(lib, f).restype = C.c_int
     if path is None:
         _engine = lib
@@ -148,7 +152,7 @@ EXPORTED_SYMBOLS = [
     "cw_launches", "cw_profile", "cw_stage_times", "cw_fma_peak", "cw_orbitals_noalloc",
     "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
     "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore", "cw_dmc_set_tmoves", "cw_dmc_counts",
-    "cw_device_bytes", "cw_results_state", "cw_state_energies",
+    "cw_device_bytes", "cw_results_state", "cw_state_energies", "cw_opt_ci", "cw_opt_ci_sums", "cw_ci_o",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

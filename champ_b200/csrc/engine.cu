@@ -69,6 +69,14 @@ struct cw_ctx {
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
   std::unordered_map<void *, size_t> alloc_bytes;
   double *bocc = nullptr;  // [nmax][K] coefficients of the occupied orbitals (c~ GEMM)
+  // CI-coefficient derivatives for optimisation (optci / SR sums)
+  double *md_sgn = nullptr;                       // [ndet] orbital-order signs
+  bool opt_ci = false, opt_oo = false;
+  int opt_w = 0;
+  double *ci_o = nullptr, *ci_ot = nullptr;       // [W][ndet], [ndet][W]
+  double *sr_o = nullptr, *sr_eo = nullptr, *sr_oo = nullptr, *oo_tmp = nullptr;
+  double sr_w = 0;
+  std::vector<void *> opt_allocs;
   int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
@@ -359,7 +367,8 @@ int nord_attrs(cw_ctx *c) {
 // class), and for every determinant the unique index of each spin part
 // (-1: the same as the reference).
 int md_define(cw_ctx *c, const cw_system_desc *d, std::vector<int> &exc, std::vector<int> &kw,
-              std::vector<double> &cdet, int nuniq[2], int ivirt[2], int iactv[2], int &numax) {
+              std::vector<double> &cdet, int nuniq[2], int ivirt[2], int iactv[2], int &numax,
+              std::vector<double> &sgn) {
   const int N = d->nelec, nd = d->ndet, nup = d->nup, ndn = N - nup;
   auto IW = [&](int k, int i) { return d->iworbd[(size_t)k * N + i]; };
   for (size_t t = 0; t < (size_t)nd * N; t++)
@@ -367,6 +376,7 @@ int md_define(cw_ctx *c, const cw_system_desc *d, std::vector<int> &exc, std::ve
   std::vector<int> numrep((size_t)nd * 2, 0), irc((size_t)nd * 2 * N, 0), iro((size_t)nd * 2 * N, 0);
   const int ns = d->nstates > 1 ? d->nstates : 1;
   cdet.assign(d->cdet, d->cdet + (size_t)ns * nd);  // [nstates][ndet]
+  sgn.assign(nd, 1.0);
   for (int k = 1; k < nd; k++) {
     int itot = 0;
     for (int iab = 0; iab < 2; iab++) {
@@ -398,8 +408,10 @@ int md_define(cw_ctx *c, const cw_system_desc *d, std::vector<int> &exc, std::ve
               itot++;
             }
     }
-    if (itot % 2)
+    if (itot % 2) {
+      sgn[k] = -1.0;
       for (int st = 0; st < ns; st++) cdet[(size_t)st * nd + k] = -cdet[(size_t)st * nd + k];
+    }
   }
   kw.assign((size_t)nd * 2, -1);
   std::vector<std::vector<int>> order(2);
@@ -551,6 +563,24 @@ int md_after_commit(cw_ctx *c, int iel) {
 }
 
 // Full local energy of every walker (hpsi).  mode 1 also adds metrop6's sums.
+// CI derivatives of every walker after a sweep's hpsi and the SR sums
+int opt_ci_accum(cw_ctx *c) {
+  const int W = c->W, nd = c->h.ndet;
+  k_md_ci_o<<<W, 128, 0, c->stream>>>(c->st, c->md, c->mdt, c->md_sgn, c->ci_o, c->ci_ot);
+  LCHK("k_md_ci_o");
+  k_sr_accum<<<(nd + 127) / 128, 128, 0, c->stream>>>(c->st, c->ci_o, c->sr_o, c->sr_eo);
+  LCHK("k_sr_accum");
+  if (c->opt_oo) {
+    // sum_w O O^T as one GEMM over the walkers: [nd x W] x [W x nd]
+    dgemm(c->stream, nd, nd, W, c->ci_ot, c->ci_o, c->oo_tmp);
+    const size_t n = (size_t)nd * nd;
+    k_add_inplace<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->sr_oo, c->oo_tmp, n);
+    LCHK("k_add_inplace");
+  }
+  c->sr_w += W;
+  return CW_OK;
+}
+
 int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullptr) {
   const CSys &h = c->h;
   const int W = c->W, N = h.N, M = h.M;
@@ -657,6 +687,8 @@ void free_dmc(cw_ctx *c) {
 
 int alloc_walkers(cw_ctx *c, int W) {
   free_dmc(c);
+  free_list(c, c->opt_allocs);  // derivative buffers are sized for the old population
+  c->opt_ci = c->opt_oo = false;
   free_list(c, c->w_allocs);
   const CSys &h = c->h;
   const int N = h.N, M = h.M, K = h.K, Oa = h.Oa, nmax = h.nmax, NQ = std::max(h.nquad, 1);
@@ -1061,9 +1093,9 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   if (d->ndet > 1) {
     // compact multideterminant tables (multideterminants_define)
     std::vector<int> exc, kw;
-    std::vector<double> cdet;
+    std::vector<double> cdet, sgn;
     int nuniq[2], ivirt[2], iactv[2], numax = 1;
-    rc = md_define(c, d, exc, kw, cdet, nuniq, ivirt, iactv, numax);
+    rc = md_define(c, d, exc, kw, cdet, nuniq, ivirt, iactv, numax, sgn);
     if (rc) return rc;
     h.ndet = d->ndet;
     for (int s2 = 0; s2 < 2; s2++) {
@@ -1081,6 +1113,8 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     CK(cudaMemcpy(dkw, kw.data(), sizeof(int) * kw.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(dcd, cdet.data(), sizeof(double) * cdet.size(), cudaMemcpyHostToDevice));
     c->mdt = MdTab{dexc, dkw, dcd, numax};
+    DALLOC(L, c->md_sgn, sgn.size());
+    CK(cudaMemcpy(c->md_sgn, sgn.data(), sizeof(double) * sgn.size(), cudaMemcpyHostToDevice));
     c->md_on = true;
     if (h.nloc > 0 && c->ecp_naov != h.K)  // the ECP block's basis-value rows must be sized
       return fail(c, CW_ERR_STATE, "ECP stage sized without multideterminant basis rows");
@@ -1131,6 +1165,7 @@ void cw_destroy(cw_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_dmc(c);
   free_list(c, c->w_allocs);
+  free_list(c, c->opt_allocs);
   free_list(c, c->sys_allocs);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1257,6 +1292,10 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
     }
     int rc = run_hpsi(c, 1);
     if (rc) return rc;
+    if (c->opt_ci) {
+      rc = opt_ci_accum(c);
+      if (rc) return rc;
+    }
     if (c->prof && c->evused > 4096) stage_collect(c);
   }
   CK(cudaEventRecord(c->ev1, c->stream));
@@ -1331,6 +1370,69 @@ int cw_results_state(cw_ctx *c, int istate, double *out) {
   out[5] = cu[3] / cu[0];
   out[6] = cu[4] / cu[0];
   out[7] = (double)c->iblk;
+  return CW_OK;
+}
+
+int cw_opt_ci(cw_ctx *c, int enable, int with_overlap) {
+  if (!c) return CW_ERR_ARG;
+  BIND(c);
+  free_list(c, c->opt_allocs);
+  c->opt_ci = c->opt_oo = false;
+  c->ci_o = c->ci_ot = c->sr_o = c->sr_eo = c->sr_oo = c->oo_tmp = nullptr;
+  c->sr_w = 0;
+  if (!enable) return CW_OK;
+  if (!c->md_on) return fail(c, CW_ERR_UNSUPPORTED, "CI derivatives need a multideterminant expansion");
+  if (c->h.nstates > 1) return fail(c, CW_ERR_UNSUPPORTED, "CI derivatives of several states are not implemented");
+  if (c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  const int W = c->W, nd = c->h.ndet;
+  if (with_overlap && (size_t)nd * nd > ((size_t)1 << 27))
+    return fail(c, CW_ERR_ARG, "overlap of %d coefficients exceeds 2^27 entries", nd);
+  auto &L = c->opt_allocs;
+  DALLOC(L, c->ci_o, (size_t)W * nd);
+  DALLOC(L, c->ci_ot, (size_t)W * nd);
+  DALLOC(L, c->sr_o, nd);
+  DALLOC(L, c->sr_eo, nd);
+  CK(cudaMemsetAsync(c->sr_o, 0, sizeof(double) * nd, c->stream));
+  CK(cudaMemsetAsync(c->sr_eo, 0, sizeof(double) * nd, c->stream));
+  if (with_overlap) {
+    DALLOC(L, c->sr_oo, (size_t)nd * nd);
+    DALLOC(L, c->oo_tmp, (size_t)nd * nd);
+    CK(cudaMemsetAsync(c->sr_oo, 0, sizeof(double) * nd * nd, c->stream));
+  }
+  c->opt_ci = true;
+  c->opt_oo = with_overlap != 0;
+  c->opt_w = W;
+  // derivatives at the current configurations (the last hpsi)
+  k_md_ci_o<<<W, 128, 0, c->stream>>>(c->st, c->md, c->mdt, c->md_sgn, c->ci_o, c->ci_ot);
+  LCHK("k_md_ci_o");
+  CK(cudaStreamSynchronize(c->stream));
+  return CW_OK;
+}
+
+int cw_ci_o(cw_ctx *c, double *out) {
+  if (!c || !out) return CW_ERR_ARG;
+  if (!c->opt_ci || c->opt_w != c->W) return fail(c, CW_ERR_STATE, "cw_opt_ci not enabled for this population");
+  BIND(c);
+  CK(cudaMemcpyAsync(out, c->ci_o, sizeof(double) * c->W * c->h.ndet, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CW_OK;
+}
+
+int cw_opt_ci_sums(cw_ctx *c, double *o, double *eo, double *oo, double *wsum) {
+  if (!c || !o || !eo || !wsum) return CW_ERR_ARG;
+  if (!c->opt_ci || c->opt_w != c->W) return fail(c, CW_ERR_STATE, "cw_opt_ci not enabled for this population");
+  if (oo && !c->opt_oo) return fail(c, CW_ERR_STATE, "overlap sums not enabled");
+  BIND(c);
+  const int nd = c->h.ndet;
+  CK(cudaMemcpyAsync(o, c->sr_o, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(eo, c->sr_eo, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream));
+  if (oo) CK(cudaMemcpyAsync(oo, c->sr_oo, sizeof(double) * nd * nd, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemsetAsync(c->sr_o, 0, sizeof(double) * nd, c->stream));
+  CK(cudaMemsetAsync(c->sr_eo, 0, sizeof(double) * nd, c->stream));
+  if (c->opt_oo) CK(cudaMemsetAsync(c->sr_oo, 0, sizeof(double) * nd * nd, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *wsum = c->sr_w;
+  c->sr_w = 0;
   return CW_OK;
 }
 

@@ -500,6 +500,45 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
   }
 }
 
+// optci_deloc (vmc/optci.f90:49-51): d ln psi / d c_k = sgn_k D_k / psi_D of
+// every determinant (sgn_k: the orbital-order sign folded into the internal
+// coefficients, so the derivative is taken for the input coefficients), in
+// both walker-major and determinant-major layouts (the latter feeds the
+// overlap GEMM).  CTA per walker.
+__global__ void k_md_ci_o(WState st, MdBuf md, MdTab tab, const double *sgn, double *o, double *ot) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const double iS = 1.0 / md.S[w];
+  for (int k = threadIdx.x; k < cs.ndet; k += blockDim.x) {
+    const int k0 = tab.kw[2 * k], k1 = tab.kw[2 * k + 1];
+    const double d0 = k0 >= 0 ? md.dd[((size_t)w * 2 + 0) * tab.numax + k0] : 1.0;
+    const double d1 = k1 >= 0 ? md.dd[((size_t)w * 2 + 1) * tab.numax + k1] : 1.0;
+    const double v = sgn[k] * (d0 * d1 * iS);
+    o[(size_t)w * cs.ndet + k] = v;
+    ot[(size_t)k * st.W + w] = v;
+  }
+}
+
+// SR sums (optwf_store's sr_o contracted per sample): sum_w O_k and
+// sum_w E_w O_k, thread per determinant, walkers in order
+__global__ void k_sr_accum(WState st, const double *o, double *sr_o, double *sr_eo) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cs.ndet) return;
+  double a = 0, b = 0;
+  for (int w = 0; w < st.W; w++) {
+    const double v = o[(size_t)w * cs.ndet + k];
+    a += v;
+    b += st.eold[w] * v;
+  }
+  sr_o[k] += a;
+  sr_eo[k] += b;
+}
+
+__global__ void k_add_inplace(double *dst, const double *src, size_t n) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] += src[t];
+}
+
 // pseudopotential B matrix: bnl[w][e][o] = sum_m P[w][e][m] coef(m, o) is
 // a GEMM launched by the host; this kernel only clears P before k_ecp
 __global__ void k_md_zero(double *p, size_t n) {

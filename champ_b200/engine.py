@@ -154,6 +154,24 @@ class Engine:
         self._check(self.lib.cw_state_energies(self.h, dptr(e), dptr(p)), "cw_state_energies")
         return e, p
 
+    # -- wave-function optimisation (CI coefficients) ----------------------
+    def opt_ci(self, enable: bool = True, overlap: bool = True):
+        self._check(self.lib.cw_opt_ci(self.h, 1 if enable else 0, 1 if overlap else 0), "cw_opt_ci")
+
+    def ci_o(self):
+        nd = self.system.iworbd.shape[0]
+        out = np.zeros((self.W, nd))
+        self._check(self.lib.cw_ci_o(self.h, dptr(out)), "cw_ci_o")
+        return out
+
+    def opt_ci_sums(self, overlap: bool = True):
+        nd = self.system.iworbd.shape[0]
+        o, eo, w = np.zeros(nd), np.zeros(nd), np.zeros(1)
+        oo = np.zeros((nd, nd)) if overlap else None
+        self._check(self.lib.cw_opt_ci_sums(self.h, dptr(o), dptr(eo), dptr(oo) if overlap else None, dptr(w)),
+                    "cw_opt_ci_sums")
+        return dict(o=o, eo=eo, oo=oo, wsum=float(w[0]))
+
     def sums(self):
         out = np.zeros((self.W, 5))
         self._check(self.lib.cw_get_sums(self.h, dptr(out)), "cw_get_sums")

@@ -173,6 +173,21 @@ int cw_results(cw_ctx *ctx, double *out);
  * the sampled state, cw_results).  CW_ERR_ARG for istate outside [0, nstates). */
 int cw_results_state(cw_ctx *ctx, int istate, double *out);
 
+/* Wave-function optimisation: derivatives of ln psi with respect to the CI
+ * coefficients (optci_deloc's ci_o, vmc/optci.f90:49-51, taken for the
+ * coefficients as given in cw_system_desc, i.e. with the orbital-order sign
+ * of multideterminants_define applied) and the stochastic-reconfiguration
+ * sums of optwf_store (vmc/optwf_handle_wf.f90:1465) over the samples of
+ * every VMC sweep: sum O_k, sum E_L O_k and, with with_overlap, the overlap
+ * sum O_k O_l (one FP64 GEMM over the walkers).  Needs a multideterminant
+ * expansion with one state; enable after cw_set_walkers (a new population
+ * disables it).  cw_opt_ci_sums copies the sums (o, eo [ndet], oo
+ * [ndet][ndet] or NULL, wsum = number of samples) and resets them;
+ * cw_ci_o gives the per-walker derivatives of the last hpsi, [nwalk][ndet]. */
+int cw_opt_ci(cw_ctx *ctx, int enable, int with_overlap);
+int cw_opt_ci_sums(cw_ctx *ctx, double *o, double *eo, double *oo, double *wsum);
+int cw_ci_o(cw_ctx *ctx, double *out);
+
 /* Per-walker local energies and psi_D of every state from the last hpsi:
  * energy, psid [nwalk][nstates]. */
 int cw_state_energies(cw_ctx *ctx, double *energy, double *psid);

@@ -71,6 +71,7 @@ struct Sys {
   int iguiding = 0;            // > 0: sample the guiding function (mstates_ctrl)
   vector<double> weights_g;    // [nstates] (mstates3; anormo = 1)
   vector<double> cdet_st;      // [nstates][ndet], sign-adjusted like cdet; row 0 = cdet
+  vector<double> detsign;      // [ndet] +-1: orbital-order sign folded into cdet
   vector<int> iworbd;  // iworbd(j) for kref=1, 1-based orbital
   vector<int> iworbd_all;      // [ndet][N] 1-based, reordered as multideterminants_define does
   // compact multideterminant tables per spin (multideterminants_define,
@@ -173,6 +174,7 @@ bool multideterminants_define(Sys &s) {
       itot[k] += iphase;
     }
     if (itot[k] % 2) {
+      s.detsign[k] = -1.0;
       s.cdet[k] = -s.cdet[k];
       for (int st = 0; st < s.nstates; st++) s.cdet_st[(size_t)st * nd + k] = -s.cdet_st[(size_t)st * nd + k];
     }
@@ -547,6 +549,11 @@ struct Walker {
   // configuration, and psi2g = sum_i w_i (psi_i/psi_1)^2 at the current one
   vector<double> psid_cur, psidn_st;
   double psi2g_o = 1.0;
+  // CI-coefficient derivatives of the last hpsi (optci_deloc's ci_o, taken
+  // with respect to the input coefficients) and the SR sums of the sweeps
+  vector<double> ci_o, sr_o, sr_eo, sr_oo;
+  double sr_w = 0;
+  bool opt_ci = false;
   double ecum, ecm2, wcum, pecum, tpbcum, pecm2, tpbcm2, ecum1, ecm21, ecum1s, ecm21s;
   Rng rng;
   bool singular = false;
@@ -1659,6 +1666,10 @@ struct Walker {
     if (s->ndn > 0) compute_ymat(1, detall[0].data(), detall[1].data(), wfmat[1].data(), ymat[1].data());
     psid = 0.0;
     for (int k = 0; k < s->ndet; k++) psid = psid + detall[0][k] * detall[1][k] * s->cdet[k];
+    // optci_deloc (vmc/optci.f90:49-51): ciprim = D_k / psid, here times the
+    // orbital-order sign so that it is d ln psi / d c_k of the input coefficients
+    ci_o.resize(s->ndet);
+    for (int k = 0; k < s->ndet; k++) ci_o[k] = s->detsign[k] * (detall[0][k] * detall[1][k] / psid);
     denergy = 0;
     dekin = 0;
     for (int iab = 0; iab < 2; iab++) {
@@ -2143,6 +2154,21 @@ bool Walker::metrop6() {
     pesum_st[st] += (e_st[st] - ekin_st[st]) * wt;
     tpbsum_st[st] += ekin_st[st] * wt;
   }
+  // SR sums of the CI derivatives (optwf_store's sr_o contracted per sample)
+  if (opt_ci) {
+    const int nd = s->ndet;
+    if (sr_o.empty()) {
+      sr_o.assign(nd, 0.0);
+      sr_eo.assign(nd, 0.0);
+      sr_oo.assign((size_t)nd * nd, 0.0);
+    }
+    sr_w += wtg;
+    for (int k = 0; k < nd; k++) {
+      sr_o[k] += wtg * ci_o[k];
+      sr_eo[k] += wtg * eold * ci_o[k];
+      for (int l = 0; l < nd; l++) sr_oo[(size_t)k * nd + l] += wtg * ci_o[k] * ci_o[l];
+    }
+  }
   return true;
 }
 
@@ -2552,6 +2578,7 @@ void *or_sys_create(const cw_system_desc *d) {
   s->K = d->nbasis; s->O = d->norb; s->ndet = d->ndet;
   s->coef.assign(d->coef, d->coef + (size_t)d->nbasis * d->norb);
   s->cdet.assign(d->cdet, d->cdet + d->ndet);
+  s->detsign.assign(d->ndet, 1.0);
   s->nstates = d->nstates > 1 ? d->nstates : 1;
   s->cdet_st.assign(d->cdet, d->cdet + (size_t)s->nstates * d->ndet);
   if (s->nstates > 1 && d->ndet < 2) {
@@ -3011,6 +3038,46 @@ void or_state_energies(void *wsp, double *e, double *psid) {
       e[k * ns + st] = ns > 1 ? w.e_st[st] : w.eold;
       psid[k * ns + st] = ns > 1 ? w.psid_st[st] : w.psido;
     }
+}
+
+void or_opt_ci(void *wsp, int enable) {
+  Walkers *ws = (Walkers *)wsp;
+  for (Walker &w : ws->w) {
+    w.opt_ci = enable != 0;
+    w.sr_o.clear(); w.sr_eo.clear(); w.sr_oo.clear();
+    w.sr_w = 0;
+  }
+}
+
+void or_ci_o(void *wsp, double *out) {
+  Walkers *ws = (Walkers *)wsp;
+  const int nd = ws->s->ndet;
+  for (size_t k = 0; k < ws->w.size(); k++)
+    for (int j = 0; j < nd; j++) out[k * nd + j] = j < (int)ws->w[k].ci_o.size() ? ws->w[k].ci_o[j] : 0.0;
+}
+
+void or_opt_ci_sums(void *wsp, double *o, double *eo, double *oo, double *wsum) {
+  // the SR sums of all walkers (ranks) since the last call, in walker order
+  Walkers *ws = (Walkers *)wsp;
+  const int nd = ws->s->ndet;
+  std::fill(o, o + nd, 0.0);
+  std::fill(eo, eo + nd, 0.0);
+  if (oo) std::fill(oo, oo + (size_t)nd * nd, 0.0);
+  *wsum = 0;
+  for (Walker &w : ws->w) {
+    if (w.sr_o.empty()) continue;
+    for (int k = 0; k < nd; k++) {
+      o[k] += w.sr_o[k];
+      eo[k] += w.sr_eo[k];
+    }
+    if (oo)
+      for (size_t t = 0; t < (size_t)nd * nd; t++) oo[t] += w.sr_oo[t];
+    *wsum += w.sr_w;
+    std::fill(w.sr_o.begin(), w.sr_o.end(), 0.0);
+    std::fill(w.sr_eo.begin(), w.sr_eo.end(), 0.0);
+    std::fill(w.sr_oo.begin(), w.sr_oo.end(), 0.0);
+    w.sr_w = 0;
+  }
 }
 
 void or_get_walkers(void *wsp, double *x, uint64_t *rng) {

@@ -53,6 +53,9 @@ int or_zerest(void *ws);
 void or_end_block(void *ws, double *block_energy);
 void or_results(void *ws, double *out);
 int or_results_state(void *ws, int istate, double *out);
+void or_opt_ci(void *ws, int enable);
+void or_ci_o(void *ws, double *out);
+void or_opt_ci_sums(void *ws, double *o, double *eo, double *oo, double *wsum);
 void or_state_energies(void *ws, double *e, double *psid);
 void or_get_walkers(void *ws, double *x, uint64_t *rng);
 void or_get_sums(void *ws, double *out);

@@ -59,6 +59,9 @@ def lib():
         L.or_results_state.argtypes = [V, C.c_int, _dp]
         L.or_results_state.restype = C.c_int
         L.or_state_energies.argtypes = [V, _dp, _dp]
+        L.or_opt_ci.argtypes = [V, C.c_int]
+        L.or_ci_o.argtypes = [V, _dp]
+        L.or_opt_ci_sums.argtypes = [V, _dp, _dp, _dp, _dp]
         L.or_get_walkers.argtypes = [V, _dp, _u64]
         L.or_get_sums.argtypes = [V, _dp]
         L.or_get_state.argtypes = [V, _dp, _dp, _dp]
@@ -189,6 +192,21 @@ class OracleWalkers:
         p = np.zeros((self.W, nstates))
         lib().or_state_energies(self.h, dp(e), dp(p))
         return e, p
+
+    def opt_ci(self, enable=True):
+        lib().or_opt_ci(self.h, 1 if enable else 0)
+
+    def ci_o(self):
+        nd = self.osys.system.iworbd.shape[0]
+        out = np.zeros((self.W, nd))
+        lib().or_ci_o(self.h, dp(out))
+        return out
+
+    def opt_ci_sums(self):
+        nd = self.osys.system.iworbd.shape[0]
+        o, eo, oo, w = np.zeros(nd), np.zeros(nd), np.zeros((nd, nd)), np.zeros(1)
+        lib().or_opt_ci_sums(self.h, dp(o), dp(eo), dp(oo), dp(w))
+        return dict(o=o, eo=eo, oo=oo, wsum=float(w[0]))
 
     def walkers(self):
         x = np.zeros((self.W, self.osys.N, 3))
