@@ -815,6 +815,8 @@ int alloc_walkers(cw_ctx *c, int W) {
     }
   }
   DALLOC(L, b.entab, (size_t)W * M * N * kEnFields);
+  b.entabf = nullptr;
+  if (c->mixed) DALLOC(L, b.entabf, (size_t)W * M * N * kEnFields);
   CK(cudaMemsetAsync(s.status, 0, sizeof(int) * W, c->stream));
   CK(cudaMemsetAsync(s.sums, 0, sizeof(double) * W * 8, c->stream));
   c->W = W;

@@ -11,6 +11,8 @@
 //                    vmc/nonloc.f90:5, nonlocj_quad4 :656)
 //   k_energy         E_L assembly (vmc/hpsi.f90:176-246) and metrop6 sums
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace cw {
@@ -26,6 +28,7 @@ struct HBuf {
   double *orball;   // [rows][Oa] chunk orbitals
   double *ctilde;   // [W][N][K]
   double *entab;    // [W][5][M][N] e-n table of the full Jastrow (k_jastrow_full)
+  float *entabf;    // [W][5][M][N] its FP32 copy, partner side of the mixed path (null in FP64)
   int chunk;        // electrons per chunk
   float *phi_hi, *phi_lo;  // mixed precision: [rows][kp] split chunk basis (null in FP64)
   int kp;
@@ -99,6 +102,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) k_jastrow_full(WS
   __syncthreads();
   const double kap = cs.scalek, asym = cs.asymp_r;
   double *tab = hb.entab + (size_t)w * kEnFields * MN;
+  float *tabf = hb.entabf ? hb.entabf + (size_t)w * kEnFields * MN : nullptr;
   double *fso = st.fso + (size_t)w * N * N;
   double *fij0 = st.fijo + ((size_t)w * 3 + 0) * N * N;
   double *fij1 = st.fijo + ((size_t)w * 3 + 1) * N * N;
@@ -118,6 +122,13 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) k_jastrow_full(WS
       tab[2 * MN + t] = -kap * dd2;
       tab[3 * MN + t] = -kap * dd1 / r;
       tab[4 * MN + t] = r2;
+      if (sizeof(T) == 4 && tabf) {
+        tabf[t] = (float)rr;
+        tabf[MN + t] = (float)(-kap * dd1);
+        tabf[2 * MN + t] = (float)(-kap * dd2);
+        tabf[3 * MN + t] = (float)(-kap * dd1 / r);
+        tabf[4 * MN + t] = (float)r2;
+      }
       st.enm[(size_t)w * 2 * MN + t] = rr;
       st.enm[((size_t)w * 2 + 1) * MN + t] = dd1 / r;
       if (rr == asym) continue;
@@ -186,11 +197,13 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) k_jastrow_full(WS
         const T z = 1 - kT * u, du1 = -kT * dd1, du2 = -kT * dd2, du1r = du1 * irijT;
         const T *Brow = sB + (size_t)row * M * 4 * NB;
         const double *Irow = sI + (size_t)row * M * 8;
-        const double *tj = tab + j;
-        // the partner's table entries of the next centre are loaded one iteration ahead
-        double nr = tj[0], nA = tj[MN], nB = tj[2 * MN], nG = tj[3 * MN], nS = tj[4 * MN];
+        // the partner's table entries of the next centre are loaded one iteration
+        // ahead; the mixed path reads them from the FP32 copy
+        using TT = typename std::conditional<sizeof(T) == 4, float, double>::type;
+        const TT *tj = (sizeof(T) == 4 ? (const TT *)(const void *)tabf : (const TT *)(const void *)tab) + j;
+        TT nr = tj[0], nA = tj[MN], nB = tj[2 * MN], nG = tj[3 * MN], nS = tj[4 * MN];
         for (int ic = 0; ic < M; ic++) {
-          const double rrj = nr;
+          const TT rrj = nr;
           const T Aj = (T)nA, Bj = (T)nB, Gj = (T)nG, Sj = (T)nS;
           if (ic + 1 < M) {
             const int o = (ic + 1) * N;
@@ -198,9 +211,9 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) k_jastrow_full(WS
           }
           const double *qi = Irow + ic * 8;
           const double rri = qi[0];
-          if (rri == asym && rrj == asym) continue;
+          if (rri == asym && rrj == (TT)asym) continue;
           const T Ai = (T)qi[1], Bi = (T)qi[2], Gi = (T)qi[3], Si = (T)qi[4];
-          const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 4 * NB, T(1 - kap * rrj), z);
+          const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 4 * NB, T(1 - (TT)kap * rrj), z);
           const T dS = Si - Sj;
           const T fuu = e.fuu * du1 * du1 + e.fu * du2;
           const T fu = e.fu * du1r;
