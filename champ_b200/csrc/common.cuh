@@ -71,6 +71,12 @@ struct GSys {
   const double *coefT;            // [K][Oa]  (active orbitals)
   const int *slot_orb;            // [2][nmax] active-orbital index of Slater column j, spin s
   const int4 *ao;                 // [K] per AO: centre, radial function (0-based), atom type, Slm index
+  // per AO, read with the AO index (lanes of a warp take consecutive AOs, so
+  // these loads coalesce where indexing the constant block by type would
+  // serialise): radial table offset, grid points of the type, packed Slm
+  // exponents (a | b << 8 | c << 16); Slm constant and rmaxwf
+  const int4 *aox;                // [K]
+  const double2 *aok;             // [K]
 };
 
 // ---------------------------------------------------------------------------
@@ -982,14 +988,16 @@ __device__ __forceinline__ void warp_basis_prepass(const GSys &g, const double *
 template <int IDER, typename Store>
 __device__ __forceinline__ void warp_basis_ao(const GSys &g, const double *rec, int m, Store out) {
   const int4 a4 = __ldg(g.ao + m);
-  const int ic = a4.x, irb = a4.y, it = a4.z, l = a4.w;
+  const int4 ax = __ldg(g.aox + m);
+  const double2 ak = __ldg(g.aok + m);
+  const int ic = a4.x, irb = a4.y, it = a4.z;
   const double *q = rec + (size_t)ic * kCenRec;
   const double r = q[3], ri = q[4];
   const int jx = (int)q[5];
   double w0 = 0, w1 = 0, w2 = 0;
-  if (r <= cs.rmaxwf[it * CW_MAX_RWF + irb]) {
-    if (jx >= 1 && jx < cs.nr[it]) {
-      const size_t tb = (size_t)(irb + cs.mrwf * it) * cs.mpts;
+  if (r <= ak.y) {
+    if (jx >= 1 && jx < ax.y) {
+      const size_t tb = (size_t)ax.x;
       const double y0 = __ldg(g.rwf + tb + jx - 1), y1 = __ldg(g.rwf + tb + jx);
       const double d0 = __ldg(g.d2rwf + tb + jx - 1), d1 = __ldg(g.d2rwf + tb + jx);
       w0 = q[6] * y0 + q[7] * y1 + q[8] * d0 + q[9] * d1;
@@ -1012,8 +1020,8 @@ __device__ __forceinline__ void warp_basis_ao(const GSys &g, const double *rec, 
       w2 = -ae[1] * w1;
     }
   }
-  const int ea = cs.slm_a[l], eb = cs.slm_b[l], ec = cs.slm_c[l];
-  const double k = cs.slm_k[l];
+  const int ea = ax.z & 255, eb = (ax.z >> 8) & 255, ec = ax.z >> 16;
+  const double k = ak.x;
   const double *X = q + 13, *Y = q + 18, *Z = q + 23;
   const double y = k * X[ea] * Y[eb] * Z[ec];
   out(m, 0, y * w0);

@@ -1065,6 +1065,22 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   DALLOC(L, aodev, aot.size());
   CK(cudaMemcpy(aodev, aot.data(), aot.size() * sizeof(int4), cudaMemcpyHostToDevice));
   c->g.ao = aodev;
+  // per-AO radial-table offset, grid size, Slm exponents / constant, rmaxwf
+  std::vector<int4> aox(d->nbasis);
+  std::vector<double2> aok(d->nbasis);
+  for (int mm = 0; mm < d->nbasis; mm++) {
+    const int irb = aot[mm].y, it = aot[mm].z, l = aot[mm].w;
+    aox[mm] = make_int4((irb + h.mrwf * it) * h.mpts, h.nr[it], h.slm_a[l] | (h.slm_b[l] << 8) | (h.slm_c[l] << 16), 0);
+    aok[mm] = make_double2(h.slm_k[l], h.rmaxwf[it * CW_MAX_RWF + irb]);
+  }
+  int4 *aoxdev;
+  double2 *aokdev;
+  DALLOC(L, aoxdev, aox.size());
+  DALLOC(L, aokdev, aok.size());
+  CK(cudaMemcpy(aoxdev, aox.data(), aox.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(aokdev, aok.data(), aok.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  c->g.aox = aoxdev;
+  c->g.aok = aokdev;
   // dynamic shared memory sizes
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
@@ -1263,7 +1279,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
     for (int i = 0; i < h.N; i++) {
       if (int rc = md_before_propose(c, i)) return rc;
       stage_begin(c, CW_ST_PROPOSE);
-      k_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, i);
+      k_propose<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, i);
       stage_end(c);
       LCHK("k_propose");
       stage_begin(c, CW_ST_JASTROW_MOVE);
@@ -1283,7 +1299,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
       }
       if (int rc = md_after_lcao(c, i)) return rc;
       stage_begin(c, CW_ST_ACCEPT);
-      k_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, i);
+      k_decide<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
       stage_end(c);
       LCHK("k_decide");
       stage_begin(c, CW_ST_COMMIT);

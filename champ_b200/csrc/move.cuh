@@ -83,50 +83,53 @@ __device__ __forceinline__ bool radial_candidate(DRng &r, double rmin, double de
   return ratio > r.uniform();
 }
 
-// The radial rejection loop with the reference's draw order.  Each lane first
-// tries kRadialSerial candidates of its own walker; the walkers still pending
-// are then taken one at a time by the whole warp, lane L testing candidate L
-// of the next 32 (its copy of the stream advanced by 2L draws).  The first
-// accepted candidate, and the stream state after it, are those of the serial
-// loop.  Every lane of the warp must call it.  Returns true when the loop gave
-// up (more than ~10^6 candidates: a non-finite walker).
-constexpr int kRadialSerial = 16;
-__device__ __noinline__ bool radial_sample(DRng &rng, bool live, double rmin, double deltar, double deltri,
-                                           double co, double zeta, double fmx, double &rtry, double &top) {
-  bool done = !live, gave_up = false;
-  for (int k = 0; k < kRadialSerial && !done; k++) done = radial_candidate(rng, rmin, deltar, deltri, co, zeta, fmx, rtry, top);
-  const int lane = threadIdx.x & 31;
-  int rounds = 0;
-  unsigned pend = __ballot_sync(0xffffffffu, !done);
-  while (pend) {
-    const int p = __ffs(pend) - 1;
-    DRng r;
-    r.s0 = __shfl_sync(0xffffffffu, rng.s0, p);
-    r.s1 = __shfl_sync(0xffffffffu, rng.s1, p);
-    r.s2 = __shfl_sync(0xffffffffu, rng.s2, p);
-    r.s3 = __shfl_sync(0xffffffffu, rng.s3, p);
-    const double rm = __shfl_sync(0xffffffffu, rmin, p), cp = __shfl_sync(0xffffffffu, co, p);
-    const double zp = __shfl_sync(0xffffffffu, zeta, p), fp = __shfl_sync(0xffffffffu, fmx, p);
-    for (int k = 0; k < 2 * lane; k++) r.next();
+// Lanes per walker in the proposal and decision kernels: the serial geometry
+// is evaluated identically by the G lanes of a walker's group, the dot
+// products and the radial candidates are spread over them.
+constexpr int kMoveGroup = 8;
+
+// group-wide sum over the kMoveGroup lanes of a walker (only the group's
+// lanes take part: other groups of the warp may have left)
+__device__ __forceinline__ double group_sum(double v) {
+  const unsigned gm = ((1u << kMoveGroup) - 1) << ((threadIdx.x & 31) & ~(kMoveGroup - 1));
+#pragma unroll
+  for (int o = kMoveGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o, kMoveGroup);
+  return v;
+}
+
+// The radial rejection loop with the reference's draw order, for the walker
+// of each group of kMoveGroup lanes: every lane of the group holds the
+// walker's stream; in each round lane g of the group tests candidate g of the
+// next kMoveGroup (its copy of the stream advanced by 2g draws).  The first
+// accepted candidate and the stream state after it are those of the serial
+// loop, and every lane of the group ends with them.  Every lane of the warp
+// must call it (the rounds continue until every group of the warp is done).
+// Returns true for a group that gave up (more than ~10^6 candidates).
+__device__ __noinline__ bool radial_sample_group(DRng &rng, double rmin, double deltar, double deltri, double co,
+                                                 double zeta, double fmx, double &rtry, double &top) {
+  const int lane = threadIdx.x & 31, g = lane & (kMoveGroup - 1), base = lane - g;
+  bool done = false, gave_up = false;
+  for (int rounds = 0; __any_sync(0xffffffffu, !done); rounds++) {
+    DRng r = rng;
+    for (int k = 0; k < 2 * g; k++) r.next();
     double rt, tp;
-    const bool ok = radial_candidate(r, rm, deltar, deltri, cp, zp, fp, rt, tp);
-    const unsigned am = __ballot_sync(0xffffffffu, ok);
-    const int ks = am ? __ffs(am) - 1 : 31;
+    const bool ok = !done && radial_candidate(r, rmin, deltar, deltri, co, zeta, fmx, rt, tp);
+    const unsigned am = (__ballot_sync(0xffffffffu, ok) >> base) & ((1u << kMoveGroup) - 1);
+    const int ks = base + (am ? __ffs(am) - 1 : kMoveGroup - 1);
     const uint64_t n0 = __shfl_sync(0xffffffffu, r.s0, ks), n1 = __shfl_sync(0xffffffffu, r.s1, ks);
     const uint64_t n2 = __shfl_sync(0xffffffffu, r.s2, ks), n3 = __shfl_sync(0xffffffffu, r.s3, ks);
     const double rtk = __shfl_sync(0xffffffffu, rt, ks), tpk = __shfl_sync(0xffffffffu, tp, ks);
-    if (lane == p) {
+    if (!done) {
       rng.s0 = n0; rng.s1 = n1; rng.s2 = n2; rng.s3 = n3;
       if (am) {
         rtry = rtk;
         top = tpk;
         done = true;
-      } else if (++rounds > 32768) {
+      } else if (rounds > (1 << 20) / kMoveGroup) {
         gave_up = true;
         done = true;
       }
     }
-    pend = __ballot_sync(0xffffffffu, !done);
   }
   return gave_up;
 }
@@ -137,17 +140,20 @@ __device__ __forceinline__ void spin_of(int iel, int &iab, int &nel, int &ish) {
 }
 
 // ---------------------------------------------------------------------------
-// Proposal: thread per walker (the sampling is a serial chain of dependent
-// FP64 operations; 32 walkers share a warp instead of one).  The drift at the
-// old position is compute_determinante_grad iflag_move=1: slmi column · dorb
-// + vj.
+// Proposal: kMoveGroup lanes per walker.  The drift at the old position
+// (compute_determinante_grad iflag_move=1: slmi column . dorb + vj) is a dot
+// product over the group; the accelerated-Metropolis geometry is a serial
+// chain that the group's lanes evaluate identically; the radial rejection
+// loop is cooperative within the group.  The group's lane 0 stores.
 // ---------------------------------------------------------------------------
-__global__ void k_propose(WState st, MoveBuf mb, int iel) {
-  // Every lane runs to the end (the radial sampling below is warp-cooperative);
-  // lanes past the population mirror the last walker and store nothing.
-  const int wt = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_propose(WState st, MoveBuf mb, int iel) {
+  // Every lane runs to the end (the radial sampling is cooperative across the
+  // warp); groups past the population mirror the last walker and store nothing.
+  const int gl = threadIdx.x & (kMoveGroup - 1);
+  const int wt = (blockIdx.x * blockDim.x + threadIdx.x) / kMoveGroup;
   const bool live = wt < st.W;
   const int w = live ? wt : st.W - 1;
+  const int lane = live ? gl : 1;  // lane 0 of a live group stores
   const int N = cs.N, nmax = cs.nmax;
   int iab, nel, ish;
   spin_of(iel, iab, nel, ish);
@@ -157,12 +163,15 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   const double *d1p = st.dorbs + (((size_t)w * 3 + 1) * N + iel) * nmax;
   const double *d2p = st.dorbs + (((size_t)w * 3 + 2) * N + iel) * nmax;
   double g0 = 0, g1 = 0, g2 = 0;
-  for (int j = 0; j < nel; j++) {
+  for (int j = gl; j < nel; j += kMoveGroup) {
     const double s = sl[j];
     g0 += s * d0p[j];
     g1 += s * d1p[j];
     g2 += s * d2p[j];
   }
+  g0 = group_sum(g0);
+  g1 = group_sum(g1);
+  g2 = group_sum(g2);
 
   const double zero = 0, one = 1, two = 2, four = 4, half = 0.5, d3b2 = 1.5, eps = 1.0e-10;
   const double deltar = cs.deltar, deltri = one / deltar, fbias = cs.fbias;
@@ -180,7 +189,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   double rv[3];
   for (int k = 0; k < 3; k++) rv[k] = st.rvmino[((size_t)w * 3 + k) * N + iel];
   const double rmin = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
-  if (live) st.rmino[(size_t)w * N + iel] = rmin;
+  if (lane == 0) st.rmino[(size_t)w * N + iel] = rmin;
   double rbot = rmin * deltri, rtop = rmin * deltar;
   double voldr = zero;
   for (int ic = 0; ic < 3; ic++) voldr += vo[ic] * rv[ic];
@@ -228,7 +237,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   }
   double bot = sqrt(rmin) * fabs(one + co * rmin) * exp(-zeta * rmin);
   double rtry, top;
-  if (radial_sample(rng, live, rmin, deltar, deltri, co, zeta, fmx, rtry, top) && live) st.status[w] |= 4;
+  if (radial_sample_group(rng, rmin, deltar, deltri, co, zeta, fmx, rtry, top) && lane == 0) st.status[w] |= 4;
   fxop = fxop * top / bot;
   double areao = t_area_d(zeta, co, rbot, rtop, bot);
   double raver = half * (rmin + rtry);
@@ -246,7 +255,10 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
     double cosphi = cos(phitry);
     top = one + term * cosphi;
     if (top > rng.uniform() * fmx) break;
-    if (guard > 1000000) { st.status[w] |= 4; break; }
+    if (guard > 1000000) {
+      if (lane == 0) st.status[w] |= 4;
+      break;
+    }
   }
   fxop = fxop * top;
   double xprime = rtry * sintht * cos(phitry);
@@ -296,7 +308,7 @@ __global__ void k_propose(WState st, MoveBuf mb, int iel) {
   m.rratio = m.rminno / rminon;
   m.nearestn = nearn;
   m.tel = iel;
-  if (!live) return;
+  if (lane != 0) return;
   mb.ms[w] = m;
   rng.store(st.rng + 4 * (size_t)w);
 }
@@ -656,9 +668,13 @@ __global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
 // Scalar state of accepted moves is committed here; k_commit applies the
 // matrix and table updates.
 // ---------------------------------------------------------------------------
-__global__ void k_decide(WState st, MoveBuf mb, GSys g, int iel) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= st.W) return;
+__global__ void __launch_bounds__(128) k_decide(WState st, MoveBuf mb, GSys g, int iel) {
+  // kMoveGroup lanes per walker: the ratio and the drift at the new point are
+  // dot products over the group, the rest is evaluated identically by the
+  // group's lanes, its lane 0 stores
+  const int lane = threadIdx.x & (kMoveGroup - 1);
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) / kMoveGroup;
+  if (w >= st.W) return;  // the whole group (one walker)
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
   spin_of(iel, iab, nel, ish);
@@ -673,17 +689,21 @@ __global__ void k_decide(WState st, MoveBuf mb, GSys g, int iel) {
   double p = zero, psidn = 0, psi2n = 0, ratio = 0;
   const double fsumn = mb.fsumn[w];
   if (!m.igeo) {
-    for (int j = 0; j < nel; j++) ratio += sl[j] * orbn[slot[j]];
+    for (int j = lane; j < nel; j += kMoveGroup) ratio += sl[j] * orbn[slot[j]];
+    ratio = group_sum(ratio);
     const double detn = st.detiab[2 * w + iab] * ratio;
     psidn = mb.md_psidn ? mb.md_psidn[w] : detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
     if (detn != 0.0) {
       double v0 = 0, v1 = 0, v2 = 0;
-      for (int j = 0; j < nel; j++) {
+      for (int j = lane; j < nel; j += kMoveGroup) {
         const double sc = sl[j] / ratio;
         v0 += sc * orbn[1 * Oa + slot[j]];
         v1 += sc * orbn[2 * Oa + slot[j]];
         v2 += sc * orbn[3 * Oa + slot[j]];
       }
+      v0 = group_sum(v0);
+      v1 = group_sum(v1);
+      v2 = group_sum(v2);
       const double *mv = mb.md_veln ? mb.md_veln + 3 * w : nullptr;
       const double vn[3] = {(mv ? mv[0] : 0.0) + v0 + mb.vjn[3 * w + 0], (mv ? mv[1] : 0.0) + v1 + mb.vjn[3 * w + 1],
                             (mv ? mv[2] : 0.0) + v2 + mb.vjn[3 * w + 2]};
@@ -746,6 +766,7 @@ __global__ void k_decide(WState st, MoveBuf mb, GSys g, int iel) {
     }
   }
   const int acc = (rng.uniform() < p) ? 1 : 0;
+  if (lane != 0) return;
   rng.store(st.rng + 4 * (size_t)w);
   m.acc = acc;
   m.ratio = ratio;
