@@ -77,7 +77,17 @@ struct GSys {
   // exponents (a | b << 8 | c << 16); Slm constant and rmaxwf
   const int4 *aox;                // [K]
   const double2 *aok;             // [K]
+  // per centre (x, y), (z, atom type as a double): read where the lanes of a
+  // warp take different centres
+  const double2 *cen;             // [M][2]
 };
+
+// centre ic from the per-centre records (two 16-byte loads)
+struct Cen { double x, y, z; int it; };
+__device__ __forceinline__ Cen cen_of(const GSys &g, int ic) {
+  const double2 a = __ldg(g.cen + 2 * ic), b = __ldg(g.cen + 2 * ic + 1);
+  return Cen{a.x, a.y, b.x, (int)b.y};
+}
 
 // ---------------------------------------------------------------------------
 // Per-walker state (walker-major; component planes so lanes over electrons
@@ -933,8 +943,9 @@ template <int IDER>
 __device__ __forceinline__ void warp_basis_prepass(const GSys &g, const double *x, double *rec, int lane) {
   for (int ic = lane; ic < cs.M; ic += 32) {
     double *q = rec + (size_t)ic * kCenRec;
-    const int it = cs.iwctype[ic];
-    const double xc0 = x[0] - cs.cent[3 * ic], xc1 = x[1] - cs.cent[3 * ic + 1], xc2 = x[2] - cs.cent[3 * ic + 2];
+    const Cen cc = cen_of(g, ic);
+    const int it = cc.it;
+    const double xc0 = x[0] - cc.x, xc1 = x[1] - cc.y, xc2 = x[2] - cc.z;
     const double r = sqrt(xc0 * xc0 + xc1 * xc1 + xc2 * xc2);
     const double ri = 1.0 / r;
     const int ig = cs.igrid[it];

@@ -1081,6 +1081,15 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(cudaMemcpy(aokdev, aok.data(), aok.size() * sizeof(double2), cudaMemcpyHostToDevice));
   c->g.aox = aoxdev;
   c->g.aok = aokdev;
+  std::vector<double2> cen(2 * (size_t)d->ncent);
+  for (int ic = 0; ic < d->ncent; ic++) {
+    cen[2 * ic] = make_double2(d->cent[3 * ic], d->cent[3 * ic + 1]);
+    cen[2 * ic + 1] = make_double2(d->cent[3 * ic + 2], (double)d->iwctype[ic]);
+  }
+  double2 *cendev;
+  DALLOC(L, cendev, cen.size());
+  CK(cudaMemcpy(cendev, cen.data(), cen.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  c->g.cen = cendev;
   // dynamic shared memory sizes
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;

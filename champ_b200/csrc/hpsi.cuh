@@ -604,7 +604,8 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
   __syncthreads();
   for (int t = threadIdx.x; t < NM; t += blockDim.x) {
     const int jj = t / M, jc = t % M;
-    const double d0 = sx[jj] - cs.cent[3 * jc], d1 = sx[N + jj] - cs.cent[3 * jc + 1], d2 = sx[2 * N + jj] - cs.cent[3 * jc + 2];
+    const Cen cc = cen_of(g, jc);
+    const double d0 = sx[jj] - cc.x, d1 = sx[N + jj] - cc.y, d2 = sx[2 * N + jj] - cc.z;
     rr_en[jj * MS + jc] = scale0<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2));
   }
   const double *xqw = st.xq + (size_t)w * 3 * NQ;
@@ -618,8 +619,10 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
       int flag = 0;
       double v[3] = {0, 0, 0}, vl = 0;
       if (t < NM) {
-        const int i = t / M, ic = t % M, ict = cs.iwctype[ic];
-        const double d0 = sx[i] - cs.cent[3 * ic], d1 = sx[N + i] - cs.cent[3 * ic + 1], d2 = sx[2 * N + i] - cs.cent[3 * ic + 2];
+        const int i = t / M, ic = t % M;
+        const Cen cc = cen_of(g, ic);
+        const int ict = cc.it;
+        const double d0 = sx[i] - cc.x, d1 = sx[N + i] - cc.y, d2 = sx[2 * N + i] - cc.z;
         const double r = fmax(1.0e-10, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
         const int lp = cs.lpot[ict];
         vl = gauss_pot_d(r, lp, ict) - cs.znuc[ict] * (1.0 / r);
@@ -667,12 +670,13 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
       // distance_quad (r_en_quad(iq,ic) = r_en(i,ic)) and the folded e-e-n
       // coefficients of the point
       for (int jc = lane; jc < M; jc += 32) {
-        double xc[3] = {xp[0] - cs.cent[3 * jc], xp[1] - cs.cent[3 * jc + 1], xp[2] - cs.cent[3 * jc + 2]};
+        const Cen cc = cen_of(g, jc);
+        double xc[3] = {xp[0] - cc.x, xp[1] - cc.y, xp[2] - cc.z};
         double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
         if (jc == ic) r = rin;
         rq[jc] = scale0<double>(r);
         if (NORD > 1)
-          een_fold0<NORD, T>(een_coef<T>(cs.iwctype[jc]), T(1 - cs.scalek * rq[jc]), bq + (size_t)jc * NB);
+          een_fold0<NORD, T>(een_coef<T>(cc.it), T(1 - cs.scalek * rq[jc]), bq + (size_t)jc * NB);
       }
       warp_basis_prepass<0>(g, xp, rec, lane);
       __syncwarp();
