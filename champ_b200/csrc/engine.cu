@@ -77,6 +77,11 @@ struct cw_ctx {
   double *sr_o = nullptr, *sr_eo = nullptr, *sr_oo = nullptr, *oo_tmp = nullptr;
   double sr_w = 0;
   std::vector<void *> opt_allocs;
+  // CUDA graph of one VMC sweep (captured on first use)
+  cudaGraph_t sweep_graph = nullptr;
+  cudaGraphExec_t sweep_exec = nullptr;
+  long sweep_launches = 0;
+  int sweep_w = 0;
   int basis_warps = 4;
   // rank-0 cumulative estimators (acuest_reduce)
   double ecum = 0, ecm2 = 0, wcum = 0, pecum = 0, tpbcum = 0, pecm2 = 0, tpbcm2 = 0, acc = 0;
@@ -577,8 +582,7 @@ int opt_ci_accum(cw_ctx *c) {
     k_add_inplace<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->sr_oo, c->oo_tmp, n);
     LCHK("k_add_inplace");
   }
-  c->sr_w += W;
-  return CW_OK;
+  return CW_OK;  // the sample count is kept by cw_vmc_steps (this part may be a graph replay)
 }
 
 int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullptr) {
@@ -685,7 +689,15 @@ void free_dmc(cw_ctx *c) {
   d = DmcHost();
 }
 
+void drop_sweep_graph(cw_ctx *c) {
+  if (c->sweep_exec) cudaGraphExecDestroy(c->sweep_exec);
+  if (c->sweep_graph) cudaGraphDestroy(c->sweep_graph);
+  c->sweep_exec = nullptr;
+  c->sweep_graph = nullptr;
+}
+
 int alloc_walkers(cw_ctx *c, int W) {
+  drop_sweep_graph(c);  // the captured sweep holds this population's buffers
   free_dmc(c);
   free_list(c, c->opt_allocs);  // derivative buffers are sized for the old population
   c->opt_ci = c->opt_oo = false;
@@ -1192,6 +1204,7 @@ void cw_destroy(cw_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_dmc(c);
   free_list(c, c->w_allocs);
+  drop_sweep_graph(c);
   free_list(c, c->opt_allocs);
   free_list(c, c->sys_allocs);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1271,60 +1284,96 @@ int cw_get_walkers(cw_ctx *c, double *x, uint64_t *rng) {
   return CW_OK;
 }
 
+// One metrop6 sweep of every walker: rotqua, the single-electron moves of
+// every electron, the sweep's hpsi and sums (and the optimisation sums).
+int vmc_sweep(cw_ctx *c) {
+  const CSys &h = c->h;
+  const int W = c->W;
+  if (h.nloc > 0) {
+    stage_begin(c, CW_ST_ROTQUA);
+    k_rotqua<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st);
+    stage_end(c);
+    LCHK("k_rotqua");
+  }
+  for (int i = 0; i < h.N; i++) {
+    if (int rc = md_before_propose(c, i)) return rc;
+    stage_begin(c, CW_ST_PROPOSE);
+    k_propose<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, i);
+    stage_end(c);
+    LCHK("k_propose");
+    stage_begin(c, CW_ST_JASTROW_MOVE);
+    NORD_DISPATCH(launch_jmove, c, i);
+    stage_end(c);
+    LCHK("k_jastrow_move");
+    const int bw = c->basis_warps;
+    stage_begin(c, CW_ST_BASIS_MOVE);
+    k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+    stage_end(c);
+    LCHK("k_basis_move");
+    stage_begin(c, CW_ST_LCAO_MOVE);
+    {
+      int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn);
+      stage_end(c);
+      if (rc) return rc;
+    }
+    if (int rc = md_after_lcao(c, i)) return rc;
+    stage_begin(c, CW_ST_ACCEPT);
+    k_decide<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+    stage_end(c);
+    LCHK("k_decide");
+    stage_begin(c, CW_ST_COMMIT);
+    k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+    stage_end(c);
+    LCHK("k_commit");
+    if (int rc = md_after_commit(c, i)) return rc;
+  }
+  int rc = run_hpsi(c, 1);
+  if (rc) return rc;
+  if (c->opt_ci) {
+    rc = opt_ci_accum(c);
+    if (rc) return rc;
+  }
+  return CW_OK;
+}
+
+// The sweep's launch sequence is the same every sweep (pointers, electrons,
+// shapes), so it is captured once into a CUDA graph and replayed: one launch
+// per sweep instead of ~6N+20.  Profiling (per-stage events) runs the launches
+// directly; a new population, optimisation sums or a restore re-capture.
 int cw_vmc_steps(cw_ctx *c, int nstep) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
   BIND(c);
-  const CSys &h = c->h;
-  const int W = c->W;
   c->launches = 0;
   CK(cudaEventRecord(c->ev0, c->stream));
-  for (int s = 0; s < nstep; s++) {
-    if (h.nloc > 0) {
-      stage_begin(c, CW_ST_ROTQUA);
-      k_rotqua<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st);
-      stage_end(c);
-      LCHK("k_rotqua");
-    }
-    for (int i = 0; i < h.N; i++) {
-      if (int rc = md_before_propose(c, i)) return rc;
-      stage_begin(c, CW_ST_PROPOSE);
-      k_propose<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, i);
-      stage_end(c);
-      LCHK("k_propose");
-      stage_begin(c, CW_ST_JASTROW_MOVE);
-      NORD_DISPATCH(launch_jmove, c, i);
-      stage_end(c);
-      LCHK("k_jastrow_move");
-      const int bw = c->basis_warps;
-      stage_begin(c, CW_ST_BASIS_MOVE);
-      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
-      stage_end(c);
-      LCHK("k_basis_move");
-      stage_begin(c, CW_ST_LCAO_MOVE);
-      {
-        int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn);
-        stage_end(c);
-        if (rc) return rc;
-      }
-      if (int rc = md_after_lcao(c, i)) return rc;
-      stage_begin(c, CW_ST_ACCEPT);
-      k_decide<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
-      stage_end(c);
-      LCHK("k_decide");
-      stage_begin(c, CW_ST_COMMIT);
-      k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
-      stage_end(c);
-      LCHK("k_commit");
-      if (int rc = md_after_commit(c, i)) return rc;
-    }
-    int rc = run_hpsi(c, 1);
-    if (rc) return rc;
-    if (c->opt_ci) {
-      rc = opt_ci_accum(c);
+  if (c->prof) {
+    for (int s = 0; s < nstep; s++) {
+      int rc = vmc_sweep(c);
       if (rc) return rc;
+      if (c->evused > 4096) stage_collect(c);
     }
-    if (c->prof && c->evused > 4096) stage_collect(c);
+  } else {
+    if (c->sweep_exec && c->sweep_w != c->W) drop_sweep_graph(c);
+    if (!c->sweep_exec) {
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      const long l0 = c->launches;
+      int rc = vmc_sweep(c);
+      cudaGraph_t gph = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
+      if (rc || e != cudaSuccess) {
+        if (gph) cudaGraphDestroy(gph);
+        if (rc) return rc;
+        return fail(c, CW_ERR_CUDA, "sweep capture failed: %s", cudaGetErrorString(e));
+      }
+      c->sweep_graph = gph;
+      c->sweep_launches = c->launches - l0;
+      c->sweep_w = c->W;
+      c->launches = l0;
+      CK(cudaGraphInstantiate(&c->sweep_exec, c->sweep_graph, 0));
+    }
+    for (int s = 0; s < nstep; s++) CK(cudaGraphLaunch(c->sweep_exec, c->stream));
+    c->launches += (long)nstep * c->sweep_launches;
   }
+  if (c->opt_ci) c->sr_w += (double)c->W * nstep;  // samples of the optimisation sums
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0;
@@ -1403,6 +1452,7 @@ int cw_results_state(cw_ctx *c, int istate, double *out) {
 int cw_opt_ci(cw_ctx *c, int enable, int with_overlap) {
   if (!c) return CW_ERR_ARG;
   BIND(c);
+  drop_sweep_graph(c);  // the sweep gains or loses the derivative launches
   free_list(c, c->opt_allocs);
   c->opt_ci = c->opt_oo = false;
   c->ci_o = c->ci_ot = c->sr_o = c->sr_eo = c->sr_oo = c->oo_tmp = nullptr;
