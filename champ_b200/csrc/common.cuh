@@ -113,6 +113,8 @@ struct WState {
   double *enm;        // [W][2][M][N] e-n table of every electron: scaled distance
                       // rr and dd1/r (rebuilt by hpsi, row of a moved electron
                       // replaced on commit)
+  float *enmf;        // [W][2][M][N] FP32 copy of enm (mixed precision only;
+                      // the FP32 pair kernel reads it), kept in step with enm
   // estimators [W][8]: wsum esum pesum tpbsum acc ecum1s ecm21s (spare)
   double *sums;
   int *status;        // [W] nonzero: singular matrix / NaN
@@ -331,9 +333,19 @@ __host__ __device__ constexpr int een_off(int nord, int k) {
   return o;
 }
 __host__ __device__ constexpr int een_nb(int nord) { return nord <= 1 ? 1 : een_off(nord, nord); }
+// FP32 layout: every k group padded to an even number of (B, dB) pairs, so a
+// group is read as 16-byte (B, dB, B', dB') quads; pads hold zeros
+__host__ __device__ constexpr int een_lenp(int nord, int k) { return (een_pmax(nord, k) - een_pmin(k) + 2) / 2 * 2; }
+__host__ __device__ constexpr int een_offp(int nord, int k) {
+  int o = 0;
+  for (int kk = 0; kk < k; kk++) o += een_lenp(nord, kk);
+  return o;
+}
+__host__ __device__ constexpr int een_nbp(int nord) { return nord <= 1 ? 2 : een_offp(nord, nord); }
 
-// B and dB/dx interleaved: BD[2*t] = B_t, BD[2*t+1] = dB_t (t = packed index)
-template <int NORD, typename T>
+// B and dB/dx interleaved: BD[2*t] = B_t, BD[2*t+1] = dB_t (t = packed index,
+// or with PAD the padded index of een_offp)
+template <int NORD, typename T, bool PAD = false>
 __device__ __forceinline__ void een_fold(const T *__restrict__ cc, T x, T *BD) {
   T xp[NORD + 1], dxp[NORD + 1];
   xp[0] = 1;
@@ -371,14 +383,28 @@ __device__ __forceinline__ void een_fold(const T *__restrict__ cc, T x, T *BD) {
       }
     }
   }
+  if (PAD) {
 #pragma unroll
-  for (int t = 0; t < een_nb(NORD); t++) {
-    BD[2 * t] = B[t];
-    BD[2 * t + 1] = dB[t];
+    for (int k = 0; k < NORD; k++) {
+#pragma unroll
+      for (int q = 0; q < een_lenp(NORD, k); q++) {
+        const bool real = q <= een_pmax(NORD, k) - een_pmin(k);
+        const int t = real ? een_off(NORD, k) + q : 0;
+        BD[2 * (een_offp(NORD, k) + q)] = real ? B[t] : T(0);
+        BD[2 * (een_offp(NORD, k) + q) + 1] = real ? dB[t] : T(0);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int t = 0; t < een_nb(NORD); t++) {
+      BD[2 * t] = B[t];
+      BD[2 * t + 1] = dB[t];
+    }
   }
 }
 
-// FP32 twin of een_apply1 (mixed-precision Jastrow): BD 8-byte aligned
+// FP32 twin of een_apply1 (mixed-precision Jastrow): BD in the padded layout
+// of een_fold<NORD, float, true>, 16-byte aligned
 template <int NORD>
 __device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float y, float z, float &fc, float &fu,
                                             float &fi, float &fj) {
@@ -390,18 +416,24 @@ __device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float 
     yp[p] = yp[p - 1] * y;
     dyp[p] = float(p) * yp[p - 1];
   }
-  const float2 *bd = reinterpret_cast<const float2 *>(BD);
+  const float4 *bd = reinterpret_cast<const float4 *>(BD);
   fc = 0; fu = 0; fi = 0; fj = 0;
   float zk = 1, zkm = 0;
 #pragma unroll
   for (int k = 0; k < NORD; k++) {
     float a = 0, ax = 0, ay = 0;
 #pragma unroll
-    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
-      const float2 v = bd[een_off(NORD, k) + p - een_pmin(k)];
+    for (int q = 0; q < een_lenp(NORD, k); q += 2) {
+      const float4 v = bd[(een_offp(NORD, k) + q) / 2];
+      const int p = een_pmin(k) + q;
       a += v.x * yp[p];
       ax += v.y * yp[p];
       ay += v.x * dyp[p];
+      if (p + 1 <= een_pmax(NORD, k)) {
+        a += v.z * yp[p + 1];
+        ax += v.w * yp[p + 1];
+        ay += v.z * dyp[p + 1];
+      }
     }
     fc += zk * a;
     fu += zkm * a;

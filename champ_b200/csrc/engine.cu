@@ -727,6 +727,8 @@ int alloc_walkers(cw_ctx *c, int W) {
   DALLOC(L, s.fjo, (size_t)W * 3 * N);
   DALLOC(L, s.fsumo, W);
   DALLOC(L, s.enm, (size_t)W * 2 * M * N);
+  s.enmf = nullptr;
+  if (c->mixed) DALLOC(L, s.enmf, (size_t)W * 2 * M * N);
   DALLOC(L, s.sums, (size_t)W * 8);
   DALLOC(L, s.status, W);
   MoveBuf &m = c->mb;
@@ -1106,7 +1108,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
     c->smem_jmove = sizeof(double) * 4 * (size_t)h.M * (8 + 2 * een_nb(nord));
-    c->smem_jmove_f32 = sizeof(float) * 4 * (size_t)h.M * (8 + 2 * een_nb(nord));
+    c->smem_jmove_f32 = sizeof(float) * 4 * (size_t)h.M * (8 + 2 * een_nbp(nord));
   }
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
@@ -2029,6 +2031,8 @@ int dmc_alloc(cw_ctx *c, int mwalk) {
   add_field(r, c->st.fjo, 3L * N);
   add_field(r, c->st.fsumo, 1);
   add_field(r, c->st.enm, 2L * h.M * N);
+  // 2MN floats per walker = MN doubles: the copy kernel moves doubles
+  if (c->st.enmf) add_field(r, reinterpret_cast<double *>(c->st.enmf), (long)h.M * N);
   if (c->md_on) {
     add_field(r, c->md.aa, 2L * nmax * h.Oa);
     add_field(r, c->md.dd, 2L * c->mdt.numax);

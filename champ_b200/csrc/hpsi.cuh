@@ -131,6 +131,10 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) k_jastrow_full(WS
       }
       st.enm[(size_t)w * 2 * MN + t] = rr;
       st.enm[((size_t)w * 2 + 1) * MN + t] = dd1 / r;
+      if (st.enmf) {
+        st.enmf[(size_t)w * 2 * MN + t] = (float)rr;
+        st.enmf[((size_t)w * 2 + 1) * MN + t] = (float)(dd1 / r);
+      }
       if (rr == asym) continue;
       double fen, feni, fenii;
       en_term<2, double>(cs.iwctype[ic], rr, fen, feni, fenii);

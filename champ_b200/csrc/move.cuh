@@ -473,8 +473,8 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
 template <int NORD>
 __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) float smemf[];
-  constexpr int NB = een_nb(NORD);
-  constexpr int PER = 8 + 2 * NB;         // shared floats per centre (one pad keeps B 8-byte aligned)
+  constexpr int NB = een_nbp(NORD);        // padded (B, dB) pairs per centre
+  constexpr int PER = 8 + 2 * NB;         // shared floats per centre (B 16-byte aligned)
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
     sh_g[ic] = -kap * dd1 / r;
     mb.enn[((size_t)w * 2 + 0) * M + ic] = rr;
     mb.enn[((size_t)w * 2 + 1) * M + ic] = dd1 / r;
-    if (NORD > 1) een_fold<NORD, float>(&cs.cf[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sh_B + (size_t)ic * 2 * NB);
+    if (NORD > 1) een_fold<NORD, float, true>(&cs.cf[cs.iwctype[ic] * CW_MAX_TERMS], 1 - kap * rr, sh_B + (size_t)ic * 2 * NB);
   }
   __syncwarp();
   const double *xw = st.x + (size_t)w * 3 * N;
@@ -542,11 +542,11 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
       const float z = 1 - kap * u;
       const float du = -kap * dd1;
       const float du_r = du / rij;
-      const double *en_rr = st.enm + (size_t)w * 2 * M * N + jj;
-      const double *en_h = en_rr + (size_t)M * N;
-      double nrr = en_rr[0], nh = en_h[0];
+      const float *en_rr = st.enmf + (size_t)w * 2 * M * N + jj;
+      const float *en_h = en_rr + (size_t)M * N;
+      float nrr = en_rr[0], nh = en_h[0];
       for (int ic = 0; ic < M; ic++) {
-        const float rrj = (float)nrr, hj = (float)nh;
+        const float rrj = nrr, hj = nh;
         if (ic + 1 < M) {
           nrr = en_rr[(size_t)(ic + 1) * N];
           nh = en_h[(size_t)(ic + 1) * N];
@@ -830,7 +830,9 @@ __global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
   const int M = cs.M;
   for (int t = tid; t < 2 * M; t += blockDim.x) {
     const int pl = t / M, ic = t % M;
-    st.enm[(((size_t)w * 2 + pl) * M + ic) * N + iel] = mb.enn[((size_t)w * 2 + pl) * M + ic];
+    const double v = mb.enn[((size_t)w * 2 + pl) * M + ic];
+    st.enm[(((size_t)w * 2 + pl) * M + ic) * N + iel] = v;
+    if (st.enmf) st.enmf[(((size_t)w * 2 + pl) * M + ic) * N + iel] = (float)v;
   }
   // jassav: pair tables and per-electron gradients
   double *fso = st.fso + (size_t)w * N * N;
