@@ -403,37 +403,37 @@ __device__ __forceinline__ void een_fold(const T *__restrict__ cc, T x, T *BD) {
   }
 }
 
-// FP32 twin of een_apply1 (mixed-precision Jastrow): BD in the padded layout
-// of een_fold<NORD, float, true>, 16-byte aligned
+// FP32 twin of een_apply1_multi<NORD, 1> (mixed-precision Jastrow): BD in the padded layout
+// of een_fold<NORD, float, true>, 16-byte aligned; the y polynomial of each k
+// group by Horner's rule with its derivative alongside
 template <int NORD>
 __device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float y, float z, float &fc, float &fu,
                                             float &fi, float &fj) {
-  float yp[NORD + 1], dyp[NORD + 1];
-  yp[0] = 1;
-  dyp[0] = 0;
-#pragma unroll
-  for (int p = 1; p <= NORD; p++) {
-    yp[p] = yp[p - 1] * y;
-    dyp[p] = float(p) * yp[p - 1];
-  }
   const float4 *bd = reinterpret_cast<const float4 *>(BD);
   fc = 0; fu = 0; fi = 0; fj = 0;
   float zk = 1, zkm = 0;
 #pragma unroll
   for (int k = 0; k < NORD; k++) {
-    float a = 0, ax = 0, ay = 0;
+    const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_offp(NORD, k);
+    float4 v[een_lenp(NORD, 1) / 2];  // k = 1 is the longest group
 #pragma unroll
-    for (int q = 0; q < een_lenp(NORD, k); q += 2) {
-      const float4 v = bd[(een_offp(NORD, k) + q) / 2];
-      const int p = een_pmin(k) + q;
-      a += v.x * yp[p];
-      ax += v.y * yp[p];
-      ay += v.x * dyp[p];
-      if (p + 1 <= een_pmax(NORD, k)) {
-        a += v.z * yp[p + 1];
-        ax += v.w * yp[p + 1];
-        ay += v.z * dyp[p + 1];
-      }
+    for (int q = 0; q < een_lenp(NORD, k); q += 2) v[q / 2] = bd[(off + q) / 2];
+    // (B, dB) of power p: quad (p - pmin) / 2, half (p - pmin) % 2
+#define EEN_B(p) (((p) - pmin) % 2 ? v[((p) - pmin) / 2].z : v[((p) - pmin) / 2].x)
+#define EEN_D(p) (((p) - pmin) % 2 ? v[((p) - pmin) / 2].w : v[((p) - pmin) / 2].y)
+    float a = EEN_B(pmax), ax = EEN_D(pmax), ay = 0;
+#pragma unroll
+    for (int p = pmax - 1; p >= pmin; p--) {
+      ay = ay * y + a;
+      a = a * y + EEN_B(p);
+      ax = ax * y + EEN_D(p);
+    }
+#undef EEN_B
+#undef EEN_D
+    if (pmin == 1) {  // k = 0 has no y^0 term
+      ay = ay * y + a;
+      a *= y;
+      ax *= y;
     }
     fc += zk * a;
     fu += zkm * a;
@@ -444,38 +444,63 @@ __device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float 
   }
 }
 
-// value and first derivatives (d/dz, d/dx, d/dy) of the folded polynomial;
-// BD in shared memory, 16-byte aligned (one vector load per (B, dB) pair)
-template <int NORD>
-__device__ __forceinline__ void een_apply1(const double *__restrict__ BD, double y, double z, double &fc,
-                                           double &fu, double &fi, double &fj) {
-  double yp[NORD + 1], dyp[NORD + 1];
-  yp[0] = 1;
-  dyp[0] = 0;
-#pragma unroll
-  for (int p = 1; p <= NORD; p++) {
-    yp[p] = yp[p - 1] * y;
-    dyp[p] = double(p) * yp[p - 1];
-  }
+// value and first derivatives (d/dz, d/dx, d/dy) of the folded polynomial
+// for P partners of one (moved electron, centre) at once: each
+// (B, dB) pair is loaded once for all of them.  The y polynomial of every k
+// group is evaluated by Horner's rule with its derivative alongside
+// (a = a y + B_p, a' = a' y + a), so no power tables are held per partner.
+template <int NORD, int P>
+__device__ __forceinline__ void een_apply1_multi(const double *__restrict__ BD, const double (&y)[P],
+                                                 const double (&z)[P], double (&fc)[P], double (&fu)[P],
+                                                 double (&fi)[P], double (&fj)[P]) {
   const double2 *bd = reinterpret_cast<const double2 *>(BD);
-  fc = 0; fu = 0; fi = 0; fj = 0;
-  double zk = 1, zkm = 0;  // z^k, k z^(k-1)
+  double zk[P], zkm[P];
+#pragma unroll
+  for (int q = 0; q < P; q++) {
+    fc[q] = 0; fu[q] = 0; fi[q] = 0; fj[q] = 0;
+    zk[q] = 1;
+    zkm[q] = 0;
+  }
 #pragma unroll
   for (int k = 0; k < NORD; k++) {
-    double a = 0, ax = 0, ay = 0;
+    const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_off(NORD, k);
+    double a[P], ax[P], ay[P];
+    {
+      const double2 v = bd[off + pmax - pmin];
 #pragma unroll
-    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
-      const double2 v = bd[een_off(NORD, k) + p - een_pmin(k)];
-      a += v.x * yp[p];
-      ax += v.y * yp[p];
-      ay += v.x * dyp[p];
+      for (int q = 0; q < P; q++) {
+        a[q] = v.x;
+        ax[q] = v.y;
+        ay[q] = 0;
+      }
     }
-    fc += zk * a;
-    fu += zkm * a;
-    fi += zk * ax;
-    fj += zk * ay;
-    zkm = double(k + 1) * zk;
-    zk *= z;
+#pragma unroll
+    for (int p = pmax - 1; p >= pmin; p--) {
+      const double2 v = bd[off + p - pmin];
+#pragma unroll
+      for (int q = 0; q < P; q++) {
+        ay[q] = ay[q] * y[q] + a[q];
+        a[q] = a[q] * y[q] + v.x;
+        ax[q] = ax[q] * y[q] + v.y;
+      }
+    }
+    if (pmin == 1) {  // k = 0 has no y^0 term: one more factor of y
+#pragma unroll
+      for (int q = 0; q < P; q++) {
+        ay[q] = ay[q] * y[q] + a[q];
+        a[q] *= y[q];
+        ax[q] *= y[q];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      fc[q] += zk[q] * a[q];
+      fu[q] += zkm[q] * a[q];
+      fi[q] += zk[q] * ax[q];
+      fj[q] += zk[q] * ay[q];
+      zkm[q] = double(k + 1) * zk[q];
+      zk[q] *= z[q];
+    }
   }
 }
 
@@ -690,28 +715,71 @@ __device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD4)
 }
 
 // all nine value/derivative sums of the e-e-n term (jastrow4.f90 fc, fu,
-// fuu, fi, fii, fj, fjj, fui, fuj) from the folded row coefficients
+// fuu, fi, fii, fj, fjj, fui, fuj) from the folded row coefficients.
+// FP64: the y polynomial of every k group by Horner's rule, its first
+// derivative and half its second derivative carried alongside (h = h y + a',
+// a' = a' y + a, a = a y + B_p; fjj doubled once at the end).  FP32: sums
+// over a table of y powers (the Horner form needs more live registers than
+// the FP32 kernel's occupancy target leaves and spills).
 template <int NORD, typename T = double>
 __device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD4, T y, T z) {
-  T yp[NORD + 1];
-  yp[0] = 1;
-#pragma unroll
-  for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
   EenOut<T> e{0, 0, 0, 0, 0, 0, 0, 0, 0};
   T zk = 1, dzk = 0, d2zk = 0;
+  if constexpr (sizeof(T) == 4) {
+    T yp[NORD + 1];
+    yp[0] = 1;
+#pragma unroll
+    for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
+#pragma unroll
+    for (int k = 0; k < NORD; k++) {
+      T a = 0, ax = 0, axx = 0, ay = 0, ayy = 0;
+#pragma unroll
+      for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
+        const int t = een_off(NORD, k) + p - een_pmin(k);
+        T b0, b1, b2;
+        ld3<T>(BD4 + 4 * t, b0, b1, b2);
+        a += b0 * yp[p];
+        ax += b1 * yp[p];
+        axx += b2 * yp[p];
+        if (p >= 1) ay += b0 * (T(p) * yp[p >= 1 ? p - 1 : 0]);
+        if (p >= 2) ayy += b0 * (T(p * (p - 1)) * yp[p >= 2 ? p - 2 : 0]);
+      }
+      e.fc += zk * a;
+      e.fu += dzk * a;
+      e.fuu += d2zk * a;
+      e.fi += zk * ax;
+      e.fii += zk * axx;
+      e.fui += dzk * ax;
+      e.fj += zk * ay;
+      e.fjj += zk * ayy;
+      e.fuj += dzk * ay;
+      d2zk = T(k + 1) * dzk;
+      dzk = T(k + 1) * zk;
+      zk *= z;
+    }
+    return e;
+  }
 #pragma unroll
   for (int k = 0; k < NORD; k++) {
-    T a = 0, ax = 0, axx = 0, ay = 0, ayy = 0;
+    const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_off(NORD, k);
+    T a, ax, axx, ay = 0, ayy = 0;  // ayy: half the second derivative
+    ld3<T>(BD4 + 4 * (off + pmax - pmin), a, ax, axx);
 #pragma unroll
-    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
-      const int t = een_off(NORD, k) + p - een_pmin(k);
+    for (int p = pmax - 1; p >= pmin; p--) {
       T b0, b1, b2;
-      ld3<T>(BD4 + 4 * t, b0, b1, b2);
-      a += b0 * yp[p];
-      ax += b1 * yp[p];
-      axx += b2 * yp[p];
-      if (p >= 1) ay += b0 * (T(p) * yp[p >= 1 ? p - 1 : 0]);
-      if (p >= 2) ayy += b0 * (T(p * (p - 1)) * yp[p >= 2 ? p - 2 : 0]);
+      ld3<T>(BD4 + 4 * (off + p - pmin), b0, b1, b2);
+      ayy = ayy * y + ay;
+      ay = ay * y + a;
+      a = a * y + b0;
+      ax = ax * y + b1;
+      axx = axx * y + b2;
+    }
+    if (pmin == 1) {  // k = 0 has no y^0 term
+      ayy = ayy * y + ay;
+      ay = ay * y + a;
+      a *= y;
+      ax *= y;
+      axx *= y;
     }
     e.fc += zk * a;
     e.fu += dzk * a;
@@ -726,6 +794,7 @@ __device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD4, T y, 
     dzk = T(k + 1) * zk;
     zk *= z;
   }
+  e.fjj *= T(2);
   return e;
 }
 

@@ -317,6 +317,10 @@ __global__ void __launch_bounds__(128) k_propose(WState st, MoveBuf mb, int iel)
 // jastrow4e, iflag=0: warp per walker, lanes over the partner electron.
 // Per-centre quantities of the moved electron are staged in shared memory.
 // ---------------------------------------------------------------------------
+// partner electrons per lane in k_jastrow_move (2 shares each coefficient load
+// between two partners but needs ~150 registers; 1 measured faster on B200)
+constexpr int kJmPartners = 1;
+
 template <int NORD>
 __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) double smem[];
@@ -361,67 +365,109 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
   __syncwarp();
   const double *xw = st.x + (size_t)w * 3 * N;
   const double *fso_i = st.fso + ((size_t)w * N + iel) * N;
+  const double asym = cs.asymp_r;
   double dfs = 0, dv0 = 0, dv1 = 0, dv2 = 0;
-  for (int jj = lane; jj < N; jj += 32) {
-    if (jj == iel) continue;
-    const double xj[3] = {xw[jj], xw[N + jj], xw[2 * N + jj]};
-    const int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
-    int isb, ipar;
-    double sspinn;
-    pair_spin(i, j, isb, ipar, sspinn);
-    double rvee[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};  // x_iel - x_jj
-    const double rij = sqrt(rvee[0] * rvee[0] + rvee[1] * rvee[1] + rvee[2] * rvee[2]);
-    double u, dd1, dd2;
-    scale2<double>(rij, u, dd1, dd2);
-    double fs = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
-    if (u != cs.asymp_r) {
-      double fee, feeu, feeuu;
-      ee_term<1, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
-      feeu = feeu * dd1 / rij;
-      fs += fee;
-      for (int k = 0; k < 3; k++) {
-        gi[k] += feeu * rvee[k];
-        gj[k] -= feeu * rvee[k];
+  // each lane takes kJmPartners partners (jj, jj + 32, ...) so that every
+  // shared coefficient load serves all of them
+  constexpr int P = kJmPartners;
+  for (int j0 = lane; j0 < N; j0 += 32 * P) {
+    bool ok[P];
+    int jj[P];
+    double rvee[P][3], rij[P], z[P], du_r[P], fs[P], gi[P][3], gj[P][3];
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      jj[q] = j0 + 32 * q;
+      ok[q] = jj[q] < N && jj[q] != iel;
+      // a partner slot past the end or on the moved electron computes on a
+      // valid neighbour index and is discarded
+      const int jc = ok[q] ? jj[q] : (iel == 0 ? N - 1 : 0);
+      const double xj[3] = {xw[jc], xw[N + jc], xw[2 * N + jc]};
+      const int i = jc < iel ? iel : jc, j = jc < iel ? jc : iel;
+      int isb, ipar;
+      double sspinn;
+      pair_spin(i, j, isb, ipar, sspinn);
+      for (int k = 0; k < 3; k++) rvee[q][k] = xi[k] - xj[k];  // x_iel - x_jj
+      rij[q] = sqrt(rvee[q][0] * rvee[q][0] + rvee[q][1] * rvee[q][1] + rvee[q][2] * rvee[q][2]);
+      double u, dd1, dd2;
+      scale2<double>(rij[q], u, dd1, dd2);
+      fs[q] = 0;
+      for (int k = 0; k < 3; k++) gi[q][k] = gj[q][k] = 0;
+      if (u != asym) {
+        double fee, feeu, feeuu;
+        ee_term<1, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+        feeu = feeu * dd1 / rij[q];
+        fs[q] += fee;
+        for (int k = 0; k < 3; k++) {
+          gi[q][k] += feeu * rvee[q][k];
+          gj[q][k] -= feeu * rvee[q][k];
+        }
       }
+      z[q] = 1 - kap * u;
+      du_r[q] = -kap * dd1 / rij[q];
     }
     if (NORD > 1) {
-      const double z = 1 - kap * u;
-      const double du_r = -kap * dd1 / rij;
-      // partner's e-n values from the walker's table (coalesced over lanes)
-      const double *en_rr = st.enm + (size_t)w * 2 * M * N + jj;
+      // partners' e-n values from the walker's table (coalesced over lanes),
+      // loaded one centre ahead
+      const double *en_rr = st.enm + (size_t)w * 2 * M * N;
       const double *en_h = en_rr + (size_t)M * N;
-      // table values of the next centre are loaded one iteration ahead
-      double nrr = en_rr[0], nh = en_h[0];
+      int jt[P];
+      double nrr[P], nh[P];
+#pragma unroll
+      for (int q = 0; q < P; q++) {
+        jt[q] = ok[q] ? jj[q] : (iel == 0 ? N - 1 : 0);
+        nrr[q] = en_rr[jt[q]];
+        nh[q] = en_h[jt[q]];
+      }
       for (int ic = 0; ic < M; ic++) {
-        const double rrj = nrr, hj = nh;
-        if (ic + 1 < M) {
-          nrr = en_rr[(size_t)(ic + 1) * N];
-          nh = en_h[(size_t)(ic + 1) * N];
-        }
+        double rrj[P], hj[P], y[P];
+        bool any = false;
         const double rri = sh_s[ic];
-        if (rri == cs.asymp_r && rrj == cs.asymp_r) continue;
-        const double rj_v[3] = {xj[0] - cs.cent[3 * ic], xj[1] - cs.cent[3 * ic + 1], xj[2] - cs.cent[3 * ic + 2]};
-        double fc, fu_, fi_, fj_;
-        een_apply1<NORD>(sh_B + (size_t)ic * 2 * NB, 1 - kap * rrj, z, fc, fu_, fi_, fj_);
-        const double fu = fu_ * du_r;
-        const double fi = fi_ * sh_g[ic];
-        const double fj = fj_ * (-kap) * hj;
-        fs += fc;
-        for (int k = 0; k < 3; k++) {
-          gi[k] += fi * sh_rv[k * M + ic] + fu * rvee[k];
-          gj[k] += fj * rj_v[k] - fu * rvee[k];
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+          rrj[q] = nrr[q];
+          hj[q] = nh[q];
+          if (ic + 1 < M) {
+            nrr[q] = en_rr[(ic + 1) * N + jt[q]];
+            nh[q] = en_h[(ic + 1) * N + jt[q]];
+          }
+          any |= ok[q] && !(rri == asym && rrj[q] == asym);
+          y[q] = 1 - kap * rrj[q];
+        }
+        if (!any) continue;
+        double fc[P], fu_[P], fi_[P], fj_[P];
+        een_apply1_multi<NORD, P>(sh_B + (size_t)ic * 2 * NB, y, z, fc, fu_, fi_, fj_);
+        const double gic = sh_g[ic];
+        const double rv[3] = {sh_rv[ic], sh_rv[M + ic], sh_rv[2 * M + ic]};
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+          if (rri == asym && rrj[q] == asym) continue;  // this pair-centre term is cut
+          // partner to centre: (x_iel - c) - (x_iel - x_jj)
+          const double rj_v[3] = {rv[0] - rvee[q][0], rv[1] - rvee[q][1], rv[2] - rvee[q][2]};
+          const double fu = fu_[q] * du_r[q];
+          const double fi = fi_[q] * gic;
+          const double fj = fj_[q] * (-kap) * hj[q];
+          fs[q] += fc[q];
+          for (int k = 0; k < 3; k++) {
+            gi[q][k] += fi * rv[k] + fu * rvee[q][k];
+            gj[q][k] += fj * rj_v[k] - fu * rvee[q][k];
+          }
         }
       }
     }
-    mb.fsn[(size_t)w * N + jj] = fs;
-    for (int k = 0; k < 3; k++) {
-      mb.fijn_i[((size_t)w * 3 + k) * N + jj] = gi[k];
-      mb.fijn_j[((size_t)w * 3 + k) * N + jj] = gj[k];
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      if (!ok[q]) continue;
+      const int jq = jj[q];
+      mb.fsn[(size_t)w * N + jq] = fs[q];
+      for (int k = 0; k < 3; k++) {
+        mb.fijn_i[((size_t)w * 3 + k) * N + jq] = gi[q][k];
+        mb.fijn_j[((size_t)w * 3 + k) * N + jq] = gj[q][k];
+      }
+      dfs += fs[q] - fso_i[jq];
+      dv0 += gi[q][0] - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + jq];
+      dv1 += gi[q][1] - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + jq];
+      dv2 += gi[q][2] - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + jq];
     }
-    dfs += fs - fso_i[jj];
-    dv0 += gi[0] - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + jj];
-    dv1 += gi[1] - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + jj];
-    dv2 += gi[2] - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + jj];
   }
   // e-n part of the moved electron
   double fen_s = 0, ge0 = 0, ge1 = 0, ge2 = 0;

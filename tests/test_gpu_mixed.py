@@ -101,3 +101,39 @@ def test_mixed_mean_energy(oracle_mod):
     # flip where the FP64 acceptance probability lies within ~1e-6 of the draw
     assert abs(res["mixed"]["accept"] - res["fp64"]["accept"]) <= 2e-4
     assert d <= 0.05 * res["fp64"]["err"]
+
+
+@pytest.mark.parametrize("config,W,tau", [("tiny", 32, 0.01), ("c0", 16, 0.005)])
+def test_mixed_dmc_steps(oracle_mod, config, W, tau):
+    """DMC through the mixed engine against the FP64 oracle on the same move
+    and population streams: same accept/branch/copy decisions, positions,
+    weights and local energies within the mixed bounds after walker copies
+    (a copied walker carries its FP64 and FP32 tables along)."""
+    from champ_b200.engine import Dmc, Engine
+    from champ_b200.system import make_synthetic
+    s = make_synthetic(config)
+    o = oracle_mod.OracleSystem(s)
+    mw = 4 * W
+    st = oracle_mod.rng_states(mw + 2)
+    xs = []
+    for w in range(W):
+        x, st[w] = o.sites(st[w])
+        xs.append(x)
+    vw = oracle_mod.OracleWalkers(o, np.array(xs), st[:W])
+    vw.steps(20, 8)
+    vw.end_block()
+    x, r = vw.walkers()
+    rng = np.concatenate([r, st[W:mw]])
+    e0 = vw.results()["energy"]
+    dg = Dmc(Engine(s, precision="mixed"), x, rng, st[mw], tau=tau, etrial=e0, mwalk=mw)
+    do = oracle_mod.OracleDmc(o, x, rng, st[mw], tau=tau, etrial=e0, mwalk=mw)
+    for step in range(10):
+        dg.steps(1)
+        do.steps(1, 8)
+        xg, wg, eg, rg = dg.walkers()
+        xo, wo, eo, ro = do.walkers()
+        assert len(wg) == len(wo), f"population sizes differ at step {step}"
+        assert np.array_equal(rg, ro), f"move streams diverged at step {step}"
+        assert rel_err(xg, xo) < 1e-5
+        assert rel_err(wg, wo) < 1e-4
+        assert np.max(np.abs(eg - eo)) <= TOL_E * max(1.0, np.max(np.abs(eo)))
