@@ -411,9 +411,9 @@ __device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float 
                                             float &fi, float &fj) {
   const float4 *bd = reinterpret_cast<const float4 *>(BD);
   fc = 0; fu = 0; fi = 0; fj = 0;
-  float zk = 1, zkm = 0;
+  // k descending: the z polynomial by Horner's rule, d/dz alongside
 #pragma unroll
-  for (int k = 0; k < NORD; k++) {
+  for (int k = NORD - 1; k >= 0; k--) {
     const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_offp(NORD, k);
     float4 v[een_lenp(NORD, 1) / 2];  // k = 1 is the longest group
 #pragma unroll
@@ -435,12 +435,10 @@ __device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float 
       a *= y;
       ax *= y;
     }
-    fc += zk * a;
-    fu += zkm * a;
-    fi += zk * ax;
-    fj += zk * ay;
-    zkm = float(k + 1) * zk;
-    zk *= z;
+    fu = fu * z + fc;
+    fc = fc * z + a;
+    fi = fi * z + ax;
+    fj = fj * z + ay;
   }
 }
 
@@ -454,15 +452,13 @@ __device__ __forceinline__ void een_apply1_multi(const double *__restrict__ BD, 
                                                  const double (&z)[P], double (&fc)[P], double (&fu)[P],
                                                  double (&fi)[P], double (&fj)[P]) {
   const double2 *bd = reinterpret_cast<const double2 *>(BD);
-  double zk[P], zkm[P];
 #pragma unroll
   for (int q = 0; q < P; q++) {
     fc[q] = 0; fu[q] = 0; fi[q] = 0; fj[q] = 0;
-    zk[q] = 1;
-    zkm[q] = 0;
   }
+  // k descending: the z polynomial by Horner's rule, d/dz alongside
 #pragma unroll
-  for (int k = 0; k < NORD; k++) {
+  for (int k = NORD - 1; k >= 0; k--) {
     const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_off(NORD, k);
     double a[P], ax[P], ay[P];
     {
@@ -494,12 +490,10 @@ __device__ __forceinline__ void een_apply1_multi(const double *__restrict__ BD, 
     }
 #pragma unroll
     for (int q = 0; q < P; q++) {
-      fc[q] += zk[q] * a[q];
-      fu[q] += zkm[q] * a[q];
-      fi[q] += zk[q] * ax[q];
-      fj[q] += zk[q] * ay[q];
-      zkm[q] = double(k + 1) * zk[q];
-      zk[q] *= z[q];
+      fu[q] = fu[q] * z[q] + fc[q];
+      fc[q] = fc[q] * z[q] + a[q];
+      fi[q] = fi[q] * z[q] + ax[q];
+      fj[q] = fj[q] * z[q] + ay[q];
     }
   }
 }
@@ -548,18 +542,16 @@ __device__ __forceinline__ float een_apply0f(const float *__restrict__ Bp, float
     Bv[2 * t] = v.x;
     Bv[2 * t + 1] = v.y;
   }
-  float yp[NORD + 1];
-  yp[0] = 1;
+  // Horner's rule in y inside each k group and in z over the groups
+  float fc = 0;
 #pragma unroll
-  for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
-  float fc = 0, zk = 1;
+  for (int k = NORD - 1; k >= 0; k--) {
+    const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_off(NORD, k);
+    float a = Bv[off + pmax - pmin];
 #pragma unroll
-  for (int k = 0; k < NORD; k++) {
-    float a = 0;
-#pragma unroll
-    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) a += Bv[een_off(NORD, k) + p - een_pmin(k)] * yp[p];
-    fc += zk * a;
-    zk *= z;
+    for (int p = pmax - 1; p >= pmin; p--) a = a * y + Bv[off + p - pmin];
+    if (pmin == 1) a *= y;  // k = 0 has no y^0 term
+    fc = fc * z + a;
   }
   return fc;
 }
@@ -575,18 +567,16 @@ __device__ __forceinline__ double een_apply0(const double *__restrict__ Bp, doub
     Bv[2 * t] = v.x;
     Bv[2 * t + 1] = v.y;
   }
-  double yp[NORD + 1];
-  yp[0] = 1;
+  // Horner's rule in y inside each k group and in z over the groups
+  double fc = 0;
 #pragma unroll
-  for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
-  double fc = 0, zk = 1;
+  for (int k = NORD - 1; k >= 0; k--) {
+    const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_off(NORD, k);
+    double a = Bv[off + pmax - pmin];
 #pragma unroll
-  for (int k = 0; k < NORD; k++) {
-    double a = 0;
-#pragma unroll
-    for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) a += Bv[een_off(NORD, k) + p - een_pmin(k)] * yp[p];
-    fc += zk * a;
-    zk *= z;
+    for (int p = pmax - 1; p >= pmin; p--) a = a * y + Bv[off + p - pmin];
+    if (pmin == 1) a *= y;  // k = 0 has no y^0 term
+    fc = fc * z + a;
   }
   return fc;
 }
@@ -715,52 +705,16 @@ __device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD4)
 }
 
 // all nine value/derivative sums of the e-e-n term (jastrow4.f90 fc, fu,
-// fuu, fi, fii, fj, fjj, fui, fuj) from the folded row coefficients.
-// FP64: the y polynomial of every k group by Horner's rule, its first
-// derivative and half its second derivative carried alongside (h = h y + a',
-// a' = a' y + a, a = a y + B_p; fjj doubled once at the end).  FP32: sums
-// over a table of y powers (the Horner form needs more live registers than
-// the FP32 kernel's occupancy target leaves and spills).
+// fuu, fi, fii, fj, fjj, fui, fuj) from the folded row coefficients.  The y
+// polynomial of every k group by Horner's rule with its first derivative and
+// half its second derivative carried alongside (h = h y + a', a' = a' y + a,
+// a = a y + B_p); the z polynomial over the groups the same way (k
+// descending); fuu and fjj doubled once at the end.
 template <int NORD, typename T = double>
 __device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD4, T y, T z) {
   EenOut<T> e{0, 0, 0, 0, 0, 0, 0, 0, 0};
-  T zk = 1, dzk = 0, d2zk = 0;
-  if constexpr (sizeof(T) == 4) {
-    T yp[NORD + 1];
-    yp[0] = 1;
 #pragma unroll
-    for (int p = 1; p <= NORD; p++) yp[p] = yp[p - 1] * y;
-#pragma unroll
-    for (int k = 0; k < NORD; k++) {
-      T a = 0, ax = 0, axx = 0, ay = 0, ayy = 0;
-#pragma unroll
-      for (int p = een_pmin(k); p <= een_pmax(NORD, k); p++) {
-        const int t = een_off(NORD, k) + p - een_pmin(k);
-        T b0, b1, b2;
-        ld3<T>(BD4 + 4 * t, b0, b1, b2);
-        a += b0 * yp[p];
-        ax += b1 * yp[p];
-        axx += b2 * yp[p];
-        if (p >= 1) ay += b0 * (T(p) * yp[p >= 1 ? p - 1 : 0]);
-        if (p >= 2) ayy += b0 * (T(p * (p - 1)) * yp[p >= 2 ? p - 2 : 0]);
-      }
-      e.fc += zk * a;
-      e.fu += dzk * a;
-      e.fuu += d2zk * a;
-      e.fi += zk * ax;
-      e.fii += zk * axx;
-      e.fui += dzk * ax;
-      e.fj += zk * ay;
-      e.fjj += zk * ayy;
-      e.fuj += dzk * ay;
-      d2zk = T(k + 1) * dzk;
-      dzk = T(k + 1) * zk;
-      zk *= z;
-    }
-    return e;
-  }
-#pragma unroll
-  for (int k = 0; k < NORD; k++) {
+  for (int k = NORD - 1; k >= 0; k--) {
     const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_off(NORD, k);
     T a, ax, axx, ay = 0, ayy = 0;  // ayy: half the second derivative
     ld3<T>(BD4 + 4 * (off + pmax - pmin), a, ax, axx);
@@ -781,19 +735,17 @@ __device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD4, T y, 
       ax *= y;
       axx *= y;
     }
-    e.fc += zk * a;
-    e.fu += dzk * a;
-    e.fuu += d2zk * a;
-    e.fi += zk * ax;
-    e.fii += zk * axx;
-    e.fui += dzk * ax;
-    e.fj += zk * ay;
-    e.fjj += zk * ayy;
-    e.fuj += dzk * ay;
-    d2zk = T(k + 1) * dzk;
-    dzk = T(k + 1) * zk;
-    zk *= z;
+    e.fuu = e.fuu * z + e.fu;
+    e.fu = e.fu * z + e.fc;
+    e.fc = e.fc * z + a;
+    e.fui = e.fui * z + e.fi;
+    e.fi = e.fi * z + ax;
+    e.fii = e.fii * z + axx;
+    e.fuj = e.fuj * z + e.fj;
+    e.fj = e.fj * z + ay;
+    e.fjj = e.fjj * z + ayy;
   }
+  e.fuu *= T(2);
   e.fjj *= T(2);
   return e;
 }
