@@ -710,6 +710,96 @@ struct Walker {
   static inline int FI(int i, int j, int N) { return i + N * j; }
   static inline int FIJ(int k, int i, int j, int N) { return k + 3 * (i + N * j); }
 
+  // ---- raw Jastrow parameter derivatives (vmc/deriv_jastrow4.f90 gvalue) ----
+  // d J / d p for every Jastrow coefficient taken on its own, before CHAMP's
+  // selection of varied parameters and its cusp-dependent c terms (a linear
+  // map applied on the host):
+  //   a part [nctype][norda+1]: q = 1 Pade numerator a(1), q = 2 Pade
+  //     denominator a(2), q >= 3 the r^(q-1) coefficient (:588-630);
+  //   b part [nspin2b][nordb+1]: the same for the e-e function, with the
+  //     sspinn factor on the Pade terms (:181-234);
+  //   c part [nctype][nterms]: the e-e-n term values pc = uu(k) ss(l) tt(m)
+  //     summed over pairs and centres of the type (:320-330).
+  // Pairs whose scaled distance is asymptotic skip the b part; pair-centre
+  // combinations with both e-n distances asymptotic skip the c part; e-n
+  // distances at the asymptote skip the a part (:150, :266, :553).
+  void jas_raw(double *out) const {
+    const int NA = s->norda + 1, NB = s->nordb + 1, NT = s->nterms;
+    const int ob = s->nctype * NA, oc = ob + s->nspin2b * NB;
+    std::fill(out, out + oc + s->nctype * NT, 0.0);
+    const double ar = s->asymp_r;
+    const int nordj = std::max(std::max(s->norda, s->nordb), s->nordc);
+    vector<double> UU(nordj + 4, 0), SS(nordj + 4, 0), TT(nordj + 4, 0), RI(nordj + 4, 0), RJ(nordj + 4, 0);
+    double *uu = &UU[3], *ss = &SS[3], *tt = &TT[3], *rri = &RI[3], *rrj = &RJ[3];
+    uu[0] = 1; ss[0] = 2; tt[0] = 1; rri[0] = 1; rrj[0] = 1;
+    for (int i = 1; i < N; i++)
+      for (int j = 0; j < i; j++) {
+        const int ij = i * (i - 1) / 2 + j;
+        double sspinn = 1;
+        int isb = 0;
+        if (i < s->nup || j >= s->nup) {
+          if (s->nspin2b == 2) isb = 1;
+          else if (s->nocuspb == 0) sspinn = 0.5;
+        }
+        double dd1;
+        scale_dist1(*s, r_ee[ij], uu[1], dd1);
+        if (uu[1] != ar) {
+          const double b1 = s->B(0, isb), b2 = s->B(1, isb);
+          double *g = out + ob + isb * NB;
+          g[0] += sspinn * uu[1] / (1 + b2 * uu[1]) - sspinn * ar / (1 + b2 * ar);
+          if (NB > 1) {
+            const double bot0 = 1 + b2 * uu[1];
+            g[1] += -sspinn * b1 * uu[1] * uu[1] / (bot0 * bot0) +
+                    sspinn * b1 * ar * ar / ((1 + b2 * ar) * (1 + b2 * ar));
+          }
+          for (int q = 3; q <= NB; q++) g[q - 1] += std::pow(uu[1], q - 1) - std::pow(ar, q - 1);
+        }
+        if (s->nordc <= 1) continue;
+        const double z = 1 - s->scalek * uu[1];
+        for (int iord = 1; iord <= s->nordc; iord++) uu[iord] = iord == 1 ? z : z * uu[iord - 1];
+        for (int ic = 0; ic < M; ic++) {
+          const int it = s->iwctype[ic];
+          double dd7, dd8;
+          scale_dist1(*s, r_en[i + N * ic], rri[1], dd7);
+          scale_dist1(*s, r_en[j + N * ic], rrj[1], dd8);
+          if (rri[1] == ar && rrj[1] == ar) continue;
+          rri[1] = 1 - s->scalek * rri[1];
+          rrj[1] = 1 - s->scalek * rrj[1];
+          for (int iord = 1; iord <= s->nordc; iord++) {
+            rri[iord] = rri[1] * rri[iord - 1];
+            rrj[iord] = rrj[1] * rrj[iord - 1];
+            ss[iord] = rri[iord] + rrj[iord];
+            tt[iord] = rri[iord] * rrj[iord];
+          }
+          double *g = out + oc + it * NT;
+          int ll = 0;
+          for (int n = 2; n <= s->nordc; n++)
+            for (int k = n - 1; k >= 0; k--) {
+              const int l_hi = (k == 0) ? n - k - 2 : n - k;
+              for (int l = l_hi; l >= 0; l--) {
+                const int m = (n - k - l) / 2;
+                if (2 * m == n - k - l) g[ll++] += uu[k] * ss[l] * tt[m];
+              }
+            }
+        }
+      }
+    for (int i = 0; i < N; i++)
+      for (int ic = 0; ic < M; ic++) {
+        const int it = s->iwctype[ic];
+        double r, dd7;
+        scale_dist1(*s, r_en[i + N * ic], r, dd7);
+        if (r == ar) continue;
+        const double a1 = s->A4(0, it), a2 = s->A4(1, it);
+        double *g = out + it * NA;
+        g[0] += r / (1 + a2 * r) - ar / (1 + a2 * ar);
+        if (NA > 1) {
+          const double bot0 = 1 + a2 * r;
+          g[1] += -a1 * r * r / (bot0 * bot0) + a1 * ar * ar / ((1 + a2 * ar) * (1 + a2 * ar));
+        }
+        for (int q = 3; q <= NA; q++) g[q - 1] += std::pow(r, q - 1) - std::pow(ar, q - 1);
+      }
+  }
+
   // ---- jastrow_factor4 (vmc/jastrow4.f90:3): full J with Laplacian ----
   void jastrow_factor4() {
     const int nordj = std::max(std::max(s->norda, s->nordb), s->nordc);
@@ -2550,6 +2640,17 @@ void dmc_end_block(DmcPop &P) {
 extern "C" {
 
 int or_nterms4(int nordc) { return nterms4(nordc); }
+
+// raw Jastrow parameter derivatives of one configuration x[N][3]
+int or_jas_nraw(void *sysp) {
+  const Sys *s = (const Sys *)sysp;
+  return s->nctype * (s->norda + 1) + s->nspin2b * (s->nordb + 1) + s->nctype * s->nterms;
+}
+void or_jas_raw(void *sys, const double *x, double *out) {
+  Walker w((const Sys *)sys);
+  w.distances(-1, x);
+  w.jas_raw(out);
+}
 
 void *or_sys_create(const cw_system_desc *d) {
   Sys *s = new Sys();

@@ -20,6 +20,8 @@ extern "C" {
 void *or_sys_create(const cw_system_desc *desc);
 void or_sys_destroy(void *sys);
 int or_nterms4(int nordc);
+int or_jas_nraw(void *sys);
+void or_jas_raw(void *sys, const double *x, double *out);
 
 /* pot_nn: nuclear repulsion (module pot, used by zerest vmc/acuest.f90). */
 double or_pot_nn(int ncent, const double *cent, const double *znuc, const int32_t *iwctype);

@@ -47,6 +47,8 @@ def lib():
         L.or_sites.argtypes = [V, _u64, _dp]
         L.or_orbitals.argtypes = [V, _dp, _dp, _dp, _dp]
         L.or_jastrow.argtypes = [V, _dp, _dp, _dp, _dp]
+        L.or_jas_nraw.argtypes = [V]
+        L.or_jas_raw.argtypes = [V, _dp, _dp]
         L.or_slater.argtypes = [V, _dp, _dp, _dp]
         L.or_hpsi.argtypes = [V, _dp, _dp, _dp, _dp, _dp]
         L.or_walkers_create.restype = V
@@ -119,6 +121,13 @@ class OracleSystem:
         d2 = np.zeros(1)
         lib().or_jastrow(self.h, dp(np.ascontiguousarray(x, float)), dp(psij), dp(v), dp(d2))
         return psij[0], v, d2[0]
+
+    def jas_raw(self, x):
+        """Raw Jastrow parameter derivatives dJ/dp of one configuration
+        (a part, b part, c part; see Walker::jas_raw)."""
+        out = np.zeros(lib().or_jas_nraw(self.h))
+        lib().or_jas_raw(self.h, dp(np.ascontiguousarray(x, float)), dp(out))
+        return out
 
     def slater(self, x):
         s = self.system

@@ -1,0 +1,121 @@
+"""Jastrow parameter derivatives of the oracle (deriv_jastrow4's gvalue),
+pinned by:
+
+* the cusp tables against the listing of dependent and varied e-e-n terms
+  in the reference's cuspexact4 header (vmc/cuspexact4.f90:1-30);
+* central finite differences of J = ln psi_J for every raw coefficient
+  (a, b, c taken on their own, the asymptotic constants following a and b);
+* central finite differences of J for every varied parameter of a jasderiv
+  selection, the cusp-fixed e-e-n terms recomputed after each perturbation
+  (cuspexact4) -- this checks the checkdepend4 map;
+* the parser of the jasderiv block."""
+import numpy as np
+import pytest
+
+from champ_b200 import jastrow_opt as jo
+from champ_b200.system import cuspinit4, make_synthetic, nterms4
+
+
+def _conf(oracle_mod, s, seed=3):
+    o = oracle_mod.OracleSystem(s)
+    st = oracle_mod.rng_states(seed + 1)
+    x, _ = o.sites(st[seed])
+    return o, x
+
+
+def _J(oracle_mod, s, x):
+    return oracle_mod.OracleSystem(s).jastrow(x)[0]
+
+
+def test_cusp_tables_match_reference_listing():
+    ee = [1, 4, 10, 19, 32, 49]
+    en = [2, 6, 12, 22, 35, 53]
+    for nord, ncum, nfree in ((5, 23, 15), (6, 37, 27), (7, 55, 43)):
+        d, iwc4, nt = cuspinit4(nord)
+        assert nt == nterms4(nord) == ncum
+        assert iwc4[1:nord] == ee[:nord - 1]
+        assert iwc4[nord:2 * nord - 1] == en[:nord - 1]
+        s = make_synthetic("tiny")
+        s.nordc = nord
+        free = jo.default_jasderiv(s).iwjasc[0]
+        assert len(free) == nfree
+    s = make_synthetic("tiny")
+    assert jo.default_jasderiv(s).iwjasc[0] == [3, 5, 7, 8, 9, 11, 13, 14, 15, 16, 17, 18, 20, 21, 23]
+    with pytest.raises(ValueError):
+        jo.checkdepend4(5, [[1, 3]])      # a cusp-fixed term may not be varied
+
+
+def _perturbed(s, part, idx, h):
+    import copy
+    t = copy.copy(s)
+    t.a4, t.b, t.c = np.array(s.a4, float).copy(), np.array(s.b, float).copy(), np.array(s.c, float).copy()
+    getattr(t, part)[idx] += h
+    t._keep = []
+    return t
+
+
+def test_raw_derivatives_finite_differences(oracle_mod):
+    s = make_synthetic("tiny")
+    o, x = _conf(oracle_mod, s)
+    raw = o.jas_raw(x)
+    lay = jo.raw_layout(s)
+    assert raw.size == lay["nraw"]
+    h = 1e-5
+    checked = 0
+    for r in range(lay["nraw"]):
+        if r < lay["b"]:
+            part, idx = "a4", divmod(r - lay["a"], lay["NA"])
+        elif r < lay["c"]:
+            part, idx = "b", divmod(r - lay["b"], lay["NB"])
+        else:
+            part, idx = "c", divmod(r - lay["c"], lay["NT"])
+        fd = (_J(oracle_mod, _perturbed(s, part, idx, h), x) -
+              _J(oracle_mod, _perturbed(s, part, idx, -h), x)) / (2 * h)
+        assert abs(fd - raw[r]) <= 2e-7 * max(1.0, abs(raw[r])), (part, idx, fd, raw[r])
+        checked += 1
+    assert checked == lay["nraw"]
+
+
+def test_param_map_finite_differences(oracle_mod):
+    s = make_synthetic("tiny")
+    o, x = _conf(oracle_mod, s, seed=5)
+    jd = jo.default_jasderiv(s)
+    P = jo.param_map(s, jd)
+    g = o.jas_raw(x) @ P
+    h = 1e-5
+    for k in range(jd.nparmj):
+        e = np.zeros(jd.nparmj)
+        e[k] = h
+        fd = (_J(oracle_mod, jo.apply_step(s, jd, e), x) - _J(oracle_mod, jo.apply_step(s, jd, -e), x)) / (2 * h)
+        assert abs(fd - g[k]) <= 2e-7 * max(1.0, abs(g[k])), (k, fd, g[k])
+
+
+def test_apply_step_keeps_cusp_conditions():
+    s = make_synthetic("tiny")
+    jd = jo.default_jasderiv(s)
+    t = jo.apply_step(s, jd, np.random.default_rng(1).normal(0, 0.01, jd.nparmj))
+    d, iwc4, nt = cuspinit4(s.nordc)
+    for it in range(s.nctype):
+        assert np.max(np.abs(d[1:, 1:] @ t.c[it])) < 1e-12
+    # a(1), b(1) are not in the default selection and stay put
+    assert np.array_equal(t.a4[:, 0], s.a4[:, 0]) and np.array_equal(t.b[:, 0], s.b[:, 0])
+
+
+def test_read_jasderiv():
+    text = """# comment line
+jasderiv
+4 4 5 15 0 0 0
+3 4 5 6
+3 4 5 6
+2 3 4 5 6
+3 5 7 8 9 11 13 14 15 16 17 18 20 21 23
+
+end
+"""
+    jd = jo.read_jasderiv(text, nctype=2)
+    assert jd.iwjasa == [[3, 4, 5, 6], [3, 4, 5, 6]]
+    assert jd.iwjasb == [[2, 3, 4, 5, 6]]
+    assert jd.iwjasc == [[3, 5, 7, 8, 9, 11, 13, 14, 15, 16, 17, 18, 20, 21, 23], []]
+    assert jd.nparmj == 4 + 4 + 5 + 15
+    with pytest.raises(ValueError):
+        jo.read_jasderiv("nothing here", nctype=1)
