@@ -22,6 +22,7 @@
 #include "move.cuh"
 #include "dmc.cuh"
 #include "mdet.cuh"
+#include "optjas.cuh"
 #include "peak.cuh"
 #include "umma.cuh"
 
@@ -69,11 +70,13 @@ struct cw_ctx {
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
   std::unordered_map<void *, size_t> alloc_bytes;
   double *bocc = nullptr;  // [nmax][K] coefficients of the occupied orbitals (c~ GEMM)
-  // CI-coefficient derivatives for optimisation (optci / SR sums)
+  // Parameter derivatives for optimisation (optjas gvalue, optci ci_o) and
+  // the SR sums over the optimisation vector [njas Jastrow | ndet CI]
   double *md_sgn = nullptr;                       // [ndet] orbital-order signs
   bool opt_ci = false, opt_oo = false;
-  int opt_w = 0;
-  double *ci_o = nullptr, *ci_ot = nullptr;       // [W][ndet], [ndet][W]
+  int opt_w = 0, opt_njas = 0, opt_np = 0, jas_nraw = 0;
+  double *opt_o = nullptr, *opt_ot = nullptr;     // [W][np], [np][W]
+  double *jas_raw = nullptr, *jas_map = nullptr;  // [W][nraw], [nraw][njas]
   double *sr_o = nullptr, *sr_eo = nullptr, *sr_oo = nullptr, *oo_tmp = nullptr;
   double sr_w = 0;
   std::vector<void *> opt_allocs;
@@ -568,16 +571,40 @@ int md_after_commit(cw_ctx *c, int iel) {
 }
 
 // Full local energy of every walker (hpsi).  mode 1 also adds metrop6's sums.
-// CI derivatives of every walker after a sweep's hpsi and the SR sums
-int opt_ci_accum(cw_ctx *c) {
-  const int W = c->W, nd = c->h.ndet;
-  k_md_ci_o<<<W, 128, 0, c->stream>>>(c->st, c->md, c->mdt, c->md_sgn, c->ci_o, c->ci_ot);
-  LCHK("k_md_ci_o");
-  k_sr_accum<<<(nd + 127) / 128, 128, 0, c->stream>>>(c->st, c->ci_o, c->sr_o, c->sr_eo);
+template <int NORD>
+void launch_jas_raw(cw_ctx *c) {
+  k_jas_raw<NORD><<<c->W, kJasThreads, 0, c->stream>>>(c->st, c->jas_raw, c->jas_nraw);
+}
+
+// Parameter derivatives of every walker at the current configurations (the
+// last hpsi): Jastrow part, then CI part of the optimisation vector
+int opt_derivs(cw_ctx *c) {
+  const int W = c->W;
+  if (c->opt_njas > 0) {
+    NORD_DISPATCH(launch_jas_raw, c);
+    LCHK("k_jas_raw");
+    const long n = (long)W * c->opt_njas;
+    k_jas_o<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(W, c->jas_raw, c->jas_nraw, c->jas_map, c->opt_njas,
+                                                                c->opt_np, c->opt_o, c->opt_ot);
+    LCHK("k_jas_o");
+  }
+  if (c->opt_ci) {
+    k_md_ci_o<<<W, 128, 0, c->stream>>>(c->st, c->md, c->mdt, c->md_sgn, c->opt_o, c->opt_ot, c->opt_np,
+                                        c->opt_njas);
+    LCHK("k_md_ci_o");
+  }
+  return CW_OK;
+}
+
+// Derivatives of every walker after a sweep's hpsi and the SR sums
+int opt_accum(cw_ctx *c) {
+  const int W = c->W, nd = c->opt_np;
+  if (int rc = opt_derivs(c)) return rc;
+  k_sr_accum<<<(nd + 127) / 128, 128, 0, c->stream>>>(c->st, c->opt_o, nd, c->sr_o, c->sr_eo);
   LCHK("k_sr_accum");
   if (c->opt_oo) {
-    // sum_w O O^T as one GEMM over the walkers: [nd x W] x [W x nd]
-    dgemm(c->stream, nd, nd, W, c->ci_ot, c->ci_o, c->oo_tmp);
+    // sum_w O O^T as one GEMM over the walkers: [np x W] x [W x np]
+    dgemm(c->stream, nd, nd, W, c->opt_ot, c->opt_o, c->oo_tmp);
     const size_t n = (size_t)nd * nd;
     k_add_inplace<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->sr_oo, c->oo_tmp, n);
     LCHK("k_add_inplace");
@@ -696,11 +723,20 @@ void drop_sweep_graph(cw_ctx *c) {
   c->sweep_graph = nullptr;
 }
 
+// drop the optimisation buffers (sized for one population)
+void opt_reset(cw_ctx *c) {
+  free_list(c, c->opt_allocs);
+  c->opt_ci = c->opt_oo = false;
+  c->opt_njas = c->opt_np = c->jas_nraw = 0;
+  c->opt_o = c->opt_ot = c->jas_raw = c->jas_map = nullptr;
+  c->sr_o = c->sr_eo = c->sr_oo = c->oo_tmp = nullptr;
+  c->sr_w = 0;
+}
+
 int alloc_walkers(cw_ctx *c, int W) {
   drop_sweep_graph(c);  // the captured sweep holds this population's buffers
   free_dmc(c);
-  free_list(c, c->opt_allocs);  // derivative buffers are sized for the old population
-  c->opt_ci = c->opt_oo = false;
+  opt_reset(c);  // derivative buffers are sized for the old population
   free_list(c, c->w_allocs);
   const CSys &h = c->h;
   const int N = h.N, M = h.M, K = h.K, Oa = h.Oa, nmax = h.nmax, NQ = std::max(h.nquad, 1);
@@ -1331,8 +1367,8 @@ int vmc_sweep(cw_ctx *c) {
   }
   int rc = run_hpsi(c, 1);
   if (rc) return rc;
-  if (c->opt_ci) {
-    rc = opt_ci_accum(c);
+  if (c->opt_np > 0) {
+    rc = opt_accum(c);
     if (rc) return rc;
   }
   return CW_OK;
@@ -1375,7 +1411,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
     for (int s = 0; s < nstep; s++) CK(cudaGraphLaunch(c->sweep_exec, c->stream));
     c->launches += (long)nstep * c->sweep_launches;
   }
-  if (c->opt_ci) c->sr_w += (double)c->W * nstep;  // samples of the optimisation sums
+  if (c->opt_np > 0) c->sr_w += (double)c->W * nstep;  // samples of the optimisation sums
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0;
@@ -1451,58 +1487,98 @@ int cw_results_state(cw_ctx *c, int istate, double *out) {
   return CW_OK;
 }
 
-int cw_opt_ci(cw_ctx *c, int enable, int with_overlap) {
-  if (!c) return CW_ERR_ARG;
+int cw_jas_nraw(cw_ctx *c, int *nraw) {
+  if (!c || !nraw) return CW_ERR_ARG;
+  const CSys &h = c->h;
+  *nraw = h.nctype * (h.norda + 1) + h.nspin2b * (h.nordb + 1) + (h.nordc > 1 ? h.nctype * h.nterms : 0);
+  return CW_OK;
+}
+
+int cw_opt_setup(cw_ctx *c, int ci, int njas, const double *jas_map, int with_overlap) {
+  if (!c || njas < 0 || (njas > 0 && !jas_map)) return CW_ERR_ARG;
   BIND(c);
   drop_sweep_graph(c);  // the sweep gains or loses the derivative launches
-  free_list(c, c->opt_allocs);
-  c->opt_ci = c->opt_oo = false;
-  c->ci_o = c->ci_ot = c->sr_o = c->sr_eo = c->sr_oo = c->oo_tmp = nullptr;
-  c->sr_w = 0;
-  if (!enable) return CW_OK;
-  if (!c->md_on) return fail(c, CW_ERR_UNSUPPORTED, "CI derivatives need a multideterminant expansion");
-  if (c->h.nstates > 1) return fail(c, CW_ERR_UNSUPPORTED, "CI derivatives of several states are not implemented");
+  opt_reset(c);
+  if (!ci && njas == 0) return CW_OK;
+  if (ci && !c->md_on) return fail(c, CW_ERR_UNSUPPORTED, "CI derivatives need a multideterminant expansion");
+  if (c->h.nstates > 1) return fail(c, CW_ERR_UNSUPPORTED, "parameter derivatives of several states are not implemented");
+  if (njas > 0 && (c->h.norda < 1 || c->h.nordb < 1))
+    return fail(c, CW_ERR_UNSUPPORTED, "Jastrow derivatives need norda >= 1 and nordb >= 1 (Pade a(2), b(2))");
   if (c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
-  const int W = c->W, nd = c->h.ndet;
-  if (with_overlap && (size_t)nd * nd > ((size_t)1 << 27))
-    return fail(c, CW_ERR_ARG, "overlap of %d coefficients exceeds 2^27 entries", nd);
+  const int W = c->W, np = njas + (ci ? c->h.ndet : 0);
+  if (with_overlap && (size_t)np * np > ((size_t)1 << 27))
+    return fail(c, CW_ERR_ARG, "overlap of %d parameters exceeds 2^27 entries", np);
   auto &L = c->opt_allocs;
-  DALLOC(L, c->ci_o, (size_t)W * nd);
-  DALLOC(L, c->ci_ot, (size_t)W * nd);
-  DALLOC(L, c->sr_o, nd);
-  DALLOC(L, c->sr_eo, nd);
-  CK(cudaMemsetAsync(c->sr_o, 0, sizeof(double) * nd, c->stream));
-  CK(cudaMemsetAsync(c->sr_eo, 0, sizeof(double) * nd, c->stream));
+  DALLOC(L, c->opt_o, (size_t)W * np);
+  DALLOC(L, c->opt_ot, (size_t)W * np);
+  DALLOC(L, c->sr_o, np);
+  DALLOC(L, c->sr_eo, np);
+  CK(cudaMemsetAsync(c->sr_o, 0, sizeof(double) * np, c->stream));
+  CK(cudaMemsetAsync(c->sr_eo, 0, sizeof(double) * np, c->stream));
   if (with_overlap) {
-    DALLOC(L, c->sr_oo, (size_t)nd * nd);
-    DALLOC(L, c->oo_tmp, (size_t)nd * nd);
-    CK(cudaMemsetAsync(c->sr_oo, 0, sizeof(double) * nd * nd, c->stream));
+    DALLOC(L, c->sr_oo, (size_t)np * np);
+    DALLOC(L, c->oo_tmp, (size_t)np * np);
+    CK(cudaMemsetAsync(c->sr_oo, 0, sizeof(double) * np * np, c->stream));
   }
-  c->opt_ci = true;
+  if (njas > 0) {
+    int nraw = 0;
+    cw_jas_nraw(c, &nraw);
+    DALLOC(L, c->jas_raw, (size_t)W * nraw);
+    DALLOC(L, c->jas_map, (size_t)nraw * njas);
+    CK(cudaMemcpyAsync(c->jas_map, jas_map, sizeof(double) * nraw * njas, cudaMemcpyHostToDevice, c->stream));
+    c->jas_nraw = nraw;
+  }
+  c->opt_ci = ci != 0;
+  c->opt_njas = njas;
+  c->opt_np = np;
   c->opt_oo = with_overlap != 0;
   c->opt_w = W;
   // derivatives at the current configurations (the last hpsi)
-  k_md_ci_o<<<W, 128, 0, c->stream>>>(c->st, c->md, c->mdt, c->md_sgn, c->ci_o, c->ci_ot);
-  LCHK("k_md_ci_o");
+  if (int rc = opt_derivs(c)) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return CW_OK;
+}
+
+int cw_opt_ci(cw_ctx *c, int enable, int with_overlap) { return cw_opt_setup(c, enable, 0, nullptr, with_overlap); }
+
+// columns [off, off+n) of the optimisation vector of every walker
+static int opt_columns(cw_ctx *c, int off, int n, double *out) {
+  BIND(c);
+  CK(cudaMemcpy2DAsync(out, sizeof(double) * n, c->opt_o + off, sizeof(double) * c->opt_np, sizeof(double) * n,
+                       c->W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return CW_OK;
 }
 
 int cw_ci_o(cw_ctx *c, double *out) {
   if (!c || !out) return CW_ERR_ARG;
-  if (!c->opt_ci || c->opt_w != c->W) return fail(c, CW_ERR_STATE, "cw_opt_ci not enabled for this population");
+  if (!c->opt_ci || c->opt_w != c->W) return fail(c, CW_ERR_STATE, "CI derivatives not enabled for this population");
+  return opt_columns(c, c->opt_njas, c->h.ndet, out);
+}
+
+int cw_jas_o(cw_ctx *c, double *out) {
+  if (!c || !out) return CW_ERR_ARG;
+  if (c->opt_njas == 0 || c->opt_w != c->W)
+    return fail(c, CW_ERR_STATE, "Jastrow derivatives not enabled for this population");
+  return opt_columns(c, 0, c->opt_njas, out);
+}
+
+int cw_jas_raw(cw_ctx *c, double *out) {
+  if (!c || !out) return CW_ERR_ARG;
+  if (c->opt_njas == 0 || c->opt_w != c->W)
+    return fail(c, CW_ERR_STATE, "Jastrow derivatives not enabled for this population");
   BIND(c);
-  CK(cudaMemcpyAsync(out, c->ci_o, sizeof(double) * c->W * c->h.ndet, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(out, c->jas_raw, sizeof(double) * c->W * c->jas_nraw, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return CW_OK;
 }
 
-int cw_opt_ci_sums(cw_ctx *c, double *o, double *eo, double *oo, double *wsum) {
+int cw_opt_sums(cw_ctx *c, double *o, double *eo, double *oo, double *wsum) {
   if (!c || !o || !eo || !wsum) return CW_ERR_ARG;
-  if (!c->opt_ci || c->opt_w != c->W) return fail(c, CW_ERR_STATE, "cw_opt_ci not enabled for this population");
+  if (c->opt_np == 0 || c->opt_w != c->W) return fail(c, CW_ERR_STATE, "optimisation sums not enabled for this population");
   if (oo && !c->opt_oo) return fail(c, CW_ERR_STATE, "overlap sums not enabled");
   BIND(c);
-  const int nd = c->h.ndet;
+  const int nd = c->opt_np;
   CK(cudaMemcpyAsync(o, c->sr_o, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(eo, c->sr_eo, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream));
   if (oo) CK(cudaMemcpyAsync(oo, c->sr_oo, sizeof(double) * nd * nd, cudaMemcpyDeviceToHost, c->stream));
@@ -1513,6 +1589,10 @@ int cw_opt_ci_sums(cw_ctx *c, double *o, double *eo, double *oo, double *wsum) {
   *wsum = c->sr_w;
   c->sr_w = 0;
   return CW_OK;
+}
+
+int cw_opt_ci_sums(cw_ctx *c, double *o, double *eo, double *oo, double *wsum) {
+  return cw_opt_sums(c, o, eo, oo, wsum);
 }
 
 int cw_state_energies(cw_ctx *c, double *energy, double *psid) {

@@ -505,7 +505,10 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
 // coefficients, so the derivative is taken for the input coefficients), in
 // both walker-major and determinant-major layouts (the latter feeds the
 // overlap GEMM).  CTA per walker.
-__global__ void k_md_ci_o(WState st, MdBuf md, MdTab tab, const double *sgn, double *o, double *ot) {
+// (columns off .. off+ndet-1 of the optimisation vector o, row stride np,
+// and the same rows of its transpose ot [np][W])
+__global__ void k_md_ci_o(WState st, MdBuf md, MdTab tab, const double *sgn, double *o, double *ot, int np,
+                          int off) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const double iS = 1.0 / md.S[w];
@@ -514,19 +517,20 @@ __global__ void k_md_ci_o(WState st, MdBuf md, MdTab tab, const double *sgn, dou
     const double d0 = k0 >= 0 ? md.dd[((size_t)w * 2 + 0) * tab.numax + k0] : 1.0;
     const double d1 = k1 >= 0 ? md.dd[((size_t)w * 2 + 1) * tab.numax + k1] : 1.0;
     const double v = sgn[k] * (d0 * d1 * iS);
-    o[(size_t)w * cs.ndet + k] = v;
-    ot[(size_t)k * st.W + w] = v;
+    o[(size_t)w * np + off + k] = v;
+    ot[(size_t)(off + k) * st.W + w] = v;
   }
 }
 
 // SR sums (optwf_store's sr_o contracted per sample): sum_w O_k and
-// sum_w E_w O_k, thread per determinant, walkers in order
-__global__ void k_sr_accum(WState st, const double *o, double *sr_o, double *sr_eo) {
+// sum_w E_w O_k over the np entries of the optimisation vector, thread per
+// entry, walkers in order
+__global__ void k_sr_accum(WState st, const double *o, int np, double *sr_o, double *sr_eo) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= cs.ndet) return;
+  if (k >= np) return;
   double a = 0, b = 0;
   for (int w = 0; w < st.W; w++) {
-    const double v = o[(size_t)w * cs.ndet + k];
+    const double v = o[(size_t)w * np + k];
     a += v;
     b += st.eold[w] * v;
   }

@@ -154,9 +154,47 @@ class Engine:
         self._check(self.lib.cw_state_energies(self.h, dptr(e), dptr(p)), "cw_state_energies")
         return e, p
 
-    # -- wave-function optimisation (CI coefficients) ----------------------
+    # -- wave-function optimisation (Jastrow and CI parameters) ------------
     def opt_ci(self, enable: bool = True, overlap: bool = True):
         self._check(self.lib.cw_opt_ci(self.h, 1 if enable else 0, 1 if overlap else 0), "cw_opt_ci")
+        self._opt_np = self.system.iworbd.shape[0] if enable else 0
+        self._opt_njas = 0
+
+    def opt_setup(self, ci: bool = False, jas_map=None, overlap: bool = True):
+        """Derivatives and SR sums over the optimisation vector [Jastrow
+        parameters | CI coefficients]; jas_map is the [nraw, njas] map of
+        jastrow_opt.param_map (None: no Jastrow parameters)."""
+        njas = 0 if jas_map is None else int(np.asarray(jas_map).shape[1])
+        m = None if jas_map is None else np.ascontiguousarray(jas_map, dtype=np.float64)
+        if m is not None and m.shape[0] != self.jas_nraw():
+            raise ValueError(f"jas_map has {m.shape[0]} rows, the engine's raw vector {self.jas_nraw()}")
+        self._check(self.lib.cw_opt_setup(self.h, 1 if ci else 0, njas, dptr(m) if m is not None else None,
+                                          1 if overlap else 0), "cw_opt_setup")
+        self._opt_njas = njas
+        self._opt_np = njas + (self.system.iworbd.shape[0] if ci else 0)
+
+    def jas_nraw(self) -> int:
+        n = C.c_int(0)
+        self._check(self.lib.cw_jas_nraw(self.h, C.byref(n)), "cw_jas_nraw")
+        return n.value
+
+    def jas_raw(self):
+        out = np.zeros((self.W, self.jas_nraw()))
+        self._check(self.lib.cw_jas_raw(self.h, dptr(out)), "cw_jas_raw")
+        return out
+
+    def jas_o(self):
+        out = np.zeros((self.W, self._opt_njas))
+        self._check(self.lib.cw_jas_o(self.h, dptr(out)), "cw_jas_o")
+        return out
+
+    def opt_sums(self, overlap: bool = True):
+        n = self._opt_np
+        o, eo, w = np.zeros(n), np.zeros(n), np.zeros(1)
+        oo = np.zeros((n, n)) if overlap else None
+        self._check(self.lib.cw_opt_sums(self.h, dptr(o), dptr(eo), dptr(oo) if overlap else None, dptr(w)),
+                    "cw_opt_sums")
+        return dict(o=o, eo=eo, oo=oo, wsum=float(w[0]))
 
     def ci_o(self):
         nd = self.system.iworbd.shape[0]

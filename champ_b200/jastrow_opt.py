@@ -219,13 +219,16 @@ def apply_step(system, jd: JasDeriv, dp) -> object:
 
 
 def default_jasderiv(system) -> JasDeriv:
-    """Every free parameter of the system: a(2) and the polynomial a terms
-    of each type (a(1) held at its cusp / pseudopotential value), b(2) and
-    the polynomial b terms, and every e-e-n term the cusp conditions leave
-    free."""
+    """Every free parameter of the system, as CHAMP's input checks allow
+    them (read_jasderiv_file, vmc/read_data_parser.f90:1622-1660): the
+    polynomial a terms of each type, and a(2) too for all-electron systems
+    (with pseudopotentials a(1) and a(2) stay fixed); b(2) and the
+    polynomial b terms (b(1) is fixed by the e-e cusp); every e-e-n term the
+    cusp conditions leave free."""
     lay = raw_layout(system)
     nct, nsb = system.nctype, int(getattr(system, "nspin2b", 1))
-    iwa = [list(range(2, lay["NA"] + 1)) for _ in range(nct)]
+    a_first = 3 if int(getattr(system, "nloc", 0)) > 0 else 2
+    iwa = [list(range(a_first, lay["NA"] + 1)) for _ in range(nct)]
     iwb = [list(range(2, lay["NB"] + 1)) for _ in range(nsb)]
     if system.nordc > 1:
         _, iwc4, nt = cuspinit4(system.nordc)

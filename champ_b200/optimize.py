@@ -29,14 +29,23 @@ def sr_matrices(sums: dict, energy: float):
     return S, g
 
 
-def sr_step(sums: dict, cdet: np.ndarray, energy: float, tau: float = 0.02, adiag: float = 0.01,
-            fixed: int = 0) -> np.ndarray:
-    """New CI coefficients after one SR step of length tau."""
+def sr_delta(sums: dict, energy: float, tau: float = 0.02, adiag: float = 0.01, fixed=None) -> np.ndarray:
+    """Parameter change of one SR step of length tau over the whole
+    optimisation vector (Jastrow parameters, then CI coefficients, as
+    cw_opt_sums lays them out); the entry `fixed` (an index, or None) is
+    held, as the one CI coefficient CHAMP leaves out of the varied set."""
     S, g = sr_matrices(sums, energy)
-    keep = np.array([k for k in range(len(cdet)) if k != fixed])
+    n = len(g)
+    keep = np.array([k for k in range(n) if k != fixed])
     Sr = S[np.ix_(keep, keep)].copy()
     Sr[np.diag_indices_from(Sr)] *= 1.0 + adiag
-    dp = np.linalg.solve(Sr, -tau * g[keep])
-    out = np.array(cdet, float).copy()
-    out[keep] += dp
-    return out
+    dp = np.zeros(n)
+    dp[keep] = np.linalg.solve(Sr, -tau * g[keep])
+    return dp
+
+
+def sr_step(sums: dict, cdet: np.ndarray, energy: float, tau: float = 0.02, adiag: float = 0.01,
+            fixed: int = 0) -> np.ndarray:
+    """New CI coefficients after one SR step of length tau (sums over the
+    CI coefficients alone)."""
+    return np.array(cdet, float) + sr_delta(sums, energy, tau, adiag, fixed)

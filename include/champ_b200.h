@@ -183,10 +183,34 @@ int cw_results_state(cw_ctx *ctx, int istate, double *out);
  * expansion with one state; enable after cw_set_walkers (a new population
  * disables it).  cw_opt_ci_sums copies the sums (o, eo [ndet], oo
  * [ndet][ndet] or NULL, wsum = number of samples) and resets them;
- * cw_ci_o gives the per-walker derivatives of the last hpsi, [nwalk][ndet]. */
+ * cw_ci_o gives the per-walker derivatives of the last hpsi, [nwalk][ndet].
+ * cw_opt_ci(ctx, e, ov) is cw_opt_setup(ctx, e, 0, NULL, ov) and
+ * cw_opt_ci_sums is cw_opt_sums. */
 int cw_opt_ci(cw_ctx *ctx, int enable, int with_overlap);
 int cw_opt_ci_sums(cw_ctx *ctx, double *o, double *eo, double *oo, double *wsum);
 int cw_ci_o(cw_ctx *ctx, double *out);
+
+/* Jastrow and CI parameters together: the optimisation vector of a walker is
+ * [njas Jastrow parameters | ndet CI coefficients when ci != 0], the layout
+ * of optwf_store's sr_o (vmc/optwf_handle_wf.f90:1517-1521).  The Jastrow
+ * part is deriv_jastrow4's gvalue (vmc/deriv_jastrow4.f90, d ln psi / d p of
+ * the varied a, b, c parameters with the cusp-fixed e-e-n terms folded in by
+ * checkdepend4's dependencies): the engine computes the raw derivative of J
+ * with respect to every Jastrow coefficient -- cw_jas_nraw entries per
+ * walker, [nctype][norda+1] a (1 = a(1), 2 = a(2), q >= 3 the r^(q-1)
+ * coefficient), [nspin2b][nordb+1] b (the same for e-e), [nctype][nterms]
+ * e-e-n terms -- and applies jas_map ([nraw][njas], row-major, built on the
+ * host from the jasderiv selection) to it.  After every VMC sweep the sums
+ * of cw_opt_sums run over the whole vector: o, eo [np], oo [np][np] (with
+ * with_overlap), wsum; np = njas + (ci ? ndet : 0).  ci = 0 and njas = 0
+ * disables.  Needs one state; Jastrow derivatives need norda, nordb >= 1.
+ * cw_jas_raw gives the raw derivatives of the last hpsi [nwalk][nraw],
+ * cw_jas_o the Jastrow part of the vector [nwalk][njas]. */
+int cw_opt_setup(cw_ctx *ctx, int ci, int njas, const double *jas_map, int with_overlap);
+int cw_opt_sums(cw_ctx *ctx, double *o, double *eo, double *oo, double *wsum);
+int cw_jas_nraw(cw_ctx *ctx, int *nraw);
+int cw_jas_raw(cw_ctx *ctx, double *out);
+int cw_jas_o(cw_ctx *ctx, double *out);
 
 /* Per-walker local energies and psi_D of every state from the last hpsi:
  * energy, psid [nwalk][nstates]. */

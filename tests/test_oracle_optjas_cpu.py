@@ -119,3 +119,26 @@ end
     assert jd.nparmj == 4 + 4 + 5 + 15
     with pytest.raises(ValueError):
         jo.read_jasderiv("nothing here", nctype=1)
+
+
+def test_sr_delta_over_the_joint_vector(oracle_mod):
+    """SR step over [Jastrow | CI]: sums of oracle samples of the tiny
+    system's Jastrow derivatives; the step is a descent direction of the
+    SR metric (g . dp = -tau g S^-1 g < 0) and leaves the held entry."""
+    from champ_b200 import optimize
+    s = make_synthetic("tiny")
+    o = oracle_mod.OracleSystem(s)
+    P = jo.param_map(s, jo.default_jasderiv(s))
+    st = oracle_mod.rng_states(24)
+    O, E = [], []
+    for w in range(24):
+        x, _ = o.sites(st[w])
+        O.append(o.jas_raw(x) @ P)
+        E.append(o.hpsi(x)["energy"])
+    O, E = np.array(O), np.array(E)
+    sums = dict(o=O.sum(0), eo=(E[:, None] * O).sum(0), oo=O.T @ O, wsum=float(len(E)))
+    S, g = optimize.sr_matrices(sums, E.mean())
+    dp = optimize.sr_delta(sums, E.mean(), tau=0.05, adiag=0.1, fixed=3)
+    assert dp[3] == 0.0
+    keep = [k for k in range(len(g)) if k != 3]
+    assert g[keep] @ dp[keep] < 0
