@@ -408,26 +408,30 @@ def run_ours(args):
         pg.close()
         return 0
     peaks, peak_kind = load_peaks()
-    fp64_peak = None
+    # the move Jastrow runs in FP64 (fp64 path) or FP32 (mixed path): its
+    # roofline denominator is the measured FMA peak of that pipe
+    fp64 = args.precision == "fp64"
+    fma_peak = None
     try:
         import ctypes as C
         from champ_b200.abi import load_engine
         t = np.zeros(1)
-        if load_engine().cw_fma_peak(local, 1, t.ctypes.data_as(C.POINTER(C.c_double))) == 0:
-            fp64_peak = float(t[0])
+        if load_engine().cw_fma_peak(local, 1 if fp64 else 0, t.ctypes.data_as(C.POINTER(C.c_double))) == 0:
+            fma_peak = float(t[0])
     except Exception:
-        fp64_peak = None
+        fma_peak = None
     alg = algorithmic(system, W)
     ms_jm, n_jm = stages["jastrow_move"]
     ms_acc, n_acc = stages["accept"]
     total_stage = sum(v[0] for v in stages.values())
     top = max(stages.items(), key=lambda kv: kv[1][0])
     jm_tflops = alg["f_jastrow_move"] / (ms_jm / n_jm * 1e-3) / 1e12
-    roof = {"kernel": "k_jastrow_move (jastrow4e, one electron, all walkers)", "bound": "fp64-simt",
-            "achieved": jm_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
-            "frac": (jm_tflops / fp64_peak) if fp64_peak else None,
-            "peak_source": "measured FP64 FMA probe (cw_fma_peak) on this GPU",
-            "traffic": jm_traffic(W) if args.precision == "fp64" else None,
+    roof = {"kernel": ("k_jastrow_move" if fp64 else "k_jastrow_move_f32") + " (jastrow4e, one electron, all walkers)",
+            "bound": "fp64-simt" if fp64 else "fp32-simt",
+            "achieved": jm_tflops, "peak": fma_peak, "unit": "TFLOP/s",
+            "frac": (jm_tflops / fma_peak) if fma_peak else None,
+            "peak_source": f"measured {'FP64' if fp64 else 'FP32'} FMA probe (cw_fma_peak) on this GPU",
+            "traffic": jm_traffic(W) if fp64 else None,
             "traffic_source": "dram bytes of one ncu capture at 2048 walkers, scaled by the walker count",
             "share_of_step": ms_jm / total_stage,
             "work_per_launch": "8*(N-1)*M*T + 8*(N-1)*nordb + 8*M*norda FLOP per walker (T=23 e-e-n terms)"}

@@ -407,16 +407,18 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
     }
     if (NORD > 1) {
       // partners' e-n values from the walker's table (coalesced over lanes),
-      // loaded one centre ahead
+      // loaded two centres ahead (the table comes from DRAM)
       const double *en_rr = st.enm + (size_t)w * 2 * M * N;
       const double *en_h = en_rr + (size_t)M * N;
       int jt[P];
-      double nrr[P], nh[P];
+      double nrr[P], nh[P], nrr2[P], nh2[P];
 #pragma unroll
       for (int q = 0; q < P; q++) {
         jt[q] = ok[q] ? jj[q] : (iel == 0 ? N - 1 : 0);
         nrr[q] = en_rr[jt[q]];
         nh[q] = en_h[jt[q]];
+        nrr2[q] = M > 1 ? en_rr[N + jt[q]] : 0.0;
+        nh2[q] = M > 1 ? en_h[N + jt[q]] : 0.0;
       }
       for (int ic = 0; ic < M; ic++) {
         double rrj[P], hj[P], y[P];
@@ -426,9 +428,11 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
         for (int q = 0; q < P; q++) {
           rrj[q] = nrr[q];
           hj[q] = nh[q];
-          if (ic + 1 < M) {
-            nrr[q] = en_rr[(ic + 1) * N + jt[q]];
-            nh[q] = en_h[(ic + 1) * N + jt[q]];
+          nrr[q] = nrr2[q];
+          nh[q] = nh2[q];
+          if (ic + 2 < M) {
+            nrr2[q] = en_rr[(ic + 2) * N + jt[q]];
+            nh2[q] = en_h[(ic + 2) * N + jt[q]];
           }
           any |= ok[q] && !(rri == asym && rrj[q] == asym);
           y[q] = 1 - kap * rrj[q];
@@ -590,12 +594,16 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
       const float du_r = du / rij;
       const float *en_rr = st.enmf + (size_t)w * 2 * M * N + jj;
       const float *en_h = en_rr + (size_t)M * N;
+      // partner table values two centres ahead
       float nrr = en_rr[0], nh = en_h[0];
+      float nrr2 = M > 1 ? en_rr[N] : 0.0f, nh2 = M > 1 ? en_h[N] : 0.0f;
       for (int ic = 0; ic < M; ic++) {
         const float rrj = nrr, hj = nh;
-        if (ic + 1 < M) {
-          nrr = en_rr[(size_t)(ic + 1) * N];
-          nh = en_h[(size_t)(ic + 1) * N];
+        nrr = nrr2;
+        nh = nh2;
+        if (ic + 2 < M) {
+          nrr2 = en_rr[(size_t)(ic + 2) * N];
+          nh2 = en_h[(size_t)(ic + 2) * N];
         }
         const float rri = sh_s[ic];
         if (rri == asym && rrj == asym) continue;

@@ -13,6 +13,8 @@ normalisation, the step holds one coefficient (`fixed`, the reference
 determinant by default) and moves the others."""
 from __future__ import annotations
 
+import copy
+
 import numpy as np
 
 
@@ -49,3 +51,45 @@ def sr_step(sums: dict, cdet: np.ndarray, energy: float, tau: float = 0.02, adia
     """New CI coefficients after one SR step of length tau (sums over the
     CI coefficients alone)."""
     return np.array(cdet, float) + sr_delta(sums, energy, tau, adiag, fixed)
+
+
+def sr_optimize(system, jd=None, ci: bool = False, nwalk: int = 256, iters: int = 5, nblock: int = 4,
+                nstep: int = 10, tau: float = 0.02, adiag: float = 0.01, precision: str = "fp64",
+                seed_offset: int = 0, engine_factory=None):
+    """SR optimisation loop over Jastrow (jasderiv selection `jd`) and, with
+    `ci`, CI parameters, as CHAMP's optwf driver runs it with method sr_n:
+    per iteration nblock VMC blocks of nstep sweeps on the engine with the
+    derivative sums on, one SR step over the joint vector (the reference CI
+    coefficient held), new parameters (cusp-fixed e-e-n terms recomputed),
+    walkers carried over to the next iteration's engine.  Returns the final
+    system and per-iteration (energy, error) of the sampled wave function."""
+    from . import jastrow_opt
+    from .engine import Engine, initial_configs, rng_states
+    make = engine_factory or (lambda s: Engine(s, precision=precision))
+    rng = rng_states(seed_offset + nwalk)[seed_offset:].copy()
+    x = initial_configs(system, rng)
+    history = []
+    for _ in range(iters):
+        eng = make(system)
+        try:
+            eng.set_walkers(x, rng)
+            P = jastrow_opt.param_map(system, jd) if jd is not None and jd.nparmj else None
+            eng.opt_setup(ci=ci, jas_map=P, overlap=True)
+            for _ in range(nblock):
+                eng.vmc_steps(nstep)
+                eng.end_block()
+            r = eng.results()
+            sums = eng.opt_sums(overlap=True)
+            x, rng = eng.walkers()
+        finally:
+            eng.close()
+        history.append((float(r["energy"]), float(r["err"])))
+        nj = 0 if P is None else P.shape[1]
+        dp = sr_delta(sums, float(r["energy"]), tau, adiag, fixed=nj if ci else None)
+        if nj:
+            system = jastrow_opt.apply_step(system, jd, dp[:nj])
+        if ci:
+            system = copy.copy(system)
+            system.cdet = np.array(system.cdet, float) + dp[nj:]
+            system._keep = []
+    return system, history

@@ -90,3 +90,18 @@ def test_opt_setup_refusals():
     eng.opt_setup()                              # disable
     with pytest.raises(EngineError):
         eng.jas_o()
+
+
+def test_sr_optimize_loop():
+    """The optwf loop on the GPU: parameters move, the cusp conditions hold
+    after every step, energies stay finite."""
+    from champ_b200 import jastrow_opt as jo
+    from champ_b200 import optimize
+    from champ_b200.system import cuspinit4, make_synthetic
+    s = make_synthetic("tiny")
+    jd = jo.default_jasderiv(s)
+    t, hist = optimize.sr_optimize(s, jd, nwalk=128, iters=3, nblock=2, nstep=5, tau=0.02)
+    assert len(hist) == 3 and all(np.isfinite(e) and np.isfinite(err) for e, err in hist)
+    assert not np.array_equal(t.c, s.c)
+    d, _, _ = cuspinit4(s.nordc)
+    assert np.max(np.abs(d[1:, 1:] @ t.c.T)) < 1e-12
