@@ -667,39 +667,45 @@ __device__ __forceinline__ void een_fold2(const T *__restrict__ cc, T x, T *BD4)
   xp[0] = 1;
 #pragma unroll
   for (int q = 1; q <= NORD; q++) xp[q] = xp[q - 1] * x;
-  T B[een_nb(NORD)], dB[een_nb(NORD)], d2B[een_nb(NORD)];
+  // one output entry at a time (gather form: every term's contributions to
+  // entry t, in term order), so only three accumulators are live
 #pragma unroll
-  for (int t = 0; t < een_nb(NORD); t++) B[t] = dB[t] = d2B[t] = 0;
-  int ll = 0;
+  for (int t = 0; t < een_nb(NORD); t++) {
+    T B = 0, dB = 0, d2B = 0;
+    int ll = 0;
 #pragma unroll
-  for (int n = 2; n <= NORD; n++) {
+    for (int n = 2; n <= NORD; n++) {
 #pragma unroll
-    for (int k = n - 1; k >= 0; k--) {
-      const int l_hi = (k == 0) ? n - k - 2 : n - k;
+      for (int k = n - 1; k >= 0; k--) {
+        const int l_hi = (k == 0) ? n - k - 2 : n - k;
 #pragma unroll
-      for (int l = l_hi; l >= 0; l--) {
-        const int m = (n - k - l) / 2;
-        if (2 * m == n - k - l) {
-          const T c = cc[ll];
-          ll++;
-          const int a = l + m, b = m;
-          const int t1 = een_off(NORD, k) + b - een_pmin(k);   // y^m   gets c x^(l+m)
-          const int t2 = een_off(NORD, k) + a - een_pmin(k);   // y^(l+m) gets c x^m
-          B[t1] += c * xp[a];
-          B[t2] += c * xp[b];
-          if (a >= 1) dB[t1] += c * T(a) * xp[a >= 1 ? a - 1 : 0];
-          if (b >= 1) dB[t2] += c * T(b) * xp[b >= 1 ? b - 1 : 0];
-          if (a >= 2) d2B[t1] += c * T(a * (a - 1)) * xp[a >= 2 ? a - 2 : 0];
-          if (b >= 2) d2B[t2] += c * T(b * (b - 1)) * xp[b >= 2 ? b - 2 : 0];
+        for (int l = l_hi; l >= 0; l--) {
+          const int m = (n - k - l) / 2;
+          if (2 * m == n - k - l) {
+            const int a = l + m, b = m;
+            const int t1 = een_off(NORD, k) + b - een_pmin(k);   // y^m   gets c x^(l+m)
+            const int t2 = een_off(NORD, k) + a - een_pmin(k);   // y^(l+m) gets c x^m
+            if (t1 == t || t2 == t) {
+              const T c = cc[ll];
+              if (t1 == t) {
+                B += c * xp[a];
+                if (a >= 1) dB += c * T(a) * xp[a >= 1 ? a - 1 : 0];
+                if (a >= 2) d2B += c * T(a * (a - 1)) * xp[a >= 2 ? a - 2 : 0];
+              }
+              if (t2 == t) {
+                B += c * xp[b];
+                if (b >= 1) dB += c * T(b) * xp[b >= 1 ? b - 1 : 0];
+                if (b >= 2) d2B += c * T(b * (b - 1)) * xp[b >= 2 ? b - 2 : 0];
+              }
+            }
+            ll++;
+          }
         }
       }
     }
-  }
-#pragma unroll
-  for (int t = 0; t < een_nb(NORD); t++) {
-    BD4[4 * t] = B[t];
-    BD4[4 * t + 1] = dB[t];
-    BD4[4 * t + 2] = d2B[t];
+    BD4[4 * t] = B;
+    BD4[4 * t + 1] = dB;
+    BD4[4 * t + 2] = d2B;
     BD4[4 * t + 3] = T(0);
   }
 }

@@ -20,11 +20,16 @@ def _engine(s, W):
     return eng, x, rng
 
 
-@pytest.mark.parametrize("config,W", [("tiny", 16), ("c0", 8)])
-def test_jastrow_derivatives(oracle_mod, config, W):
+@pytest.mark.parametrize("config,W,nspin2b", [("tiny", 16, 1), ("c0", 8, 1), ("tiny", 16, 2)])
+def test_jastrow_derivatives(oracle_mod, config, W, nspin2b):
     from champ_b200 import jastrow_opt as jo
     from champ_b200.system import make_synthetic
     s = make_synthetic(config)
+    if nspin2b == 2:                                  # like / unlike spin e-e functions
+        s.nspin2b = 2
+        b = np.array(s.b, float)
+        s.b = np.vstack([b[:1], b[:1] * 0.8 + 0.01])
+        s.b[1, 0] = 0.25
     eng, x, _ = _engine(s, W)
     jd = jo.default_jasderiv(s)
     P = jo.param_map(s, jd)

@@ -54,8 +54,21 @@ def _perturbed(s, part, idx, h):
     return t
 
 
-def test_raw_derivatives_finite_differences(oracle_mod):
+def _two_spin_classes(s):
+    """Separate e-e functions for like and unlike spins (nspin2b = 2)."""
+    s.nspin2b = 2
+    b = np.array(s.b, float)
+    s.b = np.vstack([b[:1], b[:1] * 0.8 + 0.01])
+    s.b[1, 0] = 0.25                 # like-spin cusp
+    s._keep = []
+    return s
+
+
+@pytest.mark.parametrize("nspin2b", [1, 2])
+def test_raw_derivatives_finite_differences(oracle_mod, nspin2b):
     s = make_synthetic("tiny")
+    if nspin2b == 2:
+        _two_spin_classes(s)
     o, x = _conf(oracle_mod, s)
     raw = o.jas_raw(x)
     lay = jo.raw_layout(s)
