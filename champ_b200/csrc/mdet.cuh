@@ -77,6 +77,110 @@ __device__ __forceinline__ const int *md_exc(const MdTab &t, int s, int kk) {
   return t.exc + ((size_t)s * t.numax + kk) * (1 + 2 * CW_MD_MEX);
 }
 
+// Gauss-Jordan with partial pivoting on the NR x NR excitation matrix
+// a[ir][jr] = aa[rc[ir]][ro[jr]] held in registers (row swaps by select, no
+// dynamic indexing); with INV the inverse is left in b (b[r][k] =
+// (M^-1)(r, k)).  Same operations in the same order as md_small_inv's
+// general path, so the same determinant bit for bit.
+template <int NR, bool INV>
+__device__ __forceinline__ double md_gj_nr(const double *aa, int ld, const int *rc, const int *ro, double (&b)[NR][NR]) {
+  double a[NR][NR];
+#pragma unroll
+  for (int ir = 0; ir < NR; ir++)
+#pragma unroll
+    for (int jr = 0; jr < NR; jr++) {
+      a[ir][jr] = aa[(size_t)rc[ir] * ld + ro[jr]];
+      if (INV) b[ir][jr] = (ir == jr) ? 1.0 : 0.0;
+    }
+  double det = 1.0;
+#pragma unroll
+  for (int c = 0; c < NR; c++) {
+    // first row of largest |a[r][c]| (the running maximum kept in a register:
+    // indexing a by p would move the matrix to local memory)
+    int p = c;
+    double amax = fabs(a[c][c]);
+#pragma unroll
+    for (int r = c + 1; r < NR; r++)
+      if (fabs(a[r][c]) > amax) {
+        amax = fabs(a[r][c]);
+        p = r;
+      }
+    if (p != c) {
+      det = -det;
+#pragma unroll
+      for (int k = 0; k < NR; k++) {
+        double ta = a[c][k], pa = 0, tb = INV ? b[c][k] : 0.0, pb = 0;
+#pragma unroll
+        for (int r = c + 1; r < NR; r++)
+          if (r == p) {
+            pa = a[r][k];
+            if (INV) pb = b[r][k];
+          }
+        a[c][k] = pa;
+        if (INV) b[c][k] = pb;
+#pragma unroll
+        for (int r = c + 1; r < NR; r++)
+          if (r == p) {
+            a[r][k] = ta;
+            if (INV) b[r][k] = tb;
+          }
+      }
+    }
+    const double piv = a[c][c];
+    det *= piv;
+    const double pinv = 1.0 / piv;
+#pragma unroll
+    for (int k = 0; k < NR; k++) {
+      a[c][k] *= pinv;
+      if (INV) b[c][k] *= pinv;
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      if (r == c) continue;
+      const double f = a[r][c];
+      if (f == 0.0) continue;
+#pragma unroll
+      for (int k = 0; k < NR; k++) {
+        a[r][k] -= f * a[c][k];
+        if (INV) b[r][k] -= f * b[c][k];
+      }
+    }
+  }
+  return det;
+}
+
+// determinant of the excitation matrix of e (register-resident for every
+// excitation order)
+__device__ __forceinline__ double md_small_det(const double *aa, int ld, const int *e) {
+  const int nr = e[0];
+  const int *rc = e + 1, *ro = e + 1 + CW_MD_MEX;
+  if (nr == 1) return aa[(size_t)rc[0] * ld + ro[0]];
+  if (nr == 2) {
+    const double w0 = aa[(size_t)rc[0] * ld + ro[0]], w1 = aa[(size_t)rc[1] * ld + ro[0]];
+    const double w2 = aa[(size_t)rc[0] * ld + ro[1]], w3 = aa[(size_t)rc[1] * ld + ro[1]];
+    return w0 * w3 - w2 * w1;
+  }
+  if (nr == 3) {
+    double b[3][3];
+    return md_gj_nr<3, false>(aa, ld, rc, ro, b);
+  }
+  double b[4][4];
+  return md_gj_nr<4, false>(aa, ld, rc, ro, b);
+}
+
+// ceq * M^-1 of excitation e added into Y[rc][ro] (atomics), M^-1 in
+// registers
+template <int NR>
+__device__ __forceinline__ void md_y_add_nr(const double *aa, int ld, const int *e, double ceq, double *Y) {
+  const int *rc = e + 1, *ro = e + 1 + CW_MD_MEX;
+  double b[NR][NR];
+  md_gj_nr<NR, true>(aa, ld, rc, ro, b);
+#pragma unroll
+  for (int ir = 0; ir < NR; ir++)
+#pragma unroll
+    for (int jr = 0; jr < NR; jr++) atomicAdd(&Y[rc[ir] * ld + ro[jr]], ceq * b[jr][ir]);
+}
+
 // determinant and inverse of the excitation matrix M[ir][jr] =
 // aa[rc[ir]][ro[jr]] (aa row stride ld); inverse stored column-major as
 // CHAMP's wfmat: inv[jr + nr*ir] = (M^-1)(jr, ir)
@@ -155,10 +259,16 @@ __device__ __forceinline__ double md_solve_nr(const double *aa, int ld, const in
   double det = 1.0;
 #pragma unroll
   for (int c = 0; c < NR; c++) {
+    // first row of largest |a[r][c]| (the running maximum kept in a register:
+    // indexing a by p would move the matrix to local memory)
     int p = c;
+    double amax = fabs(a[c][c]);
 #pragma unroll
     for (int r = c + 1; r < NR; r++)
-      if (fabs(a[r][c]) > fabs(a[p][c])) p = r;
+      if (fabs(a[r][c]) > amax) {
+        amax = fabs(a[r][c]);
+        p = r;
+      }
     if (p != c) {
       det = -det;
 #pragma unroll
@@ -285,12 +395,21 @@ __device__ void md_form_Y(const MdTab &tab, int s, const double *aa, const doubl
   __syncthreads();
   for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
     const int *e = md_exc(tab, s, kk);
-    double inv[CW_MD_MEX * CW_MD_MEX];
-    md_small_inv(aa, O, e, inv);
     const double ceq = dd[kk] * G[kk];
-    const int nr = e[0];
-    for (int ir = 0; ir < nr; ir++)
-      for (int jr = 0; jr < nr; jr++) atomicAdd(&Y[e[1 + ir] * O + e[1 + CW_MD_MEX + jr]], ceq * inv[jr + nr * ir]);
+    switch (e[0]) {
+      case 1: md_y_add_nr<1>(aa, O, e, ceq, Y); break;
+      case 2: {
+        double inv[4];
+        md_small_inv(aa, O, e, inv);
+#pragma unroll
+        for (int ir = 0; ir < 2; ir++)
+#pragma unroll
+          for (int jr = 0; jr < 2; jr++) atomicAdd(&Y[e[1 + ir] * O + e[1 + CW_MD_MEX + jr]], ceq * inv[jr + 2 * ir]);
+        break;
+      }
+      case 3: md_y_add_nr<3>(aa, O, e, ceq, Y); break;
+      default: md_y_add_nr<4>(aa, O, e, ceq, Y); break;
+    }
   }
   __syncthreads();
 }
@@ -363,10 +482,7 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
     }
     __syncthreads();
     double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
-    for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) {
-      double inv[CW_MD_MEX * CW_MD_MEX];
-      dd[kk] = md_small_inv(aa, O, md_exc(tab, s, kk), inv);
-    }
+    for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) dd[kk] = md_small_det(aa, O, md_exc(tab, s, kk));
   }
   __syncthreads();
   // 2. S of every state (state 0 drives the walk)
