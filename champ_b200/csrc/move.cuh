@@ -105,7 +105,7 @@ __device__ __forceinline__ double group_sum(double v) {
 // loop, and every lane of the group ends with them.  Every lane of the warp
 // must call it (the rounds continue until every group of the warp is done).
 // Returns true for a group that gave up (more than ~10^6 candidates).
-__device__ __noinline__ bool radial_sample_group(DRng &rng, double rmin, double deltar, double deltri, double co,
+__device__ __forceinline__ bool radial_sample_group(DRng &rng, double rmin, double deltar, double deltri, double co,
                                                  double zeta, double fmx, double &rtry, double &top) {
   const int lane = threadIdx.x & 31, g = lane & (kMoveGroup - 1), base = lane - g;
   bool done = false, gave_up = false;
