@@ -85,9 +85,10 @@ constexpr int kEnFields = 5;
 
 // T is the arithmetic of the pair and e-e-n terms (double: parity path,
 // float: mixed path); distances, 1/r_ij, the tables and the sums over
-// pairs stay FP64.
+// pairs stay FP64.  Four CTAs per SM in both arithmetics (the FP32 build at
+// five spilled and ran 9% slower).
 template <int NORD, typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) k_jastrow_full(WState st, HBuf hb) {
+__global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M, MN = M * N;
