@@ -1889,6 +1889,11 @@ double *g_noalloc_scratch[kNoallocMaxDevices] = {nullptr};
 
 // The array's name is only a host-side stand-in for the device symbol: its
 // device address is looked up once per device, with that device current.
+// The per-device cache below is written without a lock.  Two host threads
+// whose first calls on one device race here both store the same address,
+// so the race is benign.  The cache assumes the CUDA context of the device
+// lives as long as the process: after a cudaDeviceReset the cached address
+// is stale.
 int noalloc_scratch(cw_ctx *c, double **p) {
   const int dev = c->device;
   if (dev < 0 || dev >= kNoallocMaxDevices) return fail(c, CW_ERR_ARG, "device index out of range");

@@ -12,13 +12,20 @@ newly arrived jobs between blocks.  A job finishes when its error bar reaches
 the target (after at least two blocks) or its block budget is spent; its
 context is then released and the jobs waiting for memory are admitted.
 
+A job is charged the larger of its estimate and the bytes its context
+really holds (``cw_device_bytes``, read after creation): the estimate is an
+upper bound for single-determinant systems only, so a multideterminant job
+whose context turns out larger than what is left is released again and waits,
+first in line, for that much memory.  A job whose context creation or block
+fails (out of device memory, a singular walker) is marked failed and the
+loop serves the others.
+
 Time-to-result of a job = completion time - arrival time.  Each job draws
 its walkers' streams from its own range (``seed_offset``), so a job's
 result does not depend on which other jobs share the device.
 
-The contexts of different molecules share the device's constant system
-block, so their kernels run one context at a time (the engine serialises
-them on the device); jobs overlap at block granularity, not inside a kernel.
+Work of different jobs is interleaved block by block on the host thread;
+their kernels do not run at the same time on the device.
 CHAMP itself has no request loop (one job per MPI run); this module is the
 serving layer the engine's C ABI is designed for.
 """
@@ -142,9 +149,29 @@ class Server:
                 if used + j.est_bytes > self.budget:
                     break
                 waiting.popleft()
-                eng = self.factory(j)
+                try:
+                    eng = self.factory(j)
+                except Exception as exc:           # e.g. out of device memory: this job fails, the loop goes on
+                    j.failed = f"context creation failed: {exc}"
+                    j.done = now()
+                    self.timeline.append((j.done, "fail", j.jid))
+                    continue
                 j.device_bytes = int(eng.device_bytes())
-                used += j.est_bytes
+                # the estimate bounds single-determinant contexts only: charge
+                # what the context really holds when that is more
+                charge = max(j.est_bytes, j.device_bytes)
+                if used + charge > self.budget:
+                    eng.close()
+                    j.est_bytes = charge
+                    if charge > self.budget:
+                        j.failed = f"holds {charge} bytes, budget {self.budget}"
+                        j.done = now()
+                        self.timeline.append((j.done, "refuse", j.jid))
+                        continue
+                    waiting.appendleft(j)          # waits, first in line, for the memory it really needs
+                    break
+                j.est_bytes = charge
+                used += charge
                 self.peak_bytes = max(self.peak_bytes, used)
                 j.admitted = now()
                 self.timeline.append((j.admitted, "admit", j.jid))
@@ -157,9 +184,17 @@ class Server:
                     self.sleep(max(0.0, pending[0].arrival - now()))
                 continue
             j, eng = active.popleft()
-            eng.vmc_steps(j.nstep)
-            eng.end_block()
-            r = eng.results()
+            try:
+                eng.vmc_steps(j.nstep)
+                eng.end_block()
+                r = eng.results()
+            except Exception as exc:               # a failed block ends this job only
+                j.failed = f"block failed: {exc}"
+                j.done = now()
+                self.timeline.append((j.done, "fail", j.jid))
+                eng.close()
+                used -= j.est_bytes
+                continue
             j.blocks += 1
             j.moves += j.nstep * j.nwalk * j.system.nelec
             j.energy, j.err = float(r["energy"]), float(r["err"])

@@ -281,8 +281,13 @@ int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
  * (CW_ERR_ARG otherwise).  The first call on a device looks up that array's
  * device address (make that first call before any stream capture).  The work
  * is queued on the context's stream: out is ready after cw_sync.  All calls
- * share the one array: calls that overlap on the GPU (several contexts on
- * the same device, different streams) race on it. */
+ * share the one array.  Before a context launches on a device it waits for
+ * the work of the context that used the device before it, so calls made one
+ * after another (from one host thread, or from threads that take turns) do
+ * not overlap on the GPU.  Calls made at the same moment from several host
+ * threads, on contexts of the same device, can overlap and then race on the
+ * array.  The first-call address lookup is not locked; threads racing there
+ * store the same address, which is harmless. */
 int cw_orbitals_noalloc(cw_ctx *ctx, int npts, const double *xyz, double *out);
 
 /* ------------------------------------------------------------------------ */

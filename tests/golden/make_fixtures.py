@@ -1,7 +1,7 @@
 """Regenerates the committed golden fixtures of tests/golden/.
 
-Run in a container where the CHAMP sources are mounted (default
-/root/reference, override with CHAMP_REF).  Writes:
+Run where the CHAMP sources are available, with CHAMP_REF set to the root
+of that source tree (the script refuses to run without it).  Writes:
 
 * rng_default_seed.npz — next_uniform_double draws and jump() states of the
   reference's own vmc/xoroshiro256starstar.c (compiled into oracle/_ref by
@@ -19,11 +19,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path.insert(0, ROOT)
-REF = os.environ.get("CHAMP_REF", "/root/reference")
+REF = os.environ.get("CHAMP_REF", "")
 
 
 def rng_fixture():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
     lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libxoshiro_ref.so"))
     lib.next_uniform_double.restype = C.c_double
     seed = "18123437465549275475255231234865"
@@ -50,6 +50,8 @@ def h2_fixture():
 
 
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(os.path.join(REF, "src")):
+        sys.exit("set CHAMP_REF to the root of a CHAMP source tree")
     rng_fixture()
     h2_fixture()
     print("fixtures written to", HERE)

@@ -115,3 +115,47 @@ def test_chain_generator_sizes():
         assert s.nelec == n and s.nup + s.ndn == n
         assert abs(s.nbasis / n - 4.5) < 0.6
         assert s.norb == s.nup
+
+
+def test_failed_creation_does_not_stop_the_loop():
+    clock, log = Clock(), []
+    jobs = _jobs([(8, 64, 0.0, 0.006, 20), (8, 64, 0.0, 0.006, 20), (8, 64, 0.0, 0.006, 20)])
+
+    def factory(j):
+        if j.jid == 1:
+            raise RuntimeError("cw_create failed (status 3): out of device memory")
+        return FakeEngine(j, clock, log)
+
+    srv = serve.Server(1 << 40, engine_factory=factory, clock=clock, sleep=clock.sleep)
+    out = srv.run(jobs)
+    assert "out of device memory" in out[1].failed and out[1].blocks == 0
+    assert out[0].reached and out[2].reached
+    assert ("fail" in [ev for _, ev, j in srv.timeline if j == 1])
+
+
+class BigEngine(FakeEngine):
+    """A context that holds more than its job's estimate (multideterminant)."""
+
+    def device_bytes(self):
+        return 3 * serve.estimate_bytes(self.job.system, self.job.nwalk)
+
+
+def test_charge_is_what_the_context_holds():
+    clock, log = Clock(), []
+    jobs = _jobs([(16, 256, 0.0, 0.004, 50), (16, 256, 0.0, 0.004, 50)])
+    one = serve.estimate_bytes(jobs[0].system, 256)
+    # the budget holds both estimates, but only one context of three times the estimate
+    srv = serve.Server(4 * one, engine_factory=lambda j: BigEngine(j, clock, log), clock=clock, sleep=clock.sleep)
+    srv.run(jobs)
+    assert srv.peak_bytes <= srv.budget
+    admits = [t for t, ev, j in srv.timeline if ev == "admit"]
+    first_done = min(t for t, ev, j in srv.timeline if ev == "done")
+    assert len(admits) == 2 and admits[1] >= first_done   # the second waited for the real charge
+    assert all(j.reached for j in jobs)
+    # a context larger than the whole budget is refused after creation
+    clock2, log2 = Clock(), []
+    jb = _jobs([(16, 256, 0.0, 0.004, 50)])
+    srv2 = serve.Server(2 * one, engine_factory=lambda j: BigEngine(j, clock2, log2), clock=clock2,
+                        sleep=clock2.sleep)
+    out = srv2.run(jb)
+    assert out[0].failed and out[0].blocks == 0
