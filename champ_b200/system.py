@@ -469,7 +469,7 @@ def _type_from_shells(shells, znuc, nloc):
     for irb, (l, _, _) in enumerate(shells):
         for slm in SLM_OF_L[l]:
             aos.append((slm, irb + 1))
-    return dict(prep=prep, aos=aos, igrid=GRID_TYPE)
+    return dict(prep=prep, aos=aos, igrid=GRID_TYPE, shells=shells)
 
 
 def _bfd_like_ecp(rng, zval, lpot):
@@ -517,13 +517,35 @@ def _orthonormal(rng, k, o):
     return np.ascontiguousarray(q.T)  # [norb, nbasis]
 
 
+# Exponent (bohr^-2) of the Gaussian model density that screens a nucleus in
+# the model Hamiltonian of the trial orbitals (trial.py), unless a type sets
+# its own ("screen"): a valence cloud of mean radius about 1.3 bohr.
+SCREEN_ALPHA = 0.75
+
+
+def model_hamiltonian_orbitals(cent, types_of_centre, type_defs, norb, ecp=None):
+    """Lowest `norb` orbitals of the seeded molecule's model one-electron
+    Hamiltonian (champ_b200.trial): kinetic energy, screened nuclear
+    attraction and pseudopotential, in the molecule's Gaussian basis."""
+    from . import trial
+    shells = [td["basis"]["shells"] for td in type_defs]
+    aos = [td["basis"]["aos"] for td in type_defs]
+    prim, basis = trial.primitives(np.asarray(cent, float), types_of_centre, shells, aos, gnorm)
+    S, T = trial.overlap_kinetic(prim, len(basis["ao_cent"]))
+    znuc = np.array([td["z"] for td in type_defs], float)
+    V = trial.potential_matrix(basis, np.asarray(cent, float), types_of_centre, znuc, ecp,
+                               [td.get("screen", SCREEN_ALPHA) for td in type_defs])
+    coef, _ = trial.model_orbitals(S, T + V, norb)
+    return coef
+
+
 def _assemble(name, rng, cent, types_of_centre, type_defs, nelec, nup, norb, nocc_up, nocc_dn,
-              nloc=4, nquad=6):
+              nloc=4, nquad=6, orbitals="random"):
     nct = len(type_defs)
     basis = assemble_basis([td["basis"] for td in type_defs])
     nbasis = int(sum(len(type_defs[t]["basis"]["aos"]) for t in types_of_centre))
     znuc = np.array([td["z"] for td in type_defs], float)
-    coef = _orthonormal(rng, nbasis, norb)
+    coef = _orthonormal(rng, nbasis, norb)   # drawn in every case: the seeded stream stays the same
     iworbd = np.array([list(range(1, nocc_up + 1)) + list(range(1, nocc_dn + 1))], np.int32)
     a4, b, c = _jastrow(rng, nct, np.array([td["a1"] for td in type_defs]))
     sysd = dict(name=name, nelec=nelec, nup=nup, iwctype=np.array(types_of_centre, np.int32),
@@ -541,22 +563,49 @@ def _assemble(name, rng, cent, types_of_centre, type_defs, nelec, nup, norb, noc
         xq, yq, zq, wq = gesqua(nquad)
         sysd.update(nloc=nloc, lpot=lpot, necp_term=nterm, necp_power=power, ecp_exponent=expo,
                     ecp_coef=ecoef, nquad=nquad, xq0=xq, yq0=yq, zq0=zq, wq=wq)
+    if orbitals == "model":
+        ecp = None
+        if nloc:
+            ecp = [(lpot[it], nterm[it], power[it], expo[it], ecoef[it]) for it in range(nct)]
+        sysd["coef"] = model_hamiltonian_orbitals(cent, types_of_centre, type_defs, norb, ecp)
     return System(**sysd)
 
 
-def make_synthetic(config: str, seed: int = 20261203) -> System:
-    """Seeded synthetic molecule of one benchmark configuration.
+_MADE = {}
+
+
+def _memo(key, make):
+    """Generated molecules are deterministic: build each once per process and
+    hand out copies (callers may modify theirs)."""
+    import copy
+    if key not in _MADE:
+        _MADE[key] = make()
+    return copy.deepcopy(_MADE[key])
+
+
+def make_synthetic(config: str, seed: int = 20261203, orbitals: str = "model") -> System:
+    """Seeded synthetic molecule of one benchmark configuration (built once
+    per process, a copy returned).
 
     c0: 3 nuclei in a 4 bohr box (Z 6/1/1, ECP on the heavy atom, l_max=1,
         6-point quadrature), 8 electrons (4/4), 60 Gaussians (s/p/d,
         exponents log-uniform 0.1-20), 4 orbitals, order-5 Jastrow.
-    c1: 30 nuclei on a zig-zag chain alternating C-like (Z=4, ECP) and H-like
-        (Z=1) centres, 120 electrons (60/60), 540 Gaussians, 60 orbitals.
+    c1: 30 nuclei on a zig-zag chain alternating Cl-like (Z=7, ECP) and
+        H-like (Z=1) centres, neutral: 120 electrons (60/60), 540 Gaussians,
+        60 orbitals.
     tiny: 2 nuclei, 6 electrons, small basis (fast parity cases).
     c2: 12 nuclei, 40 electrons, 300 Gaussians, 80 orbitals, 10^4
         determinants (multideterminant DMC).
     he: He atom through the ECP path (DMC reaches the exact energy).
+
+    c1, c2: orbitals of the molecule's model one-electron Hamiltonian
+    (orbitals="model", trial.py); orbitals="random" gives a seeded random
+    orthonormal coefficient matrix instead (c0 and tiny always use that).
     """
+    return _memo(("synthetic", config, seed, orbitals), lambda: _make_synthetic(config, seed, orbitals))
+
+
+def _make_synthetic(config, seed, orbitals):
     rng = np.random.default_rng(seed)
     if config == "c0":
         while True:
@@ -570,17 +619,7 @@ def make_synthetic(config: str, seed: int = 20261203) -> System:
                    basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4)]), 1.0, 4))
         return _assemble("c0", rng, cent, [0, 1, 1], [heavy, hyd], 8, 4, 4, 4, 4)
     if config == "c1":
-        nat = 30
-        cent = np.zeros((nat, 3))
-        for i in range(nat):
-            cent[i] = (1.30 * i + rng.normal(0, 0.05), 0.75 * (i % 2) + rng.normal(0, 0.05),
-                       rng.normal(0, 0.05))
-        heavy = dict(z=4.0, lpot=2, a1=0.0,
-                     basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 1)]), 4.0, 4))
-        hyd = dict(z=1.0, lpot=1, a1=-1.0,
-                   basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 4)]), 1.0, 4))
-        types = [0 if i % 2 == 0 else 1 for i in range(nat)]
-        return _assemble("c1", rng, cent, types, [heavy, hyd], 120, 60, 60, 60, 60)
+        return _chain_molecule(rng, "c1", 30, 120, orbitals)
     if config == "tiny":
         cent = np.array([[0.0, 0.0, -0.7], [0.3, 0.2, 0.8]])
         heavy = dict(z=4.0, lpot=2, a1=0.0,
@@ -591,29 +630,37 @@ def make_synthetic(config: str, seed: int = 20261203) -> System:
     if config == "he":
         return _helium()
     if config == "c2":
-        return _c2(rng)
+        return _c2(rng, orbitals)
     raise ValueError(f"unknown synthetic config {config!r}")
 
 
-def make_chain(nelec: int, seed: int) -> System:
-    """Seeded chain molecule of the batched / serving job distribution: about
-    nelec/4 centres alternating C-like (Z=4, ECP, s/p/d basis) and H-like
-    (Z=1, s/p) as in c1, nelec electrons (ceil/floor halves), one occupied
-    orbital per up electron, basis about 4.5 x nelec Gaussians."""
-    if nelec < 2:
-        raise ValueError("a chain job needs at least 2 electrons")
-    rng = np.random.default_rng(seed)
-    nat = max(2, int(round(nelec / 4)))
+def _chain_molecule(rng, name, nat, nelec, orbitals):
+    """Zig-zag chain of nat centres alternating Cl-like heavy atoms (valence
+    charge 7, BFD-form pseudopotential with a local and an s channel, s4 p4
+    d1 basis = 22 Cartesian AOs) and H-like atoms (charge 1, s2 p4 = 14
+    AOs), 2.0 bohr apart along x and 1.2 bohr across, nelec electrons
+    (ceil/floor halves), one occupied orbital per up electron.  With nelec =
+    4 nat the molecule is neutral (a chain of HCl-like units)."""
     cent = np.zeros((nat, 3))
     for i in range(nat):
-        cent[i] = (1.30 * i + rng.normal(0, 0.05), 0.75 * (i % 2) + rng.normal(0, 0.05), rng.normal(0, 0.05))
-    heavy = dict(z=4.0, lpot=2, a1=0.0,
-                 basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 1)]), 4.0, 4))
-    hyd = dict(z=1.0, lpot=1, a1=-1.0,
+        cent[i] = (2.0 * i + rng.normal(0, 0.05), 1.2 * (i % 2) + rng.normal(0, 0.05), rng.normal(0, 0.05))
+    heavy = dict(z=7.0, lpot=2, a1=0.0, screen=0.15,
+                 basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 1)]), 7.0, 4))
+    hyd = dict(z=1.0, lpot=1, a1=-1.0, screen=0.15,
                basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 4)]), 1.0, 4))
     types = [0 if i % 2 == 0 else 1 for i in range(nat)]
     nup, ndn = (nelec + 1) // 2, nelec // 2
-    return _assemble(f"chain{nelec}", rng, cent, types, [heavy, hyd], nelec, nup, nup, nup, ndn)
+    return _assemble(name, rng, cent, types, [heavy, hyd], nelec, nup, nup, nup, ndn, orbitals=orbitals)
+
+
+def make_chain(nelec: int, seed: int, orbitals: str = "model") -> System:
+    """Seeded chain molecule of the batched / serving job distribution:
+    about nelec/4 centres of the c1 chain's two atom types (so about
+    neutral), nelec electrons, basis about 4.5 x nelec Gaussians."""
+    if nelec < 2:
+        raise ValueError("a chain job needs at least 2 electrons")
+    return _memo(("chain", nelec, seed, orbitals), lambda: _chain_molecule(
+        np.random.default_rng(seed), f"chain{nelec}", max(2, int(round(nelec / 4))), nelec, orbitals))
 
 
 def ci_expansion(rng, nup, ndn, norb, ndet, pools=(150, 500, 300, 120), nact_occ=8, nact_virt=30,
@@ -667,7 +714,7 @@ def ci_expansion(rng, nup, ndn, norb, ndet, pools=(150, 500, 300, 120), nact_occ
     return iworbd, cdet
 
 
-def _c2(rng) -> System:
+def _c2(rng, orbitals="model") -> System:
     """Config 2: 12 centres (9 C-like Z=4 with BFD-form ECP, 3 H-like), 40
     electrons (20/20; the valence charges add up to 39, so one extra
     electron), 300 Gaussians (C-like s4p5d1, H-like s4p7), 80 orbitals,
@@ -682,7 +729,7 @@ def _c2(rng) -> System:
                  basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 5), (2, 1)]), 4.0, 4))
     hyd = dict(z=1.0, lpot=1, a1=-1.0,
                basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 7)]), 1.0, 4))
-    s = _assemble("c2", rng, cent, types, [heavy, hyd], 40, 20, 80, 20, 20)
+    s = _assemble("c2", rng, cent, types, [heavy, hyd], 40, 20, 80, 20, 20, orbitals=orbitals)
     s.iworbd, s.cdet = ci_expansion(rng, 20, 20, 80, 10000)
     return s
 

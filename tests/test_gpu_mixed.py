@@ -137,3 +137,53 @@ def test_mixed_dmc_steps(oracle_mod, config, W, tau):
         assert rel_err(xg, xo) < 1e-5
         assert rel_err(wg, wo) < 1e-4
         assert np.max(np.abs(eg - eo)) <= TOL_E * max(1.0, np.max(np.abs(eo)))
+
+
+@pytest.mark.parametrize("config", ["chain37", "c2sd"])
+def test_mixed_energy_bias(oracle_mod, config):
+    """Systematic error of the mixed path's energy, on identical streams.
+
+    The FP64 and the mixed engine start from the same configurations and
+    streams; every walker whose decisions all agree (same final stream and
+    acceptance count) sampled the same configurations, so the difference of
+    its local-energy sums is the mixed path's error on those samples alone,
+    without statistical noise.  The mean of that difference over the
+    matched samples is the bias of the mixed estimator of the energy: it
+    must stay within the 0.1 mHa target (each sample's own error is bounded
+    by the 5e-5 * max(1, |E|) local-energy bound; the bias of the mean is far
+    smaller because the FP32 rounding errors of different samples have no
+    common sign).  Model trial orbitals of a 37-electron chain and of the
+    40-electron DMC molecule's reference determinant."""
+    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.system import make_chain, make_synthetic
+    if config == "chain37":
+        s = make_chain(37, 4037)
+    else:
+        s = make_synthetic("c2")
+        s.iworbd, s.cdet = s.iworbd[:1].copy(), s.cdet[:1].copy()
+    W, nstep = 512, 6
+    rng = rng_states(W)
+    x = initial_configs(s, rng)
+    pre = Engine(s)
+    pre.set_walkers(x, rng)
+    pre.vmc_steps(10)                     # equilibrated start, shared by both
+    x, rng = pre.walkers()
+    pre.close()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        e = Engine(s, precision=prec)
+        e.set_walkers(x, rng)
+        e.vmc_steps(nstep)
+        out[prec] = (e.walkers()[1], e.sums())
+        e.close()
+    (r64, s64), (rmx, smx) = out["fp64"], out["mixed"]
+    same = np.all(r64 == rmx, axis=1) & (s64[:, 4] == smx[:, 4])
+    assert same.sum() >= 0.99 * W, f"only {same.sum()} of {W} walkers took identical decisions"
+    wsum = s64[same, 0].sum()
+    bias = (smx[same, 1].sum() - s64[same, 1].sum()) / wsum
+    per_sample = np.max(np.abs(smx[same, 1] - s64[same, 1]) / s64[same, 0])
+    mean_e = s64[same, 1].sum() / wsum
+    print(f"{config}: mean E {mean_e:.5f} Ha, mixed - fp64 bias {bias * 1e3:.2e} mHa (target 0.1 mHa) over "
+          f"{int(wsum)} samples of {int(same.sum())} matched walkers; largest per-walker mean difference "
+          f"{per_sample * 1e3:.2e} mHa")
+    assert abs(bias) <= 1e-4
