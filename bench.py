@@ -29,15 +29,17 @@ sys.path.insert(0, ROOT)
 
 CONFIGS = {
     # name: (synthetic config, walkers, description)
-    "c1": ("c1", 8192, "vmc-c1: 30 centres (15 C-like Z=4 with BFD-form ECP, 15 H-like), 120 electrons "
-                       "(60/60), 540 Gaussians, 60 orbitals, order-5 Jastrow, 8192 walkers"),
+    "c1": ("c1", 8192, "vmc-c1: 30 centres on a zig-zag chain (15 Cl-like Z=7 with BFD-form ECP, 15 H-like; "
+                       "neutral), 120 electrons (60/60), 540 Gaussians, 60 orbitals (model-Hamiltonian trial "
+                       "orbitals), order-5 Jastrow, 8192 walkers"),
     "c0": ("c0", 1024, "vmc-c0: 3 centres (Z 6/1/1, ECP on the heavy atom), 8 electrons (4/4), 60 Gaussians, "
                        "4 orbitals, order-5 Jastrow, 1024 walkers"),
     "c2": ("c2", 16384, "dmc-c2: 12 centres (9 C-like Z=4 with BFD-form ECP, 3 H-like), 40 electrons (20/20), "
-                        "300 Gaussians, 80 orbitals, 10^4 determinants (1-4-fold excitations, |c_k|~k^-1.5), "
+                        "300 Gaussians, 80 orbitals (model-Hamiltonian trial orbitals), 10^4 determinants "
+                        "(1-4-fold excitations, |c_k|~k^-1.5), "
                         "order-5 Jastrow, 16384 walkers, tau=0.01, branching on"),
     "c4": ("chain", 0, "serve-c4: seeded Poisson arrivals of VMC energy jobs, each a chain molecule of the "
-                       "batched distribution (8-200 electrons, ~4.5 x electrons Gaussians, C-like Z=4 with ECP "
+                       "batched distribution (8-200 electrons, ~4.5 x electrons Gaussians, Cl-like Z=7 with ECP "
                        "and H-like centres), 256-1024 walkers, target error 0.5 mHa within a block budget, "
                        "admitted against an HBM budget on one GPU"),
 }
@@ -52,6 +54,33 @@ def jm_traffic(W):
     with open(p) as f:
         d = json.load(f)
     return (d["dram_bytes_read"] + d["dram_bytes_write"]) * W / d["walkers"]
+
+
+def update_bytes(system, W, acc):
+    """Bytes one k_decide + k_commit pair moves at W walkers and acceptance
+    `acc` in the engine's lazy update: k_decide reads the inverse column (n),
+    the new orbital rows (4 O) and the move scratch (~12 doubles) and writes
+    the state of an accepted walker (~N: position, nearest-centre rows);
+    k_commit, for the accepted walkers only, reads and writes the spin's
+    inverse (2 n^2), the column and orbital row (2 n), the orbital and
+    gradient rows of the electron (8 n), the e-n row (2 M) and the pair
+    table rows (fso, fijo, fjo: 14 N)."""
+    N, M, O = system.nelec, system.ncent, system.norb
+    n = max(system.nup, system.ndn)
+    decide = 8 * (n + 4 * O + 12 + N)
+    commit = 8 * (2 * n * n + 2 * n + 8 * n + 2 * M + 14 * N)
+    return W * (decide + acc * commit)
+
+
+def update_traffic(W):
+    """DRAM bytes of one k_decide + k_commit pair at W walkers, from the
+    committed ncu capture (per-walker traffic scaled by the walker count)."""
+    p = os.path.join(ROOT, "profiles", "k_decide_commit_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d["dram_bytes_per_pair"] * W / d["walkers"]
 
 
 def load_peaks():
@@ -228,7 +257,7 @@ def run_dmc(args):
     import torch
     rank, world, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    from champ_b200.engine import Dmc, Engine, initial_configs, rng_states
+    from champ_b200.engine import Dmc, Engine, rng_states, start_population
     from champ_b200.system import make_synthetic
     cfg, W, desc = CONFIGS[args.config]
     if args.walkers:
@@ -237,10 +266,9 @@ def run_dmc(args):
     mw = 3 * W + 1   # capacity for the branching of a crude (random-orbital) trial function
     rng_all = rng_states((mw + 1) * (rank + 1))
     rng = rng_all[rank * (mw + 1):].copy()
-    x = initial_configs(system, rng[:W].copy())
     eng = Engine(system, device=local, precision=args.precision)
-    eng.set_walkers(x, rng[:W].copy())
-    eng.vmc_steps(2)
+    start_population(eng, system, rng[:W].copy())
+    eng.vmc_steps(args.equil)
     xv, _ = eng.walkers()
     e0 = float(np.median(eng.state()[0]))   # robust against the heavy tails of E_L near nodes
     dmc = Dmc(eng, xv, rng[:mw], rng[mw], tau=0.01, etrial=e0, mwalk=mw)
@@ -346,11 +374,34 @@ def run_serve(args):
     return 0
 
 
+def efficiency_run(system, x, rng, precision, device, nblk=10, nstep=5):
+    """nblk blocks of nstep sweeps from the given walkers and streams: the
+    block estimate of CHAMP's finwrt (walkers in the role of ranks), the
+    device time of the sweeps, and the per-walker sums of the first block."""
+    from champ_b200.engine import Engine
+    e = Engine(system, device=device, precision=precision)
+    e.set_walkers(x, rng)
+    ms = 0.0
+    first = None
+    for b in range(nblk):
+        e.vmc_steps(nstep)
+        ms += e.last_ms()
+        if b == 0:
+            first = (e.walkers()[1], e.sums())
+        e.end_block()
+    r = e.results()
+    e.close()
+    r = {k: float(v) for k, v in r.items()}
+    r["t_s"] = ms * 1e-3
+    r["efficiency"] = 1.0 / (r["err"] ** 2 * r["t_s"]) if r["err"] > 0 else None
+    return r, first
+
+
 def run_ours(args):
     import torch
     rank, world, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.engine import Engine, start_population, rng_states
     from champ_b200.system import make_synthetic
     cfg, W, desc = CONFIGS[args.config]
     if args.walkers:
@@ -359,9 +410,12 @@ def run_ours(args):
     # replica r runs its own walkers: streams r*W .. r*W+W-1 of the default seed
     from champ_b200.replicas import rank_streams
     rng = rank_streams(rank, W, rng_states)
-    x = initial_configs(system, rng)
     eng = Engine(system, device=local, precision=args.precision)
-    eng.set_walkers(x, rng)
+    start_population(eng, system, rng)
+    # equilibration from the sites start (discarded), then the timed steps
+    eng.vmc_steps(args.equil)
+    x_eq, rng_eq = eng.walkers()
+    eng.set_walkers(x_eq, rng_eq)
     for _ in range(args.warmup):
         eng.vmc_steps(1)
     # --- timed region: K steps, walkers resident in HBM -------------------
@@ -374,12 +428,6 @@ def run_ours(args):
     ms_max = max_over_ranks(ms_dev, pg, local)
     moves = W * system.nelec * args.steps * world
     value = moves / (ms_max * 1e-3)
-    # efficiency 1/(err^2 t): the timed steps form one block whose walker
-    # means give the error of the mean energy (finwrt's err with walkers as
-    # ranks); t is the device time of the timed steps
-    eng.end_block()
-    res = eng.results()
-    eff = 1.0 / (res["err"] ** 2 * ms_dev * 1e-3) if res["err"] > 0 else None
     # --- per-stage timing pass (CUDA events around every launch) ----------
     eng.profile(True)
     eng.vmc_steps(1)
@@ -404,6 +452,18 @@ def run_ours(args):
     barrier(pg, local)
     e2e_s = max_over_ranks(time.perf_counter() - t0, pg, local)
     e2e = W * system.nelec * e2e_steps * world / e2e_s
+    eng.close()
+    # --- efficiency 1/(err^2 t): FP64 and mixed from the same equilibrated
+    # walkers and streams, 10 blocks each (outside the timed region) --------
+    eff = {}
+    first = {}
+    for prec in ("fp64", "mixed"):
+        eff[prec], first[prec] = efficiency_run(system, x_eq, rng_eq, prec, local, nblk=args.blocks,
+                                                nstep=args.block_steps)
+    (r64, s64), (rmx, smx) = first["fp64"], first["mixed"]
+    same = np.all(r64 == rmx, axis=1) & (s64[:, 4] == smx[:, 4])
+    wsum = float(s64[same, 0].sum())
+    bias = (float(smx[same, 1].sum()) - float(s64[same, 1].sum())) / wsum if wsum > 0 else None
     if rank != 0:
         pg.close()
         return 0
@@ -436,19 +496,26 @@ def run_ours(args):
             "share_of_step": ms_jm / total_stage,
             "work_per_launch": "8*(N-1)*M*T + 8*(N-1)*nordb + 8*M*norda FLOP per walker (T=23 e-e-n terms)"}
     # HBM-bound move update: k_decide (ratio, drift, accept) + k_commit
-    # (Sherman-Morrison rows, orbital rows, Jastrow pair rows); the
-    # algorithmic bytes are the per-move B_move of the reference algorithm
+    # (Sherman-Morrison rows, orbital rows, Jastrow pair rows of the accepted
+    # walkers; the engine updates lazily, so its bytes scale with acceptance)
     ms_cm, n_cm = stages["commit"]
     upd_ms = ms_acc / n_acc + ms_cm / n_cm
-    upd_gbs = alg["b_move"] / (upd_ms * 1e-3) / 1e9
+    acc_frac = eff[args.precision]["accept"]
+    b_upd = update_bytes(system, W, acc_frac)
+    upd_gbs = b_upd / (upd_ms * 1e-3) / 1e9
     roof_hbm = {"kernel": "k_decide + k_commit (ratio, accept, Sherman-Morrison and table commit)", "bound": "hbm",
                 "achieved": upd_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                 "frac": upd_gbs / peaks.get("hbm_gbs"), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-                "work_per_launch": "8*(2 n^2 + 6N + 8(N-1) + 4 O) bytes per walker-move"}
+                "traffic": update_traffic(W),
+                "work_per_launch": "engine's lazy update per walker-move: 8*(n + 4 O + 12 + N) B read by k_decide, "
+                                  "plus for an accepted move 8*(2 n^2 + 2 n + 8 n + 2 M + 14 N) B in k_commit; "
+                                  f"acceptance {acc_frac:.3f}"}
     cpu_rate, cpu_steps, cpu_dt = cpu_port_rate(system, os.cpu_count() or 1, os.cpu_count() or 1,
                                                 min_seconds=10.0, max_steps=1000)
     h2d = W * system.nelec * 3 * 8 + W * 32
     d2h = h2d + W * 8 * 8
+    ef64, efmx = eff["fp64"], eff["mixed"]
+    diff = efmx["energy"] - ef64["energy"]
     line = {
         "metric": "electron-moves/s", "value": value, "unit": "electron-moves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -456,15 +523,28 @@ def run_ours(args):
         "data": "synthetic",
         "config": {"workload": desc, "walkers": W, "electrons": system.nelec, "basis": system.nbasis,
                    "orbitals": system.norb, "centres": system.ncent, "precision": args.precision,
+                   "equilibration_sweeps": args.equil,
                    "l2": "per-walker state (3.8 GB of Jastrow pair tables alone) exceeds the 126 MB L2",
                    "parallelism": f"replicas x{world} (independent walker populations, no data-path collective)"},
         "e2e": {"value": e2e, "unit": "electron-moves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "path": "cw_set_walkers (pinned host x, rng) + cw_vmc_steps(1) + cw_get_walkers + cw_end_block"},
+                "path": "cw_set_walkers (pinned host x, rng; includes the zerest hpsi of every walker) + "
+                        "cw_vmc_steps(1) + cw_get_walkers + cw_end_block"},
         "roofline": roof, "roofline_hbm": roof_hbm,
-        "efficiency": {"value": eff, "unit": "1/(Ha^2 s)", "energy": res["energy"], "err": res["err"],
-                       "sigma": res["sigma"], "t_s": ms_dev * 1e-3,
-                       "note": "one block of the timed steps, walkers in the role of CHAMP ranks; "
-                               "walkers only warmed up, not equilibrated"},
+        "efficiency_fp64": {"value": ef64["efficiency"], "unit": "1/(Ha^2 s)", "energy": ef64["energy"],
+                            "err": ef64["err"], "sigma": ef64["sigma"], "tcorr": ef64["tcorr"],
+                            "accept": ef64["accept"], "t_s": ef64["t_s"]},
+        "efficiency_mixed": {"value": efmx["efficiency"], "unit": "1/(Ha^2 s)", "energy": efmx["energy"],
+                             "err": efmx["err"], "sigma": efmx["sigma"], "tcorr": efmx["tcorr"],
+                             "accept": efmx["accept"], "t_s": efmx["t_s"]},
+        "efficiency_ratio_mixed_over_fp64": (efmx["efficiency"] / ef64["efficiency"])
+        if ef64["efficiency"] and efmx["efficiency"] else None,
+        "mean_E_diff_mHa": {"value": diff * 1e3, "combined_err_mHa": 1e3 * (ef64["err"] ** 2 + efmx["err"] ** 2) ** 0.5,
+                            "bias_matched_mHa": bias * 1e3 if bias is not None else None,
+                            "matched_walkers": int(same.sum()), "target_mHa": 0.1,
+                            "note": f"{args.blocks} blocks x {args.block_steps} sweeps per precision from the same "
+                                    "equilibrated walkers and streams; walks part where a near-threshold decision "
+                                    "differs, so the difference of the means is statistical; the bias is the mean "
+                                    "E_L difference over the first block's walkers whose decisions all agreed"},
         "top_stage": {"name": top[0], "ms": top[1][0], "launches": top[1][1]},
         "stages_ms_per_step": {k: round(v[0], 3) for k, v in stages.items()},
         "cpu_baseline": {"value": cpu_rate, "unit": "electron-moves/s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -486,6 +566,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
     ap.add_argument("--walkers", type=int, default=0)
+    ap.add_argument("--equil", type=int, default=50, help="equilibration sweeps before the timed steps")
+    ap.add_argument("--blocks", type=int, default=10, help="blocks of each efficiency run")
+    ap.add_argument("--block-steps", type=int, default=5, help="sweeps per block of the efficiency runs")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--rate", type=float, default=4.0, help="c4: job arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=16.0, help="c4: HBM budget of the admitted jobs")

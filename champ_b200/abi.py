@@ -139,11 +139,17 @@ def load_engine(path: str | None = None):
     lib.cw_checkpoint_bytes.restype = C.c_long
     lib.cw_checkpoint.argtypes = [V, C.c_void_p, C.c_long]
     lib.cw_restore.argtypes = [V, C.c_void_p, C.c_long]
+    lib.cw_walker_status.argtypes = [V, C.POINTER(C.c_int32)]
+    lib.cw_psie.argtypes = [V, C.c_int, _dp, _dp, _dp]
+    lib.cw_grad.argtypes = [V, C.c_int, C.c_int, _dp]
+    lib.cw_commit.argtypes = [V, C.c_int, C.POINTER(C.c_int32)]
+    lib.cw_update_ymat.argtypes = [V, C.c_int]
     for f in ("cw_dmc_set_tmoves", "cw_dmc_counts", "cw_checkpoint", "cw_restore", "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
               "cw_rng_states", "cw_sites", "cw_sync", "cw_set_walkers", "cw_get_walkers", "cw_vmc_steps", "cw_end_block",
               "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow", "cw_slater",
               "cw_get_sums", "cw_get_state", "cw_results_state", "cw_state_energies", "cw_opt_ci",
-              "cw_opt_ci_sums", "cw_ci_o", "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o"):
+              "cw_opt_ci_sums", "cw_ci_o", "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
+              "cw_walker_status", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat"):
         getattr(lib, f).restype = C.c_int
     if path is None:
         _engine = lib
@@ -159,6 +165,7 @@ EXPORTED_SYMBOLS = [
     "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore", "cw_dmc_set_tmoves", "cw_dmc_counts",
     "cw_device_bytes", "cw_results_state", "cw_state_energies", "cw_opt_ci", "cw_opt_ci_sums", "cw_ci_o",
     "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
+    "cw_walker_status", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

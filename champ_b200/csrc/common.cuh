@@ -128,6 +128,7 @@ struct MoveScratch {
   int nearestn, igeo;
   double rvminon[3];
   double ratio;       // determinant ratio of the proposed move (k_decide)
+  double psidn;       // psi_D at a caller's point (k_hook_ratio)
   int acc;           // accepted? (k_decide)
   int tel;           // electron of a T-move (moves whose launch gives no electron)
 };

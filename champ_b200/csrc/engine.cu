@@ -21,6 +21,7 @@
 #include "hpsi.cuh"
 #include "move.cuh"
 #include "dmc.cuh"
+#include "hooks.cuh"
 #include "mdet.cuh"
 #include "optjas.cuh"
 #include "peak.cuh"
@@ -114,6 +115,11 @@ struct cw_ctx {
   float *coef_hi = nullptr, *coef_lo = nullptr;   // [Oa][kp]
   int *d_err = nullptr;                            // tensor-core stage error flags
   CUtensorMap tm_b_hi{}, tm_b_lo{}, tm_mv_hi{}, tm_mv_lo{}, tm_all_hi{}, tm_all_lo{};
+  // per-electron routines (cw_psie, cw_grad, cw_commit, cw_update_ymat)
+  double *hook_buf = nullptr;    // [W][3] points in, [W][3] values out (device)
+  int *hook_acc = nullptr;       // [W] accept flags (device)
+  int hook_psie_iel = -1;        // electron of the last cw_psie (-1: none since the last commit)
+  int hook_md_iel = -1;          // electron whose multideterminant move tables are prepared
 };
 
 namespace {
@@ -867,6 +873,9 @@ int alloc_walkers(cw_ctx *c, int W) {
   DALLOC(L, b.entab, (size_t)W * M * N * kEnFields);
   b.entabf = nullptr;
   if (c->mixed) DALLOC(L, b.entabf, (size_t)W * M * N * kEnFields);
+  DALLOC(L, c->hook_buf, (size_t)W * 6);
+  DALLOC(L, c->hook_acc, W);
+  c->hook_psie_iel = c->hook_md_iel = -1;
   CK(cudaMemsetAsync(s.status, 0, sizeof(int) * W, c->stream));
   CK(cudaMemsetAsync(s.sums, 0, sizeof(double) * W * 8, c->stream));
   c->W = W;
@@ -1304,6 +1313,14 @@ int cw_set_walkers(cw_ctx *c, int nwalk, const double *x, const uint64_t *rng) {
   return zerest(c);
 }
 
+int cw_walker_status(cw_ctx *c, int32_t *status) {
+  if (!c || !status) return CW_ERR_ARG;
+  if (c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
+  CK(cudaMemcpyAsync(status, c->st.status, sizeof(int) * c->W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CW_OK;
+}
+
 int cw_get_walkers(cw_ctx *c, double *x, uint64_t *rng) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
   const int N = c->h.N, W = c->W;
@@ -1319,6 +1336,112 @@ int cw_get_walkers(cw_ctx *c, double *x, uint64_t *rng) {
     CK(cudaMemcpyAsync(rng, c->st.rng, sizeof(uint64_t) * 4 * W, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
+  return CW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Per-electron routines for a driver that keeps metrop6 on the host
+// (psie, compute_determinante_grad, detsav + jassav, update_ymat), batched
+// over the walkers of a VMC population.  Host arrays in, host arrays out.
+// ---------------------------------------------------------------------------
+int hook_check(cw_ctx *c, int iel, const char *what) {
+  if (!c) return CW_ERR_ARG;
+  if (c->W == 0) return fail(c, CW_ERR_STATE, "%s: no walkers", what);
+  if (c->dmc.on) return fail(c, CW_ERR_STATE, "%s: the population is a DMC population", what);
+  if (iel < 0 || iel >= c->h.N) return fail(c, CW_ERR_ARG, "%s: electron %d outside [0, %d)", what, iel, c->h.N);
+  return CW_OK;
+}
+
+// multideterminant move tables of electron iel at the current configuration
+// (spin-phase sums at the first electron of a spin, drift correction at the
+// old position): what the engine's own sweep does before each proposal
+int hook_md_prepare(cw_ctx *c, int iel) {
+  if (!c->md_on || c->hook_md_iel == iel) return CW_OK;
+  int rc = md_before_propose(c, iel);
+  if (rc) return rc;
+  c->hook_md_iel = iel;
+  return CW_OK;
+}
+
+extern "C" int cw_psie(cw_ctx *c, int iel, const double *xnew, double *psid, double *psij) {
+  if (int rc = hook_check(c, iel, "cw_psie")) return rc;
+  if (!xnew) return fail(c, CW_ERR_ARG, "cw_psie: xnew is NULL");
+  BIND(c);
+  const int W = c->W;
+  if (int rc = hook_md_prepare(c, iel)) return rc;
+  CK(cudaMemcpyAsync(c->hook_buf, xnew, sizeof(double) * 3 * W, cudaMemcpyHostToDevice, c->stream));
+  k_hook_place<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->hook_buf);
+  LCHK("k_hook_place");
+  NORD_DISPATCH(launch_jmove, c, iel);
+  LCHK("k_jastrow_move");
+  const int bw = c->basis_warps;
+  k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+  LCHK("k_basis_move");
+  if (int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn)) return rc;
+  if (int rc = md_after_lcao(c, iel)) return rc;
+  double *out = c->hook_buf + (size_t)3 * W;
+  k_hook_ratio<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel, out);
+  LCHK("k_hook_ratio");
+  std::vector<double> h((size_t)2 * W);
+  CK(cudaMemcpyAsync(h.data(), out, sizeof(double) * 2 * W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (int rc = check_status(c)) return rc;
+  for (int w = 0; w < W; w++) {
+    if (psid) psid[w] = h[2 * w];
+    if (psij) psij[w] = h[2 * w + 1];
+  }
+  c->hook_psie_iel = iel;
+  return CW_OK;
+}
+
+extern "C" int cw_grad(cw_ctx *c, int iel, int iflag_move, double *vd) {
+  if (int rc = hook_check(c, iel, "cw_grad")) return rc;
+  if (!vd) return fail(c, CW_ERR_ARG, "cw_grad: vd is NULL");
+  if (iflag_move != 0 && iflag_move != 1)
+    return fail(c, CW_ERR_ARG, "cw_grad: iflag_move %d (1: current position, 0: point of the last cw_psie)",
+                iflag_move);
+  if (iflag_move == 0 && c->hook_psie_iel != iel)
+    return fail(c, CW_ERR_STATE, "cw_grad(iflag_move=0) of electron %d needs its cw_psie first", iel);
+  BIND(c);
+  const int W = c->W;
+  if (iflag_move == 1) {
+    if (int rc = hook_md_prepare(c, iel)) return rc;
+  }
+  double *out = c->hook_buf + (size_t)3 * W;
+  k_hook_grad<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel, iflag_move, out);
+  LCHK("k_hook_grad");
+  CK(cudaMemcpyAsync(vd, out, sizeof(double) * 3 * W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CW_OK;
+}
+
+extern "C" int cw_commit(cw_ctx *c, int iel, const int32_t *accept) {
+  if (int rc = hook_check(c, iel, "cw_commit")) return rc;
+  if (!accept) return fail(c, CW_ERR_ARG, "cw_commit: accept is NULL");
+  if (c->hook_psie_iel != iel)
+    return fail(c, CW_ERR_STATE, "cw_commit of electron %d needs its cw_psie first", iel);
+  BIND(c);
+  const int W = c->W;
+  CK(cudaMemcpyAsync(c->hook_acc, accept, sizeof(int) * W, cudaMemcpyHostToDevice, c->stream));
+  k_hook_accept<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, iel, c->hook_acc);
+  LCHK("k_hook_accept");
+  k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel);
+  LCHK("k_commit");
+  if (int rc = md_after_commit(c, iel)) return rc;
+  // the walk's tables changed: a cw_graph-captured sweep stays valid (same
+  // buffers), the prepared multideterminant tables of this electron do not
+  c->hook_psie_iel = -1;
+  c->hook_md_iel = -1;
+  CK(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+extern "C" int cw_update_ymat(cw_ctx *c, int iel) {
+  if (int rc = hook_check(c, iel, "cw_update_ymat")) return rc;
+  if (!c->md_on || iel + 1 >= c->h.N) return CW_OK;
+  BIND(c);
+  if (int rc = hook_md_prepare(c, iel + 1)) return rc;
+  CK(cudaStreamSynchronize(c->stream));
   return CW_OK;
 }
 

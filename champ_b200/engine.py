@@ -33,7 +33,12 @@ DEFAULT_SEED = "18123437465549275475255231234865"  # vmc/parser.f90:315
 
 
 class EngineError(RuntimeError):
-    pass
+    def __init__(self, msg, code=0):
+        super().__init__(msg)
+        self.code = code
+
+
+CW_ERR_SINGULAR = 4
 
 
 def seed_ints(cseed: str = DEFAULT_SEED) -> np.ndarray:
@@ -66,6 +71,29 @@ def initial_configs(system, rng: np.ndarray):
     return x
 
 
+def start_population(eng, system, rng: np.ndarray, max_redraws: int = 32):
+    """mc_configs_start (vmc/mc_configs.f90:33) for every walker of `eng`:
+    sites start positions drawn from each walker's stream (rng [W][4],
+    advanced in place), then cw_set_walkers.  A walker whose Slater matrix is
+    singular at its start (two same-spin electrons where the occupied
+    orbitals cannot tell them apart) draws a new sites start from its own,
+    further advanced, stream; CHAMP would stop the run there (matinv).
+    Returns the start positions."""
+    x = initial_configs(system, rng)
+    for _ in range(max_redraws):
+        try:
+            eng.set_walkers(x, rng)
+            return x
+        except EngineError as e:
+            if e.code != CW_ERR_SINGULAR:
+                raise
+        bad = np.nonzero(eng.walker_status() & 1)[0]
+        sub = np.ascontiguousarray(rng[bad])
+        x[bad] = initial_configs(system, sub)
+        rng[bad] = sub
+    raise EngineError(f"walkers still singular after {max_redraws} new start draws", CW_ERR_SINGULAR)
+
+
 class Engine:
     def __init__(self, system, device: int = 0, precision: str = "fp64"):
         self.lib = load_engine()
@@ -80,7 +108,7 @@ class Engine:
     def _check(self, rc, what):
         if rc:
             msg = self.lib.cw_last_error(self.h).decode() if self.h else ""
-            raise EngineError(f"{what} failed (status {rc}): {msg}")
+            raise EngineError(f"{what} failed (status {rc}): {msg}", rc)
 
     def close(self):
         if self.h:
@@ -99,6 +127,36 @@ class Engine:
         rng = np.ascontiguousarray(rng, np.uint64)
         self.W = rng.shape[0]
         self._check(self.lib.cw_set_walkers(self.h, self.W, dptr(x), u64ptr(rng)), "cw_set_walkers")
+
+    def walker_status(self):
+        """Per-walker status words (bit 0 singular Slater matrix, bit 1
+        non-finite local energy, bit 2 proposal rejection loop gave up)."""
+        out = np.zeros(self.W, np.int32)
+        self._check(self.lib.cw_walker_status(self.h, out.ctypes.data_as(C.POINTER(C.c_int32))), "cw_walker_status")
+        return out
+
+    # -- per-electron routines (a metrop6 kept on the host) ---------------
+    def psie(self, iel: int, xnew):
+        """psie of electron iel at xnew [W][3] for every walker: (psid, psij)."""
+        xnew = np.ascontiguousarray(xnew, np.float64)
+        psid, psij = np.zeros(self.W), np.zeros(self.W)
+        self._check(self.lib.cw_psie(self.h, iel, dptr(xnew), dptr(psid), dptr(psij)), "cw_psie")
+        return psid, psij
+
+    def grad(self, iel: int, iflag_move: int):
+        """compute_determinante_grad of electron iel: [W][3] at the current
+        position (iflag_move=1) or at the point of the last psie (0)."""
+        vd = np.zeros((self.W, 3))
+        self._check(self.lib.cw_grad(self.h, iel, iflag_move, dptr(vd)), "cw_grad")
+        return vd
+
+    def commit(self, iel: int, accept):
+        """jassav + detsav for the walkers with accept[w] set, restore for the others."""
+        a = np.ascontiguousarray(accept, np.int32)
+        self._check(self.lib.cw_commit(self.h, iel, a.ctypes.data_as(C.POINTER(C.c_int32))), "cw_commit")
+
+    def update_ymat(self, iel: int):
+        self._check(self.lib.cw_update_ymat(self.h, iel), "cw_update_ymat")
 
     def walkers(self):
         x = np.zeros((self.W, self.system.nelec, 3))

@@ -96,11 +96,10 @@ def estimate_bytes(system, nwalk: int, precision: str = "fp64", chunk_bytes: int
 
 
 def _engine_for(job: Job, precision: str, device: int):
-    from .engine import Engine, initial_configs, rng_states
+    from .engine import Engine, rng_states, start_population
     eng = Engine(job.system, device=device, precision=precision)
     rng = rng_states(job.seed_offset + job.nwalk)[job.seed_offset:].copy()
-    x = initial_configs(job.system, rng)
-    eng.set_walkers(x, rng)
+    start_population(eng, job.system, rng)
     return eng
 
 

@@ -145,6 +145,15 @@ int cw_sync(cw_ctx *ctx);
 int cw_set_walkers(cw_ctx *ctx, int nwalk, const double *x, const uint64_t *rng);
 int cw_get_walkers(cw_ctx *ctx, double *x, uint64_t *rng);
 
+/* Per-walker status words of the population, status [nwalk]: bit 0 the
+ * walker's Slater matrix was singular at its last full recompute (CHAMP
+ * stops the run there, vmc/matinv.f90:59-63), bit 1 its local energy was not
+ * finite, bit 2 a rejection loop of its proposal gave up.  A call that
+ * returned CW_ERR_SINGULAR or CW_ERR_STATE leaves the population in place,
+ * so the caller can find the walkers concerned (for example to draw new
+ * start positions for them and call cw_set_walkers again). */
+int cw_walker_status(cw_ctx *ctx, int32_t *status);
+
 /* ------------------------------------------------------------------------ */
 /* Batched drop-ins for CHAMP's per-walker routines                          */
 /* ------------------------------------------------------------------------ */
@@ -236,6 +245,46 @@ int cw_jastrow(cw_ctx *ctx, double *psij, double *v, double *d2j);
  * (vmc/determinant.f90:9): slmi [nwalk][2][nmax*nmax] with nmax=max(nup,ndn)
  * (spin iab: slmi(j+nel*(i-1)) of CHAMP), det [nwalk][2]. */
 int cw_slater(cw_ctx *ctx, double *slmi, double *det);
+
+/* ------------------------------------------------------------------------ */
+/* Per-electron routines, for a driver that keeps metrop6's electron loop on */
+/* the host (vmc/metrop_mov1_slat.f90:131-630), batched over the walkers of */
+/* a VMC population (CW_ERR_STATE for a DMC population).  The caller makes */
+/* the proposal and the accept/reject decision; the engine keeps the tables. */
+/* Per electron iel (0-based): cw_grad(iel, 1), proposal, cw_psie(iel),      */
+/* cw_grad(iel, 0), decision, cw_commit(iel), cw_update_ymat(iel); after the */
+/* last electron, cw_hpsi.                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* psie (vmc/hpsie.f90:3) of electron iel at the proposed point of every
+ * walker, xnew [nwalk][3]: distances, jastrowe (jastrow4e), determinante
+ * (orbitalse + the determinant ratio) and, with several determinants,
+ * multideterminante + determinante_psit.  psid [nwalk] = psi_D at the point
+ * (CHAMP's psid(1)), psij [nwalk] = the Jastrow exponent there (psij(1));
+ * either may be NULL.  The walkers' own tables are not changed. */
+int cw_psie(cw_ctx *ctx, int iel, const double *xnew, double *psid, double *psij);
+
+/* compute_determinante_grad (vmc/determinante.f90:69) of electron iel:
+ * vd [nwalk][3] = grad ln|psi_D| + grad J, iflag_move = 1 at the current
+ * position, 0 at the point of the last cw_psie of the same electron
+ * (CW_ERR_STATE without one). */
+int cw_grad(cw_ctx *ctx, int iel, int iflag_move, double *vd);
+
+/* The end of a move of electron iel (vmc/metrop_mov1_slat.f90:592-626):
+ * walkers with accept[w] != 0 take the point of the last cw_psie as their
+ * position, with jassav (vmc/jassav.f90:3) and detsav (vmc/detsav.f90:3:
+ * the Sherman-Morrison update of the inverse, the new orbital row and
+ * determinant); the other walkers keep their position and tables
+ * (distancese_restore).  Needs the cw_psie of the same electron. */
+int cw_commit(cw_ctx *ctx, int iel, const int32_t *accept);
+
+/* update_ymat (vmc/multideterminant.f90:562) after the move of electron
+ * iel: with several determinants the engine prepares the multideterminant
+ * tables for the move of electron iel+1 (the spin-phase sums at the first
+ * electron of a spin and the drift correction at its position); cw_grad and
+ * cw_psie prepare them as well when this call is left out.  No-op for one
+ * determinant. */
+int cw_update_ymat(cw_ctx *ctx, int iel);
 
 /* Per-walker sums since the last cw_end_block: out [nwalk][5] =
  * (wsum, esum, pesum, tpbsum, accepted moves). */

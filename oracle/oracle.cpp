@@ -3213,6 +3213,44 @@ void or_get_state(void *wsp, double *eold, double *psido, double *psijo) {
 
 
 // ----------------------------------------------------------------------------
+// Per-electron routines of walker k, for a driver that keeps metrop6 on the
+// host: psie (vmc/hpsie.f90:3) at a point, compute_determinante_grad
+// (vmc/determinante.f90:69), the accept branch of metrop6
+// (vmc/metrop_mov1_slat.f90:592-619: jassav, detsav) or distancese_restore
+// (:621-626), update_ymat (vmc/multideterminant.f90:562).
+// ----------------------------------------------------------------------------
+int or_w1_psie(void *wsp, int k, int iel, const double *xnew3, double *out) {
+  Walker &w = ((Walkers *)wsp)->w[k];
+  w.xnew = w.xold;
+  for (int c = 0; c < 3; c++) w.xnew[c + 3 * iel] = xnew3[c];
+  double psij = 0;
+  const double psid = w.psie(iel, w.xnew.data(), psij, 0);
+  out[0] = psid;
+  out[1] = psij;
+  return w.singular ? 1 : 0;
+}
+
+void or_w1_grad(void *wsp, int k, int iel, int iflag_move, double *vd) {
+  ((Walkers *)wsp)->w[k].grad(iel, iflag_move, vd);
+}
+
+void or_w1_commit(void *wsp, int k, int iel, int accept, double psidn, double psijn) {
+  Walker &w = ((Walkers *)wsp)->w[k];
+  if (accept) {
+    for (int c = 0; c < 3; c++) w.xold[c + 3 * iel] = w.xnew[c + 3 * iel];
+    w.psido = psidn;
+    w.psijo = psijn;
+    w.jassav(iel, 0);
+    w.detsav(iel);
+  } else {
+    for (int c = 0; c < 3; c++) w.xnew[c + 3 * iel] = w.xold[c + 3 * iel];
+    w.distancese_restore(iel);
+  }
+}
+
+void or_w1_update_ymat(void *wsp, int k, int iel) { ((Walkers *)wsp)->w[k].update_ymat(iel); }
+
+// ----------------------------------------------------------------------------
 // DMC
 // ----------------------------------------------------------------------------
 void *or_dmc_create(void *sysp, int nwalk, const double *x, const uint64_t *rng, const uint64_t *pop_rng,

@@ -235,6 +235,35 @@ class OracleWalkers:
         lib().or_get_state(self.h, dp(e), dp(p), dp(j))
         return e, p, j
 
+    # per-electron routines of walker k (a metrop6 kept on the host)
+    def psie(self, k, iel, xnew3):
+        """psie (vmc/hpsie.f90:3) of electron iel of walker k at xnew3: (psid, psij)."""
+        L = lib()
+        L.or_w1_psie.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp]
+        out = np.zeros(2)
+        if L.or_w1_psie(self.h, k, iel, dp(np.ascontiguousarray(xnew3, float)), dp(out)):
+            raise RuntimeError("singular multideterminant table")
+        return out[0], out[1]
+
+    def grad(self, k, iel, iflag_move):
+        """compute_determinante_grad: drift of electron iel, 1 = current, 0 = at the last psie point."""
+        L = lib()
+        L.or_w1_grad.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp]
+        v = np.zeros(3)
+        L.or_w1_grad(self.h, k, iel, iflag_move, dp(v))
+        return v
+
+    def commit(self, k, iel, accept, psidn=0.0, psijn=0.0):
+        """metrop6's accept branch (jassav, detsav) or distancese_restore."""
+        L = lib()
+        L.or_w1_commit.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.or_w1_commit(self.h, k, iel, 1 if accept else 0, float(psidn), float(psijn))
+
+    def update_ymat(self, k, iel):
+        L = lib()
+        L.or_w1_update_ymat.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.or_w1_update_ymat(self.h, k, iel)
+
 
 class OracleDmc:
     """DMC population of the oracle (dmc_ps + branching + splitj)."""

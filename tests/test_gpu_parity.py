@@ -125,8 +125,16 @@ def test_determinism(oracle_mod):
 
 
 def test_c1_hpsi(oracle_mod):
-    """The 120-electron, 30-centre, 540-AO benchmark molecule: per-walker E_L."""
+    """The 120-electron, 30-centre, 540-AO benchmark molecule: per-walker E_L
+    at configurations equilibrated by 10 oracle sweeps (a sites start can put
+    more same-spin electrons near an atom than its occupied orbitals hold,
+    where the Slater matrix is nearly singular and E_L ill-conditioned)."""
+    from champ_b200.engine import Engine
     s, eng, o, x, rng = _setup(oracle_mod, "c1", 2)
+    ow = oracle_mod.OracleWalkers(o, x, rng)
+    ow.steps(10, 2)
+    x, rng = ow.walkers()
+    eng.set_walkers(x, rng)
     h = eng.hpsi()
     for w in range(2):
         r = o.hpsi(x[w])

@@ -157,7 +157,7 @@ def test_c1_dmc_parity(oracle_mod):
     """The 120-electron molecule through the DMC move kernels (FP64)."""
     from champ_b200.system import make_synthetic
     s = make_synthetic("c1")
-    dg, do = _dmc_pair(oracle_mod, s, 4, 2, 0.01)
+    dg, do = _dmc_pair(oracle_mod, s, 4, 10, 0.01)
     for step in range(2):
         dg.steps(1)
         do.steps(1, 8)
