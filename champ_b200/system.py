@@ -451,12 +451,14 @@ def assemble_basis(types):
 # Seeded synthetic systems
 # ---------------------------------------------------------------------------
 
-def _random_shells(rng, spec):
-    """spec: list of (l, count); 3 primitives per shell, exponents log-uniform in [0.1, 20]."""
+def _random_shells(rng, spec, ranges=None):
+    """spec: list of (l, count); 3 primitives per shell, exponents log-uniform
+    in [0.1, 20], or in ranges[l] = (lo, hi) when given."""
     shells = []
     for l, cnt in spec:
+        lo, hi = ranges[l] if ranges else (0.1, 20.0)
         for _ in range(cnt):
-            ex = np.exp(rng.uniform(np.log(0.1), np.log(20.0), size=3))
+            ex = np.exp(rng.uniform(np.log(lo), np.log(hi), size=3))
             co = rng.uniform(0.2, 1.0, size=3)
             shells.append((l, ex, co))
     return shells
@@ -536,7 +538,36 @@ def model_hamiltonian_orbitals(cent, types_of_centre, type_defs, norb, ecp=None)
     V = trial.potential_matrix(basis, np.asarray(cent, float), types_of_centre, znuc, ecp,
                                [td.get("screen", SCREEN_ALPHA) for td in type_defs])
     coef, _ = trial.model_orbitals(S, T + V, norb)
-    return coef
+    return coef, basis
+
+
+def determinant_scale(basis, coef, cent, types_of_centre, znuc, nup, ndn, nconf=4, seed=12345):
+    """A constant c for the LCAO coefficients such that the Slater
+    determinants of typical configurations are of order one.
+
+    psi_D is defined up to a constant factor, and every determinant of an
+    expansion holds the same number of electrons of each spin, so scaling
+    every orbital by c scales psi_D by c^nelec and leaves ratios, drifts,
+    local energies and the walk unchanged.  Unscaled, the determinants of
+    large molecules (100 electrons of a spin) fall below the smallest FP64
+    number and psi_D underflows to zero.  c is exp(-<ln|det|>/n) over a few
+    configurations that place the electrons around the nuclei in proportion
+    to their charges (the sites rule), from a private random stream."""
+    from . import trial
+    rng = np.random.default_rng(seed)
+    z = np.array([znuc[t] for t in types_of_centre], float)
+    logs = []
+    for _ in range(nconf):
+        for n in (nup, ndn):
+            if n == 0:
+                continue
+            at = rng.choice(len(z), size=n, p=z / z.sum())
+            pts = np.asarray(cent, float)[at] + rng.normal(0.0, 0.7, size=(n, 3))
+            A = trial.ao_values(basis, np.arange(len(basis["ao_cent"])), pts) @ coef[:n].T
+            sgn, lg = np.linalg.slogdet(A)
+            if sgn != 0:
+                logs.append(lg / n)
+    return float(np.exp(-np.mean(logs))) if logs else 1.0
 
 
 def _assemble(name, rng, cent, types_of_centre, type_defs, nelec, nup, norb, nocc_up, nocc_dn,
@@ -567,7 +598,9 @@ def _assemble(name, rng, cent, types_of_centre, type_defs, nelec, nup, norb, noc
         ecp = None
         if nloc:
             ecp = [(lpot[it], nterm[it], power[it], expo[it], ecoef[it]) for it in range(nct)]
-        sysd["coef"] = model_hamiltonian_orbitals(cent, types_of_centre, type_defs, norb, ecp)
+        coef, basis_desc = model_hamiltonian_orbitals(cent, types_of_centre, type_defs, norb, ecp)
+        zn = [td["z"] for td in type_defs]
+        sysd["coef"] = coef * determinant_scale(basis_desc, coef, cent, types_of_centre, zn, nocc_up, nocc_dn)
     return System(**sysd)
 
 
@@ -590,9 +623,9 @@ def make_synthetic(config: str, seed: int = 20261203, orbitals: str = "model") -
     c0: 3 nuclei in a 4 bohr box (Z 6/1/1, ECP on the heavy atom, l_max=1,
         6-point quadrature), 8 electrons (4/4), 60 Gaussians (s/p/d,
         exponents log-uniform 0.1-20), 4 orbitals, order-5 Jastrow.
-    c1: 30 nuclei on a zig-zag chain alternating Cl-like (Z=7, ECP) and
-        H-like (Z=1) centres, neutral: 120 electrons (60/60), 540 Gaussians,
-        60 orbitals.
+    c1: 30 nuclei on a zig-zag chain alternating Cl-like (Z=7, ECP with s
+        and p channels) and H-like (Z=1) centres, neutral: 120 electrons
+        (60/60), 540 Gaussians (valence exponent ranges), 60 orbitals.
     tiny: 2 nuclei, 6 electrons, small basis (fast parity cases).
     c2: 12 nuclei, 40 electrons, 300 Gaussians, 80 orbitals, 10^4
         determinants (multideterminant DMC).
@@ -634,20 +667,28 @@ def _make_synthetic(config, seed, orbitals):
     raise ValueError(f"unknown synthetic config {config!r}")
 
 
+# Exponent ranges (bohr^-2) of the chain molecules' valence basis: s and p
+# down to diffuse 0.08, up to 6 (s) and 4 (p); one d shell between 0.3 and
+# 1.5 -- the span of pseudopotential valence basis sets, without the steep
+# core-like functions that a pseudopotential makes unnecessary.
+VALENCE_RANGES = {0: (0.08, 6.0), 1: (0.08, 4.0), 2: (0.3, 1.5)}
+
+
 def _chain_molecule(rng, name, nat, nelec, orbitals):
     """Zig-zag chain of nat centres alternating Cl-like heavy atoms (valence
-    charge 7, BFD-form pseudopotential with a local and an s channel, s4 p4
-    d1 basis = 22 Cartesian AOs) and H-like atoms (charge 1, s2 p4 = 14
-    AOs), 2.0 bohr apart along x and 1.2 bohr across, nelec electrons
-    (ceil/floor halves), one occupied orbital per up electron.  With nelec =
-    4 nat the molecule is neutral (a chain of HCl-like units)."""
+    charge 7, BFD-form pseudopotential with a local, an s and a p channel,
+    s4 p4 d1 basis = 22 Cartesian AOs) and H-like atoms (charge 1, s2 p4 =
+    14 AOs), valence basis exponents (VALENCE_RANGES), 2.0 bohr apart along x
+    and 1.2 bohr across, nelec electrons (ceil/floor halves), one occupied
+    orbital per up electron.  With nelec = 4 nat the molecule is neutral (a
+    chain of HCl-like units)."""
     cent = np.zeros((nat, 3))
     for i in range(nat):
         cent[i] = (2.0 * i + rng.normal(0, 0.05), 1.2 * (i % 2) + rng.normal(0, 0.05), rng.normal(0, 0.05))
-    heavy = dict(z=7.0, lpot=2, a1=0.0, screen=0.15,
-                 basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 1)]), 7.0, 4))
-    hyd = dict(z=1.0, lpot=1, a1=-1.0, screen=0.15,
-               basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 4)]), 1.0, 4))
+    heavy = dict(z=7.0, lpot=3, a1=0.0, screen=0.5,
+                 basis=_type_from_shells(_random_shells(rng, [(0, 4), (1, 4), (2, 1)], VALENCE_RANGES), 7.0, 4))
+    hyd = dict(z=1.0, lpot=1, a1=-1.0, screen=0.5,
+               basis=_type_from_shells(_random_shells(rng, [(0, 2), (1, 4)], VALENCE_RANGES), 1.0, 4))
     types = [0 if i % 2 == 0 else 1 for i in range(nat)]
     nup, ndn = (nelec + 1) // 2, nelec // 2
     return _assemble(name, rng, cent, types, [heavy, hyd], nelec, nup, nup, nup, ndn, orbitals=orbitals)

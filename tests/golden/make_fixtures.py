@@ -7,7 +7,9 @@ of that source tree (the script refuses to run without it).  Writes:
   reference's own vmc/xoroshiro256starstar.c (compiled into oracle/_ref by
   oracle/Makefile) for CHAMP's default seed (vmc/parser.f90:315);
 * vmc_h2_system.npz — the VMC-H2 CI case (tests/CI_test/VMC-H2) read from
-  its CHAMP input files and pre-processed as read_bas_num does.
+  its CHAMP input files and pre-processed as read_bas_num does;
+* vmc_c4h6_500_system.npz — the VMC-C4H6-ci1010_pVTZ-00500-dets CI case
+  (BFD pseudopotentials, 500 determinants) read the same way.
 """
 import ctypes as C
 import os
@@ -49,9 +51,27 @@ def h2_fixture():
     save_npz(s, os.path.join(HERE, "vmc_h2_system.npz"))
 
 
+def c4h6_fixture():
+    """tests/CI_test/VMC-C4H6-ci1010_pVTZ-00500-dets: butadiene, BFD
+    pseudopotentials (C: local + s channel, H: local), BFD-T numerical basis
+    with f functions (226 AOs), 500 determinants, Jastrow 5 5 0 (no e-e-n
+    terms).  Orbitals beyond the highest one the determinants use (89) are
+    dropped: they do not enter psi."""
+    from champ_b200.champ_io import load_champ, save_npz
+    d = os.path.join(REF, "tests", "CI_test", "VMC-C4H6-ci1010_pVTZ-00500-dets") + "/"
+    s = load_champ("vmc_c4h6_500", d + "pool/champ_v3_butadiene.xyz",
+                   d + "pool/champ_v3_BFD-T_basis_pointers.bfinfo", d + "pool", "BFD-T",
+                   d + "champ_v3_trexio_order_ci1010_pVTZ_1_orbitals.lcao", d + "TZ_1M_500.det",
+                   d + "jastrow_good_b3lyp.0", nelec=22, nup=11, nloc=4, pp_dir=d + "pool", pp_id="BFD",
+                   znuc={"C": 4.0, "H": 1.0})
+    s.coef = s.coef[:int(s.iworbd.max())].copy()
+    save_npz(s, os.path.join(HERE, "vmc_c4h6_500_system.npz"))
+
+
 if __name__ == "__main__":
     if not REF or not os.path.isdir(os.path.join(REF, "src")):
         sys.exit("set CHAMP_REF to the root of a CHAMP source tree")
     rng_fixture()
     h2_fixture()
+    c4h6_fixture()
     print("fixtures written to", HERE)
