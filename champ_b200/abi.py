@@ -144,12 +144,14 @@ def load_engine(path: str | None = None):
     lib.cw_grad.argtypes = [V, C.c_int, C.c_int, _dp]
     lib.cw_commit.argtypes = [V, C.c_int, C.POINTER(C.c_int32)]
     lib.cw_update_ymat.argtypes = [V, C.c_int]
+    lib.cw_opt_orb.argtypes = [V, C.c_int, C.POINTER(C.c_int32)]
+    lib.cw_orb_o.argtypes = [V, _dp]
     for f in ("cw_dmc_set_tmoves", "cw_dmc_counts", "cw_checkpoint", "cw_restore", "cw_dmc_init", "cw_dmc_steps", "cw_dmc_end_block", "cw_dmc_results", "cw_dmc_walkers",
               "cw_rng_states", "cw_sites", "cw_sync", "cw_set_walkers", "cw_get_walkers", "cw_vmc_steps", "cw_end_block",
               "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow", "cw_slater",
               "cw_get_sums", "cw_get_state", "cw_results_state", "cw_state_energies", "cw_opt_ci",
               "cw_opt_ci_sums", "cw_ci_o", "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
-              "cw_walker_status", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat"):
+              "cw_walker_status", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o"):
         getattr(lib, f).restype = C.c_int
     if path is None:
         _engine = lib
@@ -165,7 +167,7 @@ EXPORTED_SYMBOLS = [
     "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore", "cw_dmc_set_tmoves", "cw_dmc_counts",
     "cw_device_bytes", "cw_results_state", "cw_state_energies", "cw_opt_ci", "cw_opt_ci_sums", "cw_ci_o",
     "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
-    "cw_walker_status", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat",
+    "cw_walker_status", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

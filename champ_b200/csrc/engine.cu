@@ -67,6 +67,7 @@ struct cw_ctx {
   HBuf hb{};
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
+  size_t smem_commit = 0;  // k_commit_tile's dynamic shared memory (0: the untiled k_commit)
   int ecp_warps = 1, ecp_naov = 0, ecp_minb = 1;
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
   std::unordered_map<void *, size_t> alloc_bytes;
@@ -120,6 +121,16 @@ struct cw_ctx {
   int *hook_acc = nullptr;       // [W] accept flags (device)
   int hook_psie_iel = -1;        // electron of the last cw_psie (-1: none since the last commit)
   int hook_md_iel = -1;          // electron whose multideterminant move tables are prepared
+  // orbital-rotation derivatives (cw_opt_orb): host term list, the slot of
+  // each electron's orbital in determinant 1, and the device tables of the
+  // current optimisation set-up
+  std::vector<int> orb_ideriv;   // [n][2] 1-based (io, jo)
+  std::vector<int> ref_orb;      // [nelec] 0-based orbital of each slot of determinant 1
+  bool orb_on = false;
+  int orb_nv = 0;
+  OrbTerm *orb_terms = nullptr;
+  int *orb_vorb = nullptr;
+  double *orb_vals = nullptr;    // [W][N][nv]
 };
 
 namespace {
@@ -304,6 +315,13 @@ void launch_ecp(cw_ctx *c) {
 }
 template <int NORD>
 int set_attrs(cw_ctx *c) {
+  {
+    // tiled commit: the spin's inverse (row stride nmax+1) and three vectors
+    // in shared memory, for inverses up to 128 x 128 (140 KB)
+    const int n = c->h.nmax;
+    c->smem_commit = n <= 128 ? sizeof(double) * ((size_t)n * (n + 1) + 3 * n) : 0;
+    if (c->smem_commit) CK(raise_smem(c, k_commit_tile, c->smem_commit));
+  }
   CK(raise_smem(c, k_jastrow_move<NORD>, (size_t)(c->smem_jmove)));
   CK(raise_smem(c, k_jastrow_move_f32<NORD>, (size_t)(c->smem_jmove_f32)));
   CK(raise_smem(c, k_jastrow_full<NORD, double>, c->smem_jfull));
@@ -348,6 +366,14 @@ int set_attrs(cw_ctx *c) {
     CK(raise_smem(c, k_ecp<NORD, float, 2>, c->smem_ecp));
   }
   return CW_OK;
+}
+
+// detsav + jassav of the accepted walkers (iel < 0: each walker's T-move electron)
+void launch_commit(cw_ctx *c, int iel) {
+  if (c->smem_commit)
+    k_commit_tile<<<c->W, 128, c->smem_commit, c->stream>>>(c->st, c->mb, c->g, iel);
+  else
+    k_commit<<<c->W, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel);
 }
 
 #define NORD_DISPATCH(fn, ...)            \
@@ -599,6 +625,13 @@ int opt_derivs(cw_ctx *c) {
                                         c->opt_njas);
     LCHK("k_md_ci_o");
   }
+  if (c->orb_on) {
+    const int nt = (int)c->orb_ideriv.size() / 2;
+    const long n = (long)W * nt;
+    k_orb_o<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(c->st, nt, c->orb_terms, c->orb_nv, c->orb_vals,
+                                                                c->opt_o, c->opt_ot, c->opt_np, c->opt_np - nt);
+    LCHK("k_orb_o");
+  }
   return CW_OK;
 }
 
@@ -647,6 +680,12 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
       k_md_scatter<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->md, c->hb.orball, e0, ne);
       stage_end(c);
       LCHK("k_md_scatter");
+    }
+    if (c->orb_on) {
+      const long nv = (long)W * ne * c->orb_nv;
+      k_orb_vals<<<(unsigned)((nv + 127) / 128), 128, 0, c->stream>>>(W, N, e0, ne, h.Oa, c->hb.orball, c->orb_nv,
+                                                                       c->orb_vorb, c->orb_vals);
+      LCHK("k_orb_vals");
     }
     const long ns = (long)W * ne * h.nmax;
     stage_begin(c, CW_ST_SCATTER);
@@ -737,6 +776,11 @@ void opt_reset(cw_ctx *c) {
   c->opt_o = c->opt_ot = c->jas_raw = c->jas_map = nullptr;
   c->sr_o = c->sr_eo = c->sr_oo = c->oo_tmp = nullptr;
   c->sr_w = 0;
+  c->orb_on = false;
+  c->orb_nv = 0;
+  c->orb_terms = nullptr;
+  c->orb_vorb = nullptr;
+  c->orb_vals = nullptr;
 }
 
 int alloc_walkers(cw_ctx *c, int W) {
@@ -1082,6 +1126,8 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     for (int mm = 0; mm < d->nbasis; mm++) ct[(size_t)mm * d->norb + o] = d->coef[(size_t)o * d->nbasis + mm];
   DALLOC(L, coefT, ct.size());
   CK(cudaMemcpy(coefT, ct.data(), ct.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->ref_orb.assign(d->iworbd, d->iworbd + d->nelec);
+  for (int &v : c->ref_orb) v -= 1;
   std::vector<int> so(2 * nmax, 0);
   for (int j = 0; j < d->nup; j++) so[j] = d->iworbd[j] - 1;
   for (int j = 0; j < ndn; j++) so[nmax + j] = d->iworbd[d->nup + j] - 1;
@@ -1425,7 +1471,7 @@ extern "C" int cw_commit(cw_ctx *c, int iel, const int32_t *accept) {
   CK(cudaMemcpyAsync(c->hook_acc, accept, sizeof(int) * W, cudaMemcpyHostToDevice, c->stream));
   k_hook_accept<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, iel, c->hook_acc);
   LCHK("k_hook_accept");
-  k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel);
+  launch_commit(c, iel);
   LCHK("k_commit");
   if (int rc = md_after_commit(c, iel)) return rc;
   // the walk's tables changed: a cw_graph-captured sweep stays valid (same
@@ -1483,7 +1529,7 @@ int vmc_sweep(cw_ctx *c) {
     stage_end(c);
     LCHK("k_decide");
     stage_begin(c, CW_ST_COMMIT);
-    k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+    launch_commit(c, i);
     stage_end(c);
     LCHK("k_commit");
     if (int rc = md_after_commit(c, i)) return rc;
@@ -1622,13 +1668,14 @@ int cw_opt_setup(cw_ctx *c, int ci, int njas, const double *jas_map, int with_ov
   BIND(c);
   drop_sweep_graph(c);  // the sweep gains or loses the derivative launches
   opt_reset(c);
-  if (!ci && njas == 0) return CW_OK;
+  const int norbt = (int)c->orb_ideriv.size() / 2;
+  if (!ci && njas == 0 && norbt == 0) return CW_OK;
   if (ci && !c->md_on) return fail(c, CW_ERR_UNSUPPORTED, "CI derivatives need a multideterminant expansion");
   if (c->h.nstates > 1) return fail(c, CW_ERR_UNSUPPORTED, "parameter derivatives of several states are not implemented");
   if (njas > 0 && (c->h.norda < 1 || c->h.nordb < 1))
     return fail(c, CW_ERR_UNSUPPORTED, "Jastrow derivatives need norda >= 1 and nordb >= 1 (Pade a(2), b(2))");
   if (c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
-  const int W = c->W, np = njas + (ci ? c->h.ndet : 0);
+  const int W = c->W, np = njas + (ci ? c->h.ndet : 0) + norbt;
   if (with_overlap && (size_t)np * np > ((size_t)1 << 27))
     return fail(c, CW_ERR_ARG, "overlap of %d parameters exceeds 2^27 entries", np);
   auto &L = c->opt_allocs;
@@ -1651,12 +1698,45 @@ int cw_opt_setup(cw_ctx *c, int ci, int njas, const double *jas_map, int with_ov
     CK(cudaMemcpyAsync(c->jas_map, jas_map, sizeof(double) * nraw * njas, cudaMemcpyHostToDevice, c->stream));
     c->jas_nraw = nraw;
   }
+  if (norbt > 0) {
+    // rotation targets jo (each once) and per term the slots of io
+    std::vector<int> vorb;
+    std::vector<OrbTerm> terms(norbt);
+    for (int t = 0; t < norbt; t++) {
+      const int io = c->orb_ideriv[2 * t] - 1, jo = c->orb_ideriv[2 * t + 1] - 1;
+      int v = -1;
+      for (size_t k = 0; k < vorb.size(); k++)
+        if (vorb[k] == jo) v = (int)k;
+      if (v < 0) {
+        v = (int)vorb.size();
+        vorb.push_back(jo);
+      }
+      terms[t].v = v;
+      for (int iab = 0; iab < 2; iab++) {
+        const int nel = iab == 0 ? c->h.nup : c->h.ndn, ish = iab == 0 ? 0 : c->h.nup;
+        terms[t].slot[iab] = -1;
+        for (int j = 0; j < nel; j++)
+          if (c->ref_orb[ish + j] == io) terms[t].slot[iab] = j;
+      }
+    }
+    c->orb_nv = (int)vorb.size();
+    DALLOC(L, c->orb_terms, terms.size());
+    DALLOC(L, c->orb_vorb, vorb.size());
+    DALLOC(L, c->orb_vals, (size_t)W * c->h.N * c->orb_nv);
+    CK(cudaMemcpyAsync(c->orb_terms, terms.data(), sizeof(OrbTerm) * terms.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->orb_vorb, vorb.data(), sizeof(int) * vorb.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->orb_on = true;
+  }
   c->opt_ci = ci != 0;
   c->opt_njas = njas;
   c->opt_np = np;
   c->opt_oo = with_overlap != 0;
   c->opt_w = W;
-  // derivatives at the current configurations (the last hpsi)
+  // derivatives at the current configurations (the last hpsi; with orbital
+  // rotations the hpsi is repeated once so that it keeps the targets' values)
+  if (c->orb_on)
+    if (int rc = run_hpsi(c, 0)) return rc;
   if (int rc = opt_derivs(c)) return rc;
   CK(cudaStreamSynchronize(c->stream));
   return CW_OK;
@@ -1684,6 +1764,31 @@ int cw_jas_o(cw_ctx *c, double *out) {
   if (c->opt_njas == 0 || c->opt_w != c->W)
     return fail(c, CW_ERR_STATE, "Jastrow derivatives not enabled for this population");
   return opt_columns(c, 0, c->opt_njas, out);
+}
+
+int cw_opt_orb(cw_ctx *c, int norbterm, const int32_t *ideriv) {
+  if (!c || norbterm < 0 || (norbterm > 0 && !ideriv)) return CW_ERR_ARG;
+  if (norbterm > 0) {
+    if (c->md_on)
+      return fail(c, CW_ERR_UNSUPPORTED,
+                  "orbital-rotation derivatives of multideterminant expansions are not implemented (one determinant)");
+    if (c->h.nstates > 1) return fail(c, CW_ERR_UNSUPPORTED, "orbital-rotation derivatives of several states");
+    for (int t = 0; t < norbterm; t++) {
+      const int io = ideriv[2 * t], jo = ideriv[2 * t + 1];
+      if (io < 1 || io > c->h.Oa || jo < 1 || jo > c->h.Oa || io == jo)
+        return fail(c, CW_ERR_ARG, "orbital rotation %d: (%d, %d) outside 1..%d or io == jo", t, io, jo, c->h.Oa);
+    }
+  }
+  c->orb_ideriv.assign(ideriv, ideriv + 2 * (size_t)norbterm);
+  return CW_OK;
+}
+
+int cw_orb_o(cw_ctx *c, double *out) {
+  if (!c || !out) return CW_ERR_ARG;
+  if (!c->orb_on || c->opt_w != c->W)
+    return fail(c, CW_ERR_STATE, "orbital-rotation derivatives not enabled for this population");
+  const int nt = (int)c->orb_ideriv.size() / 2;
+  return opt_columns(c, c->opt_np - nt, nt, out);
 }
 
 int cw_jas_raw(cw_ctx *c, double *out) {
@@ -2317,7 +2422,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       stage_end(c);
       LCHK("k_dmc_decide");
       stage_begin(c, CW_ST_COMMIT);
-      k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+      launch_commit(c, i);
       stage_end(c);
       LCHK("k_commit");
       if (int rc = md_after_commit(c, i)) return rc;
@@ -2362,7 +2467,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       stage_end(c);
       LCHK("k_tmove_accept");
       stage_begin(c, CW_ST_COMMIT);
-      k_commit<<<W, 128, 0, c->stream>>>(c->st, c->mb, c->g, -1);
+      launch_commit(c, -1);
       stage_end(c);
       LCHK("k_commit(tmove)");
     }

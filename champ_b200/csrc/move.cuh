@@ -844,37 +844,16 @@ __global__ void __launch_bounds__(128) k_decide(WState st, MoveBuf mb, GSys g, i
 // Commit of an accepted move: detsav (Sherman–Morrison, determinante :47-62)
 // and jassav.  CTA per walker; rejected walkers return at once.
 // ---------------------------------------------------------------------------
-__global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
-  const int w = blockIdx.x;
-  if (w >= st.W) return;
-  if (!mb.ms[w].acc) return;
-  if (iel < 0) iel = mb.ms[w].tel;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+// Orbital rows, e-n table row and the Jastrow pair tables of the moved
+// electron (the part of detsav / jassav after the inverse).
+__device__ __forceinline__ void commit_tables(WState &st, const MoveBuf &mb, const GSys &g, int w, int iel,
+                                              const double *s_orb) {
+  const int tid = threadIdx.x;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
   spin_of(iel, iab, nel, ish);
-  const int iloc = iel - ish;
-  __shared__ double s_orb[256];
-  __shared__ double s_col[256];
-  const double ratio = mb.ms[w].ratio;
-  double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
   const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
   const int *slot = g.slot_orb + iab * nmax;
-  for (int j = tid; j < nel; j += blockDim.x) {
-    s_orb[j] = orbn[slot[j]];
-    s_col[j] = sl[(size_t)nel * iloc + j];
-  }
-  __syncthreads();
-  // rows k != iloc: slmi(:,k) -= slmi(:,iloc) * (slmi(:,k)·orb_new)/ratio
-  for (int k = wid; k < nel; k += nwarp) {
-    if (k == iloc) continue;
-    double s = 0;
-    for (int j = lane; j < nel; j += 32) s += sl[(size_t)nel * k + j] * s_orb[j];
-    s = warp_sum(s) / ratio;
-    for (int j = lane; j < nel; j += 32) sl[(size_t)nel * k + j] = sl[(size_t)nel * k + j] - s_col[j] * s;
-  }
-  for (int j = tid; j < nel; j += blockDim.x) sl[(size_t)nel * iloc + j] = s_col[j] / ratio;
-  // orbital rows of the moved electron
   for (int j = tid; j < nel; j += blockDim.x) {
     st.orbs[((size_t)w * N + iel) * nmax + j] = s_orb[j];
     for (int k = 0; k < 3; k++)
@@ -909,6 +888,89 @@ __global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
       }
     }
   }
+}
+
+__global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  if (!mb.ms[w].acc) return;
+  if (iel < 0) iel = mb.ms[w].tel;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+  const int nmax = cs.nmax, Oa = cs.Oa;
+  int iab, nel, ish;
+  spin_of(iel, iab, nel, ish);
+  const int iloc = iel - ish;
+  __shared__ double s_orb[256];
+  __shared__ double s_col[256];
+  const double ratio = mb.ms[w].ratio;
+  double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
+  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const int *slot = g.slot_orb + iab * nmax;
+  for (int j = tid; j < nel; j += blockDim.x) {
+    s_orb[j] = orbn[slot[j]];
+    s_col[j] = sl[(size_t)nel * iloc + j];
+  }
+  __syncthreads();
+  // rows k != iloc: slmi(:,k) -= slmi(:,iloc) * (slmi(:,k)·orb_new)/ratio
+  for (int k = wid; k < nel; k += nwarp) {
+    if (k == iloc) continue;
+    double s = 0;
+    for (int j = lane; j < nel; j += 32) s += sl[(size_t)nel * k + j] * s_orb[j];
+    s = warp_sum(s) / ratio;
+    for (int j = lane; j < nel; j += 32) sl[(size_t)nel * k + j] = sl[(size_t)nel * k + j] - s_col[j] * s;
+  }
+  for (int j = tid; j < nel; j += blockDim.x) sl[(size_t)nel * iloc + j] = s_col[j] / ratio;
+  commit_tables(st, mb, g, w, iel, s_orb);
+}
+
+// The same commit with the spin's inverse staged in shared memory: every
+// load of the n x n block is issued at once (coalesced), the row factors
+// (slmi(:,k)·orb_new)/ratio come from shared memory, and the updated block
+// is written back coalesced, instead of one warp walking its rows one
+// dependent global round trip after another.  Row stride nel+1 (odd) keeps
+// the row-per-thread reads free of bank conflicts.  Dynamic shared memory:
+// nel*(nel+1) + 3*nel doubles.  Same arithmetic as k_commit.
+__global__ void k_commit_tile(WState st, MoveBuf mb, GSys g, int iel) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  if (!mb.ms[w].acc) return;
+  if (iel < 0) iel = mb.ms[w].tel;
+  const int tid = threadIdx.x;
+  const int nmax = cs.nmax, Oa = cs.Oa;
+  int iab, nel, ish;
+  spin_of(iel, iab, nel, ish);
+  const int iloc = iel - ish, ld = nel + 1;
+  extern __shared__ __align__(16) double sm[];
+  double *s_inv = sm;                        // [nel][ld]
+  double *s_orb = sm + (size_t)nel * ld;     // [nel]
+  double *s_col = s_orb + nel;               // [nel]
+  double *s_fac = s_col + nel;               // [nel]
+  const double ratio = mb.ms[w].ratio;
+  double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
+  const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
+  const int *slot = g.slot_orb + iab * nmax;
+  const int nn = nel * nel;
+  for (int t = tid; t < nn; t += blockDim.x) s_inv[(t / nel) * ld + (t % nel)] = sl[t];
+  for (int j = tid; j < nel; j += blockDim.x) s_orb[j] = orbn[slot[j]];
+  __syncthreads();
+  for (int j = tid; j < nel; j += blockDim.x) s_col[j] = s_inv[iloc * ld + j];
+  // two lanes per row, each summing alternate entries; the loop bound is the
+  // same for every thread of the block, so whole warps meet the shuffle
+  for (int base = 0; base < 2 * nel; base += blockDim.x) {
+    const int k2 = base + tid, k = k2 >> 1, h = k2 & 1;
+    const bool act = k2 < 2 * nel;
+    double s = 0;
+    if (act)
+      for (int j = h; j < nel; j += 2) s += s_inv[k * ld + j] * s_orb[j];
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    if (act && h == 0) s_fac[k] = s / ratio;
+  }
+  __syncthreads();
+  for (int t = tid; t < nn; t += blockDim.x) {
+    const int k = t / nel, j = t % nel;
+    sl[t] = (k == iloc) ? s_col[j] / ratio : s_inv[k * ld + j] - s_col[j] * s_fac[k];
+  }
+  commit_tables(st, mb, g, w, iel, s_orb);
 }
 
 }  // namespace cw

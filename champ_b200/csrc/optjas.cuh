@@ -213,3 +213,54 @@ __global__ void k_jas_o(int W, const double *raw, int nraw, const double *map, i
 }
 
 }  // namespace cw
+
+namespace cw {
+// ---------------------------------------------------------------------------
+// Orbital-rotation derivatives for a single determinant (optorb_deriv's
+// orbprim, vmc/optorb.f90:5-95, whose multideterminant terms vanish for one
+// determinant): for the variation phi_io -> phi_io + a phi_jo,
+// d ln psi / d a = sum over the spins whose determinant holds io of
+// aa(irep, jo) = sum_i slmi(irep + (i-1) nel) phi_jo(r_i)
+// (multideterminant_hpsi, vmc/multideterminant.f90:66-82).
+// ---------------------------------------------------------------------------
+struct OrbTerm {
+  int slot[2];  // slot of io in the up / down determinant (-1: io not there)
+  int v;        // index of jo in the list of rotation targets
+};
+
+// values of the rotation targets at the electrons [e0, e0+ne) of every
+// walker, from the value rows of the chunk's LCAO (rows ((w*ne + e)*5 + 0)):
+// vals [W][N][nv]
+__global__ void k_orb_vals(int W, int N, int e0, int ne, int Oa, const double *__restrict__ orball, int nv,
+                           const int *__restrict__ vorb, double *__restrict__ vals) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)W * ne * nv) return;
+  const int v = (int)(t % nv);
+  const long we = t / nv;
+  const int el = (int)(we % ne), w = (int)(we / ne);
+  vals[((size_t)w * N + e0 + el) * nv + v] = orball[(size_t)we * 5 * Oa + vorb[v]];
+}
+
+// thread per (walker, term): the derivative into the optimisation vector,
+// columns [off, off + nterm) of o [W][np] and ot [np][W]
+__global__ void k_orb_o(WState st, int nterm, const OrbTerm *__restrict__ terms, int nv,
+                        const double *__restrict__ vals, double *o, double *ot, int np, int off) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)st.W * nterm) return;
+  const int k = (int)(t % nterm), w = (int)(t / nterm);
+  const int N = cs.N, nmax = cs.nmax;
+  const OrbTerm tm = terms[k];
+  double sum = 0;
+  for (int iab = 0; iab < 2; iab++) {
+    const int irep = tm.slot[iab];
+    if (irep < 0) continue;
+    const int nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
+    const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
+    double a = 0;
+    for (int i = 0; i < nel; i++) a += sl[irep + (size_t)nel * i] * vals[((size_t)w * N + ish + i) * nv + tm.v];
+    sum += a;
+  }
+  o[(size_t)w * np + off + k] = sum;
+  ot[(size_t)(off + k) * st.W + w] = sum;
+}
+}  // namespace cw

@@ -229,7 +229,19 @@ class Engine:
         self._check(self.lib.cw_opt_setup(self.h, 1 if ci else 0, njas, dptr(m) if m is not None else None,
                                           1 if overlap else 0), "cw_opt_setup")
         self._opt_njas = njas
-        self._opt_np = njas + (self.system.iworbd.shape[0] if ci else 0)
+        self._opt_np = njas + (self.system.iworbd.shape[0] if ci else 0) + getattr(self, "_opt_norb", 0)
+
+    def opt_orb(self, ideriv):
+        """Orbital rotations (io, jo), 1-based, of the optimisation vector;
+        they join it at the next opt_setup (empty: none)."""
+        d = np.ascontiguousarray(np.asarray(ideriv, np.int32).reshape(-1, 2))
+        self._check(self.lib.cw_opt_orb(self.h, d.shape[0], d.ctypes.data_as(C.POINTER(C.c_int32))), "cw_opt_orb")
+        self._opt_norb = d.shape[0]
+
+    def orb_o(self):
+        out = np.zeros((self.W, getattr(self, "_opt_norb", 0)))
+        self._check(self.lib.cw_orb_o(self.h, dptr(out)), "cw_orb_o")
+        return out
 
     def jas_nraw(self) -> int:
         n = C.c_int(0)

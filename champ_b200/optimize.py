@@ -55,9 +55,11 @@ def sr_step(sums: dict, cdet: np.ndarray, energy: float, tau: float = 0.02, adia
 
 def sr_optimize(system, jd=None, ci: bool = False, nwalk: int = 256, iters: int = 5, nblock: int = 4,
                 nstep: int = 10, tau: float = 0.02, adiag: float = 0.01, precision: str = "fp64",
-                seed_offset: int = 0, engine_factory=None):
-    """SR optimisation loop over Jastrow (jasderiv selection `jd`) and, with
-    `ci`, CI parameters, as CHAMP's optwf driver runs it with method sr_n:
+                seed_offset: int = 0, engine_factory=None, orb=None):
+    """SR optimisation loop over Jastrow (jasderiv selection `jd`), with
+    `ci` CI parameters, and with `orb` (orbital pairs [n][2], 1-based, from
+    orbital_opt.orb_terms) orbital rotations, as CHAMP's optwf driver runs
+    it with method sr_n:
     per iteration nblock VMC blocks of nstep sweeps on the engine with the
     derivative sums on, one SR step over the joint vector (the reference CI
     coefficient held), new parameters (cusp-fixed e-e-n terms recomputed),
@@ -74,6 +76,8 @@ def sr_optimize(system, jd=None, ci: bool = False, nwalk: int = 256, iters: int 
         try:
             eng.set_walkers(x, rng)
             P = jastrow_opt.param_map(system, jd) if jd is not None and jd.nparmj else None
+            if orb is not None and len(orb):
+                eng.opt_orb(orb)
             eng.opt_setup(ci=ci, jas_map=P, overlap=True)
             for _ in range(nblock):
                 eng.vmc_steps(nstep)
@@ -88,8 +92,12 @@ def sr_optimize(system, jd=None, ci: bool = False, nwalk: int = 256, iters: int 
         dp = sr_delta(sums, float(r["energy"]), tau, adiag, fixed=nj if ci else None)
         if nj:
             system = jastrow_opt.apply_step(system, jd, dp[:nj])
+        nc = len(system.cdet) if ci else 0
         if ci:
             system = copy.copy(system)
-            system.cdet = np.array(system.cdet, float) + dp[nj:]
+            system.cdet = np.array(system.cdet, float) + dp[nj:nj + nc]
             system._keep = []
+        if orb is not None and len(orb):
+            from . import orbital_opt
+            system = orbital_opt.apply_step(system, orb, dp[nj + nc:])
     return system, history

@@ -211,11 +211,26 @@ int cw_ci_o(cw_ctx *ctx, double *out);
  * e-e-n terms -- and applies jas_map ([nraw][njas], row-major, built on the
  * host from the jasderiv selection) to it.  After every VMC sweep the sums
  * of cw_opt_sums run over the whole vector: o, eo [np], oo [np][np] (with
- * with_overlap), wsum; np = njas + (ci ? ndet : 0).  ci = 0 and njas = 0
- * disables.  Needs one state; Jastrow derivatives need norda, nordb >= 1.
+ * with_overlap), wsum; np = njas + (ci ? ndet : 0) + norbterm (cw_opt_orb).
+ * ci = 0, njas = 0 and no orbital rotations disables.  Needs one state; Jastrow derivatives need norda, nordb >= 1.
  * cw_jas_raw gives the raw derivatives of the last hpsi [nwalk][nraw],
  * cw_jas_o the Jastrow part of the vector [nwalk][njas]. */
 int cw_opt_setup(cw_ctx *ctx, int ci, int njas, const double *jas_map, int with_overlap);
+
+/* Orbital rotations of the optimisation vector (ioptorb, optorb_define
+ * vmc/optorb.f90:838-1030): ideriv [norbterm][2] holds 1-based orbital
+ * indices (io, jo) of the variations phi_io -> phi_io + a phi_jo (orbitals
+ * as rows of cw_system_desc.coef).  The next cw_opt_setup appends them to
+ * the vector after the Jastrow and CI parts, in optwf_store's order
+ * (vmc/optwf_handle_wf.f90:1517-1524); norbterm = 0 removes them.  The
+ * derivative of a walker is optorb_deriv's orbprim (vmc/optorb.f90:5-95)
+ * for one determinant: sum over the spins whose determinant holds io of
+ * aa(irep, jo) = sum_i slmi(irep + (i-1) nel) orb(i, jo).  One determinant
+ * and one state (CW_ERR_UNSUPPORTED otherwise: the multideterminant zmat
+ * terms are not built).  cw_orb_o gives the per-walker derivatives of the
+ * last hpsi, [nwalk][norbterm]. */
+int cw_opt_orb(cw_ctx *ctx, int norbterm, const int32_t *ideriv);
+int cw_orb_o(cw_ctx *ctx, double *out);
 int cw_opt_sums(cw_ctx *ctx, double *o, double *eo, double *oo, double *wsum);
 int cw_jas_nraw(cw_ctx *ctx, int *nraw);
 int cw_jas_raw(cw_ctx *ctx, double *out);

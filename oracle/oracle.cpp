@@ -2652,6 +2652,39 @@ void or_jas_raw(void *sys, const double *x, double *out) {
   w.jas_raw(out);
 }
 
+// Orbital-rotation derivatives of one configuration x[N][3] for a single
+// determinant: optorb_deriv's orbprim (vmc/optorb.f90:5-95) with the
+// multideterminant terms absent (ymat = zmat = 0 for one determinant), i.e.
+// for the variation phi_io -> phi_io + a phi_jo, d ln psi / d a =
+// sum over the spins whose reference determinant holds io of
+// aa(irep, jo) = sum_i slmi(irep + (i-1) nel) orb(i, jo)
+// (multideterminant_hpsi, vmc/multideterminant.f90:66-82), irep the slot of
+// io.  ideriv [nterm][2] holds 1-based (io, jo).  Returns 1 when the
+// Slater matrix is singular.
+int or_orb_o(void *sysp, const double *x, int nterm, const int *ideriv, double *out) {
+  const Sys *s = (const Sys *)sysp;
+  Walker w(s);
+  double psid, psij, ekin, e;
+  if (!w.hpsi(x, psid, psij, ekin, e)) return 1;
+  const int N = s->N;
+  for (int t = 0; t < nterm; t++) {
+    const int io = ideriv[2 * t] - 1, jo = ideriv[2 * t + 1] - 1;
+    double o = 0;
+    for (int iab = 0; iab < 2; iab++) {
+      const int nel = iab == 0 ? s->nup : s->ndn, ish = iab == 0 ? 0 : s->nup;
+      int irep = -1;
+      for (int j = 0; j < nel; j++)
+        if (s->iworbd[ish + j] - 1 == io) irep = j;
+      if (irep < 0) continue;
+      double a = 0;
+      for (int i = 0; i < nel; i++) a += w.slmi[iab][irep + nel * i] * w.orb[(ish + i) + N * jo];
+      o += a;
+    }
+    out[t] = o;
+  }
+  return 0;
+}
+
 void *or_sys_create(const cw_system_desc *d) {
   Sys *s = new Sys();
   s->N = d->nelec; s->nup = d->nup; s->ndn = d->nelec - d->nup;

@@ -150,6 +150,17 @@ class OracleSystem:
             raise RuntimeError("singular Slater matrix")
         return dict(energy=out[0], psid=out[1], psij=out[2], ekin=out[3], pe_local=out[4], vpsp=out[5])
 
+    def orb_o(self, x, ideriv):
+        """Orbital-rotation derivatives of one configuration for the 1-based
+        pairs ideriv [n][2] (one determinant)."""
+        L = lib()
+        L.or_orb_o.argtypes = [C.c_void_p, _dp, C.c_int, _i32, _dp]
+        d = np.ascontiguousarray(np.asarray(ideriv, np.int32).reshape(-1, 2))
+        out = np.zeros(d.shape[0])
+        if L.or_orb_o(self.h, dp(np.ascontiguousarray(x, float)), d.shape[0], d.ctypes.data_as(_i32), dp(out)):
+            raise RuntimeError("singular Slater matrix")
+        return out
+
     def sites(self, state):
         x = np.zeros((self.N, 3))
         st = np.ascontiguousarray(state, np.uint64).copy()

@@ -1,0 +1,81 @@
+"""GPU parity of the orbital-rotation derivatives (optorb_deriv for one
+determinant, vmc/optorb.f90:5-95) against the oracle, and of the SR sums
+over the joint [Jastrow | orbital] vector (optwf_store's sr_o layout,
+vmc/optwf_handle_wf.f90:1517-1524)."""
+import copy
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _with_virtuals(s, n, seed=5):
+    rng = np.random.default_rng(seed)
+    t = copy.deepcopy(s)
+    t.coef = np.vstack([np.asarray(s.coef, float), rng.normal(size=(n, s.coef.shape[1])) * 0.3])
+    t._keep = []
+    return t
+
+
+@pytest.mark.parametrize("config,W", [("tiny", 16), ("chain37", 8)])
+def test_orb_derivatives_and_sr_sums(oracle_mod, config, W):
+    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.jastrow_opt import default_jasderiv, param_map
+    from champ_b200.orbital_opt import orb_terms
+    from champ_b200.system import make_chain, make_synthetic
+    base = make_synthetic("tiny") if config == "tiny" else make_chain(37, 4037)
+    s = _with_virtuals(base, 4)
+    terms = orb_terms(s, nadorb=4)
+    rng = rng_states(W)
+    x = initial_configs(s, rng)
+    eng = Engine(s)
+    eng.set_walkers(x, rng)
+    o = oracle_mod.OracleSystem(s)
+    P = param_map(s, default_jasderiv(s))
+    eng.opt_orb(terms)
+    eng.opt_setup(jas_map=P, overlap=True)
+    nj = P.shape[1]
+    # derivatives at the start configurations
+    g = eng.orb_o()
+    ref = np.array([o.orb_o(x[w], terms) for w in range(W)])
+    assert rel_err(g, ref) < 1e-10
+    # the SR sums over three sweeps against the per-sweep vectors
+    so, seo, soo = 0, 0, 0
+    for _ in range(3):
+        eng.vmc_steps(1)
+        xw, _ = eng.walkers()
+        g = eng.orb_o()
+        ref = np.array([o.orb_o(xw[w], terms) for w in range(W)])
+        assert rel_err(g, ref) < 1e-10
+        vec = np.hstack([eng.jas_o(), g])
+        e = eng.state()[0]
+        so = so + vec.sum(0)
+        seo = seo + (e[:, None] * vec).sum(0)
+        soo = soo + vec.T @ vec
+    sums = eng.opt_sums(overlap=True)
+    assert sums["wsum"] == 3 * W
+    assert rel_err(sums["o"][nj:], so[nj:]) < 1e-10
+    assert rel_err(sums["eo"], seo) < 1e-10
+    assert rel_err(sums["oo"], soo) < 1e-10
+
+
+def test_opt_orb_refusals():
+    from champ_b200.engine import Engine, EngineError, initial_configs, rng_states
+    from champ_b200.system import make_synthetic, rotation_expansion
+    md, _ = rotation_expansion(make_synthetic("tiny"), [(0, 2, 3, 0.3)], extra_orbitals=2)
+    e = Engine(md)
+    with pytest.raises(EngineError, match="multideterminant"):
+        e.opt_orb([[1, 5]])
+    s = _with_virtuals(make_synthetic("tiny"), 2)
+    e = Engine(s)
+    with pytest.raises(EngineError, match="outside"):
+        e.opt_orb([[1, 9]])
+    with pytest.raises(EngineError, match="outside"):
+        e.opt_orb([[2, 2]])
+    rng = rng_states(4)
+    e.set_walkers(initial_configs(s, rng), rng)
+    with pytest.raises(EngineError, match="not enabled"):
+        e.orb_o()
