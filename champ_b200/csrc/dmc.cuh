@@ -1,6 +1,8 @@
 // dmc.cuh — diffusion Monte Carlo step of every walker: dmc_ps
-// (dmc/dmc_ps_mov1.f90:4) with the reweighting of dmc/branching.f90 (icut_e=0,
-// icut_br=0: the ECP branch of dmc_eloc_cutoff, fratio-scaled energies).
+// (dmc/dmc_ps_mov1.f90:4) for pseudopotential wave functions and dmc_ae
+// (dmc/dmc_ae_mov1.f90:4) for all-electron ones, with the reweighting of
+// dmc/branching.f90 (icut_e=0, icut_br=0, fratio-scaled energies; the
+// dmc_eloc_cutoff branch of each).
 //
 //   k_dmc_propose   drift-diffusion proposal of electron iel (:293-318)
 //   (k_jastrow_move, k_basis_move, LCAO GEMM and k_commit are shared with VMC)
@@ -29,7 +31,7 @@ struct DmcBuf {
 // per-walker sums of one step (reduced on the host in walker order)
 enum {
   DA_DFUS2AC = 0, DA_DFUS2UN, DA_DFUS2O, DA_IACCEPT, DA_ACC, DA_TRY, DA_NACC, DA_NODECR,
-  DA_WSUM1, DA_ESUM1, DA_PESUM, DA_TPBSUM, DA_TAUSUM, DA_TMOVE, DA_NA = 16
+  DA_WSUM1, DA_ESUM1, DA_PESUM, DA_TPBSUM, DA_TAUSUM, DA_TMOVE, DA_FNORMO, DA_NA = 16
 };
 
 struct DmcScalars {
@@ -63,7 +65,88 @@ __device__ __forceinline__ void drift_old(const WState &st, int w, int e, double
   v[2] = (md_vel ? md_vel[2] : 0.0) + g2 + fjo[2 * N + e];
 }
 
-// thread per walker: drift + Gaussian diffusion of electron iel
+// nearest centre of a point: first minimum of the squared distance
+__device__ __forceinline__ int nearest_centre_d(const double x[3]) {
+  double best = 1.0e100;
+  int iw = 0;
+  for (int ic = 0; ic < cs.M; ic++) {
+    const double d0 = x[0] - cs.cent[3 * ic], d1 = x[1] - cs.cent[3 * ic + 1], d2 = x[2] - cs.cent[3 * ic + 2];
+    const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+    if (r2 < best) {
+      best = r2;
+      iw = ic;
+    }
+  }
+  return iw;
+}
+
+// All-electron moves (dmc_ae, dmc/dmc_ae_mov1.f90:227-303 forward,
+// :396-474 reverse): the drifted point of an electron at x with drift v in
+// the frame of its nearest nucleus (z along the electron, x along the
+// angular part of the drift), with the nucleus-dependent adrift, and the
+// probability qgaus of sampling the exponential around the nucleus instead
+// of the Gaussian around the drifted point.
+struct AeFrame {
+  int ic;
+  double zeta, qgaus, pgaus, xd[3];
+};
+__device__ __forceinline__ AeFrame ae_frame_d(const double x[3], const double v[3], double tau) {
+  const double one = 1, two = 2, half = 0.5, eps = 1.0e-10, adrift0 = 0.1;
+  AeFrame f;
+  f.ic = nearest_centre_d(x);
+  const double c[3] = {cs.cent[3 * f.ic], cs.cent[3 * f.ic + 1], cs.cent[3 * f.ic + 2]};
+  const double z = cs.znuc[cs.iwctype[f.ic]];
+  double rv[3], rmin = 0, vr = 0, v2 = 0;
+  for (int k = 0; k < 3; k++) {
+    rv[k] = x[k] - c[k];
+    rmin += rv[k] * rv[k];
+    vr += v[k] * rv[k];
+    v2 += v[k] * v[k];
+  }
+  rmin = sqrt(rmin);
+  vr = vr / rmin;
+  const double va = sqrt(v2);
+  f.zeta = sqrt(one / tau + z * z);
+  double zaxis[3], xaxis[3], vp = 0;
+  for (int k = 0; k < 3; k++) {
+    zaxis[k] = rv[k] / rmin;
+    xaxis[k] = v[k] - vr * zaxis[k];
+    vp += xaxis[k] * xaxis[k];
+  }
+  vp = sqrt(vp);
+  if (vp < eps) {
+    xaxis[0] = eps * (one - zaxis[0] * zaxis[0]);
+    xaxis[1] = eps * (-zaxis[0] * zaxis[1]);
+    xaxis[2] = eps * (-zaxis[0] * zaxis[2]);
+    vp = eps * sqrt(one + eps - zaxis[0] * zaxis[0]);
+  }
+  for (int k = 0; k < 3; k++) xaxis[k] = xaxis[k] / vp;
+  const double hafzr2 = (half * z * rmin) * (half * z * rmin);
+  const double adrift = (half * (1 + eps + vr / va)) + adrift0 * hafzr2 / (1 + hafzr2);
+  const double vavvt = (sqrt(one + two * adrift * v2 * tau) - one) / (adrift * v2);
+  const double rtry = rmin + vavvt * vr;
+  if (rtry > 0) {
+    f.qgaus = half * erfc(rtry / sqrt(two * tau));
+    const double xprime = vavvt * vp * rtry / (half * (rmin + rtry));
+    for (int k = 0; k < 3; k++) f.xd[k] = c[k] + xaxis[k] * xprime + zaxis[k] * rtry;
+  } else {
+    f.qgaus = half * (one + erf(-rtry / sqrt(two * tau)));
+    for (int k = 0; k < 3; k++) f.xd[k] = c[k];
+  }
+  f.pgaus = one - f.qgaus;
+  return f;
+}
+
+// (sqrt(2 pi tau))^3 / pi of dmc_ae's exponential density (dmc_ae :148)
+__device__ __forceinline__ double ae_term(double tau) {
+  const double pi = 3.141592653589793115997963468544185161590576171875;
+  const double r = sqrt(2.0 * pi * tau);
+  return r * r * r / pi;
+}
+
+// thread per walker: drift + diffusion of electron iel (dmc_ps's Gaussian
+// around the drifted point; dmc_ae's Gaussian / exponential mixture for an
+// all-electron wave function)
 __global__ void k_dmc_propose(WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, int iel) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
@@ -72,22 +155,54 @@ __global__ void k_dmc_propose(WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, i
   drift_old(st, w, iel, vo, mb.md_velo ? mb.md_velo + 3 * w : nullptr);
   for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + iel] = vo[k];
   const double tau = sc.tau, rttau = sqrt(tau), adrift = 0.5;
-  const double v2old = vo[0] * vo[0] + vo[1] * vo[1] + vo[2] * vo[2];
-  const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2old * tau) - 1.0) / (adrift * v2old);
   DRng rng;
   rng.load(st.rng + 4 * (size_t)w);
-  double dfus2o = 0;
+  double dfus2o = 0, fnormo = 1.0;
   MoveScratch &m = mb.ms[w];
-  for (int k = 0; k < 3; k++) {
-    const double drift = vavvt * vo[k];
-    const double dfus = gauss_d(rng) * rttau;
-    const double dx = drift + dfus;
-    dfus2o += dfus * dfus;
-    m.xnew[k] = st.x[((size_t)w * 3 + k) * N + iel] + dx;
+  if (cs.nloc == 0) {
+    const double xo[3] = {st.x[((size_t)w * 3 + 0) * N + iel], st.x[((size_t)w * 3 + 1) * N + iel],
+                          st.x[((size_t)w * 3 + 2) * N + iel]};
+    const AeFrame f = ae_frame_d(xo, vo, tau);
+    const double c[3] = {cs.cent[3 * f.ic], cs.cent[3 * f.ic + 1], cs.cent[3 * f.ic + 2]};
+    double xn[3] = {f.xd[0], f.xd[1], f.xd[2]}, dfusb;
+    if (rng.uniform() < f.pgaus) {
+      double dfus2b = 0;
+      for (int k = 0; k < 3; k++) {
+        const double dfus = gauss_d(rng) * rttau;
+        dfus2o += dfus * dfus;
+        xn[k] = xn[k] + dfus;
+        dfus2b += (xn[k] - c[k]) * (xn[k] - c[k]);
+      }
+      dfusb = sqrt(dfus2b);
+    } else {
+      const double u1 = rng.uniform(), u2 = rng.uniform(), u3 = rng.uniform();
+      dfusb = (-0.5 / f.zeta) * log(u1 * u2 * u3);
+      const double costht = 2.0 * (rng.uniform() - 0.5);
+      const double sintht = sqrt(1.0 - costht * costht);
+      const double phi = 2.0 * 3.141592653589793115997963468544185161590576171875 * rng.uniform();
+      for (int k = 0; k < 3; k++) {
+        const double dfus = k == 0 ? dfusb * sintht * cos(phi) : k == 1 ? dfusb * sintht * sin(phi) : dfusb * costht;
+        dfus2o += (c[k] + dfus - xn[k]) * (c[k] + dfus - xn[k]);
+        xn[k] = c[k] + dfus;
+      }
+    }
+    fnormo = f.pgaus + f.qgaus * ae_term(tau) * f.zeta * f.zeta * f.zeta * exp(-2.0 * f.zeta * dfusb + 0.5 * dfus2o / tau);
+    for (int k = 0; k < 3; k++) m.xnew[k] = xn[k];
+  } else {
+    const double v2old = vo[0] * vo[0] + vo[1] * vo[1] + vo[2] * vo[2];
+    const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2old * tau) - 1.0) / (adrift * v2old);
+    for (int k = 0; k < 3; k++) {
+      const double drift = vavvt * vo[k];
+      const double dfus = gauss_d(rng) * rttau;
+      const double dx = drift + dfus;
+      dfus2o += dfus * dfus;
+      m.xnew[k] = st.x[((size_t)w * 3 + k) * N + iel] + dx;
+    }
   }
   rng.store(st.rng + 4 * (size_t)w);
   m.igeo = 0;
   db.acc[(size_t)w * DA_NA + DA_DFUS2O] = dfus2o;
+  db.acc[(size_t)w * DA_NA + DA_FNORMO] = fnormo;
 }
 
 // thread per walker: ratio and drift at the new point, reverse diffusion,
@@ -124,16 +239,31 @@ __global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalar
   }
   const double psido = st.psido[w], psijo = st.psijo[w];
   if (psidn * psido <= 0.0) acc[DA_NODECR] += 1;  // icross=1: counted, the move is not refused
-  const double v2new = vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2];
-  const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2new * tau) - 1.0) / (adrift * v2new);
-  double dfus2n = 0;
-  for (int k = 0; k < 3; k++) {
-    const double xbac = m.xnew[k] + vavvt * vn[k];
-    const double dfus = xbac - st.x[((size_t)w * 3 + k) * N + iel];
-    dfus2n += dfus * dfus;
+  double dfus2n = 0, fnormn = 1.0;
+  if (cs.nloc == 0) {
+    // dmc_ae's reverse move: the drifted point of the new position and the
+    // density of returning to the old one
+    const AeFrame f = ae_frame_d(m.xnew, vn, tau);
+    double dfus2b = 0;
+    for (int k = 0; k < 3; k++) {
+      const double xo = st.x[((size_t)w * 3 + k) * N + iel], c = cs.cent[3 * f.ic + k];
+      dfus2b += (c - xo) * (c - xo);
+      dfus2n += (f.xd[k] - xo) * (f.xd[k] - xo);
+    }
+    const double dfusb = sqrt(dfus2b);
+    fnormn = f.pgaus + f.qgaus * ae_term(tau) * f.zeta * f.zeta * f.zeta * exp(-2.0 * f.zeta * dfusb + 0.5 * dfus2n / tau);
+  } else {
+    const double v2new = vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2];
+    const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2new * tau) - 1.0) / (adrift * v2new);
+    for (int k = 0; k < 3; k++) {
+      const double xbac = m.xnew[k] + vavvt * vn[k];
+      const double dfus = xbac - st.x[((size_t)w * 3 + k) * N + iel];
+      dfus2n += dfus * dfus;
+    }
   }
   const double dfus2o = acc[DA_DFUS2O];
-  double p = (psidn / psido) * (psidn / psido) * exp(2 * (psijn - psijo)) * exp((dfus2o - dfus2n) / (2.0 * tau)) * 1.0;
+  double p = (psidn / psido) * (psidn / psido) * exp(2 * (psijn - psijo)) * exp((dfus2o - dfus2n) / (2.0 * tau)) *
+             fnormn / acc[DA_FNORMO];
   const int age = db.iage[w];
   if (age > 50) p = p * pow(1.1, (double)(age - 50));
   p = fmin(1.0, p);
@@ -174,7 +304,28 @@ __global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode, con
     drift_old(st, w, e, v, md_vall ? md_vall + ((size_t)w * N + e) * 3 : nullptr);
     for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + e] = v[k];
     const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-    const double vavvt = (sqrt(1.0 + 2.0 * adrift * v2 * tau * 1.0) - 1.0) / (adrift * v2);
+    double vavvt;
+    if (cs.nloc == 0) {
+      // all-electron branch: adrift of the electron's nearest nucleus, with
+      // dmc_ae's adrift0 = 0.1
+      const double x[3] = {st.x[((size_t)w * 3 + 0) * N + e], st.x[((size_t)w * 3 + 1) * N + e],
+                           st.x[((size_t)w * 3 + 2) * N + e]};
+      const int ic = nearest_centre_d(x);
+      double rmin = 0, vr = 0;
+      for (int k = 0; k < 3; k++) {
+        const double rv = x[k] - cs.cent[3 * ic + k];
+        rmin += rv * rv;
+        vr += v[k] * rv;
+      }
+      rmin = sqrt(rmin);
+      vr = vr / rmin;
+      const double va = sqrt(v2), z = cs.znuc[cs.iwctype[ic]];
+      const double hafzr2 = (0.5 * z * rmin) * (0.5 * z * rmin);
+      const double adriftn = (0.5 * (1 + 1.0e-10 + vr / va)) + 0.1 * hafzr2 / (1 + hafzr2);
+      vavvt = (sqrt(1.0 + 2.0 * adriftn * v2 * tau) - 1.0) / (adriftn * v2);
+    } else {
+      vavvt = (sqrt(1.0 + 2.0 * adrift * v2 * tau * 1.0) - 1.0) / (adrift * v2);
+    }
     const double vavvn = vavvt / (tau * 1.0);
     vav2sum += vavvn * vavvn * v2;
     v2sum += v2;

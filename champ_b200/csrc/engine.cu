@@ -68,6 +68,7 @@ struct cw_ctx {
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
   size_t smem_commit = 0;  // k_commit_tile's dynamic shared memory (0: the untiled k_commit)
+  int *acc_list = nullptr, *acc_count = nullptr;  // accepted walkers of a move (k_accept_list)
   int ecp_warps = 1, ecp_naov = 0, ecp_minb = 1;
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
   std::unordered_map<void *, size_t> alloc_bytes;
@@ -370,10 +371,14 @@ int set_attrs(cw_ctx *c) {
 
 // detsav + jassav of the accepted walkers (iel < 0: each walker's T-move electron)
 void launch_commit(cw_ctx *c, int iel) {
-  if (c->smem_commit)
-    k_commit_tile<<<c->W, 128, c->smem_commit, c->stream>>>(c->st, c->mb, c->g, iel);
-  else
+  if (c->smem_commit) {
+    // the accepted walkers in order, then a fixed grid of blocks over them
+    k_accept_list<<<1, 1024, 0, c->stream>>>(c->mb.ms, c->W, c->acc_list, c->acc_count);
+    const int grid = std::max(1, std::min(c->W, 148 * 8));
+    k_commit_tile<<<grid, 128, c->smem_commit, c->stream>>>(c->st, c->mb, c->g, iel, c->acc_list, c->acc_count);
+  } else {
     k_commit<<<c->W, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel);
+  }
 }
 
 #define NORD_DISPATCH(fn, ...)            \
@@ -917,6 +922,8 @@ int alloc_walkers(cw_ctx *c, int W) {
   DALLOC(L, b.entab, (size_t)W * M * N * kEnFields);
   b.entabf = nullptr;
   if (c->mixed) DALLOC(L, b.entabf, (size_t)W * M * N * kEnFields);
+  DALLOC(L, c->acc_list, W);
+  DALLOC(L, c->acc_count, 1);
   DALLOC(L, c->hook_buf, (size_t)W * 6);
   DALLOC(L, c->hook_acc, W);
   c->hook_psie_iel = c->hook_md_iel = -1;
@@ -2253,8 +2260,6 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
                            const uint64_t *pop_rng, double tau, double etrial, int nfprod) {
   if (!c || nwalk <= 0 || mwalk < nwalk || !x || !rng || !pop_rng || !(tau > 0) || nfprod < 1)
     return fail(c, CW_ERR_ARG, "cw_dmc_init: bad arguments");
-  if (c->h.nloc == 0)
-    return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: all-electron DMC (dmc_ae) is not implemented; nloc > 0 required");
   if (c->h.nstates > 1)
     return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: several states are a VMC feature (dmc_ps samples one state)");
   BIND(c);

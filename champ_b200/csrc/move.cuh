@@ -923,18 +923,40 @@ __global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
   commit_tables(st, mb, g, w, iel, s_orb);
 }
 
+// The accepted walkers of a move, in walker order: list [W], *count.  One
+// block: each thread counts a contiguous run of walkers, a block scan gives
+// the runs' offsets.
+__global__ void __launch_bounds__(1024) k_accept_list(const MoveScratch *__restrict__ ms, int W, int *list,
+                                                      int *count) {
+  __shared__ int scan[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int per = (W + nt - 1) / nt, w0 = t * per, w1 = min(W, w0 + per);
+  int n = 0;
+  for (int w = w0; w < w1; w++) n += ms[w].acc != 0;
+  scan[t] = n;
+  __syncthreads();
+  for (int off = 1; off < nt; off <<= 1) {
+    const int v = t >= off ? scan[t - off] : 0;
+    __syncthreads();
+    scan[t] += v;
+    __syncthreads();
+  }
+  int pos = scan[t] - n;
+  for (int w = w0; w < w1; w++)
+    if (ms[w].acc) list[pos++] = w;
+  if (t == nt - 1) *count = scan[t];
+}
+
 // The same commit with the spin's inverse staged in shared memory: every
 // load of the n x n block is issued at once (coalesced), the row factors
 // (slmi(:,k)·orb_new)/ratio come from shared memory, and the updated block
 // is written back coalesced, instead of one warp walking its rows one
 // dependent global round trip after another.  Row stride nel+1 (odd) keeps
 // the row-per-thread reads free of bank conflicts.  Dynamic shared memory:
-// nel*(nel+1) + 3*nel doubles.  Same arithmetic as k_commit.
-__global__ void k_commit_tile(WState st, MoveBuf mb, GSys g, int iel) {
-  const int w = blockIdx.x;
-  if (w >= st.W) return;
-  if (!mb.ms[w].acc) return;
-  if (iel < 0) iel = mb.ms[w].tel;
+// nel*(nel+1) + 3*nel doubles.  Same arithmetic as k_commit.  The blocks
+// loop over the list of accepted walkers (k_accept_list), so no block is
+// spent on a rejected move.
+__device__ __forceinline__ void commit_tile_walker(WState &st, const MoveBuf &mb, const GSys &g, int w, int iel) {
   const int tid = threadIdx.x;
   const int nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
@@ -971,6 +993,15 @@ __global__ void k_commit_tile(WState st, MoveBuf mb, GSys g, int iel) {
     sl[t] = (k == iloc) ? s_col[j] / ratio : s_inv[k * ld + j] - s_col[j] * s_fac[k];
   }
   commit_tables(st, mb, g, w, iel, s_orb);
+}
+
+__global__ void k_commit_tile(WState st, MoveBuf mb, GSys g, int iel_arg, const int *__restrict__ list,
+                              const int *__restrict__ count) {
+  const int nacc = *count;
+  for (int q = blockIdx.x; q < nacc; q += gridDim.x) {
+    commit_tile_walker(st, mb, g, list[q], iel_arg < 0 ? mb.ms[list[q]].tel : iel_arg);
+    __syncthreads();  // the next walker reuses the shared memory
+  }
 }
 
 }  // namespace cw

@@ -355,7 +355,9 @@ int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
 int cw_orbitals_noalloc(cw_ctx *ctx, int npts, const double *xyz, double *out);
 
 /* ------------------------------------------------------------------------ */
-/* Diffusion Monte Carlo (idmc=2, nloc>0: dmc/dmc.f90:88-111)                */
+/* Diffusion Monte Carlo (idmc=2: dmc/dmc.f90:88-111); dmc_ps moves for      */
+/* pseudopotential wave functions (nloc > 0), dmc_ae moves for all-electron  */
+/* ones (nloc = 0, dmc/dmc_ae_mov1.f90:4)                                    */
 /* ------------------------------------------------------------------------ */
 
 /* Start a DMC population of nwalk walkers (capacity mwalk = CHAMP's MWALK)
@@ -370,10 +372,13 @@ int cw_dmc_init(cw_ctx *ctx, int nwalk, int mwalk, const double *x, const uint64
                 const uint64_t *pop_rng, double tau, double etrial, int nfprod);
 
 /* `nstep` DMC steps of the population, the body of dmc.f90's j loop:
- * rotqua (dmc.f90:94, one rotation for all walkers), dmc_ps
- * (dmc/dmc_ps_mov1.f90:4: per electron drift-diffusion move with the
- * Green-function acceptance; hpsi; fratio and reweighting,
- * dmc/branching.f90:27,111; population factor fprod), splitj
+ * rotqua (dmc.f90:94, one rotation for all walkers, only with a
+ * pseudopotential), dmc_ps (dmc/dmc_ps_mov1.f90:4) or, for an all-electron
+ * wave function, dmc_ae (dmc/dmc_ae_mov1.f90:4: the drift in the frame of
+ * the nearest nucleus and a Gaussian / exponential diffusion mixture) --
+ * per electron the drift-diffusion move with the Green-function
+ * acceptance; hpsi; fratio and reweighting, dmc/branching.f90:27,111;
+ * population factor fprod -- then splitj
  * (dmc/splitj.f90:3) and acues1 (dmc/acues1.f90:3).  The population size
  * changes; CW_ERR_STATE if it would exceed mwalk ("SPLITJ: MWALK exceeded"). */
 int cw_dmc_steps(cw_ctx *ctx, int nstep);

@@ -2323,19 +2323,115 @@ void vold_all(Walker &w) {
   for (int i = 0; i < w.N; i++) w.grad(i, 1, &w.vold[3 * i]);
 }
 
-// dmc_eloc_cutoff, nloc>0 branch (dmc/branching.f90:221-241) -> fratio (icut_e=0)
+// nearest centre of a point: first minimum of the squared distance
+int nearest_centre(const Sys *s, const double *x) {
+  double best = 1.0e100;
+  int iw = 0;
+  for (int ic = 0; ic < s->M; ic++) {
+    const double d0 = x[0] - s->cent[3 * ic], d1 = x[1] - s->cent[3 * ic + 1], d2 = x[2] - s->cent[3 * ic + 2];
+    const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+    if (r2 < best) {
+      best = r2;
+      iw = ic;
+    }
+  }
+  return iw;
+}
+
+// dmc_eloc_cutoff (dmc/branching.f90:201-275) -> fratio (icut_e=0).
+// Pseudopotential runs (dmc_ps passes adrift = 0.5): the plain averaged
+// drift; all-electron runs (dmc_ae passes adrift0 = 0.1): the drift of each
+// electron with the adrift of its nearest nucleus.
 double fratio_of(const Walker &w, double tau, double tratio) {
-  const double adrift = 0.5;
+  const Sys *s = w.s;
   double vav2sum = 0, v2sum = 0;
   for (int i = 0; i < w.N; i++) {
     const double *v = &w.vold[3 * i];
     double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-    double vavvt = (std::sqrt(1.0 + 2.0 * adrift * v2 * tau * tratio) - 1.0) / (adrift * v2);
-    double vavvn = vavvt / (tau * tratio);
-    vav2sum += vavvn * vavvn * v2;
+    if (s->nloc > 0) {
+      const double adrift = 0.5;
+      double vavvt = (std::sqrt(1.0 + 2.0 * adrift * v2 * tau * tratio) - 1.0) / (adrift * v2);
+      double vavvn = vavvt / (tau * tratio);
+      vav2sum += vavvn * vavvn * v2;
+    } else {
+      const double adrift = 0.1, half = 0.5, eps = 1.0e-10;
+      const double *x = &w.xold[3 * i];
+      const int ic = nearest_centre(s, x);
+      double rmin = 0, vr = 0;
+      for (int k = 0; k < 3; k++) {
+        const double rv = x[k] - s->cent[3 * ic + k];
+        rmin += rv * rv;
+        vr += v[k] * rv;
+      }
+      rmin = std::sqrt(rmin);
+      vr = vr / rmin;
+      const double va = std::sqrt(v2);
+      const double hafzr2 = (half * s->znuc[s->iwctype[ic]] * rmin) * (half * s->znuc[s->iwctype[ic]] * rmin);
+      const double adriftn = (half * (1 + eps + vr / va)) + adrift * hafzr2 / (1 + hafzr2);
+      const double vavvt = (std::sqrt(1.0 + 2.0 * adriftn * v2 * tau) - 1.0) / (adriftn * v2);
+      const double vavvn = vavvt / (tau * tratio);
+      vav2sum += vavvn * vavvn * v2;
+    }
     v2sum += v2;
   }
   return std::sqrt(vav2sum / v2sum);
+}
+
+// The drifted point of dmc_ae's move for an electron at x with drift v
+// (dmc/dmc_ae_mov1.f90:227-303 forward, :396-474 reverse): the local frame
+// of the nearest nucleus (z along the electron, x along the angular part
+// of the drift), the UNR93 drift with the nucleus-dependent adrift, and the
+// probability qgaus of sampling the exponential around the nucleus instead
+// of the Gaussian around the drifted point.
+struct AeFrame {
+  int ic;
+  double zeta, qgaus, pgaus, xd[3];
+};
+AeFrame ae_frame(const Sys *s, const double *x, const double *v, double tau) {
+  const double one = 1, two = 2, half = 0.5, eps = 1.0e-10, adrift0 = 0.1;
+  AeFrame f;
+  f.ic = nearest_centre(s, x);
+  const double *c = &s->cent[3 * f.ic];
+  const double z = s->znuc[s->iwctype[f.ic]];
+  double rv[3], rmin = 0, vr = 0, v2 = 0;
+  for (int k = 0; k < 3; k++) {
+    rv[k] = x[k] - c[k];
+    rmin += rv[k] * rv[k];
+    vr += v[k] * rv[k];
+    v2 += v[k] * v[k];
+  }
+  rmin = std::sqrt(rmin);
+  vr = vr / rmin;
+  const double va = std::sqrt(v2);
+  f.zeta = std::sqrt(one / tau + z * z);
+  double zaxis[3], xaxis[3], vp = 0;
+  for (int k = 0; k < 3; k++) {
+    zaxis[k] = rv[k] / rmin;
+    xaxis[k] = v[k] - vr * zaxis[k];
+    vp += xaxis[k] * xaxis[k];
+  }
+  vp = std::sqrt(vp);
+  if (vp < eps) {
+    xaxis[0] = eps * (one - zaxis[0] * zaxis[0]);
+    xaxis[1] = eps * (-zaxis[0] * zaxis[1]);
+    xaxis[2] = eps * (-zaxis[0] * zaxis[2]);
+    vp = eps * std::sqrt(one + eps - zaxis[0] * zaxis[0]);
+  }
+  for (int k = 0; k < 3; k++) xaxis[k] = xaxis[k] / vp;
+  const double hafzr2 = (half * z * rmin) * (half * z * rmin);
+  const double adrift = (half * (1 + eps + vr / va)) + adrift0 * hafzr2 / (1 + hafzr2);
+  const double vavvt = (std::sqrt(one + two * adrift * v2 * tau) - one) / (adrift * v2);
+  const double rtry = rmin + vavvt * vr;
+  if (rtry > 0) {
+    f.qgaus = half * std::erfc(rtry / std::sqrt(two * tau));
+    const double xprime = vavvt * vp * rtry / (half * (rmin + rtry));
+    for (int k = 0; k < 3; k++) f.xd[k] = c[k] + xaxis[k] * xprime + zaxis[k] * rtry;
+  } else {
+    f.qgaus = half * (one + std::erf(-rtry / std::sqrt(two * tau)));
+    for (int k = 0; k < 3; k++) f.xd[k] = c[k];
+  }
+  f.pgaus = one - f.qgaus;
+  return f;
 }
 
 // one walker of dmc_ps: electron moves, hpsi, weight; returns false if singular
@@ -2346,18 +2442,53 @@ bool dmc_walker(DmcPop &P, int iw, double ffi, double &wsum1, double &esum1, dou
   const double tau = P.prm.tau, rttau = std::sqrt(tau), adrift = 0.5, one = 1, two = 2, zero = 0;
   double dfus2ac = 0, dfus2un = 0, drifdif = 0, pp = 1;
   int iaccept = 0;
+  const bool ae = s->nloc == 0;
+  const double term = std::pow(std::sqrt(two * PI * tau), 3) / PI;  // dmc_ae :148
   for (int i = 0; i < w.N; i++) {
     double *vo = &w.vold[3 * i];
     w.grad(i, 1, vo);
-    double v2old = vo[0] * vo[0] + vo[1] * vo[1] + vo[2] * vo[2];
-    double vavvt = (std::sqrt(one + two * adrift * v2old * tau) - one) / (adrift * v2old);
-    double dfus2o = zero, xnew[3];
-    for (int k = 0; k < 3; k++) {
-      double drift = vavvt * vo[k];
-      double dfus = gauss_draw(w.rng) * rttau;
-      double dx = drift + dfus;
-      dfus2o += dfus * dfus;
-      xnew[k] = w.xold[k + 3 * i] + dx;
+    double dfus2o = zero, xnew[3], fnormo = one;
+    const double *xo = &w.xold[3 * i];
+    if (ae) {
+      // dmc_ae (dmc/dmc_ae_mov1.f90:227-356): drift in the nucleus frame,
+      // then a Gaussian around the drifted point with probability pgaus or
+      // an exponential around the nucleus
+      const AeFrame f = ae_frame(s, xo, vo, tau);
+      const double *c = &s->cent[3 * f.ic];
+      for (int k = 0; k < 3; k++) xnew[k] = f.xd[k];
+      double dfusb;
+      if (w.rng.uniform() < f.pgaus) {
+        double dfus2b = zero;
+        for (int k = 0; k < 3; k++) {
+          double dfus = gauss_draw(w.rng) * rttau;
+          dfus2o += dfus * dfus;
+          xnew[k] = xnew[k] + dfus;
+          dfus2b += (xnew[k] - c[k]) * (xnew[k] - c[k]);
+        }
+        dfusb = std::sqrt(dfus2b);
+      } else {
+        const double u1 = w.rng.uniform(), u2 = w.rng.uniform(), u3 = w.rng.uniform();
+        dfusb = (-0.5 / f.zeta) * std::log(u1 * u2 * u3);
+        const double costht = two * (w.rng.uniform() - 0.5);
+        const double sintht = std::sqrt(one - costht * costht);
+        const double phi = two * PI * w.rng.uniform();
+        for (int k = 0; k < 3; k++) {
+          const double dfus = k == 0 ? dfusb * sintht * std::cos(phi) : k == 1 ? dfusb * sintht * std::sin(phi) : dfusb * costht;
+          dfus2o += (c[k] + dfus - xnew[k]) * (c[k] + dfus - xnew[k]);
+          xnew[k] = c[k] + dfus;
+        }
+      }
+      fnormo = f.pgaus + f.qgaus * term * f.zeta * f.zeta * f.zeta * std::exp(-two * f.zeta * dfusb + 0.5 * dfus2o / tau);
+    } else {
+      double v2old = vo[0] * vo[0] + vo[1] * vo[1] + vo[2] * vo[2];
+      double vavvt = (std::sqrt(one + two * adrift * v2old * tau) - one) / (adrift * v2old);
+      for (int k = 0; k < 3; k++) {
+        double drift = vavvt * vo[k];
+        double dfus = gauss_draw(w.rng) * rttau;
+        double dx = drift + dfus;
+        dfus2o += dfus * dfus;
+        xnew[k] = xo[k] + dx;
+      }
     }
     for (int k = 0; k < 3; k++) w.xnew[k + 3 * i] = xnew[k];
     double psijn;
@@ -2366,17 +2497,31 @@ bool dmc_walker(DmcPop &P, int iw, double ffi, double &wsum1, double &esum1, dou
     if (w.detn != 0.0) w.grad(i, 0, vn);
     else vn[0] = vn[1] = vn[2] = 0;
     if (psidn * w.psido <= zero) nodecr++;  // icross=1: counted, not rejected
-    double v2new = vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2];
-    vavvt = (std::sqrt(one + two * adrift * v2new * tau) - one) / (adrift * v2new);
-    double dfus2n = zero;
-    for (int k = 0; k < 3; k++) {
-      double drift = vavvt * vn[k];
-      double xbac = xnew[k] + drift;
-      double dfus = xbac - w.xold[k + 3 * i];
-      dfus2n += dfus * dfus;
+    double dfus2n = zero, fnormn = one;
+    if (ae) {
+      // the reverse move (dmc_ae :396-474): the drifted point of the new
+      // position and the density of returning to the old one
+      const AeFrame f = ae_frame(s, xnew, vn, tau);
+      const double *c = &s->cent[3 * f.ic];
+      double dfus2b = zero;
+      for (int k = 0; k < 3; k++) {
+        dfus2b += (c[k] - xo[k]) * (c[k] - xo[k]);
+        dfus2n += (f.xd[k] - xo[k]) * (f.xd[k] - xo[k]);
+      }
+      const double dfusb = std::sqrt(dfus2b);
+      fnormn = f.pgaus + f.qgaus * term * f.zeta * f.zeta * f.zeta * std::exp(-two * f.zeta * dfusb + 0.5 * dfus2n / tau);
+    } else {
+      double v2new = vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2];
+      double vavvt = (std::sqrt(one + two * adrift * v2new * tau) - one) / (adrift * v2new);
+      for (int k = 0; k < 3; k++) {
+        double drift = vavvt * vn[k];
+        double xbac = xnew[k] + drift;
+        double dfus = xbac - xo[k];
+        dfus2n += dfus * dfus;
+      }
     }
     double p = (psidn / w.psido) * (psidn / w.psido) * std::exp(2 * (psijn - w.psijo)) *
-               std::exp((dfus2o - dfus2n) / (two * tau)) * 1.0;
+               std::exp((dfus2o - dfus2n) / (two * tau)) * fnormn / fnormo;
     if (P.iage[iw] > 50) p = p * std::pow(1.1, P.iage[iw] - 50);
     pp = pp * p;
     p = std::min(one, p);

@@ -105,3 +105,77 @@ def test_dmc_tmove_parity(oracle_mod, config, W):
         do.steps(1, 8)
         _compare(dg, do)
     assert dg.counts()["tmoves"] == do.tmoves() > 0
+
+
+def _all_electron(name):
+    import copy
+    import os
+    from champ_b200.system import make_synthetic
+    if name == "he":
+        s = copy.deepcopy(make_synthetic("he"))
+        s.nloc, s.nquad = 0, 0
+        s.lpot = s.necp_term = s.necp_power = s.ecp_exponent = s.ecp_coef = None
+        s.xq0 = s.yq0 = s.zq0 = s.wq = None
+        s._keep = []
+        return s
+    from champ_b200.champ_io import load_npz
+    from conftest import GOLDEN
+    return load_npz(os.path.join(GOLDEN, "vmc_h2_system.npz"))
+
+
+@pytest.mark.parametrize("name,W,tau", [("he", 32, 0.02), ("h2", 32, 0.01)])
+def test_dmc_all_electron_parity(oracle_mod, name, W, tau):
+    """dmc_ae moves (dmc/dmc_ae_mov1.f90:4) of all-electron wave functions:
+    identical populations, streams, weights, positions and energies."""
+    from champ_b200.engine import Dmc, Engine
+    s = _all_electron(name)
+    o = oracle_mod.OracleSystem(s)
+    mw = 4 * W
+    st = oracle_mod.rng_states(mw + 2)
+    xs = []
+    for w in range(W):
+        x, st[w] = o.sites(st[w])
+        xs.append(x)
+    vw = oracle_mod.OracleWalkers(o, np.array(xs), st[:W])
+    vw.steps(20, 8)
+    vw.end_block()
+    x, r = vw.walkers()
+    rng = np.concatenate([r, st[W:mw]])
+    e0 = vw.results()["energy"]
+    dg = Dmc(Engine(s), x, rng, st[mw], tau=tau, etrial=e0, mwalk=mw)
+    do = oracle_mod.OracleDmc(o, x, rng, st[mw], tau=tau, etrial=e0, mwalk=mw)
+    _compare(dg, do)
+    for step in range(5):
+        dg.steps(1)
+        do.steps(1, 8)
+        _compare(dg, do)
+    dg.end_block()
+    do.end_block()
+    rg, ro = dg.results(), do.results()
+    for k in ("energy", "nwalk", "eest", "accept", "taueff", "fprod", "eigv"):
+        assert abs(rg[k] - ro[k]) <= 1e-9 * max(1.0, abs(ro[k])), k
+
+
+def test_dmc_all_electron_helium_exact_gpu(oracle_mod):
+    """All-electron He (nodeless trial function) through the engine's dmc_ae
+    moves reaches the exact energy."""
+    from champ_b200.engine import Dmc, Engine, initial_configs, rng_states
+    from champ_b200.system import HE_EXACT
+    s = _all_electron("he")
+    W = 1024
+    st = rng_states(3 * W + 1)
+    x = initial_configs(s, st[:W].copy())
+    eng = Engine(s)
+    eng.set_walkers(x, st[:W].copy())
+    eng.vmc_steps(100)
+    xv, _ = eng.walkers()
+    e0 = float(np.mean(eng.state()[0]))
+    d = Dmc(eng, xv, st[:3 * W], st[3 * W], tau=0.02, etrial=e0, mwalk=3 * W)
+    d.steps(200)
+    d.end_block()
+    for _ in range(10):
+        d.steps(100)
+        d.end_block()
+    r = d.results()
+    print(f"all-electron He DMC {r['energy']:.5f} +- {r['err']:.5f} (exact {HE_EXACT}), accept {r['accept']:.4f}")
+    assert abs(r["energy"] - HE_EXACT) <= 3 * r["err"] + 1e-3, r

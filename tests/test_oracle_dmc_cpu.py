@@ -128,3 +128,44 @@ def test_tmoves_oracle(oracle_mod):
     dm = oracle_mod.OracleDmc(om, np.array([om.sites(st[0])[0]]), st[:4], st[4], tau=0.01, etrial=0.0, mwalk=4)
     with pytest.raises(ValueError):
         dm.set_tmoves(-1)
+
+
+def _he_all_electron():
+    import copy
+    from champ_b200.system import make_synthetic
+    s = copy.deepcopy(make_synthetic("he"))
+    s.nloc, s.nquad = 0, 0
+    s.lpot = s.necp_term = s.necp_power = s.ecp_exponent = s.ecp_coef = None
+    s.xq0 = s.yq0 = s.zq0 = s.wq = None
+    s._keep = []
+    return s
+
+
+def test_dmc_all_electron_helium_exact(oracle_mod):
+    """dmc_ae (dmc/dmc_ae_mov1.f90:4) on all-electron He with a nodeless
+    trial function reaches the exact energy: the move's drift in the
+    nucleus frame, its Gaussian / exponential mixture and the reverse
+    density, and dmc_eloc_cutoff's all-electron branch are then unbiased."""
+    from champ_b200.system import HE_EXACT
+    s = _he_all_electron()
+    o = oracle_mod.OracleSystem(s)
+    W = 400
+    st = oracle_mod.rng_states(3 * W + 1)
+    xs = []
+    for w in range(W):
+        x, st[w] = o.sites(st[w])
+        xs.append(x)
+    vw = oracle_mod.OracleWalkers(o, np.array(xs), st[:W])
+    vw.steps(200, 8)
+    vw.end_block()
+    x, r = vw.walkers()
+    rng = np.concatenate([r, st[W:3 * W]])
+    d = oracle_mod.OracleDmc(o, x, rng, st[3 * W], tau=0.02, etrial=vw.results()["energy"], mwalk=3 * W)
+    d.steps(200, 8)
+    d.end_block()
+    for _ in range(20):
+        d.steps(100, 8)
+        d.end_block()
+    res = d.results()
+    assert abs(res["energy"] - HE_EXACT) <= 3 * res["err"] + 1e-3, res
+    assert res["accept"] > 0.98
