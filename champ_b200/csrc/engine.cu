@@ -68,6 +68,7 @@ struct cw_ctx {
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
   size_t smem_commit = 0;  // k_commit_tile's dynamic shared memory (0: the untiled k_commit)
+  int big_spin = 0;        // Slater inverse and c~ on global memory (spins too large for shared memory)
   int *acc_list = nullptr, *acc_count = nullptr;  // accepted walkers of a move (k_accept_list)
   int ecp_warps = 1, ecp_naov = 0, ecp_minb = 1;
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
@@ -699,7 +700,7 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     LCHK("k_scatter_orbs");
   }
   stage_begin(c, CW_ST_SLATER_INV);
-  k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->st, c->hb);
+  k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->st, c->hb, c->big_spin);
   stage_end(c);
   LCHK("k_slater_inv");
   if (h.nloc > 0 && c->md_on) {
@@ -713,7 +714,7 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     if (c->bocc)  // rows (walker, spin, slot) of slmi times the occupied coefficient rows
       dgemm(c->stream, W * N, h.K, h.nmax, c->st.slmi, c->bocc, c->hb.ctilde);
     else
-      k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->st, c->hb, c->g);
+      k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->st, c->hb, c->g, c->big_spin);
     stage_end(c);
     LCHK("k_ctilde");
     stage_begin(c, CW_ST_ECP);
@@ -988,7 +989,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   if (d->isc < 2 || d->isc > 5) return bad("isc must be 2..5");
   const int ndn = d->nelec - d->nup;
   const int nmax = std::max(d->nup, ndn);
-  if (nmax > 128) return bad("more than 128 electrons of one spin");
+  if (nmax > 256) return bad("more than 256 electrons of one spin");
   if (precision != CW_PREC_FP64 && precision != CW_PREC_MIXED) return bad("unknown precision");
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) {
@@ -1212,8 +1213,11 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
     c->smem_jfull = sizeof(double) * (3 * (size_t)h.N + 1 + 2 * (size_t)h.M * 8 + 2 * (size_t)h.M * 4 * een_nb(nord));
   }
-  c->smem_sinv = sizeof(double) * ((size_t)nmax * nmax + nmax);
-  c->smem_ctil = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64);
+  // spins whose n x n inverse does not fit in shared memory (about 160
+  // electrons and up): the inverse and c~ kernels work on global memory
+  c->big_spin = sizeof(double) * ((size_t)nmax * nmax + (size_t)nmax * 64) > 200 * 1024 ? 1 : 0;
+  c->smem_sinv = sizeof(double) * ((c->big_spin ? 0 : (size_t)nmax * nmax) + nmax);
+  c->smem_ctil = sizeof(double) * ((c->big_spin ? 0 : (size_t)nmax * nmax) + (size_t)nmax * 64);
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
   }

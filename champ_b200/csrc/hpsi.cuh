@@ -328,18 +328,21 @@ __global__ void k_scatter_orbs(WState st, HBuf hb, GSys g, int e0, int ne) {
 // ---------------------------------------------------------------------------
 // matinv + ddx/d2dx2: CTA per (walker, spin); matrix in shared memory.
 // ---------------------------------------------------------------------------
-__global__ void k_slater_inv(WState st, HBuf hb) {
+// in_place: the factorisation runs in the walker's slmi block in global
+// memory (L2-resident) instead of shared memory, for spins too large for
+// shared memory (same arithmetic; shared memory then holds col only).
+__global__ void k_slater_inv(WState st, HBuf hb, int in_place) {
   const int w = blockIdx.x >> 1, iab = blockIdx.x & 1;
   if (w >= st.W) return;
   const int N = cs.N, nmax = cs.nmax;
   const int nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
   const int n = nel;
   extern __shared__ __align__(16) double smem[];
-  double *A = smem;              // n*n column-major: A(e,j) = orb of slot j at electron e
-  double *col = smem + n * n;    // n
   __shared__ int ipvt[256];
   __shared__ int s_p, s_sing;
   double *slmi = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
+  double *A = in_place ? slmi : smem;            // n*n column-major: A(e,j) = orb of slot j at electron e
+  double *col = in_place ? smem : smem + n * n;  // n
   if (n == 0) {
     if (threadIdx.x == 0) st.detiab[2 * w + iab] = 1.0;
     return;
@@ -466,7 +469,10 @@ __global__ void k_slater_inv(WState st, HBuf hb) {
     return;
   }
   if (threadIdx.x == 0) st.detiab[2 * w + iab] = det;
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) slmi[t] = A[t];
+  if (!in_place)
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) slmi[t] = A[t];
+  else
+    __syncthreads();  // every thread's last writes to the block before the reads below
   // ddx, d2dx2 (determinant.f90 ddot loops)
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
     double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
@@ -486,7 +492,9 @@ __global__ void k_slater_inv(WState st, HBuf hb) {
 // ---------------------------------------------------------------------------
 // c~ vectors: CTA per (walker, spin, 64-AO chunk).
 // ---------------------------------------------------------------------------
-__global__ void k_ctilde(WState st, HBuf hb, GSys g) {
+// s_global: the inverse is read from global memory (L2) rather than staged
+// in shared memory, for spins too large for shared memory
+__global__ void k_ctilde(WState st, HBuf hb, GSys g, int s_global) {
   const int nchunk = (cs.K + 63) / 64;
   const int b = blockIdx.x;
   const int chunk = b % nchunk, iab = (b / nchunk) & 1, w = b / (2 * nchunk);
@@ -495,10 +503,12 @@ __global__ void k_ctilde(WState st, HBuf hb, GSys g) {
   const int nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
   if (nel == 0) return;
   extern __shared__ __align__(16) double smem[];
-  double *S = smem;                 // nel*nel
-  double *Co = smem + nel * nel;    // [nel][64]
   const double *slmi = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
-  for (int t = threadIdx.x; t < nel * nel; t += blockDim.x) S[t] = slmi[t];
+  double *Ss = smem;                                // nel*nel (shared-memory staging)
+  double *Co = s_global ? smem : smem + nel * nel;  // [nel][64]
+  const double *S = s_global ? slmi : Ss;
+  if (!s_global)
+    for (int t = threadIdx.x; t < nel * nel; t += blockDim.x) Ss[t] = slmi[t];
   const int m0 = chunk * 64;
   for (int t = threadIdx.x; t < nel * 64; t += blockDim.x) {
     const int j = t / 64, mm = t % 64;

@@ -541,33 +541,33 @@ def model_hamiltonian_orbitals(cent, types_of_centre, type_defs, norb, ecp=None)
     return coef, basis
 
 
-def determinant_scale(basis, coef, cent, types_of_centre, znuc, nup, ndn, nconf=4, seed=12345):
-    """A constant c for the LCAO coefficients such that the Slater
-    determinants of typical configurations are of order one.
+def determinant_scale(system, basis, nconf=8, seed=12345):
+    """A constant c for the LCAO coefficients of `system` such that the
+    Slater determinants at its start configurations are of order one.
 
     psi_D is defined up to a constant factor, and every determinant of an
     expansion holds the same number of electrons of each spin, so scaling
     every orbital by c scales psi_D by c^nelec and leaves ratios, drifts,
     local energies and the walk unchanged.  Unscaled, the determinants of
     large molecules (100 electrons of a spin) fall below the smallest FP64
-    number and psi_D underflows to zero.  c is exp(-<ln|det|>/n) over a few
-    configurations that place the electrons around the nuclei in proportion
-    to their charges (the sites rule), from a private random stream."""
+    number and psi_D underflows to zero.  c is exp(-median(ln|det|)/n) over
+    nconf start configurations of CHAMP's sites rule (cw_sites, a host-side
+    routine of the engine library) drawn from a private stream."""
     from . import trial
-    rng = np.random.default_rng(seed)
-    z = np.array([znuc[t] for t in types_of_centre], float)
+    from .engine import initial_configs, rng_states
+    coef = np.asarray(system.coef, float)
+    rng = rng_states(nconf, cseed=str(seed).rjust(32, "1"))
+    x = initial_configs(system, rng)
     logs = []
-    for _ in range(nconf):
-        for n in (nup, ndn):
+    for k in range(nconf):
+        for n, e0 in ((system.nup, 0), (system.ndn, system.nup)):
             if n == 0:
                 continue
-            at = rng.choice(len(z), size=n, p=z / z.sum())
-            pts = np.asarray(cent, float)[at] + rng.normal(0.0, 0.7, size=(n, 3))
-            A = trial.ao_values(basis, np.arange(len(basis["ao_cent"])), pts) @ coef[:n].T
+            A = trial.ao_values(basis, np.arange(coef.shape[1]), x[k, e0:e0 + n]) @ coef[np.asarray(system.iworbd[0][e0:e0 + n]) - 1].T
             sgn, lg = np.linalg.slogdet(A)
             if sgn != 0:
                 logs.append(lg / n)
-    return float(np.exp(-np.mean(logs))) if logs else 1.0
+    return float(np.exp(-np.median(logs))) if logs else 1.0
 
 
 def _assemble(name, rng, cent, types_of_centre, type_defs, nelec, nup, norb, nocc_up, nocc_dn,
@@ -599,8 +599,10 @@ def _assemble(name, rng, cent, types_of_centre, type_defs, nelec, nup, norb, noc
         if nloc:
             ecp = [(lpot[it], nterm[it], power[it], expo[it], ecoef[it]) for it in range(nct)]
         coef, basis_desc = model_hamiltonian_orbitals(cent, types_of_centre, type_defs, norb, ecp)
-        zn = [td["z"] for td in type_defs]
-        sysd["coef"] = coef * determinant_scale(basis_desc, coef, cent, types_of_centre, zn, nocc_up, nocc_dn)
+        sysd["coef"] = coef
+        sysm = System(**sysd)
+        sysm.coef = coef * determinant_scale(sysm, basis_desc)
+        return sysm
     return System(**sysd)
 
 

@@ -174,3 +174,32 @@ def test_chain_vmc_stream_parity(oracle_mod, nelec, orbitals):
     big = nelec > 100
     eng, ow = _vmc_pair(oracle_mod, s, 2 if big else 8, equil=4 if big else 10)
     _stream_parity(eng, ow, 1 if big else 2)
+
+
+@pytest.mark.parametrize("nelec", [400, 333])
+def test_large_spin_hpsi(oracle_mod, nelec):
+    """Spins of 200 and 167 electrons, beyond what shared memory holds for
+    the Slater inverse (matinv, vmc/matinv.f90:22-92) and c~: the engine
+    factorises in the walker's own inverse block in global memory.  The
+    odd count (167 up, 166 down) takes the per-spin c~ kernel.  Local
+    energy, psi_D and the inverse against the oracle at the sites start."""
+    from champ_b200.engine import Engine, initial_configs, rng_states
+    from champ_b200.system import make_chain
+    s = make_chain(nelec, 4000 + nelec, orbitals="random")
+    W = 2
+    rng = rng_states(W)
+    x = initial_configs(s, rng)
+    eng = Engine(s)
+    eng.set_walkers(x, rng)
+    o = oracle_mod.OracleSystem(s)
+    h = eng.hpsi()
+    slmi, det = eng.slater()
+    r = o.hpsi(x[0])
+    assert abs(h["energy"][0] - r["energy"]) <= 1e-9 * max(1.0, abs(r["energy"]))
+    assert abs(h["psid"][0] - r["psid"]) <= 1e-9 * abs(r["psid"])
+    rs, rdet = o.slater(x[0])
+    for iab, nel in enumerate((s.nup, s.ndn)):
+        assert rel_err(slmi[0, iab, :nel * nel], rs[iab, :nel * nel]) < 1e-9
+        assert abs(det[0, iab] - rdet[iab]) <= 1e-9 * abs(rdet[iab])
+    eng.vmc_steps(1)   # the move path at these sizes runs (untiled commit, global inverse)
+    assert np.all(eng.walker_status() == 0)
