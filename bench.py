@@ -38,6 +38,10 @@ CONFIGS = {
                         "300 Gaussians, 80 orbitals (model-Hamiltonian trial orbitals), 10^4 determinants "
                         "(1-4-fold excitations, |c_k|~k^-1.5), "
                         "order-5 Jastrow, 16384 walkers, tau=0.01, branching on"),
+    "c3": ("chain", 0, "batched-c3: 64 chain molecules of seeded sizes (8-200 electrons, ~4.5 x electrons "
+                       "Gaussians, Cl-like Z=7 with BFD-form ECP and H-like centres, seeded random orthonormal "
+                       "orbitals, order-5 Jastrow), 256-4096 walkers each, all resident at once; a step is one "
+                       "sweep of every system, issued concurrently on one stream per system"),
     "c4": ("chain", 0, "serve-c4: seeded Poisson arrivals of VMC energy jobs, each a chain molecule of the "
                        "batched distribution (8-200 electrons, ~4.5 x electrons Gaussians, Cl-like Z=7 with ECP "
                        "and H-like centres), 256-1024 walkers, target error 0.5 mHa within a block budget, "
@@ -319,6 +323,28 @@ def run_dmc(args):
     return 0
 
 
+def device_overlap(blocks, slots):
+    """Device-clock view of the served blocks: the summed block time over the
+    time the device held at least one block (above 1: blocks of different
+    jobs ran at the same time), and the most blocks in flight at once."""
+    if not blocks:
+        return None
+    ev = sorted([(s, 1) for _, s, _ in blocks] + [(e, -1) for _, _, e in blocks])
+    run = most = 0
+    busy = 0
+    last = None
+    for tns, d in ev:
+        if run > 0 and last is not None:
+            busy += tns - last
+        run += d
+        most = max(most, run)
+        last = tns
+    total = sum(e - s for _, s, e in blocks)
+    return {"blocks": len(blocks), "worker_slots": slots, "sum_block_s": round(total * 1e-9, 4),
+            "device_occupied_s": round(busy * 1e-9, 4), "ratio": round(total / max(busy, 1), 3),
+            "most_in_flight": most}
+
+
 def run_serve(args):
     """Serving loop (config c4): p50/p99 time-to-result of a Poisson stream of jobs."""
     import torch
@@ -340,8 +366,8 @@ def run_serve(args):
                           seed_offset=int(np.sum(nwk[:i]))) for i in range(n)]
 
     # warm-up: the module loads and every kernel is compiled into the context once
-    serve.Server(budget, precision=args.precision, device=local).run(jobs(min(args.warmup, 2), None))
-    srv = serve.Server(budget, precision=args.precision, device=local)
+    serve.Server(budget, precision=args.precision, device=local, slots=args.slots).run(jobs(min(args.warmup, 2), None))
+    srv = serve.Server(budget, precision=args.precision, device=local, slots=args.slots)
     with ClockSampler(local) as clk:
         barrier(pg, local)
         t0 = time.perf_counter()
@@ -364,12 +390,106 @@ def run_serve(args):
                    "parallelism": f"replicas x{world} (independent job streams)"},
         "serving": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in summ.items()},
         "peak_admitted_gb": round(srv.peak_bytes / (1 << 30), 3),
+        "overlap": device_overlap(srv.device_blocks, args.slots),
         "e2e": {"value": p50, "unit": "s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "path": "host job specs -> engine contexts (walkers and streams uploaded) -> block results read back"},
         "clocks": clk.summary(),
         "gpu_launches": None,
     }
     print(json.dumps(line), flush=True)
+    pg.close()
+    return 0
+
+
+def batched_rate(systems, walkers, precision, device, steps, warmup, slots):
+    """Sweeps of every system's own context, issued from `slots` worker
+    threads (each context on its own stream).  Returns electron-moves/s over
+    the device-clock span of the timed sweeps (first start stamp to last end
+    stamp of all contexts), the wall time, and the summed device time of the
+    contexts' own sweeps."""
+    import concurrent.futures as cf
+    from champ_b200.engine import Engine, rng_states, start_population
+    engines = []
+    off = 0
+    for s, w in zip(systems, walkers):
+        e = Engine(s, device=device, precision=precision)
+        start_population(e, s, rng_states(off + w)[off:].copy())
+        off += w
+        engines.append(e)
+
+    def sweep(e, n):
+        e.stamp()
+        e.vmc_steps(n)
+        e.stamp()
+        e.sync()
+
+    with cf.ThreadPoolExecutor(max_workers=slots) as pool:
+        list(pool.map(lambda e: sweep(e, warmup), engines))      # graph capture + warm-up
+        t0 = time.perf_counter()
+        list(pool.map(lambda e: sweep(e, steps), engines))
+        wall = time.perf_counter() - t0
+    st = [e.stamps()[-2:] for e in engines]
+    span_ns = max(int(b) for _, b in st) - min(int(a) for a, _ in st)
+    own_ns = sum(int(b) - int(a) for a, b in st)
+    moves = sum(w * s.nelec for s, w in zip(systems, walkers)) * steps
+    launches = sum(e.launches() for e in engines)
+    for e in engines:
+        e.close()
+    return moves / (span_ns * 1e-9), wall, own_ns * 1e-9, span_ns * 1e-9, launches
+
+
+def run_batched(args):
+    """Config c3: many uneven systems resident at once, swept concurrently."""
+    import torch
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from champ_b200 import serve
+    from champ_b200.system import make_chain
+    _, _, desc = CONFIGS[args.config]
+    nsys = args.systems
+    rng = np.random.default_rng(5151 + rank)
+    nel = rng.integers(8, 201, size=nsys)
+    nwk = rng.integers(256, 4097, size=nsys)
+    systems = [make_chain(int(n), 3000 + 97 * rank + i, orbitals="random") for i, n in enumerate(nel)]
+    budget = args.budget_gb * (1 << 30)
+    need = sum(serve.estimate_bytes(s, int(w), "mixed") for s, w in zip(systems, nwk))
+    scale = min(1.0, budget / need)
+    walkers = [max(64, int(w * scale)) for w in nwk]
+    res = {}
+    with ClockSampler(local) as clk:
+        for prec in ("fp64", "mixed"):
+            barrier(pg, local)
+            res[prec] = batched_rate(systems, walkers, prec, local, args.steps, max(args.warmup, 1), args.slots)
+            barrier(pg, local)
+    value = max_over_ranks(1.0 / res[args.precision][0], pg, local)
+    value = world / value
+    if rank != 0:
+        pg.close()
+        return 0
+    r = res[args.precision]
+    moves_step = sum(w * s.nelec for s, w in zip(systems, walkers))
+    line = {
+        "metric": "electron-moves/s", "value": value, "unit": "electron-moves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r[3] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "mixed", "data": "synthetic",
+        "config": {"workload": desc, "systems": nsys, "electrons_min_max": [int(nel.min()), int(nel.max())],
+                   "walkers_total": int(sum(walkers)), "walker_scale": round(scale, 4),
+                   "walker_note": "drawn counts scaled so that all systems' contexts fit the HBM budget at once",
+                   "hbm_budget_gb": args.budget_gb, "worker_threads": args.slots, "precision": args.precision,
+                   "l2": "per-walker state of every system far exceeds the 126 MB L2",
+                   "parallelism": f"replicas x{world}"},
+        "batched": {p: {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4),
+                        "sum_of_context_device_s": round(v[2], 4),
+                        "concurrency": round(v[2] / v[3], 2), "wall_s": round(v[1], 4)}
+                    for p, v in res.items()},
+        "mixed_over_fp64": round(res["mixed"][0] / res["fp64"][0], 3),
+        "e2e": {"value": None, "unit": "electron-moves/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "path": "not measured for the batched config"},
+        "clocks": clk.summary(), "gpu_launches": int(r[4]),
+        "moves_per_step": int(moves_step),
+    }
+    print(json.dumps(line))
     pg.close()
     return 0
 
@@ -571,17 +691,25 @@ def main():
     ap.add_argument("--block-steps", type=int, default=5, help="sweeps per block of the efficiency runs")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--rate", type=float, default=4.0, help="c4: job arrivals per second")
-    ap.add_argument("--budget-gb", type=float, default=16.0, help="c4: HBM budget of the admitted jobs")
+    ap.add_argument("--budget-gb", type=float, default=None,
+                    help="c3/c4: HBM budget of the resident contexts (default 120 for c3, 16 for c4)")
+    ap.add_argument("--systems", type=int, default=64, help="c3: systems resident at once")
+    ap.add_argument("--slots", type=int, default=16, help="c3/c4: worker threads (contexts with work in flight)")
     args = ap.parse_args()
+    if args.budget_gb is None:
+        args.budget_gb = 120.0 if args.config == "c3" else 16.0
     if args.impl == "reference":
-        if args.config == "c4":
-            print(json.dumps({"impl": "reference", "unavailable": "CHAMP has no request loop (one job per run)"}))
+        if args.config in ("c3", "c4"):
+            print(json.dumps({"impl": "reference", "unavailable": "CHAMP runs one system per job (no batching "
+                                                                  "across systems, no request loop)"}))
             return 0
         return run_reference(args)
     if args.config == "c2":
         return run_dmc(args)
     if args.config == "c4":
         return run_serve(args)
+    if args.config == "c3":
+        return run_batched(args)
     return run_ours(args)
 
 

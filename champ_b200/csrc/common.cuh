@@ -1,9 +1,12 @@
 // common.cuh — device-side building blocks of the walker engine.
 //
-// System constants live in __constant__ memory (every lane of a warp reads
-// the same centre/type parameters in lock-step, so constant-cache broadcast
-// is the right home).  Large tables (radial splines, LCAO coefficients) live
-// in global memory and stay L2-resident.
+// System constants travel with every launch as a __grid_constant__ kernel
+// parameter (the parameter bank is served by the constant cache, so lanes
+// reading the same type parameters in lock-step get a broadcast) — one
+// block per context, so contexts of different systems run their kernels
+// side by side on one device.  Per-centre records and large tables (radial
+// splines, LCAO coefficients) live in the context's global memory and stay
+// L2-resident.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -18,7 +21,8 @@
 #define CW_MAX_ELEC 1024
 
 // ---------------------------------------------------------------------------
-// Constant-memory system description
+// System description passed by value to every kernel (at most the 32764
+// bytes a kernel parameter list may hold)
 // ---------------------------------------------------------------------------
 struct CSys {
   int N, nup, ndn, M, nctype, K, Oa, nmax;
@@ -27,10 +31,11 @@ struct CSys {
   double scalek, asymp_r, asymp_jasb[2];
   double deltar, deltat, fbias, pecent, cdet;
   int mrwf, mpts, mbastyp;
-  // per centre
-  double cent[CW_MAX_CENT * 3];
-  int iwctype[CW_MAX_CENT];
-  int ao_first[CW_MAX_CENT + 1];
+  // per centre, in the context's global memory: coordinates [M][3], atom
+  // type [M], first AO [M + 1]
+  const double *cent;
+  const int *iwctype;
+  const int *ao_first;
   // per type
   double znuc[CW_MAX_TYPES];
   int nrbas[CW_MAX_TYPES], igrid[CW_MAX_TYPES], nr[CW_MAX_TYPES], nbastyp[CW_MAX_TYPES];
@@ -60,8 +65,7 @@ struct CSys {
   double slm_k[36];
 };
 
-// the one system block of the engine translation unit
-__constant__ CSys cs;
+static_assert(sizeof(CSys) <= 31 * 1024, "the system block must fit a kernel parameter list");
 
 // Global-memory tables of the system.
 struct GSys {
@@ -168,7 +172,7 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
 // determinant_psig (vmc/determinant_psig.f90:3) with anormo = 1 from the S
 // of every state (psi_i/psi_1 = S_i/S_1, one orbital set and Jastrow):
 // psi2g = w_1 + sum_{i>1} w_i (S_i/S_1)^2
-__device__ __forceinline__ double md_psig(const double *S, int ns) {
+__device__ __forceinline__ double md_psig(const CSys &cs, const double *S, int ns) {
   double g = cs.wg[0];
   for (int i = 1; i < ns; i++) {
     const double r = S[i] / S[0];
@@ -212,7 +216,7 @@ struct DRng {
 // scale_dist family (vmc/scale_dist.f90:57-353)
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ T scale0(T r) {
+__device__ __forceinline__ T scale0(const CSys &cs, T r) {
   const T k = (T)cs.scalek;
   if (cs.scalek == 0) return r;
   if (cs.isc == 2) return (T(1) - exp(-k * r)) / k;
@@ -224,7 +228,7 @@ __device__ __forceinline__ T scale0(T r) {
   return r * (T(1) / pow(T(1) + pow(k * r, T(3)), T(1) / T(3)));
 }
 template <typename T>
-__device__ __forceinline__ void scale2(T r, T &rr, T &dd1, T &dd2) {
+__device__ __forceinline__ void scale2(const CSys &cs, T r, T &rr, T &dd1, T &dd2) {
   const T k = (T)cs.scalek;
   if (cs.scalek == 0) { rr = r; dd1 = 1; dd2 = 0; return; }
   if (cs.isc == 2) {
@@ -759,16 +763,16 @@ __device__ __forceinline__ EenOut<T> een_apply2(const T *__restrict__ BD4, T y, 
 
 // e-e-n coefficients of atom type it in the compute precision
 template <typename T>
-__device__ __forceinline__ const T *een_coef(int it);
+__device__ __forceinline__ const T *een_coef(const CSys &cs, int it);
 template <>
-__device__ __forceinline__ const double *een_coef<double>(int it) { return &cs.c[it * CW_MAX_TERMS]; }
+__device__ __forceinline__ const double *een_coef<double>(const CSys &cs, int it) { return &cs.c[it * CW_MAX_TERMS]; }
 template <>
-__device__ __forceinline__ const float *een_coef<float>(int it) { return &cs.cf[it * CW_MAX_TERMS]; }
+__device__ __forceinline__ const float *een_coef<float>(const CSys &cs, int it) { return &cs.cf[it * CW_MAX_TERMS]; }
 
 // Padé + polynomial e-e term (jastrow4.f90 ee part) at scaled u:
 // returns fee, d fee/du, d2 fee/du2 (MODE>=2)
 template <int MODE, typename T>
-__device__ __forceinline__ void ee_term(int isb, int ipar, T sspinn, T u, T &fee, T &feeu, T &feeuu) {
+__device__ __forceinline__ void ee_term(const CSys &cs, int isb, int ipar, T sspinn, T u, T &fee, T &feeu, T &feeuu) {
   const int nb = cs.nordb + 1;
   T b0 = (T)cs.b[isb * nb + 0], b1 = (T)cs.b[isb * nb + 1];
   T top = sspinn * b0 * u, topu = sspinn * b0;
@@ -791,7 +795,7 @@ __device__ __forceinline__ void ee_term(int isb, int ipar, T sspinn, T u, T &fee
 
 // Padé + polynomial e-n term (jastrow4.f90 en part) at scaled r
 template <int MODE, typename T>
-__device__ __forceinline__ void en_term(int it, T r, T &fen, T &feni, T &fenii) {
+__device__ __forceinline__ void en_term(const CSys &cs, int it, T r, T &fen, T &feni, T &fenii) {
   const int na = cs.norda + 1;
   T a0 = (T)cs.a4[it * na + 0], a1 = (T)cs.a4[it * na + 1];
   T top = a0 * r, topi = a0;
@@ -879,7 +883,7 @@ __device__ __forceinline__ void slm_eval(int l, double x, double y, double z, do
 // displacement xc (= x - cent).  out(m, d) receives value (d=0), gradient
 // (d=1..3, ider>=1) and Laplacian (d=4, ider>=2).
 template <typename Store>
-__device__ __forceinline__ void basis_centre(const GSys &g, int ic, const double *xc, int ider, Store out) {
+__device__ __forceinline__ void basis_centre(const CSys &cs, const GSys &g, int ic, const double *xc, int ider, Store out) {
   // basis_fns + splfit (vmc/splfit.f90:3-94) for every radial function of
   // the centre.  The grid interval (jx, ref0, ref1) depends only on r and
   // the atom type, so it is located once per centre; r0*arg^(jx-1) comes
@@ -1000,7 +1004,7 @@ __device__ __forceinline__ void basis_centre(const GSys &g, int ic, const double
 constexpr int kCenRec = 28;  // doubles per centre record
 
 template <int IDER>
-__device__ __forceinline__ void warp_basis_prepass(const GSys &g, const double *x, double *rec, int lane) {
+__device__ __forceinline__ void warp_basis_prepass(const CSys &cs, const GSys &g, const double *x, double *rec, int lane) {
   for (int ic = lane; ic < cs.M; ic += 32) {
     double *q = rec + (size_t)ic * kCenRec;
     const Cen cc = cen_of(g, ic);
@@ -1057,7 +1061,7 @@ __device__ __forceinline__ void warp_basis_prepass(const GSys &g, const double *
 
 // value (d=0), gradient (d=1..3, IDER>=1), Laplacian (d=4, IDER>=2) of AO m
 template <int IDER, typename Store>
-__device__ __forceinline__ void warp_basis_ao(const GSys &g, const double *rec, int m, Store out) {
+__device__ __forceinline__ void warp_basis_ao(const CSys &cs, const GSys &g, const double *rec, int m, Store out) {
   const int4 a4 = __ldg(g.ao + m);
   const int4 ax = __ldg(g.aox + m);
   const double2 ak = __ldg(g.aok + m);
@@ -1118,7 +1122,7 @@ __device__ __forceinline__ void warp_basis_ao(const GSys &g, const double *rec, 
 }
 
 // gauss_pot (vmc/readps_gauss.f90:57): channel l is CHAMP's 1-based index
-__device__ __forceinline__ double gauss_pot_d(double r, int l, int ict) {
+__device__ __forceinline__ double gauss_pot_d(const CSys &cs, double r, int l, int ict) {
   double v = 0, rsq = r * r;
   const int base = (ict * 4 + (l - 1)) * 16;
   const int nt = cs.necp_term[ict * 4 + (l - 1)];
@@ -1140,7 +1144,7 @@ __device__ __forceinline__ double yl0_d(int l, double costh) {
 }
 
 // pair spin classification of jastrow4 (isb, ipar, sspinn) for i > j
-__device__ __forceinline__ void pair_spin(int i, int j, int &isb, int &ipar, double &sspinn) {
+__device__ __forceinline__ void pair_spin(const CSys &cs, int i, int j, int &isb, int &ipar, double &sspinn) {
   sspinn = 1;
   isb = 0;
   ipar = 0;

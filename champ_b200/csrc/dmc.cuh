@@ -47,7 +47,7 @@ __device__ __forceinline__ double gauss_d(DRng &r) {
 
 // drift of electron e: slmi row · dorbs + vj (compute_determinante_grad
 // iflag_move=1)
-__device__ __forceinline__ void drift_old(const WState &st, int w, int e, double v[3],
+__device__ __forceinline__ void drift_old(const CSys &cs, const WState &st, int w, int e, double v[3],
                                           const double *md_vel = nullptr) {
   const int N = cs.N, nmax = cs.nmax;
   const int iab = e < cs.nup ? 0 : 1, nel = iab == 0 ? cs.nup : cs.ndn, ish = iab == 0 ? 0 : cs.nup;
@@ -66,7 +66,7 @@ __device__ __forceinline__ void drift_old(const WState &st, int w, int e, double
 }
 
 // nearest centre of a point: first minimum of the squared distance
-__device__ __forceinline__ int nearest_centre_d(const double x[3]) {
+__device__ __forceinline__ int nearest_centre_d(const CSys &cs, const double x[3]) {
   double best = 1.0e100;
   int iw = 0;
   for (int ic = 0; ic < cs.M; ic++) {
@@ -90,10 +90,10 @@ struct AeFrame {
   int ic;
   double zeta, qgaus, pgaus, xd[3];
 };
-__device__ __forceinline__ AeFrame ae_frame_d(const double x[3], const double v[3], double tau) {
+__device__ __forceinline__ AeFrame ae_frame_d(const CSys &cs, const double x[3], const double v[3], double tau) {
   const double one = 1, two = 2, half = 0.5, eps = 1.0e-10, adrift0 = 0.1;
   AeFrame f;
-  f.ic = nearest_centre_d(x);
+  f.ic = nearest_centre_d(cs, x);
   const double c[3] = {cs.cent[3 * f.ic], cs.cent[3 * f.ic + 1], cs.cent[3 * f.ic + 2]};
   const double z = cs.znuc[cs.iwctype[f.ic]];
   double rv[3], rmin = 0, vr = 0, v2 = 0;
@@ -147,12 +147,12 @@ __device__ __forceinline__ double ae_term(double tau) {
 // thread per walker: drift + diffusion of electron iel (dmc_ps's Gaussian
 // around the drifted point; dmc_ae's Gaussian / exponential mixture for an
 // all-electron wave function)
-__global__ void k_dmc_propose(WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, int iel) {
+__global__ void k_dmc_propose(const __grid_constant__ CSys cs, WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, int iel) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   const int N = cs.N;
   double vo[3];
-  drift_old(st, w, iel, vo, mb.md_velo ? mb.md_velo + 3 * w : nullptr);
+  drift_old(cs, st, w, iel, vo, mb.md_velo ? mb.md_velo + 3 * w : nullptr);
   for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + iel] = vo[k];
   const double tau = sc.tau, rttau = sqrt(tau), adrift = 0.5;
   DRng rng;
@@ -162,7 +162,7 @@ __global__ void k_dmc_propose(WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, i
   if (cs.nloc == 0) {
     const double xo[3] = {st.x[((size_t)w * 3 + 0) * N + iel], st.x[((size_t)w * 3 + 1) * N + iel],
                           st.x[((size_t)w * 3 + 2) * N + iel]};
-    const AeFrame f = ae_frame_d(xo, vo, tau);
+    const AeFrame f = ae_frame_d(cs, xo, vo, tau);
     const double c[3] = {cs.cent[3 * f.ic], cs.cent[3 * f.ic + 1], cs.cent[3 * f.ic + 2]};
     double xn[3] = {f.xd[0], f.xd[1], f.xd[2]}, dfusb;
     if (rng.uniform() < f.pgaus) {
@@ -207,7 +207,7 @@ __global__ void k_dmc_propose(WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, i
 
 // thread per walker: ratio and drift at the new point, reverse diffusion,
 // acceptance p = |psi_n/psi_o|^2 G(o<-n)/G(n<-o) with the age boost
-__global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalars sc, int iel) {
+__global__ void k_dmc_decide(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalars sc, int iel) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
@@ -243,7 +243,7 @@ __global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalar
   if (cs.nloc == 0) {
     // dmc_ae's reverse move: the drifted point of the new position and the
     // density of returning to the old one
-    const AeFrame f = ae_frame_d(m.xnew, vn, tau);
+    const AeFrame f = ae_frame_d(cs, m.xnew, vn, tau);
     double dfus2b = 0;
     for (int k = 0; k < 3; k++) {
       const double xo = st.x[((size_t)w * 3 + k) * N + iel], c = cs.cent[3 * f.ic + k];
@@ -292,7 +292,7 @@ __global__ void k_dmc_decide(WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalar
 // Warp per walker, after hpsi: drift of every electron, fratio
 // (dmc_eloc_cutoff, nloc>0 branch), and for mode 1 the reweighting
 // (calculate_reweight) and the walker's sums of the step.
-__global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode, const double *md_vall) {
+__global__ void k_dmc_weights(const __grid_constant__ CSys cs, WState st, DmcBuf db, DmcScalars sc, int mode, const double *md_vall) {
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= st.W) return;
@@ -301,7 +301,7 @@ __global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode, con
   double vav2sum = 0, v2sum = 0;
   for (int e = lane; e < N; e += 32) {
     double v[3];
-    drift_old(st, w, e, v, md_vall ? md_vall + ((size_t)w * N + e) * 3 : nullptr);
+    drift_old(cs, st, w, e, v, md_vall ? md_vall + ((size_t)w * N + e) * 3 : nullptr);
     for (int k = 0; k < 3; k++) db.vold[((size_t)w * 3 + k) * N + e] = v[k];
     const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
     double vavvt;
@@ -310,7 +310,7 @@ __global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode, con
       // dmc_ae's adrift0 = 0.1
       const double x[3] = {st.x[((size_t)w * 3 + 0) * N + e], st.x[((size_t)w * 3 + 1) * N + e],
                            st.x[((size_t)w * 3 + 2) * N + e]};
-      const int ic = nearest_centre_d(x);
+      const int ic = nearest_centre_d(cs, x);
       double rmin = 0, vr = 0;
       for (int k = 0; k < 3; k++) {
         const double rv = x[k] - cs.cent[3 * ic + k];
@@ -368,7 +368,7 @@ __global__ void k_dmc_weights(WState st, DmcBuf db, DmcScalars sc, int mode, con
 // each lane sums a contiguous chunk, a warp scan finds the chunk, its lane
 // walks it.  The proposed point is r_en(e, ic) times the rotated quadrature
 // direction about the centre.
-__global__ void k_tmove_select(WState st, MoveBuf mb, const double *tv, DmcScalars sc) {
+__global__ void k_tmove_select(const __grid_constant__ CSys cs, WState st, MoveBuf mb, const double *tv, DmcScalars sc) {
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= st.W) return;
@@ -449,7 +449,7 @@ __global__ void k_tmove_select(WState st, MoveBuf mb, const double *tv, DmcScala
 // T-move of the chosen electron, always accepted (icasula = -1): ratio at
 // the point, psi_D, psi_J, commit of the scalars; k_commit applies the
 // matrix and table updates.  Thread per walker.
-__global__ void k_tmove_accept(WState st, MoveBuf mb, GSys g, DmcBuf db) {
+__global__ void k_tmove_accept(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, DmcBuf db) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   MoveScratch &m = mb.ms[w];
@@ -486,7 +486,7 @@ struct QuadRot {
   double x[CW_MAX_QUAD], y[CW_MAX_QUAD], z[CW_MAX_QUAD];
 };
 
-__global__ void k_set_quad(WState st, QuadRot q) {
+__global__ void k_set_quad(const __grid_constant__ CSys cs, WState st, QuadRot q) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   const int NQ = cs.nquad;

@@ -68,7 +68,11 @@ struct cw_ctx {
   std::vector<void *> w_allocs;
   size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
   size_t smem_commit = 0;  // k_commit_tile's dynamic shared memory (0: the untiled k_commit)
+  unsigned long long *d_stamps = nullptr;  // device-clock stamps (cw_stamp), kStampCap slots
+  int nstamp = 0;
+  int commit_grid = 1;     // k_commit_tile's grid: the blocks resident at once
   int big_spin = 0;        // Slater inverse and c~ on global memory (spins too large for shared memory)
+  int ecp_rr_global = 0;   // k_ecp's e-n distances on global memory (hb.ecp_rr)
   int *acc_list = nullptr, *acc_count = nullptr;  // accepted walkers of a move (k_accept_list)
   int ecp_warps = 1, ecp_naov = 0, ecp_minb = 1;
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
@@ -247,26 +251,12 @@ void stage_collect(cw_ctx *c) {
   c->evused = 0;
 }
 
-// The system constants live in one __constant__ block per device.  Every
-// entry point that launches kernels binds its context first: when another
-// context's constants are loaded, that context's queued work is waited for
-// and this context's constants are uploaded.  Contexts of different systems
-// on one device therefore serialise; contexts on different devices do not.
-cw_ctx *g_const_owner[64] = {nullptr};
-
+// Every kernel receives its context's system block by value, so entry points
+// only select the context's device; contexts of different systems on one
+// device run their work side by side, each on its own stream.
 int bind(cw_ctx *c) {
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
-  const int dev = c->device & 63;
-  cw_ctx *o = g_const_owner[dev];
-  if (o == c) return CW_OK;
-  if (o && o->stream) {
-    e = cudaStreamSynchronize(o->stream);
-    if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "waiting for another context: %s", cudaGetErrorString(e));
-  }
-  e = cudaMemcpyToSymbol(cs, &c->h, sizeof(CSys));
-  if (e != cudaSuccess) return fail(c, CW_ERR_CUDA, "constant upload: %s", cudaGetErrorString(e));
-  g_const_owner[dev] = c;
   return CW_OK;
 }
 
@@ -293,26 +283,26 @@ void launch_jmove(cw_ctx *c, int iel) {
   const int warps = 4;
   dim3 grid((c->W + warps - 1) / warps);
   if (c->mixed)
-    k_jastrow_move_f32<NORD><<<grid, 32 * warps, c->smem_jmove_f32, c->stream>>>(c->st, c->mb, iel);
+    k_jastrow_move_f32<NORD><<<grid, 32 * warps, c->smem_jmove_f32, c->stream>>>(c->h, c->st, c->mb, iel);
   else
-    k_jastrow_move<NORD><<<grid, 32 * warps, c->smem_jmove, c->stream>>>(c->st, c->mb, iel);
+    k_jastrow_move<NORD><<<grid, 32 * warps, c->smem_jmove, c->stream>>>(c->h, c->st, c->mb, iel);
 }
 template <int NORD>
 void launch_jfull(cw_ctx *c) {
   if (c->mixed)
-    k_jastrow_full<NORD, float><<<c->W, 128, c->smem_jfull, c->stream>>>(c->st, c->hb);
+    k_jastrow_full<NORD, float><<<c->W, 128, c->smem_jfull, c->stream>>>(c->h, c->st, c->hb);
   else
-    k_jastrow_full<NORD, double><<<c->W, 128, c->smem_jfull, c->stream>>>(c->st, c->hb);
+    k_jastrow_full<NORD, double><<<c->W, 128, c->smem_jfull, c->stream>>>(c->h, c->st, c->hb);
 }
 template <int NORD>
 void launch_ecp(cw_ctx *c) {
   const dim3 grid(c->W), block(32 * c->ecp_warps);
   if (c->mixed) {
-    if (c->ecp_minb == 2) k_ecp<NORD, float, 2><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
-    else k_ecp<NORD, float, 1><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+    if (c->ecp_minb == 2) k_ecp<NORD, float, 2><<<grid, block, c->smem_ecp, c->stream>>>(c->h, c->st, c->hb, c->g);
+    else k_ecp<NORD, float, 1><<<grid, block, c->smem_ecp, c->stream>>>(c->h, c->st, c->hb, c->g);
   } else {
-    if (c->ecp_minb == 2) k_ecp<NORD, double, 2><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
-    else k_ecp<NORD, double, 1><<<grid, block, c->smem_ecp, c->stream>>>(c->st, c->hb, c->g);
+    if (c->ecp_minb == 2) k_ecp<NORD, double, 2><<<grid, block, c->smem_ecp, c->stream>>>(c->h, c->st, c->hb, c->g);
+    else k_ecp<NORD, double, 1><<<grid, block, c->smem_ecp, c->stream>>>(c->h, c->st, c->hb, c->g);
   }
 }
 template <int NORD>
@@ -322,7 +312,14 @@ int set_attrs(cw_ctx *c) {
     // in shared memory, for inverses up to 128 x 128 (140 KB)
     const int n = c->h.nmax;
     c->smem_commit = n <= 128 ? sizeof(double) * ((size_t)n * (n + 1) + 3 * n) : 0;
-    if (c->smem_commit) CK(raise_smem(c, k_commit_tile, c->smem_commit));
+    if (c->smem_commit) {
+      CK(raise_smem(c, k_commit_tile, c->smem_commit));
+      // one wave of resident blocks loops over the accepted walkers
+      int nsm = 0, per = 0;
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_commit_tile, 128, c->smem_commit));
+      c->commit_grid = std::max(1, nsm * std::max(1, per));
+    }
   }
   CK(raise_smem(c, k_jastrow_move<NORD>, (size_t)(c->smem_jmove)));
   CK(raise_smem(c, k_jastrow_move_f32<NORD>, (size_t)(c->smem_jmove_f32)));
@@ -336,6 +333,9 @@ int set_attrs(cw_ctx *c) {
     const int tbytes = c->mixed ? 4 : 8, nb = 2 * ((een_nb(NORD) + 1) / 2);
     const int naov = c->ecp_naov;
     int best = 0;
+    // the walker's scaled e-n distances go to global memory only when no
+    // block shape fits them in shared memory
+    for (int rrg = 0; rrg <= 1 && best == 0; rrg++)
     for (int minb = 1; minb <= 2; minb++) {
       cudaFuncAttributes fa;
       if (c->mixed)
@@ -344,7 +344,7 @@ int set_attrs(cw_ctx *c) {
         CK(minb == 2 ? cudaFuncGetAttributes(&fa, k_ecp<NORD, double, 2>) : cudaFuncGetAttributes(&fa, k_ecp<NORD, double, 1>));
       const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
       for (int nw = 4; nw <= kEcpMaxWarps; nw++) {
-        const size_t bytes = sizeof(double) * (ecp_base_doubles(c->h.N, c->h.M, 32 * nw) +
+        const size_t bytes = sizeof(double) * (ecp_base_doubles(c->h.N, c->h.M, 32 * nw, rrg) +
                                                (size_t)nw * ecp_warp_doubles(c->h.M, nb, tbytes, naov)) +
                              fa.sharedSizeBytes;
         if (bytes > 227 * 1024) continue;
@@ -355,6 +355,7 @@ int set_attrs(cw_ctx *c) {
           c->ecp_warps = nw;
           c->ecp_minb = minb;
           c->smem_ecp = bytes - fa.sharedSizeBytes;
+          c->ecp_rr_global = rrg;
         } else if (blocks > 0 && blocks * nw == best && minb == c->ecp_minb) {
           c->ecp_warps = nw;
           c->smem_ecp = bytes - fa.sharedSizeBytes;
@@ -370,15 +371,16 @@ int set_attrs(cw_ctx *c) {
   return CW_OK;
 }
 
-// detsav + jassav of the accepted walkers (iel < 0: each walker's T-move electron)
-void launch_commit(cw_ctx *c, int iel) {
+// detsav + jassav of the accepted walkers (iel < 0: each walker's T-move electron);
+// listed: k_decide has already listed them
+void launch_commit(cw_ctx *c, int iel, bool listed = false) {
   if (c->smem_commit) {
     // the accepted walkers in order, then a fixed grid of blocks over them
-    k_accept_list<<<1, 1024, 0, c->stream>>>(c->mb.ms, c->W, c->acc_list, c->acc_count);
-    const int grid = std::max(1, std::min(c->W, 148 * 8));
-    k_commit_tile<<<grid, 128, c->smem_commit, c->stream>>>(c->st, c->mb, c->g, iel, c->acc_list, c->acc_count);
+    if (!listed) k_accept_list<<<1, 1024, 0, c->stream>>>(c->mb.ms, c->W, c->acc_list, c->acc_count);
+    const int grid = std::max(1, std::min(c->W, c->commit_grid));
+    k_commit_tile<<<grid, 128, c->smem_commit, c->stream>>>(c->h, c->st, c->mb, c->g, iel, c->acc_list, c->acc_count);
   } else {
-    k_commit<<<c->W, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel);
+    k_commit<<<c->W, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->g, iel);
   }
 }
 
@@ -581,12 +583,12 @@ int md_before_propose(cw_ctx *c, int iel) {
   const int W = c->W;
   if (iel == 0 || (iel == h.nup && h.ndn > 0)) {
     stage_begin(c, CW_ST_MDET);
-    k_md_phase<<<W, 128, c->smem_md_phase, c->stream>>>(c->st, c->md, c->mdt, iel == 0 ? 0 : 1);
+    k_md_phase<<<W, 128, c->smem_md_phase, c->stream>>>(c->h, c->st, c->md, c->mdt, iel == 0 ? 0 : 1);
     stage_end(c);
     LCHK("k_md_phase");
   }
   stage_begin(c, CW_ST_MDET);
-  k_md_drift_old<<<W, 128, c->smem_md_drift, c->stream>>>(c->st, c->md, c->mdt, c->g, iel);
+  k_md_drift_old<<<W, 128, c->smem_md_drift, c->stream>>>(c->h, c->st, c->md, c->mdt, c->g, iel);
   stage_end(c);
   LCHK("k_md_drift_old");
   return CW_OK;
@@ -594,7 +596,7 @@ int md_before_propose(cw_ctx *c, int iel) {
 int md_after_lcao(cw_ctx *c, int iel) {
   if (!c->md_on) return CW_OK;
   stage_begin(c, CW_ST_MDET);
-  k_md_move<<<c->W, 128, c->smem_md_move, c->stream>>>(c->st, c->mb, c->md, c->mdt, c->g, iel);
+  k_md_move<<<c->W, 128, c->smem_md_move, c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, c->g, iel);
   stage_end(c);
   LCHK("k_md_move");
   return CW_OK;
@@ -602,7 +604,7 @@ int md_after_lcao(cw_ctx *c, int iel) {
 int md_after_commit(cw_ctx *c, int iel) {
   if (!c->md_on) return CW_OK;
   stage_begin(c, CW_ST_MDET);
-  k_md_commit<<<c->W, 128, 0, c->stream>>>(c->st, c->mb, c->md, c->mdt, iel);
+  k_md_commit<<<c->W, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, iel);
   stage_end(c);
   LCHK("k_md_commit");
   return CW_OK;
@@ -611,7 +613,7 @@ int md_after_commit(cw_ctx *c, int iel) {
 // Full local energy of every walker (hpsi).  mode 1 also adds metrop6's sums.
 template <int NORD>
 void launch_jas_raw(cw_ctx *c) {
-  k_jas_raw<NORD><<<c->W, kJasThreads, 0, c->stream>>>(c->st, c->jas_raw, c->jas_nraw);
+  k_jas_raw<NORD><<<c->W, kJasThreads, 0, c->stream>>>(c->h, c->st, c->jas_raw, c->jas_nraw);
 }
 
 // Parameter derivatives of every walker at the current configurations (the
@@ -627,14 +629,14 @@ int opt_derivs(cw_ctx *c) {
     LCHK("k_jas_o");
   }
   if (c->opt_ci) {
-    k_md_ci_o<<<W, 128, 0, c->stream>>>(c->st, c->md, c->mdt, c->md_sgn, c->opt_o, c->opt_ot, c->opt_np,
+    k_md_ci_o<<<W, 128, 0, c->stream>>>(c->h, c->st, c->md, c->mdt, c->md_sgn, c->opt_o, c->opt_ot, c->opt_np,
                                         c->opt_njas);
     LCHK("k_md_ci_o");
   }
   if (c->orb_on) {
     const int nt = (int)c->orb_ideriv.size() / 2;
     const long n = (long)W * nt;
-    k_orb_o<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(c->st, nt, c->orb_terms, c->orb_nv, c->orb_vals,
+    k_orb_o<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(c->h, c->st, nt, c->orb_terms, c->orb_nv, c->orb_vals,
                                                                 c->opt_o, c->opt_ot, c->opt_np, c->opt_np - nt);
     LCHK("k_orb_o");
   }
@@ -671,7 +673,7 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     const long nwarps = (long)W * ne;
     const int bw = c->basis_warps;
     stage_begin(c, CW_ST_BASIS_ALL);
-    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->hb, c->g, e0, ne);
     stage_end(c);
     LCHK("k_basis_all");
     stage_begin(c, CW_ST_LCAO_ALL);
@@ -683,7 +685,7 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     if (c->md_on) {
       const long nt = (long)W * ne * h.Oa;
       stage_begin(c, CW_ST_SCATTER);
-      k_md_scatter<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st, c->md, c->hb.orball, e0, ne);
+      k_md_scatter<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->h, c->st, c->md, c->hb.orball, e0, ne);
       stage_end(c);
       LCHK("k_md_scatter");
     }
@@ -695,12 +697,12 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     }
     const long ns = (long)W * ne * h.nmax;
     stage_begin(c, CW_ST_SCATTER);
-    k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, c->stream>>>(c->h, c->st, c->hb, c->g, e0, ne);
     stage_end(c);
     LCHK("k_scatter_orbs");
   }
   stage_begin(c, CW_ST_SLATER_INV);
-  k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->st, c->hb, c->big_spin);
+  k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->h, c->st, c->hb, c->big_spin);
   stage_end(c);
   LCHK("k_slater_inv");
   if (h.nloc > 0 && c->md_on) {
@@ -714,7 +716,7 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     if (c->bocc)  // rows (walker, spin, slot) of slmi times the occupied coefficient rows
       dgemm(c->stream, W * N, h.K, h.nmax, c->st.slmi, c->bocc, c->hb.ctilde);
     else
-      k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->st, c->hb, c->g, c->big_spin);
+      k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->h, c->st, c->hb, c->g, c->big_spin);
     stage_end(c);
     LCHK("k_ctilde");
     stage_begin(c, CW_ST_ECP);
@@ -731,12 +733,12 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
   }
   if (c->md_on) {
     stage_begin(c, CW_ST_MDET);
-    k_md_hpsi<<<W, 128, c->smem_md_hpsi, c->stream>>>(c->st, c->md, c->mdt, c->g);
+    k_md_hpsi<<<W, 128, c->smem_md_hpsi, c->stream>>>(c->h, c->st, c->md, c->mdt, c->g);
     stage_end(c);
     LCHK("k_md_hpsi");
   }
   stage_begin(c, CW_ST_ENERGY);
-  k_energy<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->hb, mode, d_e, d_ekin);
+  k_energy<<<(W + 3) / 4, 128, 0, c->stream>>>(c->h, c->st, c->hb, mode, d_e, d_ekin);
   stage_end(c);
   LCHK("k_energy");
   return CW_OK;
@@ -867,6 +869,8 @@ int alloc_walkers(cw_ctx *c, int W) {
   if (h.nloc > 0) DALLOC(L, b.ctilde, (size_t)W * N * K);
   m.md_velo = m.md_veln = m.md_psidn = nullptr;
   b.tvpsp = nullptr;
+  b.ecp_rr = nullptr;
+  if (h.nloc > 0 && c->ecp_rr_global) DALLOC(L, b.ecp_rr, (size_t)W * N * (M | 1));
   b.md_P = nullptr;
   b.md_den = b.md_S = nullptr;
   b.md_S_ms = b.md_den_ms = nullptr;
@@ -951,7 +955,7 @@ int zerest(cw_ctx *c) {
   int rc = run_hpsi(c, 0);
   if (rc) return rc;
   const long nt = (long)W * h.N;
-  k_nearest<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st);
+  k_nearest<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->h, c->st);
   LCHK("k_nearest");
   CK(cudaMemsetAsync(c->st.sums, 0, sizeof(double) * W * 8, c->stream));
   c->ecum = c->ecm2 = c->wcum = c->pecum = c->tpbcum = c->pecm2 = c->tpbcm2 = c->acc = 0;
@@ -960,6 +964,15 @@ int zerest(cw_ctx *c) {
   c->iblk = 0;
   c->passes = 0;
   return check_status(c);
+}
+
+// one thread writes the device's global nanosecond clock when the stream
+// reaches it
+constexpr int kStampCap = 1 << 14;
+__global__ void k_stamp(unsigned long long *slot) {
+  unsigned long long ns;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ns));
+  *slot = ns;
 }
 
 }  // namespace
@@ -1025,13 +1038,12 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   }
   h.mrwf = d->mrwf; h.mpts = d->mrwf_pts; h.mbastyp = d->mbastyp;
   int m = 0;
+  std::vector<int> ao_first(d->ncent + 1);
   for (int ic = 0; ic < d->ncent; ic++) {
-    for (int k = 0; k < 3; k++) h.cent[3 * ic + k] = d->cent[3 * ic + k];
-    h.iwctype[ic] = d->iwctype[ic];
-    h.ao_first[ic] = m;
+    ao_first[ic] = m;
     m += d->nbastyp[d->iwctype[ic]];
   }
-  h.ao_first[d->ncent] = m;
+  ao_first[d->ncent] = m;
   if (m != d->nbasis) return fail(c, CW_ERR_ARG, "sum of nbastyp over centres (%d) != nbasis (%d)", m, d->nbasis);
   for (int it = 0; it < d->nctype; it++) {
     h.znuc[it] = d->znuc[it];
@@ -1107,15 +1119,21 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
       h.slm_k[l] = K_[l];
     }
   }
-  {
-    // another context's queued kernels may still read the constant block
-    cw_ctx *o = g_const_owner[device & 63];
-    if (o && o->stream) CK(cudaStreamSynchronize(o->stream));
-  }
-  CK(cudaMemcpyToSymbol(cs, &h, sizeof(CSys)));
-  g_const_owner[device & 63] = c;
   // global tables
   auto &L = c->sys_allocs;
+  {
+    double *cent;
+    int *iwct, *aof;
+    DALLOC(L, cent, 3 * (size_t)d->ncent);
+    DALLOC(L, iwct, d->ncent);
+    DALLOC(L, aof, d->ncent + 1);
+    CK(cudaMemcpy(cent, d->cent, 3 * (size_t)d->ncent * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(iwct, d->iwctype, d->ncent * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(aof, ao_first.data(), (d->ncent + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    h.cent = cent;
+    h.iwctype = iwct;
+    h.ao_first = aof;
+  }
   const size_t nt = (size_t)d->nctype * d->mrwf * d->mrwf_pts;
   double *rwf, *d2rwf, *coefT;
   int *iwl, *iwr, *slot;
@@ -1168,7 +1186,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   for (int ic = 0; ic < d->ncent; ic++) {
     const int it = d->iwctype[ic];
     for (int ib = 0; ib < d->nbastyp[it]; ib++) {
-      const int mm = h.ao_first[ic] + ib;
+      const int mm = ao_first[ic] + ib;
       aot[mm] = make_int4(ic, d->iwrwf[it * d->mbastyp + ib] - 1, it, d->iwlbas[it * d->mbastyp + ib]);
       if (aot[mm].w < 1 || aot[mm].w > 35 || aot[mm].y < 0 || aot[mm].y >= d->nrbas[it])
         return fail(c, CW_ERR_ARG, "basis pointer out of range (centre %d, AO %d)", ic, ib);
@@ -1246,7 +1264,6 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
       h.md_ivirt[s2] = ivirt[s2];
       h.md_iactv[s2] = iactv[s2];
     }
-    CK(cudaMemcpyToSymbol(cs, &h, sizeof(CSys)));
     int *dexc, *dkw;
     double *dcd;
     DALLOC(L, dexc, exc.size());
@@ -1304,13 +1321,13 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
 
 void cw_destroy(cw_ctx *c) {
   if (!c) return;
-  if (g_const_owner[c->device & 63] == c) g_const_owner[c->device & 63] = nullptr;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_dmc(c);
   free_list(c, c->w_allocs);
   drop_sweep_graph(c);
   free_list(c, c->opt_allocs);
   free_list(c, c->sys_allocs);
+  if (c->d_stamps) cudaFree(c->d_stamps);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -1370,6 +1387,30 @@ int cw_set_walkers(cw_ctx *c, int nwalk, const double *x, const uint64_t *rng) {
   return zerest(c);
 }
 
+int cw_stamp(cw_ctx *c) {
+  if (!c) return CW_ERR_ARG;
+  BIND(c);
+  if (!c->d_stamps) {
+    CK(cudaMalloc(&c->d_stamps, sizeof(unsigned long long) * kStampCap));
+    c->dev_bytes += sizeof(unsigned long long) * kStampCap;
+  }
+  if (c->nstamp >= kStampCap) return fail(c, CW_ERR_STATE, "more than %d stamps", kStampCap);
+  k_stamp<<<1, 1, 0, c->stream>>>(c->d_stamps + c->nstamp);
+  LCHK("k_stamp");
+  c->nstamp++;
+  return CW_OK;
+}
+
+int cw_stamps(cw_ctx *c, int64_t *ns, int n) {
+  if (!c || (n > 0 && !ns)) return CW_ERR_ARG;
+  const int m = std::min(n, c->nstamp);
+  if (m > 0) {
+    CK(cudaMemcpyAsync(ns, c->d_stamps, sizeof(int64_t) * m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return c->nstamp;
+}
+
 int cw_walker_status(cw_ctx *c, int32_t *status) {
   if (!c || !status) return CW_ERR_ARG;
   if (c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
@@ -1427,17 +1468,17 @@ extern "C" int cw_psie(cw_ctx *c, int iel, const double *xnew, double *psid, dou
   const int W = c->W;
   if (int rc = hook_md_prepare(c, iel)) return rc;
   CK(cudaMemcpyAsync(c->hook_buf, xnew, sizeof(double) * 3 * W, cudaMemcpyHostToDevice, c->stream));
-  k_hook_place<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->hook_buf);
+  k_hook_place<<<(W + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->hook_buf);
   LCHK("k_hook_place");
   NORD_DISPATCH(launch_jmove, c, iel);
   LCHK("k_jastrow_move");
   const int bw = c->basis_warps;
-  k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+  k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->mb, c->g);
   LCHK("k_basis_move");
   if (int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn)) return rc;
   if (int rc = md_after_lcao(c, iel)) return rc;
   double *out = c->hook_buf + (size_t)3 * W;
-  k_hook_ratio<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel, out);
+  k_hook_ratio<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->g, iel, out);
   LCHK("k_hook_ratio");
   std::vector<double> h((size_t)2 * W);
   CK(cudaMemcpyAsync(h.data(), out, sizeof(double) * 2 * W, cudaMemcpyDeviceToHost, c->stream));
@@ -1465,7 +1506,7 @@ extern "C" int cw_grad(cw_ctx *c, int iel, int iflag_move, double *vd) {
     if (int rc = hook_md_prepare(c, iel)) return rc;
   }
   double *out = c->hook_buf + (size_t)3 * W;
-  k_hook_grad<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, iel, iflag_move, out);
+  k_hook_grad<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->g, iel, iflag_move, out);
   LCHK("k_hook_grad");
   CK(cudaMemcpyAsync(vd, out, sizeof(double) * 3 * W, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1480,7 +1521,7 @@ extern "C" int cw_commit(cw_ctx *c, int iel, const int32_t *accept) {
   BIND(c);
   const int W = c->W;
   CK(cudaMemcpyAsync(c->hook_acc, accept, sizeof(int) * W, cudaMemcpyHostToDevice, c->stream));
-  k_hook_accept<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, iel, c->hook_acc);
+  k_hook_accept<<<(W + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, c->mb, iel, c->hook_acc);
   LCHK("k_hook_accept");
   launch_commit(c, iel);
   LCHK("k_commit");
@@ -1509,14 +1550,15 @@ int vmc_sweep(cw_ctx *c) {
   const int W = c->W;
   if (h.nloc > 0) {
     stage_begin(c, CW_ST_ROTQUA);
-    k_rotqua<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st);
+    k_rotqua<<<(W + 127) / 128, 128, 0, c->stream>>>(c->h, c->st);
     stage_end(c);
     LCHK("k_rotqua");
   }
   for (int i = 0; i < h.N; i++) {
     if (int rc = md_before_propose(c, i)) return rc;
     stage_begin(c, CW_ST_PROPOSE);
-    k_propose<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, i);
+    k_propose<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, c->mb, i,
+                                                                  c->smem_commit ? c->acc_count : nullptr);
     stage_end(c);
     LCHK("k_propose");
     stage_begin(c, CW_ST_JASTROW_MOVE);
@@ -1525,7 +1567,7 @@ int vmc_sweep(cw_ctx *c) {
     LCHK("k_jastrow_move");
     const int bw = c->basis_warps;
     stage_begin(c, CW_ST_BASIS_MOVE);
-    k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+    k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->mb, c->g);
     stage_end(c);
     LCHK("k_basis_move");
     stage_begin(c, CW_ST_LCAO_MOVE);
@@ -1536,11 +1578,12 @@ int vmc_sweep(cw_ctx *c) {
     }
     if (int rc = md_after_lcao(c, i)) return rc;
     stage_begin(c, CW_ST_ACCEPT);
-    k_decide<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->st, c->mb, c->g, i);
+    k_decide<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->g, i,
+                                                                 c->smem_commit ? c->acc_list : nullptr, c->acc_count);
     stage_end(c);
     LCHK("k_decide");
     stage_begin(c, CW_ST_COMMIT);
-    launch_commit(c, i);
+    launch_commit(c, i, true);
     stage_end(c);
     LCHK("k_commit");
     if (int rc = md_after_commit(c, i)) return rc;
@@ -1925,7 +1968,7 @@ int cw_orbitals(cw_ctx *c, double *orb, double *dorb, double *ddorb) {
     const int ne = std::min(ec, N - e0);
     const long nwarps = (long)W * ne;
     const int bw = c->basis_warps;
-    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->hb, c->g, e0, ne);
+    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->hb, c->g, e0, ne);
     LCHK("k_basis_all");
     {
       int rc = lcao(c, false, W * ne * 5, c->hb.phi, c->hb.orball);
@@ -2149,7 +2192,7 @@ int noalloc_scratch(cw_ctx *c, double **p) {
 
 // basis functions (value, gradient, Laplacian) of npts points, thread per
 // (point, centre); rows (p*5 + d) of phi, as k_basis_all writes them.
-__global__ void k_basis_points(GSys g, int npts, const double *__restrict__ xyz, double *__restrict__ phi) {
+__global__ void k_basis_points(const __grid_constant__ CSys cs, GSys g, int npts, const double *__restrict__ xyz, double *__restrict__ phi) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int M = cs.M, K = cs.K;
   if (t >= (long)npts * M) return;
@@ -2158,7 +2201,7 @@ __global__ void k_basis_points(GSys g, int npts, const double *__restrict__ xyz,
   const double xc[3] = {xyz[3 * p] - cs.cent[3 * ic], xyz[3 * p + 1] - cs.cent[3 * ic + 1],
                         xyz[3 * p + 2] - cs.cent[3 * ic + 2]};
   double *row = phi + (size_t)p * 5 * K;
-  basis_centre(g, ic, xc, 2, [&](int a, int d, double v) { row[(size_t)d * K + a] = v; });
+  basis_centre(cs, g, ic, xc, 2, [&](int a, int d, double v) { row[(size_t)d * K + a] = v; });
 }
 }  // namespace
 
@@ -2177,7 +2220,7 @@ extern "C" int cw_orbitals_noalloc(cw_ctx *c, int npts, const double *xyz, doubl
   int rc = noalloc_scratch(c, &phi);
   if (rc) return rc;
   const long nt = (long)npts * h.M;
-  k_basis_points<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->g, npts, xyz, phi);
+  k_basis_points<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->h, c->g, npts, xyz, phi);
   LCHK("k_basis_points");
   dgemm(c->stream, npts * 5, h.Oa, h.K, phi, c->g.coefT, out);
   LCHK("dgemm(noalloc)");
@@ -2300,10 +2343,10 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
   d.wdsumo = nwalk;
   const DmcScalars sc{tau, etrial, d.eest, 1.0, 1.0};
   if (c->md_on) {
-    k_md_drift_all<<<(unsigned)(((long)nwalk * N + 3) / 4), 128, 0, c->stream>>>(c->st, c->md, c->g, c->md_vall);
+    k_md_drift_all<<<(unsigned)(((long)nwalk * N + 3) / 4), 128, 0, c->stream>>>(c->h, c->st, c->md, c->g, c->md_vall);
     LCHK("k_md_drift_all");
   }
-  k_dmc_weights<<<(nwalk + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 0, c->md_vall);
+  k_dmc_weights<<<(nwalk + 3) / 4, 128, 0, c->stream>>>(c->h, c->st, b, sc, 0, c->md_vall);
   LCHK("k_dmc_weights(init)");
   for (int w = 0; w < nwalk; w++) d.h_wt[w] = 1.0;
   CK(cudaMemcpyAsync(b.wt, d.h_wt, sizeof(double) * nwalk, cudaMemcpyHostToDevice, c->stream));
@@ -2390,7 +2433,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
         q.z[iq] = h.xq0[iq] * f[2] + h.yq0[iq] * f[5] + h.zq0[iq] * f[8];
       }
       stage_begin(c, CW_ST_ROTQUA);
-      k_set_quad<<<(W + 127) / 128, 128, 0, c->stream>>>(c->st, q);
+      k_set_quad<<<(W + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, q);
       stage_end(c);
       LCHK("k_set_quad");
     }
@@ -2407,7 +2450,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
     for (int i = 0; i < h.N; i++) {
       if (int rc = md_before_propose(c, i)) return rc;
       stage_begin(c, CW_ST_PROPOSE);
-      k_dmc_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, b, sc, i);
+      k_dmc_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, b, sc, i);
       stage_end(c);
       LCHK("k_dmc_propose");
       stage_begin(c, CW_ST_JASTROW_MOVE);
@@ -2416,7 +2459,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       LCHK("k_jastrow_move");
       const int bw = c->basis_warps;
       stage_begin(c, CW_ST_BASIS_MOVE);
-      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->mb, c->g);
       stage_end(c);
       LCHK("k_basis_move");
       stage_begin(c, CW_ST_LCAO_MOVE);
@@ -2427,7 +2470,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       }
       if (int rc = md_after_lcao(c, i)) return rc;
       stage_begin(c, CW_ST_ACCEPT);
-      k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, b, sc, i);
+      k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, c->g, b, sc, i);
       stage_end(c);
       LCHK("k_dmc_decide");
       stage_begin(c, CW_ST_COMMIT);
@@ -2442,18 +2485,18 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
     if (rc) return rc;
     if (c->md_on) {
       stage_begin(c, CW_ST_MDET);
-      k_md_drift_all<<<(unsigned)(((long)W * h.N + 3) / 4), 128, 0, c->stream>>>(c->st, c->md, c->g, c->md_vall);
+      k_md_drift_all<<<(unsigned)(((long)W * h.N + 3) / 4), 128, 0, c->stream>>>(c->h, c->st, c->md, c->g, c->md_vall);
       stage_end(c);
       LCHK("k_md_drift_all");
     }
     stage_begin(c, CW_ST_DMC_WEIGHTS);
-    k_dmc_weights<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, b, sc, 1, c->md_vall);
+    k_dmc_weights<<<(W + 3) / 4, 128, 0, c->stream>>>(c->h, c->st, b, sc, 1, c->md_vall);
     stage_end(c);
     LCHK("k_dmc_weights");
     if (d.icasula == -1) {
       // T-moves (dmc_ps :701-735): choice, then the forced move of each walker's electron
       stage_begin(c, CW_ST_TMOVE);
-      k_tmove_select<<<(W + 3) / 4, 128, 0, c->stream>>>(c->st, c->mb, c->hb.tvpsp, sc);
+      k_tmove_select<<<(W + 3) / 4, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->hb.tvpsp, sc);
       stage_end(c);
       LCHK("k_tmove_select");
       stage_begin(c, CW_ST_JASTROW_MOVE);
@@ -2462,7 +2505,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       LCHK("k_jastrow_move(tmove)");
       const int bw = c->basis_warps;
       stage_begin(c, CW_ST_BASIS_MOVE);
-      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->st, c->mb, c->g);
+      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->mb, c->g);
       stage_end(c);
       LCHK("k_basis_move(tmove)");
       stage_begin(c, CW_ST_LCAO_MOVE);
@@ -2472,7 +2515,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
         if (rc2) return rc2;
       }
       stage_begin(c, CW_ST_TMOVE);
-      k_tmove_accept<<<(W + 63) / 64, 64, 0, c->stream>>>(c->st, c->mb, c->g, b);
+      k_tmove_accept<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, c->g, b);
       stage_end(c);
       LCHK("k_tmove_accept");
       stage_begin(c, CW_ST_COMMIT);
@@ -2789,7 +2832,7 @@ int ck_restore(cw_ctx *c, const uint8_t *buf, size_t n) {
   rc = run_hpsi(c, 0);
   if (rc) return rc;
   const long nt = (long)W * N;
-  k_nearest<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->st);
+  k_nearest<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->h, c->st);
   LCHK("k_nearest");
   CK(cudaMemcpyAsync(c->st.sums, sums.data(), sizeof(double) * sums.size(), cudaMemcpyHostToDevice, c->stream));
   c->ecum = vg[0]; c->ecm2 = vg[1]; c->wcum = vg[2]; c->pecum = vg[3]; c->tpbcum = vg[4];

@@ -14,7 +14,7 @@ namespace cw {
 // nearest centre (metrop6's rminn, nearestn, rvminn, kept for the next
 // proposal around it) is found as the reference does (first minimum of the
 // squared distance, vmc/metrop_mov1_slat.f90:327-340).
-__global__ void k_hook_place(WState st, MoveBuf mb, const double *__restrict__ xnew) {
+__global__ void k_hook_place(const __grid_constant__ CSys cs, WState st, MoveBuf mb, const double *__restrict__ xnew) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   MoveScratch &m = mb.ms[w];
@@ -45,13 +45,13 @@ __global__ void k_hook_place(WState st, MoveBuf mb, const double *__restrict__ x
 // moved electron's new orbital row (determinante, vmc/determinante.f90:40-46,
 // the same group dot product as k_decide), psi_D at the point and J there.
 // out [W][2] = (psid, psij).  kMoveGroup lanes per walker.
-__global__ void __launch_bounds__(128) k_hook_ratio(WState st, MoveBuf mb, GSys g, int iel, double *out) {
+__global__ void __launch_bounds__(128) k_hook_ratio(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, int iel, double *out) {
   const int lane = threadIdx.x & (kMoveGroup - 1);
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) / kMoveGroup;
   if (w >= st.W) return;
   const int nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
-  spin_of(iel, iab, nel, ish);
+  spin_of(cs, iel, iab, nel, ish);
   const int iloc = iel - ish;
   const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * iloc;
   const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
@@ -74,14 +74,14 @@ __global__ void __launch_bounds__(128) k_hook_ratio(WState st, MoveBuf mb, GSys 
 // gradient, + the multideterminant correction), 0 at the point of the last
 // psie (the updated inverse column slmi/ratio . the new orbital gradients).
 // The sums run in the order of k_propose and k_decide.  out [W][3].
-__global__ void __launch_bounds__(128) k_hook_grad(WState st, MoveBuf mb, GSys g, int iel, int iflag_move,
+__global__ void __launch_bounds__(128) k_hook_grad(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, int iel, int iflag_move,
                                                    double *out) {
   const int lane = threadIdx.x & (kMoveGroup - 1);
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) / kMoveGroup;
   if (w >= st.W) return;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
-  spin_of(iel, iab, nel, ish);
+  spin_of(cs, iel, iab, nel, ish);
   const int iloc = iel - ish;
   const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * iloc;
   double v[3];
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(128) k_hook_grad(WState st, MoveBuf mb, GSys g
 // centre and the determinant take the point's values; k_commit then applies
 // detsav and jassav to those walkers (the others keep their tables, which
 // is distancese_restore: the engine never overwrote them).
-__global__ void k_hook_accept(WState st, MoveBuf mb, int iel, const int *__restrict__ accept) {
+__global__ void k_hook_accept(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel, const int *__restrict__ accept) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   MoveScratch &m = mb.ms[w];

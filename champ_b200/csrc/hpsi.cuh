@@ -33,6 +33,7 @@ struct HBuf {
   float *phi_hi, *phi_lo;  // mixed precision: [rows][kp] split chunk basis (null in FP64)
   int kp;
   double *tvpsp;           // [W][N][nquad][M] T-move matrix elements (null without T-moves)
+  double *ecp_rr;          // [W][N][M|1] k_ecp's scaled e-n distances where they do not fit shared memory (else null)
   // multideterminant (null for one determinant)
   double *md_P;            // [W][N][K] pseudopotential quadrature basis sums
   const double *md_den;    // [W][2] energy / kinetic corrections
@@ -88,7 +89,7 @@ constexpr int kEnFields = 5;
 // pairs stay FP64.  Four CTAs per SM in both arithmetics (the FP32 build at
 // five spilled and ran 9% slower).
 template <int NORD, typename T>
-__global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
+__global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__ CSys cs, WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M, MN = M * N;
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
       const double v0 = sx[e] - cs.cent[3 * ic], v1 = sx[N + e] - cs.cent[3 * ic + 1], v2 = sx[2 * N + e] - cs.cent[3 * ic + 2];
       const double r2 = v0 * v0 + v1 * v1 + v2 * v2, r = sqrt(r2);
       double rr, dd1, dd2;
-      scale2<double>(r, rr, dd1, dd2);
+      scale2<double>(cs, r, rr, dd1, dd2);
       const int t = ic * N + e;
       tab[t] = rr;
       tab[MN + t] = -kap * dd1;
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
       }
       if (rr == asym) continue;
       double fen, feni, fenii;
-      en_term<2, double>(cs.iwctype[ic], rr, fen, feni, fenii);
+      en_term<2, double>(cs, cs.iwctype[ic], rr, fen, feni, fenii);
       fenii = fenii * dd1 * dd1 + feni * dd2;
       feni = feni * dd1 / r;
       fs += fen;
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
 #pragma unroll
       for (int f = 0; f < kEnFields; f++) q[f] = tab[f * MN + ic * N + i];
       for (int k = 0; k < 3; k++) q[kEnFields + k] = sx[k * N + i] - cs.cent[3 * ic + k];
-      if (NORD > 1) een_fold2<NORD, T>(een_coef<T>(cs.iwctype[ic]), T(1 - kap * q[0]), sB + (size_t)t * 4 * NB);
+      if (NORD > 1) een_fold2<NORD, T>(een_coef<T>(cs, cs.iwctype[ic]), T(1 - kap * q[0]), sB + (size_t)t * 4 * NB);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < npa + npb; t += blockDim.x) {
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
       const int i = row == 0 ? ia : ib, j = row == 0 ? t : t - npa;
       int isb, ipar;
       double sspinn;
-      pair_spin(i, j, isb, ipar, sspinn);
+      pair_spin(cs, i, j, isb, ipar, sspinn);
       const double xj[3] = {sx[j], sx[N + j], sx[2 * N + j]};
       const double rv[3] = {sx[i] - xj[0], sx[N + i] - xj[1], sx[2 * N + i] - xj[2]};
       const double rij2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2], rij = sqrt(rij2);
@@ -184,11 +185,11 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
       const T rijT = (T)rij, irijT = (T)irij, rij2T = (T)rij2;
       const T rvT[3] = {(T)rv[0], (T)rv[1], (T)rv[2]};
       T u, dd1, dd2;
-      scale2<T>(rijT, u, dd1, dd2);
+      scale2<T>(cs, rijT, u, dd1, dd2);
       T fs = 0, d2 = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
       if (u != (T)cs.asymp_r) {
         T fee, feeu, feeuu;
-        ee_term<2, T>(isb, ipar, (T)sspinn, u, fee, feeu, feeuu);
+        ee_term<2, T>(cs, isb, ipar, (T)sspinn, u, fee, feeu, feeuu);
         feeuu = feeuu * dd1 * dd1 + feeu * dd2;
         feeu = feeu * dd1 * irijT;
         fs += fee;
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(WState st, HBuf hb) {
 // basis functions with Laplacian for electrons [e0, e0+ne): warp per
 // (walker, electron); rows ((w*ne + e)*5 + d).
 // ---------------------------------------------------------------------------
-__global__ void k_basis_all(WState st, HBuf hb, GSys g, int e0, int ne) {
+__global__ void k_basis_all(const __grid_constant__ CSys cs, WState st, HBuf hb, GSys g, int e0, int ne) {
   extern __shared__ __align__(16) double smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -289,13 +290,13 @@ __global__ void k_basis_all(WState st, HBuf hb, GSys g, int e0, int ne) {
   const double x[3] = {st.x[((size_t)w * 3 + 0) * N + e], st.x[((size_t)w * 3 + 1) * N + e],
                        st.x[((size_t)w * 3 + 2) * N + e]};
   double *rec = smem + (size_t)wib * cs.M * kCenRec;
-  warp_basis_prepass<2>(g, x, rec, lane);
+  warp_basis_prepass<2>(cs, g, x, rec, lane);
   __syncwarp();
   if (hb.phi_hi) {
     const int kp = hb.kp;
     float *hi = hb.phi_hi + ((size_t)gw * 5) * kp, *lo = hb.phi_lo + ((size_t)gw * 5) * kp;
     for (int m = lane; m < K; m += 32)
-      warp_basis_ao<2>(g, rec, m, [&](int a, int d, double v) {
+      warp_basis_ao<2>(cs, g, rec, m, [&](int a, int d, double v) {
         float h, l;
         split_tf32(v, h, l);
         hi[(size_t)d * kp + a] = h;
@@ -305,10 +306,10 @@ __global__ void k_basis_all(WState st, HBuf hb, GSys g, int e0, int ne) {
   }
   double *phi = hb.phi + ((size_t)gw * 5) * K;
   for (int m = lane; m < K; m += 32)
-    warp_basis_ao<2>(g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
+    warp_basis_ao<2>(cs, g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
 }
 
-__global__ void k_scatter_orbs(WState st, HBuf hb, GSys g, int e0, int ne) {
+__global__ void k_scatter_orbs(const __grid_constant__ CSys cs, WState st, HBuf hb, GSys g, int e0, int ne) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   if (t >= (long)st.W * ne * nmax) return;
@@ -331,7 +332,7 @@ __global__ void k_scatter_orbs(WState st, HBuf hb, GSys g, int e0, int ne) {
 // in_place: the factorisation runs in the walker's slmi block in global
 // memory (L2-resident) instead of shared memory, for spins too large for
 // shared memory (same arithmetic; shared memory then holds col only).
-__global__ void k_slater_inv(WState st, HBuf hb, int in_place) {
+__global__ void k_slater_inv(const __grid_constant__ CSys cs, WState st, HBuf hb, int in_place) {
   const int w = blockIdx.x >> 1, iab = blockIdx.x & 1;
   if (w >= st.W) return;
   const int N = cs.N, nmax = cs.nmax;
@@ -494,7 +495,7 @@ __global__ void k_slater_inv(WState st, HBuf hb, int in_place) {
 // ---------------------------------------------------------------------------
 // s_global: the inverse is read from global memory (L2) rather than staged
 // in shared memory, for spins too large for shared memory
-__global__ void k_ctilde(WState st, HBuf hb, GSys g, int s_global) {
+__global__ void k_ctilde(const __grid_constant__ CSys cs, WState st, HBuf hb, GSys g, int s_global) {
   const int nchunk = (cs.K + 63) / 64;
   const int b = blockIdx.x;
   const int chunk = b % nchunk, iab = (b / nchunk) & 1, w = b / (2 * nchunk);
@@ -528,12 +529,12 @@ __global__ void k_ctilde(WState st, HBuf hb, GSys g, int s_global) {
 // Pseudopotential: CTA per walker, warps over (pair, quadrature point).
 // ---------------------------------------------------------------------------
 template <int NORD>
-__device__ __forceinline__ double psinl_d(double u, double rri, double rrj, int it) {
+__device__ __forceinline__ double psinl_d(const CSys &cs, double u, double rri, double rrj, int it) {
   if (rri == cs.asymp_r && rrj == cs.asymp_r) return 0.0;
   const double k = cs.scalek;
   return een_poly<NORD, 0, double>(&cs.c[it * CW_MAX_TERMS], 1 - k * u, 1 - k * rri, 1 - k * rrj).fc;
 }
-__device__ __forceinline__ double psianl_d(double rri, int it) {
+__device__ __forceinline__ double psianl_d(const CSys &cs, double rri, int it) {
   if (rri == cs.asymp_r) return 0.0;
   const int na = cs.norda + 1;
   double v = cs.a4[it * na] * rri / (1.0 + cs.a4[it * na + 1] * rri) - cs.asymp_jasa[it];
@@ -545,7 +546,7 @@ __device__ __forceinline__ double psianl_d(double rri, int it) {
   return v;
 }
 template <typename T>
-__device__ __forceinline__ T psibnl_t(T u, int isb, int ipar, T sspinn) {
+__device__ __forceinline__ T psibnl_t(const CSys &cs, T u, int isb, int ipar, T sspinn) {
   if (u == (T)cs.asymp_r) return 0;
   const int nb = cs.nordb + 1;
   T fee = (T)cs.b[isb * nb] * u / (1 + (T)cs.b[isb * nb + 1] * u);
@@ -557,8 +558,8 @@ __device__ __forceinline__ T psibnl_t(T u, int isb, int ipar, T sspinn) {
   }
   return v;
 }
-__device__ __forceinline__ double psibnl_d(double u, int isb, int ipar, double sspinn) {
-  return psibnl_t<double>(u, isb, ipar, sspinn);
+__device__ __forceinline__ double psibnl_d(const CSys &cs, double u, int isb, int ipar, double sspinn) {
+  return psibnl_t<double>(cs, u, isb, ipar, sspinn);
 }
 
 // Shared-memory plan of k_ecp (in doubles, every region 16-byte aligned):
@@ -569,8 +570,8 @@ __device__ __forceinline__ double psibnl_d(double u, int isb, int ipar, double s
 //   its basis prepass [M][kCenRec] and, for multideterminant wave functions,
 //   its basis values [K] (reused by the pseudopotential B matrix).
 constexpr int kEcpMaxWarps = 16;
-__host__ __device__ inline size_t ecp_base_doubles(int N, int M, int cap) {
-  const size_t b = (size_t)N * (M | 1) + 3 * (size_t)N + 3 * (size_t)cap + (size_t)(cap + 1) / 2;
+__host__ __device__ inline size_t ecp_base_doubles(int N, int M, int cap, int rr_global) {
+  const size_t b = (rr_global ? 0 : (size_t)N * (M | 1)) + 3 * (size_t)N + 3 * (size_t)cap + (size_t)(cap + 1) / 2;
   return b + (b & 1);
 }
 __host__ __device__ inline size_t ecp_warp_doubles(int M, int nb, int tbytes, int naov) {
@@ -592,7 +593,7 @@ __host__ __device__ inline size_t ecp_warp_doubles(int M, int nb, int tbytes, in
 // holds at most blockDim entries; a walker with more active pairs is
 // processed in several passes, in the same order.
 template <int NORD, typename T, int MINB>  // MINB: blocks per SM the register budget is set for
-__global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf hb, GSys g) {
+__global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(const __grid_constant__ CSys cs, WState st, HBuf hb, GSys g) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M, K = cs.K, NQ = cs.nquad, NM = N * M;
@@ -600,13 +601,14 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
   constexpr int NB = 2 * ((een_nb(NORD) + 1) / 2);
   extern __shared__ __align__(16) double smem[];
   const int MS = M | 1;                         // row stride of rr_en
-  double *rr_en = smem;                         // [N][MS]
-  double *sx = rr_en + (size_t)N * MS;          // [3][N]
+  const int rrg = hb.ecp_rr != nullptr;         // rr_en in global memory (large molecules)
+  double *rr_en = rrg ? hb.ecp_rr + (size_t)w * N * MS : smem;  // [N][MS]
+  double *sx = smem + (rrg ? 0 : (size_t)N * MS);              // [3][N]
   double *lst_v = sx + 3 * N;                   // [cap][3] non-local channel potentials
   int *lst_ie = reinterpret_cast<int *>(lst_v + 3 * cap);  // [cap] i*M + ic
   const int naov = hb.md_P ? K : 0;
   const size_t wsd = ecp_warp_doubles(M, NB, (int)sizeof(T), naov);
-  double *wsp = smem + ecp_base_doubles(N, M, cap) + (size_t)wid * wsd;
+  double *wsp = smem + ecp_base_doubles(N, M, cap, rrg) + (size_t)wid * wsd;
   double *rq = wsp;                             // [M]
   T *bq = reinterpret_cast<T *>(wsp + M + (M & 1));  // [M][NB]
   double *aov = wsp + wsd - (naov + (naov & 1));      // [K] basis values (multideterminant)
@@ -621,7 +623,7 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
     const int jj = t / M, jc = t % M;
     const Cen cc = cen_of(g, jc);
     const double d0 = sx[jj] - cc.x, d1 = sx[N + jj] - cc.y, d2 = sx[2 * N + jj] - cc.z;
-    rr_en[jj * MS + jc] = scale0<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+    rr_en[jj * MS + jc] = scale0<double>(cs, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
   }
   const double *xqw = st.xq + (size_t)w * 3 * NQ;
   const double *fso = st.fso + (size_t)w * N * N;
@@ -640,11 +642,11 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
         const double d0 = sx[i] - cc.x, d1 = sx[N + i] - cc.y, d2 = sx[2 * N + i] - cc.z;
         const double r = fmax(1.0e-10, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
         const int lp = cs.lpot[ict];
-        vl = gauss_pot_d(r, lp, ict) - cs.znuc[ict] * (1.0 / r);
+        vl = gauss_pot_d(cs, r, lp, ict) - cs.znuc[ict] * (1.0 / r);
 #pragma unroll
         for (int l = 1; l <= 3; l++) {
           if (l <= lp - 1) {
-            v[l - 1] = gauss_pot_d(r, l, ict);
+            v[l - 1] = gauss_pot_d(cs, r, l, ict);
             if (fabs(v[l - 1]) > 1.0e-4) flag = 1;
           }
         }
@@ -689,18 +691,18 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
         double xc[3] = {xp[0] - cc.x, xp[1] - cc.y, xp[2] - cc.z};
         double r = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
         if (jc == ic) r = rin;
-        rq[jc] = scale0<double>(r);
+        rq[jc] = scale0<double>(cs, r);
         if (NORD > 1)
-          een_fold0<NORD, T>(een_coef<T>(cc.it), T(1 - cs.scalek * rq[jc]), bq + (size_t)jc * NB);
+          een_fold0<NORD, T>(een_coef<T>(cs, cc.it), T(1 - cs.scalek * rq[jc]), bq + (size_t)jc * NB);
       }
-      warp_basis_prepass<0>(g, xp, rec, lane);
+      warp_basis_prepass<0>(cs, g, xp, rec, lane);
       __syncwarp();
       // determinant ratio (nonlocd_quad) via c~: basis values (ider=0) of the
       // point contracted on the fly
       const double *ct = hb.ctilde + ((size_t)w * N + i) * K;
       double dr = 0;
       for (int m = lane; m < K; m += 32)
-        warp_basis_ao<0>(g, rec, m, [&](int, int, double v) {
+        warp_basis_ao<0>(cs, g, rec, m, [&](int, int, double v) {
           dr += v * ct[m];
           if (naov) aov[m] = v;
         });
@@ -712,11 +714,11 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
         const int pi = jj < i ? i : jj, pj = jj < i ? jj : i;
         int isb, ipar;
         double sspinn;
-        pair_spin(pi, pj, isb, ipar, sspinn);
+        pair_spin(cs, pi, pj, isb, ipar, sspinn);
         const double dx0 = sx[jj] - xp[0], dx1 = sx[N + jj] - xp[1], dx2 = sx[2 * N + jj] - xp[2];
         const double rij = sqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
-        const T u = scale0<T>((T)rij);
-        T f = psibnl_t<T>(u, isb, ipar, (T)sspinn);
+        const T u = scale0<T>(cs, (T)rij);
+        T f = psibnl_t<T>(cs, u, isb, ipar, (T)sspinn);
         if (NORD > 1) {
           // psinl (vmc/nonlpsi.f90:4) through the folded coefficients of the point
           const T kT = (T)cs.scalek, z = 1 - kT * u;
@@ -732,7 +734,7 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
         fsum += (double)f - fso[(size_t)i * N + jj];
       }
       double fen = 0;
-      for (int jc = lane; jc < M; jc += 32) fen += psianl_d(rq[jc], cs.iwctype[jc]);
+      for (int jc = lane; jc < M; jc += 32) fen += psianl_d(cs, rq[jc], cs.iwctype[jc]);
       fsum = warp_sum(fsum) + (warp_sum(fen) - fso[(size_t)i * N + i]);
       double term = 0;
       for (int l = 1; l <= cs.lpot[ict] - 1; l++) term += yl0_d(l, costh) * lst_v[3 * a + (l - 1)];
@@ -773,7 +775,7 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(WState st, HBuf
 // E_L assembly + metrop6's per-step sums (warp per walker).
 // mode: 0 = hpsi only (zerest, parity hook), 1 = end of a metrop6 sweep
 // ---------------------------------------------------------------------------
-__global__ void k_energy(WState st, HBuf hb, int mode, double *out_e, double *out_ekin) {
+__global__ void k_energy(const __grid_constant__ CSys cs, WState st, HBuf hb, int mode, double *out_e, double *out_ekin) {
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= st.W) return;
@@ -818,7 +820,7 @@ __global__ void k_energy(WState st, HBuf hb, int mode, double *out_e, double *ou
   st.psido[w] = psid;
   st.psijo[w] = psij;
   // guiding function (metrop6 :652-657, :732): psi2g from the S of every state
-  const double psi2g = (cs.iguiding > 0 && hb.md_S_ms) ? md_psig(hb.md_S_ms + (size_t)w * cs.nstates, cs.nstates) : 1.0;
+  const double psi2g = (cs.iguiding > 0 && hb.md_S_ms) ? md_psig(cs, hb.md_S_ms + (size_t)w * cs.nstates, cs.nstates) : 1.0;
   st.psi2o[w] = log(fabs(psi2g)) + 2 * (log(fabs(psid)) + psij);
   if (!isfinite(energy)) st.status[w] |= 2;
   if (out_e) out_e[w] = energy;
@@ -899,7 +901,7 @@ __host__ __device__ inline void rotqua_frame(DRng &rng, double f[9]) {
   f[6] = yy1 * u2 - zz1 * u1; f[7] = yy2 * u2 - zz2 * u1; f[8] = yy3 * u2 - zz3 * u1;
 }
 
-__global__ void k_rotqua(WState st) {
+__global__ void k_rotqua(const __grid_constant__ CSys cs, WState st) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   DRng rng;
@@ -917,7 +919,7 @@ __global__ void k_rotqua(WState st) {
 }
 
 // zerest's nearest-nucleus tables: thread per (walker, electron)
-__global__ void k_nearest(WState st) {
+__global__ void k_nearest(const __grid_constant__ CSys cs, WState st) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int N = cs.N;
   if (t >= (long)st.W * N) return;

@@ -77,6 +77,20 @@ __device__ __forceinline__ const int *md_exc(const MdTab &t, int s, int kk) {
   return t.exc + ((size_t)s * t.numax + kk) * (1 + 2 * CW_MD_MEX);
 }
 
+// One excitation entry and its phase weight G held in registers, so that a
+// loop over the unique spin-determinants loads the next entry while it
+// solves the current one (the table and G come from L2 / DRAM).
+struct MdExcPf {
+  int e[1 + 2 * CW_MD_MEX];
+  double g;
+  __device__ __forceinline__ void load(const MdTab &tab, int s, int kk, const double *G) {
+    const int *p = md_exc(tab, s, kk);
+#pragma unroll
+    for (int i = 0; i < 1 + 2 * CW_MD_MEX; i++) e[i] = __ldg(p + i);
+    g = G[kk];
+  }
+};
+
 // Gauss-Jordan with partial pivoting on the NR x NR excitation matrix
 // a[ir][jr] = aa[rc[ir]][ro[jr]] held in registers (row swaps by select, no
 // dynamic indexing); with INV the inverse is left in b (b[r][k] =
@@ -351,7 +365,7 @@ __device__ __forceinline__ double md_block_sum(double v, double *red) {
 }
 
 // orbital rows of every orbital and the kinetic B of one electron chunk
-__global__ void k_md_scatter(WState st, MdBuf md, const double *orball, int e0, int ne) {
+__global__ void k_md_scatter(const __grid_constant__ CSys cs, WState st, MdBuf md, const double *orball, int e0, int ne) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int N = cs.N, O = cs.Oa;
   if (t >= (long)st.W * ne * O) return;
@@ -370,7 +384,7 @@ __global__ void k_md_scatter(WState st, MdBuf md, const double *orball, int e0, 
 }
 
 // G_s (and its kref-equivalent part) from the other spin's ratios; smem-free
-__device__ void md_form_G(const MdTab &tab, const MdBuf &md, int w, int s, double *G, double *red,
+__device__ void md_form_G(const CSys &cs, const MdTab &tab, const MdBuf &md, int w, int s, double *G, double *red,
                           const double *cdet) {
   const int NU = cs.md_nuniq[s];
   for (int kk = threadIdx.x; kk <= NU; kk += blockDim.x) G[kk] = 0.0;
@@ -389,7 +403,7 @@ __device__ void md_form_G(const MdTab &tab, const MdBuf &md, int w, int s, doubl
 }
 
 // Y_s into shared memory Y[n][O] from aa (row stride O), ratios dd and G
-__device__ void md_form_Y(const MdTab &tab, int s, const double *aa, const double *dd, const double *G, double *Y) {
+__device__ void md_form_Y(const CSys &cs, const MdTab &tab, int s, const double *aa, const double *dd, const double *G, double *Y) {
   const int n = s == 0 ? cs.nup : cs.ndn, O = cs.Oa, NU = cs.md_nuniq[s];
   for (int t = threadIdx.x; t < n * O; t += blockDim.x) Y[t] = 0.0;
   __syncthreads();
@@ -419,7 +433,7 @@ __device__ void md_form_Y(const MdTab &tab, int s, const double *aa, const doubl
 // gradients b_k[v] of every orbital at the electron, aa and Y (row stride
 // O); lanes of one warp over the virtual orbitals.  Returns the
 // detratio-scaled sum on every lane.
-__device__ void md_velocity_warp(int s, const double *c, const double *b0, const double *b1, const double *b2,
+__device__ void md_velocity_warp(const CSys &cs, int s, const double *c, const double *b0, const double *b1, const double *b2,
                                  int bstride_slot /*1*/, const double *aa, const double *Y, const int *slot_orb,
                                  double detratio, double vel[3]) {
   const int n = s == 0 ? cs.nup : cs.ndn, O = cs.Oa;
@@ -451,7 +465,7 @@ __device__ void md_velocity_warp(int s, const double *c, const double *b0, const
 // hpsi part: CTA (128 threads) per walker.  Shared: slmi of one spin (n*n),
 // X and X_kin (n*n each), Y (n*O), G (numax+1), reduction scratch.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab, GSys g) {
+__global__ void __launch_bounds__(128) k_md_hpsi(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, GSys g) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
@@ -544,8 +558,8 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
     const int nv = O - ivirt, na = n - iactv;
     if (ns == 1) {
       // one state: Y first, then tildem contracted with it on the fly
-      md_form_G(tab, md, w, s, G, red, tab.cdet);
-      md_form_Y(tab, s, aa, dd, G, Y);
+      md_form_G(cs, tab, md, w, s, G, red, tab.cdet);
+      md_form_Y(cs, tab, s, aa, dd, G, Y);
       double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
       for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
     }
@@ -582,8 +596,8 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
       continue;
     }
     for (int stt = 0; stt < ns; stt++) {
-      md_form_G(tab, md, w, s, G, red, tab.cdet + (size_t)stt * cs.ndet);
-      md_form_Y(tab, s, aa, dd, G, Y);
+      md_form_G(cs, tab, md, w, s, G, red, tab.cdet + (size_t)stt * cs.ndet);
+      md_form_Y(cs, tab, s, aa, dd, G, Y);
       if (stt == 0) {
         double *yg = md.ymat + ((size_t)w * 2 + s) * nmax * O;
         for (int t = threadIdx.x; t < n * O; t += blockDim.x) yg[t] = Y[t];
@@ -623,7 +637,7 @@ __global__ void __launch_bounds__(128) k_md_hpsi(WState st, MdBuf md, MdTab tab,
 // overlap GEMM).  CTA per walker.
 // (columns off .. off+ndet-1 of the optimisation vector o, row stride np,
 // and the same rows of its transpose ot [np][W])
-__global__ void k_md_ci_o(WState st, MdBuf md, MdTab tab, const double *sgn, double *o, double *ot, int np,
+__global__ void k_md_ci_o(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, const double *sgn, double *o, double *ot, int np,
                           int off) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
@@ -668,7 +682,7 @@ __global__ void k_md_zero(double *p, size_t n) {
 
 // drift operands t_k[v] = b_k[v] - sum_j b_k[occ_j] aa[j][v] of one
 // electron (multideterminante_grad's gmat without the slmi factor), shared
-__device__ __forceinline__ void md_form_t(int s, const double *b0, const double *b1, const double *b2,
+__device__ __forceinline__ void md_form_t(const CSys &cs, int s, const double *b0, const double *b1, const double *b2,
                                           const double *aa, const int *slot_orb, double *t) {
   const int n = s == 0 ? cs.nup : cs.ndn, O = cs.Oa, ivirt = cs.md_ivirt[s];
   for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) {
@@ -689,7 +703,7 @@ __device__ __forceinline__ void md_form_t(int s, const double *b0, const double 
 // drift correction of every electron at the current configuration right
 // after hpsi (dmc_ps :516), from the Y matrix hpsi just built: warp per
 // (walker, electron); vall [W][N][3]
-__global__ void k_md_drift_all(WState st, MdBuf md, GSys g, double *vall) {
+__global__ void k_md_drift_all(const __grid_constant__ CSys cs, WState st, MdBuf md, GSys g, double *vall) {
   const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
   if (gw >= (long)st.W * N) return;
@@ -701,14 +715,14 @@ __global__ void k_md_drift_all(WState st, MdBuf md, GSys g, double *vall) {
   const double *b2 = md.dorbA + (((size_t)w * 3 + 2) * N + e) * O;
   const double detratio = st.detiab[2 * w] * st.detiab[2 * w + 1] / st.psido[w];
   double vel[3];
-  md_velocity_warp(s, c, b0, b1, b2, 1, md.aa + ((size_t)w * 2 + s) * nmax * O,
+  md_velocity_warp(cs, s, c, b0, b1, b2, 1, md.aa + ((size_t)w * 2 + s) * nmax * O,
                    md.ymat + ((size_t)w * 2 + s) * nmax * O, g.slot_orb + s * nmax, detratio, vel);
   if ((threadIdx.x & 31) == 0)
     for (int k = 0; k < 3; k++) vall[((size_t)w * N + e) * 3 + k] = vel[k];
 }
 
 // G_s before the moves of spin s: CTA (128) per walker
-__global__ void __launch_bounds__(128) k_md_phase(WState st, MdBuf md, MdTab tab, int s) {
+__global__ void __launch_bounds__(128) k_md_phase(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, int s) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   extern __shared__ __align__(16) double smem[];
@@ -716,7 +730,7 @@ __global__ void __launch_bounds__(128) k_md_phase(WState st, MdBuf md, MdTab tab
   __shared__ double red[4];
   const int ng = cs.iguiding > 0 ? cs.nstates : 1;  // states whose G the moves need
   for (int stt = 0; stt < ng; stt++) {
-    md_form_G(tab, md, w, s, G, red, tab.cdet + (size_t)stt * cs.ndet);
+    md_form_G(cs, tab, md, w, s, G, red, tab.cdet + (size_t)stt * cs.ndet);
     double *gG = md.G + ((size_t)w * ng + stt) * (tab.numax + 1);
     for (int kk = threadIdx.x; kk <= cs.md_nuniq[s]; kk += blockDim.x) gG[kk] = G[kk];
     __syncthreads();
@@ -727,7 +741,7 @@ __global__ void __launch_bounds__(128) k_md_phase(WState st, MdBuf md, MdTab tab
 // matrix: vel = detratio * sum_kk d_kk G_kk sum_jr t[ro_jr] (M_kk^-1 c)[jr]
 // with c the column of A^-1 of the electron (the Y contraction regrouped per
 // excitation).  CTA (128) per walker; shared: c (nmax), t (3*O), aa (nmax*O).
-__global__ void __launch_bounds__(128) k_md_drift_old(WState st, MdBuf md, MdTab tab, GSys g, int iel) {
+__global__ void __launch_bounds__(128) k_md_drift_old(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
@@ -742,7 +756,7 @@ __global__ void __launch_bounds__(128) k_md_drift_old(WState st, MdBuf md, MdTab
   for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = sl[j];
   for (int q = threadIdx.x; q < n * O; q += blockDim.x) A[q] = aa[q];
   __syncthreads();
-  md_form_t(s, md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O, md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O,
+  md_form_t(cs, s, md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O, md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O,
             md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O, A, g.slot_orb + s * nmax, t);
   __syncthreads();
   const double *G = md.G + (size_t)w * (cs.iguiding > 0 ? cs.nstates : 1) * (tab.numax + 1);
@@ -772,7 +786,7 @@ __global__ void __launch_bounds__(128) k_md_drift_old(WState st, MdBuf md, MdTab
       vg[2] += f * a2;
     }
     if (threadIdx.x == 0) {
-      const double gi = 1.0 / md_psig(S, ns);
+      const double gi = 1.0 / md_psig(cs, S, ns);
       md.velo[3 * w] = vg[0] * gi;
       md.velo[3 * w + 1] = vg[1] * gi;
       md.velo[3 * w + 2] = vg[2] * gi;
@@ -780,10 +794,15 @@ __global__ void __launch_bounds__(128) k_md_drift_old(WState st, MdBuf md, MdTab
     return;
   }
   double v0 = 0, v1 = 0, v2 = 0;
-  for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) {
+  const int NU = cs.md_nuniq[s];
+  MdExcPf nx;
+  if ((int)threadIdx.x < NU) nx.load(tab, s, threadIdx.x, G);
+  for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
+    const MdExcPf cur = nx;
+    if (kk + (int)blockDim.x < NU) nx.load(tab, s, kk + blockDim.x, G);
     double gv[3];
-    const double d = md_ratio_contract(A, O, md_exc(tab, s, kk), c, t, O, gv);
-    const double ce = d * G[kk];
+    const double d = md_ratio_contract(A, O, cur.e, c, t, O, gv);
+    const double ce = d * cur.g;
     v0 += ce * gv[0];
     v1 += ce * gv[1];
     v2 += ce * gv[2];
@@ -804,7 +823,7 @@ __global__ void __launch_bounds__(128) k_md_drift_old(WState st, MdBuf md, MdTab
 // phi_new(occ_i) aa[i][v]) / R (the Sherman-Morrison form of
 // slmin * orb_new), the excitation ratios, S, psi_D and the drift at the new
 // point.  Shared: c, slot values (nmax each), w (O), t (3*O), aa_new (nmax*O).
-__global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md, MdTab tab, GSys g, int iel) {
+__global__ void __launch_bounds__(128) k_md_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, MdBuf md, MdTab tab, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int O = cs.Oa, nmax = cs.nmax;
@@ -853,7 +872,7 @@ __global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md
   }
   __syncthreads();
   // column iel of the updated inverse is c / R; drift operands at the new point
-  md_form_t(s, orbn + O, orbn + 2 * O, orbn + 3 * O, An, g.slot_orb + s * nmax, t);
+  md_form_t(cs, s, orbn + O, orbn + 2 * O, orbn + 3 * O, An, g.slot_orb + s * nmax, t);
   __syncthreads();
   for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = c[j] / R;
   __syncthreads();
@@ -890,7 +909,7 @@ __global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md
     if (threadIdx.x == 0) {
       const double detn_ref = st.detiab[2 * w + s] * R;
       const double dpair = s == 0 ? detn_ref * st.detiab[2 * w + 1] : st.detiab[2 * w] * detn_ref;
-      const double g = md_psig(s_Sn, ns), gi = 1.0 / g;
+      const double g = md_psig(cs, s_Sn, ns), gi = 1.0 / g;
       double vg[3] = {0, 0, 0};
       for (int stt = 0; stt < ns; stt++) {
         const double r = s_Sn[stt] / s_Sn[0], f = cs.wg[stt] * r * r / s_Sn[stt];
@@ -909,11 +928,15 @@ __global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md
     return;
   }
   double sp = 0, v0 = 0, v1 = 0, v2 = 0;
+  MdExcPf nx;
+  if ((int)threadIdx.x < NU) nx.load(tab, s, threadIdx.x, G);
   for (int kk = threadIdx.x; kk < NU; kk += blockDim.x) {
+    const MdExcPf cur = nx;
+    if (kk + (int)blockDim.x < NU) nx.load(tab, s, kk + blockDim.x, G);
     double gv[3];
-    const double d = md_ratio_contract(An, O, md_exc(tab, s, kk), c, t, O, gv);
+    const double d = md_ratio_contract(An, O, cur.e, c, t, O, gv);
     ddn[kk] = d;
-    const double ce = d * G[kk];
+    const double ce = d * cur.g;
     sp += ce;
     v0 += ce * gv[0];
     v1 += ce * gv[1];
@@ -943,7 +966,7 @@ __global__ void __launch_bounds__(128) k_md_move(WState st, MoveBuf mb, MdBuf md
 
 // commit of an accepted move (after k_commit): aa += c (x) w on the
 // virtual columns, ratios, S, and the gradient row of the moved electron
-__global__ void k_md_commit(WState st, MoveBuf mb, MdBuf md, MdTab tab, int iel) {
+__global__ void k_md_commit(const __grid_constant__ CSys cs, WState st, MoveBuf mb, MdBuf md, MdTab tab, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W || !mb.ms[w].acc) return;
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;

@@ -14,7 +14,7 @@
 
 namespace cw {
 
-__device__ __forceinline__ double thetamx_d(double r, double z) {
+__device__ __forceinline__ double thetamx_d(const CSys &cs, double r, double z) {
   return cs.deltat + (2.0 - cs.deltat) / (1.0 + (z * r) * (z * r));
 }
 
@@ -134,7 +134,7 @@ __device__ __forceinline__ bool radial_sample_group(DRng &rng, double rmin, doub
   return gave_up;
 }
 
-__device__ __forceinline__ void spin_of(int iel, int &iab, int &nel, int &ish) {
+__device__ __forceinline__ void spin_of(const CSys &cs, int iel, int &iab, int &nel, int &ish) {
   if (iel < cs.nup) { iab = 0; nel = cs.nup; ish = 0; }
   else { iab = 1; nel = cs.ndn; ish = cs.nup; }
 }
@@ -146,9 +146,13 @@ __device__ __forceinline__ void spin_of(int iel, int &iab, int &nel, int &ish) {
 // chain that the group's lanes evaluate identically; the radial rejection
 // loop is cooperative within the group.  The group's lane 0 stores.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_propose(WState st, MoveBuf mb, int iel) {
+__global__ void __launch_bounds__(128) k_propose(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel,
+                                                 int *acc_count) {
   // Every lane runs to the end (the radial sampling is cooperative across the
   // warp); groups past the population mirror the last walker and store nothing.
+  // acc_count (optional): the accepted-walker count k_decide appends to,
+  // emptied here (the previous move's commit has finished reading it).
+  if (acc_count && blockIdx.x == 0 && threadIdx.x == 0) *acc_count = 0;
   const int gl = threadIdx.x & (kMoveGroup - 1);
   const int wt = (blockIdx.x * blockDim.x + threadIdx.x) / kMoveGroup;
   const bool live = wt < st.W;
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(128) k_propose(WState st, MoveBuf mb, int iel)
   const int lane = live ? gl : 1;  // lane 0 of a live group stores
   const int N = cs.N, nmax = cs.nmax;
   int iab, nel, ish;
-  spin_of(iel, iab, nel, ish);
+  spin_of(cs, iel, iab, nel, ish);
   const int iloc = iel - ish;
   const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * iloc;
   const double *d0p = st.dorbs + (((size_t)w * 3 + 0) * N + iel) * nmax;
@@ -241,7 +245,7 @@ __global__ void __launch_bounds__(128) k_propose(WState st, MoveBuf mb, int iel)
   fxop = fxop * top / bot;
   double areao = t_area_d(zeta, co, rbot, rtop, bot);
   double raver = half * (rmin + rtry);
-  double deltt = thetamx_d(raver, znear);
+  double deltt = thetamx_d(cs, raver, znear);
   double costht = one - deltt * rng.uniform();
   double zprime = rtry * costht;
   double sintht = sqrt(one - costht * costht);
@@ -293,7 +297,7 @@ __global__ void __launch_bounds__(128) k_propose(WState st, MoveBuf mb, int iel)
   rminon = sqrt(rminon);
   dot = dot / (rminn * rminon);
   const double ravern = half * (rminn + rminon);
-  const double delttn = thetamx_d(ravern, cs.znuc[cs.iwctype[nearn]]);
+  const double delttn = thetamx_d(cs, ravern, cs.znuc[cs.iwctype[nearn]]);
   m.igeo = (rminon > rminn * deltar || dot < one - delttn) ? 1 : 0;
   for (int k = 0; k < 3; k++) {
     m.xnew[k] = xn[k];
@@ -322,7 +326,7 @@ __global__ void __launch_bounds__(128) k_propose(WState st, MoveBuf mb, int iel)
 constexpr int kJmPartners = 1;
 
 template <int NORD>
-__global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, int iel) {
+__global__ void __launch_bounds__(128, 5) k_jastrow_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) double smem[];
   constexpr int NB = een_nb(NORD);        // folded coefficients per centre
   constexpr int PER = 8 + 2 * NB;         // shared doubles per centre (one pad keeps B 16-byte aligned)
@@ -354,7 +358,7 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
     const double r = sqrt(r2);
     sh_r[ic] = r;
     double rr, dd1, dd2;
-    scale2<double>(r, rr, dd1, dd2);
+    scale2<double>(cs, r, rr, dd1, dd2);
     sh_s[ic] = rr;
     sh_d[ic] = dd1;
     sh_g[ic] = -kap * dd1 / r;
@@ -385,16 +389,16 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
       const int i = jc < iel ? iel : jc, j = jc < iel ? jc : iel;
       int isb, ipar;
       double sspinn;
-      pair_spin(i, j, isb, ipar, sspinn);
+      pair_spin(cs, i, j, isb, ipar, sspinn);
       for (int k = 0; k < 3; k++) rvee[q][k] = xi[k] - xj[k];  // x_iel - x_jj
       rij[q] = sqrt(rvee[q][0] * rvee[q][0] + rvee[q][1] * rvee[q][1] + rvee[q][2] * rvee[q][2]);
       double u, dd1, dd2;
-      scale2<double>(rij[q], u, dd1, dd2);
+      scale2<double>(cs, rij[q], u, dd1, dd2);
       fs[q] = 0;
       for (int k = 0; k < 3; k++) gi[q][k] = gj[q][k] = 0;
       if (u != asym) {
         double fee, feeu, feeuu;
-        ee_term<1, double>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+        ee_term<1, double>(cs, isb, ipar, sspinn, u, fee, feeu, feeuu);
         feeu = feeu * dd1 / rij[q];
         fs[q] += fee;
         for (int k = 0; k < 3; k++) {
@@ -482,7 +486,7 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
     const double ri = sh_r[ic];
     const double dd7 = sh_d[ic];
     double fen, feni, fenii;
-    en_term<1, double>(it, rri, fen, feni, fenii);
+    en_term<1, double>(cs, it, rri, fen, feni, fenii);
     feni = feni * dd7 / ri;
     fen_s += fen;
     ge0 += feni * sh_rv[0 * M + ic];
@@ -521,7 +525,7 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(WState st, MoveBuf mb, 
 // and the row sums against the stored FP64 tables (dfs, dv) stay FP64.
 // ---------------------------------------------------------------------------
 template <int NORD>
-__global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf mb, int iel) {
+__global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) float smemf[];
   constexpr int NB = een_nbp(NORD);        // padded (B, dB) pairs per centre
   constexpr int PER = 8 + 2 * NB;         // shared floats per centre (B 16-byte aligned)
@@ -553,7 +557,7 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
     const float r = sqrtf(r2);
     sh_r[ic] = r;
     float rr, dd1, dd2;
-    scale2<float>(r, rr, dd1, dd2);
+    scale2<float>(cs, r, rr, dd1, dd2);
     sh_s[ic] = rr;
     sh_d[ic] = dd1;
     sh_g[ic] = -kap * dd1 / r;
@@ -571,16 +575,16 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
     const int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
     int isb, ipar;
     double sspinn_d;
-    pair_spin(i, j, isb, ipar, sspinn_d);
+    pair_spin(cs, i, j, isb, ipar, sspinn_d);
     const float sspinn = (float)sspinn_d;
     const float rvee[3] = {(float)(xi[0] - xj[0]), (float)(xi[1] - xj[1]), (float)(xi[2] - xj[2])};
     const float rij = sqrtf(rvee[0] * rvee[0] + rvee[1] * rvee[1] + rvee[2] * rvee[2]);
     float u, dd1, dd2;
-    scale2<float>(rij, u, dd1, dd2);
+    scale2<float>(cs, rij, u, dd1, dd2);
     float fs = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
     if (u != asym) {
       float fee, feeu, feeuu;
-      ee_term<1, float>(isb, ipar, sspinn, u, fee, feeu, feeuu);
+      ee_term<1, float>(cs, isb, ipar, sspinn, u, fee, feeu, feeuu);
       feeu = feeu * dd1 / rij;
       fs += fee;
       for (int k = 0; k < 3; k++) {
@@ -638,7 +642,7 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
     const float rri = sh_s[ic];
     if (rri == asym) continue;
     float fen, feni, fenii;
-    en_term<1, float>(it, rri, fen, feni, fenii);
+    en_term<1, float>(cs, it, rri, fen, feni, fenii);
     feni = feni * sh_d[ic] / sh_r[ic];
     fen_s += fen;
     ge0 += feni * sh_rv[0 * M + ic];
@@ -674,7 +678,7 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(WState st, MoveBuf 
 // Basis functions of the moved electron (basis_fns ider=1): warp per walker,
 // per-centre prepass then lanes over AOs.
 // ---------------------------------------------------------------------------
-__global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
+__global__ void k_basis_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g) {
   extern __shared__ __align__(16) double smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -699,11 +703,11 @@ __global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
   }
   double *rec = smem + (size_t)wib * cs.M * kCenRec;
   const double x[3] = {mv.xnew[0], mv.xnew[1], mv.xnew[2]};
-  warp_basis_prepass<1>(g, x, rec, lane);
+  warp_basis_prepass<1>(cs, g, x, rec, lane);
   __syncwarp();
   if (hi) {
     for (int m = lane; m < K; m += 32)
-      warp_basis_ao<1>(g, rec, m, [&](int a, int d, double v) {
+      warp_basis_ao<1>(cs, g, rec, m, [&](int a, int d, double v) {
         float h, l;
         split_tf32(v, h, l);
         hi[(size_t)d * kp + a] = h;
@@ -712,7 +716,7 @@ __global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
     return;
   }
   for (int m = lane; m < K; m += 32)
-    warp_basis_ao<1>(g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
+    warp_basis_ao<1>(cs, g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
 }
 
 // ---------------------------------------------------------------------------
@@ -722,7 +726,8 @@ __global__ void k_basis_move(WState st, MoveBuf mb, GSys g) {
 // Scalar state of accepted moves is committed here; k_commit applies the
 // matrix and table updates.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_decide(WState st, MoveBuf mb, GSys g, int iel) {
+__global__ void __launch_bounds__(128) k_decide(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, int iel,
+                                                int *acc_list, int *acc_count) {
   // kMoveGroup lanes per walker: the ratio and the drift at the new point are
   // dot products over the group, the rest is evaluated identically by the
   // group's lanes, its lane 0 stores
@@ -731,7 +736,7 @@ __global__ void __launch_bounds__(128) k_decide(WState st, MoveBuf mb, GSys g, i
   if (w >= st.W) return;  // the whole group (one walker)
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
-  spin_of(iel, iab, nel, ish);
+  spin_of(cs, iel, iab, nel, ish);
   const int iloc = iel - ish;
   MoveScratch &m = mb.ms[w];
   const double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax + (size_t)nel * iloc;
@@ -824,6 +829,9 @@ __global__ void __launch_bounds__(128) k_decide(WState st, MoveBuf mb, GSys g, i
   rng.store(st.rng + 4 * (size_t)w);
   m.acc = acc;
   m.ratio = ratio;
+  // accepted walkers listed for the commit (in arrival order: each walker's
+  // commit touches its own state only, so the order does not matter)
+  if (acc && acc_list) acc_list[atomicAdd(acc_count, 1)] = w;
   if (acc) {
     st.psi2o[w] = psi2n;
     st.psido[w] = psidn;
@@ -846,18 +854,18 @@ __global__ void __launch_bounds__(128) k_decide(WState st, MoveBuf mb, GSys g, i
 // ---------------------------------------------------------------------------
 // Orbital rows, e-n table row and the Jastrow pair tables of the moved
 // electron (the part of detsav / jassav after the inverse).
-__device__ __forceinline__ void commit_tables(WState &st, const MoveBuf &mb, const GSys &g, int w, int iel,
-                                              const double *s_orb) {
+__device__ __forceinline__ void commit_tables(const CSys &cs, WState &st, const MoveBuf &mb, const GSys &g, int w, int iel) {
   const int tid = threadIdx.x;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
-  spin_of(iel, iab, nel, ish);
+  spin_of(cs, iel, iab, nel, ish);
   const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
   const int *slot = g.slot_orb + iab * nmax;
   for (int j = tid; j < nel; j += blockDim.x) {
-    st.orbs[((size_t)w * N + iel) * nmax + j] = s_orb[j];
+    const int sj = slot[j];
+    st.orbs[((size_t)w * N + iel) * nmax + j] = orbn[sj];
     for (int k = 0; k < 3; k++)
-      st.dorbs[(((size_t)w * 3 + k) * N + iel) * nmax + j] = orbn[(1 + k) * Oa + slot[j]];
+      st.dorbs[(((size_t)w * 3 + k) * N + iel) * nmax + j] = orbn[(1 + k) * Oa + sj];
   }
   // e-n table row of the moved electron
   const int M = cs.M;
@@ -890,7 +898,7 @@ __device__ __forceinline__ void commit_tables(WState &st, const MoveBuf &mb, con
   }
 }
 
-__global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
+__global__ void k_commit(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   if (!mb.ms[w].acc) return;
@@ -898,7 +906,7 @@ __global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
   const int nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
-  spin_of(iel, iab, nel, ish);
+  spin_of(cs, iel, iab, nel, ish);
   const int iloc = iel - ish;
   __shared__ double s_orb[256];
   __shared__ double s_col[256];
@@ -920,7 +928,7 @@ __global__ void k_commit(WState st, MoveBuf mb, GSys g, int iel) {
     for (int j = lane; j < nel; j += 32) sl[(size_t)nel * k + j] = sl[(size_t)nel * k + j] - s_col[j] * s;
   }
   for (int j = tid; j < nel; j += blockDim.x) sl[(size_t)nel * iloc + j] = s_col[j] / ratio;
-  commit_tables(st, mb, g, w, iel, s_orb);
+  commit_tables(cs, st, mb, g, w, iel);
 }
 
 // The accepted walkers of a move, in walker order: list [W], *count.  One
@@ -947,20 +955,20 @@ __global__ void __launch_bounds__(1024) k_accept_list(const MoveScratch *__restr
   if (t == nt - 1) *count = scan[t];
 }
 
-// The same commit with the spin's inverse staged in shared memory: every
-// load of the n x n block is issued at once (coalesced), the row factors
-// (slmi(:,k)·orb_new)/ratio come from shared memory, and the updated block
-// is written back coalesced, instead of one warp walking its rows one
-// dependent global round trip after another.  Row stride nel+1 (odd) keeps
-// the row-per-thread reads free of bank conflicts.  Dynamic shared memory:
-// nel*(nel+1) + 3*nel doubles.  Same arithmetic as k_commit.  The blocks
-// loop over the list of accepted walkers (k_accept_list), so no block is
-// spent on a rejected move.
-__device__ __forceinline__ void commit_tile_walker(WState &st, const MoveBuf &mb, const GSys &g, int w, int iel) {
-  const int tid = threadIdx.x;
+// The same commit with the spin's inverse staged in shared memory: the n x n
+// block is copied with asynchronous 8-byte copies (cp.async, sm_80+), all in
+// flight at once, and while they land the block writes the orbital rows and
+// the Jastrow pair tables (independent of the inverse); then the row factors
+// (slmi(:,k)·orb_new)/ratio come from shared memory and the updated block is
+// written back row by row, coalesced.  Row stride nel+1 (odd) keeps the
+// row-per-lane-pair reads free of bank conflicts.  Dynamic shared memory:
+// nel*(nel+1) + 3*nel doubles.  Same arithmetic as k_commit.  The blocks loop
+// over the list of accepted walkers, so no block is spent on a rejected move.
+__device__ __forceinline__ void commit_tile_walker(const CSys &cs, WState &st, const MoveBuf &mb, const GSys &g, int w, int iel) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
   const int nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
-  spin_of(iel, iab, nel, ish);
+  spin_of(cs, iel, iab, nel, ish);
   const int iloc = iel - ish, ld = nel + 1;
   extern __shared__ __align__(16) double sm[];
   double *s_inv = sm;                        // [nel][ld]
@@ -971,9 +979,16 @@ __device__ __forceinline__ void commit_tile_walker(WState &st, const MoveBuf &mb
   double *sl = st.slmi + ((size_t)w * 2 + iab) * nmax * nmax;
   const double *orbn = mb.orbn + (size_t)w * 4 * Oa;
   const int *slot = g.slot_orb + iab * nmax;
-  const int nn = nel * nel;
-  for (int t = tid; t < nn; t += blockDim.x) s_inv[(t / nel) * ld + (t % nel)] = sl[t];
+  const unsigned s_base = (unsigned)__cvta_generic_to_shared(s_inv);
+  for (int k = wid; k < nel; k += nwarp)
+    for (int j = lane; j < nel; j += 32)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s_base + 8u * (unsigned)(k * ld + j)),
+                   "l"(sl + (size_t)nel * k + j)
+                   : "memory");
+  asm volatile("cp.async.commit_group;" ::: "memory");
   for (int j = tid; j < nel; j += blockDim.x) s_orb[j] = orbn[slot[j]];
+  commit_tables(cs, st, mb, g, w, iel);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
   for (int j = tid; j < nel; j += blockDim.x) s_col[j] = s_inv[iloc * ld + j];
   // two lanes per row, each summing alternate entries; the loop bound is the
@@ -988,18 +1003,18 @@ __device__ __forceinline__ void commit_tile_walker(WState &st, const MoveBuf &mb
     if (act && h == 0) s_fac[k] = s / ratio;
   }
   __syncthreads();
-  for (int t = tid; t < nn; t += blockDim.x) {
-    const int k = t / nel, j = t % nel;
-    sl[t] = (k == iloc) ? s_col[j] / ratio : s_inv[k * ld + j] - s_col[j] * s_fac[k];
+  for (int k = wid; k < nel; k += nwarp) {
+    const double f = s_fac[k];
+    for (int j = lane; j < nel; j += 32)
+      sl[(size_t)nel * k + j] = (k == iloc) ? s_col[j] / ratio : s_inv[k * ld + j] - s_col[j] * f;
   }
-  commit_tables(st, mb, g, w, iel, s_orb);
 }
 
-__global__ void k_commit_tile(WState st, MoveBuf mb, GSys g, int iel_arg, const int *__restrict__ list,
+__global__ void k_commit_tile(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, int iel_arg, const int *__restrict__ list,
                               const int *__restrict__ count) {
   const int nacc = *count;
   for (int q = blockIdx.x; q < nacc; q += gridDim.x) {
-    commit_tile_walker(st, mb, g, list[q], iel_arg < 0 ? mb.ms[list[q]].tel : iel_arg);
+    commit_tile_walker(cs, st, mb, g, list[q], iel_arg < 0 ? mb.ms[list[q]].tel : iel_arg);
     __syncthreads();  // the next walker reuses the shared memory
   }
 }

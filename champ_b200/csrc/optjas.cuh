@@ -73,7 +73,7 @@ __device__ __forceinline__ void jas_flush(const double (&acc)[NV], int nv, doubl
 constexpr int kJasThreads = 128;
 
 template <int NORD>
-__global__ void __launch_bounds__(kJasThreads) k_jas_raw(WState st, double *raw, int nraw) {
+__global__ void __launch_bounds__(kJasThreads) k_jas_raw(const __grid_constant__ CSys cs, WState st, double *raw, int nraw) {
   constexpr int NTC = NORD > 1 ? een_nterms(NORD) : 1;
   constexpr int NAM = CW_MAX_NORD + 1;
   __shared__ double red[(kJasThreads / 32) * (NTC > 2 * NAM ? NTC : 2 * NAM)];
@@ -132,10 +132,10 @@ __global__ void __launch_bounds__(kJasThreads) k_jas_raw(WState st, double *raw,
       int i, j, isb, ipar;
       double sspinn;
       pair_of(p, i, j);
-      pair_spin(i, j, isb, ipar, sspinn);
+      pair_spin(cs, i, j, isb, ipar, sspinn);
       const double d0 = xw[i] - xw[j], d1 = xw[N + i] - xw[N + j], d2 = xw[2 * N + i] - xw[2 * N + j];
       double u, dd1, dd2;
-      scale2<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2), u, dd1, dd2);
+      scale2<double>(cs, sqrt(d0 * d0 + d1 * d1 + d2 * d2), u, dd1, dd2);
       if (u == ar) continue;
       const double b1 = cs.b[isb * NB], b2 = cs.b[isb * NB + 1];
       const double bot0 = 1 + b2 * u;
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(kJasThreads) k_jas_raw(WState st, double *raw,
         pair_of(p, i, j);
         const double d0 = xw[i] - xw[j], d1 = xw[N + i] - xw[N + j], d2 = xw[2 * N + i] - xw[2 * N + j];
         double u, dd1, dd2;
-        scale2<double>(sqrt(d0 * d0 + d1 * d1 + d2 * d2), u, dd1, dd2);
+        scale2<double>(cs, sqrt(d0 * d0 + d1 * d1 + d2 * d2), u, dd1, dd2);
         double uu[NORD + 1];
         uu[0] = 1;
         uu[1] = 1 - kap * u;
@@ -243,7 +243,7 @@ __global__ void k_orb_vals(int W, int N, int e0, int ne, int Oa, const double *_
 
 // thread per (walker, term): the derivative into the optimisation vector,
 // columns [off, off + nterm) of o [W][np] and ot [np][W]
-__global__ void k_orb_o(WState st, int nterm, const OrbTerm *__restrict__ terms, int nv,
+__global__ void k_orb_o(const __grid_constant__ CSys cs, WState st, int nterm, const OrbTerm *__restrict__ terms, int nv,
                         const double *__restrict__ vals, double *o, double *ot, int np, int off) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)st.W * nterm) return;

@@ -135,6 +135,24 @@ class Engine:
         self._check(self.lib.cw_walker_status(self.h, out.ctypes.data_as(C.POINTER(C.c_int32))), "cw_walker_status")
         return out
 
+    def sync(self):
+        """Wait for the context's queued work."""
+        self._check(self.lib.cw_sync(self.h), "cw_sync")
+
+    def stamp(self):
+        """Enqueue a device-clock stamp on the context's stream."""
+        self._check(self.lib.cw_stamp(self.h), "cw_stamp")
+
+    def stamps(self):
+        """All device-clock stamps of the context so far (ns), after its
+        queued work has finished."""
+        n = self.lib.cw_stamps(self.h, None, 0)
+        out = np.zeros(max(n, 1), np.int64)
+        n = self.lib.cw_stamps(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)), n)
+        if n < 0:
+            self._check(n, "cw_stamps")
+        return out[:n]
+
     # -- per-electron routines (a metrop6 kept on the host) ---------------
     def psie(self, iel: int, xnew):
         """psie of electron iel at xnew [W][3] for every walker: (psid, psij)."""

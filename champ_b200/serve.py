@@ -5,12 +5,15 @@ Jobs arrive over time.  A job is admitted as soon as its device-memory
 estimate fits into what the HBM budget has left, first come first served (a
 job never overtakes an earlier one that does not fit yet).  From then on it
 keeps its engine context -- walker population, Slater inverses, Jastrow
-tables, accumulators -- resident on the device until it finishes.  The loop
-advances the admitted jobs one block at a time, round-robin (a block is
-``nstep`` sweeps followed by the block average, CHAMP's acuest), and admits
-newly arrived jobs between blocks.  A job finishes when its error bar reaches
-the target (after at least two blocks) or its block budget is spent; its
-context is then released and the jobs waiting for memory are admitted.
+tables, accumulators -- resident on the device until it finishes.  At most
+``slots`` jobs are admitted at a time; every admitted job has one block in
+flight (a block is ``nstep`` sweeps followed by the block average, CHAMP's
+acuest), issued from a worker thread on the job's own CUDA stream, so the
+blocks of different jobs run on the device at the same time (each kernel
+carries its own system's constants).  Newly arrived jobs are admitted
+whenever a block ends.  A job finishes when its error bar reaches the target
+(after at least two blocks) or its block budget is spent; its context is
+then released and the jobs waiting for memory or a slot are admitted.
 
 A job is charged the larger of its estimate and the bytes its context
 really holds (``cw_device_bytes``, read after creation): the estimate is an
@@ -24,15 +27,18 @@ Time-to-result of a job = completion time - arrival time.  Each job draws
 its walkers' streams from its own range (``seed_offset``), so a job's
 result does not depend on which other jobs share the device.
 
-Work of different jobs is interleaved block by block on the host thread;
-their kernels do not run at the same time on the device.
+``executor`` replaces the worker threads (``InlineExecutor`` runs the blocks
+in flight one after the other on the loop's own thread: the round-robin
+order of a single host thread, used by the host-side tests).
 CHAMP itself has no request loop (one job per MPI run); this module is the
 serving layer the engine's C ABI is designed for.
 """
 from __future__ import annotations
 
 import collections
+import concurrent.futures as cf
 import dataclasses
+import itertools
 import math
 import time
 
@@ -103,19 +109,65 @@ def _engine_for(job: Job, precision: str, device: int):
     return eng
 
 
+def _block(eng, nstep: int):
+    """One block of a job: (block averages, device-clock start and end in ns,
+    or None where the engine keeps no device clock)."""
+    stamp = getattr(eng, "stamp", None)
+    if stamp:
+        stamp()
+    eng.vmc_steps(nstep)
+    eng.end_block()
+    if stamp:
+        stamp()
+    r = eng.results()
+    dev = tuple(int(v) for v in eng.stamps()[-2:]) if stamp else None
+    return r, dev
+
+
+class InlineExecutor:
+    """Runs the submitted calls on the calling thread, one after the other in
+    submission order, when the server waits for them."""
+
+    def __init__(self):
+        self.queue = []
+
+    def submit(self, fn, *args):
+        f = cf.Future()
+        self.queue.append((f, fn, args))
+        return f
+
+    def wait(self, fs, timeout=None, return_when=cf.FIRST_COMPLETED):
+        queue, self.queue = self.queue, []
+        for f, fn, args in queue:
+            try:
+                f.set_result(fn(*args))
+            except Exception as exc:
+                f.set_exception(exc)
+        return set(fs), set()
+
+    def shutdown(self, wait: bool = True):
+        pass
+
+
 class Server:
-    """One GPU, one HBM budget; `run` serves a list of jobs with arrival times."""
+    """One GPU, one HBM budget; `run` serves a list of jobs with arrival times,
+    at most `slots` of them on the device at once."""
 
     def __init__(self, budget_bytes: int, precision: str = "fp64", device: int = 0, engine_factory=None,
-                 clock=time.perf_counter, sleep=time.sleep):
+                 clock=time.perf_counter, sleep=time.sleep, slots: int = 8, executor=None):
         self.budget = int(budget_bytes)
         self.precision = precision
         self.device = device
         self.factory = engine_factory or (lambda job: _engine_for(job, precision, device))
         self.clock = clock
         self.sleep = sleep
+        self.slots = max(1, int(slots))
+        self.executor = executor
         self.peak_bytes = 0          # largest sum of admitted estimates
+        self.peak_running = 0        # most jobs with a block in flight at once
         self.timeline = []           # (time, event, job id)
+        self.blocks = []             # (job id, start, end) of every block, host clock
+        self.device_blocks = []      # (job id, start ns, end ns) of every block, device clock
 
     def run(self, jobs):
         jobs = sorted(jobs, key=lambda j: (j.arrival, j.jid))
@@ -123,12 +175,19 @@ class Server:
             j.est_bytes = estimate_bytes(j.system, j.nwalk, self.precision)
         pending = collections.deque(jobs)
         waiting = collections.deque()
-        active = collections.deque()   # (job, engine) in round-robin order
+        inflight = {}                  # future -> (submission number, job, engine, start time)
+        seq = itertools.count()
         used = 0
+        pool = self.executor or cf.ThreadPoolExecutor(max_workers=self.slots)
         t0 = self.clock()
 
         def now():
             return self.clock() - t0
+
+        def submit(j, eng):
+            start = now()
+            inflight[pool.submit(_block, eng, j.nstep)] = (next(seq), j, eng, start)
+            self.peak_running = max(self.peak_running, len(inflight))
 
         def arrive_and_admit():
             nonlocal used
@@ -137,7 +196,7 @@ class Server:
                 j = pending.popleft()
                 waiting.append(j)
                 self.timeline.append((t, "arrive", j.jid))
-            while waiting:
+            while waiting and len(inflight) < self.slots:
                 j = waiting[0]
                 if j.est_bytes > self.budget:      # can never fit: refuse, do not block the queue
                     waiting.popleft()
@@ -174,37 +233,47 @@ class Server:
                 self.peak_bytes = max(self.peak_bytes, used)
                 j.admitted = now()
                 self.timeline.append((j.admitted, "admit", j.jid))
-                active.append((j, eng))
+                submit(j, eng)
 
-        while pending or waiting or active:
-            arrive_and_admit()
-            if not active:
-                if pending:
-                    self.sleep(max(0.0, pending[0].arrival - now()))
-                continue
-            j, eng = active.popleft()
-            try:
-                eng.vmc_steps(j.nstep)
-                eng.end_block()
-                r = eng.results()
-            except Exception as exc:               # a failed block ends this job only
-                j.failed = f"block failed: {exc}"
-                j.done = now()
-                self.timeline.append((j.done, "fail", j.jid))
-                eng.close()
-                used -= j.est_bytes
-                continue
-            j.blocks += 1
-            j.moves += j.nstep * j.nwalk * j.system.nelec
-            j.energy, j.err = float(r["energy"]), float(r["err"])
-            j.reached = j.blocks >= 2 and j.err <= j.target_err
-            if j.reached or j.blocks >= j.max_blocks:
-                j.done = now()
-                self.timeline.append((j.done, "done", j.jid))
-                eng.close()
-                used -= j.est_bytes
-            else:
-                active.append((j, eng))
+        try:
+            while pending or waiting or inflight:
+                arrive_and_admit()
+                if not inflight:
+                    if pending:
+                        self.sleep(max(0.0, pending[0].arrival - now()))
+                    continue
+                timeout = max(0.0, pending[0].arrival - now()) if pending else None
+                done, _ = getattr(pool, "wait", cf.wait)(list(inflight), timeout=timeout,
+                                                         return_when=cf.FIRST_COMPLETED)
+                for f in sorted(done, key=lambda f: inflight[f][0]):
+                    _, j, eng, start = inflight.pop(f)
+                    end = now()
+                    self.blocks.append((j.jid, start, end))
+                    try:
+                        r, dev = f.result()
+                    except Exception as exc:           # a failed block ends this job only
+                        j.failed = f"block failed: {exc}"
+                        j.done = end
+                        self.timeline.append((j.done, "fail", j.jid))
+                        eng.close()
+                        used -= j.est_bytes
+                        continue
+                    if dev:
+                        self.device_blocks.append((j.jid, *dev))
+                    j.blocks += 1
+                    j.moves += j.nstep * j.nwalk * j.system.nelec
+                    j.energy, j.err = float(r["energy"]), float(r["err"])
+                    j.reached = j.blocks >= 2 and j.err <= j.target_err
+                    if j.reached or j.blocks >= j.max_blocks:
+                        j.done = end
+                        self.timeline.append((j.done, "done", j.jid))
+                        eng.close()
+                        used -= j.est_bytes
+                    else:
+                        submit(j, eng)
+        finally:
+            if self.executor is None:
+                pool.shutdown(wait=True)
         return jobs
 
 

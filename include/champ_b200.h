@@ -154,6 +154,15 @@ int cw_get_walkers(cw_ctx *ctx, double *x, uint64_t *rng);
  * start positions for them and call cw_set_walkers again). */
 int cw_walker_status(cw_ctx *ctx, int32_t *status);
 
+/* Device-clock stamps: cw_stamp enqueues, on the context's stream, a write of
+ * the device's global nanosecond clock into the context's next stamp slot
+ * (up to 16384 per context); cw_stamps waits for the stream, copies the first
+ * min(n, count) stamps to ns and returns the count.  Stamps around blocks of
+ * work of several contexts give the device-side timeline on which their
+ * overlap is read (no CHAMP counterpart: a serving aid). */
+int cw_stamp(cw_ctx *ctx);
+int cw_stamps(cw_ctx *ctx, int64_t *ns, int n);
+
 /* ------------------------------------------------------------------------ */
 /* Batched drop-ins for CHAMP's per-walker routines                          */
 /* ------------------------------------------------------------------------ */

@@ -56,7 +56,8 @@ def _jobs(specs):
 
 
 def _server(budget, clock, log):
-    return serve.Server(budget, engine_factory=lambda j: FakeEngine(j, clock, log), clock=clock, sleep=clock.sleep)
+    return serve.Server(budget, engine_factory=lambda j: FakeEngine(j, clock, log), clock=clock, sleep=clock.sleep,
+                        executor=serve.InlineExecutor())
 
 
 def test_budget_and_fifo_admission():
@@ -126,7 +127,8 @@ def test_failed_creation_does_not_stop_the_loop():
             raise RuntimeError("cw_create failed (status 3): out of device memory")
         return FakeEngine(j, clock, log)
 
-    srv = serve.Server(1 << 40, engine_factory=factory, clock=clock, sleep=clock.sleep)
+    srv = serve.Server(1 << 40, engine_factory=factory, clock=clock, sleep=clock.sleep,
+                        executor=serve.InlineExecutor())
     out = srv.run(jobs)
     assert "out of device memory" in out[1].failed and out[1].blocks == 0
     assert out[0].reached and out[2].reached
@@ -145,7 +147,8 @@ def test_charge_is_what_the_context_holds():
     jobs = _jobs([(16, 256, 0.0, 0.004, 50), (16, 256, 0.0, 0.004, 50)])
     one = serve.estimate_bytes(jobs[0].system, 256)
     # the budget holds both estimates, but only one context of three times the estimate
-    srv = serve.Server(4 * one, engine_factory=lambda j: BigEngine(j, clock, log), clock=clock, sleep=clock.sleep)
+    srv = serve.Server(4 * one, engine_factory=lambda j: BigEngine(j, clock, log), clock=clock, sleep=clock.sleep,
+                        executor=serve.InlineExecutor())
     srv.run(jobs)
     assert srv.peak_bytes <= srv.budget
     admits = [t for t, ev, j in srv.timeline if ev == "admit"]
@@ -156,6 +159,53 @@ def test_charge_is_what_the_context_holds():
     clock2, log2 = Clock(), []
     jb = _jobs([(16, 256, 0.0, 0.004, 50)])
     srv2 = serve.Server(2 * one, engine_factory=lambda j: BigEngine(j, clock2, log2), clock=clock2,
-                        sleep=clock2.sleep)
+                        sleep=clock2.sleep, executor=serve.InlineExecutor())
     out = srv2.run(jb)
     assert out[0].failed and out[0].blocks == 0
+
+
+class SleepEngine:
+    """A block takes `block_s` seconds of wall time on a worker thread (the
+    device's share of a real block), with the GIL released."""
+
+    def __init__(self, job, block_s=0.05):
+        import time
+        self.job, self.block_s, self.sleep = job, block_s, time.sleep
+        self.blocks = 0
+
+    def device_bytes(self):
+        return 0
+
+    def vmc_steps(self, n):
+        self.sleep(self.block_s)
+
+    def end_block(self):
+        self.blocks += 1
+
+    def results(self):
+        return dict(energy=-1.0, err=1.0)
+
+    def close(self):
+        pass
+
+
+@pytest.mark.parametrize("slots", [1, 2, 4])
+def test_worker_slots_overlap(slots):
+    """Worker threads: every admitted job has a block in flight, at most
+    `slots` at once, and blocks of different jobs overlap in time."""
+    import time
+    jobs = _jobs([(16, 64, 0.0, 1e-9, 3)] * 4)
+    srv = serve.Server(1 << 40, engine_factory=lambda j: SleepEngine(j), slots=slots)
+    t0 = time.perf_counter()
+    srv.run(jobs)
+    wall = time.perf_counter() - t0
+    assert all(j.blocks == 3 and not j.failed for j in jobs)
+    assert srv.peak_running == slots
+    # the most blocks running at any instant
+    ev = sorted([(s, 1) for _, s, e in srv.blocks] + [(e, -1) for _, s, e in srv.blocks], key=lambda x: (x[0], x[1]))
+    most = run = 0
+    for _, d in ev:
+        run += d
+        most = max(most, run)
+    assert most == slots
+    assert wall < 12 * 0.05 / slots + 0.3      # 12 blocks of 50 ms, `slots` at a time
