@@ -368,10 +368,11 @@ def run_serve(args):
     # warm-up: the module loads and every kernel is compiled into the context once
     serve.Server(budget, precision=args.precision, device=local, slots=args.slots).run(jobs(min(args.warmup, 2), None))
     srv = serve.Server(budget, precision=args.precision, device=local, slots=args.slots)
+    job_list = jobs(njobs, arrivals)     # the molecules are generated before the clock starts
     with ClockSampler(local) as clk:
         barrier(pg, local)
         t0 = time.perf_counter()
-        done = srv.run(jobs(njobs, arrivals))
+        done = srv.run(job_list)
         torch.cuda.synchronize(local)
         makespan = time.perf_counter() - t0
         barrier(pg, local)
@@ -387,6 +388,7 @@ def run_serve(args):
         "data": "synthetic",
         "config": {"workload": desc, "jobs": njobs, "rate_per_s": args.rate, "hbm_budget_gb": args.budget_gb,
                    "precision": args.precision, "block": "5 sweeps", "max_blocks": 12,
+                   "worker_slots": args.slots,
                    "parallelism": f"replicas x{world} (independent job streams)"},
         "serving": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in summ.items()},
         "peak_admitted_gb": round(srv.peak_bytes / (1 << 30), 3),

@@ -449,7 +449,8 @@ __global__ void k_tmove_select(const __grid_constant__ CSys cs, WState st, MoveB
 // T-move of the chosen electron, always accepted (icasula = -1): ratio at
 // the point, psi_D, psi_J, commit of the scalars; k_commit applies the
 // matrix and table updates.  Thread per walker.
-__global__ void k_tmove_accept(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, DmcBuf db) {
+__global__ void k_tmove_accept(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, DmcBuf db,
+                               const double *md_psidn) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   MoveScratch &m = mb.ms[w];
@@ -465,7 +466,8 @@ __global__ void k_tmove_accept(const __grid_constant__ CSys cs, WState st, MoveB
   double ratio = 0;
   for (int j = 0; j < nel; j++) ratio += sl[j] * orbn[slot[j]];
   const double detn = st.detiab[2 * w + iab] * ratio;
-  const double psidn = detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
+  // multideterminant: psi_D of the expansion at the point (k_md_move)
+  const double psidn = md_psidn ? md_psidn[w] : detn * st.detiab[2 * w + (1 - iab)] * cs.cdet;
   if (detn == 0.0) {
     st.status[w] |= 1;
     m.acc = 0;

@@ -114,7 +114,7 @@ struct cw_ctx {
   MdTab mdt{};
   MdBuf md{};
   double *md_vall = nullptr;     // [W][N][3] drift corrections of every electron (DMC)
-  size_t smem_md_hpsi = 0, smem_md_phase = 0, smem_md_move = 0, smem_md_drift = 0;
+  size_t smem_md_hpsi = 0, smem_md_phase = 0, smem_md_move = 0, smem_md_drift = 0, smem_md_tmove = 0;
   // mixed precision: tensor-core LCAO (TF32 x3) operands and tensor maps
   bool mixed = false;
   int kp = 0, np = 0, umma_st = 0;
@@ -583,7 +583,7 @@ int md_before_propose(cw_ctx *c, int iel) {
   const int W = c->W;
   if (iel == 0 || (iel == h.nup && h.ndn > 0)) {
     stage_begin(c, CW_ST_MDET);
-    k_md_phase<<<W, 128, c->smem_md_phase, c->stream>>>(c->h, c->st, c->md, c->mdt, iel == 0 ? 0 : 1);
+    k_md_phase<<<W, 128, c->smem_md_phase, c->stream>>>(c->h, c->st, c->md, c->mdt, iel == 0 ? 0 : 1, nullptr);
     stage_end(c);
     LCHK("k_md_phase");
   }
@@ -764,6 +764,7 @@ int check_status(cw_ctx *c) {
 void free_dmc(cw_ctx *c) {
   DmcHost &d = c->dmc;
   free_list(c, d.allocs);
+  c->hb.tvpsp = c->hb.tvtrj = nullptr;  // held in d.allocs
   for (void *p : {(void *)d.h_acc, (void *)d.h_wt, (void *)d.h_iage, (void *)d.h_copy})
     if (p) cudaFreeHost(p);
   d = DmcHost();
@@ -869,6 +870,7 @@ int alloc_walkers(cw_ctx *c, int W) {
   if (h.nloc > 0) DALLOC(L, b.ctilde, (size_t)W * N * K);
   m.md_velo = m.md_veln = m.md_psidn = nullptr;
   b.tvpsp = nullptr;
+  b.tvtrj = nullptr;
   b.ecp_rr = nullptr;
   if (h.nloc > 0 && c->ecp_rr_global) DALLOC(L, b.ecp_rr, (size_t)W * N * (M | 1));
   b.md_P = nullptr;
@@ -1283,6 +1285,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     c->smem_md_phase = sizeof(double) * ((size_t)numax + 1);
     c->smem_md_move = sizeof(double) * (2 * (size_t)nmax + 4 * O + (size_t)nmax * O);
     c->smem_md_drift = sizeof(double) * ((size_t)nmax + 3 * O + (size_t)nmax * O);
+    c->smem_md_tmove = sizeof(double) * (2 * O + (size_t)nmax + h.K + (h.K & 1) + 4 * (size_t)h.M * kCenRec);
     const size_t lim = 227 * 1024;
     if (c->smem_md_hpsi > lim || c->smem_md_move > lim)
       return fail(c, CW_ERR_UNSUPPORTED, "multideterminant tables exceed shared memory (nmax %d, norb %d, %d unique)",
@@ -1291,6 +1294,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     CK(raise_smem(c, k_md_phase, (size_t)(c->smem_md_phase)));
     CK(raise_smem(c, k_md_move, (size_t)(c->smem_md_move)));
     CK(raise_smem(c, k_md_drift_old, (size_t)(c->smem_md_drift)));
+    if (c->smem_md_tmove <= lim) CK(raise_smem(c, k_md_tmove, (size_t)(c->smem_md_tmove)));
   }
   if (precision == CW_PREC_MIXED) {
     // tensor-core LCAO: coefficients split once into TF32 hi/lo, [Oa][kp]
@@ -2479,10 +2483,19 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       LCHK("k_commit");
       if (int rc = md_after_commit(c, i)) return rc;
     }
-    if (d.icasula == -1)
+    if (d.icasula == -1) {
       CK(cudaMemsetAsync(c->hb.tvpsp, 0, sizeof(double) * (size_t)W * h.N * h.nquad * h.M, c->stream));
+      if (c->hb.tvtrj) CK(cudaMemsetAsync(c->hb.tvtrj, 0, sizeof(double) * (size_t)W * h.N * h.nquad * h.M, c->stream));
+    }
     int rc = run_hpsi(c, 0);
     if (rc) return rc;
+    if (d.icasula == -1 && c->md_on) {
+      // the excitations' part of the T-move elements (dmc_ps :473), from hpsi's Y
+      stage_begin(c, CW_ST_TMOVE);
+      k_md_tmove<<<W, 128, c->smem_md_tmove, c->stream>>>(c->h, c->st, c->md, c->hb, c->g);
+      stage_end(c);
+      LCHK("k_md_tmove");
+    }
     if (c->md_on) {
       stage_begin(c, CW_ST_MDET);
       k_md_drift_all<<<(unsigned)(((long)W * h.N + 3) / 4), 128, 0, c->stream>>>(c->h, c->st, c->md, c->g, c->md_vall);
@@ -2514,14 +2527,29 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
         stage_end(c);
         if (rc2) return rc2;
       }
+      if (c->md_on) {
+        // psi_D of the expansion at each walker's point: G of the moved spin
+        // (as at the start of its phase), then multideterminante
+        stage_begin(c, CW_ST_MDET);
+        k_md_phase<<<W, 128, c->smem_md_phase, c->stream>>>(c->h, c->st, c->md, c->mdt, -1, c->mb.ms);
+        k_md_move<<<W, 128, c->smem_md_move, c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, c->g, -1);
+        stage_end(c);
+        LCHK("k_md_move(tmove)");
+      }
       stage_begin(c, CW_ST_TMOVE);
-      k_tmove_accept<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, c->g, b);
+      k_tmove_accept<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, c->g, b, c->md_on ? c->md.psidn : nullptr);
       stage_end(c);
       LCHK("k_tmove_accept");
       stage_begin(c, CW_ST_COMMIT);
       launch_commit(c, -1);
       stage_end(c);
       LCHK("k_commit(tmove)");
+      if (c->md_on) {
+        stage_begin(c, CW_ST_MDET);
+        k_md_commit<<<W, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, -1);
+        stage_end(c);
+        LCHK("k_md_commit(tmove)");
+      }
     }
     CK(cudaMemcpyAsync(d.h_acc, b.acc, sizeof(double) * W * DA_NA, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(d.h_wt, b.wt, sizeof(double) * W, cudaMemcpyDeviceToHost, c->stream));
@@ -2901,13 +2929,16 @@ extern "C" int cw_dmc_set_tmoves(cw_ctx *c, int icasula) {
   if (!c || !c->dmc.on) return fail(c, CW_ERR_STATE, "cw_dmc_set_tmoves: no DMC population");
   if (icasula != 0 && icasula != -1) return fail(c, CW_ERR_UNSUPPORTED, "T-moves: icasula %d (0 or -1 supported)", icasula);
   if (icasula != 0 && c->h.nloc == 0) return fail(c, CW_ERR_ARG, "T-moves need a pseudopotential (nloc > 0)");
-  if (icasula != 0 && c->md_on)
-    return fail(c, CW_ERR_UNSUPPORTED, "T-moves of multideterminant wave functions are not implemented");
+  if (icasula != 0 && c->h.nstates > 1)
+    return fail(c, CW_ERR_UNSUPPORTED, "T-moves of multi-state wave functions are not implemented");
+  if (icasula != 0 && c->md_on && c->smem_md_tmove > 227 * 1024)
+    return fail(c, CW_ERR_UNSUPPORTED, "multideterminant T-move stage exceeds shared memory");
   BIND(c);
   DmcHost &d = c->dmc;
   if (icasula != 0 && !c->hb.tvpsp) {
     const CSys &h = c->h;
     DALLOC(d.allocs, c->hb.tvpsp, (size_t)d.mwalk * h.N * h.nquad * h.M);
+    if (c->md_on) DALLOC(d.allocs, c->hb.tvtrj, (size_t)d.mwalk * h.N * h.nquad * h.M);
   }
   d.icasula = icasula;
   return CW_OK;

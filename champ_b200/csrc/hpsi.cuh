@@ -34,6 +34,7 @@ struct HBuf {
   int kp;
   double *tvpsp;           // [W][N][nquad][M] T-move matrix elements (null without T-moves)
   double *ecp_rr;          // [W][N][M|1] k_ecp's scaled e-n distances where they do not fit shared memory (else null)
+  double *tvtrj;           // [W][N][nquad][M] radial x Jastrow factor of each T-move element (multideterminant T-moves, else null)
   // multideterminant (null for one determinant)
   double *md_P;            // [W][N][K] pseudopotential quadrature basis sums
   const double *md_den;    // [W][2] energy / kinetic corrections
@@ -741,8 +742,10 @@ __global__ void __launch_bounds__(32 * kEcpMaxWarps, MINB) k_ecp(const __grid_co
       const double trj = term * cs.wq[q] * exp(fsum);
       if (i < cs.nup) vp0 += trj * dr;
       else vp1 += trj * dr;
-      if (hb.tvpsp && lane == 0)  // transition matrix element of a T-move (nonloc.f90:296)
+      if (hb.tvpsp && lane == 0) {  // transition matrix element of a T-move (nonloc.f90:296)
         hb.tvpsp[(((size_t)w * N + i) * NQ + q) * M + ic] = dr * trj;
+        if (hb.tvtrj) hb.tvtrj[(((size_t)w * N + i) * NQ + q) * M + ic] = trj;
+      }
       if (hb.md_P) {
         // pseudopotential B matrix of every orbital (nonloc.f90:271): the
         // basis values of the point weighted by trj, contracted with coef later

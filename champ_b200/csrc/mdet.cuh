@@ -721,10 +721,16 @@ __global__ void k_md_drift_all(const __grid_constant__ CSys cs, WState st, MdBuf
     for (int k = 0; k < 3; k++) vall[((size_t)w * N + e) * 3 + k] = vel[k];
 }
 
-// G_s before the moves of spin s: CTA (128) per walker
-__global__ void __launch_bounds__(128) k_md_phase(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, int s) {
+// G_s before the moves of spin s: CTA (128) per walker.  s < 0: the spin of
+// each walker's T-move electron (ms[w].tel; walkers without one are skipped)
+__global__ void __launch_bounds__(128) k_md_phase(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, int s,
+                                                  const MoveScratch *ms) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
+  if (s < 0) {
+    if (ms[w].igeo) return;
+    s = ms[w].tel < cs.nup ? 0 : 1;
+  }
   extern __shared__ __align__(16) double smem[];
   double *G = smem;  // numax+1
   __shared__ double red[4];
@@ -826,6 +832,7 @@ __global__ void __launch_bounds__(128) k_md_drift_old(const __grid_constant__ CS
 __global__ void __launch_bounds__(128) k_md_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, MdBuf md, MdTab tab, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
+  if (iel < 0) iel = mb.ms[w].tel;  // T-move: each walker's own electron
   const int O = cs.Oa, nmax = cs.nmax;
   const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
   const int ivirt = cs.md_ivirt[s], NU = cs.md_nuniq[s];
@@ -969,6 +976,7 @@ __global__ void __launch_bounds__(128) k_md_move(const __grid_constant__ CSys cs
 __global__ void k_md_commit(const __grid_constant__ CSys cs, WState st, MoveBuf mb, MdBuf md, MdTab tab, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W || !mb.ms[w].acc) return;
+  if (iel < 0) iel = mb.ms[w].tel;  // T-move: each walker's own electron
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
   const int s = iel < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn;
   const int ivirt = cs.md_ivirt[s];
@@ -988,6 +996,90 @@ __global__ void k_md_commit(const __grid_constant__ CSys cs, WState st, MoveBuf 
   if (md.Sn_ms)
     for (int stt = threadIdx.x; stt < cs.nstates; stt += blockDim.x)
       md.S_ms[(size_t)w * cs.nstates + stt] = md.Sn_ms[(size_t)w * cs.nstates + stt];
+}
+
+// multideterminant_tmove (dmc/multideterminant_tmove.f90:3): the
+// excitations' part of every T-move element, after hpsi has built Y.  The
+// element of electron i at quadrature point x_q gains
+//   detratio * trj * sum_jrep (b(jrep) - sum_j b(occ_j) aa(j,jrep)) * Yc(jrep),
+//   Yc(jrep) = sum_{irep >= iactv} Y(jrep, irep) slmi(irep, i),
+// b the orbital values at x_q, trj the element's radial x Jastrow factor
+// (tvtrj, written by k_ecp).  Regrouped per electron as a vector over the
+// basis, Zb = coef Z with Z(v) = Yc(v) on the virtual columns minus, on each
+// occupied orbital occ_j, sum_v aa(j,v) Yc(v), each point costs one basis
+// evaluation and a dot product with Zb.  CTA (128) per walker; shared: Yc,
+// Z (O each), the aa factors (nmax), Zb (K), per warp the basis prepass.
+__global__ void __launch_bounds__(128) k_md_tmove(const __grid_constant__ CSys cs, WState st, MdBuf md, HBuf hb, GSys g) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, M = cs.M, K = cs.K, O = cs.Oa, NQ = cs.nquad, nmax = cs.nmax;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  extern __shared__ __align__(16) double smem[];
+  double *Yc = smem;                     // [O]
+  double *Z = Yc + O;                    // [O]
+  double *zo = Z + O;                    // [nmax]
+  double *Zb = zo + nmax;                // [K]
+  double *rec = Zb + K + (K & 1) + (size_t)wid * M * kCenRec;  // [M][kCenRec] per warp
+  const double detratio = st.detiab[2 * w] * st.detiab[2 * w + 1] / st.psido[w];
+  const double *sx = st.x + (size_t)w * 3 * N;
+  const double *xqw = st.xq + (size_t)w * 3 * NQ;
+  for (int i = 0; i < N; i++) {
+    const double *trow = hb.tvtrj + ((size_t)w * N + i) * NQ * M;
+    int any = 0;
+    for (int k = threadIdx.x; k < NQ * M; k += blockDim.x)
+      if (trow[k] != 0.0) any = 1;
+    if (!__syncthreads_or(any)) continue;  // the electron has no element (uniform)
+    const int s = i < cs.nup ? 0 : 1, n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+    const int ivirt = cs.md_ivirt[s], iactv = cs.md_iactv[s];
+    const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (i - ish);
+    const double *Y = md.ymat + ((size_t)w * 2 + s) * nmax * O;
+    const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+    const int *slot = g.slot_orb + s * nmax;
+    for (int v = threadIdx.x; v < O; v += blockDim.x) {
+      double y = 0;
+      if (v >= ivirt)
+        for (int irep = iactv; irep < n; irep++) y += Y[(size_t)irep * O + v] * sl[irep];
+      Yc[v] = y;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      double a = 0;
+      for (int v = ivirt; v < O; v++) a += aa[(size_t)j * O + v] * Yc[v];
+      zo[j] = a;
+    }
+    __syncthreads();
+    for (int v = threadIdx.x; v < O; v += blockDim.x) {
+      double z = v >= ivirt ? Yc[v] : 0.0;
+      for (int j = 0; j < n; j++)
+        if (slot[j] == v) z -= zo[j];
+      Z[v] = z;
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < K; m += blockDim.x) {
+      double b = 0;
+      for (int v = 0; v < O; v++) b += g.coefT[(size_t)m * O + v] * Z[v];
+      Zb[m] = b;
+    }
+    __syncthreads();
+    // the electron's quadrature points, warp per point
+    for (int u = wid; u < NQ * M; u += nw) {
+      const double trj = trow[u];
+      if (trj == 0.0) continue;
+      const int q = u / M, ic = u - q * M;
+      const double ri_v[3] = {sx[i] - cs.cent[3 * ic], sx[N + i] - cs.cent[3 * ic + 1], sx[2 * N + i] - cs.cent[3 * ic + 2]};
+      const double rin = sqrt(ri_v[0] * ri_v[0] + ri_v[1] * ri_v[1] + ri_v[2] * ri_v[2]);
+      const double xp[3] = {rin * xqw[q] + cs.cent[3 * ic], rin * xqw[NQ + q] + cs.cent[3 * ic + 1],
+                            rin * xqw[2 * NQ + q] + cs.cent[3 * ic + 2]};
+      warp_basis_prepass<0>(cs, g, xp, rec, lane);
+      __syncwarp();
+      double d = 0;
+      for (int m = lane; m < K; m += 32) warp_basis_ao<0>(cs, g, rec, m, [&](int, int, double v) { d += v * Zb[m]; });
+      d = warp_sum(d);
+      if (lane == 0) hb.tvpsp[(((size_t)w * N + i) * NQ + q) * M + ic] += detratio * trj * d;
+      __syncwarp();
+    }
+    __syncthreads();
+  }
 }
 
 }  // namespace cw

@@ -541,6 +541,10 @@ struct Walker {
   // ecp
   vector<double> vps;  // vps(i,ic,l) [i + N*(ic + M*l)]
   vector<double> tvpsp;  // t_vpsp(ic,iq,i) [(i*nquad + iq)*M + ic] of the last hpsi (T-moves)
+  // multideterminant T-moves: the quadrature points of the last nonloc
+  // (iel, ic, iq) and b_t(iorb, point) = orbital value x term_radial_jas
+  vector<int> tq_iel, tq_ic, tq_iq;
+  vector<double> tq_trj, btq;  // [npt], [npt][O]
   // estimators (estsum, forcewt, est*)
   double esum, wsum, pesum, tpbsum, acc, esum1;
   // several states: energies and psi_D of the last hpsi, block sums per state
@@ -1344,6 +1348,31 @@ struct Walker {
     const int iab = (iel == s->nup - 1) ? 1 : 0;
     compute_ymat(iab, detall[0].data(), detall[1].data(), wfmat[iab].data(), ymat[iab].data());
   }
+  // multideterminant_tmove (dmc/multideterminant_tmove.f90:3, icasula < 0):
+  // every quadrature point's T-move element gains the excitations' part,
+  // detratio * sum_{jrep >= ivirt, irep >= iactv} ymat(jrep,irep) gmat(irep,jrep)
+  // with gmat(irep,jrep) = (b_t(jrep) - sum_j b_t(occ_j) aa(j,jrep)) slmi(irep,jel).
+  // psi_D is linear in the moved electron's orbital row, so the element
+  // becomes psi_D(x_q)/psi_D(x) * term_radial_jas exactly.
+  void md_tmove(double psid) {
+    if (s->ndet == 1) return;
+    const double detratio = detiab[0] * detiab[1] / psid;
+    for (size_t q = 0; q < tq_iel.size(); q++) {
+      const int iel = tq_iel[q];
+      const int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup, jel = iel - ish;
+      const Sys::MdSpin &m = s->md[iab];
+      const double *bt = btq.data() + (size_t)O * q;
+      double sum = 0;
+      for (int jrep = m.ivirt; jrep < O; jrep++) {
+        double dum = 0;
+        for (int j = 0; j < nel; j++) dum = dum + bt[occ(j + ish)] * aa[iab][j + (size_t)nel * jrep];
+        dum = bt[jrep] - dum;
+        for (int irep = m.iactv; irep < nel; irep++)
+          sum = sum + ymat[iab][jrep + (size_t)O * irep] * (dum * slmi[iab][irep + (size_t)nel * jel]);
+      }
+      tvpsp[((size_t)iel * s->nquad + tq_iq[q]) * M + tq_ic[q]] += sum * detratio;
+    }
+  }
   // determinante_ref_grad (vmc/determinante.f90:285) with the given slmi column
   void ref_grad(int iel, const double *sl, const double *dorbv /* dorb(norb,3) */, int ldo, double *v) {
     int iab = iel < s->nup ? 0 : 1, nel = nel_of(iab), ish = iab == 0 ? 0 : s->nup;
@@ -1579,6 +1608,7 @@ struct Walker {
   void nonloc(const double *x, double *vpsp_det) {
     vpsp_det[0] = vpsp_det[1] = 0;
     std::fill(tvpsp.begin(), tvpsp.end(), 0.0);
+    tq_iel.clear(); tq_ic.clear(); tq_iq.clear(); tq_trj.clear(); btq.clear();
     // enumerate quadrature points (iel outer, ic middle, iq inner)
     struct QP { int iel, ic, iq; double costh, x[3]; };
     vector<QP> qp;
@@ -1680,6 +1710,12 @@ struct Walker {
       vpsp_det[iab] += trj * det_ratio[q];
       // transition matrix element of a T-move to this point (nonloc.f90:296-298)
       tvpsp[((size_t)iel * s->nquad + qp[q].iq) * M + ic] = det_ratio[q] * trj;
+      tq_iel.push_back(iel);
+      tq_ic.push_back(ic);
+      tq_iq.push_back(qp[q].iq);
+      tq_trj.push_back(trj);
+      if (s->ndet > 1)  // b_t (nonloc.f90:299-301) for multideterminant_tmove
+        for (int iorb = 0; iorb < O; iorb++) btq.push_back(orbq_all[iorb + (size_t)O * q] * trj);
       // pseudopotential contribution to the B matrix (nonloc.f90:271-273)
       if (s->ndet > 1)
         for (int iorb = 0; iorb < O; iorb++) bmat[iorb + (size_t)O * iel] += trj * orbq_all[iorb + (size_t)O * q];
@@ -2553,6 +2589,7 @@ bool dmc_walker(DmcPop &P, int iw, double ffi, double &wsum1, double &esum1, dou
   if (!w.hpsi(w.xold.data(), psidn, psijn, ekino, enew)) return false;
   w.psido = psidn;  // dmc_ps :516 drifts with the hpsi value of psid
   vold_all(w);
+  if (P.prm.icasula == -1 && s->nloc > 0) w.md_tmove(psidn);  // dmc_ps :473
   double taunow = tauprim * 1.0;
   double fration = fratio_of(w, tau, one);
   // calculate_reweight (icut_e=0, icut_br=0)
@@ -2631,6 +2668,8 @@ bool tmove_walker(DmcPop &P, int iw) {
   w.psijo = psijn;
   w.jassav(iel, 0);
   w.detsav(iel);
+  // dmc_ps :726-727: the moved spin's phase ends, the other spin's Y sees it
+  w.update_ymat(iel < s->nup ? s->nup - 1 : N - 1);
   P.iage[iw] = 0;
   P.tmoved[iw] = 1;
   return true;
@@ -3167,6 +3206,32 @@ int or_hpsi(void *sys, const double *x, const double *xq, const double *yq, cons
   return 0;
 }
 
+// T-move elements of one configuration (nonloc + multideterminant_tmove):
+// every quadrature point of the last nonloc (up to cap), out rows
+// (iel, ic, iq, term_radial_jas, t_vpsp); returns the count (-1: singular)
+int or_tmove_elements(void *sys, const double *x, const double *xq, const double *yq, const double *zq, int cap,
+                      double *out, double *psid_out) {
+  const Sys *s = (const Sys *)sys;
+  Walker w(s);
+  if (xq) {
+    w.xq.assign(xq, xq + s->nquad);
+    w.yq.assign(yq, yq + s->nquad);
+    w.zq.assign(zq, zq + s->nquad);
+  }
+  double psid, psij, ekin, e, extra[2];
+  if (!w.hpsi(x, psid, psij, ekin, e, extra)) return -1;
+  w.md_tmove(psid);
+  *psid_out = psid;
+  const int n = (int)w.tq_iel.size();
+  for (int q = 0; q < n && q < cap; q++) {
+    const int iel = w.tq_iel[q], ic = w.tq_ic[q], iq = w.tq_iq[q];
+    double *o = out + 5 * (size_t)q;
+    o[0] = iel; o[1] = ic; o[2] = iq; o[3] = w.tq_trj[q];
+    o[4] = w.tvpsp[((size_t)iel * s->nquad + iq) * s->M + ic];
+  }
+  return n;
+}
+
 void *or_walkers_create(void *sysp, int nwalk, const double *x, const uint64_t *rng) {
   const Sys *s = (const Sys *)sysp;
   Walkers *ws = new Walkers();
@@ -3475,7 +3540,7 @@ void or_dmc_destroy(void *p) { delete (DmcPop *)p; }
 int or_dmc_set_tmoves(void *p, int icasula) {
   DmcPop *P = (DmcPop *)p;
   if (icasula != 0 && icasula != -1) return 1;
-  if (icasula != 0 && (P->s->ndet > 1 || P->s->nloc == 0)) return 1;
+  if (icasula != 0 && (P->s->nloc == 0 || P->s->nstates > 1)) return 1;
   P->prm.icasula = icasula;
   return 0;
 }

@@ -150,6 +150,24 @@ class OracleSystem:
             raise RuntimeError("singular Slater matrix")
         return dict(energy=out[0], psid=out[1], psij=out[2], ekin=out[3], pe_local=out[4], vpsp=out[5])
 
+    def tmove_elements(self, x, quad=None, cap=1 << 16):
+        """T-move elements of one configuration after hpsi (nonloc, and
+        multideterminant_tmove for an expansion): rows (iel, ic, iq,
+        term_radial_jas, t_vpsp) of every quadrature point, and psi_D."""
+        L = lib()
+        L.or_tmove_elements.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp]
+        L.or_tmove_elements.restype = C.c_int
+        out = np.zeros((cap, 5))
+        psid = np.zeros(1)
+        if quad is None:
+            q = [None, None, None]
+        else:
+            q = [dp(np.ascontiguousarray(a, float)) for a in quad]
+        n = L.or_tmove_elements(self.h, dp(np.ascontiguousarray(x, float)), q[0], q[1], q[2], cap, dp(out), dp(psid))
+        if n < 0:
+            raise RuntimeError("singular Slater matrix")
+        return out[:min(n, cap)], float(psid[0])
+
     def orb_o(self, x, ideriv):
         """Orbital-rotation derivatives of one configuration for the 1-based
         pairs ideriv [n][2] (one determinant)."""

@@ -10,9 +10,18 @@ from conftest import rel_err
 pytestmark = pytest.mark.gpu
 
 
+def _md32():
+    from champ_b200.system import make_synthetic, rotation_expansion
+    rots = [(0, 2, 3, 0.3), (0, 1, 5, -0.25), (0, 0, 6, 0.15), (1, 1, 4, 0.2), (1, 0, 7, -0.1)]
+    md, _ = rotation_expansion(make_synthetic("tiny"), rots, extra_orbitals=4)
+    md.cdet = np.random.default_rng(3).normal(size=md.cdet.shape) * 0.3
+    md.cdet[0] = 1.0
+    return md
+
+
 def _vmc_start(oracle_mod, config, W, nslot, vmc_steps):
     from champ_b200.system import make_synthetic
-    s = make_synthetic(config)
+    s = _md32() if config == "md32" else make_synthetic(config)
     o = oracle_mod.OracleSystem(s)
     st = oracle_mod.rng_states(nslot + 2)
     xs = []
@@ -101,6 +110,27 @@ def test_dmc_tmove_parity(oracle_mod, config, W):
     do = oracle_mod.OracleDmc(o, x, rng, pop, tau=0.02, etrial=e0, mwalk=mw)
     do.set_tmoves(-1)
     for step in range(5):
+        dg.steps(1)
+        do.steps(1, 8)
+        _compare(dg, do)
+    assert dg.counts()["tmoves"] == do.tmoves() > 0
+
+
+@pytest.mark.parametrize("config,W,nstep", [("md32", 32, 5), ("c2", 6, 2)])
+def test_dmc_tmove_md_parity(oracle_mod, config, W, nstep):
+    """T-moves of multideterminant wave functions (multideterminant_tmove):
+    the elements gain the excitations' part from hpsi's Y, the chosen
+    electron's move is priced with the expansion's psi_D; same choices,
+    moved electrons and populations as the oracle, on a 32-determinant
+    expansion with permuted orbitals and on the 10^4-determinant molecule."""
+    from champ_b200.engine import Dmc, Engine
+    mw = 4 * W
+    s, o, e0, x, rng, pop = _vmc_start(oracle_mod, config, W, mw, 6)
+    dg = Dmc(Engine(s), x, rng, pop, tau=0.02, etrial=e0, mwalk=mw)
+    dg.set_tmoves(-1)
+    do = oracle_mod.OracleDmc(o, x, rng, pop, tau=0.02, etrial=e0, mwalk=mw)
+    do.set_tmoves(-1)
+    for step in range(nstep):
         dg.steps(1)
         do.steps(1, 8)
         _compare(dg, do)
