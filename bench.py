@@ -412,11 +412,16 @@ def batched_rate(systems, walkers, precision, device, steps, warmup, slots):
     import concurrent.futures as cf
     from champ_b200.engine import Engine, rng_states, start_population
     engines = []
+    tiles = {}
     off = 0
     for s, w in zip(systems, walkers):
         e = Engine(s, device=device, precision=precision)
         start_population(e, s, rng_states(off + w)[off:].copy())
         off += w
+        if precision == "fp64":   # per-system LCAO tiles (the mixed path's tensor-core kernel has one)
+            ch = e.autotune(3)
+            key = f"{ch['lcao_move_tile']}/{ch['lcao_all_tile']}"
+            tiles[key] = tiles.get(key, 0) + 1
         engines.append(e)
 
     def sweep(e, n):
@@ -437,7 +442,7 @@ def batched_rate(systems, walkers, precision, device, steps, warmup, slots):
     launches = sum(e.launches() for e in engines)
     for e in engines:
         e.close()
-    return moves / (span_ns * 1e-9), wall, own_ns * 1e-9, span_ns * 1e-9, launches
+    return moves / (span_ns * 1e-9), wall, own_ns * 1e-9, span_ns * 1e-9, launches, tiles
 
 
 def run_batched(args):
@@ -486,6 +491,8 @@ def run_batched(args):
                         "concurrency": round(v[2] / v[3], 2), "wall_s": round(v[1], 4)}
                     for p, v in res.items()},
         "mixed_over_fp64": round(res["mixed"][0] / res["fp64"][0], 3),
+        "autotuned_lcao_tiles": {"note": "N tiles (move/all-electron) picked per system by cw_autotune, FP64 path",
+                                 "systems_per_choice": res["fp64"][5]},
         "e2e": {"value": None, "unit": "electron-moves/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "path": "not measured for the batched config"},
         "clocks": clk.summary(), "gpu_launches": int(r[4]),

@@ -141,6 +141,7 @@ def load_engine(path: str | None = None):
     lib.cw_restore.argtypes = [V, C.c_void_p, C.c_long]
     lib.cw_walker_status.argtypes = [V, C.POINTER(C.c_int32)]
     lib.cw_stamp.argtypes = [V]
+    lib.cw_autotune.argtypes = [V, C.c_int, C.POINTER(C.c_int32)]
     lib.cw_stamps.argtypes = [V, C.POINTER(C.c_int64), C.c_int]
     lib.cw_psie.argtypes = [V, C.c_int, _dp, _dp, _dp]
     lib.cw_grad.argtypes = [V, C.c_int, C.c_int, _dp]
@@ -153,7 +154,7 @@ def load_engine(path: str | None = None):
               "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow", "cw_slater",
               "cw_get_sums", "cw_get_state", "cw_results_state", "cw_state_energies", "cw_opt_ci",
               "cw_opt_ci_sums", "cw_ci_o", "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
-              "cw_walker_status", "cw_stamp", "cw_stamps", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o"):
+              "cw_walker_status", "cw_stamp", "cw_stamps", "cw_autotune", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o"):
         getattr(lib, f).restype = C.c_int
     if path is None:
         _engine = lib
@@ -169,7 +170,7 @@ EXPORTED_SYMBOLS = [
     "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore", "cw_dmc_set_tmoves", "cw_dmc_counts",
     "cw_device_bytes", "cw_results_state", "cw_state_energies", "cw_opt_ci", "cw_opt_ci_sums", "cw_ci_o",
     "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
-    "cw_walker_status", "cw_stamp", "cw_stamps", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o",
+    "cw_walker_status", "cw_stamp", "cw_stamps", "cw_autotune", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

@@ -67,6 +67,15 @@ struct CSys {
 
 static_assert(sizeof(CSys) <= 31 * 1024, "the system block must fit a kernel parameter list");
 
+// asynchronous 8-byte global -> shared copy (sm_80+): a thread issues all of
+// its copies back to back and waits once (cp_async8_wait) before the block
+// barrier that publishes them
+__device__ __forceinline__ void cp_async8(double *dst_smem, const double *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Global-memory tables of the system.
 struct GSys {
   const double *rwf, *d2rwf;      // [nctype][mrwf][mpts]
@@ -444,6 +453,60 @@ __device__ __forceinline__ void een_apply1f(const float *__restrict__ BD, float 
     fc = fc * z + a;
     fi = fi * z + ax;
     fj = fj * z + ay;
+  }
+}
+
+// een_apply1f for P partners of one (moved electron, centre) at once: each
+// (B, dB, B', dB') quad is loaded once for all of them
+template <int NORD, int P>
+__device__ __forceinline__ void een_apply1f_multi(const float *__restrict__ BD, const float (&y)[P], const float (&z)[P],
+                                                  float (&fc)[P], float (&fu)[P], float (&fi)[P], float (&fj)[P]) {
+  const float4 *bd = reinterpret_cast<const float4 *>(BD);
+#pragma unroll
+  for (int q = 0; q < P; q++) {
+    fc[q] = 0; fu[q] = 0; fi[q] = 0; fj[q] = 0;
+  }
+#pragma unroll
+  for (int k = NORD - 1; k >= 0; k--) {
+    const int pmin = een_pmin(k), pmax = een_pmax(NORD, k), off = een_offp(NORD, k);
+    float4 v[een_lenp(NORD, 1) / 2];
+#pragma unroll
+    for (int q = 0; q < een_lenp(NORD, k); q += 2) v[q / 2] = bd[(off + q) / 2];
+#define EEN_B(p) (((p) - pmin) % 2 ? v[((p) - pmin) / 2].z : v[((p) - pmin) / 2].x)
+#define EEN_D(p) (((p) - pmin) % 2 ? v[((p) - pmin) / 2].w : v[((p) - pmin) / 2].y)
+    float a[P], ax[P], ay[P];
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      a[q] = EEN_B(pmax);
+      ax[q] = EEN_D(pmax);
+      ay[q] = 0;
+    }
+#pragma unroll
+    for (int p = pmax - 1; p >= pmin; p--) {
+#pragma unroll
+      for (int q = 0; q < P; q++) {
+        ay[q] = ay[q] * y[q] + a[q];
+        a[q] = a[q] * y[q] + EEN_B(p);
+        ax[q] = ax[q] * y[q] + EEN_D(p);
+      }
+    }
+#undef EEN_B
+#undef EEN_D
+    if (pmin == 1) {
+#pragma unroll
+      for (int q = 0; q < P; q++) {
+        ay[q] = ay[q] * y[q] + a[q];
+        a[q] *= y[q];
+        ax[q] *= y[q];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      fu[q] = fu[q] * z[q] + fc[q];
+      fc[q] = fc[q] * z[q] + a[q];
+      fi[q] = fi[q] * z[q] + ax[q];
+      fj[q] = fj[q] * z[q] + ay[q];
+    }
   }
 }
 

@@ -147,8 +147,11 @@ __device__ __forceinline__ double ae_term(double tau) {
 // thread per walker: drift + diffusion of electron iel (dmc_ps's Gaussian
 // around the drifted point; dmc_ae's Gaussian / exponential mixture for an
 // all-electron wave function)
-__global__ void k_dmc_propose(const __grid_constant__ CSys cs, WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, int iel) {
+__global__ void k_dmc_propose(const __grid_constant__ CSys cs, WState st, MoveBuf mb, DmcBuf db, DmcScalars sc, int iel,
+                              int *acc_count) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  // acc_count (optional): the accepted-walker count k_dmc_decide appends to
+  if (acc_count && w == 0) *acc_count = 0;
   if (w >= st.W) return;
   const int N = cs.N;
   double vo[3];
@@ -207,7 +210,8 @@ __global__ void k_dmc_propose(const __grid_constant__ CSys cs, WState st, MoveBu
 
 // thread per walker: ratio and drift at the new point, reverse diffusion,
 // acceptance p = |psi_n/psi_o|^2 G(o<-n)/G(n<-o) with the age boost
-__global__ void k_dmc_decide(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalars sc, int iel) {
+__global__ void k_dmc_decide(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, DmcBuf db, DmcScalars sc, int iel,
+                             int *acc_list, int *acc_count) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
@@ -277,6 +281,7 @@ __global__ void k_dmc_decide(const __grid_constant__ CSys cs, WState st, MoveBuf
   rng.store(st.rng + 4 * (size_t)w);
   m.acc = a;
   m.ratio = ratio;
+  if (a && acc_list) acc_list[atomicAdd(acc_count, 1)] = w;  // for the commit (order free)
   if (a) {
     acc[DA_IACCEPT] = 1;
     acc[DA_NACC] += 1;

@@ -71,6 +71,7 @@ struct cw_ctx {
   unsigned long long *d_stamps = nullptr;  // device-clock stamps (cw_stamp), kStampCap slots
   int nstamp = 0;
   int commit_grid = 1;     // k_commit_tile's grid: the blocks resident at once
+  int gemm_bn_move = 64, gemm_bn_all = 64;  // N tiles of the FP64 LCAO GEMMs (cw_autotune)
   int big_spin = 0;        // Slater inverse and c~ on global memory (spins too large for shared memory)
   int ecp_rr_global = 0;   // k_ecp's e-n distances on global memory (hb.ecp_rr)
   int *acc_list = nullptr, *acc_count = nullptr;  // accepted walkers of a move (k_accept_list)
@@ -283,7 +284,7 @@ void launch_jmove(cw_ctx *c, int iel) {
   const int warps = 4;
   dim3 grid((c->W + warps - 1) / warps);
   if (c->mixed)
-    k_jastrow_move_f32<NORD><<<grid, 32 * warps, c->smem_jmove_f32, c->stream>>>(c->h, c->st, c->mb, iel);
+    k_jastrow_move_f32<NORD, kJmF32Partners><<<grid, 32 * warps, c->smem_jmove_f32, c->stream>>>(c->h, c->st, c->mb, iel);
   else
     k_jastrow_move<NORD><<<grid, 32 * warps, c->smem_jmove, c->stream>>>(c->h, c->st, c->mb, iel);
 }
@@ -322,7 +323,7 @@ int set_attrs(cw_ctx *c) {
     }
   }
   CK(raise_smem(c, k_jastrow_move<NORD>, (size_t)(c->smem_jmove)));
-  CK(raise_smem(c, k_jastrow_move_f32<NORD>, (size_t)(c->smem_jmove_f32)));
+  CK(raise_smem(c, k_jastrow_move_f32<NORD, kJmF32Partners>, (size_t)(c->smem_jmove_f32)));
   CK(raise_smem(c, k_jastrow_full<NORD, double>, c->smem_jfull));
   CK(raise_smem(c, k_jastrow_full<NORD, float>, c->smem_jfull));
   if (c->h.nloc > 0) {
@@ -563,7 +564,7 @@ __global__ void k_split_rows(const double *src, int rows, int K, float *hi, floa
 int lcao(cw_ctx *c, bool move, int M, const double *phi64, double *out) {
   const CSys &h = c->h;
   if (!c->mixed) {
-    dgemm(c->stream, M, h.Oa, h.K, phi64, c->g.coefT, out);
+    dgemm(c->stream, M, h.Oa, h.K, phi64, c->g.coefT, out, move ? c->gemm_bn_move : c->gemm_bn_all);
     return launch_check(c, "dgemm");
   }
   const CUtensorMap &ahi = move ? c->tm_mv_hi : c->tm_all_hi;
@@ -1248,7 +1249,10 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(raise_smem(c, k_basis_all, (size_t)(c->smem_basis)));
   CK(raise_smem(c, k_slater_inv, (size_t)(c->smem_sinv)));
   CK(raise_smem(c, k_ctilde, (size_t)(c->smem_ctil)));
-  CK(raise_smem(c, k_dgemm_mma, (size_t)(kMmaSmem)));
+  CK(raise_smem(c, k_dgemm_mma<32>, mma_smem(32)));
+  CK(raise_smem(c, k_dgemm_mma<48>, mma_smem(48)));
+  CK(raise_smem(c, k_dgemm_mma<64>, mma_smem(64)));
+  CK(raise_smem(c, k_dgemm_mma<80>, mma_smem(80)));
   c->mixed = precision == CW_PREC_MIXED;
   c->ecp_naov = d->ndet > 1 ? h.K : 0;  // the ECP stage keeps the point's basis values for the B matrix
   int rc = nord_attrs(c);
@@ -1283,8 +1287,8 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     const size_t O = h.Oa;
     c->smem_md_hpsi = sizeof(double) * (4 * (size_t)nmax * nmax + (h.nstates > 1 ? 3 : 1) * (size_t)nmax * O + numax + 1);
     c->smem_md_phase = sizeof(double) * ((size_t)numax + 1);
-    c->smem_md_move = sizeof(double) * (2 * (size_t)nmax + 4 * O + (size_t)nmax * O);
-    c->smem_md_drift = sizeof(double) * ((size_t)nmax + 3 * O + (size_t)nmax * O);
+    c->smem_md_move = sizeof(double) * (2 * (size_t)nmax + 4 * O + (size_t)nmax * O + 3 * (size_t)nmax);
+    c->smem_md_drift = sizeof(double) * ((size_t)nmax + 3 * O + (size_t)nmax * O + 3 * (size_t)nmax);
     c->smem_md_tmove = sizeof(double) * (2 * O + (size_t)nmax + h.K + (h.K & 1) + 4 * (size_t)h.M * kCenRec);
     const size_t lim = 227 * 1024;
     if (c->smem_md_hpsi > lim || c->smem_md_move > lim)
@@ -1389,6 +1393,46 @@ int cw_set_walkers(cw_ctx *c, int nwalk, const double *x, const uint64_t *rng) {
   CK(cudaMemsetAsync(c->st.status, 0, sizeof(int) * nwalk, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return zerest(c);
+}
+
+int cw_autotune(cw_ctx *c, int reps, int32_t *choice) {
+  if (!c) return CW_ERR_ARG;
+  if (c->W == 0) return fail(c, CW_ERR_STATE, "cw_autotune: no walkers");
+  BIND(c);
+  const CSys &h = c->h;
+  reps = std::max(1, reps);
+  // N tile of the FP64 tensor-core LCAO for this context's two shapes (the
+  // move's 4 rows per walker, the all-electron chunk's 5 rows per electron):
+  // each candidate timed on the context's own scratch buffers, which every
+  // sweep rewrites before reading, so the walk is untouched
+  auto tune = [&](int M, const double *A, double *C, int &best) -> int {
+    float tbest = 0;
+    for (int bn : kMmaTiles) {
+      dgemm(c->stream, M, h.Oa, h.K, A, c->g.coefT, C, bn);  // warm-up
+      CK(cudaEventRecord(c->ev0, c->stream));
+      for (int r = 0; r < reps; r++) dgemm(c->stream, M, h.Oa, h.K, A, c->g.coefT, C, bn);
+      CK(cudaEventRecord(c->ev1, c->stream));
+      CK(cudaEventSynchronize(c->ev1));
+      LCHK("dgemm(autotune)");
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      if (bn == kMmaTiles[0] || ms < tbest) {
+        tbest = ms;
+        best = bn;
+      }
+    }
+    return CW_OK;
+  };
+  if (!c->mixed) {
+    if (int rc = tune(c->W * 4, c->mb.phi, c->mb.orbn, c->gemm_bn_move)) return rc;
+    if (int rc = tune(c->W * c->hb.chunk * 5, c->hb.phi, c->hb.orball, c->gemm_bn_all)) return rc;
+  }
+  drop_sweep_graph(c);  // the next sweep is captured with the chosen tiles
+  if (choice) {
+    choice[0] = c->gemm_bn_move;
+    choice[1] = c->gemm_bn_all;
+  }
+  return CW_OK;
 }
 
 int cw_stamp(cw_ctx *c) {
@@ -2311,8 +2355,11 @@ extern "C" int cw_dmc_init(cw_ctx *c, int nwalk, int mwalk, const double *x, con
                            const uint64_t *pop_rng, double tau, double etrial, int nfprod) {
   if (!c || nwalk <= 0 || mwalk < nwalk || !x || !rng || !pop_rng || !(tau > 0) || nfprod < 1)
     return fail(c, CW_ERR_ARG, "cw_dmc_init: bad arguments");
-  if (c->h.nstates > 1)
-    return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: several states are a VMC feature (dmc_ps samples one state)");
+  // several states: dmc_ps propagates and estimates state 1 alone (psidn(1),
+  // enew(1)); the other CI vectors ride along unused.  Sampling a guiding
+  // function is a VMC feature.
+  if (c->h.nstates > 1 && c->h.iguiding > 0)
+    return fail(c, CW_ERR_UNSUPPORTED, "cw_dmc_init: a guiding function (iguiding > 0) is a VMC feature");
   BIND(c);
   int rc = dmc_alloc(c, mwalk);
   if (rc) return rc;
@@ -2454,7 +2501,8 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
     for (int i = 0; i < h.N; i++) {
       if (int rc = md_before_propose(c, i)) return rc;
       stage_begin(c, CW_ST_PROPOSE);
-      k_dmc_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, b, sc, i);
+      k_dmc_propose<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, b, sc, i,
+                                                        c->smem_commit ? c->acc_count : nullptr);
       stage_end(c);
       LCHK("k_dmc_propose");
       stage_begin(c, CW_ST_JASTROW_MOVE);
@@ -2474,11 +2522,12 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       }
       if (int rc = md_after_lcao(c, i)) return rc;
       stage_begin(c, CW_ST_ACCEPT);
-      k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, c->g, b, sc, i);
+      k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, c->g, b, sc, i,
+                                                       c->smem_commit ? c->acc_list : nullptr, c->acc_count);
       stage_end(c);
       LCHK("k_dmc_decide");
       stage_begin(c, CW_ST_COMMIT);
-      launch_commit(c, i);
+      launch_commit(c, i, true);
       stage_end(c);
       LCHK("k_commit");
       if (int rc = md_after_commit(c, i)) return rc;

@@ -122,14 +122,18 @@ k_dgemm(int M, int N, int K, const double *__restrict__ A, const double *__restr
 
 // ---------------------------------------------------------------------------
 // FP64 tensor-core variant (mma.sync m16n8k4 .f64; tcgen05 has no FP64 kind):
-// 128x64 output tile per CTA, 4 warps of 32x64 (2x8 m16n8 accumulators in
-// registers), 16-deep K slices in a 3-stage cp.async ring.  Shared rows are
-// padded (A: 20 doubles, B: 68) so that the fragment loads of a half-warp hit
-// 16 distinct 8-byte bank pairs.  Needs K and N even (16-byte row chunks);
-// out-of-range chunks are zero-filled by the copy.
+// 128 x BN output tile per CTA, 4 warps of 32 x BN (2 x BN/8 m16n8
+// accumulators in registers), 16-deep K slices in a 3-stage cp.async ring.
+// Shared rows are padded (A: 20 doubles, B: BN + 4) so that the fragment
+// loads of a half-warp hit 16 distinct 8-byte bank pairs.  Needs K and N even
+// (16-byte row chunks); out-of-range chunks are zero-filled by the copy.  BN
+// (32, 48, 64 or 80 orbitals) is picked per context by timing (cw_autotune);
+// every output element sums its K slices in the same order whatever the tile.
 // ---------------------------------------------------------------------------
-constexpr int kMmaBM = 128, kMmaBN = 64, kMmaBK = 16, kMmaSA = kMmaBK + 4, kMmaSB = kMmaBN + 4, kMmaStages = 3;
-constexpr size_t kMmaSmem = sizeof(double) * (size_t)kMmaStages * (kMmaBM * kMmaSA + kMmaBK * kMmaSB);
+constexpr int kMmaBM = 128, kMmaBK = 16, kMmaSA = kMmaBK + 4, kMmaStages = 3;
+constexpr size_t mma_smem(int bn) {
+  return sizeof(double) * (size_t)kMmaStages * (kMmaBM * kMmaSA + kMmaBK * (bn + 4));
+}
 
 __device__ __forceinline__ void cp_async16(double *dst, const double *src, int bytes) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -146,9 +150,10 @@ __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], const double (&a)[2]
                : "d"(a[0]), "d"(a[1]), "d"(b));
 }
 
+template <int BN>
 __global__ void __launch_bounds__(128, 2)
 k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C) {
-  constexpr int BM = kMmaBM, BN = kMmaBN, BK = kMmaBK, SA = kMmaSA, SB = kMmaSB, ST = kMmaStages;
+  constexpr int BM = kMmaBM, BK = kMmaBK, SA = kMmaSA, SB = BN + 4, ST = kMmaStages, NI = BN / 8;
   extern __shared__ __align__(16) double gsm[];
   double *As = gsm;                          // [ST][BM][SA]
   double *Bs = gsm + (size_t)ST * BM * SA;   // [ST][BK][SB]
@@ -173,11 +178,11 @@ k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__r
       cp_async16(Bs + ((size_t)s * BK + r) * SB + nc, ok ? B + (size_t)gk * N + gn : B, ok ? 16 : 0);
     }
   };
-  double acc[2][8][4];
+  double acc[2][NI][4];
 #pragma unroll
   for (int mi = 0; mi < 2; mi++)
 #pragma unroll
-    for (int ni = 0; ni < 8; ni++)
+    for (int ni = 0; ni < NI; ni++)
 #pragma unroll
       for (int q = 0; q < 4; q++) acc[mi][ni][q] = 0.0;
 #pragma unroll
@@ -194,18 +199,18 @@ k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__r
     const double *bs = Bs + (size_t)(kt % ST) * BK * SB;
 #pragma unroll
     for (int k4 = 0; k4 < BK; k4 += 4) {
-      double a[2][2], b[8];
+      double a[2][2], b[NI];
 #pragma unroll
       for (int mi = 0; mi < 2; mi++) {
         a[mi][0] = as[(mi * 16 + g) * SA + k4 + t];
         a[mi][1] = as[(mi * 16 + g + 8) * SA + k4 + t];
       }
 #pragma unroll
-      for (int ni = 0; ni < 8; ni++) b[ni] = bs[(k4 + t) * SB + ni * 8 + g];
+      for (int ni = 0; ni < NI; ni++) b[ni] = bs[(k4 + t) * SB + ni * 8 + g];
 #pragma unroll
       for (int mi = 0; mi < 2; mi++)
 #pragma unroll
-        for (int ni = 0; ni < 8; ni++) dmma_16x8x4(acc[mi][ni], a[mi], b[ni]);
+        for (int ni = 0; ni < NI; ni++) dmma_16x8x4(acc[mi][ni], a[mi], b[ni]);
     }
   }
   cp_async_wait<0>();
@@ -217,7 +222,7 @@ k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__r
       const int gm = m0 + warp * 32 + mi * 16 + g + 8 * h;
       if (gm >= M) continue;
 #pragma unroll
-      for (int ni = 0; ni < 8; ni++) {
+      for (int ni = 0; ni < NI; ni++) {
         const int gn = n0 + ni * 8 + 2 * t;
         if (gn < N) *reinterpret_cast<double2 *>(C + (size_t)gm * N + gn) = make_double2(acc[mi][ni][2 * h], acc[mi][ni][2 * h + 1]);
       }
@@ -225,11 +230,25 @@ k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__r
   }
 }
 
-inline void dgemm(cudaStream_t s, int M, int N, int K, const double *A, const double *B, double *C) {
+// N tiles of the tensor-core GEMM the autotuner chooses from
+constexpr int kMmaTiles[4] = {32, 48, 64, 80};
+
+template <int BN>
+inline void launch_dgemm_mma(cudaStream_t s, int M, int N, int K, const double *A, const double *B, double *C) {
+  dim3 grid((M + kMmaBM - 1) / kMmaBM, (N + BN - 1) / BN);
+  k_dgemm_mma<BN><<<grid, 128, mma_smem(BN), s>>>(M, N, K, A, B, C);
+}
+
+// bn: N tile of the tensor-core kernel (one of kMmaTiles)
+inline void dgemm(cudaStream_t s, int M, int N, int K, const double *A, const double *B, double *C, int bn = 64) {
   const bool al16 = ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(C)) & 15) == 0;
   if (N > 16 && (K % 2) == 0 && (N % 2) == 0 && al16) {
-    dim3 grid((M + kMmaBM - 1) / kMmaBM, (N + kMmaBN - 1) / kMmaBN);
-    k_dgemm_mma<<<grid, 128, kMmaSmem, s>>>(M, N, K, A, B, C);
+    switch (bn) {
+      case 32: launch_dgemm_mma<32>(s, M, N, K, A, B, C); break;
+      case 48: launch_dgemm_mma<48>(s, M, N, K, A, B, C); break;
+      case 80: launch_dgemm_mma<80>(s, M, N, K, A, B, C); break;
+      default: launch_dgemm_mma<64>(s, M, N, K, A, B, C); break;
+    }
   } else if (N <= 16) {
     constexpr int BM = 64, BN = 16, BK = 16, TM = 4, TN = 1;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);

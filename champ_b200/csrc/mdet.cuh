@@ -681,23 +681,32 @@ __global__ void k_md_zero(double *p, size_t n) {
 }
 
 // drift operands t_k[v] = b_k[v] - sum_j b_k[occ_j] aa[j][v] of one
-// electron (multideterminante_grad's gmat without the slmi factor), shared
+// electron (multideterminante_grad's gmat without the slmi factor), shared.
+// The occupied orbitals' values b_k[occ_j] are staged in bo [3][n] first, so
+// the column sums read shared memory only.  Ends with a block barrier.
 __device__ __forceinline__ void md_form_t(const CSys &cs, int s, const double *b0, const double *b1, const double *b2,
-                                          const double *aa, const int *slot_orb, double *t) {
+                                          const double *aa, const int *slot_orb, double *t, double *bo) {
   const int n = s == 0 ? cs.nup : cs.ndn, O = cs.Oa, ivirt = cs.md_ivirt[s];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const int oj = slot_orb[j];
+    bo[j] = b0[oj];
+    bo[n + j] = b1[oj];
+    bo[2 * n + j] = b2[oj];
+  }
+  __syncthreads();
   for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) {
     double t0 = 0, t1 = 0, t2 = 0;
     for (int j = 0; j < n; j++) {
       const double a = aa[j * O + v];
-      const int oj = slot_orb[j];
-      t0 += b0[oj] * a;
-      t1 += b1[oj] * a;
-      t2 += b2[oj] * a;
+      t0 += bo[j] * a;
+      t1 += bo[n + j] * a;
+      t2 += bo[2 * n + j] * a;
     }
     t[v] = b0[v] - t0;
     t[O + v] = b1[v] - t1;
     t[2 * O + v] = b2[v] - t2;
   }
+  __syncthreads();
 }
 
 // drift correction of every electron at the current configuration right
@@ -747,7 +756,7 @@ __global__ void __launch_bounds__(128) k_md_phase(const __grid_constant__ CSys c
 // matrix: vel = detratio * sum_kk d_kk G_kk sum_jr t[ro_jr] (M_kk^-1 c)[jr]
 // with c the column of A^-1 of the electron (the Y contraction regrouped per
 // excitation).  CTA (128) per walker; shared: c (nmax), t (3*O), aa (nmax*O).
-__global__ void __launch_bounds__(128) k_md_drift_old(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, GSys g, int iel) {
+__global__ void __launch_bounds__(128, 5) k_md_drift_old(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
@@ -756,14 +765,16 @@ __global__ void __launch_bounds__(128) k_md_drift_old(const __grid_constant__ CS
   double *c = smem;              // nmax
   double *t = c + nmax;          // 3*O
   double *A = t + 3 * O;         // nmax*O
+  double *bo = A + (size_t)nmax * O;  // 3*nmax
   __shared__ double red[4];
   const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
   const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+  for (int q = threadIdx.x; q < n * O; q += blockDim.x) cp_async8(A + q, aa + q);
   for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = sl[j];
-  for (int q = threadIdx.x; q < n * O; q += blockDim.x) A[q] = aa[q];
+  cp_async8_wait();
   __syncthreads();
   md_form_t(cs, s, md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O, md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O,
-            md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O, A, g.slot_orb + s * nmax, t);
+            md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O, A, g.slot_orb + s * nmax, t, bo);
   __syncthreads();
   const double *G = md.G + (size_t)w * (cs.iguiding > 0 ? cs.nstates : 1) * (tab.numax + 1);
   if (cs.iguiding > 0) {
@@ -829,7 +840,7 @@ __global__ void __launch_bounds__(128) k_md_drift_old(const __grid_constant__ CS
 // phi_new(occ_i) aa[i][v]) / R (the Sherman-Morrison form of
 // slmin * orb_new), the excitation ratios, S, psi_D and the drift at the new
 // point.  Shared: c, slot values (nmax each), w (O), t (3*O), aa_new (nmax*O).
-__global__ void __launch_bounds__(128) k_md_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, MdBuf md, MdTab tab, GSys g, int iel) {
+__global__ void __launch_bounds__(128, 5) k_md_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, MdBuf md, MdTab tab, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   if (iel < 0) iel = mb.ms[w].tel;  // T-move: each walker's own electron
@@ -842,6 +853,7 @@ __global__ void __launch_bounds__(128) k_md_move(const __grid_constant__ CSys cs
   double *wv = ps + nmax;                 // O
   double *t = wv + O;                     // 3*O
   double *An = t + 3 * O;                 // nmax*O
+  double *bo = An + (size_t)nmax * O;     // 3*nmax
   __shared__ double red[4];
   __shared__ double s_R;
   if (mb.ms[w].igeo) {
@@ -850,6 +862,9 @@ __global__ void __launch_bounds__(128) k_md_move(const __grid_constant__ CSys cs
   }
   const double *orbn = mb.orbn + (size_t)w * 4 * O;
   const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
+  // the spin's aa block lands in shared memory while the ratio is formed
+  const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+  for (int q = threadIdx.x; q < n * O; q += blockDim.x) cp_async8(An + q, aa + q);
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     c[j] = sl[j];
     ps[j] = orbn[g.slot_orb[s * nmax + j]];
@@ -860,26 +875,25 @@ __global__ void __launch_bounds__(128) k_md_move(const __grid_constant__ CSys cs
     for (int j = 0; j < n; j++) r += c[j] * ps[j];
     s_R = r;
   }
+  cp_async8_wait();
   __syncthreads();
   const double R = s_R;
   if (R == 0.0) {
     if (threadIdx.x == 0) md.psidn[w] = 0.0;
     return;
   }
-  const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
   for (int v = ivirt + threadIdx.x; v < O; v += blockDim.x) {
     double tt = 0;
-    for (int i = 0; i < n; i++) tt += ps[i] * aa[i * O + v];
+    for (int i = 0; i < n; i++) tt += ps[i] * An[i * O + v];
     wv[v] = (orbn[v] - tt) / R;
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < n * O; q += blockDim.x) {
-    const int i = q / O, v = q % O;
-    An[q] = v >= ivirt ? aa[q] + c[i] * wv[v] : 0.0;
-  }
+  for (int i = threadIdx.x >> 5; i < n; i += blockDim.x >> 5)  // warps over rows, lanes over columns
+    for (int v = threadIdx.x & 31; v < O; v += 32)
+      An[i * O + v] = v >= ivirt ? An[i * O + v] + c[i] * wv[v] : 0.0;
   __syncthreads();
   // column iel of the updated inverse is c / R; drift operands at the new point
-  md_form_t(cs, s, orbn + O, orbn + 2 * O, orbn + 3 * O, An, g.slot_orb + s * nmax, t);
+  md_form_t(cs, s, orbn + O, orbn + 2 * O, orbn + 3 * O, An, g.slot_orb + s * nmax, t, bo);
   __syncthreads();
   for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = c[j] / R;
   __syncthreads();

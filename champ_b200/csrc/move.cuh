@@ -524,8 +524,14 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(const __grid_constant__
 // per-pair value and gradients); coordinates differ in FP64 before the cast,
 // and the row sums against the stored FP64 tables (dfs, dv) stay FP64.
 // ---------------------------------------------------------------------------
-template <int NORD>
-__global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
+// partners per lane of k_jastrow_move_f32: four share each coefficient quad
+// load (235 registers unbounded; bounded to three blocks per SM it spills a
+// little and measured 29.0 against 30.9 ms per 8192-walker sweep for one
+// partner, and 36.0 with two blocks per SM and no spills)
+constexpr int kJmF32Partners = 4;
+
+template <int NORD, int P>
+__global__ void __launch_bounds__(128, P == 1 ? 8 : (P == 2 ? 4 : 3)) k_jastrow_move_f32(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
   extern __shared__ __align__(16) float smemf[];
   constexpr int NB = een_nbp(NORD);        // padded (B, dB) pairs per centre
   constexpr int PER = 8 + 2 * NB;         // shared floats per centre (B 16-byte aligned)
@@ -569,71 +575,110 @@ __global__ void __launch_bounds__(128, 8) k_jastrow_move_f32(const __grid_consta
   const double *xw = st.x + (size_t)w * 3 * N;
   const double *fso_i = st.fso + ((size_t)w * N + iel) * N;
   double dfs = 0, dv0 = 0, dv1 = 0, dv2 = 0;
-  for (int jj = lane; jj < N; jj += 32) {
-    if (jj == iel) continue;
-    const double xj[3] = {xw[jj], xw[N + jj], xw[2 * N + jj]};
-    const int i = jj < iel ? iel : jj, j = jj < iel ? jj : iel;
-    int isb, ipar;
-    double sspinn_d;
-    pair_spin(cs, i, j, isb, ipar, sspinn_d);
-    const float sspinn = (float)sspinn_d;
-    const float rvee[3] = {(float)(xi[0] - xj[0]), (float)(xi[1] - xj[1]), (float)(xi[2] - xj[2])};
-    const float rij = sqrtf(rvee[0] * rvee[0] + rvee[1] * rvee[1] + rvee[2] * rvee[2]);
-    float u, dd1, dd2;
-    scale2<float>(cs, rij, u, dd1, dd2);
-    float fs = 0, gi[3] = {0, 0, 0}, gj[3] = {0, 0, 0};
-    if (u != asym) {
-      float fee, feeu, feeuu;
-      ee_term<1, float>(cs, isb, ipar, sspinn, u, fee, feeu, feeuu);
-      feeu = feeu * dd1 / rij;
-      fs += fee;
-      for (int k = 0; k < 3; k++) {
-        gi[k] += feeu * rvee[k];
-        gj[k] -= feeu * rvee[k];
+  // each lane takes P partners (jj, jj + 32, ...): every coefficient quad
+  // loaded from shared memory serves all of them
+  for (int j0 = lane; j0 < N; j0 += 32 * P) {
+    bool ok[P];
+    int jj[P];
+    double xj[P][3];
+    float rvee[P][3], rij[P], z[P], du_r[P], fs[P], gi[P][3], gj[P][3];
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      jj[q] = j0 + 32 * q;
+      ok[q] = jj[q] < N && jj[q] != iel;
+      // a slot past the end or on the moved electron computes on a valid
+      // neighbour and is discarded
+      const int jc = ok[q] ? jj[q] : (iel == 0 ? N - 1 : 0);
+      jj[q] = jc == jj[q] ? jj[q] : jc;
+      xj[q][0] = xw[jc]; xj[q][1] = xw[N + jc]; xj[q][2] = xw[2 * N + jc];
+      const int i = jc < iel ? iel : jc, j = jc < iel ? jc : iel;
+      int isb, ipar;
+      double sspinn_d;
+      pair_spin(cs, i, j, isb, ipar, sspinn_d);
+      const float sspinn = (float)sspinn_d;
+      for (int k = 0; k < 3; k++) rvee[q][k] = (float)(xi[k] - xj[q][k]);
+      rij[q] = sqrtf(rvee[q][0] * rvee[q][0] + rvee[q][1] * rvee[q][1] + rvee[q][2] * rvee[q][2]);
+      float u, dd1, dd2;
+      scale2<float>(cs, rij[q], u, dd1, dd2);
+      fs[q] = 0;
+      for (int k = 0; k < 3; k++) gi[q][k] = gj[q][k] = 0;
+      if (u != asym) {
+        float fee, feeu, feeuu;
+        ee_term<1, float>(cs, isb, ipar, sspinn, u, fee, feeu, feeuu);
+        feeu = feeu * dd1 / rij[q];
+        fs[q] += fee;
+        for (int k = 0; k < 3; k++) {
+          gi[q][k] += feeu * rvee[q][k];
+          gj[q][k] -= feeu * rvee[q][k];
+        }
       }
+      z[q] = 1 - kap * u;
+      du_r[q] = (-kap * dd1) / rij[q];
     }
     if (NORD > 1) {
-      const float z = 1 - kap * u;
-      const float du = -kap * dd1;
-      const float du_r = du / rij;
-      const float *en_rr = st.enmf + (size_t)w * 2 * M * N + jj;
+      // partners' table values two centres ahead
+      const float *en_rr = st.enmf + (size_t)w * 2 * M * N;
       const float *en_h = en_rr + (size_t)M * N;
-      // partner table values two centres ahead
-      float nrr = en_rr[0], nh = en_h[0];
-      float nrr2 = M > 1 ? en_rr[N] : 0.0f, nh2 = M > 1 ? en_h[N] : 0.0f;
+      float nrr[P], nh[P], nrr2[P], nh2[P];
+#pragma unroll
+      for (int q = 0; q < P; q++) {
+        nrr[q] = en_rr[jj[q]];
+        nh[q] = en_h[jj[q]];
+        nrr2[q] = M > 1 ? en_rr[N + jj[q]] : 0.0f;
+        nh2[q] = M > 1 ? en_h[N + jj[q]] : 0.0f;
+      }
       for (int ic = 0; ic < M; ic++) {
-        const float rrj = nrr, hj = nh;
-        nrr = nrr2;
-        nh = nh2;
-        if (ic + 2 < M) {
-          nrr2 = en_rr[(size_t)(ic + 2) * N];
-          nh2 = en_h[(size_t)(ic + 2) * N];
-        }
+        float rrj[P], hj[P], y[P];
+        bool any = false;
         const float rri = sh_s[ic];
-        if (rri == asym && rrj == asym) continue;
-        const float rj_v[3] = {(float)(xj[0] - cs.cent[3 * ic]), (float)(xj[1] - cs.cent[3 * ic + 1]),
-                               (float)(xj[2] - cs.cent[3 * ic + 2])};
-        float fc, fu_, fi_, fj_;
-        een_apply1f<NORD>(sh_B + (size_t)ic * 2 * NB, 1 - kap * rrj, z, fc, fu_, fi_, fj_);
-        const float fu = fu_ * du_r;
-        const float fi = fi_ * sh_g[ic];
-        const float fj = fj_ * (-kap) * hj;
-        fs += fc;
-        for (int k = 0; k < 3; k++) {
-          gi[k] += fi * sh_rv[k * M + ic] + fu * rvee[k];
-          gj[k] += fj * rj_v[k] - fu * rvee[k];
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+          rrj[q] = nrr[q];
+          hj[q] = nh[q];
+          nrr[q] = nrr2[q];
+          nh[q] = nh2[q];
+          if (ic + 2 < M) {
+            nrr2[q] = en_rr[(size_t)(ic + 2) * N + jj[q]];
+            nh2[q] = en_h[(size_t)(ic + 2) * N + jj[q]];
+          }
+          any |= ok[q] && !(rri == asym && rrj[q] == asym);
+          y[q] = 1 - kap * rrj[q];
+        }
+        if (!any) continue;
+        float fc[P], fu_[P], fi_[P], fj_[P];
+        een_apply1f_multi<NORD, P>(sh_B + (size_t)ic * 2 * NB, y, z, fc, fu_, fi_, fj_);
+        const double c0 = cs.cent[3 * ic], c1 = cs.cent[3 * ic + 1], c2 = cs.cent[3 * ic + 2];
+        const float gic = sh_g[ic];
+        const float rv[3] = {sh_rv[ic], sh_rv[M + ic], sh_rv[2 * M + ic]};
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+          if (rri == asym && rrj[q] == asym) continue;  // this pair-centre term is cut
+          const float rj_v[3] = {(float)(xj[q][0] - c0), (float)(xj[q][1] - c1), (float)(xj[q][2] - c2)};
+          const float fu = fu_[q] * du_r[q];
+          const float fi = fi_[q] * gic;
+          const float fj = fj_[q] * (-kap) * hj[q];
+          fs[q] += fc[q];
+          for (int k = 0; k < 3; k++) {
+            gi[q][k] += fi * rv[k] + fu * rvee[q][k];
+            gj[q][k] += fj * rj_v[k] - fu * rvee[q][k];
+          }
         }
       }
     }
-    mb.fsn[(size_t)w * N + jj] = fs;
-    for (int k = 0; k < 3; k++) {
-      mb.fijn_i[((size_t)w * 3 + k) * N + jj] = gi[k];
-      mb.fijn_j[((size_t)w * 3 + k) * N + jj] = gj[k];
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      if (!ok[q]) continue;
+      const int jq = jj[q];
+      mb.fsn[(size_t)w * N + jq] = fs[q];
+      for (int k = 0; k < 3; k++) {
+        mb.fijn_i[((size_t)w * 3 + k) * N + jq] = gi[q][k];
+        mb.fijn_j[((size_t)w * 3 + k) * N + jq] = gj[q][k];
+      }
+      dfs += (double)fs[q] - fso_i[jq];
+      dv0 += (double)gi[q][0] - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + jq];
+      dv1 += (double)gi[q][1] - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + jq];
+      dv2 += (double)gi[q][2] - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + jq];
     }
-    dfs += (double)fs - fso_i[jj];
-    dv0 += (double)gi[0] - st.fijo[(((size_t)w * 3 + 0) * N + iel) * N + jj];
-    dv1 += (double)gi[1] - st.fijo[(((size_t)w * 3 + 1) * N + iel) * N + jj];
-    dv2 += (double)gi[2] - st.fijo[(((size_t)w * 3 + 2) * N + iel) * N + jj];
   }
   // e-n part of the moved electron
   float fen_s = 0, ge0 = 0, ge1 = 0, ge2 = 0;

@@ -135,6 +135,13 @@ class Engine:
         self._check(self.lib.cw_walker_status(self.h, out.ctypes.data_as(C.POINTER(C.c_int32))), "cw_walker_status")
         return out
 
+    def autotune(self, reps: int = 5) -> dict:
+        """Pick the LCAO GEMM tiles of this context by timing (cw_autotune);
+        returns the chosen N tiles."""
+        out = np.zeros(2, np.int32)
+        self._check(self.lib.cw_autotune(self.h, int(reps), out.ctypes.data_as(C.POINTER(C.c_int32))), "cw_autotune")
+        return dict(lcao_move_tile=int(out[0]), lcao_all_tile=int(out[1]))
+
     def sync(self):
         """Wait for the context's queued work."""
         self._check(self.lib.cw_sync(self.h), "cw_sync")

@@ -161,6 +161,15 @@ int cw_walker_status(cw_ctx *ctx, int32_t *status);
  * work of several contexts give the device-side timeline on which their
  * overlap is read (no CHAMP counterpart: a serving aid). */
 int cw_stamp(cw_ctx *ctx);
+
+/* Tile autotuner (no CHAMP counterpart): times each N tile (32, 48, 64, 80
+ * orbitals) of the FP64 tensor-core LCAO contraction on this context's two
+ * shapes (the move's 4 rows per walker, the all-electron chunk's 5 rows per
+ * electron), reps launches each, and keeps the fastest; the choice changes
+ * no result (every output sums its K slices in the same order).  Needs the
+ * walkers (cw_set_walkers); choice [2] (nullable) receives the move and
+ * all-electron tiles.  The mixed path's tensor-core kernel has one tile. */
+int cw_autotune(cw_ctx *ctx, int reps, int32_t *choice);
 int cw_stamps(cw_ctx *ctx, int64_t *ns, int n);
 
 /* ------------------------------------------------------------------------ */

@@ -130,8 +130,48 @@ def test_multistate_refusals():
     s.weights_g = np.array([0.0, 1.0, 1.0])      # state 1 must carry weight
     with pytest.raises(EngineError):
         Engine(s)
-    s.iguiding = 0
+    s.weights_g = np.array([1.0, 1.0, 1.0])      # DMC does not sample a guiding function
     rng = rng_states(9)
     x = initial_configs(s, rng[:4].copy())
-    with pytest.raises(EngineError):
+    with pytest.raises(EngineError, match="guiding"):
         Dmc(Engine(s), x, rng[:8], rng[8], tau=0.01, etrial=-1.0, mwalk=8)
+
+
+def test_multistate_dmc_is_state_one(oracle_mod):
+    """dmc_ps propagates and estimates state 1 alone (psidn(1), enew(1)):
+    DMC of the three-state wave function takes the same steps as DMC of its
+    first CI vector on its own (same populations, walkers, weights and
+    energies), and the oracle agrees."""
+    import copy
+    from champ_b200.engine import Dmc, Engine
+    s3 = _system()
+    s1 = copy.deepcopy(s3)
+    s1.cdet_states = None
+    W, mw = 16, 64
+    o = oracle_mod.OracleSystem(s1)
+    st = oracle_mod.rng_states(mw + 2)
+    xs = []
+    for w in range(W):
+        x, st[w] = o.sites(st[w])
+        xs.append(x)
+    vw = oracle_mod.OracleWalkers(o, np.array(xs), st[:W])
+    vw.steps(8, 4)
+    vw.end_block()
+    x, r = vw.walkers()
+    rng = np.concatenate([r, st[W:mw]])
+    e0 = vw.results()["energy"]
+    runs = {}
+    for name, s in (("three", s3), ("one", s1)):
+        d = Dmc(Engine(s), x, rng, st[mw], tau=0.01, etrial=e0, mwalk=mw)
+        d.steps(5)
+        runs[name] = d.walkers()
+    do = oracle_mod.OracleDmc(o, x, rng, st[mw], tau=0.01, etrial=e0, mwalk=mw)
+    do.steps(5, 4)
+    ref = do.walkers()
+    for name in ("three", "one"):
+        xg, wg, eg, rg = runs[name]
+        assert len(wg) == len(ref[1])
+        assert np.array_equal(rg, ref[3])
+        assert rel_err(xg, ref[0]) < 1e-9 and rel_err(wg, ref[1]) < 1e-9 and rel_err(eg, ref[2]) < 1e-9
+    assert np.array_equal(runs["three"][3], runs["one"][3])
+    assert rel_err(runs["three"][2], runs["one"][2]) < 1e-12
