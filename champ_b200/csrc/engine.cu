@@ -489,10 +489,13 @@ int md_define(cw_ctx *c, const cw_system_desc *d, std::vector<int> &exc, std::ve
       iwun[i] = j;
       if (j == i) uniq.push_back(i);
     }
-    for (int pass = 0; pass < 3; pass++)
+    // grouped by excitation order (1, 2, 3, then 4 and above), so that the
+    // lanes of a warp, which take consecutive unique determinants, run the
+    // same-size solve
+    for (int pass = 0; pass < 4; pass++)
       for (int k : uniq) {
         const int nr = numrep[k * 2 + iab];
-        if ((pass == 0 && nr == 1) || (pass == 1 && nr == 2) || (pass == 2 && nr > 2)) order[iab].push_back(k);
+        if ((pass < 3 && nr == pass + 1) || (pass == 3 && nr > 3)) order[iab].push_back(k);
       }
     std::vector<int> kidx(nd, -1);
     for (size_t kk = 0; kk < order[iab].size(); kk++) kidx[order[iab][kk]] = (int)kk;
