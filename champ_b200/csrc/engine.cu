@@ -2219,6 +2219,10 @@ static __device__ __align__(256) double cw_noalloc_phi[CW_NOALLOC_SCRATCH_DOUBLE
 namespace {
 constexpr int kNoallocMaxDevices = 64;
 double *g_noalloc_scratch[kNoallocMaxDevices] = {nullptr};
+// the last call's completion on each device: the next call, from any
+// context (any stream), waits for it before it writes the shared array
+std::mutex g_noalloc_mu;
+cudaEvent_t g_noalloc_done[kNoallocMaxDevices] = {nullptr};
 
 // The array's name is only a host-side stand-in for the device symbol: its
 // device address is looked up once per device, with that device current.
@@ -2270,11 +2274,23 @@ extern "C" int cw_orbitals_noalloc(cw_ctx *c, int npts, const double *xyz, doubl
   double *phi = nullptr;
   int rc = noalloc_scratch(c, &phi);
   if (rc) return rc;
+  // calls on different contexts run on different streams: order them on the
+  // device through the previous call's completion event (outside stream
+  // capture; a captured call is ordered by its graph's launches)
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(c->stream, &cap));
+  cudaEvent_t &done = g_noalloc_done[c->device];
+  if (cap == cudaStreamCaptureStatusNone) {
+    if (!done) CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CK(cudaStreamWaitEvent(c->stream, done, 0));
+  }
   const long nt = (long)npts * h.M;
   k_basis_points<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->h, c->g, npts, xyz, phi);
   LCHK("k_basis_points");
   dgemm(c->stream, npts * 5, h.Oa, h.K, phi, c->g.coefT, out);
   LCHK("dgemm(noalloc)");
+  if (cap == cudaStreamCaptureStatusNone) CK(cudaEventRecord(done, c->stream));
   return CW_OK;
 }
 

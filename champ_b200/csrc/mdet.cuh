@@ -997,9 +997,9 @@ __global__ void k_md_commit(const __grid_constant__ CSys cs, WState st, MoveBuf 
   double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
   const double *cv = md.cvec + (size_t)w * nmax;
   const double *wg = md.wvec + (size_t)w * O;
-  for (int q = threadIdx.x; q < n * O; q += blockDim.x) {
-    const int i = q / O, v = q % O;
-    if (v >= ivirt) aa[q] = aa[q] + cv[i] * wg[v];
+  for (int i = threadIdx.x >> 5; i < n; i += blockDim.x >> 5) {  // warps over rows, lanes over columns
+    const double ci = cv[i];
+    for (int v = ivirt + (threadIdx.x & 31); v < O; v += 32) aa[i * O + v] = aa[i * O + v] + ci * wg[v];
   }
   double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
   for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) dd[kk] = md.ddn[(size_t)w * tab.numax + kk];

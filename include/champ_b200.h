@@ -363,13 +363,12 @@ int cw_stage_times(cw_ctx *ctx, double *ms, long *launches);
  * (CW_ERR_ARG otherwise).  The first call on a device looks up that array's
  * device address (make that first call before any stream capture).  The work
  * is queued on the context's stream: out is ready after cw_sync.  All calls
- * share the one array.  Before a context launches on a device it waits for
- * the work of the context that used the device before it, so calls made one
- * after another (from one host thread, or from threads that take turns) do
- * not overlap on the GPU.  Calls made at the same moment from several host
- * threads, on contexts of the same device, can overlap and then race on the
- * array.  The first-call address lookup is not locked; threads racing there
- * store the same address, which is harmless. */
+ * share the one array.  Each call's work waits on the device for the previous
+ * call's (a per-device completion event, taken under a host lock), so calls
+ * from any contexts and host threads do not overlap on the GPU; calls made
+ * inside a stream capture are ordered by their graphs' launches only.  The
+ * first-call address lookup is not locked; threads racing there store the
+ * same address, which is harmless. */
 int cw_orbitals_noalloc(cw_ctx *ctx, int npts, const double *xyz, double *out);
 
 /* ------------------------------------------------------------------------ */
