@@ -643,6 +643,12 @@ int opt_derivs(cw_ctx *c) {
     k_orb_o<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(c->h, c->st, nt, c->orb_terms, c->orb_nv, c->orb_vals,
                                                                 c->opt_o, c->opt_ot, c->opt_np, c->opt_np - nt);
     LCHK("k_orb_o");
+    if (c->md_on) {
+      const size_t smem = sizeof(double) * ((size_t)c->h.Oa * c->h.nmax + (size_t)c->h.nmax * c->h.nmax);
+      k_md_orb_o<<<W, 128, smem, c->stream>>>(c->h, c->st, c->md, nt, c->orb_terms, c->orb_nv, c->orb_vals, c->opt_o,
+                                               c->opt_ot, c->opt_np, c->opt_np - nt);
+      LCHK("k_md_orb_o");
+    }
   }
   return CW_OK;
 }
@@ -1301,6 +1307,10 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
     CK(raise_smem(c, k_md_phase, (size_t)(c->smem_md_phase)));
     CK(raise_smem(c, k_md_move, (size_t)(c->smem_md_move)));
     CK(raise_smem(c, k_md_drift_old, (size_t)(c->smem_md_drift)));
+    {
+      const size_t zs = sizeof(double) * ((size_t)O * nmax + (size_t)nmax * nmax);
+      if (zs <= lim) CK(raise_smem(c, k_md_orb_o, zs));
+    }
     if (c->smem_md_tmove <= lim) CK(raise_smem(c, k_md_tmove, (size_t)(c->smem_md_tmove)));
   }
   if (precision == CW_PREC_MIXED) {
@@ -1817,6 +1827,7 @@ int cw_opt_setup(cw_ctx *c, int ci, int njas, const double *jas_map, int with_ov
         vorb.push_back(jo);
       }
       terms[t].v = v;
+      terms[t].io = io;
       for (int iab = 0; iab < 2; iab++) {
         const int nel = iab == 0 ? c->h.nup : c->h.ndn, ish = iab == 0 ? 0 : c->h.nup;
         terms[t].slot[iab] = -1;
@@ -1874,10 +1885,11 @@ int cw_jas_o(cw_ctx *c, double *out) {
 int cw_opt_orb(cw_ctx *c, int norbterm, const int32_t *ideriv) {
   if (!c || norbterm < 0 || (norbterm > 0 && !ideriv)) return CW_ERR_ARG;
   if (norbterm > 0) {
-    if (c->md_on)
-      return fail(c, CW_ERR_UNSUPPORTED,
-                  "orbital-rotation derivatives of multideterminant expansions are not implemented (one determinant)");
     if (c->h.nstates > 1) return fail(c, CW_ERR_UNSUPPORTED, "orbital-rotation derivatives of several states");
+    if (c->md_on && norbterm > 1024)
+      return fail(c, CW_ERR_UNSUPPORTED, "orbital rotations of an expansion: at most 1024 pairs (%d)", norbterm);
+    if (c->md_on && sizeof(double) * ((size_t)c->h.Oa * c->h.nmax + (size_t)c->h.nmax * c->h.nmax) > 227 * 1024)
+      return fail(c, CW_ERR_UNSUPPORTED, "orbital rotations of an expansion: zmat tables exceed shared memory");
     for (int t = 0; t < norbterm; t++) {
       const int io = ideriv[2 * t], jo = ideriv[2 * t + 1];
       if (io < 1 || io > c->h.Oa || jo < 1 || jo > c->h.Oa || io == jo)

@@ -226,6 +226,7 @@ namespace cw {
 struct OrbTerm {
   int slot[2];  // slot of io in the up / down determinant (-1: io not there)
   int v;        // index of jo in the list of rotation targets
+  int io;       // io itself (active-orbital index, 0-based)
 };
 
 // values of the rotation targets at the electrons [e0, e0+ne) of every
@@ -262,5 +263,68 @@ __global__ void k_orb_o(const __grid_constant__ CSys cs, WState st, int nterm, c
   }
   o[(size_t)w * np + off + k] = sum;
   ot[(size_t)(off + k) * st.W + w] = sum;
+}
+// Expansions: optorb_deriv's excitation part (vmc/optorb.f90:62-84), added
+// to k_orb_o's reference part: detratio * sum over spins of
+//   sum_i zmat(io,i) orb(i,jo)   (io a virtual orbital, io >= ivirt)
+// - sum_i aaz(irep,i) orb(i,jo)  (io held by the reference at slot irep),
+// with compute_zmat's (vmc/multideterminant.f90:491-560)
+//   zmat(v,irep) = sum_{krep >= iactv} Y(v,krep) slmi(krep,irep)   (v >= ivirt)
+//   aaz(j,irep)  = sum_{v >= ivirt} aa(j,v) zmat(v,irep).
+// CTA per walker; shared: zmat [O][nmax] and aaz [nmax][nmax] of one spin.
+__global__ void __launch_bounds__(128) k_md_orb_o(const __grid_constant__ CSys cs, WState st, MdBuf md, int nterm,
+                                                  const OrbTerm *__restrict__ terms, int nv,
+                                                  const double *__restrict__ vals, double *o, double *ot, int np,
+                                                  int off) {
+  const int w = blockIdx.x;
+  if (w >= st.W) return;
+  const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
+  extern __shared__ __align__(16) double smem[];
+  double *zm = smem;                       // [O][nmax]: zmat(v, irep) at v * nmax + irep
+  double *az = zm + (size_t)O * nmax;      // [nmax][nmax]: aaz(j, irep) at j * nmax + irep
+  const double detratio = st.detiab[2 * w] * st.detiab[2 * w + 1] / st.psido[w];
+  // each thread keeps the running sums of its terms across the two spins
+  constexpr int kMaxPer = 8;
+  double dpsi[kMaxPer];
+  for (int q = 0; q < kMaxPer; q++) dpsi[q] = 0.0;
+  for (int s = 0; s < 2; s++) {
+    const int n = s == 0 ? cs.nup : cs.ndn, ish = s == 0 ? 0 : cs.nup;
+    if (n == 0) continue;
+    const int ivirt = cs.md_ivirt[s], iactv = cs.md_iactv[s];
+    const double *Y = md.ymat + ((size_t)w * 2 + s) * nmax * O;   // Y(v, krep) at krep * O + v
+    const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;    // aa(j, v) at j * O + v
+    const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax;
+    __syncthreads();  // the previous spin's tables are no longer read
+    for (int q = threadIdx.x; q < (O - ivirt) * n; q += blockDim.x) {
+      const int v = ivirt + q / n, irep = q - (q / n) * n;
+      double z = 0;
+      for (int krep = iactv; krep < n; krep++) z += Y[(size_t)krep * O + v] * sl[krep + (size_t)n * irep];
+      zm[(size_t)v * nmax + irep] = z;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+      const int j = q / n, irep = q - (q / n) * n;
+      double z = 0;
+      for (int v = ivirt; v < O; v++) z += aa[(size_t)j * O + v] * zm[(size_t)v * nmax + irep];
+      az[(size_t)j * nmax + irep] = z;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x, q = 0; k < nterm && q < kMaxPer; k += blockDim.x, q++) {
+      const OrbTerm tm = terms[k];
+      const double *ov = vals + ((size_t)w * N + ish) * nv + tm.v;  // orb(ish + i, jo) at i * nv
+      double d = dpsi[q];
+      if (tm.io >= ivirt)
+        for (int i = 0; i < n; i++) d = d + zm[(size_t)tm.io * nmax + i] * ov[(size_t)i * nv];
+      const int irep = tm.slot[s];
+      if (irep >= 0)
+        for (int i = 0; i < n; i++) d = d - az[(size_t)irep * nmax + i] * ov[(size_t)i * nv];
+      dpsi[q] = d;
+    }
+  }
+  for (int k = threadIdx.x, q = 0; k < nterm && q < kMaxPer; k += blockDim.x, q++) {
+    const double v = dpsi[q] * detratio + o[(size_t)w * np + off + k];
+    o[(size_t)w * np + off + k] = v;
+    ot[(size_t)(off + k) * st.W + w] = v;
+  }
 }
 }  // namespace cw

@@ -2866,6 +2866,53 @@ int or_orb_o(void *sysp, const double *x, int nterm, const int *ideriv, double *
     }
     out[t] = o;
   }
+  if (s->ndet == 1) return 0;
+  // expansions: optorb_deriv's orbprim (vmc/optorb.f90:46-95) adds
+  // detratio * dorb_psi, dorb_psi = sum over spins of sum_i zmat(io,i) orb(i,jo)
+  // (io virtual) - sum_i aaz(irep,i) orb(i,jo) (io in the reference), with
+  // compute_zmat's (vmc/multideterminant.f90:491-560)
+  // zmat(jrep,irep) = sum_{krep >= iactv} ymat(jrep,krep) slmi(krep,irep) and
+  // aaz(jrep,irep) = sum_{krep >= ivirt} aa(jrep,krep) zmat(krep,irep)
+  const int O = s->O;
+  const double detratio = w.detiab[0] * w.detiab[1] / psid;
+  vector<double> zmat[2], aaz[2];
+  for (int iab = 0; iab < 2; iab++) {
+    const int nel = iab == 0 ? s->nup : s->ndn;
+    const Sys::MdSpin &m = s->md[iab];
+    zmat[iab].assign((size_t)O * std::max(nel, 1), 0.0);
+    aaz[iab].assign((size_t)std::max(nel, 1) * std::max(nel, 1), 0.0);
+    if (nel == 0) continue;
+    for (int irep = 0; irep < nel; irep++)
+      for (int jrep = m.ivirt; jrep < O; jrep++) {
+        double z = 0;
+        for (int krep = m.iactv; krep < nel; krep++)
+          z = z + w.ymat[iab][jrep + (size_t)O * krep] * w.slmi[iab][krep + (size_t)nel * irep];
+        zmat[iab][jrep + (size_t)O * irep] = z;
+      }
+    for (int irep = 0; irep < nel; irep++)
+      for (int jrep = 0; jrep < nel; jrep++) {
+        double z = 0;
+        for (int krep = m.ivirt; krep < O; krep++)
+          z = z + w.aa[iab][jrep + (size_t)nel * krep] * zmat[iab][krep + (size_t)O * irep];
+        aaz[iab][jrep + (size_t)nel * irep] = z;
+      }
+  }
+  for (int t = 0; t < nterm; t++) {
+    const int io = ideriv[2 * t] - 1, jo = ideriv[2 * t + 1] - 1;
+    double dpsi = 0;
+    for (int iab = 0; iab < 2; iab++) {
+      const int nel = iab == 0 ? s->nup : s->ndn, ish = iab == 0 ? 0 : s->nup;
+      if (nel == 0) continue;
+      if (io >= s->md[iab].ivirt)
+        for (int i = 0; i < nel; i++) dpsi = dpsi + zmat[iab][io + (size_t)O * i] * w.orb[(ish + i) + N * jo];
+      int irep = -1;
+      for (int j = 0; j < nel; j++)
+        if (s->iworbd[ish + j] - 1 == io) irep = j;
+      if (irep >= 0)
+        for (int i = 0; i < nel; i++) dpsi = dpsi - aaz[iab][irep + (size_t)nel * i] * w.orb[(ish + i) + N * jo];
+    }
+    out[t] = dpsi * detratio + out[t];
+  }
   return 0;
 }
 

@@ -82,3 +82,39 @@ def test_orb_step_first_order(oracle_mod):
         pred = o.orb_o(x[w], terms) @ da
         got = _lnpsid(oracle_mod, apply_step(s, terms, da), x[w]) - _lnpsid(oracle_mod, s, x[w])
         assert abs(got - pred) <= 1e-3 * abs(pred) + 1e-12
+
+
+def _md32():
+    from champ_b200.system import make_synthetic, rotation_expansion
+    rots = [(0, 2, 3, 0.3), (0, 1, 5, -0.25), (0, 0, 6, 0.15), (1, 1, 4, 0.2), (1, 0, 7, -0.1)]
+    md, _ = rotation_expansion(make_synthetic("tiny"), rots, extra_orbitals=4)
+    md.cdet = np.random.default_rng(3).normal(size=md.cdet.shape) * 0.3
+    md.cdet[0] = 1.0
+    return _with_virtuals(md, 2, seed=8)
+
+
+def test_orb_o_finite_differences_multideterminant(oracle_mod):
+    """Expansions (optorb_deriv's zmat and aaz terms, compute_zmat): d ln psi
+    / d a of every varied pair of a 32-determinant expansion with permuted
+    orbital lists against central differences of the expansion's psi_D."""
+    from champ_b200.engine import initial_configs, rng_states
+    from champ_b200.orbital_opt import apply_step, orb_terms
+    s = _md32()
+    terms = orb_terms(s, nadorb=2)
+    assert len(terms) > 0
+    rng = rng_states(3)
+    x = initial_configs(s, rng)
+    o = oracle_mod.OracleSystem(s)
+    h = 1e-5
+    worst = 0.0
+    for w in range(3):
+        d = o.orb_o(x[w], terms)
+        for t in range(len(terms)):
+            da = np.zeros(len(terms))
+            da[t] = h
+            fp = _lnpsid(oracle_mod, apply_step(s, terms, da), x[w])
+            fm = _lnpsid(oracle_mod, apply_step(s, terms, -da), x[w])
+            fd = (fp - fm) / (2 * h)
+            worst = max(worst, abs(d[t] - fd) / max(1.0, abs(fd)))
+            assert abs(d[t] - fd) <= 1e-6 * max(1.0, abs(fd)), (w, tuple(terms[t]), d[t], fd)
+    print(f"{len(terms)} pairs, worst difference {worst:.1e}")
