@@ -403,12 +403,15 @@ def run_serve(args):
     return 0
 
 
-def batched_rate(systems, walkers, precision, device, steps, warmup, slots):
-    """Sweeps of every system's own context, issued from `slots` worker
-    threads (each context on its own stream).  Returns electron-moves/s over
-    the device-clock span of the timed sweeps (first start stamp to last end
-    stamp of all contexts), the wall time, and the summed device time of the
-    contexts' own sweeps."""
+def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode="graph"):
+    """Sweeps of every system's own context, all at once: mode "graph" runs
+    them as one CUDA graph of the contexts' sweep graphs (cw_batch_vmc_steps,
+    one launch per sweep, timed with the batch's events); mode "threads"
+    issues each context's sweeps from `slots` worker threads on its own stream
+    (timed from device-clock stamps; the summed device time of the contexts'
+    own sweeps is returned too).  Returns electron-moves/s over the device
+    span of the timed sweeps, the wall time, that sum (None for "graph"), the
+    span, the launches and the autotuned tiles."""
     import concurrent.futures as cf
     from champ_b200.engine import Engine, rng_states, start_population
     engines = []
@@ -424,25 +427,37 @@ def batched_rate(systems, walkers, precision, device, steps, warmup, slots):
             tiles[key] = tiles.get(key, 0) + 1
         engines.append(e)
 
-    def sweep(e, n):
-        e.stamp()
-        e.vmc_steps(n)
-        e.stamp()
-        e.sync()
-
-    with cf.ThreadPoolExecutor(max_workers=slots) as pool:
-        list(pool.map(lambda e: sweep(e, warmup), engines))      # graph capture + warm-up
-        t0 = time.perf_counter()
-        list(pool.map(lambda e: sweep(e, steps), engines))
-        wall = time.perf_counter() - t0
-    st = [e.stamps()[-2:] for e in engines]
-    span_ns = max(int(b) for _, b in st) - min(int(a) for a, _ in st)
-    own_ns = sum(int(b) - int(a) for a, b in st)
     moves = sum(w * s.nelec for s, w in zip(systems, walkers)) * steps
+    if mode == "graph":
+        # one CUDA graph of all systems' sweep graphs: one launch per sweep
+        from champ_b200.engine import Batch
+        b = Batch(engines)
+        b.vmc_steps(warmup)                                      # captures + warm-up
+        t0 = time.perf_counter()
+        b.vmc_steps(steps)
+        wall = time.perf_counter() - t0
+        span_s = b.last_ms() * 1e-3
+        b.close()
+        own_s = None
+    else:
+        def sweep(e, n):
+            e.stamp()
+            e.vmc_steps(n)
+            e.stamp()
+            e.sync()
+
+        with cf.ThreadPoolExecutor(max_workers=slots) as pool:
+            list(pool.map(lambda e: sweep(e, warmup), engines))  # graph capture + warm-up
+            t0 = time.perf_counter()
+            list(pool.map(lambda e: sweep(e, steps), engines))
+            wall = time.perf_counter() - t0
+        st = [e.stamps()[-2:] for e in engines]
+        span_s = (max(int(b) for _, b in st) - min(int(a) for a, _ in st)) * 1e-9
+        own_s = sum(int(b) - int(a) for a, b in st) * 1e-9
     launches = sum(e.launches() for e in engines)
     for e in engines:
         e.close()
-    return moves / (span_ns * 1e-9), wall, own_ns * 1e-9, span_ns * 1e-9, launches, tiles
+    return moves / span_s, wall, own_s, span_s, launches, tiles
 
 
 def run_batched(args):
@@ -468,6 +483,10 @@ def run_batched(args):
             barrier(pg, local)
             res[prec] = batched_rate(systems, walkers, prec, local, args.steps, max(args.warmup, 1), args.slots)
             barrier(pg, local)
+        barrier(pg, local)
+        threads = batched_rate(systems, walkers, args.precision, local, args.steps, max(args.warmup, 1), args.slots,
+                               mode="threads")
+        barrier(pg, local)
     value = max_over_ranks(1.0 / res[args.precision][0], pg, local)
     value = world / value
     if rank != 0:
@@ -483,13 +502,18 @@ def run_batched(args):
         "config": {"workload": desc, "systems": nsys, "electrons_min_max": [int(nel.min()), int(nel.max())],
                    "walkers_total": int(sum(walkers)), "walker_scale": round(scale, 4),
                    "walker_note": "drawn counts scaled so that all systems' contexts fit the HBM budget at once",
-                   "hbm_budget_gb": args.budget_gb, "worker_threads": args.slots, "precision": args.precision,
+                   "hbm_budget_gb": args.budget_gb, "precision": args.precision,
+                   "batching": "all systems' sweeps in one CUDA graph (cw_batch_vmc_steps)",
                    "l2": "per-walker state of every system far exceeds the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
-        "batched": {p: {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4),
-                        "sum_of_context_device_s": round(v[2], 4),
-                        "concurrency": round(v[2] / v[3], 2), "wall_s": round(v[1], 4)}
+        "batched": {p: {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4), "wall_s": round(v[1], 4),
+                        "mode": "one CUDA graph of all systems' sweep graphs, one launch per sweep"}
                     for p, v in res.items()},
+        "batched_threads": {"precision": args.precision, "moves_per_s": round(threads[0], 1),
+                            "device_span_s": round(threads[3], 4),
+                            "sum_of_context_device_s": round(threads[2], 4),
+                            "concurrency": round(threads[2] / threads[3], 2), "wall_s": round(threads[1], 4),
+                            "mode": f"each system's sweeps from {args.slots} worker threads on its own stream"},
         "mixed_over_fp64": round(res["mixed"][0] / res["fp64"][0], 3),
         "autotuned_lcao_tiles": {"note": "N tiles (move/all-electron) picked per system by cw_autotune, FP64 path",
                                  "systems_per_choice": res["fp64"][5]},

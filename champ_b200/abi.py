@@ -142,6 +142,16 @@ def load_engine(path: str | None = None):
     lib.cw_walker_status.argtypes = [V, C.POINTER(C.c_int32)]
     lib.cw_stamp.argtypes = [V]
     lib.cw_autotune.argtypes = [V, C.c_int, C.POINTER(C.c_int32)]
+    lib.cw_batch_create.argtypes = [C.POINTER(V), C.POINTER(V), C.c_int]
+    lib.cw_batch_create.restype = C.c_int
+    lib.cw_batch_vmc_steps.argtypes = [V, C.c_int]
+    lib.cw_batch_vmc_steps.restype = C.c_int
+    lib.cw_batch_last_ms.argtypes = [V]
+    lib.cw_batch_last_ms.restype = C.c_float
+    lib.cw_batch_last_error.argtypes = [V]
+    lib.cw_batch_last_error.restype = C.c_char_p
+    lib.cw_batch_destroy.argtypes = [V]
+    lib.cw_batch_destroy.restype = None
     lib.cw_stamps.argtypes = [V, C.POINTER(C.c_int64), C.c_int]
     lib.cw_psie.argtypes = [V, C.c_int, _dp, _dp, _dp]
     lib.cw_grad.argtypes = [V, C.c_int, C.c_int, _dp]
@@ -154,7 +164,8 @@ def load_engine(path: str | None = None):
               "cw_results", "cw_hpsi", "cw_orbitals", "cw_jastrow", "cw_slater",
               "cw_get_sums", "cw_get_state", "cw_results_state", "cw_state_energies", "cw_opt_ci",
               "cw_opt_ci_sums", "cw_ci_o", "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
-              "cw_walker_status", "cw_stamp", "cw_stamps", "cw_autotune", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o"):
+              "cw_walker_status", "cw_stamp", "cw_stamps", "cw_autotune", "cw_psie", "cw_grad", "cw_commit",
+              "cw_update_ymat", "cw_opt_orb", "cw_orb_o"):
         getattr(lib, f).restype = C.c_int
     if path is None:
         _engine = lib
@@ -170,7 +181,8 @@ EXPORTED_SYMBOLS = [
     "cw_checkpoint_bytes", "cw_checkpoint", "cw_restore", "cw_dmc_set_tmoves", "cw_dmc_counts",
     "cw_device_bytes", "cw_results_state", "cw_state_energies", "cw_opt_ci", "cw_opt_ci_sums", "cw_ci_o",
     "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
-    "cw_walker_status", "cw_stamp", "cw_stamps", "cw_autotune", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o",
+    "cw_walker_status", "cw_stamp", "cw_stamps", "cw_autotune", "cw_batch_create", "cw_batch_vmc_steps",
+    "cw_batch_last_ms", "cw_batch_last_error", "cw_batch_destroy", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

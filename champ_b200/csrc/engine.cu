@@ -72,6 +72,7 @@ struct cw_ctx {
   int nstamp = 0;
   int commit_grid = 1;     // k_commit_tile's grid: the blocks resident at once
   int gemm_bn_move = 64, gemm_bn_all = 64;  // N tiles of the FP64 LCAO GEMMs (cw_autotune)
+  int md_pending = -1;     // electron whose multideterminant commit rides on the next drift kernel
   int big_spin = 0;        // Slater inverse and c~ on global memory (spins too large for shared memory)
   int ecp_rr_global = 0;   // k_ecp's e-n distances on global memory (hb.ecp_rr)
   int *acc_list = nullptr, *acc_count = nullptr;  // accepted walkers of a move (k_accept_list)
@@ -92,6 +93,7 @@ struct cw_ctx {
   // CUDA graph of one VMC sweep (captured on first use)
   cudaGraph_t sweep_graph = nullptr;
   cudaGraphExec_t sweep_exec = nullptr;
+  long sweep_gen = 0;      // captures of the sweep so far (a batch rebuilds on change)
   long sweep_launches = 0;
   int sweep_w = 0;
   int basis_warps = 4;
@@ -591,8 +593,12 @@ int md_before_propose(cw_ctx *c, int iel) {
     stage_end(c);
     LCHK("k_md_phase");
   }
+  // a commit deferred by md_after_commit (the previous electron of this spin)
+  // runs inside the drift kernel, which stages the same aa block
+  const int prev = c->md_pending;
+  c->md_pending = -1;
   stage_begin(c, CW_ST_MDET);
-  k_md_drift_old<<<W, 128, c->smem_md_drift, c->stream>>>(c->h, c->st, c->md, c->mdt, c->g, iel);
+  k_md_drift_old<<<W, 128, c->smem_md_drift, c->stream>>>(c->h, c->st, c->md, c->mdt, c->g, iel, c->mb, prev);
   stage_end(c);
   LCHK("k_md_drift_old");
   return CW_OK;
@@ -605,8 +611,15 @@ int md_after_lcao(cw_ctx *c, int iel) {
   LCHK("k_md_move");
   return CW_OK;
 }
-int md_after_commit(cw_ctx *c, int iel) {
+// defer: the caller's next call is md_before_propose(iel + 1) (a sweep or
+// step loop), which then performs this commit; not at the end of a spin's
+// electrons (the next spin's phase needs this spin's ratios)
+int md_after_commit(cw_ctx *c, int iel, bool defer = false) {
   if (!c->md_on) return CW_OK;
+  if (defer && iel + 1 < c->h.N && iel + 1 != c->h.nup) {
+    c->md_pending = iel;
+    return CW_OK;
+  }
   stage_begin(c, CW_ST_MDET);
   k_md_commit<<<c->W, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, iel);
   stage_end(c);
@@ -1516,6 +1529,7 @@ int hook_check(cw_ctx *c, int iel, const char *what) {
 // old position): what the engine's own sweep does before each proposal
 int hook_md_prepare(cw_ctx *c, int iel) {
   if (!c->md_on || c->hook_md_iel == iel) return CW_OK;
+  c->md_pending = -1;  // the per-electron routines commit at once (cw_commit)
   int rc = md_before_propose(c, iel);
   if (rc) return rc;
   c->hook_md_iel = iel;
@@ -1615,6 +1629,7 @@ int vmc_sweep(cw_ctx *c) {
     stage_end(c);
     LCHK("k_rotqua");
   }
+  c->md_pending = -1;
   for (int i = 0; i < h.N; i++) {
     if (int rc = md_before_propose(c, i)) return rc;
     stage_begin(c, CW_ST_PROPOSE);
@@ -1647,7 +1662,7 @@ int vmc_sweep(cw_ctx *c) {
     launch_commit(c, i, true);
     stage_end(c);
     LCHK("k_commit");
-    if (int rc = md_after_commit(c, i)) return rc;
+    if (int rc = md_after_commit(c, i, true)) return rc;
   }
   int rc = run_hpsi(c, 1);
   if (rc) return rc;
@@ -1662,6 +1677,30 @@ int vmc_sweep(cw_ctx *c) {
 // shapes), so it is captured once into a CUDA graph and replayed: one launch
 // per sweep instead of ~6N+20.  Profiling (per-stage events) runs the launches
 // directly; a new population, optimisation sums or a restore re-capture.
+// the sweep's launches captured into c->sweep_graph (and instantiated) if
+// the population changed or nothing is captured yet
+static int ensure_sweep_graph(cw_ctx *c) {
+  if (c->sweep_exec && c->sweep_w != c->W) drop_sweep_graph(c);
+  if (c->sweep_exec) return CW_OK;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const long l0 = c->launches;
+  int rc = vmc_sweep(c);
+  cudaGraph_t gph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
+  if (rc || e != cudaSuccess) {
+    if (gph) cudaGraphDestroy(gph);
+    if (rc) return rc;
+    return fail(c, CW_ERR_CUDA, "sweep capture failed: %s", cudaGetErrorString(e));
+  }
+  c->sweep_graph = gph;
+  c->sweep_launches = c->launches - l0;
+  c->sweep_w = c->W;
+  c->sweep_gen++;
+  c->launches = l0;
+  CK(cudaGraphInstantiate(&c->sweep_exec, c->sweep_graph, 0));
+  return CW_OK;
+}
+
 int cw_vmc_steps(cw_ctx *c, int nstep) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
   BIND(c);
@@ -1674,24 +1713,7 @@ int cw_vmc_steps(cw_ctx *c, int nstep) {
       if (c->evused > 4096) stage_collect(c);
     }
   } else {
-    if (c->sweep_exec && c->sweep_w != c->W) drop_sweep_graph(c);
-    if (!c->sweep_exec) {
-      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      const long l0 = c->launches;
-      int rc = vmc_sweep(c);
-      cudaGraph_t gph = nullptr;
-      const cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
-      if (rc || e != cudaSuccess) {
-        if (gph) cudaGraphDestroy(gph);
-        if (rc) return rc;
-        return fail(c, CW_ERR_CUDA, "sweep capture failed: %s", cudaGetErrorString(e));
-      }
-      c->sweep_graph = gph;
-      c->sweep_launches = c->launches - l0;
-      c->sweep_w = c->W;
-      c->launches = l0;
-      CK(cudaGraphInstantiate(&c->sweep_exec, c->sweep_graph, 0));
-    }
+    if (int rc = ensure_sweep_graph(c)) return rc;
     for (int s = 0; s < nstep; s++) CK(cudaGraphLaunch(c->sweep_exec, c->stream));
     c->launches += (long)nstep * c->sweep_launches;
   }
@@ -2307,6 +2329,128 @@ extern "C" int cw_orbitals_noalloc(cw_ctx *c, int npts, const double *xyz, doubl
 }
 
 // ===========================================================================
+// Batches of contexts (no CHAMP counterpart): the VMC sweeps of several
+// systems as one CUDA graph whose child nodes are the contexts' own captured
+// sweep graphs, with no edges between them, so one graph launch advances
+// every system by one sweep and the device runs the systems side by side.
+// ===========================================================================
+struct cw_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, join = nullptr;
+  std::vector<cw_ctx *> ctx;
+  std::vector<long> gen;       // the contexts' sweep captures the graph was built from
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  float last_ms = 0;
+  std::string err;
+};
+
+namespace {
+int bfail(cw_batch *b, int code, const char *msg) {
+  if (b) b->err = msg;
+  return code;
+}
+}  // namespace
+
+extern "C" int cw_batch_create(cw_batch **out, cw_ctx **ctxs, int n) {
+  if (!out || !ctxs || n <= 0) return CW_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; i++)
+    if (!ctxs[i] || ctxs[i]->device != ctxs[0]->device) return CW_ERR_ARG;
+  cw_batch *b = new cw_batch();
+  b->device = ctxs[0]->device;
+  b->ctx.assign(ctxs, ctxs + n);
+  b->gen.assign(n, -1);
+  if (cudaSetDevice(b->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
+    delete b;
+    return CW_ERR_CUDA;
+  }
+  *out = b;
+  return CW_OK;
+}
+
+extern "C" void cw_batch_destroy(cw_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (cudaEvent_t e : {b->ev0, b->ev1, b->join})
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+extern "C" const char *cw_batch_last_error(const cw_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+extern "C" float cw_batch_last_ms(const cw_batch *b) { return b ? b->last_ms : 0.0f; }
+
+// nstep sweeps of every context of the batch: each context's sweep graph is
+// (re)captured where needed, the batch graph rebuilt when any of them
+// changed, then launched nstep times on the batch's stream, ordered after
+// each context's queued work and before its next.  A context that reports a
+// failure status names itself in the batch's error (its own cw_last_error
+// has the detail).
+extern "C" int cw_batch_vmc_steps(cw_batch *b, int nstep) {
+  if (!b || nstep < 0) return CW_ERR_ARG;
+  if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "cudaSetDevice failed");
+  bool stale = !b->exec;
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    cw_ctx *c = b->ctx[i];
+    if (c->W == 0) return bfail(b, CW_ERR_STATE, "a context of the batch has no walkers");
+    if (c->prof) return bfail(b, CW_ERR_STATE, "a context of the batch is profiling its launches");
+    if (int rc = ensure_sweep_graph(c)) return bfail(b, rc, "a context's sweep capture failed");
+    if (b->gen[i] != c->sweep_gen) stale = true;
+  }
+  if (stale) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    if (cudaGraphCreate(&b->graph, 0) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "cudaGraphCreate failed");
+    for (size_t i = 0; i < b->ctx.size(); i++) {
+      cudaGraphNode_t node;
+      if (cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, b->ctx[i]->sweep_graph) != cudaSuccess)
+        return bfail(b, CW_ERR_CUDA, "cudaGraphAddChildGraphNode failed");
+      b->gen[i] = b->ctx[i]->sweep_gen;
+    }
+    if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess)
+      return bfail(b, CW_ERR_CUDA, "cudaGraphInstantiate of the batch failed");
+  }
+  // after every context's queued work ...
+  for (cw_ctx *c : b->ctx) {
+    if (cudaEventRecord(b->join, c->stream) != cudaSuccess || cudaStreamWaitEvent(b->stream, b->join, 0) != cudaSuccess)
+      return bfail(b, CW_ERR_CUDA, "ordering the batch after its contexts failed");
+  }
+  cudaEventRecord(b->ev0, b->stream);
+  for (int s = 0; s < nstep; s++)
+    if (cudaGraphLaunch(b->exec, b->stream) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "batch graph launch failed");
+  cudaEventRecord(b->ev1, b->stream);
+  // ... and before each context's next work
+  cudaEventRecord(b->join, b->stream);
+  for (cw_ctx *c : b->ctx)
+    if (cudaStreamWaitEvent(c->stream, b->join, 0) != cudaSuccess)
+      return bfail(b, CW_ERR_CUDA, "ordering the contexts after the batch failed");
+  if (cudaEventSynchronize(b->ev1) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "batch sweeps failed");
+  cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    cw_ctx *c = b->ctx[i];
+    c->passes += nstep;
+    c->launches = (long)nstep * c->sweep_launches;
+    if (c->opt_np > 0) c->sr_w += (double)c->W * nstep;
+    if (int rc = check_status(c)) {
+      b->err = "context " + std::to_string(i) + ": " + c->err;
+      return rc;
+    }
+  }
+  return CW_OK;
+}
+
+// ===========================================================================
 // Diffusion Monte Carlo: one population per context (CHAMP's per-rank dmc
 // arrays).  Walker slots 0..mwalk-1 live in the walker arrays allocated for
 // mwalk; kernels run over the nwalk active ones.
@@ -2529,6 +2673,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
     const DmcScalars sc{d.tau, d.etrial, d.eest, ffi, d.fprod};
     CK(cudaMemsetAsync(b.acc, 0, sizeof(double) * W * DA_NA, c->stream));
     CK(cudaMemcpyAsync(b.eprev, c->st.eold, sizeof(double) * W, cudaMemcpyDeviceToDevice, c->stream));
+    c->md_pending = -1;
     for (int i = 0; i < h.N; i++) {
       if (int rc = md_before_propose(c, i)) return rc;
       stage_begin(c, CW_ST_PROPOSE);
@@ -2561,7 +2706,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       launch_commit(c, i, true);
       stage_end(c);
       LCHK("k_commit");
-      if (int rc = md_after_commit(c, i)) return rc;
+      if (int rc = md_after_commit(c, i, true)) return rc;
     }
     if (d.icasula == -1) {
       CK(cudaMemsetAsync(c->hb.tvpsp, 0, sizeof(double) * (size_t)W * h.N * h.nquad * h.M, c->stream));

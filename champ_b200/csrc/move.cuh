@@ -321,8 +321,10 @@ __global__ void __launch_bounds__(128) k_propose(const __grid_constant__ CSys cs
 // jastrow4e, iflag=0: warp per walker, lanes over the partner electron.
 // Per-centre quantities of the moved electron are staged in shared memory.
 // ---------------------------------------------------------------------------
-// partner electrons per lane in k_jastrow_move (2 shares each coefficient load
-// between two partners but needs ~150 registers; 1 measured faster on B200)
+// partner electrons per lane in k_jastrow_move: 2 shares each coefficient load
+// between two partners but needs ~150 registers; bounded to four blocks per
+// SM it spills and measured 39.3 against 39.9 ms per 8192-walker sweep of the
+// 120-electron molecule (bitwise the same walk), so one is kept
 constexpr int kJmPartners = 1;
 
 template <int NORD>

@@ -368,6 +368,42 @@ class Engine:
         return slmi, det
 
 
+class Batch:
+    """Several engines (one device) advanced together: each cw_batch_vmc_steps
+    call runs nstep sweeps of every engine through one CUDA graph launch per
+    sweep (the engines' own sweep graphs as parallel child nodes)."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        self.lib = self.engines[0].lib
+        arr = (C.c_void_p * len(self.engines))(*[e.h for e in self.engines])
+        h = C.c_void_p()
+        rc = self.lib.cw_batch_create(C.byref(h), arr, len(self.engines))
+        if rc:
+            raise EngineError(f"cw_batch_create failed (status {rc})", rc)
+        self.h = h
+
+    def vmc_steps(self, nstep: int):
+        rc = self.lib.cw_batch_vmc_steps(self.h, int(nstep))
+        if rc:
+            msg = self.lib.cw_batch_last_error(self.h).decode()
+            raise EngineError(f"cw_batch_vmc_steps failed (status {rc}): {msg}", rc)
+
+    def last_ms(self) -> float:
+        return float(self.lib.cw_batch_last_ms(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.cw_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Dmc:
     """One DMC population (one CHAMP rank's walkers) on an ``Engine``."""
 

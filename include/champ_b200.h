@@ -170,6 +170,23 @@ int cw_stamp(cw_ctx *ctx);
  * walkers (cw_set_walkers); choice [2] (nullable) receives the move and
  * all-electron tiles.  The mixed path's tensor-core kernel has one tile. */
 int cw_autotune(cw_ctx *ctx, int reps, int32_t *choice);
+
+/* Batches of contexts (no CHAMP counterpart; the batched configuration of
+ * many systems).  A batch holds contexts of one device; cw_batch_vmc_steps
+ * advances every one of them by nstep metrop6 sweeps through one CUDA graph
+ * whose child nodes are the contexts' own captured sweep graphs (captured
+ * here where needed), with no edges between them: one graph launch per sweep
+ * for all systems, which the device runs side by side.  The batch's work is
+ * ordered after each context's queued work and before its next, so
+ * cw_end_block, cw_results etc. are used per context as after cw_vmc_steps;
+ * each context's results are bitwise those of cw_vmc_steps on it alone.
+ * cw_batch_last_ms: device time of the last call's sweeps. */
+typedef struct cw_batch cw_batch;
+int cw_batch_create(cw_batch **batch, cw_ctx **ctxs, int nctx);
+int cw_batch_vmc_steps(cw_batch *batch, int nstep);
+float cw_batch_last_ms(const cw_batch *batch);
+const char *cw_batch_last_error(const cw_batch *batch);
+void cw_batch_destroy(cw_batch *batch);
 int cw_stamps(cw_ctx *ctx, int64_t *ns, int n);
 
 /* ------------------------------------------------------------------------ */
