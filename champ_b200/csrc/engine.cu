@@ -72,7 +72,6 @@ struct cw_ctx {
   int nstamp = 0;
   int commit_grid = 1;     // k_commit_tile's grid: the blocks resident at once
   int gemm_bn_move = 64, gemm_bn_all = 64;  // N tiles of the FP64 LCAO GEMMs (cw_autotune)
-  int md_pending = -1;     // electron whose multideterminant commit rides on the next drift kernel
   int big_spin = 0;        // Slater inverse and c~ on global memory (spins too large for shared memory)
   int ecp_rr_global = 0;   // k_ecp's e-n distances on global memory (hb.ecp_rr)
   int *acc_list = nullptr, *acc_count = nullptr;  // accepted walkers of a move (k_accept_list)
@@ -593,12 +592,8 @@ int md_before_propose(cw_ctx *c, int iel) {
     stage_end(c);
     LCHK("k_md_phase");
   }
-  // a commit deferred by md_after_commit (the previous electron of this spin)
-  // runs inside the drift kernel, which stages the same aa block
-  const int prev = c->md_pending;
-  c->md_pending = -1;
   stage_begin(c, CW_ST_MDET);
-  k_md_drift_old<<<W, 128, c->smem_md_drift, c->stream>>>(c->h, c->st, c->md, c->mdt, c->g, iel, c->mb, prev);
+  k_md_drift_old<<<W, 128, c->smem_md_drift, c->stream>>>(c->h, c->st, c->md, c->mdt, c->g, iel);
   stage_end(c);
   LCHK("k_md_drift_old");
   return CW_OK;
@@ -611,15 +606,8 @@ int md_after_lcao(cw_ctx *c, int iel) {
   LCHK("k_md_move");
   return CW_OK;
 }
-// defer: the caller's next call is md_before_propose(iel + 1) (a sweep or
-// step loop), which then performs this commit; not at the end of a spin's
-// electrons (the next spin's phase needs this spin's ratios)
-int md_after_commit(cw_ctx *c, int iel, bool defer = false) {
+int md_after_commit(cw_ctx *c, int iel) {
   if (!c->md_on) return CW_OK;
-  if (defer && iel + 1 < c->h.N && iel + 1 != c->h.nup) {
-    c->md_pending = iel;
-    return CW_OK;
-  }
   stage_begin(c, CW_ST_MDET);
   k_md_commit<<<c->W, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, iel);
   stage_end(c);
@@ -1529,7 +1517,6 @@ int hook_check(cw_ctx *c, int iel, const char *what) {
 // old position): what the engine's own sweep does before each proposal
 int hook_md_prepare(cw_ctx *c, int iel) {
   if (!c->md_on || c->hook_md_iel == iel) return CW_OK;
-  c->md_pending = -1;  // the per-electron routines commit at once (cw_commit)
   int rc = md_before_propose(c, iel);
   if (rc) return rc;
   c->hook_md_iel = iel;
@@ -1629,7 +1616,6 @@ int vmc_sweep(cw_ctx *c) {
     stage_end(c);
     LCHK("k_rotqua");
   }
-  c->md_pending = -1;
   for (int i = 0; i < h.N; i++) {
     if (int rc = md_before_propose(c, i)) return rc;
     stage_begin(c, CW_ST_PROPOSE);
@@ -1662,7 +1648,7 @@ int vmc_sweep(cw_ctx *c) {
     launch_commit(c, i, true);
     stage_end(c);
     LCHK("k_commit");
-    if (int rc = md_after_commit(c, i, true)) return rc;
+    if (int rc = md_after_commit(c, i)) return rc;
   }
   int rc = run_hpsi(c, 1);
   if (rc) return rc;
@@ -2673,7 +2659,6 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
     const DmcScalars sc{d.tau, d.etrial, d.eest, ffi, d.fprod};
     CK(cudaMemsetAsync(b.acc, 0, sizeof(double) * W * DA_NA, c->stream));
     CK(cudaMemcpyAsync(b.eprev, c->st.eold, sizeof(double) * W, cudaMemcpyDeviceToDevice, c->stream));
-    c->md_pending = -1;
     for (int i = 0; i < h.N; i++) {
       if (int rc = md_before_propose(c, i)) return rc;
       stage_begin(c, CW_ST_PROPOSE);
@@ -2706,7 +2691,7 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
       launch_commit(c, i, true);
       stage_end(c);
       LCHK("k_commit");
-      if (int rc = md_after_commit(c, i, true)) return rc;
+      if (int rc = md_after_commit(c, i)) return rc;
     }
     if (d.icasula == -1) {
       CK(cudaMemsetAsync(c->hb.tvpsp, 0, sizeof(double) * (size_t)W * h.N * h.nquad * h.M, c->stream));

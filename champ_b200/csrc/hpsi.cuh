@@ -100,6 +100,9 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__
   double *sx = smem;                      // [3][N]
   double *sI = sx + 3 * N + (3 * N & 1);  // [2][M][8] table entries and e-n vectors of the batch's rows
   T *sB = reinterpret_cast<T *>(sI + 2 * M * 8);  // [2][M][4*NB] folded rows (16-byte aligned)
+  // FP32 path: the rows' fields in FP32 [2][M][8], in the half of the folded
+  // rows' space that FP32 coefficients leave free (used only for NORD > 1)
+  float *sIf = reinterpret_cast<float *>(sB + 2 * M * 4 * NB);
   __shared__ double red[4];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
   __syncthreads();
@@ -169,6 +172,8 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__
 #pragma unroll
       for (int f = 0; f < kEnFields; f++) q[f] = tab[f * MN + ic * N + i];
       for (int k = 0; k < 3; k++) q[kEnFields + k] = sx[k * N + i] - cs.cent[3 * ic + k];
+      if (sizeof(T) == 4 && NORD > 1)
+        for (int f = 0; f < 8; f++) sIf[(size_t)t * 8 + f] = (float)q[f];
       if (NORD > 1) een_fold2<NORD, T>(een_coef<T>(cs, cs.iwctype[ic]), T(1 - kap * q[0]), sB + (size_t)t * 4 * NB);
     }
     __syncthreads();
@@ -204,6 +209,7 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__
         const T z = 1 - kT * u, du1 = -kT * dd1, du2 = -kT * dd2, du1r = du1 * irijT;
         const T *Brow = sB + (size_t)row * M * 4 * NB;
         const double *Irow = sI + (size_t)row * M * 8;
+        const float *IrowF = sIf + (size_t)row * M * 8;
         // the partner's table entries of the next centre are loaded one iteration
         // ahead; the mixed path reads them from the FP32 copy
         using TT = typename std::conditional<sizeof(T) == 4, float, double>::type;
@@ -219,7 +225,17 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__
           const double *qi = Irow + ic * 8;
           const double rri = qi[0];
           if (rri == asym && rrj == (TT)asym) continue;
-          const T Ai = (T)qi[1], Bi = (T)qi[2], Gi = (T)qi[3], Si = (T)qi[4];
+          // the row's fields in T (the mixed path reads the FP32 copy made at
+          // the batch's start instead of converting each one here)
+          T Ai, Bi, Gi, Si, vi0, vi1, vi2;
+          if constexpr (sizeof(T) == 4) {
+            const float4 f0 = *reinterpret_cast<const float4 *>(IrowF + ic * 8);
+            const float4 f1 = *reinterpret_cast<const float4 *>(IrowF + ic * 8 + 4);
+            Ai = f0.y; Bi = f0.z; Gi = f0.w; Si = f1.x; vi0 = f1.y; vi1 = f1.z; vi2 = f1.w;
+          } else {
+            Ai = (T)qi[1]; Bi = (T)qi[2]; Gi = (T)qi[3]; Si = (T)qi[4];
+            vi0 = (T)qi[5]; vi1 = (T)qi[6]; vi2 = (T)qi[7];
+          }
           const EenOut<T> e = een_apply2<NORD, T>(Brow + (size_t)ic * 4 * NB, T(1 - (TT)kap * rrj), z);
           const T dS = Si - Sj;
           const T fuu = e.fuu * du1 * du1 + e.fu * du2;
@@ -229,9 +245,9 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__
           fs += e.fc;
           const T vj0 = (T)(xj[0] - cs.cent[3 * ic]), vj1 = (T)(xj[1] - cs.cent[3 * ic + 1]),
                   vj2 = (T)(xj[2] - cs.cent[3 * ic + 2]);
-          gi[0] += fi * (T)qi[5] + fu * rvT[0];
-          gi[1] += fi * (T)qi[6] + fu * rvT[1];
-          gi[2] += fi * (T)qi[7] + fu * rvT[2];
+          gi[0] += fi * vi0 + fu * rvT[0];
+          gi[1] += fi * vi1 + fu * rvT[1];
+          gi[2] += fi * vi2 + fu * rvT[2];
           gj[0] += fj * vj0 - fu * rvT[0];
           gj[1] += fj * vj1 - fu * rvT[1];
           gj[2] += fj * vj2 - fu * rvT[2];

@@ -756,11 +756,7 @@ __global__ void __launch_bounds__(128) k_md_phase(const __grid_constant__ CSys c
 // matrix: vel = detratio * sum_kk d_kk G_kk sum_jr t[ro_jr] (M_kk^-1 c)[jr]
 // with c the column of A^-1 of the electron (the Y contraction regrouped per
 // excitation).  CTA (128) per walker; shared: c (nmax), t (3*O), aa (nmax*O).
-// iel_prev >= 0: first the commit of that electron's move (the same spin,
-// the move before this one), as k_md_commit does, on the aa block staged here
-// (so the block is read once for both)
-__global__ void __launch_bounds__(128, 5) k_md_drift_old(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, GSys g, int iel,
-                                                         MoveBuf mb, int iel_prev) {
+__global__ void __launch_bounds__(128, 5) k_md_drift_old(const __grid_constant__ CSys cs, WState st, MdBuf md, MdTab tab, GSys g, int iel) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, O = cs.Oa, nmax = cs.nmax;
@@ -772,36 +768,11 @@ __global__ void __launch_bounds__(128, 5) k_md_drift_old(const __grid_constant__
   double *bo = A + (size_t)nmax * O;  // 3*nmax
   __shared__ double red[4];
   const double *sl = st.slmi + ((size_t)w * 2 + s) * nmax * nmax + (size_t)n * (iel - ish);
-  double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
+  const double *aa = md.aa + ((size_t)w * 2 + s) * nmax * O;
   for (int q = threadIdx.x; q < n * O; q += blockDim.x) cp_async8(A + q, aa + q);
   for (int j = threadIdx.x; j < n; j += blockDim.x) c[j] = sl[j];
   cp_async8_wait();
   __syncthreads();
-  if (iel_prev >= 0 && mb.ms[w].acc) {
-    // k_md_commit of iel_prev: aa += c (x) w on the virtual columns, ratios,
-    // S, the gradient row of the moved electron
-    const int ivirt = cs.md_ivirt[s];
-    const double *cv = md.cvec + (size_t)w * nmax;
-    const double *wg = md.wvec + (size_t)w * O;
-    for (int i = threadIdx.x >> 5; i < n; i += blockDim.x >> 5) {
-      const double ci = cv[i];
-      for (int v = ivirt + (threadIdx.x & 31); v < O; v += 32) {
-        const double a = A[i * O + v] + ci * wg[v];
-        A[i * O + v] = a;
-        aa[i * O + v] = a;
-      }
-    }
-    double *dd = md.dd + ((size_t)w * 2 + s) * tab.numax;
-    for (int kk = threadIdx.x; kk < cs.md_nuniq[s]; kk += blockDim.x) dd[kk] = md.ddn[(size_t)w * tab.numax + kk];
-    const double *orbn = mb.orbn + (size_t)w * 4 * O;
-    for (int o = threadIdx.x; o < O; o += blockDim.x)
-      for (int k = 0; k < 3; k++) md.dorbA[(((size_t)w * 3 + k) * N + iel_prev) * O + o] = orbn[(1 + k) * O + o];
-    if (threadIdx.x == 0) md.S[w] = md.Sn[w];
-    if (md.Sn_ms)
-      for (int stt = threadIdx.x; stt < cs.nstates; stt += blockDim.x)
-        md.S_ms[(size_t)w * cs.nstates + stt] = md.Sn_ms[(size_t)w * cs.nstates + stt];
-    __syncthreads();
-  }
   md_form_t(cs, s, md.dorbA + (((size_t)w * 3 + 0) * N + iel) * O, md.dorbA + (((size_t)w * 3 + 1) * N + iel) * O,
             md.dorbA + (((size_t)w * 3 + 2) * N + iel) * O, A, g.slot_orb + s * nmax, t, bo);
   __syncthreads();
