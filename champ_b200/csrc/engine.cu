@@ -66,7 +66,7 @@ struct cw_ctx {
   MoveBuf mb{};
   HBuf hb{};
   std::vector<void *> w_allocs;
-  size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
+  size_t smem_jmove = 0, smem_jmove_f32 = 0, smem_jfull = 0, smem_jfull_f32 = 0, smem_sinv = 0, smem_ctil = 0, smem_ecp = 0, smem_basis = 0;
   size_t smem_commit = 0;  // k_commit_tile's dynamic shared memory (0: the untiled k_commit)
   unsigned long long *d_stamps = nullptr;  // device-clock stamps (cw_stamp), kStampCap slots
   int nstamp = 0;
@@ -292,7 +292,7 @@ void launch_jmove(cw_ctx *c, int iel) {
 template <int NORD>
 void launch_jfull(cw_ctx *c) {
   if (c->mixed)
-    k_jastrow_full<NORD, float><<<c->W, 128, c->smem_jfull, c->stream>>>(c->h, c->st, c->hb);
+    k_jastrow_full<NORD, float><<<c->W, 128, c->smem_jfull_f32, c->stream>>>(c->h, c->st, c->hb);
   else
     k_jastrow_full<NORD, double><<<c->W, 128, c->smem_jfull, c->stream>>>(c->h, c->st, c->hb);
 }
@@ -326,7 +326,7 @@ int set_attrs(cw_ctx *c) {
   CK(raise_smem(c, k_jastrow_move<NORD>, (size_t)(c->smem_jmove)));
   CK(raise_smem(c, k_jastrow_move_f32<NORD, kJmF32Partners>, (size_t)(c->smem_jmove_f32)));
   CK(raise_smem(c, k_jastrow_full<NORD, double>, c->smem_jfull));
-  CK(raise_smem(c, k_jastrow_full<NORD, float>, c->smem_jfull));
+  CK(raise_smem(c, k_jastrow_full<NORD, float>, c->smem_jfull_f32));
   if (c->h.nloc > 0) {
     // warps per ECP block and register budget (two builds: one block per SM,
     // or two with at most 64 registers): the most resident warps per SM under
@@ -1243,6 +1243,9 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   {
     const int nord = h.nordc <= 1 ? 1 : h.nordc;
     c->smem_jfull = sizeof(double) * (3 * (size_t)h.N + 1 + 2 * (size_t)h.M * 8 + 2 * (size_t)h.M * 4 * een_nb(nord));
+    // FP32: the folded rows in floats, then the rows' fields in floats
+    c->smem_jfull_f32 = sizeof(double) * (3 * (size_t)h.N + 1 + 2 * (size_t)h.M * 8) +
+                        sizeof(float) * (2 * (size_t)h.M * 4 * een_nb(nord) + 2 * (size_t)h.M * 8);
   }
   // spins whose n x n inverse does not fit in shared memory (about 160
   // electrons and up): the inverse and c~ kernels work on global memory

@@ -90,7 +90,7 @@ constexpr int kEnFields = 5;
 // pairs stay FP64.  Four CTAs per SM in both arithmetics (the FP32 build at
 // five spilled and ran 9% slower).
 template <int NORD, typename T>
-__global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__ CSys cs, WState st, HBuf hb) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jastrow_full(const __grid_constant__ CSys cs, WState st, HBuf hb) {
   const int w = blockIdx.x;
   if (w >= st.W) return;
   const int N = cs.N, M = cs.M, MN = M * N;
@@ -100,8 +100,8 @@ __global__ void __launch_bounds__(128, 4) k_jastrow_full(const __grid_constant__
   double *sx = smem;                      // [3][N]
   double *sI = sx + 3 * N + (3 * N & 1);  // [2][M][8] table entries and e-n vectors of the batch's rows
   T *sB = reinterpret_cast<T *>(sI + 2 * M * 8);  // [2][M][4*NB] folded rows (16-byte aligned)
-  // FP32 path: the rows' fields in FP32 [2][M][8], in the half of the folded
-  // rows' space that FP32 coefficients leave free (used only for NORD > 1)
+  // FP32 path: the rows' fields in FP32 [2][M][8] after the folded rows
+  // (used only for NORD > 1)
   float *sIf = reinterpret_cast<float *>(sB + 2 * M * 4 * NB);
   __shared__ double red[4];
   for (int t = threadIdx.x; t < 3 * N; t += blockDim.x) sx[t] = st.x[(size_t)w * 3 * N + t];
