@@ -406,7 +406,9 @@ def run_serve(args):
 def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode="graph"):
     """Sweeps of every system's own context, all at once: mode "graph" runs
     them as one CUDA graph of the contexts' sweep graphs (cw_batch_vmc_steps,
-    one launch per sweep, timed with the batch's events); mode "threads"
+    one launch per sweep, timed with the batch's events); mode "ragged" as one
+    launch per move stage over every system's walkers (cw_batch_set_ragged,
+    same graph launch and timing); mode "threads"
     issues each context's sweeps from `slots` worker threads on its own stream
     (timed from device-clock stamps; the summed device time of the contexts'
     own sweeps is returned too).  Returns electron-moves/s over the device
@@ -428,15 +430,21 @@ def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode
         engines.append(e)
 
     moves = sum(w * s.nelec for s, w in zip(systems, walkers)) * steps
-    if mode == "graph":
-        # one CUDA graph of all systems' sweep graphs: one launch per sweep
+    extra_launches = 0
+    if mode in ("graph", "ragged"):
+        # one CUDA graph per sweep: the systems' own sweep graphs as child
+        # nodes, or (ragged) one launch per move stage over all systems
         from champ_b200.engine import Batch
-        b = Batch(engines)
+        b = Batch(engines, ragged=(mode == "ragged"))
         b.vmc_steps(warmup)                                      # captures + warm-up
         t0 = time.perf_counter()
         b.vmc_steps(steps)
         wall = time.perf_counter() - t0
         span_s = b.last_ms() * 1e-3
+        if mode == "ragged":
+            info = b.info()
+            extra_launches = steps * (info["ragged_launches"] + info["system_launches"])
+            tiles = {"ragged_lcao_tile": info["lcao_bn"]}
         b.close()
         own_s = None
     else:
@@ -454,7 +462,7 @@ def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode
         st = [e.stamps()[-2:] for e in engines]
         span_s = (max(int(b) for _, b in st) - min(int(a) for a, _ in st)) * 1e-9
         own_s = sum(int(b) - int(a) for a, b in st) * 1e-9
-    launches = sum(e.launches() for e in engines)
+    launches = sum(e.launches() for e in engines) + extra_launches
     for e in engines:
         e.close()
     return moves / span_s, wall, own_s, span_s, launches, tiles
@@ -477,11 +485,14 @@ def run_batched(args):
     need = sum(serve.estimate_bytes(s, int(w), "mixed") for s, w in zip(systems, nwk))
     scale = min(1.0, budget / need)
     walkers = [max(64, int(w * scale)) for w in nwk]
-    res = {}
+    res, rag = {}, {}
     with ClockSampler(local) as clk:
         for prec in ("fp64", "mixed"):
             barrier(pg, local)
             res[prec] = batched_rate(systems, walkers, prec, local, args.steps, max(args.warmup, 1), args.slots)
+            barrier(pg, local)
+            rag[prec] = batched_rate(systems, walkers, prec, local, args.steps, max(args.warmup, 1), args.slots,
+                                     mode="ragged")
             barrier(pg, local)
         barrier(pg, local)
         threads = batched_rate(systems, walkers, args.precision, local, args.steps, max(args.warmup, 1), args.slots,
@@ -509,6 +520,11 @@ def run_batched(args):
         "batched": {p: {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4), "wall_s": round(v[1], 4),
                         "mode": "one CUDA graph of all systems' sweep graphs, one launch per sweep"}
                     for p, v in res.items()},
+        "batched_ragged": {p: {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4),
+                               "wall_s": round(v[1], 4), "launches": v[4], "lcao_tile": v[5],
+                               "mode": "one launch per move stage over every system's walkers "
+                                       "(cw_batch_set_ragged), systems' hpsi on their own streams, one graph"}
+                           for p, v in rag.items()},
         "batched_threads": {"precision": args.precision, "moves_per_s": round(threads[0], 1),
                             "device_span_s": round(threads[3], 4),
                             "sum_of_context_device_s": round(threads[2], 4),

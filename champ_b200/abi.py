@@ -152,6 +152,10 @@ def load_engine(path: str | None = None):
     lib.cw_batch_last_error.restype = C.c_char_p
     lib.cw_batch_destroy.argtypes = [V]
     lib.cw_batch_destroy.restype = None
+    lib.cw_batch_set_ragged.argtypes = [V, C.c_int]
+    lib.cw_batch_set_ragged.restype = C.c_int
+    lib.cw_batch_info.argtypes = [V, C.POINTER(C.c_int64)]
+    lib.cw_batch_info.restype = C.c_int
     lib.cw_stamps.argtypes = [V, C.POINTER(C.c_int64), C.c_int]
     lib.cw_psie.argtypes = [V, C.c_int, _dp, _dp, _dp]
     lib.cw_grad.argtypes = [V, C.c_int, C.c_int, _dp]
@@ -182,7 +186,7 @@ EXPORTED_SYMBOLS = [
     "cw_device_bytes", "cw_results_state", "cw_state_energies", "cw_opt_ci", "cw_opt_ci_sums", "cw_ci_o",
     "cw_opt_setup", "cw_opt_sums", "cw_jas_nraw", "cw_jas_raw", "cw_jas_o",
     "cw_walker_status", "cw_stamp", "cw_stamps", "cw_autotune", "cw_batch_create", "cw_batch_vmc_steps",
-    "cw_batch_last_ms", "cw_batch_last_error", "cw_batch_destroy", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o",
+    "cw_batch_last_ms", "cw_batch_last_error", "cw_batch_destroy", "cw_batch_set_ragged", "cw_batch_info", "cw_psie", "cw_grad", "cw_commit", "cw_update_ymat", "cw_opt_orb", "cw_orb_o",
 ]
 STAGES = ["rotqua", "propose", "jastrow_move", "basis_move", "lcao_move", "accept", "jastrow_full",
           "basis_all", "lcao_all", "scatter", "slater_inv", "ctilde", "ecp", "energy", "commit", "dmc_weights", "splitj", "mdet", "tmove"]

@@ -26,6 +26,7 @@
 #include "optjas.cuh"
 #include "peak.cuh"
 #include "umma.cuh"
+#include "ragged.cuh"
 
 
 using namespace cw;
@@ -2333,6 +2334,13 @@ struct cw_batch {
   cudaGraphExec_t exec = nullptr;
   float last_ms = 0;
   std::string err;
+  // ragged mode: one launch per move stage over every system's walkers
+  bool ragged = false;
+  int rag_bn = 0;               // N tile of the grouped FP64 LCAO (timed at build)
+  long rag_launches = 0;        // ragged launches per sweep
+  long rag_ctx_launches = 0;    // the systems' own hpsi launches per sweep
+  std::vector<void *> rag_allocs;
+  std::vector<cudaEvent_t> rag_fork, rag_done;  // per system: start and end of its hpsi branch
 };
 
 namespace {
@@ -2362,12 +2370,24 @@ extern "C" int cw_batch_create(cw_batch **out, cw_ctx **ctxs, int n) {
   return CW_OK;
 }
 
+namespace {
+void rag_free(cw_batch *b) {
+  for (void *p : b->rag_allocs) cudaFree(p);
+  b->rag_allocs.clear();
+  for (cudaEvent_t e : b->rag_fork) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->rag_done) cudaEventDestroy(e);
+  b->rag_fork.clear();
+  b->rag_done.clear();
+}
+}  // namespace
+
 extern "C" void cw_batch_destroy(cw_batch *b) {
   if (!b) return;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  rag_free(b);
   for (cudaEvent_t e : {b->ev0, b->ev1, b->join})
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -2378,12 +2398,375 @@ extern "C" const char *cw_batch_last_error(const cw_batch *b) { return b ? b->er
 
 extern "C" float cw_batch_last_ms(const cw_batch *b) { return b ? b->last_ms : 0.0f; }
 
+// ---------------------------------------------------------------------------
+// Ragged mode: the moves of every system of the batch in one launch per move
+// stage (ragged.cuh).  The systems are sorted by electron count, so the ones
+// still moving at step k are a prefix of the slot array; after a system's
+// last electron its hpsi (and optimisation sums) run on its own stream,
+// forked from the batch's stream inside the same captured graph, while the
+// larger systems keep moving.
+// ---------------------------------------------------------------------------
+namespace {
+
+int nord_class(const cw_ctx *c) {
+  const int n = c->h.nordc <= 1 ? 1 : c->h.nordc;
+  return n > 7 ? 7 : n;
+}
+
+// why the batch's systems cannot advance as one ragged batch ("" if they can)
+std::string rag_refusal(const cw_batch *b) {
+  if (b->ctx.size() > (size_t)kRagMaxSlots) return "more than " + std::to_string(kRagMaxSlots) + " systems";
+  const cw_ctx *c0 = b->ctx[0];
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    const cw_ctx *c = b->ctx[i];
+    const std::string who = "system " + std::to_string(i) + ": ";
+    if (c->W == 0) return who + "no walkers";
+    if (c->dmc.on) return who + "a DMC population";
+    if (c->md_on) return who + "a multideterminant expansion (one determinant only)";
+    if (c->prof) return who + "profiling its launches";
+    if (!c->smem_commit) return who + "a spin above 128 electrons";
+    if (c->mixed != c0->mixed) return "the systems mix FP64 and mixed precision";
+    if (nord_class(c) != nord_class(c0)) return "the systems' e-e-n orders differ";
+  }
+  return "";
+}
+
+template <class T>
+T *rag_upload(cw_batch *b, const std::vector<T> &v) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, sizeof(T) * std::max<size_t>(1, v.size())) != cudaSuccess) return nullptr;
+  b->rag_allocs.push_back(p);
+  if (!v.empty() && cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return nullptr;
+  return static_cast<T *>(p);
+}
+
+// blocks of `per` walkers for every slot: (slot, block of the slot); off[i] =
+// blocks of the first i slots
+std::vector<int2> rag_map(const std::vector<int> &W, int per, std::vector<int> &off) {
+  std::vector<int2> m;
+  off.assign(W.size() + 1, 0);
+  for (size_t i = 0; i < W.size(); i++) {
+    const int nb = (W[i] + per - 1) / per;
+    for (int k = 0; k < nb; k++) m.push_back(make_int2((int)i, k));
+    off[i + 1] = (int)m.size();
+  }
+  return m;
+}
+
+// the FP64 move LCAO of context c runs on the tensor cores when alone (dgemm's test)
+bool rag_dmma_ok(const cw_ctx *c) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(c->mb.phi) | reinterpret_cast<uintptr_t>(c->g.coefT) |
+                      reinterpret_cast<uintptr_t>(c->mb.orbn);
+  return c->h.Oa > 16 && c->h.K % 2 == 0 && c->h.Oa % 2 == 0 && (a & 15) == 0;
+}
+
+std::vector<RagTile> rag_tiles(const std::vector<cw_ctx *> &sc, bool mixed, int bn, std::vector<int> &off) {
+  std::vector<RagTile> t;
+  off.assign(sc.size() + 1, 0);
+  for (size_t i = 0; i < sc.size(); i++) {
+    const cw_ctx *c = sc[i];
+    const int M = 4 * c->W, N = c->h.Oa;
+    if (mixed) {
+      for (int m0 = 0; m0 < M; m0 += 128) t.push_back(RagTile{(int)i, 2, m0, 0});
+    } else if (rag_dmma_ok(c)) {
+      for (int n0 = 0; n0 < N; n0 += bn)
+        for (int m0 = 0; m0 < M; m0 += kMmaBM) t.push_back(RagTile{(int)i, 0, m0, n0});
+    } else {
+      for (int n0 = 0; n0 < N; n0 += kRagSimtBN)
+        for (int m0 = 0; m0 < M; m0 += kRagSimtBM) t.push_back(RagTile{(int)i, 1, m0, n0});
+    }
+    off[i + 1] = (int)t.size();
+  }
+  return t;
+}
+
+void rag_lcao(cudaStream_t s, bool mixed, int bn, int grid, size_t smem, const RagSlot *sl, const RagTile *t) {
+  if (grid <= 0) return;
+  if (mixed) {
+    k_lcao_tf32x3_rag<<<grid, 128, smem, s>>>(sl, t);
+    return;
+  }
+  switch (bn) {
+    case 32: k_lcao_rag<32><<<grid, 128, smem, s>>>(sl, t); break;
+    case 48: k_lcao_rag<48><<<grid, 128, smem, s>>>(sl, t); break;
+    case 80: k_lcao_rag<80><<<grid, 128, smem, s>>>(sl, t); break;
+    default: k_lcao_rag<64><<<grid, 128, smem, s>>>(sl, t); break;
+  }
+}
+
+template <int NORD>
+cudaError_t rag_jmove_attr(bool mixed, size_t smem) {
+  if (mixed)
+    return cudaFuncSetAttribute(k_jastrow_move_f32_rag<NORD, kJmF32Partners>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaFuncSetAttribute(k_jastrow_move_rag<NORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+template <int NORD>
+void rag_jmove(cudaStream_t s, bool mixed, int grid, size_t smem, const CSys *csa, const RagSlot *sl, const int2 *map,
+               int k) {
+  if (mixed) k_jastrow_move_f32_rag<NORD, kJmF32Partners><<<grid, 128, smem, s>>>(csa, sl, map, k);
+  else k_jastrow_move_rag<NORD><<<grid, 128, smem, s>>>(csa, sl, map, k);
+}
+#define RAG_NORD(nc, fn, ...)              \
+  switch (nc) {                            \
+    case 1: fn<1>(__VA_ARGS__); break;     \
+    case 2: fn<2>(__VA_ARGS__); break;     \
+    case 3: fn<3>(__VA_ARGS__); break;     \
+    case 4: fn<4>(__VA_ARGS__); break;     \
+    case 5: fn<5>(__VA_ARGS__); break;     \
+    case 6: fn<6>(__VA_ARGS__); break;     \
+    default: fn<7>(__VA_ARGS__); break;    \
+  }
+template <int NORD>
+void rag_jmove_attr_v(cudaError_t &e, bool mixed, size_t smem) { e = rag_jmove_attr<NORD>(mixed, smem); }
+
+#define RAG_CK(x, what)                                              \
+  do {                                                               \
+    cudaError_t e_ = (x);                                            \
+    if (e_ != cudaSuccess)                                           \
+      return bfail(b, CW_ERR_CUDA, (std::string(what) + ": " + cudaGetErrorString(e_)).c_str()); \
+  } while (0)
+
+// Device tables, launch shapes, the LCAO tile (timed) and the captured graph
+// of one ragged sweep of every system.  Runs on the batch's stream, which
+// already follows every context's queued work.
+int rag_build(cw_batch *b) {
+  rag_free(b);
+  const int n = (int)b->ctx.size();
+  std::vector<int> order(n);
+  for (int i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->ctx[x]->h.N > b->ctx[y]->h.N; });
+  std::vector<cw_ctx *> sc(n);
+  std::vector<int> W(n), nel(n);
+  for (int i = 0; i < n; i++) {
+    sc[i] = b->ctx[order[i]];
+    W[i] = sc[i]->W;
+    nel[i] = sc[i]->h.N;
+  }
+  const bool mixed = sc[0]->mixed;
+  const int ncls = nord_class(sc[0]);
+  // constant blocks, tensor maps, slots
+  std::vector<CSys> hcs(n);
+  std::vector<CUtensorMap> htm(mixed ? 4 * n : 0);
+  for (int i = 0; i < n; i++) {
+    hcs[i] = sc[i]->h;
+    if (mixed) {
+      htm[4 * i + 0] = sc[i]->tm_mv_hi;
+      htm[4 * i + 1] = sc[i]->tm_mv_lo;
+      htm[4 * i + 2] = sc[i]->tm_b_hi;
+      htm[4 * i + 3] = sc[i]->tm_b_lo;
+    }
+  }
+  const CSys *d_cs = rag_upload(b, hcs);
+  const CUtensorMap *d_tm = mixed ? rag_upload(b, htm) : nullptr;
+  if (!d_cs || (mixed && !d_tm)) return bfail(b, CW_ERR_CUDA, "ragged batch: device tables");
+  std::vector<RagSlot> hs(n);
+  for (int i = 0; i < n; i++) {
+    cw_ctx *c = sc[i];
+    RagSlot &r = hs[i];
+    r.st = c->st;
+    r.mb = c->mb;
+    r.g = c->g;
+    r.acc_list = c->acc_list;
+    r.acc_count = c->acc_count;
+    r.W = c->W;
+    r.K = c->h.K;
+    r.Oa = c->h.Oa;
+    r.tm = mixed ? d_tm + 4 * i : nullptr;
+    r.np = c->np;
+    r.stages = c->umma_st;
+    r.err = c->d_err;
+  }
+  const RagSlot *d_slots = rag_upload(b, hs);
+  // block maps
+  int bw = 4;
+  int maxM = 0;
+  size_t smem_jm = 0, smem_commit = 0, smem_umma = 0;
+  for (cw_ctx *c : sc) {
+    bw = std::min(bw, c->basis_warps);
+    maxM = std::max(maxM, c->h.M);
+    smem_jm = std::max(smem_jm, mixed ? c->smem_jmove_f32 : c->smem_jmove);
+    smem_commit = std::max(smem_commit, c->smem_commit);
+    smem_umma = std::max(smem_umma, c->smem_umma);
+  }
+  const size_t smem_basis = (size_t)bw * maxM * kCenRec * sizeof(double);
+  std::vector<int> off16, off4, offbw, offrot;
+  const int2 *d_g16 = rag_upload(b, rag_map(W, 128 / kMoveGroup, off16));
+  const int2 *d_g4 = rag_upload(b, rag_map(W, 4, off4));
+  const int2 *d_gbw = rag_upload(b, rag_map(W, bw, offbw));
+  std::vector<int> Wrot(n);
+  for (int i = 0; i < n; i++) Wrot[i] = sc[i]->h.nloc > 0 ? W[i] : 0;
+  const int2 *d_rot = rag_upload(b, rag_map(Wrot, 128, offrot));
+  if (!d_slots || !d_g16 || !d_g4 || !d_gbw || !d_rot) return bfail(b, CW_ERR_CUDA, "ragged batch: block maps");
+  // launch attributes
+  cudaError_t ea = cudaSuccess;
+  RAG_NORD(ncls, rag_jmove_attr_v, ea, mixed, smem_jm);
+  RAG_CK(ea, "ragged move Jastrow attributes");
+  RAG_CK(cudaFuncSetAttribute(k_basis_move_rag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_basis),
+         "ragged basis attributes");
+  RAG_CK(cudaFuncSetAttribute(k_commit_rag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_commit),
+         "ragged commit attributes");
+  int nsm = 0, per = 0;
+  RAG_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device), "device attributes");
+  RAG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_commit_rag, 128, smem_commit), "commit occupancy");
+  const int commit_grid = std::max(1, nsm * std::max(1, per));
+  // LCAO tiles: the N tile of the tensor-core tiles is timed over the whole
+  // batch (every output sums its K slices in the same order whatever the tile)
+  std::vector<int> offt;
+  const RagTile *d_tiles = nullptr;
+  size_t smem_lcao = 0;
+  if (mixed) {
+    d_tiles = rag_upload(b, rag_tiles(sc, true, 0, offt));
+    smem_lcao = smem_umma;
+    RAG_CK(cudaFuncSetAttribute(k_lcao_tf32x3_rag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_lcao),
+           "ragged tensor-core LCAO attributes");
+    b->rag_bn = 0;
+  } else {
+    RAG_CK(cudaFuncSetAttribute(k_lcao_rag<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mma_smem(32)), "lcao");
+    RAG_CK(cudaFuncSetAttribute(k_lcao_rag<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mma_smem(48)), "lcao");
+    RAG_CK(cudaFuncSetAttribute(k_lcao_rag<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mma_smem(64)), "lcao");
+    RAG_CK(cudaFuncSetAttribute(k_lcao_rag<80>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mma_smem(80)), "lcao");
+    float best = 0;
+    for (int bn : kMmaTiles) {
+      std::vector<int> o;
+      const RagTile *dt = rag_upload(b, rag_tiles(sc, false, bn, o));
+      if (!dt) return bfail(b, CW_ERR_CUDA, "ragged batch: LCAO tiles");
+      const int grid = o[n];
+      rag_lcao(b->stream, false, bn, grid, mma_smem(bn), d_slots, dt);  // warm-up
+      RAG_CK(cudaEventRecord(b->ev0, b->stream), "tile timing");
+      for (int r = 0; r < 3; r++) rag_lcao(b->stream, false, bn, grid, mma_smem(bn), d_slots, dt);
+      RAG_CK(cudaEventRecord(b->ev1, b->stream), "tile timing");
+      RAG_CK(cudaEventSynchronize(b->ev1), "tile timing");
+      RAG_CK(cudaGetLastError(), "ragged LCAO");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+      if (!d_tiles || ms < best) {
+        best = ms;
+        d_tiles = dt;
+        offt = o;
+        b->rag_bn = bn;
+      }
+    }
+    smem_lcao = mma_smem(b->rag_bn);
+  }
+  if (!d_tiles) return bfail(b, CW_ERR_CUDA, "ragged batch: LCAO tiles");
+  // events of the systems' hpsi branches
+  b->rag_fork.assign(n, nullptr);
+  b->rag_done.assign(n, nullptr);
+  for (int i = 0; i < n; i++) {
+    RAG_CK(cudaEventCreateWithFlags(&b->rag_fork[i], cudaEventDisableTiming), "events");
+    RAG_CK(cudaEventCreateWithFlags(&b->rag_done[i], cudaEventDisableTiming), "events");
+  }
+  // capture one sweep
+  cudaStream_t s = b->stream;
+  RAG_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "ragged capture");
+  long nl = 0, nc = 0;
+  int rc = CW_OK;
+  std::string why;
+  int forked = 0;
+  if (offrot[n] > 0) {
+    k_rotqua_rag<<<offrot[n], 128, 0, s>>>(d_cs, d_slots, d_rot);
+    nl++;
+  }
+  int A = n;
+  for (int k = 0; k < nel[0] && rc == CW_OK; k++) {
+    while (A > 0 && nel[A - 1] <= k) A--;
+    k_propose_rag<<<off16[A], 128, 0, s>>>(d_cs, d_slots, d_g16, k);
+    RAG_NORD(ncls, rag_jmove, s, mixed, off4[A], smem_jm, d_cs, d_slots, d_g4, k);
+    k_basis_move_rag<<<offbw[A], 32 * bw, smem_basis, s>>>(d_cs, d_slots, d_gbw);
+    rag_lcao(s, mixed, b->rag_bn, offt[A], smem_lcao, d_slots, d_tiles);
+    k_decide_rag<<<off16[A], 128, 0, s>>>(d_cs, d_slots, d_g16, k);
+    k_commit_rag<<<commit_grid, 128, smem_commit, s>>>(d_cs, d_slots, A, k);
+    nl += 6;
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+      rc = CW_ERR_CUDA;
+      why = std::string("ragged launch: ") + cudaGetErrorString(le);
+      break;
+    }
+    // the systems whose last electron just moved: hpsi on their own streams
+    for (int i = A - 1; i >= 0 && nel[i] == k + 1; i--) {
+      cw_ctx *c = sc[i];
+      if (cudaEventRecord(b->rag_fork[i], s) != cudaSuccess ||
+          cudaStreamWaitEvent(c->stream, b->rag_fork[i], 0) != cudaSuccess) {
+        rc = CW_ERR_CUDA;
+        why = "ragged capture: fork";
+        break;
+      }
+      forked++;
+      const long l0 = c->launches;
+      rc = run_hpsi(c, 1);
+      if (rc == CW_OK && c->opt_np > 0) rc = opt_accum(c);
+      nc += c->launches - l0;
+      c->launches = l0;
+      cudaEventRecord(b->rag_done[i], c->stream);
+      cudaStreamWaitEvent(s, b->rag_done[i], 0);
+      if (rc) {
+        why = "system " + std::to_string(order[i]) + ": " + c->err;
+        break;
+      }
+    }
+  }
+  cudaGraph_t gph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(s, &gph);
+  if (rc != CW_OK || ee != cudaSuccess) {
+    if (gph) cudaGraphDestroy(gph);
+    cudaGetLastError();
+    if (rc == CW_OK) {
+      rc = CW_ERR_CUDA;
+      why = std::string("ragged capture: ") + cudaGetErrorString(ee);
+    }
+    return bfail(b, rc, why.c_str());
+  }
+  if (forked != n) {
+    cudaGraphDestroy(gph);
+    return bfail(b, CW_ERR_STATE, "ragged capture: a system's hpsi was not scheduled");
+  }
+  b->graph = gph;
+  b->rag_launches = nl;
+  b->rag_ctx_launches = nc;
+  RAG_CK(cudaGraphInstantiate(&b->exec, b->graph, 0), "ragged graph instantiate");
+  return CW_OK;
+}
+
+}  // namespace
+
+// Ragged mode on or off: refused (with the reason) when a system cannot join
+extern "C" int cw_batch_set_ragged(cw_batch *b, int on) {
+  if (!b) return CW_ERR_ARG;
+  if (on) {
+    const std::string why = rag_refusal(b);
+    if (!why.empty()) return bfail(b, CW_ERR_UNSUPPORTED, ("ragged batch: " + why).c_str());
+  }
+  if (b->ragged != (on != 0)) {
+    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "cudaSetDevice failed");
+    cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->ragged = on != 0;
+  }
+  return CW_OK;
+}
+
+// [ragged, LCAO N tile, ragged launches per sweep, the systems' own hpsi launches per sweep]
+extern "C" int cw_batch_info(const cw_batch *b, int64_t *info) {
+  if (!b || !info) return CW_ERR_ARG;
+  info[0] = b->ragged ? 1 : 0;
+  info[1] = b->rag_bn;
+  info[2] = b->rag_launches;
+  info[3] = b->rag_ctx_launches;
+  return CW_OK;
+}
+
 // nstep sweeps of every context of the batch: each context's sweep graph is
 // (re)captured where needed, the batch graph rebuilt when any of them
 // changed, then launched nstep times on the batch's stream, ordered after
 // each context's queued work and before its next.  A context that reports a
 // failure status names itself in the batch's error (its own cw_last_error
-// has the detail).
+// has the detail).  In ragged mode the batch graph is the ragged sweep.
 extern "C" int cw_batch_vmc_steps(cw_batch *b, int nstep) {
   if (!b || nstep < 0) return CW_ERR_ARG;
   if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "cudaSetDevice failed");
@@ -2395,25 +2778,33 @@ extern "C" int cw_batch_vmc_steps(cw_batch *b, int nstep) {
     if (int rc = ensure_sweep_graph(c)) return bfail(b, rc, "a context's sweep capture failed");
     if (b->gen[i] != c->sweep_gen) stale = true;
   }
-  if (stale) {
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
-    if (cudaGraphCreate(&b->graph, 0) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "cudaGraphCreate failed");
-    for (size_t i = 0; i < b->ctx.size(); i++) {
-      cudaGraphNode_t node;
-      if (cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, b->ctx[i]->sweep_graph) != cudaSuccess)
-        return bfail(b, CW_ERR_CUDA, "cudaGraphAddChildGraphNode failed");
-      b->gen[i] = b->ctx[i]->sweep_gen;
-    }
-    if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess)
-      return bfail(b, CW_ERR_CUDA, "cudaGraphInstantiate of the batch failed");
+  if (b->ragged) {
+    const std::string why = rag_refusal(b);
+    if (!why.empty()) return bfail(b, CW_ERR_UNSUPPORTED, ("ragged batch: " + why).c_str());
   }
   // after every context's queued work ...
   for (cw_ctx *c : b->ctx) {
     if (cudaEventRecord(b->join, c->stream) != cudaSuccess || cudaStreamWaitEvent(b->stream, b->join, 0) != cudaSuccess)
       return bfail(b, CW_ERR_CUDA, "ordering the batch after its contexts failed");
+  }
+  if (stale) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    if (b->ragged) {
+      if (int rc = rag_build(b)) return rc;
+    } else {
+      if (cudaGraphCreate(&b->graph, 0) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "cudaGraphCreate failed");
+      for (size_t i = 0; i < b->ctx.size(); i++) {
+        cudaGraphNode_t node;
+        if (cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, b->ctx[i]->sweep_graph) != cudaSuccess)
+          return bfail(b, CW_ERR_CUDA, "cudaGraphAddChildGraphNode failed");
+      }
+      if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess)
+        return bfail(b, CW_ERR_CUDA, "cudaGraphInstantiate of the batch failed");
+    }
+    for (size_t i = 0; i < b->ctx.size(); i++) b->gen[i] = b->ctx[i]->sweep_gen;
   }
   cudaEventRecord(b->ev0, b->stream);
   for (int s = 0; s < nstep; s++)
@@ -2429,7 +2820,7 @@ extern "C" int cw_batch_vmc_steps(cw_batch *b, int nstep) {
   for (size_t i = 0; i < b->ctx.size(); i++) {
     cw_ctx *c = b->ctx[i];
     c->passes += nstep;
-    c->launches = (long)nstep * c->sweep_launches;
+    c->launches = b->ragged ? 0 : (long)nstep * c->sweep_launches;
     if (c->opt_np > 0) c->sr_w += (double)c->W * nstep;
     if (int rc = check_status(c)) {
       b->err = "context " + std::to_string(i) + ": " + c->err;

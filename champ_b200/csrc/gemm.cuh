@@ -14,15 +14,16 @@
 
 namespace cw {
 
+// One BM x BN output tile at (m0, n0); As/Bs: the two-stage shared slices.
+// Every output element sums its K terms in order, one FMA each, whatever the
+// tile shape.
 template <int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
-k_dgemm(int M, int N, int K, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C) {
+__device__ __forceinline__ void dgemm_simt_tile(int M, int N, int K, const double *__restrict__ A,
+                                                const double *__restrict__ B, double *__restrict__ C, int m0, int n0,
+                                                double (*As)[BK][BM + 2], double (*Bs)[BK][BN]) {
   constexpr int NT = (BM / TM) * (BN / TN);
-  __shared__ __align__(16) double As[2][BK][BM + 2];
-  __shared__ __align__(16) double Bs[2][BK][BN];
   const int tid = threadIdx.x;
   const int tx = tid % (BN / TN), ty = tid / (BN / TN);
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   double acc[TM][TN];
 #pragma unroll
   for (int i = 0; i < TM; i++)
@@ -119,6 +120,13 @@ k_dgemm(int M, int N, int K, const double *__restrict__ A, const double *__restr
     }
   }
 }
+template <int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+k_dgemm(int M, int N, int K, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C) {
+  __shared__ __align__(16) double As[2][BK][BM + 2];
+  __shared__ __align__(16) double Bs[2][BK][BN];
+  dgemm_simt_tile<BM, BN, BK, TM, TN>(M, N, K, A, B, C, blockIdx.x * BM, blockIdx.y * BN, As, Bs);
+}
 
 // ---------------------------------------------------------------------------
 // FP64 tensor-core variant (mma.sync m16n8k4 .f64; tcgen05 has no FP64 kind):
@@ -150,16 +158,16 @@ __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], const double (&a)[2]
                : "d"(a[0]), "d"(a[1]), "d"(b));
 }
 
+// One 128 x BN output tile at (m0, n0); gsm: mma_smem(BN) bytes of shared memory
 template <int BN>
-__global__ void __launch_bounds__(128, 2)
-k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C) {
+__device__ __forceinline__ void dgemm_mma_tile(int M, int N, int K, const double *__restrict__ A,
+                                               const double *__restrict__ B, double *__restrict__ C, int m0, int n0,
+                                               double *gsm) {
   constexpr int BM = kMmaBM, BK = kMmaBK, SA = kMmaSA, SB = BN + 4, ST = kMmaStages, NI = BN / 8;
-  extern __shared__ __align__(16) double gsm[];
   double *As = gsm;                          // [ST][BM][SA]
   double *Bs = gsm + (size_t)ST * BM * SA;   // [ST][BK][SB]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int nk = (K + BK - 1) / BK;
   auto load_stage = [&](int kt, int s) {
     const int k0 = kt * BK;
@@ -228,6 +236,12 @@ k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__r
       }
     }
   }
+}
+template <int BN>
+__global__ void __launch_bounds__(128, 2)
+k_dgemm_mma(int M, int N, int K, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C) {
+  extern __shared__ __align__(16) double gsm[];
+  dgemm_mma_tile<BN>(M, N, K, A, B, C, blockIdx.x * kMmaBM, blockIdx.y * BN, gsm);
 }
 
 // N tiles of the tensor-core GEMM the autotuner chooses from

@@ -923,8 +923,8 @@ __host__ __device__ inline void rotqua_frame(DRng &rng, double f[9]) {
   f[6] = yy1 * u2 - zz1 * u1; f[7] = yy2 * u2 - zz2 * u1; f[8] = yy3 * u2 - zz3 * u1;
 }
 
-__global__ void k_rotqua(const __grid_constant__ CSys cs, WState st) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void rotqua_body(const CSys &cs, const WState &st, const int bid) {
+  const int w = bid * blockDim.x + threadIdx.x;
   if (w >= st.W) return;
   DRng rng;
   rng.load(st.rng + 4 * (size_t)w);
@@ -939,6 +939,7 @@ __global__ void k_rotqua(const __grid_constant__ CSys cs, WState st) {
   }
   rng.store(st.rng + 4 * (size_t)w);
 }
+__global__ void k_rotqua(const __grid_constant__ CSys cs, WState st) { rotqua_body(cs, st, blockIdx.x); }
 
 // zerest's nearest-nucleus tables: thread per (walker, electron)
 __global__ void k_nearest(const __grid_constant__ CSys cs, WState st) {

@@ -146,15 +146,19 @@ __device__ __forceinline__ void spin_of(const CSys &cs, int iel, int &iab, int &
 // chain that the group's lanes evaluate identically; the radial rejection
 // loop is cooperative within the group.  The group's lane 0 stores.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_propose(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel,
-                                                 int *acc_count) {
+// The kernels of a move are written as bodies over a block index `bid`, so
+// the same code runs one system per launch (bid = blockIdx.x) and, in
+// ragged.cuh, many systems per launch (bid = the block's index within its
+// system's share of the launch).
+__device__ __forceinline__ void propose_body(const CSys &cs, const WState &st, const MoveBuf &mb, int iel,
+                                             int *acc_count, const int bid) {
   // Every lane runs to the end (the radial sampling is cooperative across the
   // warp); groups past the population mirror the last walker and store nothing.
   // acc_count (optional): the accepted-walker count k_decide appends to,
   // emptied here (the previous move's commit has finished reading it).
-  if (acc_count && blockIdx.x == 0 && threadIdx.x == 0) *acc_count = 0;
+  if (acc_count && bid == 0 && threadIdx.x == 0) *acc_count = 0;
   const int gl = threadIdx.x & (kMoveGroup - 1);
-  const int wt = (blockIdx.x * blockDim.x + threadIdx.x) / kMoveGroup;
+  const int wt = (bid * blockDim.x + threadIdx.x) / kMoveGroup;
   const bool live = wt < st.W;
   const int w = live ? wt : st.W - 1;
   const int lane = live ? gl : 1;  // lane 0 of a live group stores
@@ -316,6 +320,10 @@ __global__ void __launch_bounds__(128) k_propose(const __grid_constant__ CSys cs
   mb.ms[w] = m;
   rng.store(st.rng + 4 * (size_t)w);
 }
+__global__ void __launch_bounds__(128) k_propose(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel,
+                                                 int *acc_count) {
+  propose_body(cs, st, mb, iel, acc_count, blockIdx.x);
+}
 
 // ---------------------------------------------------------------------------
 // jastrow4e, iflag=0: warp per walker, lanes over the partner electron.
@@ -328,13 +336,14 @@ __global__ void __launch_bounds__(128) k_propose(const __grid_constant__ CSys cs
 constexpr int kJmPartners = 1;
 
 template <int NORD>
-__global__ void __launch_bounds__(128, 5) k_jastrow_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
+__device__ __forceinline__ void jastrow_move_body(const CSys &cs, const WState &st, const MoveBuf &mb, int iel,
+                                                  const int bid) {
   extern __shared__ __align__(16) double smem[];
   constexpr int NB = een_nb(NORD);        // folded coefficients per centre
   constexpr int PER = 8 + 2 * NB;         // shared doubles per centre (one pad keeps B 16-byte aligned)
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int w = (bid * blockDim.x + threadIdx.x) >> 5;
   const int M = cs.M, N = cs.N;
   double *sh = smem + (size_t)wib * M * PER;
   // per centre ic: rvec(3), r, scaled r, dd1, -kappa dd1 / r, then B[NB], dB[NB]
@@ -519,6 +528,10 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(const __grid_constant__
     mb.vjn[3 * w + 2] = fjo[2 * N + iel] + dv2;
   }
 }
+template <int NORD>
+__global__ void __launch_bounds__(128, 5) k_jastrow_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
+  jastrow_move_body<NORD>(cs, st, mb, iel, blockIdx.x);
+}
 
 // ---------------------------------------------------------------------------
 // Mixed-precision jastrow4e: the same warp-per-walker kernel with the pair
@@ -533,13 +546,14 @@ __global__ void __launch_bounds__(128, 5) k_jastrow_move(const __grid_constant__
 constexpr int kJmF32Partners = 4;
 
 template <int NORD, int P>
-__global__ void __launch_bounds__(128, P == 1 ? 8 : (P == 2 ? 4 : 3)) k_jastrow_move_f32(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
+__device__ __forceinline__ void jastrow_move_f32_body(const CSys &cs, const WState &st, const MoveBuf &mb, int iel,
+                                                      const int bid) {
   extern __shared__ __align__(16) float smemf[];
   constexpr int NB = een_nbp(NORD);        // padded (B, dB) pairs per centre
   constexpr int PER = 8 + 2 * NB;         // shared floats per centre (B 16-byte aligned)
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int w = (bid * blockDim.x + threadIdx.x) >> 5;
   const int M = cs.M, N = cs.N;
   float *sh = smemf + (size_t)wib * M * PER;
   float *sh_rv = sh, *sh_r = sh + 3 * M, *sh_s = sh + 4 * M, *sh_d = sh + 5 * M, *sh_g = sh + 6 * M, *sh_B = sh + 8 * M;
@@ -720,15 +734,20 @@ __global__ void __launch_bounds__(128, P == 1 ? 8 : (P == 2 ? 4 : 3)) k_jastrow_
     mb.vjn[3 * w + 2] = fjo[2 * N + iel] + dv2;
   }
 }
+template <int NORD, int P>
+__global__ void __launch_bounds__(128, P == 1 ? 8 : (P == 2 ? 4 : 3)) k_jastrow_move_f32(const __grid_constant__ CSys cs, WState st, MoveBuf mb, int iel) {
+  jastrow_move_f32_body<NORD, P>(cs, st, mb, iel, blockIdx.x);
+}
 
 // ---------------------------------------------------------------------------
 // Basis functions of the moved electron (basis_fns ider=1): warp per walker,
 // per-centre prepass then lanes over AOs.
 // ---------------------------------------------------------------------------
-__global__ void k_basis_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g) {
+__device__ __forceinline__ void basis_move_body(const CSys &cs, const WState &st, const MoveBuf &mb, const GSys &g,
+                                                const int bid) {
   extern __shared__ __align__(16) double smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int w = (bid * blockDim.x + threadIdx.x) >> 5;
   if (w >= st.W) return;
   const int K = cs.K;
   const MoveScratch &mv = mb.ms[w];
@@ -765,6 +784,9 @@ __global__ void k_basis_move(const __grid_constant__ CSys cs, WState st, MoveBuf
   for (int m = lane; m < K; m += 32)
     warp_basis_ao<1>(cs, g, rec, m, [&](int a, int d, double v) { phi[(size_t)d * K + a] = v; });
 }
+__global__ void k_basis_move(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g) {
+  basis_move_body(cs, st, mb, g, blockIdx.x);
+}
 
 // ---------------------------------------------------------------------------
 // Accept / reject: thread per walker.  Ratio and drift at the new point
@@ -773,13 +795,13 @@ __global__ void k_basis_move(const __grid_constant__ CSys cs, WState st, MoveBuf
 // Scalar state of accepted moves is committed here; k_commit applies the
 // matrix and table updates.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_decide(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, int iel,
-                                                int *acc_list, int *acc_count) {
+__device__ __forceinline__ void decide_body(const CSys &cs, const WState &st, const MoveBuf &mb, const GSys &g,
+                                            int iel, int *acc_list, int *acc_count, const int bid) {
   // kMoveGroup lanes per walker: the ratio and the drift at the new point are
   // dot products over the group, the rest is evaluated identically by the
   // group's lanes, its lane 0 stores
   const int lane = threadIdx.x & (kMoveGroup - 1);
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) / kMoveGroup;
+  const int w = (bid * blockDim.x + threadIdx.x) / kMoveGroup;
   if (w >= st.W) return;  // the whole group (one walker)
   const int N = cs.N, nmax = cs.nmax, Oa = cs.Oa;
   int iab, nel, ish;
@@ -893,6 +915,10 @@ __global__ void __launch_bounds__(128) k_decide(const __grid_constant__ CSys cs,
       st.x[((size_t)w * 3 + k) * N + iel] = m.xnew[k];
     }
   }
+}
+__global__ void __launch_bounds__(128) k_decide(const __grid_constant__ CSys cs, WState st, MoveBuf mb, GSys g, int iel,
+                                                int *acc_list, int *acc_count) {
+  decide_body(cs, st, mb, g, iel, acc_list, acc_count, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -128,10 +128,13 @@ __host__ inline size_t umma_smem_bytes(int np) {
   return 1024 + (size_t)umma_stages(np) * umma_stage_bytes(np) + 256;
 }
 
-__global__ void __launch_bounds__(128, 2)
-    k_lcao_tf32x3(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
-                  const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo, int M, int K,
-                  int np, int nc, int stages, double *__restrict__ C, int ldc, int *err) {
+// One 128-row tile at row m0.  The tensor maps are kernel parameters (one
+// system per launch) or 64-byte-aligned objects in global memory written
+// before the launch (several systems per launch).
+__device__ __forceinline__ void lcao_tf32x3_tile(const CUtensorMap *ta_hi, const CUtensorMap *ta_lo,
+                                                 const CUtensorMap *tb_hi, const CUtensorMap *tb_lo, int M, int K,
+                                                 int np, int nc, int stages, double *__restrict__ C, int ldc,
+                                                 int *err, const int m0) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -145,7 +148,6 @@ __global__ void __launch_bounds__(128, 2)
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nk = (K + 31) / 32;
-  const int m0 = blockIdx.x * 128;
   const uint32_t ncols = np <= 32 ? 32u : np <= 64 ? 64u : np <= 128 ? 128u : 256u;
 
   if (threadIdx.x == 0) {
@@ -182,10 +184,10 @@ __global__ void __launch_bounds__(128, 2)
       if (*s_abort) break;
       uint8_t *st = sb + (size_t)s * stage_bytes;
       mbar_expect_tx(&full[s], stage_bytes);
-      tma_load_2d(st, &ta_hi, &full[s], kb * 32, m0);
-      tma_load_2d(st + a_bytes, &ta_lo, &full[s], kb * 32, m0);
-      tma_load_2d(st + 2 * a_bytes, &tb_hi, &full[s], kb * 32, 0);
-      tma_load_2d(st + 2 * a_bytes + b_bytes, &tb_lo, &full[s], kb * 32, 0);
+      tma_load_2d(st, ta_hi, &full[s], kb * 32, m0);
+      tma_load_2d(st + a_bytes, ta_lo, &full[s], kb * 32, m0);
+      tma_load_2d(st + 2 * a_bytes, tb_hi, &full[s], kb * 32, 0);
+      tma_load_2d(st + 2 * a_bytes + b_bytes, tb_lo, &full[s], kb * 32, 0);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
@@ -239,6 +241,12 @@ __global__ void __launch_bounds__(128, 2)
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
   }
+}
+__global__ void __launch_bounds__(128, 2)
+    k_lcao_tf32x3(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
+                  const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo, int M, int K,
+                  int np, int nc, int stages, double *__restrict__ C, int ldc, int *err) {
+  lcao_tf32x3_tile(&ta_hi, &ta_lo, &tb_hi, &tb_lo, M, K, np, nc, stages, C, ldc, err, blockIdx.x * 128);
 }
 
 }  // namespace cw

@@ -371,9 +371,11 @@ class Engine:
 class Batch:
     """Several engines (one device) advanced together: each cw_batch_vmc_steps
     call runs nstep sweeps of every engine through one CUDA graph launch per
-    sweep (the engines' own sweep graphs as parallel child nodes)."""
+    sweep (the engines' own sweep graphs as parallel child nodes), or, with
+    ``ragged=True``, through one launch per move stage over every engine's
+    walkers."""
 
-    def __init__(self, engines):
+    def __init__(self, engines, ragged: bool = False):
         self.engines = list(engines)
         self.lib = self.engines[0].lib
         arr = (C.c_void_p * len(self.engines))(*[e.h for e in self.engines])
@@ -382,6 +384,22 @@ class Batch:
         if rc:
             raise EngineError(f"cw_batch_create failed (status {rc})", rc)
         self.h = h
+        if ragged:
+            self.set_ragged(True)
+
+    def set_ragged(self, on: bool):
+        rc = self.lib.cw_batch_set_ragged(self.h, 1 if on else 0)
+        if rc:
+            msg = self.lib.cw_batch_last_error(self.h).decode()
+            raise EngineError(f"cw_batch_set_ragged failed (status {rc}): {msg}", rc)
+
+    def info(self) -> dict:
+        v = (C.c_int64 * 4)()
+        rc = self.lib.cw_batch_info(self.h, v)
+        if rc:
+            raise EngineError(f"cw_batch_info failed (status {rc})", rc)
+        return {"ragged": bool(v[0]), "lcao_bn": int(v[1]), "ragged_launches": int(v[2]),
+                "system_launches": int(v[3])}
 
     def vmc_steps(self, nstep: int):
         rc = self.lib.cw_batch_vmc_steps(self.h, int(nstep))
