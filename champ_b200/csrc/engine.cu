@@ -57,6 +57,10 @@ struct cw_ctx {
   int device = 0, precision = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // second stream of a captured sweep: the moved electron's basis and LCAO
+  // run beside its move Jastrow (both need only the proposal)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   CSys h;                 // host copy of the constant block
   GSys g{};               // device tables
@@ -566,16 +570,17 @@ __global__ void k_split_rows(const double *src, int rows, int K, float *hi, floa
 
 // LCAO contraction of M basis rows: tensor cores (TF32 x3) in the mixed
 // path, FP64 CUDA-core GEMM otherwise.
-int lcao(cw_ctx *c, bool move, int M, const double *phi64, double *out) {
+int lcao(cw_ctx *c, bool move, int M, const double *phi64, double *out, cudaStream_t strm = nullptr) {
   const CSys &h = c->h;
+  cudaStream_t s = strm ? strm : c->stream;
   if (!c->mixed) {
-    dgemm(c->stream, M, h.Oa, h.K, phi64, c->g.coefT, out, move ? c->gemm_bn_move : c->gemm_bn_all);
+    dgemm(s, M, h.Oa, h.K, phi64, c->g.coefT, out, move ? c->gemm_bn_move : c->gemm_bn_all);
     return launch_check(c, "dgemm");
   }
   const CUtensorMap &ahi = move ? c->tm_mv_hi : c->tm_all_hi;
   const CUtensorMap &alo = move ? c->tm_mv_lo : c->tm_all_lo;
-  k_lcao_tf32x3<<<(M + 127) / 128, 128, c->smem_umma, c->stream>>>(ahi, alo, c->tm_b_hi, c->tm_b_lo, M, h.K, c->np,
-                                                                   h.Oa, c->umma_st, out, h.Oa, c->d_err);
+  k_lcao_tf32x3<<<(M + 127) / 128, 128, c->smem_umma, s>>>(ahi, alo, c->tm_b_hi, c->tm_b_lo, M, h.K, c->np,
+                                                           h.Oa, c->umma_st, out, h.Oa, c->d_err);
   return launch_check(c, "k_lcao_tf32x3");
 }
 
@@ -599,10 +604,10 @@ int md_before_propose(cw_ctx *c, int iel) {
   LCHK("k_md_drift_old");
   return CW_OK;
 }
-int md_after_lcao(cw_ctx *c, int iel) {
+int md_after_lcao(cw_ctx *c, int iel, cudaStream_t strm = nullptr) {
   if (!c->md_on) return CW_OK;
   stage_begin(c, CW_ST_MDET);
-  k_md_move<<<c->W, 128, c->smem_md_move, c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, c->g, iel);
+  k_md_move<<<c->W, 128, c->smem_md_move, strm ? strm : c->stream>>>(c->h, c->st, c->mb, c->md, c->mdt, c->g, iel);
   stage_end(c);
   LCHK("k_md_move");
   return CW_OK;
@@ -1028,6 +1033,9 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&c->ev0));
   CK(cudaEventCreate(&c->ev1));
+  CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
   CSys &h = c->h;
   std::memset(&h, 0, sizeof h);
   h.N = d->nelec; h.nup = d->nup; h.ndn = ndn; h.M = d->ncent; h.nctype = d->nctype;
@@ -1356,7 +1364,10 @@ void cw_destroy(cw_ctx *c) {
   if (c->d_stamps) cudaFree(c->d_stamps);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1627,22 +1638,35 @@ int vmc_sweep(cw_ctx *c) {
                                                                   c->smem_commit ? c->acc_count : nullptr);
     stage_end(c);
     LCHK("k_propose");
+    // the move Jastrow and the basis + LCAO of the proposed point depend only
+    // on the proposal: outside profiling they run side by side (the basis
+    // and LCAO on the side stream, joined before the decision)
+    const bool fork = !c->prof;
+    if (fork) {
+      CK(cudaEventRecord(c->ev_fork, c->stream));
+      CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    }
     stage_begin(c, CW_ST_JASTROW_MOVE);
     NORD_DISPATCH(launch_jmove, c, i);
     stage_end(c);
     LCHK("k_jastrow_move");
+    cudaStream_t bs = fork ? c->side : c->stream;
     const int bw = c->basis_warps;
     stage_begin(c, CW_ST_BASIS_MOVE);
-    k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->mb, c->g);
+    k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, bs>>>(c->h, c->st, c->mb, c->g);
     stage_end(c);
     LCHK("k_basis_move");
     stage_begin(c, CW_ST_LCAO_MOVE);
     {
-      int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn);
+      int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn, bs);
       stage_end(c);
       if (rc) return rc;
     }
-    if (int rc = md_after_lcao(c, i)) return rc;
+    if (int rc = md_after_lcao(c, i, bs)) return rc;  // needs the proposal and the LCAO only
+    if (fork) {
+      CK(cudaEventRecord(c->ev_join, c->side));
+      CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    }
     stage_begin(c, CW_ST_ACCEPT);
     k_decide<<<(W * kMoveGroup + 127) / 128, 128, 0, c->stream>>>(c->h, c->st, c->mb, c->g, i,
                                                                  c->smem_commit ? c->acc_list : nullptr, c->acc_count);
@@ -2336,6 +2360,8 @@ struct cw_batch {
   std::string err;
   // ragged mode: one launch per move stage over every system's walkers
   bool ragged = false;
+  cudaStream_t side = nullptr;  // ragged sweeps: basis + LCAO beside the move Jastrow
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int rag_bn = 0;               // N tile of the grouped FP64 LCAO (timed at build)
   long rag_launches = 0;        // ragged launches per sweep
   long rag_ctx_launches = 0;    // the systems' own hpsi launches per sweep
@@ -2361,8 +2387,11 @@ extern "C" int cw_batch_create(cw_batch **out, cw_ctx **ctxs, int n) {
   b->gen.assign(n, -1);
   if (cudaSetDevice(b->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
-      cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     delete b;
     return CW_ERR_CUDA;
   }
@@ -2388,8 +2417,9 @@ extern "C" void cw_batch_destroy(cw_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   rag_free(b);
-  for (cudaEvent_t e : {b->ev0, b->ev1, b->join})
+  for (cudaEvent_t e : {b->ev0, b->ev1, b->join, b->ev_fork, b->ev_join})
     if (e) cudaEventDestroy(e);
+  if (b->side) cudaStreamDestroy(b->side);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -2673,9 +2703,14 @@ int rag_build(cw_batch *b) {
   for (int k = 0; k < nel[0] && rc == CW_OK; k++) {
     while (A > 0 && nel[A - 1] <= k) A--;
     k_propose_rag<<<off16[A], 128, 0, s>>>(d_cs, d_slots, d_g16, k);
+    // the move Jastrow beside the basis + LCAO (both need only the proposal)
+    cudaEventRecord(b->ev_fork, s);
+    cudaStreamWaitEvent(b->side, b->ev_fork, 0);
     RAG_NORD(ncls, rag_jmove, s, mixed, off4[A], smem_jm, d_cs, d_slots, d_g4, k);
-    k_basis_move_rag<<<offbw[A], 32 * bw, smem_basis, s>>>(d_cs, d_slots, d_gbw);
-    rag_lcao(s, mixed, b->rag_bn, offt[A], smem_lcao, d_slots, d_tiles);
+    k_basis_move_rag<<<offbw[A], 32 * bw, smem_basis, b->side>>>(d_cs, d_slots, d_gbw);
+    rag_lcao(b->side, mixed, b->rag_bn, offt[A], smem_lcao, d_slots, d_tiles);
+    cudaEventRecord(b->ev_join, b->side);
+    cudaStreamWaitEvent(s, b->ev_join, 0);
     k_decide_rag<<<off16[A], 128, 0, s>>>(d_cs, d_slots, d_g16, k);
     k_commit_rag<<<commit_grid, 128, smem_commit, s>>>(d_cs, d_slots, A, k);
     nl += 6;
@@ -3060,22 +3095,34 @@ extern "C" int cw_dmc_steps(cw_ctx *c, int nstep) {
                                                         c->smem_commit ? c->acc_count : nullptr);
       stage_end(c);
       LCHK("k_dmc_propose");
+      // move Jastrow beside basis + LCAO + multideterminant ratios (all need
+      // only the proposal), joined before the decision; in order when profiling
+      const bool fork = !c->prof;
+      if (fork) {
+        CK(cudaEventRecord(c->ev_fork, c->stream));
+        CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+      }
       stage_begin(c, CW_ST_JASTROW_MOVE);
       NORD_DISPATCH(launch_jmove, c, i);
       stage_end(c);
       LCHK("k_jastrow_move");
+      cudaStream_t bs = fork ? c->side : c->stream;
       const int bw = c->basis_warps;
       stage_begin(c, CW_ST_BASIS_MOVE);
-      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->mb, c->g);
+      k_basis_move<<<(unsigned)((W + bw - 1) / bw), 32 * bw, c->smem_basis, bs>>>(c->h, c->st, c->mb, c->g);
       stage_end(c);
       LCHK("k_basis_move");
       stage_begin(c, CW_ST_LCAO_MOVE);
       {
-        int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn);
+        int rc = lcao(c, true, W * 4, c->mb.phi, c->mb.orbn, bs);
         stage_end(c);
         if (rc) return rc;
       }
-      if (int rc = md_after_lcao(c, i)) return rc;
+      if (int rc = md_after_lcao(c, i, bs)) return rc;
+      if (fork) {
+        CK(cudaEventRecord(c->ev_join, c->side));
+        CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+      }
       stage_begin(c, CW_ST_ACCEPT);
       k_dmc_decide<<<(W + 63) / 64, 64, 0, c->stream>>>(c->h, c->st, c->mb, c->g, b, sc, i,
                                                        c->smem_commit ? c->acc_list : nullptr, c->acc_count);
