@@ -61,6 +61,7 @@ struct cw_ctx {
   // run beside its move Jastrow (both need only the proposal)
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_jas = nullptr;  // hpsi: the full Jastrow done (the expansion's kinetic rows need its gradient)
   std::string err;
   CSys h;                 // host copy of the constant block
   GSys g{};               // device tables
@@ -679,10 +680,22 @@ int opt_accum(cw_ctx *c) {
 int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullptr) {
   const CSys &h = c->h;
   const int W = c->W, N = h.N, M = h.M;
+  // The full Jastrow and the orbital chain (basis, LCAO, scatter, Slater
+  // inverse, c~) share no buffer: outside profiling the chain runs on the
+  // side stream beside the Jastrow, joined before the ECP stage.  An
+  // expansion's kinetic rows (k_md_scatter) use the Jastrow gradient, so
+  // there the chain waits for the Jastrow before its first scatter.
+  const bool fork = !c->prof;
+  cudaStream_t os = fork ? c->side : c->stream;
+  if (fork) {
+    CK(cudaEventRecord(c->ev_fork, c->stream));
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+  }
   stage_begin(c, CW_ST_JASTROW_FULL);
   NORD_DISPATCH(launch_jfull, c);
   stage_end(c);
   LCHK("k_jastrow_full");
+  if (fork && c->md_on) CK(cudaEventRecord(c->ev_jas, c->stream));
   // orbitals in electron chunks
   const int ec = c->hb.chunk;
   for (int e0 = 0; e0 < N; e0 += ec) {
@@ -690,52 +703,59 @@ int run_hpsi(cw_ctx *c, int mode, double *d_e = nullptr, double *d_ekin = nullpt
     const long nwarps = (long)W * ne;
     const int bw = c->basis_warps;
     stage_begin(c, CW_ST_BASIS_ALL);
-    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, c->stream>>>(c->h, c->st, c->hb, c->g, e0, ne);
+    k_basis_all<<<(unsigned)((nwarps + bw - 1) / bw), 32 * bw, c->smem_basis, os>>>(c->h, c->st, c->hb, c->g, e0, ne);
     stage_end(c);
     LCHK("k_basis_all");
     stage_begin(c, CW_ST_LCAO_ALL);
     {
-      int rc = lcao(c, false, W * ne * 5, c->hb.phi, c->hb.orball);
+      int rc = lcao(c, false, W * ne * 5, c->hb.phi, c->hb.orball, os);
       stage_end(c);
       if (rc) return rc;
     }
     if (c->md_on) {
       const long nt = (long)W * ne * h.Oa;
+      if (fork && e0 == 0) CK(cudaStreamWaitEvent(os, c->ev_jas, 0));
       stage_begin(c, CW_ST_SCATTER);
-      k_md_scatter<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(c->h, c->st, c->md, c->hb.orball, e0, ne);
+      k_md_scatter<<<(unsigned)((nt + 127) / 128), 128, 0, os>>>(c->h, c->st, c->md, c->hb.orball, e0, ne);
       stage_end(c);
       LCHK("k_md_scatter");
     }
     if (c->orb_on) {
       const long nv = (long)W * ne * c->orb_nv;
-      k_orb_vals<<<(unsigned)((nv + 127) / 128), 128, 0, c->stream>>>(W, N, e0, ne, h.Oa, c->hb.orball, c->orb_nv,
-                                                                       c->orb_vorb, c->orb_vals);
+      k_orb_vals<<<(unsigned)((nv + 127) / 128), 128, 0, os>>>(W, N, e0, ne, h.Oa, c->hb.orball, c->orb_nv,
+                                                               c->orb_vorb, c->orb_vals);
       LCHK("k_orb_vals");
     }
     const long ns = (long)W * ne * h.nmax;
     stage_begin(c, CW_ST_SCATTER);
-    k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, c->stream>>>(c->h, c->st, c->hb, c->g, e0, ne);
+    k_scatter_orbs<<<(unsigned)((ns + 127) / 128), 128, 0, os>>>(c->h, c->st, c->hb, c->g, e0, ne);
     stage_end(c);
     LCHK("k_scatter_orbs");
   }
   stage_begin(c, CW_ST_SLATER_INV);
-  k_slater_inv<<<2 * W, 128, c->smem_sinv, c->stream>>>(c->h, c->st, c->hb, c->big_spin);
+  k_slater_inv<<<2 * W, 128, c->smem_sinv, os>>>(c->h, c->st, c->hb, c->big_spin);
   stage_end(c);
   LCHK("k_slater_inv");
   if (h.nloc > 0 && c->md_on) {
     const size_t np = (size_t)W * N * h.K;
-    k_md_zero<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(c->md.P, np);
+    k_md_zero<<<(unsigned)((np + 255) / 256), 256, 0, os>>>(c->md.P, np);
     LCHK("k_md_zero");
   }
   if (h.nloc > 0) {
     const int nchunk = (h.K + 63) / 64;
     stage_begin(c, CW_ST_CTILDE);
     if (c->bocc)  // rows (walker, spin, slot) of slmi times the occupied coefficient rows
-      dgemm(c->stream, W * N, h.K, h.nmax, c->st.slmi, c->bocc, c->hb.ctilde);
+      dgemm(os, W * N, h.K, h.nmax, c->st.slmi, c->bocc, c->hb.ctilde);
     else
-      k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, c->stream>>>(c->h, c->st, c->hb, c->g, c->big_spin);
+      k_ctilde<<<2 * W * nchunk, 256, c->smem_ctil, os>>>(c->h, c->st, c->hb, c->g, c->big_spin);
     stage_end(c);
     LCHK("k_ctilde");
+  }
+  if (fork) {
+    CK(cudaEventRecord(c->ev_join, c->side));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  }
+  if (h.nloc > 0) {
     stage_begin(c, CW_ST_ECP);
     NORD_DISPATCH(launch_ecp, c);
     stage_end(c);
@@ -1036,6 +1056,7 @@ int cw_create(cw_ctx **out, const cw_system_desc *d, int device, int precision) 
   CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_jas, cudaEventDisableTiming));
   CSys &h = c->h;
   std::memset(&h, 0, sizeof h);
   h.N = d->nelec; h.nup = d->nup; h.ndn = ndn; h.M = d->ncent; h.nctype = d->nctype;
@@ -1366,6 +1387,7 @@ void cw_destroy(cw_ctx *c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->ev_jas) cudaEventDestroy(c->ev_jas);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
