@@ -403,7 +403,7 @@ def run_serve(args):
     return 0
 
 
-def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode="graph"):
+def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode="graph", bands=1):
     """Sweeps of every system's own context, all at once: mode "graph" runs
     them as one CUDA graph of the contexts' sweep graphs (cw_batch_vmc_steps,
     one launch per sweep, timed with the batch's events); mode "ragged" as one
@@ -435,7 +435,7 @@ def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode
         # one CUDA graph per sweep: the systems' own sweep graphs as child
         # nodes, or (ragged) one launch per move stage over all systems
         from champ_b200.engine import Batch
-        b = Batch(engines, ragged=(mode == "ragged"))
+        b = Batch(engines, ragged=(bands if mode == "ragged" else 0))
         b.vmc_steps(warmup)                                      # captures + warm-up
         t0 = time.perf_counter()
         b.vmc_steps(steps)
@@ -444,7 +444,7 @@ def batched_rate(systems, walkers, precision, device, steps, warmup, slots, mode
         if mode == "ragged":
             info = b.info()
             extra_launches = steps * (info["ragged_launches"] + info["system_launches"])
-            tiles = {"ragged_lcao_tile": info["lcao_bn"]}
+            tiles = {"ragged_lcao_tile": info["lcao_bn"], "bands": info["bands"]}
         b.close()
         own_s = None
     else:
@@ -491,9 +491,10 @@ def run_batched(args):
             barrier(pg, local)
             res[prec] = batched_rate(systems, walkers, prec, local, args.steps, max(args.warmup, 1), args.slots)
             barrier(pg, local)
-            rag[prec] = batched_rate(systems, walkers, prec, local, args.steps, max(args.warmup, 1), args.slots,
-                                     mode="ragged")
-            barrier(pg, local)
+            for nb in (1, args.bands):
+                rag[(prec, nb)] = batched_rate(systems, walkers, prec, local, args.steps, max(args.warmup, 1),
+                                               args.slots, mode="ragged", bands=nb)
+                barrier(pg, local)
         barrier(pg, local)
         threads = batched_rate(systems, walkers, args.precision, local, args.steps, max(args.warmup, 1), args.slots,
                                mode="threads")
@@ -520,11 +521,12 @@ def run_batched(args):
         "batched": {p: {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4), "wall_s": round(v[1], 4),
                         "mode": "one CUDA graph of all systems' sweep graphs, one launch per sweep"}
                     for p, v in res.items()},
-        "batched_ragged": {p: {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4),
-                               "wall_s": round(v[1], 4), "launches": v[4], "lcao_tile": v[5],
-                               "mode": "one launch per move stage over every system's walkers "
-                                       "(cw_batch_set_ragged), systems' hpsi on their own streams, one graph"}
-                           for p, v in rag.items()},
+        "batched_ragged": {f"{p}_bands{nb}": {"moves_per_s": round(v[0], 1), "device_span_s": round(v[3], 4),
+                                              "wall_s": round(v[1], 4), "launches": v[4], "lcao_tile": v[5],
+                                              "mode": "one launch per move stage over the walkers of every system "
+                                                      "of a band (cw_batch_set_ragged), bands side by side, "
+                                                      "systems' hpsi on their own streams, one graph"}
+                           for (p, nb), v in rag.items()},
         "batched_threads": {"precision": args.precision, "moves_per_s": round(threads[0], 1),
                             "device_span_s": round(threads[3], 4),
                             "sum_of_context_device_s": round(threads[2], 4),
@@ -744,6 +746,7 @@ def main():
                     help="c3/c4: HBM budget of the resident contexts (default 120 for c3, 16 for c4)")
     ap.add_argument("--systems", type=int, default=64, help="c3: systems resident at once")
     ap.add_argument("--slots", type=int, default=16, help="c3/c4: worker threads (contexts with work in flight)")
+    ap.add_argument("--bands", type=int, default=4, help="c3: bands of systems of the banded ragged run")
     args = ap.parse_args()
     if args.budget_gb is None:
         args.budget_gb = 120.0 if args.config == "c3" else 16.0

@@ -2382,12 +2382,15 @@ struct cw_batch {
   std::string err;
   // ragged mode: one launch per move stage over every system's walkers
   bool ragged = false;
-  cudaStream_t side = nullptr;  // ragged sweeps: basis + LCAO beside the move Jastrow
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr;  // ragged capture: start of the bands
   int rag_bn = 0;               // N tile of the grouped FP64 LCAO (timed at build)
   long rag_launches = 0;        // ragged launches per sweep
   long rag_ctx_launches = 0;    // the systems' own hpsi launches per sweep
+  int rag_bands = 1;            // bands asked for (cw_batch_set_ragged)
+  int rag_nband = 0;            // bands of the built graph
   std::vector<void *> rag_allocs;
+  std::vector<cudaStream_t> rag_streams;  // each band's two streams
+  std::vector<cudaEvent_t> rag_events;    // each band's fork, join and end events
   std::vector<cudaEvent_t> rag_fork, rag_done;  // per system: start and end of its hpsi branch
 };
 
@@ -2409,11 +2412,9 @@ extern "C" int cw_batch_create(cw_batch **out, cw_ctx **ctxs, int n) {
   b->gen.assign(n, -1);
   if (cudaSetDevice(b->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
     delete b;
     return CW_ERR_CUDA;
   }
@@ -2425,6 +2426,10 @@ namespace {
 void rag_free(cw_batch *b) {
   for (void *p : b->rag_allocs) cudaFree(p);
   b->rag_allocs.clear();
+  for (cudaEvent_t e : b->rag_events) cudaEventDestroy(e);
+  b->rag_events.clear();
+  for (cudaStream_t st : b->rag_streams) cudaStreamDestroy(st);
+  b->rag_streams.clear();
   for (cudaEvent_t e : b->rag_fork) cudaEventDestroy(e);
   for (cudaEvent_t e : b->rag_done) cudaEventDestroy(e);
   b->rag_fork.clear();
@@ -2439,9 +2444,8 @@ extern "C" void cw_batch_destroy(cw_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   rag_free(b);
-  for (cudaEvent_t e : {b->ev0, b->ev1, b->join, b->ev_fork, b->ev_join})
+  for (cudaEvent_t e : {b->ev0, b->ev1, b->join, b->ev_fork})
     if (e) cudaEventDestroy(e);
-  if (b->side) cudaStreamDestroy(b->side);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -2631,7 +2635,8 @@ int rag_build(cw_batch *b) {
     r.err = c->d_err;
   }
   const RagSlot *d_slots = rag_upload(b, hs);
-  // block maps
+  if (!d_slots) return bfail(b, CW_ERR_CUDA, "ragged batch: slots");
+  // launch shapes common to all bands
   int bw = 4;
   int maxM = 0;
   size_t smem_jm = 0, smem_commit = 0, smem_umma = 0;
@@ -2643,15 +2648,11 @@ int rag_build(cw_batch *b) {
     smem_umma = std::max(smem_umma, c->smem_umma);
   }
   const size_t smem_basis = (size_t)bw * maxM * kCenRec * sizeof(double);
-  std::vector<int> off16, off4, offbw, offrot;
-  const int2 *d_g16 = rag_upload(b, rag_map(W, 128 / kMoveGroup, off16));
-  const int2 *d_g4 = rag_upload(b, rag_map(W, 4, off4));
-  const int2 *d_gbw = rag_upload(b, rag_map(W, bw, offbw));
+  std::vector<int> offrot;
   std::vector<int> Wrot(n);
   for (int i = 0; i < n; i++) Wrot[i] = sc[i]->h.nloc > 0 ? W[i] : 0;
   const int2 *d_rot = rag_upload(b, rag_map(Wrot, 128, offrot));
-  if (!d_slots || !d_g16 || !d_g4 || !d_gbw || !d_rot) return bfail(b, CW_ERR_CUDA, "ragged batch: block maps");
-  // launch attributes
+  if (!d_rot) return bfail(b, CW_ERR_CUDA, "ragged batch: block maps");
   cudaError_t ea = cudaSuccess;
   RAG_NORD(ncls, rag_jmove_attr_v, ea, mixed, smem_jm);
   RAG_CK(ea, "ragged move Jastrow attributes");
@@ -2663,13 +2664,10 @@ int rag_build(cw_batch *b) {
   RAG_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device), "device attributes");
   RAG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_commit_rag, 128, smem_commit), "commit occupancy");
   const int commit_grid = std::max(1, nsm * std::max(1, per));
-  // LCAO tiles: the N tile of the tensor-core tiles is timed over the whole
+  // LCAO tile: the N tile of the tensor-core tiles is timed over the whole
   // batch (every output sums its K slices in the same order whatever the tile)
-  std::vector<int> offt;
-  const RagTile *d_tiles = nullptr;
   size_t smem_lcao = 0;
   if (mixed) {
-    d_tiles = rag_upload(b, rag_tiles(sc, true, 0, offt));
     smem_lcao = smem_umma;
     RAG_CK(cudaFuncSetAttribute(k_lcao_tf32x3_rag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_lcao),
            "ragged tensor-core LCAO attributes");
@@ -2693,16 +2691,58 @@ int rag_build(cw_batch *b) {
       RAG_CK(cudaGetLastError(), "ragged LCAO");
       float ms = 0;
       cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-      if (!d_tiles || ms < best) {
+      if (b->rag_bn == 0 || ms < best) {
         best = ms;
-        d_tiles = dt;
-        offt = o;
         b->rag_bn = bn;
       }
     }
     smem_lcao = mma_smem(b->rag_bn);
   }
-  if (!d_tiles) return bfail(b, CW_ERR_CUDA, "ragged batch: LCAO tiles");
+  // bands: contiguous runs of the sorted systems with about equal moves per
+  // sweep, each its own chain of ragged launches on its own streams
+  std::vector<int> cut{0};
+  {
+    double tot = 0, acc = 0;
+    for (int i = 0; i < n; i++) tot += (double)W[i] * nel[i];
+    const int want = std::max(1, std::min(b->rag_bands, n));
+    for (int i = 0; i < n; i++) {
+      acc += (double)W[i] * nel[i];
+      if ((int)cut.size() < want && i + 1 < n && acc >= tot * (double)cut.size() / want) cut.push_back(i + 1);
+    }
+    cut.push_back(n);
+  }
+  const int nband = (int)cut.size() - 1;
+  struct Band {
+    int s0, s1;
+    std::vector<int> off16, off4, offbw, offt;
+    const int2 *g16, *g4, *gbw;
+    const RagTile *tiles;
+    cudaStream_t main, side;
+    cudaEvent_t fork, join, end;
+  };
+  std::vector<Band> band(nband);
+  for (int g = 0; g < nband; g++) {
+    Band &B = band[g];
+    B.s0 = cut[g];
+    B.s1 = cut[g + 1];
+    const std::vector<int> Wg(W.begin() + B.s0, W.begin() + B.s1);
+    const std::vector<cw_ctx *> scg(sc.begin() + B.s0, sc.begin() + B.s1);
+    B.g16 = rag_upload(b, rag_map(Wg, 128 / kMoveGroup, B.off16));
+    B.g4 = rag_upload(b, rag_map(Wg, 4, B.off4));
+    B.gbw = rag_upload(b, rag_map(Wg, bw, B.offbw));
+    B.tiles = rag_upload(b, rag_tiles(scg, mixed, b->rag_bn, B.offt));
+    if (!B.g16 || !B.g4 || !B.gbw || !B.tiles) return bfail(b, CW_ERR_CUDA, "ragged batch: band maps");
+    B.main = B.side = nullptr;
+    B.fork = B.join = B.end = nullptr;
+    RAG_CK(cudaStreamCreateWithFlags(&B.main, cudaStreamNonBlocking), "band streams");
+    b->rag_streams.push_back(B.main);
+    RAG_CK(cudaStreamCreateWithFlags(&B.side, cudaStreamNonBlocking), "band streams");
+    b->rag_streams.push_back(B.side);
+    for (cudaEvent_t *e : {&B.fork, &B.join, &B.end}) {
+      RAG_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "band events");
+      b->rag_events.push_back(*e);
+    }
+  }
   // events of the systems' hpsi branches
   b->rag_fork.assign(n, nullptr);
   b->rag_done.assign(n, nullptr);
@@ -2710,7 +2750,7 @@ int rag_build(cw_batch *b) {
     RAG_CK(cudaEventCreateWithFlags(&b->rag_fork[i], cudaEventDisableTiming), "events");
     RAG_CK(cudaEventCreateWithFlags(&b->rag_done[i], cudaEventDisableTiming), "events");
   }
-  // capture one sweep
+  // capture one sweep: rotqua of every system, then the bands side by side
   cudaStream_t s = b->stream;
   RAG_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "ragged capture");
   long nl = 0, nc = 0;
@@ -2721,50 +2761,69 @@ int rag_build(cw_batch *b) {
     k_rotqua_rag<<<offrot[n], 128, 0, s>>>(d_cs, d_slots, d_rot);
     nl++;
   }
-  int A = n;
-  for (int k = 0; k < nel[0] && rc == CW_OK; k++) {
-    while (A > 0 && nel[A - 1] <= k) A--;
-    k_propose_rag<<<off16[A], 128, 0, s>>>(d_cs, d_slots, d_g16, k);
-    // the move Jastrow beside the basis + LCAO (both need only the proposal)
-    cudaEventRecord(b->ev_fork, s);
-    cudaStreamWaitEvent(b->side, b->ev_fork, 0);
-    RAG_NORD(ncls, rag_jmove, s, mixed, off4[A], smem_jm, d_cs, d_slots, d_g4, k);
-    k_basis_move_rag<<<offbw[A], 32 * bw, smem_basis, b->side>>>(d_cs, d_slots, d_gbw);
-    rag_lcao(b->side, mixed, b->rag_bn, offt[A], smem_lcao, d_slots, d_tiles);
-    cudaEventRecord(b->ev_join, b->side);
-    cudaStreamWaitEvent(s, b->ev_join, 0);
-    k_decide_rag<<<off16[A], 128, 0, s>>>(d_cs, d_slots, d_g16, k);
-    k_commit_rag<<<commit_grid, 128, smem_commit, s>>>(d_cs, d_slots, A, k);
-    nl += 6;
-    const cudaError_t le = cudaGetLastError();
-    if (le != cudaSuccess) {
+  cudaEventRecord(b->ev_fork, s);
+  for (int g = 0; g < nband && rc == CW_OK; g++) {
+    Band &B = band[g];
+    const CSys *cs = d_cs + B.s0;
+    const RagSlot *sl = d_slots + B.s0;
+    const int nbs = B.s1 - B.s0;
+    const int *ne = nel.data() + B.s0;
+    cudaStream_t bm = B.main;
+    if (cudaStreamWaitEvent(bm, b->ev_fork, 0) != cudaSuccess) {
       rc = CW_ERR_CUDA;
-      why = std::string("ragged launch: ") + cudaGetErrorString(le);
+      why = "ragged capture: band fork";
       break;
     }
-    // the systems whose last electron just moved: hpsi on their own streams
-    for (int i = A - 1; i >= 0 && nel[i] == k + 1; i--) {
-      cw_ctx *c = sc[i];
-      if (cudaEventRecord(b->rag_fork[i], s) != cudaSuccess ||
-          cudaStreamWaitEvent(c->stream, b->rag_fork[i], 0) != cudaSuccess) {
+    int A = nbs;
+    for (int k = 0; k < ne[0] && rc == CW_OK; k++) {
+      while (A > 0 && ne[A - 1] <= k) A--;
+      k_propose_rag<<<B.off16[A], 128, 0, bm>>>(cs, sl, B.g16, k);
+      // the move Jastrow beside the basis + LCAO (both need only the proposal)
+      cudaEventRecord(B.fork, bm);
+      cudaStreamWaitEvent(B.side, B.fork, 0);
+      RAG_NORD(ncls, rag_jmove, bm, mixed, B.off4[A], smem_jm, cs, sl, B.g4, k);
+      k_basis_move_rag<<<B.offbw[A], 32 * bw, smem_basis, B.side>>>(cs, sl, B.gbw);
+      rag_lcao(B.side, mixed, b->rag_bn, B.offt[A], smem_lcao, sl, B.tiles);
+      cudaEventRecord(B.join, B.side);
+      cudaStreamWaitEvent(bm, B.join, 0);
+      k_decide_rag<<<B.off16[A], 128, 0, bm>>>(cs, sl, B.g16, k);
+      k_commit_rag<<<commit_grid, 128, smem_commit, bm>>>(cs, sl, A, k);
+      nl += 6;
+      const cudaError_t le = cudaGetLastError();
+      if (le != cudaSuccess) {
         rc = CW_ERR_CUDA;
-        why = "ragged capture: fork";
+        why = std::string("ragged launch: ") + cudaGetErrorString(le);
         break;
       }
-      forked++;
-      const long l0 = c->launches;
-      rc = run_hpsi(c, 1);
-      if (rc == CW_OK && c->opt_np > 0) rc = opt_accum(c);
-      nc += c->launches - l0;
-      c->launches = l0;
-      cudaEventRecord(b->rag_done[i], c->stream);
-      cudaStreamWaitEvent(s, b->rag_done[i], 0);
-      if (rc) {
-        why = "system " + std::to_string(order[i]) + ": " + c->err;
-        break;
+      // the band's systems whose last electron just moved: hpsi on their own streams
+      for (int j = A - 1; j >= 0 && ne[j] == k + 1; j--) {
+        const int i = B.s0 + j;
+        cw_ctx *c = sc[i];
+        if (cudaEventRecord(b->rag_fork[i], bm) != cudaSuccess ||
+            cudaStreamWaitEvent(c->stream, b->rag_fork[i], 0) != cudaSuccess) {
+          rc = CW_ERR_CUDA;
+          why = "ragged capture: fork";
+          break;
+        }
+        forked++;
+        const long l0 = c->launches;
+        rc = run_hpsi(c, 1);
+        if (rc == CW_OK && c->opt_np > 0) rc = opt_accum(c);
+        nc += c->launches - l0;
+        c->launches = l0;
+        cudaEventRecord(b->rag_done[i], c->stream);
+        if (rc) {
+          why = "system " + std::to_string(order[i]) + ": " + c->err;
+          break;
+        }
       }
     }
+    cudaEventRecord(B.end, bm);
   }
+  // join every band and every system's hpsi branch
+  for (int g = 0; g < nband; g++)
+    if (band[g].end) cudaStreamWaitEvent(s, band[g].end, 0);
+  for (int i = 0; i < n; i++) cudaStreamWaitEvent(s, b->rag_done[i], 0);
   cudaGraph_t gph = nullptr;
   const cudaError_t ee = cudaStreamEndCapture(s, &gph);
   if (rc != CW_OK || ee != cudaSuccess) {
@@ -2780,6 +2839,7 @@ int rag_build(cw_batch *b) {
     cudaGraphDestroy(gph);
     return bfail(b, CW_ERR_STATE, "ragged capture: a system's hpsi was not scheduled");
   }
+  b->rag_nband = nband;
   b->graph = gph;
   b->rag_launches = nl;
   b->rag_ctx_launches = nc;
@@ -2789,32 +2849,37 @@ int rag_build(cw_batch *b) {
 
 }  // namespace
 
-// Ragged mode on or off: refused (with the reason) when a system cannot join
-extern "C" int cw_batch_set_ragged(cw_batch *b, int on) {
-  if (!b) return CW_ERR_ARG;
-  if (on) {
+// Ragged mode off (bands = 0) or on with that many bands of systems (each
+// band its own chain of launches); refused (with the reason) when a system
+// cannot join
+extern "C" int cw_batch_set_ragged(cw_batch *b, int bands) {
+  if (!b || bands < 0) return CW_ERR_ARG;
+  if (bands) {
     const std::string why = rag_refusal(b);
     if (!why.empty()) return bfail(b, CW_ERR_UNSUPPORTED, ("ragged batch: " + why).c_str());
   }
-  if (b->ragged != (on != 0)) {
+  if (b->ragged != (bands != 0) || (bands && bands != b->rag_bands)) {
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, CW_ERR_CUDA, "cudaSetDevice failed");
     cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
-    b->ragged = on != 0;
+    b->ragged = bands != 0;
+    if (bands) b->rag_bands = bands;
   }
   return CW_OK;
 }
 
-// [ragged, LCAO N tile, ragged launches per sweep, the systems' own hpsi launches per sweep]
+// [bands asked for (0: off), LCAO N tile, ragged launches per sweep, the
+//  systems' own hpsi launches per sweep, bands of the built graph]
 extern "C" int cw_batch_info(const cw_batch *b, int64_t *info) {
   if (!b || !info) return CW_ERR_ARG;
-  info[0] = b->ragged ? 1 : 0;
+  info[0] = b->ragged ? b->rag_bands : 0;
   info[1] = b->rag_bn;
   info[2] = b->rag_launches;
   info[3] = b->rag_ctx_launches;
+  info[4] = b->rag_nband;
   return CW_OK;
 }
 

@@ -372,10 +372,11 @@ class Batch:
     """Several engines (one device) advanced together: each cw_batch_vmc_steps
     call runs nstep sweeps of every engine through one CUDA graph launch per
     sweep (the engines' own sweep graphs as parallel child nodes), or, with
-    ``ragged=True``, through one launch per move stage over every engine's
-    walkers."""
+    ``ragged`` = True or a band count, through one launch per move stage over
+    the walkers of every engine of a band (bands of systems of about equal
+    work, side by side)."""
 
-    def __init__(self, engines, ragged: bool = False):
+    def __init__(self, engines, ragged: bool | int = False):
         self.engines = list(engines)
         self.lib = self.engines[0].lib
         arr = (C.c_void_p * len(self.engines))(*[e.h for e in self.engines])
@@ -385,21 +386,21 @@ class Batch:
             raise EngineError(f"cw_batch_create failed (status {rc})", rc)
         self.h = h
         if ragged:
-            self.set_ragged(True)
+            self.set_ragged(ragged)
 
-    def set_ragged(self, on: bool):
-        rc = self.lib.cw_batch_set_ragged(self.h, 1 if on else 0)
+    def set_ragged(self, bands: bool | int):
+        rc = self.lib.cw_batch_set_ragged(self.h, int(bands))
         if rc:
             msg = self.lib.cw_batch_last_error(self.h).decode()
             raise EngineError(f"cw_batch_set_ragged failed (status {rc}): {msg}", rc)
 
     def info(self) -> dict:
-        v = (C.c_int64 * 4)()
+        v = (C.c_int64 * 5)()
         rc = self.lib.cw_batch_info(self.h, v)
         if rc:
             raise EngineError(f"cw_batch_info failed (status {rc})", rc)
-        return {"ragged": bool(v[0]), "lcao_bn": int(v[1]), "ragged_launches": int(v[2]),
-                "system_launches": int(v[3])}
+        return {"ragged": bool(v[0]), "bands_asked": int(v[0]), "lcao_bn": int(v[1]),
+                "ragged_launches": int(v[2]), "system_launches": int(v[3]), "bands": int(v[4])}
 
     def vmc_steps(self, nstep: int):
         rc = self.lib.cw_batch_vmc_steps(self.h, int(nstep))

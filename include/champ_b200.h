@@ -182,26 +182,29 @@ int cw_autotune(cw_ctx *ctx, int reps, int32_t *choice);
  * each context's results are bitwise those of cw_vmc_steps on it alone.
  * cw_batch_last_ms: device time of the last call's sweeps.
  *
- * cw_batch_set_ragged(batch, 1) switches the batch to one launch per move
- * stage over every system's walkers (systems of different electron, centre,
- * basis and orbital counts): electron k of every system with more than k
- * electrons moves in the same six launches, each block working on one
- * system's walkers; after its last electron a system's hpsi runs on its own
- * stream inside the same graph.  Each system takes the walk it takes alone:
+ * cw_batch_set_ragged(batch, bands) with bands >= 1 switches the batch to
+ * one launch per move stage over the walkers of many systems (of different
+ * electron, centre, basis and orbital counts): the systems, sorted by
+ * electron count, are cut into `bands` runs of about equal work; in a band,
+ * electron k of every system with more than k electrons moves in the same
+ * six launches, each block working on one system's walkers, and the bands'
+ * chains run side by side; after its last electron a system's hpsi runs on
+ * its own stream inside the same graph.  bands = 0 returns to the child
+ * graphs.  Each system takes the walk it takes alone:
  * the same random streams and decisions, bitwise in mixed precision, to
  * rounding (1e-10 relative over a few sweeps) in FP64.  Refused (CW_ERR_UNSUPPORTED, reason in cw_batch_last_error)
  * unless every system is a one-determinant VMC population with spins of at
  * most 128 electrons, the same precision and the same e-e-n order.
- * cw_batch_info: [ragged, N tile of the grouped FP64 LCAO (timed when the
- * graph is built), ragged launches per sweep, the systems' own hpsi
- * launches per sweep]. */
+ * cw_batch_info: [bands asked for (0: not ragged), N tile of the grouped
+ * FP64 LCAO (timed when the graph is built), ragged launches per sweep, the
+ * systems' own hpsi launches per sweep, bands of the built graph]. */
 typedef struct cw_batch cw_batch;
 int cw_batch_create(cw_batch **batch, cw_ctx **ctxs, int nctx);
 int cw_batch_vmc_steps(cw_batch *batch, int nstep);
 float cw_batch_last_ms(const cw_batch *batch);
 const char *cw_batch_last_error(const cw_batch *batch);
 void cw_batch_destroy(cw_batch *batch);
-int cw_batch_set_ragged(cw_batch *batch, int on);
+int cw_batch_set_ragged(cw_batch *batch, int bands);
 int cw_batch_info(const cw_batch *batch, int64_t *info);
 int cw_stamps(cw_ctx *ctx, int64_t *ns, int n);
 

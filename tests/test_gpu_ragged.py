@@ -102,6 +102,30 @@ def test_ragged_mixed_matches_alone():
     _check_ragged(_systems()[:3] + _systems()[4:], (80, 64, 48, 72), "mixed")
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ragged_bands_match_alone(precision):
+    """Three bands of systems, each its own chain of ragged launches."""
+    from champ_b200.engine import Batch
+    systems = _systems()
+    walkers = (96, 64, 48, 40, 72)
+    alone = _alone(systems, walkers, precision)
+    engines = _engines(systems, walkers, precision)
+    b = Batch(engines, ragged=3)
+    b.vmc_steps(2)
+    info = b.info()
+    assert info["bands_asked"] == 3 and info["bands"] == 3
+    nel = sorted((s.nelec for s in systems), reverse=True)
+    assert 6 * nel[0] + 1 < info["ragged_launches"] <= 6 * sum(nel) + 1
+    for e in engines:
+        e.end_block()
+    b.vmc_steps(2)
+    for i, (e, (wa, sa, ra)) in enumerate(zip(engines, alone)):
+        _same_walk(e, wa, sa, ra, precision, i)
+    b.close()
+    for e in engines:
+        e.close()
+
+
 def test_ragged_back_to_child_graphs():
     """Switching ragged mode off returns to the child-graph batch, same walk."""
     from champ_b200.engine import Batch
