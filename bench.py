@@ -616,9 +616,7 @@ def run_ours(args):
     for _ in range(e2e_steps):
         eng.set_walkers(x_h, r_h)          # H2D: positions + streams (zerest recompute)
         eng.vmc_steps(1)
-        xx, rr = eng.walkers()             # D2H: positions + streams
-        x_h[...] = xx
-        r_h[...] = rr
+        eng.walkers(x_h, r_h)              # D2H: positions + streams, into the pinned buffers
         eng.end_block()                    # D2H: per-walker sums
     barrier(pg, local)
     e2e_s = max_over_ranks(time.perf_counter() - t0, pg, local)
@@ -699,7 +697,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{world} (independent walker populations, no data-path collective)"},
         "e2e": {"value": e2e, "unit": "electron-moves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "cw_set_walkers (pinned host x, rng; includes the zerest hpsi of every walker) + "
-                        "cw_vmc_steps(1) + cw_get_walkers + cw_end_block"},
+                        "cw_vmc_steps(1) + cw_get_walkers (into the pinned x, rng) + cw_end_block"},
         "roofline": roof, "roofline_hbm": roof_hbm,
         "efficiency_fp64": {"value": ef64["efficiency"], "unit": "1/(Ha^2 s)", "energy": ef64["energy"],
                             "err": ef64["err"], "sigma": ef64["sigma"], "tcorr": ef64["tcorr"],

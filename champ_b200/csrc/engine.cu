@@ -81,6 +81,7 @@ struct cw_ctx {
   int big_spin = 0;        // Slater inverse and c~ on global memory (spins too large for shared memory)
   int ecp_rr_global = 0;   // k_ecp's e-n distances on global memory (hb.ecp_rr)
   int *acc_list = nullptr, *acc_count = nullptr;  // accepted walkers of a move (k_accept_list)
+  double *xstage = nullptr;  // [W][N][3] positions in the caller's layout (cw_set_walkers / cw_get_walkers)
   int ecp_warps = 1, ecp_naov = 0, ecp_minb = 1;
   size_t dev_bytes = 0;  // bytes of this context's cudaMalloc allocations
   std::unordered_map<void *, size_t> alloc_bytes;
@@ -840,6 +841,7 @@ int alloc_walkers(cw_ctx *c, int W) {
   WState &s = c->st;
   s.W = W;
   DALLOC(L, s.x, (size_t)W * 3 * N);
+  DALLOC(L, c->xstage, (size_t)W * 3 * N);
   DALLOC(L, s.rng, (size_t)W * 4);
   DALLOC(L, s.xq, (size_t)W * 3 * NQ);
   DALLOC(L, s.rmino, (size_t)W * N);
@@ -981,15 +983,8 @@ int zerest(cw_ctx *c) {
   const CSys &h = c->h;
   const int W = c->W, NQ = h.nquad;
   if (NQ > 0) {
-    std::vector<double> xq((size_t)W * 3 * NQ);
-    for (int w = 0; w < W; w++)
-      for (int q = 0; q < NQ; q++) {
-        xq[(size_t)w * 3 * NQ + q] = h.xq0[q];
-        xq[(size_t)w * 3 * NQ + NQ + q] = h.yq0[q];
-        xq[(size_t)w * 3 * NQ + 2 * NQ + q] = h.zq0[q];
-      }
-    CK(cudaMemcpyAsync(c->st.xq, xq.data(), sizeof(double) * xq.size(), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    k_xq_unrotated<<<(W + 127) / 128, 128, 0, c->stream>>>(c->h, c->st);
+    LCHK("k_xq_unrotated");
   }
   int rc = run_hpsi(c, 0);
   if (rc) return rc;
@@ -1434,15 +1429,15 @@ int cw_set_walkers(cw_ctx *c, int nwalk, const double *x, const uint64_t *rng) {
     int rc = alloc_walkers(c, nwalk);
     if (rc) return rc;
   }
+  // the caller's array as it is (one copy; pinned memory goes straight to
+  // the device), reordered on the device
   const int N = c->h.N;
-  std::vector<double> xt((size_t)nwalk * 3 * N);
-  for (int w = 0; w < nwalk; w++)
-    for (int e = 0; e < N; e++)
-      for (int k = 0; k < 3; k++) xt[((size_t)w * 3 + k) * N + e] = x[((size_t)w * N + e) * 3 + k];
-  CK(cudaMemcpyAsync(c->st.x, xt.data(), sizeof(double) * xt.size(), cudaMemcpyHostToDevice, c->stream));
+  const long nt = (long)nwalk * N;
+  CK(cudaMemcpyAsync(c->xstage, x, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, c->stream));
+  k_x_from_host<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(nwalk, N, c->xstage, c->st.x);
+  LCHK("k_x_from_host");
   CK(cudaMemcpyAsync(c->st.rng, rng, sizeof(uint64_t) * 4 * nwalk, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->st.status, 0, sizeof(int) * nwalk, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
   return zerest(c);
 }
 
@@ -1521,18 +1516,15 @@ int cw_walker_status(cw_ctx *c, int32_t *status) {
 int cw_get_walkers(cw_ctx *c, double *x, uint64_t *rng) {
   if (!c || c->W == 0) return fail(c, CW_ERR_STATE, "no walkers");
   const int N = c->h.N, W = c->W;
+  BIND(c);
   if (x) {
-    std::vector<double> xt((size_t)W * 3 * N);
-    CK(cudaMemcpyAsync(xt.data(), c->st.x, sizeof(double) * xt.size(), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int w = 0; w < W; w++)
-      for (int e = 0; e < N; e++)
-        for (int k = 0; k < 3; k++) x[((size_t)w * N + e) * 3 + k] = xt[((size_t)w * 3 + k) * N + e];
+    const long nt = (long)W * N;
+    k_x_to_host<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(W, N, c->st.x, c->xstage);
+    LCHK("k_x_to_host");
+    CK(cudaMemcpyAsync(x, c->xstage, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, c->stream));
   }
-  if (rng) {
-    CK(cudaMemcpyAsync(rng, c->st.rng, sizeof(uint64_t) * 4 * W, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-  }
+  if (rng) CK(cudaMemcpyAsync(rng, c->st.rng, sizeof(uint64_t) * 4 * W, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return CW_OK;
 }
 

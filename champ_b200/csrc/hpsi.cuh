@@ -941,6 +941,40 @@ __device__ __forceinline__ void rotqua_body(const CSys &cs, const WState &st, co
 }
 __global__ void k_rotqua(const __grid_constant__ CSys cs, WState st) { rotqua_body(cs, st, blockIdx.x); }
 
+// Positions between the caller's layout [W][N][3] (CHAMP's xold(3,nelec)
+// per walker) and the engine's [W][3][N]: thread per (walker, electron).
+__global__ void k_x_from_host(int W, int N, const double *__restrict__ src, double *__restrict__ dst) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)W * N) return;
+  const long w = t / N, e = t % N;
+  const double *p = src + 3 * t;
+  dst[(w * 3 + 0) * N + e] = p[0];
+  dst[(w * 3 + 1) * N + e] = p[1];
+  dst[(w * 3 + 2) * N + e] = p[2];
+}
+__global__ void k_x_to_host(int W, int N, const double *__restrict__ src, double *__restrict__ dst) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)W * N) return;
+  const long w = t / N, e = t % N;
+  double *p = dst + 3 * t;
+  p[0] = src[(w * 3 + 0) * N + e];
+  p[1] = src[(w * 3 + 1) * N + e];
+  p[2] = src[(w * 3 + 2) * N + e];
+}
+
+// zerest's unrotated quadrature points of every walker: thread per walker
+__global__ void k_xq_unrotated(const __grid_constant__ CSys cs, WState st) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.W) return;
+  const int NQ = cs.nquad;
+  double *xq = st.xq + (size_t)w * 3 * NQ;
+  for (int q = 0; q < NQ; q++) {
+    xq[q] = cs.xq0[q];
+    xq[NQ + q] = cs.yq0[q];
+    xq[2 * NQ + q] = cs.zq0[q];
+  }
+}
+
 // zerest's nearest-nucleus tables: thread per (walker, electron)
 __global__ void k_nearest(const __grid_constant__ CSys cs, WState st) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;

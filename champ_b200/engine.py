@@ -183,11 +183,18 @@ class Engine:
     def update_ymat(self, iel: int):
         self._check(self.lib.cw_update_ymat(self.h, iel), "cw_update_ymat")
 
-    def walkers(self):
-        x = np.zeros((self.W, self.system.nelec, 3))
-        r = np.zeros((self.W, 4), np.uint64)
-        self._check(self.lib.cw_get_walkers(self.h, dptr(x), u64ptr(r)), "cw_get_walkers")
-        return x, r
+    def walkers(self, x=None, rng=None):
+        """Positions [W][nelec][3] and random streams [W][4]; written into
+        the given C-contiguous arrays when passed (e.g. pinned host buffers,
+        which the device writes directly), else into new ones."""
+        if x is None:
+            x = np.zeros((self.W, self.system.nelec, 3))
+        if rng is None:
+            rng = np.zeros((self.W, 4), np.uint64)
+        if x.shape != (self.W, self.system.nelec, 3) or rng.shape != (self.W, 4):
+            raise ValueError(f"walkers: arrays of shape {x.shape}, {rng.shape} for {self.W} walkers")
+        self._check(self.lib.cw_get_walkers(self.h, dptr(x), u64ptr(rng)), "cw_get_walkers")
+        return x, rng
 
     # -- VMC driver --------------------------------------------------------
     def vmc_steps(self, nstep: int):
