@@ -37,3 +37,25 @@ def test_graph_replay_matches_direct_launches(cfg):
     a.vmc_steps(1)
     b.vmc_steps(1)
     assert np.array_equal(a.walkers()[0], b.walkers()[0])
+
+
+def test_walkers_round_trip_through_caller_buffers():
+    """cw_set_walkers / cw_get_walkers move positions in the caller's
+    [W][N][3] layout (reordered on the device): the positions come back
+    exactly, into new arrays or into the caller's (pinned) buffers."""
+    import torch
+    e, x, rng = _engine("c0", W=37)
+    x0, r0 = e.walkers()
+    assert np.array_equal(x0, x) and np.array_equal(r0, rng)
+    xp = torch.empty(x.shape, dtype=torch.float64, pin_memory=True).numpy()
+    rp = torch.empty(rng.shape, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    e.vmc_steps(1)
+    out = e.walkers(xp, rp)
+    assert out[0] is xp and out[1] is rp
+    x1, r1 = e.walkers()
+    assert np.array_equal(xp, x1) and np.array_equal(rp, r1)
+    e.set_walkers(xp, rp)                # from pinned buffers: the same walkers back
+    assert np.array_equal(e.walkers()[0], x1)
+    with pytest.raises(ValueError):
+        e.walkers(np.zeros((36, x.shape[1], 3)), rp)
+    e.close()
