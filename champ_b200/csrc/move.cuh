@@ -663,13 +663,14 @@ __device__ __forceinline__ void jastrow_move_f32_body(const CSys &cs, const WSta
         if (!any) continue;
         float fc[P], fu_[P], fi_[P], fj_[P];
         een_apply1f_multi<NORD, P>(sh_B + (size_t)ic * 2 * NB, y, z, fc, fu_, fi_, fj_);
-        const double c0 = cs.cent[3 * ic], c1 = cs.cent[3 * ic + 1], c2 = cs.cent[3 * ic + 2];
         const float gic = sh_g[ic];
         const float rv[3] = {sh_rv[ic], sh_rv[M + ic], sh_rv[2 * M + ic]};
 #pragma unroll
         for (int q = 0; q < P; q++) {
           if (rri == asym && rrj[q] == asym) continue;  // this pair-centre term is cut
-          const float rj_v[3] = {(float)(xj[q][0] - c0), (float)(xj[q][1] - c1), (float)(xj[q][2] - c2)};
+          // partner-to-centre vector x_j - c = (x_i - c) - (x_i - x_j), from the
+          // FP32 vectors already held (no FP64 difference and conversion per term)
+          const float rj_v[3] = {rv[0] - rvee[q][0], rv[1] - rvee[q][1], rv[2] - rvee[q][2]};
           const float fu = fu_[q] * du_r[q];
           const float fi = fi_[q] * gic;
           const float fj = fj_[q] * (-kap) * hj[q];
